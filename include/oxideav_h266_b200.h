@@ -1,0 +1,309 @@
+/*
+ * oxideav_h266_b200.h — C ABI of the B200-native H.266/VVC in-loop filter chain.
+ *
+ * The chain is the decoder's picture-level filter stage, in the crate's order:
+ * LMCS inverse luma map -> deblocking -> SAO -> ALF (+ CC-ALF).  Every entry
+ * point mirrors one function of the Rust crate oxideav-h266 (v0.0.8) and takes
+ * the same data, restated as plain C structs: sample planes are u16 row-major
+ * with a stride, CU records are in decode order, CTB parameter arrays are in
+ * raster CTB order.  Results are bit-exact with the crate's CPU filters.
+ *
+ * Memory: a picture's plane pointers are either host pointers
+ * (H266_MEM_HOST: the call copies the planes to the device and back) or
+ * device pointers on the context's device (H266_MEM_DEVICE: filtered in
+ * place on the context's stream).  Side information (CU lists, CTB arrays,
+ * APS tables) is always passed in host memory.
+ *
+ * Errors: every function returns H266_OK (0) or a negative H266_ERR_* code
+ * and never aborts; h266_last_error() returns a message for the calling
+ * thread's last failure.  The crate's filter functions are infallible and
+ * panic on malformed input; here malformed input is rejected up front.
+ *
+ * Threading: a context is used by one thread at a time.  Calls on different
+ * contexts may run concurrently.
+ */
+#ifndef OXIDEAV_H266_B200_H
+#define OXIDEAV_H266_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define H266_OK 0
+#define H266_ERR_INVALID_ARGUMENT (-1)
+#define H266_ERR_GRID_MISMATCH (-2)    /* CTB array dims != picture CTB grid   */
+#define H266_ERR_LMCS_CONFORMANCE (-3) /* derive_lmcs rejected the payload      */
+#define H266_ERR_OUT_OF_MEMORY (-4)    /* device allocation failed              */
+#define H266_ERR_TIMEOUT (-5)          /* a bounded device wait expired         */
+#define H266_ERR_CUDA (-6)             /* any other CUDA runtime failure        */
+#define H266_ERR_UNSUPPORTED (-7)      /* input outside the supported subset    */
+#define H266_ERR_NO_DEVICE (-8)        /* no usable CUDA device                 */
+
+/* ---- constants (src/aps.rs:21-33, src/lmcs.rs:42) ---------------------- */
+#define H266_NUM_ALF_FILTERS 25
+#define H266_ALF_LUMA_NUM_COEFF 12
+#define H266_ALF_CHROMA_NUM_COEFF 6
+#define H266_ALF_CC_NUM_COEFF 7
+#define H266_ALF_MAX_CHROMA_ALT 8
+#define H266_ALF_MAX_CC_FILTERS 4
+#define H266_LMCS_NUM_BINS 16
+/* DeblockCu::qp_c sentinel selecting the legacy QpY + offset arm
+ * (src/deblock.rs:366-368, DEBLOCK_QP_C_LEGACY). */
+#define H266_DEBLOCK_QP_C_LEGACY INT32_MIN
+
+typedef enum h266_mem_kind { H266_MEM_HOST = 0, H266_MEM_DEVICE = 1 } h266_mem_kind;
+
+/* ---- picture buffers (src/reconstruct.rs:41-52, 112-145) --------------- */
+typedef struct h266_plane {
+    uint16_t *samples;  /* row-major, stride * height samples                */
+    uint64_t stride;    /* samples per row, >= width                          */
+    uint32_t width;     /* visible width in samples                           */
+    uint32_t height;    /* visible height in samples                          */
+    uint32_t bit_depth; /* 8..16                                              */
+    uint32_t reserved;
+} h266_plane;
+
+/* PictureBuffer: 4:2:0 luma + two chroma planes of the same bit depth. */
+typedef struct h266_picture {
+    h266_plane luma, cb, cr;
+    uint32_t mem; /* h266_mem_kind of all three sample pointers */
+    uint32_t reserved;
+} h266_picture;
+
+/* ---- deblocking (src/deblock.rs:52-161, 330-394) ----------------------- */
+typedef struct h266_tb_split { /* TbSplit, src/deblock.rs:127-149 */
+    uint8_t vertical;
+    uint8_t n_bounds; /* 1..3 */
+    uint8_t luma_only;
+    uint8_t reserved0;
+    uint32_t bounds[3];
+    uint8_t y_coded[4];
+    uint8_t cb_coded[4];
+    uint8_t cr_coded[4];
+} h266_tb_split;
+
+typedef struct h266_tu64_cbf_map { /* Tu64CbfMap, src/deblock.rs:156-161 */
+    uint8_t y[2][2];               /* [tile_y][tile_x] */
+    uint8_t cb[2][2];
+    uint8_t cr[2][2];
+} h266_tu64_cbf_map;
+
+typedef struct h266_deblock_cu { /* DeblockCu, src/deblock.rs:52-122 */
+    uint32_t x, y, w, h;
+    int32_t qp_y;
+    int32_t qp_c[3]; /* [QpCb, QpCr, QpCbCr]; qp_c[0] == H266_DEBLOCK_QP_C_LEGACY -> legacy arm */
+    uint8_t intra, tu_y_coded, tu_cb_coded, tu_cr_coded;
+    uint8_t bdpcm_luma, bdpcm_chroma, plt, joint_cbcr2;
+    uint8_t ciip, ibc, has_num_sb, has_tu64;
+    uint8_t has_tb_split, reserved[3];
+    uint32_t num_sb_x, num_sb_y; /* num_sb = Some((x, y)) when has_num_sb */
+    h266_tu64_cbf_map tu64;      /* tu64 = Some(..) when has_tu64 */
+    h266_tb_split tb_split;      /* tb_split = Some(..) when has_tb_split */
+} h266_deblock_cu;
+
+typedef struct h266_deblock_mv_cell { /* DeblockMvCell, src/deblock.rs:329-337 */
+    uint8_t pred_l0, pred_l1, reserved[2];
+    int32_t poc_l0, poc_l1;
+    int32_t mv_l0[2], mv_l1[2]; /* 1/16 luma sample units */
+} h266_deblock_mv_cell;
+
+typedef struct h266_deblock_mv_grid { /* DeblockMvGrid, src/deblock.rs:344-348 */
+    const h266_deblock_mv_cell *cells;
+    uint64_t cells_w, cells_h;
+} h266_deblock_mv_grid;
+
+typedef struct h266_deblock_params { /* DeblockParams, src/deblock.rs:375-393 */
+    uint32_t disabled;
+    int32_t luma_beta_offset_div2, luma_tc_offset_div2;
+    int32_t cb_beta_offset_div2, cb_tc_offset_div2;
+    int32_t cr_beta_offset_div2, cr_tc_offset_div2;
+    int32_t chroma_qp_offset_cb, chroma_qp_offset_cr;
+    uint32_t bit_depth;
+    uint32_t ctb_log2_size_y;
+} h266_deblock_params;
+
+/* ---- SAO (src/sao.rs:53-340) ------------------------------------------- */
+typedef struct h266_sao_ctb { /* SaoCtb, src/sao.rs:134-144 */
+    uint8_t sao_type_idx;     /* 0 not applied, 1 band offset, 2 edge offset */
+    uint8_t eo_class;         /* 0 hor, 1 ver, 2 135deg, 3 45deg */
+    uint8_t band_position;    /* 0..31 */
+    uint8_t reserved;
+    int32_t offset_val[5];    /* SaoOffsetVal after eq. 153; [0] == 0 */
+} h266_sao_ctb;
+
+typedef struct h266_sao_ctb_params { h266_sao_ctb luma, cb, cr; } h266_sao_ctb_params;
+
+typedef struct h266_sao_picture { /* SaoPicture, src/sao.rs:211-217 */
+    uint32_t pic_width_in_ctbs_y, pic_height_in_ctbs_y;
+    const h266_sao_ctb_params *ctbs; /* raster CTB order */
+} h266_sao_picture;
+
+typedef struct h266_sao_config { /* SaoConfig, src/sao.rs:327-340 */
+    uint32_t luma_used, chroma_used, bit_depth, ctb_log2_size_y, chroma_format_idc;
+} h266_sao_config;
+
+/* ---- ALF (src/alf.rs:67-206, src/aps.rs:77-102) ------------------------- */
+typedef struct h266_alf_ctb { /* AlfCtb, src/alf.rs:66-87 */
+    uint8_t luma_on, cb_on, cr_on;
+    uint8_t luma_filt_set_idx; /* <16 fixed set, >=16 APS slot idx-16 */
+    uint8_t cb_alt_idx, cr_alt_idx;
+    uint8_t cc_cb_idc, cc_cr_idc; /* 0 off, k -> CC filter k-1 */
+} h266_alf_ctb;
+
+typedef struct h266_alf_picture { /* AlfPicture, src/alf.rs:90-96 */
+    uint32_t pic_width_in_ctbs_y, pic_height_in_ctbs_y;
+    const h266_alf_ctb *ctbs;
+} h266_alf_picture;
+
+typedef struct h266_alf_config { /* AlfConfig, src/alf.rs:136-158 */
+    uint32_t alf_enabled, cb_enabled, cr_enabled, cc_cb_enabled, cc_cr_enabled;
+    uint32_t bit_depth, ctb_log2_size_y, chroma_format_idc;
+} h266_alf_config;
+
+/* AlfApsData (src/aps.rs:77-102) with its Vec fields as fixed arrays plus
+ * explicit lengths.  n_luma_filters must be 25 when the luma flag is set. */
+typedef struct h266_alf_aps_data {
+    uint8_t alf_luma_filter_signal_flag, alf_chroma_filter_signal_flag;
+    uint8_t alf_cc_cb_filter_signal_flag, alf_cc_cr_filter_signal_flag;
+    uint8_t alf_luma_clip_flag, alf_chroma_clip_flag, reserved[2];
+    uint32_t alf_chroma_num_alt_filters_minus1;
+    uint32_t n_luma_filters;   /* luma_coeff.len()  */
+    uint32_t n_chroma_filters; /* chroma_coeff.len() (0..8) */
+    uint32_t n_cc_cb_filters;  /* cc_cb_coeff.len() (0..4) */
+    uint32_t n_cc_cr_filters;  /* cc_cr_coeff.len() (0..4) */
+    int32_t luma_coeff[H266_NUM_ALF_FILTERS][H266_ALF_LUMA_NUM_COEFF];
+    uint8_t luma_clip_idx[H266_NUM_ALF_FILTERS][H266_ALF_LUMA_NUM_COEFF];
+    int32_t chroma_coeff[H266_ALF_MAX_CHROMA_ALT][H266_ALF_CHROMA_NUM_COEFF];
+    uint8_t chroma_clip_idx[H266_ALF_MAX_CHROMA_ALT][H266_ALF_CHROMA_NUM_COEFF];
+    int32_t cc_cb_coeff[H266_ALF_MAX_CC_FILTERS][H266_ALF_CC_NUM_COEFF];
+    int32_t cc_cr_coeff[H266_ALF_MAX_CC_FILTERS][H266_ALF_CC_NUM_COEFF];
+} h266_alf_aps_data;
+
+typedef struct h266_alf_aps_binding { /* AlfApsBinding, src/alf.rs:179-195 */
+    const h266_alf_aps_data *const *luma_apses; /* entries may be NULL (None) */
+    uint32_t n_luma_apses;
+    uint32_t reserved;
+    const h266_alf_aps_data *chroma_aps; /* NULL = None */
+    const h266_alf_aps_data *cc_cb_aps;
+    const h266_alf_aps_data *cc_cr_aps;
+} h266_alf_aps_binding;
+
+/* ---- LMCS (src/lmcs.rs:50-153) ----------------------------------------- */
+typedef struct h266_lmcs_data { /* LmcsData, src/lmcs.rs:50-76 */
+    uint8_t lmcs_min_bin_idx, lmcs_delta_max_bin_idx, lmcs_delta_cw_prec_minus1;
+    uint8_t lmcs_delta_abs_crs, lmcs_delta_sign_crs_flag, reserved[3];
+    uint32_t lmcs_delta_abs_cw[H266_LMCS_NUM_BINS];
+    uint8_t lmcs_delta_sign_cw_flag[H266_LMCS_NUM_BINS];
+} h266_lmcs_data;
+
+typedef struct h266_lmcs_derived { /* LmcsDerived, src/lmcs.rs:126-153 */
+    uint32_t bit_depth, org_cw;
+    uint32_t lmcs_cw[H266_LMCS_NUM_BINS];
+    uint32_t input_pivot[H266_LMCS_NUM_BINS];
+    uint32_t lmcs_pivot[H266_LMCS_NUM_BINS + 1];
+    uint32_t scale_coeff[H266_LMCS_NUM_BINS];
+    uint32_t inv_scale_coeff[H266_LMCS_NUM_BINS];
+    int32_t lmcs_delta_crs;
+    uint32_t chroma_scale_coeff[H266_LMCS_NUM_BINS];
+} h266_lmcs_derived;
+
+/* ---- whole chain (src/ctu.rs:11822-12065) ------------------------------- */
+typedef struct h266_in_loop_filter_args {
+    /* LMCS inverse map before deblocking (src/ctu.rs:11837-11851); NULL = off */
+    const h266_lmcs_derived *lmcs;
+    uint32_t lmcs_min_bin_idx, lmcs_max_bin_idx;
+    /* deblocking inputs (src/ctu.rs:12006-12025) */
+    const h266_deblock_cu *cus;
+    uint64_t n_cus;
+    const h266_deblock_cu *chroma_cus; /* NULL = share the luma records */
+    uint64_t n_chroma_cus;
+    const h266_deblock_mv_grid *mv_grid; /* NULL = None */
+    h266_deblock_params deblock;
+    uint32_t chroma_format_idc;
+    uint32_t reserved0;
+    const uint32_t *no_filter_cols;
+    uint64_t n_no_filter_cols;
+    const uint32_t *no_filter_rows;
+    uint64_t n_no_filter_rows;
+    /* SAO (src/ctu.rs:12026-12040); sao == NULL skips the pass */
+    const h266_sao_picture *sao;
+    h266_sao_config sao_cfg;
+    uint32_t reserved1;
+    /* ALF (src/ctu.rs:12046-12063); alf == NULL skips the pass */
+    const h266_alf_picture *alf;
+    h266_alf_config alf_cfg;
+    const h266_alf_aps_binding *alf_binding;
+    /* SAO / ALF clip bounds (0, gated lines..., extent); clip_cols == NULL = None */
+    const uint32_t *clip_cols;
+    uint64_t n_clip_cols;
+    const uint32_t *clip_rows;
+    uint64_t n_clip_rows;
+} h266_in_loop_filter_args;
+
+/* ---- context ------------------------------------------------------------ */
+typedef struct h266_ctx h266_ctx;
+
+/* Create a context on CUDA device `device` with its own stream and device
+ * scratch.  Fails with H266_ERR_NO_DEVICE when the device is absent. */
+int h266_ctx_create(int device, h266_ctx **out);
+int h266_ctx_destroy(h266_ctx *ctx);
+/* Use the caller's cudaStream_t (passed as void*) for later device work;
+ * NULL restores the context's own stream. */
+int h266_ctx_set_stream(h266_ctx *ctx, void *cuda_stream);
+/* Block until all work queued on the context's stream has finished. */
+int h266_ctx_synchronize(h266_ctx *ctx);
+/* Message for the calling thread's last failed call ("" if none). */
+const char *h266_last_error(void);
+/* Number of kernels this context has launched since creation. */
+uint64_t h266_ctx_kernel_launches(const h266_ctx *ctx);
+
+/* ---- filters ------------------------------------------------------------ */
+
+/* LmcsData::derive / derive_lmcs (src/lmcs.rs:113, 302-404): the §7.4.3.19
+ * derivations with every conformance check.  Host-only arithmetic.
+ * Returns H266_ERR_LMCS_CONFORMANCE where the crate returns Err. */
+int h266_derive_lmcs(const h266_lmcs_data *data, uint32_t bit_depth, h266_lmcs_derived *out);
+
+/* Whole-plane LMCS inverse luma map, the loop at src/ctu.rs:11837-11851 over
+ * LmcsDerived::idx_y_inv + inverse_map_luma_sample (src/lmcs.rs:209, 230). */
+int h266_lmcs_inverse_map_luma(h266_ctx *ctx, h266_picture *pic, const h266_lmcs_derived *lmcs,
+                               uint32_t lmcs_min_bin_idx, uint32_t lmcs_max_bin_idx);
+
+/* apply_deblocking_clipped (src/deblock.rs:497-617). chroma_cus may be NULL
+ * (None), mv_grid may be NULL (None). */
+int h266_apply_deblocking_clipped(h266_ctx *ctx, h266_picture *pic, const h266_deblock_cu *cus,
+                                  uint64_t n_cus, const h266_deblock_cu *chroma_cus,
+                                  uint64_t n_chroma_cus, const h266_deblock_mv_grid *mv_grid,
+                                  const h266_deblock_params *params, uint32_t chroma_format_idc,
+                                  const uint32_t *no_filter_cols, uint64_t n_no_filter_cols,
+                                  const uint32_t *no_filter_rows, uint64_t n_no_filter_rows);
+
+/* apply_sao_clipped (src/sao.rs:389-497). col_bd == NULL means no tile bounds. */
+int h266_apply_sao_clipped(h266_ctx *ctx, h266_picture *pic, const h266_sao_picture *sao_pic,
+                           const h266_sao_config *cfg, const uint32_t *col_bd, uint64_t n_col_bd,
+                           const uint32_t *row_bd, uint64_t n_row_bd);
+
+/* apply_alf_clipped (src/alf.rs:235-434), CC-ALF included. */
+int h266_apply_alf_clipped(h266_ctx *ctx, h266_picture *pic, const h266_alf_picture *alf_pic,
+                           const h266_alf_config *cfg, const h266_alf_aps_binding *binding,
+                           const uint32_t *col_bd, uint64_t n_col_bd, const uint32_t *row_bd,
+                           uint64_t n_row_bd);
+
+/* CtuWalker::apply_in_loop_filters_with_alf (src/ctu.rs:11822-12065) after its
+ * gate lists are built: LMCS inverse -> deblock -> SAO -> ALF in one call. */
+int h266_apply_in_loop_filters(h266_ctx *ctx, h266_picture *pic, const h266_in_loop_filter_args *args);
+
+/* Batched form of h266_apply_in_loop_filters: n independent pictures (any mix
+ * of sizes and bit depths) filtered by shared launches.  No counterpart in
+ * the crate, which filters one picture per call (src/stream.rs:768). */
+int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *const *pics,
+                                     const h266_in_loop_filter_args *const *args);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OXIDEAV_H266_B200_H */
