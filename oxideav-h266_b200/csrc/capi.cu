@@ -1,0 +1,676 @@
+// C ABI of the filter chain: contexts, argument validation, side-information
+// packing and the per-filter / whole-chain entry points declared in
+// include/oxideav_h266_b200.h.
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <string>
+
+#include "fixed_filters.h"
+#include "internal.h"
+
+static_assert(sizeof(h266_plane) == 32, "h266_plane");
+static_assert(sizeof(h266_picture) == 104, "h266_picture");
+static_assert(sizeof(h266_deblock_cu) == 96, "h266_deblock_cu");
+static_assert(sizeof(h266_deblock_mv_cell) == 28, "h266_deblock_mv_cell");
+static_assert(sizeof(h266_deblock_params) == 44, "h266_deblock_params");
+static_assert(sizeof(h266_sao_ctb) == 24, "h266_sao_ctb");
+static_assert(sizeof(h266_sao_ctb_params) == 72, "h266_sao_ctb_params");
+static_assert(sizeof(h266_alf_ctb) == 8, "h266_alf_ctb");
+static_assert(sizeof(h266_alf_aps_data) == 1992, "h266_alf_aps_data");
+static_assert(sizeof(h266_lmcs_data) == 88, "h266_lmcs_data");
+static_assert(sizeof(h266_lmcs_derived) == 400, "h266_lmcs_derived");
+static_assert(sizeof(h266_in_loop_filter_args) == 256, "h266_in_loop_filter_args");
+
+namespace h266 {
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const std::string &msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int cuda_error(cudaError_t e, const char *what) {
+  const int code = e == cudaErrorMemoryAllocation ? H266_ERR_OUT_OF_MEMORY : H266_ERR_CUDA;
+  return set_error(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int DevBuf::ensure(size_t bytes) {
+  if (bytes <= cap) return H266_OK;
+  if (ptr) H266_CUDA(cudaDeviceSynchronize());  // queued work may still read the old allocation
+  release();
+  size_t want = std::max<size_t>(bytes, 256);
+  want = want + want / 4;  // headroom against regrowth
+  H266_CUDA(cudaMalloc(&ptr, want));
+  cap = want;
+  return H266_OK;
+}
+
+void DevBuf::release() {
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  cap = 0;
+}
+
+// Pinned host staging for one side-information upload per call.
+struct Staging {
+  uint8_t *ptr = nullptr;
+  size_t cap = 0, used = 0;
+  int ensure(size_t bytes) {
+    if (bytes <= cap) return H266_OK;
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    size_t want = bytes + bytes / 4 + 4096;
+    H266_CUDA(cudaHostAlloc((void **)&ptr, want, cudaHostAllocDefault));
+    cap = want;
+    return H266_OK;
+  }
+};
+
+}  // namespace h266
+
+using namespace h266;
+
+struct h266_ctx {
+  int device = 0;
+  cudaStream_t own = nullptr, stream = nullptr;
+  cudaEvent_t staged = nullptr;  // last side-information upload done reading the staging buffer
+  uint64_t launches = 0;
+  DevBuf io[3];       // device copies of host pictures
+  DevBuf scratch[3];  // deblocked planes read by the SAO / ALF pass
+  DevBuf lut;         // LMCS inverse LUT
+  DevBuf side;        // side information
+  Staging stage;
+  DeblockPlan plan;
+  std::vector<uint8_t> blob;  // side information assembled on the host
+};
+
+namespace {
+
+struct Guard {  // makes the context's device current for the call
+  int prev = -1;
+  explicit Guard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~Guard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+int check_ctx(h266_ctx *ctx) { return ctx ? H266_OK : set_error(H266_ERR_INVALID_ARGUMENT, "NULL context"); }
+
+int check_picture(const h266_picture *pic) {
+  if (!pic) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL picture");
+  if (pic->mem != H266_MEM_HOST && pic->mem != H266_MEM_DEVICE)
+    return set_error(H266_ERR_INVALID_ARGUMENT, "picture.mem must be H266_MEM_HOST or H266_MEM_DEVICE");
+  const h266_plane *pl[3] = {&pic->luma, &pic->cb, &pic->cr};
+  for (int i = 0; i < 3; ++i) {
+    const h266_plane &p = *pl[i];
+    if (p.width > 65535 || p.height > 65535) return set_error(H266_ERR_UNSUPPORTED, "plane larger than 65535");
+    if ((uint64_t)p.width * p.height == 0) continue;
+    if (!p.samples) return set_error(H266_ERR_INVALID_ARGUMENT, "plane samples pointer is NULL");
+    if (p.stride < p.width) return set_error(H266_ERR_INVALID_ARGUMENT, "plane stride < width");
+    if (p.bit_depth < 8 || p.bit_depth > 16) return set_error(H266_ERR_INVALID_ARGUMENT, "plane bit_depth must be 8..16");
+  }
+  if ((uint64_t)pic->luma.width * pic->luma.height == 0)
+    return set_error(H266_ERR_INVALID_ARGUMENT, "empty luma plane");
+  return H266_OK;
+}
+
+DPlane dplane(const h266_plane &p, uint16_t *ptr, int64_t stride) {
+  return DPlane{ptr, stride, (int)p.width, (int)p.height};
+}
+
+// Device views of the picture: the caller's planes (device memory) or the
+// context's copies of them (host memory, uploaded here).
+int picture_to_device(h266_ctx *ctx, const h266_picture &pic, DPlane out[3]) {
+  const h266_plane *pl[3] = {&pic.luma, &pic.cb, &pic.cr};
+  for (int i = 0; i < 3; ++i) {
+    const h266_plane &p = *pl[i];
+    const bool empty = (uint64_t)p.width * p.height == 0;
+    if (pic.mem == H266_MEM_DEVICE || empty) {
+      out[i] = dplane(p, p.samples, (int64_t)std::max<uint64_t>(p.stride, 1));
+      continue;
+    }
+    const size_t row = (size_t)p.width * 2;
+    H266_TRY(ctx->io[i].ensure(row * p.height));
+    H266_CUDA(cudaMemcpy2DAsync(ctx->io[i].ptr, row, p.samples, (size_t)p.stride * 2, row, p.height,
+                                cudaMemcpyHostToDevice, ctx->stream));
+    out[i] = dplane(p, ctx->io[i].as<uint16_t>(), p.width);
+  }
+  return H266_OK;
+}
+
+int picture_from_device(h266_ctx *ctx, const h266_picture &pic) {
+  if (pic.mem == H266_MEM_DEVICE) return H266_OK;
+  const h266_plane *pl[3] = {&pic.luma, &pic.cb, &pic.cr};
+  for (int i = 0; i < 3; ++i) {
+    const h266_plane &p = *pl[i];
+    if ((uint64_t)p.width * p.height == 0) continue;
+    const size_t row = (size_t)p.width * 2;
+    H266_CUDA(cudaMemcpy2DAsync(p.samples, (size_t)p.stride * 2, ctx->io[i].ptr, row, row, p.height,
+                                cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  H266_CUDA(cudaStreamSynchronize(ctx->stream));
+  return H266_OK;
+}
+
+// ---------------------------------------------------------------- side-information blob
+struct Blob {
+  std::vector<uint8_t> &b;
+  size_t put(const void *p, size_t n) {  // 256-byte aligned sections
+    size_t off = (b.size() + 255) & ~(size_t)255;
+    b.resize(off + n);
+    if (n) std::memcpy(b.data() + off, p, n);
+    return off;
+  }
+};
+
+int upload_blob(h266_ctx *ctx, uint8_t **dev_base) {
+  const size_t n = ctx->blob.size();
+  H266_TRY(ctx->side.ensure(n));
+  H266_CUDA(cudaEventSynchronize(ctx->staged));  // previous upload finished reading the staging buffer
+  H266_TRY(ctx->stage.ensure(n));
+  std::memcpy(ctx->stage.ptr, ctx->blob.data(), n);
+  H266_CUDA(cudaMemcpyAsync(ctx->side.ptr, ctx->stage.ptr, n, cudaMemcpyHostToDevice, ctx->stream));
+  H266_CUDA(cudaEventRecord(ctx->staged, ctx->stream));
+  *dev_base = ctx->side.as<uint8_t>();
+  return H266_OK;
+}
+
+// ---------------------------------------------------------------- pass-2 tables
+void chroma_sub(uint32_t cfi, int &sw, int &sh) {  // SaoConfig / AlfConfig::chroma_subsampling
+  sw = cfi == 1 || cfi == 2 ? 2 : 1;
+  sh = cfi == 1 ? 2 : 1;
+}
+
+// `span` of apply_sao_clipped (src/sao.rs:429-436) / clip_rect_for_ctb (src/alf.rs:1084-1091)
+void span(const uint32_t *b, uint64_t n, uint32_t v, int mx, int &lo, int &hi) {
+  for (uint64_t i = 0; i + 1 < n; ++i)
+    if (v >= b[i] && v < b[i + 1]) {
+      lo = (int)b[i];
+      hi = std::min((int)b[i + 1], mx);
+      return;
+    }
+  lo = 0;
+  hi = mx;
+}
+
+int alf_clip_value(int bd, int idx) {  // Table 8 (resolve_clip_value, src/alf.rs:627-644)
+  static const int kDrop[4] = {0, 3, 5, 7};
+  bd = std::min(std::max(bd, 8), 16);
+  return 1 << (bd - kDrop[idx & 3]);
+}
+
+struct Pass2Inputs {
+  const h266_sao_picture *sao = nullptr;
+  const h266_sao_config *sao_cfg = nullptr;
+  const h266_alf_picture *alf = nullptr;
+  const h266_alf_config *alf_cfg = nullptr;
+  const h266_alf_aps_binding *binding = nullptr;
+  const uint32_t *cols = nullptr, *rows = nullptr;
+  uint64_t n_cols = 0, n_rows = 0;
+};
+
+struct Pass2Host {
+  std::vector<CtbDev> ctbs;
+  std::vector<int32_t> luma_tab;  // slots * 600: coeff[300] then clip[300]
+  Pass2Args args;
+  bool do_sao = false, do_alf = false;
+};
+
+int check_bounds(const uint32_t *b, uint64_t n, uint32_t extent, uint32_t ctb, const char *what) {
+  if (n && !b) return set_error(H266_ERR_INVALID_ARGUMENT, std::string(what) + ": NULL list");
+  for (uint64_t i = 0; i < n; ++i)
+    if (b[i] < extent && b[i] % ctb != 0)
+      return set_error(H266_ERR_UNSUPPORTED, std::string(what) + ": clip bound not on the CTB grid");
+  return H266_OK;
+}
+
+int build_pass2(const h266_picture &pic, const Pass2Inputs &in, Pass2Host &h) {
+  Pass2Args &a = h.args;
+  std::memset(&a, 0, sizeof a);
+  const bool sao_on = in.sao && in.sao_cfg && (in.sao_cfg->luma_used || in.sao_cfg->chroma_used);
+  const bool alf_on = in.alf && in.alf_cfg && in.alf_cfg->alf_enabled;
+  h.do_sao = sao_on;
+  h.do_alf = alf_on;
+  if (!sao_on && !alf_on) return H266_OK;
+  uint32_t bd = 0, log2 = 0, cfi = 0;
+  if (sao_on) {
+    bd = in.sao_cfg->bit_depth;
+    log2 = in.sao_cfg->ctb_log2_size_y;
+    cfi = in.sao_cfg->chroma_format_idc;
+  }
+  if (alf_on) {
+    if (sao_on && (in.alf_cfg->bit_depth != bd || in.alf_cfg->ctb_log2_size_y != log2 ||
+                   in.alf_cfg->chroma_format_idc != cfi))
+      return set_error(H266_ERR_UNSUPPORTED, "SAO and ALF configs disagree on bit depth / CTB size / chroma format");
+    bd = in.alf_cfg->bit_depth;
+    log2 = in.alf_cfg->ctb_log2_size_y;
+    cfi = in.alf_cfg->chroma_format_idc;
+  }
+  if (bd < 8 || bd > 16) return set_error(H266_ERR_INVALID_ARGUMENT, "SAO/ALF bit_depth must be 8..16");
+  if (log2 < 5 || log2 > 7) return set_error(H266_ERR_UNSUPPORTED, "SAO/ALF need CtbLog2SizeY in 5..7");
+  if (cfi > 3) return set_error(H266_ERR_INVALID_ARGUMENT, "chroma_format_idc must be 0..3");
+  const uint32_t ctb = 1u << log2;
+  H266_TRY(check_bounds(in.cols, in.n_cols, pic.luma.width, ctb, "clip cols"));
+  H266_TRY(check_bounds(in.rows, in.n_rows, pic.luma.height, ctb, "clip rows"));
+  uint32_t wc = 0, hc = 0;
+  if (sao_on) {
+    wc = in.sao->pic_width_in_ctbs_y;
+    hc = in.sao->pic_height_in_ctbs_y;
+    if ((uint64_t)wc * hc && !in.sao->ctbs) return set_error(H266_ERR_INVALID_ARGUMENT, "SaoPicture.ctbs is NULL");
+  }
+  if (alf_on) {
+    if ((uint64_t)in.alf->pic_width_in_ctbs_y * in.alf->pic_height_in_ctbs_y && !in.alf->ctbs)
+      return set_error(H266_ERR_INVALID_ARGUMENT, "AlfPicture.ctbs is NULL");
+    if (sao_on && (in.alf->pic_width_in_ctbs_y != wc || in.alf->pic_height_in_ctbs_y != hc))
+      return set_error(H266_ERR_GRID_MISMATCH, "SaoPicture and AlfPicture CTB grids differ");
+    wc = in.alf->pic_width_in_ctbs_y;
+    hc = in.alf->pic_height_in_ctbs_y;
+  }
+  if ((uint64_t)wc * hc > (1u << 24)) return set_error(H266_ERR_UNSUPPORTED, "CTB grid too large");
+  int sw, sh;
+  chroma_sub(cfi, sw, sh);
+  const int pw = (int)pic.luma.width, ph = (int)pic.luma.height;
+  const bool chroma = cfi != 0 && (uint64_t)pic.cb.width * pic.cb.height + (uint64_t)pic.cr.width * pic.cr.height > 0;
+  const h266_alf_aps_binding *b = in.binding;
+  const h266_alf_aps_data *caps = (alf_on && b) ? b->chroma_aps : nullptr;
+  const h266_alf_aps_data *ccaps[2] = {(alf_on && b) ? b->cc_cb_aps : nullptr, (alf_on && b) ? b->cc_cr_aps : nullptr};
+  if (caps && caps->n_chroma_filters > 8) return set_error(H266_ERR_INVALID_ARGUMENT, "chroma APS: more than 8 filters");
+  if (ccaps[0] && ccaps[0]->n_cc_cb_filters > 4) return set_error(H266_ERR_INVALID_ARGUMENT, "CC-ALF Cb: more than 4 filters");
+  if (ccaps[1] && ccaps[1]->n_cc_cr_filters > 4) return set_error(H266_ERR_INVALID_ARGUMENT, "CC-ALF Cr: more than 4 filters");
+  h.ctbs.assign((size_t)wc * hc, CtbDev{});
+  h.luma_tab.clear();
+  std::map<int, int> slot_of;  // luma_filt_set_idx -> compact slot, -1 = unresolved
+  for (uint32_t ry = 0; ry < hc; ++ry)
+    for (uint32_t rx = 0; rx < wc; ++rx) {
+      CtbDev &d = h.ctbs[(size_t)ry * wc + rx];
+      std::memset(&d, 0, sizeof d);
+      d.luma_set = -1;
+      d.chroma_filt[0] = d.chroma_filt[1] = -1;
+      d.cc_filt[0] = d.cc_filt[1] = -1;
+      int r[4] = {0, 0, pw, ph};
+      if (in.cols) {
+        span(in.cols, in.n_cols, rx * ctb, pw, r[0], r[2]);
+        span(in.rows, in.n_rows, ry * ctb, ph, r[1], r[3]);
+      }
+      for (int k = 0; k < 4; ++k) d.rect[k] = (uint16_t)r[k];
+      if (sao_on) {
+        const h266_sao_ctb_params &s = in.sao->ctbs[(size_t)ry * wc + rx];
+        const h266_sao_ctb *src[3] = {&s.luma, &s.cb, &s.cr};
+        for (int c = 0; c < 3; ++c) {
+          const bool used = c == 0 ? in.sao_cfg->luma_used != 0 : (in.sao_cfg->chroma_used && cfi != 0);
+          const h266_sao_ctb &sc = *src[c];
+          if (!used || (sc.sao_type_idx != 1 && sc.sao_type_idx != 2)) continue;
+          d.sao[c].type = sc.sao_type_idx;
+          d.sao[c].eo_class = sc.eo_class & 3;
+          d.sao[c].band_pos = sc.band_position;
+          for (int k = 0; k < 4; ++k) {
+            if (sc.offset_val[k + 1] < -32768 || sc.offset_val[k + 1] > 32767)
+              return set_error(H266_ERR_UNSUPPORTED, "SAO offset outside int16");
+            d.sao[c].off[k] = (int16_t)sc.offset_val[k + 1];
+          }
+        }
+      }
+      if (alf_on) {
+        const h266_alf_ctb &p = in.alf->ctbs[(size_t)ry * wc + rx];
+        if (p.luma_on) {  // resolve_luma_filter_set, src/alf.rs:564-595
+          const int idx = p.luma_filt_set_idx;
+          auto it = slot_of.find(idx);
+          int slot = -1;
+          if (it != slot_of.end()) {
+            slot = it->second;
+          } else {
+            const h266_alf_aps_data *aps = nullptr;
+            bool ok = idx < 16;
+            if (!ok && b && (uint32_t)(idx - 16) < b->n_luma_apses && b->luma_apses && b->luma_apses[idx - 16]) {
+              aps = b->luma_apses[idx - 16];
+              ok = aps->alf_luma_filter_signal_flag != 0;
+              if (ok && aps->n_luma_filters < 25)
+                return set_error(H266_ERR_INVALID_ARGUMENT, "luma APS signals fewer than 25 filters");
+            }
+            if (ok) {
+              slot = (int)(h.luma_tab.size() / 600);
+              h.luma_tab.resize(h.luma_tab.size() + 600);
+              int32_t *t = &h.luma_tab[(size_t)slot * 600];
+              for (int c = 0; c < 25; ++c)
+                for (int j = 0; j < 12; ++j) {
+                  t[c * 12 + j] = idx < 16 ? kFixedSetCoeff[(idx * 25 + c) * 12 + j] : aps->luma_coeff[c][j];
+                  t[300 + c * 12 + j] = alf_clip_value((int)bd, idx < 16 ? 0 : aps->luma_clip_idx[c][j]);
+                }
+            }
+            slot_of[idx] = slot;
+          }
+          d.luma_set = (int16_t)slot;
+        }
+        if (chroma) {
+          const uint32_t en[2] = {in.alf_cfg->cb_enabled && p.cb_on, in.alf_cfg->cr_enabled && p.cr_on};
+          const uint8_t alt[2] = {p.cb_alt_idx, p.cr_alt_idx};
+          for (int c = 0; c < 2; ++c)
+            if (en[c] && caps && caps->alf_chroma_filter_signal_flag && alt[c] < caps->n_chroma_filters)
+              d.chroma_filt[c] = (int8_t)alt[c];
+          const uint32_t cen[2] = {in.alf_cfg->cc_cb_enabled && p.cc_cb_idc != 0,
+                                   in.alf_cfg->cc_cr_enabled && p.cc_cr_idc != 0};
+          const uint8_t idc[2] = {p.cc_cb_idc, p.cc_cr_idc};
+          for (int c = 0; c < 2; ++c) {
+            if (!cen[c] || !ccaps[c]) continue;
+            const uint32_t n = c == 0 ? ccaps[c]->n_cc_cb_filters : ccaps[c]->n_cc_cr_filters;
+            if ((uint32_t)(idc[c] - 1) < n) d.cc_filt[c] = (int8_t)(idc[c] - 1);
+          }
+        }
+      }
+    }
+  if (caps)
+    for (uint32_t f = 0; f < caps->n_chroma_filters; ++f)
+      for (int k = 0; k < 6; ++k) {
+        a.tables.chroma_coeff[f][k] = caps->chroma_coeff[f][k];
+        a.tables.chroma_clip[f][k] = alf_clip_value((int)bd, caps->chroma_clip_idx[f][k]);
+      }
+  for (int c = 0; c < 2; ++c)
+    if (ccaps[c])
+      for (int f = 0; f < 4; ++f)
+        for (int k = 0; k < 7; ++k) a.tables.cc_coeff[c][f][k] = c == 0 ? ccaps[c]->cc_cb_coeff[f][k] : ccaps[c]->cc_cr_coeff[f][k];
+  a.bit_depth = (int)bd;
+  a.ctb_log2 = (int)log2;
+  a.sub_w = sw;
+  a.sub_h = sh;
+  a.chroma = chroma ? 1 : 0;
+  a.w_ctbs = (int)wc;
+  a.h_ctbs = (int)hc;
+  a.pic_w = pw;
+  a.pic_h = ph;
+  a.ext_w = std::max<int>(pw, (int)pic.cb.width * sw);
+  a.ext_w = std::max<int>(a.ext_w, (int)pic.cr.width * sw);
+  a.ext_h = std::max<int>(ph, (int)pic.cb.height * sh);
+  a.ext_h = std::max<int>(a.ext_h, (int)pic.cr.height * sh);
+  a.tiles_x = (a.ext_w + 31) / 32;
+  a.tiles_y = (a.ext_h + 31) / 32;
+  a.has_clip = in.cols != nullptr;
+  a.sao_luma = sao_on && in.sao_cfg->luma_used;
+  a.sao_chroma = sao_on && in.sao_cfg->chroma_used && cfi != 0;
+  return H266_OK;
+}
+
+// Side information of one call, assembled into ctx->blob and uploaded once.
+struct Staged {
+  size_t ctb = 0, tab = 0, seg[2] = {0, 0}, comp[2] = {0, 0};
+  uint8_t *base = nullptr;
+};
+
+void stage_deblock(h266_ctx *ctx, Staged &st) {
+  Blob blob{ctx->blob};
+  DeblockPlan &pl = ctx->plan;
+  for (int d = 0; d < 2; ++d) {
+    st.seg[d] = blob.put(pl.segs[d].data(), pl.segs[d].size() * sizeof(EdgeSeg));
+    st.comp[d] = blob.put(pl.comp[d].data(), pl.comp[d].size() * sizeof(uint32_t));
+  }
+}
+
+void stage_pass2(h266_ctx *ctx, const Pass2Host &h, Staged &st) {
+  Blob blob{ctx->blob};
+  st.ctb = blob.put(h.ctbs.data(), h.ctbs.size() * sizeof(CtbDev));
+  st.tab = blob.put(h.luma_tab.data(), h.luma_tab.size() * sizeof(int32_t));
+}
+
+// Runs pass 2 (SAO and/or ALF) from `src` into the picture planes `dst`.
+int run_pass2(h266_ctx *ctx, Pass2Host &h, const Staged &st, const DPlane src[3], const DPlane dst[3]) {
+  Pass2Args &a = h.args;
+  for (int i = 0; i < 3; ++i) {
+    a.src[i] = src[i];
+    a.dst[i] = dst[i];
+  }
+  a.ctbs = reinterpret_cast<const CtbDev *>(st.base + st.ctb);
+  a.tables.luma_coeff = reinterpret_cast<int32_t *>(st.base + st.tab);  // per slot: coeff[300], clip[300]
+  a.tables.luma_clip = a.tables.luma_coeff + 300;
+  return launch_pass2(ctx->stream, a, h.do_sao, h.do_alf, &ctx->launches);
+}
+
+int ensure_scratch(h266_ctx *ctx, const DPlane p[3], DPlane s[3]) {
+  for (int i = 0; i < 3; ++i) {
+    const size_t n = (size_t)std::max(p[i].w, 0) * std::max(p[i].h, 0);
+    H266_TRY(ctx->scratch[i].ensure(std::max<size_t>(n, 1) * 2));
+    s[i] = DPlane{ctx->scratch[i].as<uint16_t>(), std::max(p[i].w, 1), p[i].w, p[i].h};
+  }
+  return H266_OK;
+}
+
+int run_deblock(h266_ctx *ctx, const Staged &st, const DPlane planes[3], int bd) {
+  DeblockPlan &pl = ctx->plan;
+  return launch_deblock(ctx->stream, planes, bd, reinterpret_cast<const EdgeSeg *>(st.base + st.seg[0]),
+                        reinterpret_cast<const uint32_t *>(st.base + st.comp[0]), (uint32_t)pl.comp[0].size() - 1,
+                        reinterpret_cast<const EdgeSeg *>(st.base + st.seg[1]),
+                        reinterpret_cast<const uint32_t *>(st.base + st.comp[1]), (uint32_t)pl.comp[1].size() - 1,
+                        &ctx->launches);
+}
+
+int check_lmcs(const h266_lmcs_derived *l, uint32_t mn, uint32_t mx) {
+  if (!l) return H266_OK;
+  if (l->bit_depth < 8 || l->bit_depth > 16) return set_error(H266_ERR_INVALID_ARGUMENT, "LMCS bit_depth must be 8..16");
+  if (mn > 15 || mx > 15) return set_error(H266_ERR_INVALID_ARGUMENT, "LMCS bin index out of range");
+  return H266_OK;
+}
+
+// The chain for one picture whose planes are already device views `P`.
+int chain_on_device(h266_ctx *ctx, const h266_picture &pic, const DPlane P[3], const h266_in_loop_filter_args &a) {
+  H266_TRY(check_lmcs(a.lmcs, a.lmcs_min_bin_idx, a.lmcs_max_bin_idx));
+  H266_TRY(build_deblock_plan(pic, a.cus, a.n_cus, a.chroma_cus, a.n_chroma_cus, a.mv_grid, a.deblock,
+                              a.chroma_format_idc, a.no_filter_cols, a.n_no_filter_cols, a.no_filter_rows,
+                              a.n_no_filter_rows, ctx->plan));
+  Pass2Inputs in;
+  in.sao = a.sao;
+  in.sao_cfg = a.sao ? &a.sao_cfg : nullptr;
+  in.alf = a.alf;
+  in.alf_cfg = a.alf ? &a.alf_cfg : nullptr;
+  in.binding = a.alf_binding;
+  in.cols = a.clip_cols;
+  in.rows = a.clip_rows;
+  in.n_cols = a.n_clip_cols;
+  in.n_rows = a.n_clip_rows;
+  if (a.clip_cols && !a.clip_rows) return set_error(H266_ERR_INVALID_ARGUMENT, "clip_rows is NULL while clip_cols is not");
+  Pass2Host h;
+  H266_TRY(build_pass2(pic, in, h));
+  const uint16_t *lut = nullptr;
+  if (a.lmcs) {
+    H266_TRY(ctx->lut.ensure(65536 * 2));
+    H266_TRY(launch_lmcs_lut(ctx->stream, ctx->lut.as<uint16_t>(), *a.lmcs, a.lmcs_min_bin_idx, a.lmcs_max_bin_idx,
+                             &ctx->launches));
+    lut = ctx->lut.as<uint16_t>();
+  }
+  const int dbd = (int)a.deblock.bit_depth;
+  Staged st;
+  ctx->blob.clear();
+  stage_deblock(ctx, st);
+  if (h.do_sao || h.do_alf) stage_pass2(ctx, h, st);
+  H266_TRY(upload_blob(ctx, &st.base));
+  if (!h.do_sao && !h.do_alf) {  // everything in place on the picture
+    if (lut) H266_TRY(launch_plane_map(ctx->stream, P[0], P[0], lut, &ctx->launches));
+    return run_deblock(ctx, st, P, dbd);
+  }
+  DPlane S[3];
+  H266_TRY(ensure_scratch(ctx, P, S));
+  for (int i = 0; i < 3; ++i) H266_TRY(launch_plane_map(ctx->stream, S[i], P[i], i == 0 ? lut : nullptr, &ctx->launches));
+  H266_TRY(run_deblock(ctx, st, S, dbd));
+  return run_pass2(ctx, h, st, S, P);
+}
+
+}  // namespace
+
+// ======================================================================= C ABI
+extern "C" {
+
+const char *h266_last_error(void) { return g_last_error.c_str(); }
+
+int h266_ctx_create(int device, h266_ctx **out) {
+  if (!out) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL out");
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    return set_error(H266_ERR_NO_DEVICE, "no CUDA device");
+  }
+  if (device < 0 || device >= n) return set_error(H266_ERR_NO_DEVICE, "device ordinal out of range");
+  Guard g(device);
+  h266_ctx *c = new h266_ctx();
+  c->device = device;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->staged, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventRecord(c->staged, c->own);
+  if (e != cudaSuccess) {
+    delete c;
+    return cuda_error(e, "h266_ctx_create");
+  }
+  c->stream = c->own;
+  *out = c;
+  return H266_OK;
+}
+
+int h266_ctx_destroy(h266_ctx *ctx) {
+  if (!ctx) return H266_OK;
+  Guard g(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (int i = 0; i < 3; ++i) {
+    ctx->io[i].release();
+    ctx->scratch[i].release();
+  }
+  ctx->lut.release();
+  ctx->side.release();
+  if (ctx->stage.ptr) cudaFreeHost(ctx->stage.ptr);
+  if (ctx->staged) cudaEventDestroy(ctx->staged);
+  if (ctx->own) cudaStreamDestroy(ctx->own);
+  delete ctx;
+  return H266_OK;
+}
+
+int h266_ctx_set_stream(h266_ctx *ctx, void *stream) {
+  H266_TRY(check_ctx(ctx));
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own;
+  return H266_OK;
+}
+
+int h266_ctx_synchronize(h266_ctx *ctx) {
+  H266_TRY(check_ctx(ctx));
+  Guard g(ctx->device);
+  H266_CUDA(cudaStreamSynchronize(ctx->stream));
+  return H266_OK;
+}
+
+uint64_t h266_ctx_kernel_launches(const h266_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+int h266_derive_lmcs(const h266_lmcs_data *data, uint32_t bit_depth, h266_lmcs_derived *out) {
+  return derive_lmcs(data, bit_depth, out);
+}
+
+int h266_lmcs_inverse_map_luma(h266_ctx *ctx, h266_picture *pic, const h266_lmcs_derived *lmcs, uint32_t mn,
+                               uint32_t mx) {
+  H266_TRY(check_ctx(ctx));
+  H266_TRY(check_picture(pic));
+  if (!lmcs) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL lmcs");
+  H266_TRY(check_lmcs(lmcs, mn, mx));
+  Guard g(ctx->device);
+  DPlane P[3];
+  H266_TRY(picture_to_device(ctx, *pic, P));
+  H266_TRY(ctx->lut.ensure(65536 * 2));
+  H266_TRY(launch_lmcs_lut(ctx->stream, ctx->lut.as<uint16_t>(), *lmcs, mn, mx, &ctx->launches));
+  H266_TRY(launch_plane_map(ctx->stream, P[0], P[0], ctx->lut.as<uint16_t>(), &ctx->launches));
+  return picture_from_device(ctx, *pic);
+}
+
+int h266_apply_deblocking_clipped(h266_ctx *ctx, h266_picture *pic, const h266_deblock_cu *cus, uint64_t n_cus,
+                                  const h266_deblock_cu *chroma_cus, uint64_t n_chroma_cus,
+                                  const h266_deblock_mv_grid *mv_grid, const h266_deblock_params *params,
+                                  uint32_t cfi, const uint32_t *nf_cols, uint64_t n_cols, const uint32_t *nf_rows,
+                                  uint64_t n_rows) {
+  H266_TRY(check_ctx(ctx));
+  H266_TRY(check_picture(pic));
+  if (!params) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL params");
+  if ((n_cus && !cus) || (n_cols && !nf_cols) || (n_rows && !nf_rows))
+    return set_error(H266_ERR_INVALID_ARGUMENT, "NULL list with nonzero length");
+  Guard g(ctx->device);
+  H266_TRY(build_deblock_plan(*pic, cus, n_cus, chroma_cus, n_chroma_cus, mv_grid, *params, cfi, nf_cols, n_cols,
+                              nf_rows, n_rows, ctx->plan));
+  DPlane P[3];
+  H266_TRY(picture_to_device(ctx, *pic, P));
+  Staged st;
+  ctx->blob.clear();
+  stage_deblock(ctx, st);
+  H266_TRY(upload_blob(ctx, &st.base));
+  H266_TRY(run_deblock(ctx, st, P, (int)params->bit_depth));
+  return picture_from_device(ctx, *pic);
+}
+
+static int pass2_entry(h266_ctx *ctx, h266_picture *pic, const Pass2Inputs &in) {
+  H266_TRY(check_ctx(ctx));
+  H266_TRY(check_picture(pic));
+  if (in.cols && !in.rows) return set_error(H266_ERR_INVALID_ARGUMENT, "row bounds NULL while col bounds are not");
+  Guard g(ctx->device);
+  Pass2Host h;
+  H266_TRY(build_pass2(*pic, in, h));
+  DPlane P[3];
+  H266_TRY(picture_to_device(ctx, *pic, P));
+  if (h.do_sao || h.do_alf) {
+    Staged st;
+    ctx->blob.clear();
+    stage_pass2(ctx, h, st);
+    H266_TRY(upload_blob(ctx, &st.base));
+    DPlane S[3];
+    H266_TRY(ensure_scratch(ctx, P, S));
+    for (int i = 0; i < 3; ++i) H266_TRY(launch_plane_map(ctx->stream, S[i], P[i], nullptr, &ctx->launches));
+    H266_TRY(run_pass2(ctx, h, st, S, P));
+  }
+  return picture_from_device(ctx, *pic);
+}
+
+int h266_apply_sao_clipped(h266_ctx *ctx, h266_picture *pic, const h266_sao_picture *sao_pic,
+                           const h266_sao_config *cfg, const uint32_t *col_bd, uint64_t n_col, const uint32_t *row_bd,
+                           uint64_t n_row) {
+  if (!sao_pic || !cfg) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL SAO picture / config");
+  Pass2Inputs in;
+  in.sao = sao_pic;
+  in.sao_cfg = cfg;
+  in.cols = col_bd;
+  in.rows = row_bd;
+  in.n_cols = n_col;
+  in.n_rows = n_row;
+  return pass2_entry(ctx, pic, in);
+}
+
+int h266_apply_alf_clipped(h266_ctx *ctx, h266_picture *pic, const h266_alf_picture *alf_pic,
+                           const h266_alf_config *cfg, const h266_alf_aps_binding *binding, const uint32_t *col_bd,
+                           uint64_t n_col, const uint32_t *row_bd, uint64_t n_row) {
+  if (!alf_pic || !cfg) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL ALF picture / config");
+  Pass2Inputs in;
+  in.alf = alf_pic;
+  in.alf_cfg = cfg;
+  in.binding = binding;
+  in.cols = col_bd;
+  in.rows = row_bd;
+  in.n_cols = n_col;
+  in.n_rows = n_row;
+  return pass2_entry(ctx, pic, in);
+}
+
+int h266_apply_in_loop_filters(h266_ctx *ctx, h266_picture *pic, const h266_in_loop_filter_args *args) {
+  H266_TRY(check_ctx(ctx));
+  H266_TRY(check_picture(pic));
+  if (!args) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL args");
+  Guard g(ctx->device);
+  DPlane P[3];
+  H266_TRY(picture_to_device(ctx, *pic, P));
+  H266_TRY(chain_on_device(ctx, *pic, P, *args));
+  return picture_from_device(ctx, *pic);
+}
+
+int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *const *pics,
+                                     const h266_in_loop_filter_args *const *args) {
+  H266_TRY(check_ctx(ctx));
+  if (n && (!pics || !args)) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL batch arrays");
+  for (uint32_t i = 0; i < n; ++i) H266_TRY(h266_apply_in_loop_filters(ctx, pics[i], args[i]));
+  return H266_OK;
+}
+
+}  // extern "C"

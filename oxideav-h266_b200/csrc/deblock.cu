@@ -1,0 +1,676 @@
+// Deblocking (H.266 §8.8.3) for the B200 filter chain.
+//
+// Host side: the reference walks its CU list in decode order and filters every
+// edge segment in place, sequentially (src/deblock.rs:687-983).  The walk's
+// edge derivation -- positions, bS, maxFilterLength, beta / tC -- reads no
+// samples, so it is done up front here and produces an explicit segment list.
+// Segments are then grouped into components: two segments of the same pass
+// and plane that lie on the same 4-line (luma) or 2-line (chroma) band and
+// whose sample footprints overlap along the edge normal are in one component.
+// A segment's footprint is [pos - R(mflP), pos + R(mflQ)) with R(m) = 4 for
+// m <= 3 and m + 1 otherwise: every sample the decision or the filters of
+// src/deblock.rs:1224-2075 read or write lies inside it.  Segments of
+// different components therefore touch disjoint samples and commute; inside
+// a component the segments keep the reference's processing order.  The
+// vertical pass runs to completion before the horizontal one, as in
+// apply_deblocking_clipped (src/deblock.rs:540-615).
+//
+// Device side: one thread per component replays its segments with the
+// reference's clamped reads and bounds-checked Clip1 writes on global memory.
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+#include "internal.h"
+
+namespace h266 {
+namespace {
+
+// ---------------------------------------------------------------- tables
+// Table 43 (β′, tC′) as in src/deblock.rs:401-418.
+const int kBeta[64] = {0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  6,  7,  8,  9,  10, 11,
+                       12, 13, 14, 15, 16, 17, 18, 20, 22, 24, 26, 28, 30, 32, 34, 36, 38, 40, 42, 44, 46, 48,
+                       50, 52, 54, 56, 58, 60, 62, 64, 66, 68, 70, 72, 74, 76, 78, 80, 82, 84, 86, 88};
+const int kTc[66] = {0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,   0,   0,   0,   0,   0,   0,   0,   3,   4,   4,   4,
+                     4,  5,  5,  5,  5,  7,  7,  8,  9,  10, 10,  11,  13,  14,  15,  17,  19,  21,  24,  25,  29,  33,
+                     36, 41, 45, 51, 57, 64, 71, 80, 89, 100, 112, 125, 141, 157, 177, 198, 222, 250, 280, 314, 352, 395};
+
+inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// eqs. 1276-1279 (src/deblock.rs:424-452)
+inline int beta_of(int q, int bd) { return kBeta[clampi(q, 0, 63)] * (1 << (bd - 8)); }
+inline int tc_of(int q, int bd) {
+  int t = kTc[clampi(q, 0, 65)];
+  if (bd < 10) return (t + (1 << (9 - bd))) >> (10 - bd);
+  return t * (1 << (bd - 10));
+}
+
+// ---------------------------------------------------------------- CU geometry
+// The per-CU transform-block queries of src/deblock.rs:163-320, for one CU.
+struct Cu {
+  const h266_deblock_cu &c;
+  uint32_t rel(int lx, int ly, bool vert) const {
+    return vert ? (uint32_t)clampi(lx - (int)c.x, 0, (int)c.w - 1) : (uint32_t)clampi(ly - (int)c.y, 0, (int)c.h - 1);
+  }
+  int split_index(uint32_t r) const {
+    int idx = 0;
+    for (int i = 0; i < c.tb_split.n_bounds; ++i)
+      if (r >= c.tb_split.bounds[i]) idx = i + 1;
+    return idx;
+  }
+  uint32_t split_len(uint32_t r, uint32_t dim) const {
+    uint32_t lo = 0, hi = dim;
+    for (int i = 0; i < c.tb_split.n_bounds; ++i) {
+      if (r < c.tb_split.bounds[i]) {
+        hi = c.tb_split.bounds[i];
+        break;
+      }
+      lo = c.tb_split.bounds[i];
+    }
+    return hi - lo;
+  }
+  bool coded(uint32_t comp, int lx, int ly) const {  // tu_coded_at
+    if (c.has_tu64) {
+      uint32_t tx = std::min(rel(lx, ly, true) / 64, 1u), ty = std::min(rel(lx, ly, false) / 64, 1u);
+      return comp == 0 ? c.tu64.y[ty][tx] : (comp == 1 ? c.tu64.cb[ty][tx] : c.tu64.cr[ty][tx]);
+    }
+    if (c.has_tb_split && (comp == 0 || !c.tb_split.luma_only)) {
+      int i = split_index(rel(lx, ly, c.tb_split.vertical != 0));
+      return comp == 0 ? c.tb_split.y_coded[i] : (comp == 1 ? c.tb_split.cb_coded[i] : c.tb_split.cr_coded[i]);
+    }
+    return comp == 0 ? c.tu_y_coded : (comp == 1 ? c.tu_cb_coded : c.tu_cr_coded);
+  }
+  uint32_t tb_len(int lx, int ly, bool vert, bool chroma) const {  // luma_tb_len / chroma_tb_len (luma units)
+    uint32_t dim = vert ? c.w : c.h;
+    if (c.has_tu64 && dim > 64) return std::min(dim - (rel(lx, ly, vert) / 64) * 64, 64u);
+    if (c.has_tb_split && (c.tb_split.vertical != 0) == vert && !(chroma && c.tb_split.luma_only))
+      return split_len(rel(lx, ly, vert), dim);
+    return dim;
+  }
+  bool tb_boundary(uint32_t off, bool vert, bool chroma) const {  // is_{luma,chroma}_tb_boundary
+    uint32_t dim = vert ? c.w : c.h;
+    if (off == 0 || off >= dim) return false;
+    if (c.has_tu64 && dim > 64) return off % 64 == 0;
+    if (c.has_tb_split && (c.tb_split.vertical != 0) == vert && !(chroma && c.tb_split.luma_only)) {
+      for (int i = 0; i < c.tb_split.n_bounds; ++i)
+        if (c.tb_split.bounds[i] == off) return true;
+    }
+    return false;
+  }
+};
+
+struct MvGrid {
+  const h266_deblock_mv_grid *g;
+  h266_deblock_mv_cell at(int x, int y) const {  // DeblockMvGrid::at_luma
+    h266_deblock_mv_cell d;
+    std::memset(&d, 0, sizeof d);
+    if (!g || x < 0 || y < 0) return d;
+    uint64_t cx = (uint64_t)x / 4, cy = (uint64_t)y / 4;
+    if (cx >= g->cells_w || cy >= g->cells_h) return d;
+    return g->cells[cy * g->cells_w + cx];
+  }
+};
+
+bool mv_far(const int32_t *a, const int32_t *b) { return std::abs(a[0] - b[0]) >= 8 || std::abs(a[1] - b[1]) >= 8; }
+
+// §8.8.3.5 motion arm, src/deblock.rs:992-1045
+bool motion_differs(const h266_deblock_mv_cell &p, const h266_deblock_mv_cell &q) {
+  int np = (p.pred_l0 != 0) + (p.pred_l1 != 0), nq = (q.pred_l0 != 0) + (q.pred_l1 != 0);
+  if (np != nq) return true;
+  if (np == 0) return false;
+  if (np == 1) {
+    int pp = p.pred_l0 ? p.poc_l0 : p.poc_l1, qp = q.pred_l0 ? q.poc_l0 : q.poc_l1;
+    if (pp != qp) return true;
+    return mv_far(p.pred_l0 ? p.mv_l0 : p.mv_l1, q.pred_l0 ? q.mv_l0 : q.mv_l1);
+  }
+  bool straight_refs = p.poc_l0 == q.poc_l0 && p.poc_l1 == q.poc_l1;
+  bool swapped_refs = p.poc_l0 == q.poc_l1 && p.poc_l1 == q.poc_l0;
+  if (!straight_refs && !swapped_refs) return true;
+  bool straight = mv_far(p.mv_l0, q.mv_l0) || mv_far(p.mv_l1, q.mv_l1);
+  bool crossed = mv_far(p.mv_l0, q.mv_l1) || mv_far(p.mv_l1, q.mv_l0);
+  if (p.poc_l0 != p.poc_l1) return straight_refs ? straight : crossed;
+  return straight && crossed;
+}
+
+struct PlaneCfg {
+  uint32_t comp, sub_w, sub_h;
+  int beta_off, tc_off, qp_off, bd;
+  uint32_t ctb;
+};
+
+struct Emitted {
+  EdgeSeg s;
+  uint32_t order;
+};
+
+class Walker {
+ public:
+  Walker(const h266_deblock_cu *cus, size_t n, int pw, int ph) : cus_(cus), n_(n) {
+    cw_ = (pw + 3) / 4;
+    ch_ = (ph + 3) / 4;
+    grid_.assign((size_t)cw_ * ch_, -1);
+    for (size_t i = 0; i < n; ++i) {  // CuGrid::build, later CUs win
+      const h266_deblock_cu &c = cus[i];
+      int x0 = c.x / 4, y0 = c.y / 4;
+      int x1 = std::min<int64_t>(((int64_t)c.x + c.w + 3) / 4, cw_), y1 = std::min<int64_t>(((int64_t)c.y + c.h + 3) / 4, ch_);
+      for (int y = y0; y < y1; ++y)
+        for (int x = x0; x < x1; ++x) grid_[(size_t)y * cw_ + x] = (int64_t)i;
+    }
+  }
+  int64_t at(int x, int y) const {
+    if (x < 0 || y < 0 || x / 4 >= cw_ || y / 4 >= ch_) return -1;
+    return grid_[(size_t)(y / 4) * cw_ + x / 4];
+  }
+  // deblock_cu_dir (src/deblock.rs:707-983) for every CU, recording segments.
+  void walk(const PlaneCfg &pc, bool vert, const MvGrid &mv, const uint32_t *nf, uint64_t n_nf,
+            std::vector<Emitted> &out) const {
+    for (size_t idx = 0; idx < n_; ++idx) walk_cu(pc, vert, mv, nf, n_nf, idx, out);
+  }
+
+ private:
+  void walk_cu(const PlaneCfg &pc, bool vert, const MvGrid &mv, const uint32_t *nf, uint64_t n_nf, size_t idx,
+               std::vector<Emitted> &out) const;
+  const h266_deblock_cu *cus_;
+  size_t n_;
+  int cw_, ch_;
+  std::vector<int64_t> grid_;
+};
+
+int bs_of(uint32_t comp, const h266_deblock_cu &p, const h266_deblock_cu &q, const MvGrid &mv, int px, int py,
+          int qx, int qy, bool is_tb, bool idc2) {  // derive_bs, src/deblock.rs:1055-1119
+  if (comp == 0 ? (p.bdpcm_luma && q.bdpcm_luma) : (p.bdpcm_chroma && q.bdpcm_chroma)) return 0;
+  if (p.intra || q.intra || p.ciip || q.ciip) return 2;
+  if (is_tb && (Cu{p}.coded(comp, px, py) || Cu{q}.coded(comp, qx, qy))) return 1;
+  if (comp != 0 || !idc2) return 0;
+  if ((p.ibc != 0) != (q.ibc != 0)) return 1;
+  if (p.ibc) {
+    if (mv.g) return mv_far(mv.at(px, py).mv_l0, mv.at(qx, qy).mv_l0) ? 1 : 0;
+    return 0;
+  }
+  if (mv.g && motion_differs(mv.at(px, py), mv.at(qx, qy))) return 1;
+  return 0;
+}
+
+void Walker::walk_cu(const PlaneCfg &pc, bool vert, const MvGrid &mv, const uint32_t *nf, uint64_t n_nf, size_t idx,
+                     std::vector<Emitted> &out) const {
+  const h266_deblock_cu &cu = cus_[idx];
+  const bool chroma = pc.comp != 0;
+  if (chroma && ((vert ? cu.x / pc.sub_w : cu.y / pc.sub_h) % 8) != 0) return;
+  const uint32_t n_cb = vert ? cu.w : cu.h, n_other = vert ? cu.h : cu.w, lead = vert ? cu.x : cu.y;
+  bool gated = false;
+  for (uint64_t i = 0; i < n_nf; ++i) gated |= nf[i] == lead;
+  const bool filter_edge = lead != 0 && !gated;
+  const uint32_t step = chroma ? 8 * (vert ? pc.sub_w : pc.sub_h) : 4;
+  const uint32_t seg = chroma ? 2 * (vert ? pc.sub_h : pc.sub_w) : 4;
+  uint32_t nsb = 1;
+  if (!chroma && cu.has_num_sb) nsb = std::max(vert ? cu.num_sb_x : cu.num_sb_y, 1u);
+  const uint32_t sb = std::max(8u, n_cb / nsb), n8 = std::max(n_cb / 8, 1u);
+  const uint32_t last_sb = std::min(n8 - 1, nsb - 1);
+  const uint32_t ctb_h_c = pc.ctb / std::max(pc.sub_h, 1u);
+  Cu q_geo{cu};
+  for (uint32_t off = 0; off < n_cb; off += step) {
+    const bool is_tb = off == 0 ? filter_edge : q_geo.tb_boundary(off, vert, chroma);
+    const bool is_sb = !chroma && off % sb == 0 && off / sb <= last_sb && (off > 0 || filter_edge);
+    if (!is_tb && !is_sb) continue;
+    for (uint32_t k = 0; k < n_other; k += seg) {
+      const int qx = (int)(vert ? cu.x + off : cu.x + k), qy = (int)(vert ? cu.y + k : cu.y + off);
+      const int px = vert ? qx - 1 : qx, py = vert ? qy : qy - 1;
+      int64_t pi = off == 0 ? at(px, py) : (int64_t)idx;
+      if (pi < 0 || (off == 0 && pi == (int64_t)idx)) continue;
+      const h266_deblock_cu &p = cus_[pi];
+      const int bs = bs_of(pc.comp, p, cu, mv, px, py, qx, qy, is_tb, is_sb);
+      if (bs == 0) continue;
+      uint32_t mp, mq;
+      int qp;
+      bool ctb_row = false;
+      if (!chroma) {
+        mp = mq = 0;
+        if (is_tb) {
+          uint32_t wq = q_geo.tb_len(qx, qy, vert, false), wp = Cu{p}.tb_len(px, py, vert, false);
+          if (wp <= 4 || wq <= 4) mp = mq = 1;
+          else {
+            mp = wp >= 32 ? 7 : 3;
+            mq = wq >= 32 ? 7 : 3;
+          }
+        }
+        if (is_sb) {  // §8.8.3.4 overlay, src/deblock.rs:856-901
+          if (off == 0) {
+            if (nsb > 1) mq = std::min(mq, 5u);
+            if (p.has_num_sb) mp = std::min(mp, 5u);
+          } else {
+            auto tb_at = [&](int64_t z) {
+              if (z < 0 || z >= (int64_t)n_cb) return false;
+              return z == 0 ? filter_edge : q_geo.tb_boundary((uint32_t)z, vert, false);
+            };
+            if (is_tb) {
+              mp = std::min(mp, 5u);
+              mq = std::min(mq, 5u);
+            } else if (tb_at((int64_t)off - 4) || tb_at((int64_t)off + 4)) {
+              mp = mq = 1;
+            } else if (off / sb == 1 || off / sb == n8 - 1 || tb_at((int64_t)off - sb) || tb_at((int64_t)off + sb)) {
+              mp = mq = 2;
+            } else {
+              mp = mq = 3;
+            }
+          }
+        }
+        ctb_row = !vert && off == 0 && pc.ctb > 0 && cu.y % pc.ctb == 0;
+        qp = (p.qp_y + cu.qp_y + 1) >> 1;  // eq. 1274 (no LADF)
+      } else {
+        const uint32_t sub = vert ? pc.sub_w : pc.sub_h;
+        const uint32_t wq = q_geo.tb_len(qx, qy, vert, true) / sub, wp = Cu{p}.tb_len(px, py, vert, true) / sub;
+        if (wp >= 8 && wq >= 8) {
+          const bool row = !vert && off == 0 && ctb_h_c > 0 && (cu.y / pc.sub_h) % ctb_h_c == 0;
+          mp = row ? 1 : 3;
+          mq = 3;
+        } else {
+          mp = mq = 1;
+        }
+        auto pick = [&](const h266_deblock_cu &c) {  // src/deblock.rs:1155-1163
+          if (c.qp_c[0] == INT32_MIN) return clampi(c.qp_y + pc.qp_off, 0, 63);
+          if (c.joint_cbcr2) return (int)c.qp_c[2];
+          return (int)c.qp_c[pc.comp == 1 ? 0 : 1];
+        };
+        qp = (pick(p) + pick(cu) + 1) >> 1;  // eq. 1343
+      }
+      const int beta = beta_of(qp + pc.beta_off * 2, pc.bd);
+      const int tc = tc_of(qp + 2 * (bs - 1) + pc.tc_off * 2, pc.bd);
+      if (tc == 0) continue;  // every filter arm is a no-op at tC = 0
+      if (chroma && mp == 1 && mq == 1 && bs != 2) continue;  // src/deblock.rs:1823, 1888
+      Emitted e;
+      e.s.x = (uint16_t)(chroma ? qx / (int)pc.sub_w : qx);
+      e.s.y = (uint16_t)(chroma ? qy / (int)pc.sub_h : qy);
+      e.s.beta = (uint16_t)beta;
+      e.s.tc = (uint16_t)tc;
+      e.s.plane = (uint8_t)pc.comp;
+      e.s.bs = (uint8_t)bs;
+      e.s.mfl = (uint8_t)(mp << 4 | mq);
+      e.s.flags = (uint8_t)((vert ? 1 : 0) | (ctb_row ? 2 : 0) | (p.plt ? 4 : 0) | (cu.plt ? 8 : 0));
+      e.order = (uint32_t)out.size();
+      out.push_back(e);
+    }
+  }
+}
+
+inline int reach(int m) { return m <= 3 ? 4 : m + 1; }
+
+// Groups one (pass, plane) segment list into components and appends them.
+void group(std::vector<Emitted> &segs, std::vector<EdgeSeg> &dst, std::vector<uint32_t> &comp, uint32_t &max_len) {
+  const size_t n = segs.size();
+  if (n == 0) return;
+  struct Key {
+    uint32_t band;
+    int32_t start, end;
+    uint32_t i;
+  };
+  std::vector<Key> keys(n);
+  for (size_t i = 0; i < n; ++i) {
+    const EdgeSeg &s = segs[i].s;
+    const bool vert = s.flags & 1;
+    const int pos = vert ? s.x : s.y;
+    keys[i] = Key{vert ? s.y : s.x, pos - reach(s.mfl >> 4), pos + reach(s.mfl & 15), (uint32_t)i};
+  }
+  std::sort(keys.begin(), keys.end(), [](const Key &a, const Key &b) {
+    return a.band != b.band ? a.band < b.band : (a.start != b.start ? a.start < b.start : a.i < b.i);
+  });
+  std::vector<uint32_t> members;
+  size_t i = 0;
+  while (i < n) {
+    size_t j = i + 1;
+    int32_t end = keys[i].end;
+    while (j < n && keys[j].band == keys[i].band && keys[j].start < end) {
+      end = std::max(end, keys[j].end);
+      ++j;
+    }
+    members.clear();
+    for (size_t t = i; t < j; ++t) members.push_back(keys[t].i);
+    std::sort(members.begin(), members.end(), [&](uint32_t a, uint32_t b) { return segs[a].order < segs[b].order; });
+    comp.push_back((uint32_t)dst.size());
+    for (uint32_t m : members) dst.push_back(segs[m].s);
+    max_len = std::max<uint32_t>(max_len, (uint32_t)(j - i));
+    i = j;
+  }
+}
+
+}  // namespace
+
+int build_deblock_plan(const h266_picture &pic, const h266_deblock_cu *cus, uint64_t n_cus,
+                       const h266_deblock_cu *chroma_cus, uint64_t n_chroma, const h266_deblock_mv_grid *mv,
+                       const h266_deblock_params &params, uint32_t cfi, const uint32_t *nf_cols, uint64_t n_cols,
+                       const uint32_t *nf_rows, uint64_t n_rows, DeblockPlan &plan) {
+  for (int d = 0; d < 2; ++d) {
+    plan.segs[d].clear();
+    plan.comp[d].clear();
+    plan.max_comp_len[d] = 0;
+  }
+  if (params.disabled) return H266_OK;
+  if (params.bit_depth < 8 || params.bit_depth > 16)
+    return set_error(H266_ERR_INVALID_ARGUMENT, "deblock: bit_depth must be 8..16");
+  if (params.ctb_log2_size_y > 16) return set_error(H266_ERR_INVALID_ARGUMENT, "deblock: ctb_log2_size_y too large");
+  const h266_deblock_cu *lists[2] = {cus, chroma_cus};
+  const uint64_t counts[2] = {n_cus, n_chroma};
+  for (int l = 0; l < 2; ++l)
+    for (uint64_t i = 0; i < counts[l]; ++i) {
+      const h266_deblock_cu &c = lists[l][i];
+      // Segment bands are 4-line aligned; every VVC CU lies on the 4x4 grid.
+      if ((c.x | c.y | c.w | c.h) & 3 || c.w == 0 || c.h == 0)
+        return set_error(H266_ERR_UNSUPPORTED, "deblock: CU position/size not on the 4x4 luma grid");
+      if ((uint64_t)c.x + c.w > 65535 || (uint64_t)c.y + c.h > 65535)
+        return set_error(H266_ERR_UNSUPPORTED, "deblock: CU beyond 65535 samples");
+      if (c.has_tb_split && (c.tb_split.n_bounds < 1 || c.tb_split.n_bounds > 3))
+        return set_error(H266_ERR_INVALID_ARGUMENT, "deblock: tb_split.n_bounds must be 1..3");
+    }
+  const int bd = (int)params.bit_depth;
+  const uint32_t ctb = 1u << params.ctb_log2_size_y;
+  const int pw = (int)pic.luma.width, ph = (int)pic.luma.height;
+  MvGrid mvg{mv};
+  std::vector<Emitted> em;
+  Walker luma(cus, n_cus, pw, ph);
+  PlaneCfg lc{0, 1, 1, params.luma_beta_offset_div2, params.luma_tc_offset_div2, 0, bd, ctb};
+  for (int d = 0; d < 2; ++d) {
+    em.clear();
+    luma.walk(lc, d == 0, mvg, d == 0 ? nf_cols : nf_rows, d == 0 ? n_cols : n_rows, em);
+    group(em, plan.segs[d], plan.comp[d], plan.max_comp_len[d]);
+  }
+  if (cfi != 0) {
+    const bool sep = chroma_cus != nullptr;
+    Walker cwalk(sep ? chroma_cus : cus, sep ? n_chroma : n_cus, pw, ph);
+    PlaneCfg cc[2] = {{1, 2, 2, params.cb_beta_offset_div2, params.cb_tc_offset_div2, params.chroma_qp_offset_cb, bd, ctb},
+                      {2, 2, 2, params.cr_beta_offset_div2, params.cr_tc_offset_div2, params.chroma_qp_offset_cr, bd, ctb}};
+    MvGrid none{nullptr};
+    for (int c = 0; c < 2; ++c)
+      for (int d = 0; d < 2; ++d) {
+        em.clear();
+        cwalk.walk(cc[c], d == 0, none, d == 0 ? nf_cols : nf_rows, d == 0 ? n_cols : n_rows, em);
+        group(em, plan.segs[d], plan.comp[d], plan.max_comp_len[d]);
+      }
+  }
+  for (int d = 0; d < 2; ++d) plan.comp[d].push_back((uint32_t)plan.segs[d].size());
+  return H266_OK;
+}
+
+// ===================================================================== device
+namespace {
+
+__device__ __forceinline__ int rdc(const DPlane &p, int x, int y) {
+  x = min(max(x, 0), p.w - 1);
+  y = min(max(y, 0), p.h - 1);
+  return p.s[(int64_t)y * p.stride + x];
+}
+__device__ __forceinline__ void wrc(const DPlane &p, int x, int y, int v, int maxv) {
+  if (x < 0 || y < 0 || x >= p.w || y >= p.h) return;
+  p.s[(int64_t)y * p.stride + x] = (uint16_t)min(max(v, 0), maxv);
+}
+__device__ __forceinline__ int clampd(int v, int lo, int hi) { return min(max(v, lo), hi); }
+
+// One luma edge segment: §8.8.3.6.2 decision + §8.8.3.6.7 / .8 filters
+// (luma_edge_decision / run_luma_filter / short_luma_apply / long_luma_apply,
+// src/deblock.rs:1224-1776).  The decision reads lines 0 and 3 before any
+// write and every line is filtered from its own samples, so the four lines
+// are loaded once: v[k][8 + d] holds the sample at distance d from q0.
+__device__ void luma_segment(const DPlane &P, const EdgeSeg &e, int maxv) {
+  const bool vert = e.flags & 1;
+  const int tc = e.tc, beta = e.beta;
+  int mp = e.mfl >> 4, mq = e.mfl & 15;
+  const int cx = e.x, cy = e.y;
+  int v[4][16];
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int d = -8; d < 8; ++d) v[k][8 + d] = vert ? rdc(P, cx + d, cy + k) : rdc(P, cx + k, cy + d);
+#define PS(i, k) v[k][7 - (i)]
+#define QS(j, k) v[k][8 + (j)]
+  const int dp0 = abs(PS(2, 0) - 2 * PS(1, 0) + PS(0, 0)), dp3 = abs(PS(2, 3) - 2 * PS(1, 3) + PS(0, 3));
+  const int dq0 = abs(QS(2, 0) - 2 * QS(1, 0) + QS(0, 0)), dq3 = abs(QS(2, 3) - 2 * QS(1, 3) + QS(0, 3));
+  const int sp0 = abs(PS(3, 0) - PS(0, 0)), sq0 = abs(QS(0, 0) - QS(3, 0)), spq0 = abs(PS(0, 0) - QS(0, 0));
+  const int sp3 = abs(PS(3, 3) - PS(0, 3)), sq3 = abs(QS(0, 3) - QS(3, 3)), spq3 = abs(PS(0, 3) - QS(0, 3));
+  const int tc_gate = (5 * tc + 1) >> 1;
+  bool p_large = mp > 3 && !(e.flags & 2);
+  const bool q_large = mq > 3;
+  bool long_ok = false;
+  if (p_large || q_large) {
+    int dp0l = dp0, dp3l = dp3, dq0l = dq0, dq3l = dq3;
+    if (p_large) {
+      dp0l = (dp0 + abs(PS(5, 0) - 2 * PS(4, 0) + PS(3, 0)) + 1) >> 1;
+      dp3l = (dp3 + abs(PS(5, 3) - 2 * PS(4, 3) + PS(3, 3)) + 1) >> 1;
+    } else {
+      mp = 3;
+    }
+    if (q_large) {
+      dq0l = (dq0 + abs(QS(5, 0) - 2 * QS(4, 0) + QS(3, 0)) + 1) >> 1;
+      dq3l = (dq3 + abs(QS(5, 3) - 2 * QS(4, 3) + QS(3, 3)) + 1) >> 1;
+    }
+    int sp0l = sp0, sp3l = sp3, sq0l = sq0, sq3l = sq3;
+    if (mp == 7) {
+      sp0l += abs(PS(7, 0) - PS(6, 0) - PS(5, 0) + PS(4, 0));
+      sp3l += abs(PS(7, 3) - PS(6, 3) - PS(5, 3) + PS(4, 3));
+    }
+    if (mq == 7) {
+      sq0l += abs(QS(4, 0) - QS(5, 0) - QS(6, 0) + QS(7, 0));
+      sq3l += abs(QS(4, 3) - QS(5, 3) - QS(6, 3) + QS(7, 3));
+    }
+    if ((dp0l + dq0l) + (dp3l + dq3l) < beta) {
+      const int t1 = (3 * beta) >> 5, t2 = beta >> 4;
+      bool ok = true;
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int k = r ? 3 : 0;
+        const int dpq = r ? dp3l + dq3l : dp0l + dq0l;
+        int spl = r ? sp3l : sp0l, sql = r ? sq3l : sq0l;
+        if (p_large) spl = (spl + abs(PS(3, k) - PS(mp, k)) + 1) >> 1;
+        if (q_large) sql = (sql + abs(QS(3, k) - QS(mq, k)) + 1) >> 1;
+        ok = ok && 2 * dpq < t2 && spl + sql < t1 && (r ? spq3 : spq0) < tc_gate;
+      }
+      long_ok = ok;
+    }
+  }
+  int wp = 0, wq = 0;  // samples written on each side of every line
+  const bool plt_p = e.flags & 4, plt_q = e.flags & 8;
+  if (long_ok) {
+    // refMiddle per (mflP, mflQ), eqs. 1389-1394; refP / refQ eqs. 1395-1396
+    const int F7[7] = {59, 50, 41, 32, 23, 14, 5}, F5[5] = {58, 45, 32, 19, 6}, F3[3] = {53, 32, 11};
+    const int T7[7] = {6, 5, 4, 3, 2, 1, 1}, T5[5] = {6, 5, 4, 3, 2}, T3[3] = {6, 4, 2};
+    const int *fp = mp == 7 ? F7 : (mp == 5 ? F5 : F3), *tp = mp == 7 ? T7 : (mp == 5 ? T5 : T3);
+    const int *fq = mq == 7 ? F7 : (mq == 5 ? F5 : F3), *tq = mq == 7 ? T7 : (mq == 5 ? T5 : T3);
+    for (int k = 0; k < 4; ++k) {
+      int p[8], q[8];
+      for (int i = 0; i < 8; ++i) {  // unread entries are zero in the reference's arrays
+        p[i] = i <= mp ? PS(i, k) : 0;
+        q[i] = i <= mq ? QS(i, k) : 0;
+      }
+      int mid;
+      if (mp == 5 && mq == 5)
+        mid = (p[4] + p[3] + 2 * (p[2] + p[1] + p[0] + q[0] + q[1] + q[2]) + q[3] + q[4] + 8) >> 4;
+      else if (mp == mq)
+        mid = (p[6] + p[5] + p[4] + p[3] + p[2] + p[1] + 2 * (p[0] + q[0]) + q[1] + q[2] + q[3] + q[4] + q[5] + q[6] +
+               8) >> 4;
+      else if ((mp == 7 && mq == 5) || (mp == 5 && mq == 7))
+        mid = (p[5] + p[4] + p[3] + p[2] + 2 * (p[1] + p[0] + q[0] + q[1]) + q[2] + q[3] + q[4] + q[5] + 8) >> 4;
+      else if ((mp == 5 && mq == 3) || (mp == 3 && mq == 5))
+        mid = (p[3] + p[2] + p[1] + p[0] + q[0] + q[1] + q[2] + q[3] + 4) >> 3;
+      else if (mp == 3 && mq == 7)
+        mid = (2 * (p[2] + p[1] + p[0] + q[0]) + p[0] + p[1] + q[1] + q[2] + q[3] + q[4] + q[5] + q[6] + 8) >> 4;
+      else
+        mid = (p[6] + p[5] + p[4] + p[3] + p[2] + p[1] + 2 * (q[2] + q[1] + q[0] + p[0]) + q[0] + q[1] + 8) >> 4;
+      const int rp = (p[mp] + p[mp - 1] + 1) >> 1, rq = (q[mq] + q[mq - 1] + 1) >> 1;
+      for (int i = 0; i < mp; ++i) {
+        const int lim = (tc * tp[i]) >> 1;
+        PS(i, k) = clampd((mid * fp[i] + rp * (64 - fp[i]) + 32) >> 6, p[i] - lim, p[i] + lim);
+      }
+      for (int j = 0; j < mq; ++j) {
+        const int lim = (tc * tq[j]) >> 1;
+        QS(j, k) = clampd((mid * fq[j] + rq * (64 - fq[j]) + 32) >> 6, q[j] - lim, q[j] + lim);
+      }
+    }
+    wp = plt_p ? 0 : mp;
+    wq = plt_q ? 0 : mq;
+    for (int k = 0; k < 4; ++k) {
+      for (int i = 0; i < wp; ++i)
+        if (vert) wrc(P, cx - i - 1, cy + k, PS(i, k), maxv);
+        else wrc(P, cx + k, cy - i - 1, PS(i, k), maxv);
+      for (int j = 0; j < wq; ++j)
+        if (vert) wrc(P, cx + j, cy + k, QS(j, k), maxv);
+        else wrc(P, cx + k, cy + j, QS(j, k), maxv);
+    }
+    return;
+  }
+  const int d = dp0 + dq0 + dp3 + dq3;
+  if (d >= beta) return;  // dE = 0
+  bool strong = false;
+  if (mp > 2 && mq > 2) {
+    const int t1 = beta >> 3, t2 = beta >> 2;
+    strong = 2 * (dp0 + dq0) < t2 && sp0 + sq0 < t1 && spq0 < tc_gate && 2 * (dp3 + dq3) < t2 &&
+             sp3 + sq3 < t1 && spq3 < tc_gate;
+  }
+  if (strong) mp = mq = 3;
+  const int side_gate = (beta + (beta >> 1)) >> 3;
+  const bool dep = mp > 1 && mq > 1 && dp0 + dp3 < side_gate;
+  const bool deq = mp > 1 && mq > 1 && dq0 + dq3 < side_gate;
+  for (int k = 0; k < 4; ++k) {
+    const int p3 = PS(3, k), p2 = PS(2, k), p1 = PS(1, k), p0 = PS(0, k);
+    const int q0 = QS(0, k), q1 = QS(1, k), q2 = QS(2, k), q3 = QS(3, k);
+    int np = 0, nq = 0;  // samples written this line, from p0 / q0 outwards
+    int out_p[3], out_q[3];
+    if (strong) {
+      out_p[0] = clampd((p2 + 2 * p1 + 2 * p0 + 2 * q0 + q1 + 4) >> 3, p0 - 3 * tc, p0 + 3 * tc);
+      out_p[1] = clampd((p2 + p1 + p0 + q0 + 2) >> 2, p1 - 2 * tc, p1 + 2 * tc);
+      out_p[2] = clampd((2 * p3 + 3 * p2 + p1 + p0 + q0 + 4) >> 3, p2 - tc, p2 + tc);
+      out_q[0] = clampd((p1 + 2 * p0 + 2 * q0 + 2 * q1 + q2 + 4) >> 3, q0 - 3 * tc, q0 + 3 * tc);
+      out_q[1] = clampd((p0 + q0 + q1 + q2 + 2) >> 2, q1 - 2 * tc, q1 + 2 * tc);
+      out_q[2] = clampd((p0 + q0 + q1 + 3 * q2 + 2 * q3 + 4) >> 3, q2 - tc, q2 + tc);
+      np = nq = 3;
+    } else {
+      const int raw = (9 * (q0 - p0) - 3 * (q1 - p1) + 8) >> 4;
+      if (abs(raw) < tc * 10) {
+        const int delta = clampd(raw, -tc, tc);
+        out_p[0] = p0 + delta;
+        out_q[0] = q0 - delta;
+        np = nq = 1;
+        if (dep) {
+          out_p[1] = p1 + clampd((((p2 + p0 + 1) >> 1) - p1 + delta) >> 1, -(tc >> 1), tc >> 1);
+          np = 2;
+        }
+        if (deq) {
+          out_q[1] = q1 + clampd((((q2 + q0 + 1) >> 1) - q1 - delta) >> 1, -(tc >> 1), tc >> 1);
+          nq = 2;
+        }
+      }
+    }
+    if (plt_p) np = 0;
+    if (plt_q) nq = 0;
+    for (int i = 0; i < np; ++i)
+      if (vert) wrc(P, cx - i - 1, cy + k, out_p[i], maxv);
+      else wrc(P, cx + k, cy - i - 1, out_p[i], maxv);
+    for (int j = 0; j < nq; ++j)
+      if (vert) wrc(P, cx + j, cy + k, out_q[j], maxv);
+      else wrc(P, cx + k, cy + j, out_q[j], maxv);
+  }
+#undef PS
+#undef QS
+}
+
+// One chroma edge segment (2 lines): run_chroma_filter_v / _h with the strong
+// decision and filters of src/deblock.rs:1803-2075.
+__device__ void chroma_segment(const DPlane &P, const EdgeSeg &e, int maxv) {
+  const bool vert = e.flags & 1;
+  const int tc = e.tc, beta = e.beta, mp = e.mfl >> 4, mq = e.mfl & 15;
+  const int cx = e.x, cy = e.y;
+  const bool plt_p = e.flags & 4, plt_q = e.flags & 8;
+  int v[2][8];  // v[k][4 + d], d in [-4, 3]
+#pragma unroll
+  for (int k = 0; k < 2; ++k)
+#pragma unroll
+    for (int d = -4; d < 4; ++d) v[k][4 + d] = vert ? rdc(P, cx + d, cy + k) : rdc(P, cx + k, cy + d);
+  const bool eligible = vert ? (mp == 3 && mq == 3) : (mq == 3 && (mp == 3 || mp == 1));
+  const bool short_p = !vert && mp == 1;
+  if (eligible) {
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int p1 = v[k][2], p0 = v[k][3], q0 = v[k][4], q1 = v[k][5], q2 = v[k][6], q3 = v[k][7];
+      const int p3 = short_p ? p1 : v[k][0], p2 = short_p ? p1 : v[k][1];
+      const int dpq = 2 * (abs(p2 - 2 * p1 + p0) + abs(q2 - 2 * q1 + q0));
+      ok = ok && dpq < (beta >> 2) && abs(p3 - p0) + abs(q0 - q3) < (beta >> 3) && abs(p0 - q0) < ((5 * tc + 1) >> 1);
+    }
+    if (ok) {
+      for (int k = 0; k < 2; ++k) {
+        const int p3 = v[k][0], p2 = v[k][1], p1 = v[k][2], p0 = v[k][3];
+        const int q0 = v[k][4], q1 = v[k][5], q2 = v[k][6], q3 = v[k][7];
+        int op[3], oq[3], np;
+        if (short_p) {
+          op[0] = clampd((3 * p1 + 2 * p0 + q0 + q1 + q2 + 4) >> 3, p0 - tc, p0 + tc);
+          oq[0] = clampd((2 * p1 + p0 + 2 * q0 + q1 + q2 + q3 + 4) >> 3, q0 - tc, q0 + tc);
+          np = 1;
+        } else {
+          op[0] = clampd((p3 + p2 + p1 + 2 * p0 + q0 + q1 + q2 + 4) >> 3, p0 - tc, p0 + tc);
+          op[1] = clampd((2 * p3 + p2 + 2 * p1 + p0 + q0 + q1 + 4) >> 3, p1 - tc, p1 + tc);
+          op[2] = clampd((3 * p3 + 2 * p2 + p1 + p0 + q0 + 4) >> 3, p2 - tc, p2 + tc);
+          oq[0] = clampd((p2 + p1 + p0 + 2 * q0 + q1 + q2 + q3 + 4) >> 3, q0 - tc, q0 + tc);
+          np = 3;
+        }
+        oq[1] = clampd((p1 + p0 + q0 + 2 * q1 + q2 + 2 * q3 + 4) >> 3, q1 - tc, q1 + tc);
+        oq[2] = clampd((p0 + q0 + q1 + 2 * q2 + 3 * q3 + 4) >> 3, q2 - tc, q2 + tc);
+        if (!plt_p)
+          for (int i = 0; i < np; ++i)
+            if (vert) wrc(P, cx - i - 1, cy + k, op[i], maxv);
+            else wrc(P, cx + k, cy - i - 1, op[i], maxv);
+        if (!plt_q)
+          for (int j = 0; j < 3; ++j)
+            if (vert) wrc(P, cx + j, cy + k, oq[j], maxv);
+            else wrc(P, cx + k, cy + j, oq[j], maxv);
+      }
+      return;
+    }
+  }
+  for (int k = 0; k < 2; ++k) {  // weak filter, eqs. 1421-1423
+    const int p1 = v[k][2], p0 = v[k][3], q0 = v[k][4], q1 = v[k][5];
+    const int delta = clampd(((q0 - p0) * 4 + p1 - q1 + 4) >> 3, -tc, tc);
+    if (!plt_p) {
+      if (vert) wrc(P, cx - 1, cy + k, p0 + delta, maxv);
+      else wrc(P, cx + k, cy - 1, p0 + delta, maxv);
+    }
+    if (!plt_q) {
+      if (vert) wrc(P, cx, cy + k, q0 - delta, maxv);
+      else wrc(P, cx + k, cy, q0 - delta, maxv);
+    }
+  }
+}
+
+struct Planes3 {
+  DPlane p[3];
+};
+
+__global__ void __launch_bounds__(128) k_deblock_components(Planes3 planes, const EdgeSeg *__restrict__ segs,
+                                                            const uint32_t *__restrict__ comp, uint32_t n_comp,
+                                                            int maxv) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_comp) return;
+  const uint32_t b = comp[c], e = comp[c + 1];
+  for (uint32_t i = b; i < e; ++i) {
+    const EdgeSeg s = segs[i];
+    if (s.plane == 0) luma_segment(planes.p[0], s, maxv);
+    else chroma_segment(planes.p[s.plane], s, maxv);
+  }
+}
+
+}  // namespace
+
+int launch_deblock(cudaStream_t st, const DPlane planes[3], int bit_depth, const EdgeSeg *d_segs_v,
+                   const uint32_t *d_comp_v, uint32_t n_comp_v, const EdgeSeg *d_segs_h, const uint32_t *d_comp_h,
+                   uint32_t n_comp_h, uint64_t *launches) {
+  Planes3 p3{{planes[0], planes[1], planes[2]}};
+  const int maxv = (1 << bit_depth) - 1;
+  if (n_comp_v) {
+    k_deblock_components<<<(n_comp_v + 127) / 128, 128, 0, st>>>(p3, d_segs_v, d_comp_v, n_comp_v, maxv);
+    H266_CUDA(cudaGetLastError());
+    ++*launches;
+  }
+  if (n_comp_h) {
+    k_deblock_components<<<(n_comp_h + 127) / 128, 128, 0, st>>>(p3, d_segs_h, d_comp_h, n_comp_h, maxv);
+    H266_CUDA(cudaGetLastError());
+    ++*launches;
+  }
+  return H266_OK;
+}
+
+}  // namespace h266

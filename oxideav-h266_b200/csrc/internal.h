@@ -1,0 +1,141 @@
+// Internal declarations shared by the CUDA translation units of the filter
+// chain library (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "oxideav_h266_b200.h"
+
+namespace h266 {
+
+// ---------------------------------------------------------------- errors
+struct Status {
+  int code = H266_OK;
+  bool ok() const { return code == H266_OK; }
+};
+int set_error(int code, const std::string &msg);  // records msg for h266_last_error, returns code
+int cuda_error(cudaError_t e, const char *what);   // H266_ERR_CUDA (or OUT_OF_MEMORY) with context
+#define H266_CUDA(call)                                   \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return cuda_error(e_, #call);  \
+  } while (0)
+#define H266_TRY(call)          \
+  do {                          \
+    int rc_ = (call);           \
+    if (rc_ != H266_OK) return rc_; \
+  } while (0)
+
+// ---------------------------------------------------------------- device buffers
+// A growable device allocation owned by a context.
+struct DevBuf {
+  void *ptr = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes);
+  void release();
+  template <class T>
+  T *as() const {
+    return static_cast<T *>(ptr);
+  }
+};
+
+// A device plane view used by the kernels.
+struct DPlane {
+  uint16_t *s;
+  int64_t stride;  // samples
+  int w, h;
+};
+
+// ---------------------------------------------------------------- deblocking
+// One edge segment of the reference's deblocking walk: a 4-line luma or a
+// 2-line chroma piece of a vertical or horizontal edge.  (x, y) is q0 of the
+// segment's first line in the plane's own sample grid.
+struct EdgeSeg {
+  uint16_t x, y;
+  uint16_t beta, tc;
+  uint8_t plane;  // 0 luma, 1 cb, 2 cr
+  uint8_t bs;
+  uint8_t mfl;    // mfl_p << 4 | mfl_q
+  uint8_t flags;  // bit0 vertical, bit1 ctb_row (luma EDGE_HOR CTB row), bit2 plt_p, bit3 plt_q
+};
+static_assert(sizeof(EdgeSeg) == 12, "EdgeSeg layout");
+
+// Host-side deblocking plan: segments grouped into independent components.
+// Segments of one component touch overlapping samples and are listed in the
+// reference's processing order; different components touch disjoint samples.
+struct DeblockPlan {
+  std::vector<EdgeSeg> segs[2];      // [0] vertical pass, [1] horizontal pass
+  std::vector<uint32_t> comp[2];     // component start offsets (+ final end)
+  uint32_t max_comp_len[2] = {0, 0};
+};
+
+int build_deblock_plan(const h266_picture &pic, const h266_deblock_cu *cus, uint64_t n_cus,
+                       const h266_deblock_cu *chroma_cus, uint64_t n_chroma, const h266_deblock_mv_grid *mv,
+                       const h266_deblock_params &params, uint32_t cfi, const uint32_t *nf_cols, uint64_t n_cols,
+                       const uint32_t *nf_rows, uint64_t n_rows, DeblockPlan &plan);
+
+// Launches the two deblocking passes (vertical then horizontal) in place on
+// the three device planes.  seg/comp point at device copies of the plan.
+int launch_deblock(cudaStream_t st, const DPlane planes[3], int bit_depth, const EdgeSeg *d_segs_v,
+                   const uint32_t *d_comp_v, uint32_t n_comp_v, const EdgeSeg *d_segs_h, const uint32_t *d_comp_h,
+                   uint32_t n_comp_h, uint64_t *launches);
+
+// ---------------------------------------------------------------- LMCS
+int derive_lmcs(const h266_lmcs_data *d, uint32_t bd, h266_lmcs_derived *o);
+// Builds the 65536-entry inverse-map LUT on the device (one entry per u16 input).
+int launch_lmcs_lut(cudaStream_t st, uint16_t *d_lut, const h266_lmcs_derived &l, uint32_t mn, uint32_t mx,
+                    uint64_t *launches);
+// dst = lut ? lut[src] : src over a plane (dst may equal src).
+int launch_plane_map(cudaStream_t st, DPlane dst, DPlane src, const uint16_t *d_lut, uint64_t *launches);
+
+// ---------------------------------------------------------------- SAO / ALF
+struct SaoCtbDev {  // one component's SAO parameters for one CTB
+  uint8_t type, eo_class, band_pos, pad;
+  int16_t off[4];   // SaoOffsetVal[1..4]
+};
+struct CtbDev {      // everything pass 2 needs per CTB
+  SaoCtbDev sao[3];  // 36 bytes
+  uint16_t rect[4];  // SAO / ALF clip rectangle, luma samples (x0, y0, x1, y1)
+  int16_t luma_set;  // ALF luma filter set slot, -1 = luma ALF off
+  int8_t chroma_filt[2];  // chroma ALF alt filter per cb/cr, -1 = off
+  int8_t cc_filt[2];      // CC-ALF filter per cb/cr, -1 = off
+  int8_t pad[2];
+};
+static_assert(sizeof(CtbDev) == 52, "CtbDev layout");
+
+struct AlfTablesDev {
+  // luma filter sets: slot -> [25 classes][12] coefficients and clip values
+  const int32_t *luma_coeff;  // slot s at [s * 600, s * 600 + 300)
+  const int32_t *luma_clip;   // slot s at [s * 600, s * 600 + 300) (resolved AlfClip values)
+  int32_t chroma_coeff[8][6];
+  int32_t chroma_clip[8][6];
+  int32_t cc_coeff[2][4][7];  // [cb/cr][filter][tap]
+};
+
+struct Pass2Args {
+  DPlane src[3];  // input planes (post-deblock)
+  DPlane dst[3];  // output planes
+  int bit_depth;
+  int ctb_log2;
+  int sub_w, sub_h;       // chroma subsampling of the SAO / ALF config
+  int chroma;             // chroma planes present (cfi != 0 and non-empty)
+  int w_ctbs, h_ctbs;     // CTB parameter grid
+  int tiles_x, tiles_y;   // 32x32 luma tiles
+  int ext_w, ext_h;       // luma extent the tile grid covers
+  int pic_w, pic_h;       // luma picture dims
+  int has_clip;           // tile / slice clip bounds given
+  // SAO
+  int sao_luma, sao_chroma;
+  // ALF
+  int alf_luma_any, alf_chroma_cb, alf_chroma_cr, alf_cc_cb, alf_cc_cr;
+  const CtbDev *ctbs;
+  AlfTablesDev tables;
+};
+
+int launch_pass2(cudaStream_t st, const Pass2Args &a, bool do_sao, bool do_alf, uint64_t *launches);
+
+}  // namespace h266

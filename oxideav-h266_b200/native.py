@@ -1,0 +1,201 @@
+"""ctypes binding of the CUDA library (liboxideav_h266_b200.so) and a thin
+host API mirroring the reference crate's filter functions.
+
+    ctx = Context(0)
+    ctx.apply_in_loop_filters(pic, args)        # CtuWalker::apply_in_loop_filters_with_alf
+    ctx.apply_deblocking_clipped(pic, args)     # deblock.rs apply_deblocking_clipped
+    ctx.apply_sao_clipped(pic, args)            # sao.rs apply_sao_clipped
+    ctx.apply_alf_clipped(pic, args)            # alf.rs apply_alf_clipped
+    ctx.lmcs_inverse_map_luma(pic, args)        # ctu.rs:11837-11851 over lmcs.rs
+
+`pic` is a workloads.PictureData (host planes, filtered in place through
+host<->device copies) or a DevicePicture (torch CUDA tensors, filtered in
+place on the device).  There is no CPU implementation behind this module:
+if the library is missing or no GPU is present, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+
+import numpy as np
+
+from . import abi
+from .workloads import FilterArgsData, PictureData
+
+LIB_PATH = pathlib.Path(__file__).resolve().parent / "liboxideav_h266_b200.so"
+_LIB = None
+
+# Every symbol declared in include/oxideav_h266_b200.h.
+EXPORTS = [
+    "h266_ctx_create", "h266_ctx_destroy", "h266_ctx_set_stream", "h266_ctx_synchronize", "h266_last_error",
+    "h266_ctx_kernel_launches", "h266_derive_lmcs", "h266_lmcs_inverse_map_luma", "h266_apply_deblocking_clipped",
+    "h266_apply_sao_clipped", "h266_apply_alf_clipped", "h266_apply_in_loop_filters",
+    "h266_apply_in_loop_filters_batch",
+]
+
+
+class H266Error(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"h266 error {code} ({abi.ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"CUDA library {LIB_PATH.name} is not built; run __graft_entry__.build()")
+        L = C.CDLL(str(LIB_PATH))
+        vp, u64, u32, i32 = C.c_void_p, C.c_uint64, C.c_uint32, C.c_int
+        L.h266_ctx_create.argtypes = [i32, C.POINTER(vp)]
+        L.h266_ctx_destroy.argtypes = [vp]
+        L.h266_ctx_set_stream.argtypes = [vp, vp]
+        L.h266_ctx_synchronize.argtypes = [vp]
+        L.h266_last_error.restype = C.c_char_p
+        L.h266_ctx_kernel_launches.argtypes = [vp]
+        L.h266_ctx_kernel_launches.restype = u64
+        L.h266_derive_lmcs.argtypes = [vp, u32, vp]
+        L.h266_lmcs_inverse_map_luma.argtypes = [vp, vp, vp, u32, u32]
+        L.h266_apply_deblocking_clipped.argtypes = [vp, vp, vp, u64, vp, u64, vp, vp, u32, vp, u64, vp, u64]
+        L.h266_apply_sao_clipped.argtypes = [vp, vp, vp, vp, vp, u64, vp, u64]
+        L.h266_apply_alf_clipped.argtypes = [vp, vp, vp, vp, vp, vp, u64, vp, u64]
+        L.h266_apply_in_loop_filters.argtypes = [vp, vp, vp]
+        L.h266_apply_in_loop_filters_batch.argtypes = [vp, u32, vp, vp]
+        _LIB = L
+    return _LIB
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise H266Error(rc, lib().h266_last_error().decode(errors="replace"))
+
+
+def _u32(values):
+    if values is None:
+        return None, 0, None
+    vals = list(values)
+    arr = np.ascontiguousarray(np.asarray(vals or [0], dtype=np.uint32))
+    return arr.ctypes.data, len(vals), arr
+
+
+def derive_lmcs(data: abi.LmcsData, bit_depth: int) -> abi.LmcsDerived:
+    """LmcsData::derive (src/lmcs.rs:113); raises H266Error(-3) where the crate returns Err."""
+    out = abi.LmcsDerived()
+    _check(lib().h266_derive_lmcs(C.byref(data), bit_depth, C.byref(out)))
+    return out
+
+
+class DevicePicture:
+    """Three uint16 planes resident on the GPU (torch tensors, int16 storage)."""
+
+    def __init__(self, luma, cb, cr, bit_depth: int):
+        self.luma, self.cb, self.cr, self.bit_depth = luma, cb, cr, bit_depth
+
+    @staticmethod
+    def from_host(pic: PictureData, device: int = 0) -> "DevicePicture":
+        import torch
+
+        dev = torch.device("cuda", device)
+        planes = [torch.from_numpy(np.ascontiguousarray(p).view(np.int16)).to(dev) for p in pic.planes()]
+        return DevicePicture(*planes, pic.bit_depth)
+
+    def to_host(self) -> PictureData:
+        planes = [p.cpu().numpy().view(np.uint16).copy() for p in (self.luma, self.cb, self.cr)]
+        return PictureData(*planes, self.bit_depth)
+
+    def to_ctypes(self) -> abi.Picture:
+        pic = abi.Picture()
+        for name, t in zip(("luma", "cb", "cr"), (self.luma, self.cb, self.cr)):
+            pl = getattr(pic, name)
+            pl.samples = t.data_ptr() if t.numel() else None
+            pl.stride = max(t.shape[1], 1)
+            pl.width = t.shape[1]
+            pl.height = t.shape[0]
+            pl.bit_depth = self.bit_depth
+        pic.mem = abi.MEM_DEVICE
+        return pic
+
+
+class Context:
+    """One h266_ctx: a CUDA device, a stream and the library's device scratch."""
+
+    def __init__(self, device: int = 0):
+        self.device = device
+        h = C.c_void_p()
+        _check(lib().h266_ctx_create(device, C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if self._h:
+            lib().h266_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def kernel_launches(self) -> int:
+        return lib().h266_ctx_kernel_launches(self._h)
+
+    def synchronize(self):
+        _check(lib().h266_ctx_synchronize(self._h))
+
+    def set_stream(self, stream_ptr: int | None):
+        _check(lib().h266_ctx_set_stream(self._h, stream_ptr))
+
+    # -- filters ----------------------------------------------------------
+    def apply_in_loop_filters(self, pic, fa: FilterArgsData):
+        cp = pic.to_ctypes()
+        a, keep = fa.to_ctypes()
+        _check(lib().h266_apply_in_loop_filters(self._h, C.byref(cp), C.byref(a)))
+
+    def apply_in_loop_filters_batch(self, pics, fas):
+        cps = [p.to_ctypes() for p in pics]
+        built = [f.to_ctypes() for f in fas]
+        P = (C.c_void_p * len(pics))(*[C.addressof(c) for c in cps])
+        A = (C.c_void_p * len(pics))(*[C.addressof(a) for a, _ in built])
+        _check(lib().h266_apply_in_loop_filters_batch(self._h, len(pics), P, A))
+
+    def apply_deblocking_clipped(self, pic, fa: FilterArgsData):
+        cp = pic.to_ctypes()
+        g, kg = fa.mv_grid()
+        cols, ncols, k1 = _u32(fa.no_filter_cols)
+        rows, nrows, k2 = _u32(fa.no_filter_rows)
+        ccus = fa.chroma_cus.ctypes.data if fa.chroma_cus is not None else None
+        nc = len(fa.chroma_cus) if fa.chroma_cus is not None else 0
+        _check(lib().h266_apply_deblocking_clipped(
+            self._h, C.byref(cp), fa.cus.ctypes.data if len(fa.cus) else None, len(fa.cus), ccus, nc,
+            C.byref(g) if g is not None else None, C.byref(fa.deblock), fa.chroma_format_idc, cols, ncols, rows,
+            nrows))
+
+    def apply_sao_clipped(self, pic, fa: FilterArgsData, use_clip: bool = True):
+        cp = pic.to_ctypes()
+        s = fa.sao_picture()
+        cols, ncols, k1 = _u32(fa.clip_cols if use_clip else None)
+        rows, nrows, k2 = _u32(fa.clip_rows if use_clip else None)
+        _check(lib().h266_apply_sao_clipped(self._h, C.byref(cp), C.byref(s), C.byref(fa.sao_cfg), cols, ncols,
+                                            rows, nrows))
+
+    def apply_alf_clipped(self, pic, fa: FilterArgsData, use_clip: bool = True):
+        cp = pic.to_ctypes()
+        a = fa.alf_picture()
+        b, keep = fa.binding()
+        cols, ncols, k1 = _u32(fa.clip_cols if use_clip else None)
+        rows, nrows, k2 = _u32(fa.clip_rows if use_clip else None)
+        _check(lib().h266_apply_alf_clipped(self._h, C.byref(cp), C.byref(a), C.byref(fa.alf_cfg), C.byref(b),
+                                            cols, ncols, rows, nrows))
+
+    def lmcs_inverse_map_luma(self, pic, fa: FilterArgsData):
+        cp = pic.to_ctypes()
+        _check(lib().h266_lmcs_inverse_map_luma(self._h, C.byref(cp), C.byref(fa.lmcs), fa.lmcs_min_bin,
+                                                fa.lmcs_max_bin))

@@ -479,3 +479,148 @@ def config4(seed: int = 4000):
     if kind == 1:
         return make_workload(seed, 1920, 1080, 10, 7, ccalf=True, lmcs=True, n_luma_aps=2)
     return make_workload(seed, 3840, 2160, 10, 7, ccalf=True, lmcs=True, n_luma_aps=2)
+
+
+# ---------------------------------------------------------------------------
+# stress partitions for deblocking parity
+# ---------------------------------------------------------------------------
+def _mtt_partition(rng, W, H, ctb, min_size=4, p_stop=0.35):
+    """Quad / binary multi-type-tree split of every CTB down to 4-sample blocks,
+    leaves in decode (tree) order."""
+    leaves = []
+
+    def rec(x, y, w, h):
+        if x >= W or y >= H:
+            return
+        crosses = x + w > W or y + h > H
+        opts = []
+        if w == h and w > min_size:
+            opts.append("q")
+        if w > min_size:
+            opts.append("v")
+        if h > min_size:
+            opts.append("h")
+        stop = not crosses and (w <= 64 and h <= 64 or rng.random() < 0.3) and rng.random() < p_stop
+        if not opts or (stop and not crosses):
+            if not crosses:
+                leaves.append((x, y, w, h))
+            return
+        if crosses:
+            opts = [o for o in opts if o == "q"] or opts
+        o = opts[int(rng.integers(0, len(opts)))]
+        if o == "q":
+            hw = w // 2
+            for dy in (0, hw):
+                for dx in (0, hw):
+                    rec(x + dx, y + dy, hw, hw)
+        elif o == "v":
+            rec(x, y, w // 2, h)
+            rec(x + w // 2, y, w // 2, h)
+        else:
+            rec(x, y, w, h // 2)
+            rec(x, y + h // 2, w, h // 2)
+
+    for cy in range(0, H, ctb):
+        for cx in range(0, W, ctb):
+            rec(cx, cy, ctb, ctb)
+    return leaves
+
+
+def _stress_cus(rng, leaves, allow_inter=True):
+    n = len(leaves)
+    cus = np.zeros(n, dtype=abi.DEBLOCK_CU)
+    arr = np.array(leaves, dtype=np.int64)
+    cus["x"], cus["y"], cus["w"], cus["h"] = arr[:, 0], arr[:, 1], arr[:, 2], arr[:, 3]
+    cus["qp_y"] = rng.integers(-6, 64, size=n)
+    legacy = rng.random(n) < 0.5
+    qpc = rng.integers(0, 64, size=(n, 3))
+    cus["qp_c"] = np.where(legacy[:, None], abi.DEBLOCK_QP_C_LEGACY, qpc)
+    cus["joint_cbcr2"] = rng.random(n) < 0.2
+    inter = (rng.random(n) < 0.6) if allow_inter else np.zeros(n, bool)
+    cus["intra"] = ~inter
+    for f in ("tu_y_coded", "tu_cb_coded", "tu_cr_coded"):
+        cus[f] = rng.random(n) < 0.5
+    cus["bdpcm_luma"] = (~inter) & (rng.random(n) < 0.1)
+    cus["bdpcm_chroma"] = (~inter) & (rng.random(n) < 0.1)
+    cus["plt"] = rng.random(n) < 0.05
+    cus["ciip"] = inter & (rng.random(n) < 0.05)
+    cus["ibc"] = inter & (rng.random(n) < 0.1)
+    for i in range(n):
+        x, y, w, h = leaves[i]
+        if inter[i] and rng.random() < 0.25:
+            cus["has_num_sb"][i] = 1
+            cus["num_sb_x"][i] = max(1, w // int(rng.choice([4, 8, 16])))
+            cus["num_sb_y"][i] = max(1, h // int(rng.choice([4, 8, 16])))
+        if (w > 64 or h > 64) and rng.random() < 0.7:
+            cus["has_tu64"][i] = 1
+            for f in ("tu64_y", "tu64_cb", "tu64_cr"):
+                cus[f][i] = rng.random((2, 2)) < 0.5
+        elif rng.random() < 0.25:
+            vert = bool(rng.integers(0, 2))
+            dim = w if vert else h
+            cand = list(range(4, dim, 4))
+            if cand:
+                k = int(rng.integers(1, min(3, len(cand)) + 1))
+                b = sorted(rng.choice(cand, size=k, replace=False).tolist())
+                cus["has_tb_split"][i] = 1
+                cus["ts_vertical"][i] = vert
+                cus["ts_n_bounds"][i] = k
+                cus["ts_bounds"][i][:k] = b
+                cus["ts_luma_only"][i] = rng.random() < 0.5
+                for f in ("ts_y_coded", "ts_cb_coded", "ts_cr_coded"):
+                    cus[f][i] = rng.random(4) < 0.5
+    return cus, inter
+
+
+def stress_workload(seed: int, width: int = 256, height: int = 192, bit_depth: int = 10, ctb_log2: int = 6,
+                    dual_tree: bool = False, tiles: bool = False):
+    """Deblocking stress picture: 4..128-sample multi-type-tree CUs with TB splits,
+    sub-block grids, 64-sample TU tiling, palette / BDPCM / IBC / CIIP flags,
+    explicit chroma QPs, random offsets and motion; full SAO/ALF/LMCS on top."""
+    pic, fa = make_workload(seed, width, height, bit_depth, ctb_log2, inter_frac=0.0, n_luma_aps=2, n_chroma_alt=2,
+                            ccalf=True, lmcs=True, alf_fixed_frac=0.3)
+    rng = np.random.Generator(np.random.PCG64(seed + 7777))
+    ctb = 1 << ctb_log2
+    leaves = _mtt_partition(rng, width, height, ctb)
+    cus, inter = _stress_cus(rng, leaves)
+    # re-draw the content so the CU edges are real discontinuities
+    scale = 1 << (bit_depth - 8)
+    mx = (1 << bit_depth) - 1
+    for plane, sub in ((pic.luma, 1), (pic.cb, 2), (pic.cr, 2)):
+        for (x, y, w, h), d in zip(leaves, rng.integers(-12, 13, size=len(leaves)) * scale):
+            sl = plane[y // sub:(y + h) // sub, x // sub:(x + w) // sub]
+            sl[...] = np.clip(sl.astype(np.int64) + d, 0, mx).astype(np.uint16)
+    fa.cus = cus
+    cw_, ch_ = -(-width // 4), -(-height // 4)
+    mv = np.zeros((ch_, cw_), dtype=abi.MV_CELL)
+    for i in np.nonzero(inter)[0]:
+        x, y, w, h = leaves[i]
+        cell = mv[y // 4:(y + h) // 4, x // 4:(x + w) // 4]
+        # per-4x4 motion inside sub-block CUs, per-CU otherwise
+        shape = cell.shape if cus["has_num_sb"][i] else (1, 1)
+        pred = rng.integers(1, 4, size=shape)  # 1 L0, 2 L1, 3 bi
+        cell["pred_l0"] = (pred & 1) != 0
+        cell["pred_l1"] = (pred & 2) != 0
+        cell["poc_l0"] = rng.choice([3, 5, 7], size=shape)
+        cell["poc_l1"] = rng.choice([5, 9], size=shape)
+        cell["mv_l0"] = rng.integers(-2, 3, size=shape + (2,)) * 4
+        cell["mv_l1"] = rng.integers(-2, 3, size=shape + (2,)) * 4
+    fa.mv = mv
+    d = fa.deblock
+    for f in ("luma_beta_offset_div2", "luma_tc_offset_div2", "cb_beta_offset_div2", "cb_tc_offset_div2",
+              "cr_beta_offset_div2", "cr_tc_offset_div2"):
+        setattr(d, f, int(rng.integers(-3, 4)))
+    d.chroma_qp_offset_cb = int(rng.integers(-4, 5))
+    d.chroma_qp_offset_cr = int(rng.integers(-4, 5))
+    if dual_tree:
+        cleaves = _mtt_partition(rng, width, height, ctb, min_size=8)
+        fa.chroma_cus, _ = _stress_cus(rng, cleaves, allow_inter=False)
+    if tiles:
+        w_ctbs, h_ctbs = -(-width // ctb), -(-height // ctb)
+        cols = sorted(set(int(v) for v in rng.integers(1, max(2, w_ctbs), size=2)))
+        rows = sorted(set(int(v) for v in rng.integers(1, max(2, h_ctbs), size=1)))
+        fa.no_filter_cols = [c * ctb for c in cols if c * ctb < width]
+        fa.no_filter_rows = [r * ctb for r in rows if r * ctb < height]
+        fa.clip_cols = [0] + fa.no_filter_cols + [width]
+        fa.clip_rows = [0] + fa.no_filter_rows + [height]
+    return pic, fa

@@ -1,0 +1,155 @@
+"""GPU parity: every filter of the CUDA library against the oracle (bit-exact,
+integer arithmetic; tolerance 0) and against the reference's own
+known-answer tests.  Calls go through the C ABI."""
+import numpy as np
+import pytest
+
+import oracle
+from kat_util import KATS, build_args, build_picture, check
+from oxideav_h266_b200 import native
+from oxideav_h266_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = native.Context(0)
+    yield c
+    c.close()
+
+
+def assert_same(got, want, what):
+    for name, a, b in zip(("luma", "cb", "cr"), got.planes(), want.planes()):
+        if not np.array_equal(a, b):
+            ys, xs = np.nonzero(a != b)
+            raise AssertionError(f"{what}: {name} differs at {len(ys)} samples, first (x={xs[0]}, y={ys[0]}): "
+                                 f"gpu {a[ys[0], xs[0]]} oracle {b[ys[0], xs[0]]}")
+
+
+@pytest.mark.parametrize("case", KATS["cases"], ids=[c["name"] for c in KATS["cases"]])
+def test_reference_kats_on_gpu(ctx, case):
+    pic = build_picture(case["pic"])
+    before = pic.copy()
+    fa = build_args(case, pic)
+    want = pic.copy()
+    if case["kind"] == "deblock":
+        ctx.apply_deblocking_clipped(pic, fa)
+        oracle.apply_deblocking_clipped(want, fa)
+    elif case["kind"] == "sao":
+        ctx.apply_sao_clipped(pic, fa, use_clip=False)
+        oracle.apply_sao_clipped(want, fa, use_clip=False)
+    else:
+        ctx.apply_alf_clipped(pic, fa, use_clip=False)
+        oracle.apply_alf_clipped(want, fa, use_clip=False)
+    check(case, before, pic)
+    assert_same(pic, want, case["name"])
+
+
+def small_c2(seed):
+    return W.config2(seed, 640, 360)
+
+
+WORKLOADS = {
+    "c1": lambda s: W.config1(1000 + s),
+    "c2_small": lambda s: small_c2(2000 + s),
+    "stress": lambda s: W.stress_workload(3000 + s),
+    "stress_dual": lambda s: W.stress_workload(4000 + s, dual_tree=True, bit_depth=8),
+    "stress_tiles": lambda s: W.stress_workload(5000 + s, tiles=True, ctb_log2=5),
+    "ctb64_8bit": lambda s: W.make_workload(6000 + s, 832, 480, 8, 6, ccalf=True, lmcs=True, n_luma_aps=2,
+                                            alf_fixed_frac=0.5),
+    "odd_tail": lambda s: W.make_workload(7000 + s, 200, 136, 10, 7, inter_frac=0.5, ccalf=True, lmcs=True),
+}
+
+
+@pytest.mark.parametrize("kind", list(WORKLOADS))
+@pytest.mark.parametrize("seed", [0, 1])
+def test_deblock_parity(ctx, kind, seed):
+    pic, fa = WORKLOADS[kind](seed)
+    got, want = pic.copy(), pic.copy()
+    ctx.apply_deblocking_clipped(got, fa)
+    oracle.apply_deblocking_clipped(want, fa)
+    assert not want.equal(pic)
+    assert_same(got, want, f"deblock {kind}/{seed}")
+
+
+@pytest.mark.parametrize("kind", list(WORKLOADS))
+@pytest.mark.parametrize("use_clip", [False, True])
+def test_sao_alf_parity(ctx, kind, use_clip):
+    pic, fa = WORKLOADS[kind](0)
+    for name in ("sao", "alf"):
+        got, want = pic.copy(), pic.copy()
+        getattr(ctx, f"apply_{name}_clipped")(got, fa, use_clip=use_clip)
+        getattr(oracle, f"apply_{name}_clipped")(want, fa, use_clip=use_clip)
+        assert_same(got, want, f"{name} {kind} clip={use_clip}")
+
+
+@pytest.mark.parametrize("kind", ["c2_small", "stress"])
+def test_lmcs_parity(ctx, kind):
+    pic, fa = WORKLOADS[kind](0)
+    got, want = pic.copy(), pic.copy()
+    ctx.lmcs_inverse_map_luma(got, fa)
+    oracle.lmcs_inverse_map_luma(want, fa)
+    assert_same(got, want, f"lmcs {kind}")
+
+
+@pytest.mark.parametrize("kind", list(WORKLOADS))
+def test_chain_parity_host(ctx, kind):
+    pic, fa = WORKLOADS[kind](1)
+    got, want = pic.copy(), pic.copy()
+    ctx.apply_in_loop_filters(got, fa)
+    oracle.apply_in_loop_filters(want, fa)
+    assert_same(got, want, f"chain {kind}")
+
+
+def test_chain_parity_device_planes(ctx):
+    pic, fa = small_c2(11)
+    want = pic.copy()
+    oracle.apply_in_loop_filters(want, fa)
+    dev = native.DevicePicture.from_host(pic)
+    ctx.apply_in_loop_filters(dev, fa)
+    ctx.synchronize()
+    assert_same(dev.to_host(), want, "chain device")
+
+
+def test_chain_full_size_1080p(ctx):
+    pic, fa = W.config2(2000)
+    got, want = pic.copy(), pic.copy()
+    ctx.apply_in_loop_filters(got, fa)
+    oracle.apply_in_loop_filters(want, fa)
+    assert_same(got, want, "chain 1080p")
+
+
+def test_chain_full_size_2160p_tiles(ctx):
+    pic, fa = W.config3(3000)
+    got, want = pic.copy(), pic.copy()
+    ctx.apply_in_loop_filters(got, fa)
+    oracle.apply_in_loop_filters(want, fa)
+    assert_same(got, want, "chain 2160p tiles")
+
+
+def test_batch_mixed_sizes(ctx):
+    items = [W.config4(4000 + i) for i in range(3)]
+    pics = [p.copy() for p, _ in items]
+    fas = [f for _, f in items]
+    ctx.apply_in_loop_filters_batch(pics, fas)
+    for (p, f), got in zip(items, pics):
+        want = p.copy()
+        oracle.apply_in_loop_filters(want, f)
+        assert_same(got, want, "batch")
+
+
+def test_repeat_calls_are_deterministic(ctx):
+    pic, fa = W.stress_workload(99)
+    a, b = pic.copy(), pic.copy()
+    ctx.apply_in_loop_filters(a, fa)
+    ctx.apply_in_loop_filters(b, fa)
+    assert a.equal(b)
+
+
+def test_unsupported_ctb_size_is_rejected(ctx):
+    pic, fa = W.config1()
+    fa.sao_cfg.ctb_log2_size_y = 4
+    with pytest.raises(native.H266Error) as e:
+        ctx.apply_sao_clipped(pic.copy(), fa)
+    assert e.value.code == -7
