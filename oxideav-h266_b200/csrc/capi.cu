@@ -278,6 +278,16 @@ int build_pass2(const h266_picture &pic, const Pass2Inputs &in, Pass2Host &h) {
   chroma_sub(cfi, sw, sh);
   const int pw = (int)pic.luma.width, ph = (int)pic.luma.height;
   const bool chroma = cfi != 0 && (uint64_t)pic.cb.width * pic.cb.height + (uint64_t)pic.cr.width * pic.cr.height > 0;
+  if (chroma) {  // PictureBuffer chroma is floor or ceil of luma / SubWidthC (src/reconstruct.rs:130-139)
+    const h266_plane *cp[2] = {&pic.cb, &pic.cr};
+    for (const h266_plane *c : cp) {
+      if ((uint64_t)c->width * c->height == 0) continue;
+      const uint32_t fw = pic.luma.width / sw, cw = (pic.luma.width + sw - 1) / sw;
+      const uint32_t fh = pic.luma.height / sh, ch = (pic.luma.height + sh - 1) / sh;
+      if (c->width < fw || c->width > cw || c->height < fh || c->height > ch)
+        return set_error(H266_ERR_UNSUPPORTED, "chroma plane size does not match the luma size and chroma format");
+    }
+  }
   const h266_alf_aps_binding *b = in.binding;
   const h266_alf_aps_data *caps = (alf_on && b) ? b->chroma_aps : nullptr;
   const h266_alf_aps_data *ccaps[2] = {(alf_on && b) ? b->cc_cb_aps : nullptr, (alf_on && b) ? b->cc_cr_aps : nullptr};

@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(NTHREADS) k_sao_alf(const __grid_constant__ Pa
 
   // ------------------------------------------------------------ luma
   const DPlane LS = a.src[0], LD = a.dst[0];
-  const bool have_luma = LS.w > 0 && LS.h > 0;
+  const bool have_luma = LS.w > 0 && LS.h > 0 && X0 < LS.w && Y0 < LS.h;  // tile starts inside the picture
   const bool luma_alf = DO_ALF && me && me->luma_set >= 0 && have_luma;
   const bool need_sl = have_luma;  // CC-ALF also reads sL
   if (need_sl) {
