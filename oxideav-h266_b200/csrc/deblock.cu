@@ -340,10 +340,11 @@ int build_deblock_plan(const h266_picture &pic, const h266_deblock_cu *cus, uint
                        const uint32_t *nf_rows, uint64_t n_rows, DeblockPlan &plan) {
   for (int d = 0; d < 2; ++d) {
     plan.segs[d].clear();
-    plan.comp[d].clear();
+    plan.comp[d].assign(1, 0);  // component offsets end with the total count
     plan.max_comp_len[d] = 0;
   }
   if (params.disabled) return H266_OK;
+  for (int d = 0; d < 2; ++d) plan.comp[d].clear();
   if (params.bit_depth < 8 || params.bit_depth > 16)
     return set_error(H266_ERR_INVALID_ARGUMENT, "deblock: bit_depth must be 8..16");
   if (params.ctb_log2_size_y > 16) return set_error(H266_ERR_INVALID_ARGUMENT, "deblock: ctb_log2_size_y too large");
