@@ -1,0 +1,338 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the B200 in-loop filter chain.
+
+Workload (one step): the whole chain -- LMCS inverse map, deblocking, SAO,
+ALF and CC-ALF -- over a batch of seeded synthetic 1920x1080 4:2:0 10-bit
+pictures generated like the 1080p benchmark config (50 % inter CUs with a
+motion grid, 4 luma ALF APSs switched per CTU, CC-ALF, LMCS).  The batch's
+planes (199 MB for 32 pictures) exceed the 126 MB L2, so no flush is needed.
+
+  value     device-resident throughput: side information resident in resident
+            plans (h266_chain_plan_*), samples resident in HBM, CUDA-event
+            timed on the stream the library launches on, max over ranks.
+  e2e       the same work through the reference-facing call
+            h266_apply_in_loop_filters with host (pinned) buffers: per picture
+            the side-information build, H2D copies, kernels and D2H copies.
+  roofline  the SAO/ALF tile kernel (the top kernel) timed per launch with
+            CUDA events inside the run, against the measured HBM copy
+            bandwidth.
+  cpu_baseline  the oracle (C++ restatement of the crate's filters) on all
+            host cores, one picture per thread, on a bounded sample.
+
+Multi-GPU: replicas (pictures are independent; no collective on the data
+path), each rank filters its own batch; weak scaling.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+WIDTH, HEIGHT, BITDEPTH = 1920, 1080, 10
+METRIC = "filter-chain Mpx/s 1080p/2160p 10-bit bit-exact"
+# DRAM bytes per luma pixel of the SAO/ALF kernel from `ncu` (profiles/); None until captured
+SAO_ALF_TRAFFIC_PER_PX = None
+
+
+def _import_pkg():
+    pkg = ROOT / "oxideav-h266_b200"
+    if "oxideav_h266_b200" not in sys.modules:
+        spec = importlib.util.spec_from_file_location("oxideav_h266_b200", pkg / "__init__.py",
+                                                      submodule_search_locations=[str(pkg)])
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules["oxideav_h266_b200"] = mod
+        spec.loader.exec_module(mod)
+    if str(ROOT) not in sys.path:
+        sys.path.insert(0, str(ROOT))
+
+
+def measured_peaks():
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text()), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8 and parts[0].replace(".", "").isdigit():
+                rows.append(parts)
+        try:
+            self.path.unlink()
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[0]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[4:8]) if v.lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][1]), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())}
+
+
+def bad_clocks(c):
+    if any(r in c.get("reasons", []) for r in ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown")):
+        return True
+    sm, mx = c.get("sm_mhz"), c.get("sm_max_mhz")
+    return bool(sm and mx and sm < 0.5 * mx and "sw_power_cap" not in c.get("reasons", []))
+
+
+def make_batch(rank: int, n: int):
+    from oxideav_h266_b200 import workloads as W
+
+    return [W.config2(2000 + 1000 * rank + i, WIDTH, HEIGHT) for i in range(n)]
+
+
+def cpu_baseline(items, threads: int):
+    """Oracle chain on `threads` host threads over a bounded sample (each
+    picture of the batch twice)."""
+    import oracle
+
+    pics = [p.copy() for p, _ in items] * 2
+    fas = [f for _, f in items] * 2
+    oracle.lib()
+    t0 = time.perf_counter()
+    used = oracle.apply_in_loop_filters_mt(pics, fas, threads)
+    dt = time.perf_counter() - t0
+    mpx = len(pics) * WIDTH * HEIGHT / 1e6
+    return {"value": round(mpx / dt, 2), "unit": "Mpx/s", "cores": used, "kind": "port",
+            "sample": f"{len(pics)} pictures 1920x1080 10-bit (chain), one per thread, {dt:.1f} s wall"}
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    from oxideav_h266_b200 import native
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    items = make_batch(rank, args.batch)
+    ctx = native.Context(local_rank)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    dev = [native.DevicePicture.from_host(p, local_rank) for p, _ in items]
+    plans = [ctx.plan(p, f) for p, f in items]
+    torch.cuda.synchronize()
+
+    def step():
+        for pl, d in zip(plans, dev):
+            pl.execute(d)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    props = torch.cuda.get_device_properties(local_rank)
+    gpu_id = f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(local_rank)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    for attempt in range(2):
+        barrier()
+        torch.cuda.synchronize()
+        l0 = ctx.kernel_launches
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(gpu_id) as cs:
+            start.record(stream)
+            for _ in range(args.steps):
+                step()
+            end.record(stream)
+            torch.cuda.synchronize()
+        barrier()
+        ms = start.elapsed_time(end)
+        launches = ctx.kernel_launches - l0
+        clocks = cs.summary()
+        if not bad_clocks(clocks):
+            break
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    px_per_step = args.batch * WIDTH * HEIGHT
+    value = world * px_per_step * args.steps / (ms_max / 1e3) / 1e6
+
+    # roofline of the SAO/ALF tile kernel: per-launch CUDA-event durations in a profiled run
+    ctx.set_profiling(True)
+    prof_steps = min(args.steps, 5)
+    for _ in range(prof_steps):
+        step()
+    prof = ctx.profile()
+    ctx.set_profiling(False)
+    ms_sa, n_sa = prof["sao_alf"]
+    alg_bytes = 6 * WIDTH * HEIGHT  # u16 4:2:0 planes read once + written once per launch (one picture)
+    per_launch_s = ms_sa / max(n_sa, 1) / 1e3
+    peaks, peak_kind = measured_peaks()
+    achieved = alg_bytes / per_launch_s / 1e9
+    total_ms = sum(v[0] for v in prof.values())
+    roofline = {
+        "kernel": "k_sao_alf (SAO + ALF classification + 7x7/5x5 + CC-ALF tile pass)",
+        "bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+        "frac": round(achieved / peaks["hbm_gbs"], 4), "peak_source": peak_kind,
+        "traffic": (round(SAO_ALF_TRAFFIC_PER_PX * WIDTH * HEIGHT) if SAO_ALF_TRAFFIC_PER_PX else None),
+        "algorithmic_bytes_per_launch": alg_bytes, "launch_us": round(per_launch_s * 1e6, 2),
+        "share_of_device_time": {k: round(v[0] / total_ms, 3) for k, v in prof.items() if total_ms > 0},
+    }
+
+    # e2e: reference-facing call with pinned host buffers
+    e2e = None
+    if rank == 0 or world > 1:
+        host = []
+        for p, f in items:
+            planes = []
+            for a in p.planes():
+                t_ = torch.empty(a.shape, dtype=torch.int16, pin_memory=True)
+                arr = t_.numpy().view(np.uint16)
+                arr[...] = a
+                planes.append((t_, arr))
+            from oxideav_h266_b200.workloads import PictureData
+
+            host.append((PictureData(*[x[1] for x in planes], p.bit_depth), planes, f))
+        e_steps = max(1, min(args.steps, 3))
+        for hp, _, f in host[:2]:
+            ctx.apply_in_loop_filters(hp, f)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e_steps):
+            for hp, _, f in host:
+                ctx.apply_in_loop_filters(hp, f)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        te = torch.tensor([dt], dtype=torch.float64, device="cuda")
+        if dist:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        plane_bytes = sum(a.nbytes for p, _ in items for a in p.planes())
+        e2e = {"value": round(world * px_per_step * e_steps / float(te.item()) / 1e6, 2), "unit": "Mpx/s",
+               "h2d_bytes_per_step": plane_bytes, "d2h_bytes_per_step": plane_bytes,
+               "path": "h266_apply_in_loop_filters, H266_MEM_HOST pinned planes, side info built per call"}
+
+    cpu = None
+    if rank == 0 and world == 1:
+        cpu = cpu_baseline(items[:16], os.cpu_count() or 1)
+
+    for pl in plans:
+        pl.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": "Mpx/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic (seeded 1080p config generator)",
+            "config": {"workload": f"c2_1080p10_x{args.batch}", "width": WIDTH, "height": HEIGHT,
+                       "bit_depth": BITDEPTH, "pictures_per_step_per_gpu": args.batch,
+                       "chain": "LMCS-1 -> deblock -> SAO -> ALF -> CC-ALF", "parallelism": f"replicas x{world}",
+                       "l2": f"inputs larger than L2 ({args.batch * 6.2:.0f} MB per GPU)"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    ctx.close()
+
+
+def run_reference(args, rank, world):
+    """CPU reference arm: the oracle restatement of the crate's chain on all host
+    threads (the Rust crate cannot be built here)."""
+    if rank != 0:
+        return
+    import oracle
+
+    threads = os.cpu_count() or 1
+    per_step = max(threads, 4)
+    items = make_batch(0, per_step)
+    oracle.lib()
+    times = []
+    for i in range(args.warmup + args.steps):
+        pics = [p.copy() for p, _ in items]
+        t0 = time.perf_counter()
+        oracle.apply_in_loop_filters_mt(pics, [f for _, f in items], threads)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    total = sum(times)
+    value = per_step * WIDTH * HEIGHT * len(times) / total / 1e6
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "Mpx/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total / len(times) * 1e3, 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic (seeded 1080p config generator)",
+        "config": {"workload": f"c2_1080p10_x{per_step}", "width": WIDTH, "height": HEIGHT, "bit_depth": BITDEPTH},
+        "impl": "reference",
+        "cpu_baseline": {"value": round(value, 2), "unit": "Mpx/s", "cores": threads, "kind": "port",
+                         "sample": f"{per_step} pictures per step, one per thread"},
+        "e2e": {"value": round(value, 2), "unit": "Mpx/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    _import_pkg()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -261,6 +261,19 @@ const char *h266_last_error(void);
 /* Number of kernels this context has launched since creation. */
 uint64_t h266_ctx_kernel_launches(const h266_ctx *ctx);
 
+/* Per-kernel-family device time, for metrics and roofline accounting.  No
+ * counterpart in the crate.  While profiling is on, every launch is bracketed
+ * by CUDA events on the context's stream; h266_ctx_profile synchronizes the
+ * stream, returns the accumulated milliseconds and launch counts per family
+ * and resets them. */
+#define H266_PROF_LMCS 0    /* LMCS LUT build and LUT-mapped plane copy      */
+#define H266_PROF_DEBLOCK 1 /* deblocking edge-segment passes               */
+#define H266_PROF_SAO_ALF 2 /* SAO / ALF / CC-ALF tile pass                 */
+#define H266_PROF_COPY 3    /* plain plane copies into scratch              */
+#define H266_PROF_FAMILIES 4
+int h266_ctx_set_profiling(h266_ctx *ctx, int on);
+int h266_ctx_profile(h266_ctx *ctx, double ms[H266_PROF_FAMILIES], uint64_t launches[H266_PROF_FAMILIES]);
+
 /* ---- filters ------------------------------------------------------------ */
 
 /* LmcsData::derive / derive_lmcs (src/lmcs.rs:113, 302-404): the §7.4.3.19
@@ -302,6 +315,22 @@ int h266_apply_in_loop_filters(h266_ctx *ctx, h266_picture *pic, const h266_in_l
  * the crate, which filters one picture per call (src/stream.rs:768). */
 int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *const *pics,
                                      const h266_in_loop_filter_args *const *args);
+
+/* ---- resident plans ------------------------------------------------------
+ * A plan holds one picture's filter side information on the device (deblock
+ * edge segments, CTB parameter and APS tables, LMCS LUT) plus its scratch
+ * planes, so the chain can run again on new samples with no host work.  No
+ * counterpart in the crate, which rebuilds everything per call
+ * (src/ctu.rs:11822-12065); the encoder's repeated ALF trials
+ * (src/alf_enc.rs:244-1055) and a serving loop that keeps per-stream state
+ * resident are the users.  `pic` gives only the plane sizes and bit depth at
+ * create time; execute takes device planes of exactly that geometry and runs
+ * asynchronously on the context's stream. */
+typedef struct h266_chain_plan h266_chain_plan;
+int h266_chain_plan_create(h266_ctx *ctx, const h266_picture *pic, const h266_in_loop_filter_args *args,
+                           h266_chain_plan **out);
+int h266_chain_plan_execute(h266_ctx *ctx, h266_chain_plan *plan, h266_picture *pic);
+int h266_chain_plan_destroy(h266_chain_plan *plan);
 
 #ifdef __cplusplus
 }

@@ -84,6 +84,25 @@ struct h266_ctx {
   Staging stage;
   DeblockPlan plan;
   std::vector<uint8_t> blob;  // side information assembled on the host
+  // profiling: CUDA events around every launch, resolved in h266_ctx_profile
+  bool prof = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
+  double prof_ms[H266_PROF_FAMILIES] = {0};
+  uint64_t prof_n[H266_PROF_FAMILIES] = {0};
+};
+
+// A chain whose side information is resident on the device (h266_chain_plan_create).
+struct h266_chain_plan {
+  int device = 0;
+  h266_picture geom{};  // plane sizes / bit depths the plan was built for
+  h266::DevBuf side, lut, scratch[3];
+  bool lmcs = false, pass2 = false;
+  int deblock_bd = 8;
+  uint32_t n_comp[2] = {0, 0};
+  size_t off_seg[2] = {0, 0}, off_comp[2] = {0, 0}, off_ctb = 0, off_tab = 0;
+  h266::Pass2Args args{};
+  bool do_sao = false, do_alf = false;
 };
 
 namespace {
@@ -98,6 +117,36 @@ struct Guard {  // makes the context's device current for the call
     int cur = -1;
     cudaGetDevice(&cur);
     if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// Brackets a launch with profiling events when profiling is on.
+struct Prof {
+  h266_ctx *ctx;
+  int fam;
+  cudaEvent_t a = nullptr;
+  static cudaEvent_t take(h266_ctx *c) {
+    if (!c->ev_pool.empty()) {
+      cudaEvent_t e = c->ev_pool.back();
+      c->ev_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+  }
+  Prof(h266_ctx *c, int family) : ctx(c), fam(family) {
+    if (ctx->prof) {
+      a = take(ctx);
+      cudaEventRecord(a, ctx->stream);
+    }
+  }
+  ~Prof() {
+    if (a) {
+      cudaEvent_t b = take(ctx);
+      cudaEventRecord(b, ctx->stream);
+      ctx->ev_pending.push_back({fam, {a, b}});
+    }
   }
 };
 
@@ -428,16 +477,17 @@ void stage_pass2(h266_ctx *ctx, const Pass2Host &h, Staged &st) {
 }
 
 // Runs pass 2 (SAO and/or ALF) from `src` into the picture planes `dst`.
-int run_pass2(h266_ctx *ctx, Pass2Host &h, const Staged &st, const DPlane src[3], const DPlane dst[3]) {
-  Pass2Args &a = h.args;
+int run_pass2(h266_ctx *ctx, Pass2Args a, bool do_sao, bool do_alf, const uint8_t *base, size_t off_ctb,
+              size_t off_tab, const DPlane src[3], const DPlane dst[3]) {
   for (int i = 0; i < 3; ++i) {
     a.src[i] = src[i];
     a.dst[i] = dst[i];
   }
-  a.ctbs = reinterpret_cast<const CtbDev *>(st.base + st.ctb);
-  a.tables.luma_coeff = reinterpret_cast<int32_t *>(st.base + st.tab);  // per slot: coeff[300], clip[300]
+  a.ctbs = reinterpret_cast<const CtbDev *>(base + off_ctb);
+  a.tables.luma_coeff = reinterpret_cast<const int32_t *>(base + off_tab);  // per slot: coeff[300], clip[300]
   a.tables.luma_clip = a.tables.luma_coeff + 300;
-  return launch_pass2(ctx->stream, a, h.do_sao, h.do_alf, &ctx->launches);
+  Prof pf(ctx, H266_PROF_SAO_ALF);
+  return launch_pass2(ctx->stream, a, do_sao, do_alf, &ctx->launches);
 }
 
 int ensure_scratch(h266_ctx *ctx, const DPlane p[3], DPlane s[3]) {
@@ -449,13 +499,23 @@ int ensure_scratch(h266_ctx *ctx, const DPlane p[3], DPlane s[3]) {
   return H266_OK;
 }
 
-int run_deblock(h266_ctx *ctx, const Staged &st, const DPlane planes[3], int bd) {
-  DeblockPlan &pl = ctx->plan;
-  return launch_deblock(ctx->stream, planes, bd, reinterpret_cast<const EdgeSeg *>(st.base + st.seg[0]),
-                        reinterpret_cast<const uint32_t *>(st.base + st.comp[0]), (uint32_t)pl.comp[0].size() - 1,
-                        reinterpret_cast<const EdgeSeg *>(st.base + st.seg[1]),
-                        reinterpret_cast<const uint32_t *>(st.base + st.comp[1]), (uint32_t)pl.comp[1].size() - 1,
-                        &ctx->launches);
+int run_deblock(h266_ctx *ctx, const uint8_t *base, const size_t off_seg[2], const size_t off_comp[2],
+                const uint32_t n_comp[2], const DPlane planes[3], int bd) {
+  Prof pf(ctx, H266_PROF_DEBLOCK);
+  return launch_deblock(ctx->stream, planes, bd, reinterpret_cast<const EdgeSeg *>(base + off_seg[0]),
+                        reinterpret_cast<const uint32_t *>(base + off_comp[0]), n_comp[0],
+                        reinterpret_cast<const EdgeSeg *>(base + off_seg[1]),
+                        reinterpret_cast<const uint32_t *>(base + off_comp[1]), n_comp[1], &ctx->launches);
+}
+
+int plane_map(h266_ctx *ctx, DPlane dst, DPlane src, const uint16_t *lut) {
+  Prof pf(ctx, lut ? H266_PROF_LMCS : H266_PROF_COPY);
+  return launch_plane_map(ctx->stream, dst, src, lut, &ctx->launches);
+}
+
+int build_lut(h266_ctx *ctx, uint16_t *lut, const h266_lmcs_derived &l, uint32_t mn, uint32_t mx) {
+  Prof pf(ctx, H266_PROF_LMCS);
+  return launch_lmcs_lut(ctx->stream, lut, l, mn, mx, &ctx->launches);
 }
 
 int check_lmcs(const h266_lmcs_derived *l, uint32_t mn, uint32_t mx) {
@@ -465,9 +525,19 @@ int check_lmcs(const h266_lmcs_derived *l, uint32_t mn, uint32_t mx) {
   return H266_OK;
 }
 
-// The chain for one picture whose planes are already device views `P`.
-int chain_on_device(h266_ctx *ctx, const h266_picture &pic, const DPlane P[3], const h266_in_loop_filter_args &a) {
+// Host-side preparation of one chain call: deblocking plan (ctx->plan), pass-2
+// tables, and the side-information blob (ctx->blob) with its section offsets.
+struct Prepared {
+  Pass2Host h;
+  Staged st;
+  uint32_t n_comp[2] = {0, 0};
+};
+
+int prepare_chain(h266_ctx *ctx, const h266_picture &pic, const h266_in_loop_filter_args &a, Prepared &pr) {
   H266_TRY(check_lmcs(a.lmcs, a.lmcs_min_bin_idx, a.lmcs_max_bin_idx));
+  if ((a.n_cus && !a.cus) || (a.n_no_filter_cols && !a.no_filter_cols) || (a.n_no_filter_rows && !a.no_filter_rows))
+    return set_error(H266_ERR_INVALID_ARGUMENT, "NULL list with nonzero length");
+  if (a.clip_cols && !a.clip_rows) return set_error(H266_ERR_INVALID_ARGUMENT, "clip_rows is NULL while clip_cols is not");
   H266_TRY(build_deblock_plan(pic, a.cus, a.n_cus, a.chroma_cus, a.n_chroma_cus, a.mv_grid, a.deblock,
                               a.chroma_format_idc, a.no_filter_cols, a.n_no_filter_cols, a.no_filter_rows,
                               a.n_no_filter_rows, ctx->plan));
@@ -481,31 +551,48 @@ int chain_on_device(h266_ctx *ctx, const h266_picture &pic, const DPlane P[3], c
   in.rows = a.clip_rows;
   in.n_cols = a.n_clip_cols;
   in.n_rows = a.n_clip_rows;
-  if (a.clip_cols && !a.clip_rows) return set_error(H266_ERR_INVALID_ARGUMENT, "clip_rows is NULL while clip_cols is not");
-  Pass2Host h;
-  H266_TRY(build_pass2(pic, in, h));
+  H266_TRY(build_pass2(pic, in, pr.h));
+  ctx->blob.clear();
+  stage_deblock(ctx, pr.st);
+  if (pr.h.do_sao || pr.h.do_alf) stage_pass2(ctx, pr.h, pr.st);
+  for (int d = 0; d < 2; ++d) pr.n_comp[d] = (uint32_t)ctx->plan.comp[d].size() - 1;
+  return H266_OK;
+}
+
+// Launches the chain: LMCS (LUT already built) -> deblock -> SAO/ALF.  With a
+// pass 2 the deblocked planes go to the scratch planes S, else in place.
+int exec_chain(h266_ctx *ctx, const uint8_t *base, const Staged &st, const uint32_t n_comp[2], const Pass2Host &h,
+               const uint16_t *lut, int dbd, const DPlane P[3], const DPlane S[3]) {
+  if (!h.do_sao && !h.do_alf) {
+    if (lut) H266_TRY(plane_map(ctx, P[0], P[0], lut));
+    return run_deblock(ctx, base, st.seg, st.comp, n_comp, P, dbd);
+  }
+  for (int i = 0; i < 3; ++i) H266_TRY(plane_map(ctx, S[i], P[i], i == 0 ? lut : nullptr));
+  H266_TRY(run_deblock(ctx, base, st.seg, st.comp, n_comp, S, dbd));
+  return run_pass2(ctx, h.args, h.do_sao, h.do_alf, base, st.ctb, st.tab, S, P);
+}
+
+// The chain for one picture whose planes are already device views `P`.
+int chain_on_device(h266_ctx *ctx, const h266_picture &pic, const DPlane P[3], const h266_in_loop_filter_args &a) {
+  Prepared pr;
+  H266_TRY(prepare_chain(ctx, pic, a, pr));
+  H266_TRY(upload_blob(ctx, &pr.st.base));
   const uint16_t *lut = nullptr;
   if (a.lmcs) {
     H266_TRY(ctx->lut.ensure(65536 * 2));
-    H266_TRY(launch_lmcs_lut(ctx->stream, ctx->lut.as<uint16_t>(), *a.lmcs, a.lmcs_min_bin_idx, a.lmcs_max_bin_idx,
-                             &ctx->launches));
+    H266_TRY(build_lut(ctx, ctx->lut.as<uint16_t>(), *a.lmcs, a.lmcs_min_bin_idx, a.lmcs_max_bin_idx));
     lut = ctx->lut.as<uint16_t>();
   }
-  const int dbd = (int)a.deblock.bit_depth;
-  Staged st;
-  ctx->blob.clear();
-  stage_deblock(ctx, st);
-  if (h.do_sao || h.do_alf) stage_pass2(ctx, h, st);
-  H266_TRY(upload_blob(ctx, &st.base));
-  if (!h.do_sao && !h.do_alf) {  // everything in place on the picture
-    if (lut) H266_TRY(launch_plane_map(ctx->stream, P[0], P[0], lut, &ctx->launches));
-    return run_deblock(ctx, st, P, dbd);
-  }
   DPlane S[3];
-  H266_TRY(ensure_scratch(ctx, P, S));
-  for (int i = 0; i < 3; ++i) H266_TRY(launch_plane_map(ctx->stream, S[i], P[i], i == 0 ? lut : nullptr, &ctx->launches));
-  H266_TRY(run_deblock(ctx, st, S, dbd));
-  return run_pass2(ctx, h, st, S, P);
+  if (pr.h.do_sao || pr.h.do_alf) H266_TRY(ensure_scratch(ctx, P, S));
+  return exec_chain(ctx, pr.st.base, pr.st, pr.n_comp, pr.h, lut, (int)a.deblock.bit_depth, P, S);
+}
+
+bool same_geometry(const h266_picture &a, const h266_picture &b) {
+  const h266_plane *x[3] = {&a.luma, &a.cb, &a.cr}, *y[3] = {&b.luma, &b.cb, &b.cr};
+  for (int i = 0; i < 3; ++i)
+    if (x[i]->width != y[i]->width || x[i]->height != y[i]->height || x[i]->bit_depth != y[i]->bit_depth) return false;
+  return true;
 }
 
 }  // namespace
@@ -585,8 +672,8 @@ int h266_lmcs_inverse_map_luma(h266_ctx *ctx, h266_picture *pic, const h266_lmcs
   DPlane P[3];
   H266_TRY(picture_to_device(ctx, *pic, P));
   H266_TRY(ctx->lut.ensure(65536 * 2));
-  H266_TRY(launch_lmcs_lut(ctx->stream, ctx->lut.as<uint16_t>(), *lmcs, mn, mx, &ctx->launches));
-  H266_TRY(launch_plane_map(ctx->stream, P[0], P[0], ctx->lut.as<uint16_t>(), &ctx->launches));
+  H266_TRY(build_lut(ctx, ctx->lut.as<uint16_t>(), *lmcs, mn, mx));
+  H266_TRY(plane_map(ctx, P[0], P[0], ctx->lut.as<uint16_t>()));
   return picture_from_device(ctx, *pic);
 }
 
@@ -609,7 +696,8 @@ int h266_apply_deblocking_clipped(h266_ctx *ctx, h266_picture *pic, const h266_d
   ctx->blob.clear();
   stage_deblock(ctx, st);
   H266_TRY(upload_blob(ctx, &st.base));
-  H266_TRY(run_deblock(ctx, st, P, (int)params->bit_depth));
+  const uint32_t n_comp[2] = {(uint32_t)ctx->plan.comp[0].size() - 1, (uint32_t)ctx->plan.comp[1].size() - 1};
+  H266_TRY(run_deblock(ctx, st.base, st.seg, st.comp, n_comp, P, (int)params->bit_depth));
   return picture_from_device(ctx, *pic);
 }
 
@@ -629,8 +717,8 @@ static int pass2_entry(h266_ctx *ctx, h266_picture *pic, const Pass2Inputs &in) 
     H266_TRY(upload_blob(ctx, &st.base));
     DPlane S[3];
     H266_TRY(ensure_scratch(ctx, P, S));
-    for (int i = 0; i < 3; ++i) H266_TRY(launch_plane_map(ctx->stream, S[i], P[i], nullptr, &ctx->launches));
-    H266_TRY(run_pass2(ctx, h, st, S, P));
+    for (int i = 0; i < 3; ++i) H266_TRY(plane_map(ctx, S[i], P[i], nullptr));
+    H266_TRY(run_pass2(ctx, h.args, h.do_sao, h.do_alf, st.base, st.ctb, st.tab, S, P));
   }
   return picture_from_device(ctx, *pic);
 }
@@ -680,6 +768,131 @@ int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *co
   H266_TRY(check_ctx(ctx));
   if (n && (!pics || !args)) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL batch arrays");
   for (uint32_t i = 0; i < n; ++i) H266_TRY(h266_apply_in_loop_filters(ctx, pics[i], args[i]));
+  return H266_OK;
+}
+
+int h266_ctx_set_profiling(h266_ctx *ctx, int on) {
+  H266_TRY(check_ctx(ctx));
+  ctx->prof = on != 0;
+  return H266_OK;
+}
+
+int h266_ctx_profile(h266_ctx *ctx, double ms[H266_PROF_FAMILIES], uint64_t launches[H266_PROF_FAMILIES]) {
+  H266_TRY(check_ctx(ctx));
+  Guard g(ctx->device);
+  H266_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (auto &e : ctx->ev_pending) {
+    float t = 0;
+    H266_CUDA(cudaEventElapsedTime(&t, e.second.first, e.second.second));
+    ctx->prof_ms[e.first] += t;
+    ctx->prof_n[e.first] += 1;
+    ctx->ev_pool.push_back(e.second.first);
+    ctx->ev_pool.push_back(e.second.second);
+  }
+  ctx->ev_pending.clear();
+  for (int i = 0; i < H266_PROF_FAMILIES; ++i) {
+    if (ms) ms[i] = ctx->prof_ms[i];
+    if (launches) launches[i] = ctx->prof_n[i];
+    ctx->prof_ms[i] = 0;
+    ctx->prof_n[i] = 0;
+  }
+  return H266_OK;
+}
+
+int h266_chain_plan_create(h266_ctx *ctx, const h266_picture *pic, const h266_in_loop_filter_args *args,
+                           h266_chain_plan **out) {
+  H266_TRY(check_ctx(ctx));
+  if (!out || !args) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL argument");
+  *out = nullptr;
+  if (!pic) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL picture");
+  h266_picture geom = *pic;
+  geom.mem = H266_MEM_DEVICE;
+  h266_plane *gp[3] = {&geom.luma, &geom.cb, &geom.cr};
+  for (h266_plane *p : gp) {  // only the geometry is used; give check_picture a stand-in pointer
+    p->samples = reinterpret_cast<uint16_t *>(uintptr_t(16));
+    if (p->stride < p->width) p->stride = p->width;
+  }
+  H266_TRY(check_picture(&geom));
+  Guard g(ctx->device);
+  Prepared pr;
+  H266_TRY(prepare_chain(ctx, geom, *args, pr));
+  h266_chain_plan *pl = new h266_chain_plan();
+  pl->device = ctx->device;
+  pl->geom = geom;
+  auto fail = [&](int rc) {
+    h266_chain_plan_destroy(pl);
+    return rc;
+  };
+  int rc = pl->side.ensure(ctx->blob.size());
+  if (rc != H266_OK) return fail(rc);
+  cudaError_t e = cudaMemcpy(pl->side.ptr, ctx->blob.data(), ctx->blob.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return fail(cuda_error(e, "plan upload"));
+  pl->lmcs = args->lmcs != nullptr;
+  if (pl->lmcs) {
+    if ((rc = pl->lut.ensure(65536 * 2)) != H266_OK) return fail(rc);
+    if ((rc = build_lut(ctx, pl->lut.as<uint16_t>(), *args->lmcs, args->lmcs_min_bin_idx, args->lmcs_max_bin_idx)) !=
+        H266_OK)
+      return fail(rc);
+  }
+  pl->pass2 = pr.h.do_sao || pr.h.do_alf;
+  if (pl->pass2) {
+    const h266_plane *sp[3] = {&geom.luma, &geom.cb, &geom.cr};
+    for (int i = 0; i < 3; ++i)
+      if ((rc = pl->scratch[i].ensure(std::max<size_t>((size_t)sp[i]->width * sp[i]->height, 1) * 2)) != H266_OK)
+        return fail(rc);
+  }
+  pl->deblock_bd = (int)args->deblock.bit_depth;
+  for (int d = 0; d < 2; ++d) {
+    pl->n_comp[d] = pr.n_comp[d];
+    pl->off_seg[d] = pr.st.seg[d];
+    pl->off_comp[d] = pr.st.comp[d];
+  }
+  pl->off_ctb = pr.st.ctb;
+  pl->off_tab = pr.st.tab;
+  pl->args = pr.h.args;
+  pl->do_sao = pr.h.do_sao;
+  pl->do_alf = pr.h.do_alf;
+  e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return fail(cuda_error(e, "plan LUT"));
+  *out = pl;
+  return H266_OK;
+}
+
+int h266_chain_plan_execute(h266_ctx *ctx, h266_chain_plan *plan, h266_picture *pic) {
+  H266_TRY(check_ctx(ctx));
+  if (!plan) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL plan");
+  H266_TRY(check_picture(pic));
+  if (pic->mem != H266_MEM_DEVICE) return set_error(H266_ERR_INVALID_ARGUMENT, "plans execute on device pictures");
+  if (!same_geometry(*pic, plan->geom)) return set_error(H266_ERR_INVALID_ARGUMENT, "picture geometry differs from the plan");
+  if (plan->device != ctx->device) return set_error(H266_ERR_INVALID_ARGUMENT, "plan belongs to another device");
+  Guard g(ctx->device);
+  DPlane P[3], S[3];
+  H266_TRY(picture_to_device(ctx, *pic, P));
+  for (int i = 0; i < 3; ++i)
+    S[i] = DPlane{plan->pass2 ? plan->scratch[i].as<uint16_t>() : nullptr, std::max(P[i].w, 1), P[i].w, P[i].h};
+  Staged st;
+  st.base = plan->side.as<uint8_t>();
+  for (int d = 0; d < 2; ++d) {
+    st.seg[d] = plan->off_seg[d];
+    st.comp[d] = plan->off_comp[d];
+  }
+  st.ctb = plan->off_ctb;
+  st.tab = plan->off_tab;
+  Pass2Host h;
+  h.args = plan->args;
+  h.do_sao = plan->do_sao;
+  h.do_alf = plan->do_alf;
+  return exec_chain(ctx, st.base, st, plan->n_comp, h, plan->lmcs ? plan->lut.as<uint16_t>() : nullptr,
+                    plan->deblock_bd, P, S);
+}
+
+int h266_chain_plan_destroy(h266_chain_plan *plan) {
+  if (!plan) return H266_OK;
+  Guard g(plan->device);
+  plan->side.release();
+  plan->lut.release();
+  for (auto &b : plan->scratch) b.release();
+  delete plan;
   return H266_OK;
 }
 

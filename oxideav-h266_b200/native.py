@@ -31,8 +31,10 @@ EXPORTS = [
     "h266_ctx_create", "h266_ctx_destroy", "h266_ctx_set_stream", "h266_ctx_synchronize", "h266_last_error",
     "h266_ctx_kernel_launches", "h266_derive_lmcs", "h266_lmcs_inverse_map_luma", "h266_apply_deblocking_clipped",
     "h266_apply_sao_clipped", "h266_apply_alf_clipped", "h266_apply_in_loop_filters",
-    "h266_apply_in_loop_filters_batch",
+    "h266_apply_in_loop_filters_batch", "h266_ctx_set_profiling", "h266_ctx_profile", "h266_chain_plan_create",
+    "h266_chain_plan_execute", "h266_chain_plan_destroy",
 ]
+PROF_FAMILIES = ("lmcs", "deblock", "sao_alf", "copy")
 
 
 class H266Error(RuntimeError):
@@ -62,6 +64,11 @@ def lib():
         L.h266_apply_alf_clipped.argtypes = [vp, vp, vp, vp, vp, vp, u64, vp, u64]
         L.h266_apply_in_loop_filters.argtypes = [vp, vp, vp]
         L.h266_apply_in_loop_filters_batch.argtypes = [vp, u32, vp, vp]
+        L.h266_ctx_set_profiling.argtypes = [vp, i32]
+        L.h266_ctx_profile.argtypes = [vp, vp, vp]
+        L.h266_chain_plan_create.argtypes = [vp, vp, vp, C.POINTER(vp)]
+        L.h266_chain_plan_execute.argtypes = [vp, vp, vp]
+        L.h266_chain_plan_destroy.argtypes = [vp]
         _LIB = L
     return _LIB
 
@@ -153,6 +160,19 @@ class Context:
     def set_stream(self, stream_ptr: int | None):
         _check(lib().h266_ctx_set_stream(self._h, stream_ptr))
 
+    def set_profiling(self, on: bool):
+        _check(lib().h266_ctx_set_profiling(self._h, int(on)))
+
+    def profile(self) -> dict:
+        """{family: (ms, launches)} accumulated since the last read (synchronizes)."""
+        ms = (C.c_double * 4)()
+        n = (C.c_uint64 * 4)()
+        _check(lib().h266_ctx_profile(self._h, ms, n))
+        return {f: (ms[i], n[i]) for i, f in enumerate(PROF_FAMILIES)}
+
+    def plan(self, pic, fa: FilterArgsData) -> "ChainPlan":
+        return ChainPlan(self, pic, fa)
+
     # -- filters ----------------------------------------------------------
     def apply_in_loop_filters(self, pic, fa: FilterArgsData):
         cp = pic.to_ctypes()
@@ -199,3 +219,30 @@ class Context:
         cp = pic.to_ctypes()
         _check(lib().h266_lmcs_inverse_map_luma(self._h, C.byref(cp), C.byref(fa.lmcs), fa.lmcs_min_bin,
                                                 fa.lmcs_max_bin))
+
+
+class ChainPlan:
+    """h266_chain_plan: one picture's side information resident on the device."""
+
+    def __init__(self, ctx: Context, pic, fa: FilterArgsData):
+        self.ctx = ctx
+        cp = pic.to_ctypes()
+        a, keep = fa.to_ctypes()
+        h = C.c_void_p()
+        _check(lib().h266_chain_plan_create(ctx._h, C.byref(cp), C.byref(a), C.byref(h)))
+        self._h = h
+
+    def execute(self, pic: DevicePicture):
+        cp = pic.to_ctypes()
+        _check(lib().h266_chain_plan_execute(self.ctx._h, self._h, C.byref(cp)))
+
+    def close(self):
+        if self._h:
+            lib().h266_chain_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

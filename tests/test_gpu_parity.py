@@ -153,3 +153,29 @@ def test_unsupported_ctb_size_is_rejected(ctx):
     with pytest.raises(native.H266Error) as e:
         ctx.apply_sao_clipped(pic.copy(), fa)
     assert e.value.code == -7
+
+
+def test_resident_plan_matches_direct_chain(ctx):
+    pic, fa = small_c2(21)
+    want = pic.copy()
+    oracle.apply_in_loop_filters(want, fa)
+    plan = ctx.plan(pic, fa)
+    dev = native.DevicePicture.from_host(pic)
+    plan.execute(dev)
+    ctx.synchronize()
+    assert_same(dev.to_host(), want, "plan")
+    dev2 = native.DevicePicture.from_host(pic)  # the plan runs again on fresh samples
+    plan.execute(dev2)
+    ctx.synchronize()
+    assert_same(dev2.to_host(), want, "plan rerun")
+    plan.close()
+
+
+def test_profiling_counts_every_family(ctx):
+    pic, fa = small_c2(22)
+    ctx.set_profiling(True)
+    ctx.apply_in_loop_filters(pic.copy(), fa)
+    prof = ctx.profile()
+    ctx.set_profiling(False)
+    assert prof["deblock"][1] == 2 and prof["sao_alf"][1] == 1 and prof["lmcs"][1] == 2
+    assert all(ms >= 0 for ms, _ in prof.values())
