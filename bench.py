@@ -65,7 +65,7 @@ def measured_peaks():
 class ClockSampler:
     """nvidia-smi clock / throttle sampling during the timed region."""
 
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
 
@@ -78,7 +78,7 @@ class ClockSampler:
         try:
             self.path.parent.mkdir(exist_ok=True)
             self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={self.FIELDS}",
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
         except Exception:
@@ -98,10 +98,13 @@ class ClockSampler:
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         rows = []
-        for line in self.path.read_text().splitlines():
+        lines = self.path.read_text().splitlines()
+        uuids = {l.split(",")[0].strip() for l in lines if l.count(",") >= 8}
+        mine = self.gpu_id if self.gpu_id in uuids else (sorted(uuids)[0] if len(uuids) == 1 else None)
+        for line in lines:
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 8 and parts[0].replace(".", "").isdigit():
-                rows.append(parts)
+            if len(parts) >= 9 and parts[0] == mine and parts[1].replace(".", "").isdigit():
+                rows.append(parts[1:])
         try:
             self.path.unlink()
         except Exception:
@@ -175,7 +178,7 @@ def run_ours(args, rank, world, local_rank):
             dist.barrier()
 
     props = torch.cuda.get_device_properties(local_rank)
-    gpu_id = f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(local_rank)
+    gpu_id = f"GPU-{props.uuid}" if getattr(props, "uuid", None) else ""
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
