@@ -332,6 +332,28 @@ int h266_chain_plan_create(h266_ctx *ctx, const h266_picture *pic, const h266_in
 int h266_chain_plan_execute(h266_ctx *ctx, h266_chain_plan *plan, h266_picture *pic);
 int h266_chain_plan_destroy(h266_chain_plan *plan);
 
+/* ---- allocation-free chain ---------------------------------------------------
+ * No counterpart in the reference.  The whole chain (as h266_apply_in_loop_filters)
+ * on device planes, for callers that cannot call cudaMalloc at run time: code
+ * running inside CUDA-graph stream capture, real-time decode loops that ban
+ * allocator calls once streaming starts, hosts whose device memory belongs to
+ * their own pool.  The call allocates nothing: its scratch (side information,
+ * LMCS LUT, deblocked planes) lives in one fixed device array of
+ * H266_NOALLOC_SCRATCH_BYTES that every GPU loading the library keeps until the
+ * process exits.  The caller passes the picture (H266_MEM_DEVICE planes,
+ * filtered in place) and the stream (NULL = legacy default stream).
+ *   - Pictures whose scratch need exceeds the array are rejected with
+ *     H266_ERR_UNSUPPORTED and a message naming both sizes (1920x1080 4:2:0
+ *     fits; 3840x2160 does not).
+ *   - The first call on a device looks up the array's device address; make that
+ *     first call before any stream capture begins.
+ *   - All calls share the one array and every call overwrites it: calls whose
+ *     work overlaps on the GPU (other streams, other threads) race.  Serialize
+ *     them on one stream.
+ *   - Host-side side-information building still uses ordinary host memory. */
+#define H266_NOALLOC_SCRATCH_BYTES (16u << 20)
+int h266_apply_in_loop_filters_noalloc(h266_picture *pic, const h266_in_loop_filter_args *args, void *cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

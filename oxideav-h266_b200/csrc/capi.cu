@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 
 #include "fixed_filters.h"
@@ -897,3 +898,93 @@ int h266_chain_plan_destroy(h266_chain_plan *plan) {
 }
 
 }  // extern "C"
+
+// ======================================================================= allocation-free chain
+//
+// For callers that must not allocate device memory at run time: code running
+// while a CUDA graph is being captured, real-time decode loops that forbid
+// allocator calls (and their latency) once streaming has started, and hosts
+// that hand the whole device budget to their own pool.  The chain's scratch --
+// the side information of the call, the LMCS LUT and the deblocked planes the
+// SAO / ALF pass reads -- lives in this fixed device array instead of in a
+// context.  Every GPU that loads the library holds the array until the process
+// exits.
+namespace {
+
+static __device__ __align__(256) uint8_t g_noalloc_scratch[H266_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 256;
+std::mutex g_noalloc_mu;
+uint8_t *g_noalloc_ptr[kMaxDevices] = {nullptr};
+
+// Device address of g_noalloc_scratch on the current device.  In host code the
+// symbol is only a host-side stand-in, so the address is looked up once per
+// device with that device current.
+int noalloc_scratch(uint8_t **out) {
+  int dev = -1;
+  H266_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return set_error(H266_ERR_UNSUPPORTED, "device ordinal beyond 255");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    g_noalloc_ptr[dev] = static_cast<uint8_t *>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return H266_OK;
+}
+
+inline size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+}  // namespace
+
+extern "C" int h266_apply_in_loop_filters_noalloc(h266_picture *pic, const h266_in_loop_filter_args *args,
+                                                  void *cuda_stream) {
+  H266_TRY(check_picture(pic));
+  if (!args) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL args");
+  if (pic->mem != H266_MEM_DEVICE)
+    return set_error(H266_ERR_INVALID_ARGUMENT, "the allocation-free chain takes device planes (H266_MEM_DEVICE)");
+  uint8_t *scratch = nullptr;
+  H266_TRY(noalloc_scratch(&scratch));
+  // A context object on the stack carries the stream and host-side staging
+  // vectors; it owns no device memory and no CUDA handles.
+  h266_ctx local;
+  H266_CUDA(cudaGetDevice(&local.device));
+  local.stream = (cudaStream_t)cuda_stream;
+  Prepared pr;
+  H266_TRY(prepare_chain(&local, *pic, *args, pr));
+  // Scratch layout: [side information][LMCS LUT][three deblocked planes].
+  const size_t blob = align256(local.blob.size());
+  const size_t lut_off = blob, lut_bytes = args->lmcs ? align256(65536 * 2) : 0;
+  size_t planes_off = lut_off + lut_bytes, need = planes_off;
+  const bool pass2 = pr.h.do_sao || pr.h.do_alf;
+  const h266_plane *pl[3] = {&pic->luma, &pic->cb, &pic->cr};
+  size_t plane_off[3] = {0, 0, 0};
+  for (int i = 0; i < 3; ++i) {
+    plane_off[i] = need;
+    if (pass2) need += align256((size_t)pl[i]->width * pl[i]->height * 2);
+  }
+  if (need > H266_NOALLOC_SCRATCH_BYTES)
+    return set_error(H266_ERR_UNSUPPORTED, "picture needs " + std::to_string(need) +
+                                               " bytes of scratch; the allocation-free chain has " +
+                                               std::to_string((size_t)H266_NOALLOC_SCRATCH_BYTES));
+  // Every scratch region is written in full below before anything reads it,
+  // so no region needs clearing.
+  if (!local.blob.empty())
+    H266_CUDA(cudaMemcpyAsync(scratch, local.blob.data(), local.blob.size(), cudaMemcpyHostToDevice, local.stream));
+  pr.st.base = scratch;
+  const uint16_t *lut = nullptr;
+  if (args->lmcs) {
+    uint16_t *l = reinterpret_cast<uint16_t *>(scratch + lut_off);
+    H266_TRY(build_lut(&local, l, *args->lmcs, args->lmcs_min_bin_idx, args->lmcs_max_bin_idx));
+    lut = l;
+  }
+  DPlane P[3], S[3];
+  for (int i = 0; i < 3; ++i) {
+    P[i] = dplane(*pl[i], pl[i]->samples, (int64_t)std::max<uint64_t>(pl[i]->stride, 1));
+    S[i] = DPlane{reinterpret_cast<uint16_t *>(scratch + plane_off[i]), std::max<int>((int)pl[i]->width, 1),
+                  (int)pl[i]->width, (int)pl[i]->height};
+  }
+  return exec_chain(&local, scratch, pr.st, pr.n_comp, pr.h, lut, (int)args->deblock.bit_depth, P, S);
+}

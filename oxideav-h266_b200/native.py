@@ -32,7 +32,7 @@ EXPORTS = [
     "h266_ctx_kernel_launches", "h266_derive_lmcs", "h266_lmcs_inverse_map_luma", "h266_apply_deblocking_clipped",
     "h266_apply_sao_clipped", "h266_apply_alf_clipped", "h266_apply_in_loop_filters",
     "h266_apply_in_loop_filters_batch", "h266_ctx_set_profiling", "h266_ctx_profile", "h266_chain_plan_create",
-    "h266_chain_plan_execute", "h266_chain_plan_destroy",
+    "h266_chain_plan_execute", "h266_chain_plan_destroy", "h266_apply_in_loop_filters_noalloc",
 ]
 PROF_FAMILIES = ("lmcs", "deblock", "sao_alf", "copy")
 
@@ -69,6 +69,7 @@ def lib():
         L.h266_chain_plan_create.argtypes = [vp, vp, vp, C.POINTER(vp)]
         L.h266_chain_plan_execute.argtypes = [vp, vp, vp]
         L.h266_chain_plan_destroy.argtypes = [vp]
+        L.h266_apply_in_loop_filters_noalloc.argtypes = [vp, vp, vp]
         _LIB = L
     return _LIB
 
