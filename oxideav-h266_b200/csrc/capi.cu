@@ -2,6 +2,7 @@
 // packing and the per-filter / whole-chain entry points declared in
 // include/oxideav_h266_b200.h.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -91,6 +92,7 @@ struct h266_ctx {
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
   double prof_ms[H266_PROF_FAMILIES] = {0};
   uint64_t prof_n[H266_PROF_FAMILIES] = {0};
+  bool force_scalar = false;  // H266_FORCE_SCALAR_ALF=1: scalar SAO/ALF kernel (cross-checks)
 };
 
 // A chain whose side information is resident on the device (h266_chain_plan_create).
@@ -101,9 +103,9 @@ struct h266_chain_plan {
   bool lmcs = false, pass2 = false;
   int deblock_bd = 8;
   uint32_t n_comp[2] = {0, 0};
-  size_t off_seg[2] = {0, 0}, off_comp[2] = {0, 0}, off_ctb = 0, off_tab = 0;
+  size_t off_seg[2] = {0, 0}, off_comp[2] = {0, 0}, off_ctb = 0, off_tab = 0, off_pack = 0;
   h266::Pass2Args args{};
-  bool do_sao = false, do_alf = false;
+  bool do_sao = false, do_alf = false, packed = false;
 };
 
 namespace {
@@ -268,10 +270,50 @@ struct Pass2Inputs {
 
 struct Pass2Host {
   std::vector<CtbDev> ctbs;
-  std::vector<int32_t> luma_tab;  // slots * 600: coeff[300] then clip[300]
+  std::vector<int32_t> luma_tab;      // slots * 600: coeff[300] then clip[300]
+  std::vector<uint32_t> luma_packed;  // packed-arithmetic form, see AlfTablesDev
   Pass2Args args;
   bool do_sao = false, do_alf = false;
+  bool packed = false;  // run the packed 16x2 kernel
 };
+
+// eqs. 1442-1445: coefficient / clip permutation per transposeIdx
+const int kTranspose[4][12] = {{0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11},
+                               {9, 4, 10, 8, 1, 5, 11, 7, 3, 0, 2, 6},
+                               {0, 3, 2, 1, 8, 7, 6, 5, 4, 9, 10, 11},
+                               {9, 8, 10, 4, 3, 7, 11, 5, 1, 0, 2, 6}};
+
+// Builds the packed tables; returns false when an input is outside the packed
+// path's range (then the scalar kernel runs).
+bool build_packed(Pass2Host &h, int bd, uint32_t cfi, const h266_alf_aps_data *caps) {
+  if (bd > 14 || (cfi != 0 && cfi != 1)) return false;
+  auto in8 = [](int v) { return v >= -128 && v <= 127; };
+  const size_t slots = h.luma_tab.size() / 600;
+  h.luma_packed.assign(slots * 100 * 36, 0);
+  for (size_t s = 0; s < slots; ++s)
+    for (int c = 0; c < 25; ++c)
+      for (int t = 0; t < 4; ++t)
+        for (int k = 0; k < 12; ++k) {
+          const int src = kTranspose[t][k];
+          const int coef = h.luma_tab[s * 600 + c * 12 + src], clip = h.luma_tab[s * 600 + 300 + c * 12 + src];
+          if (!in8(coef)) return false;
+          uint32_t *w = &h.luma_packed[((s * 100) + c * 4 + t) * 36 + 3 * k];
+          w[0] = ((uint32_t)clip & 0xFFFF) | ((uint32_t)clip << 16);
+          w[1] = ((uint32_t)(-clip) & 0xFFFF) | ((uint32_t)(-clip) << 16);
+          w[2] = (uint32_t)coef & 0xFF;
+        }
+  if (caps)
+    for (uint32_t f = 0; f < caps->n_chroma_filters; ++f)
+      for (int k = 0; k < 6; ++k) {
+        const int coef = caps->chroma_coeff[f][k], clip = alf_clip_value(bd, caps->chroma_clip_idx[f][k]);
+        if (!in8(coef)) return false;
+        uint32_t *w = &h.args.tables.chroma_packed[f * 18 + 3 * k];
+        w[0] = ((uint32_t)clip & 0xFFFF) | ((uint32_t)clip << 16);
+        w[1] = ((uint32_t)(-clip) & 0xFFFF) | ((uint32_t)(-clip) << 16);
+        w[2] = (uint32_t)coef & 0xFF;
+      }
+  return true;
+}
 
 int check_bounds(const uint32_t *b, uint64_t n, uint32_t extent, uint32_t ctb, const char *what) {
   if (n && !b) return set_error(H266_ERR_INVALID_ARGUMENT, std::string(what) + ": NULL list");
@@ -453,12 +495,14 @@ int build_pass2(const h266_picture &pic, const Pass2Inputs &in, Pass2Host &h) {
   a.has_clip = in.cols != nullptr;
   a.sao_luma = sao_on && in.sao_cfg->luma_used;
   a.sao_chroma = sao_on && in.sao_cfg->chroma_used && cfi != 0;
+  h.packed = build_packed(h, (int)bd, cfi, caps);
+  if (!h.packed) h.luma_packed.clear();
   return H266_OK;
 }
 
 // Side information of one call, assembled into ctx->blob and uploaded once.
 struct Staged {
-  size_t ctb = 0, tab = 0, seg[2] = {0, 0}, comp[2] = {0, 0};
+  size_t ctb = 0, tab = 0, pack = 0, seg[2] = {0, 0}, comp[2] = {0, 0};
   uint8_t *base = nullptr;
 };
 
@@ -475,19 +519,22 @@ void stage_pass2(h266_ctx *ctx, const Pass2Host &h, Staged &st) {
   Blob blob{ctx->blob};
   st.ctb = blob.put(h.ctbs.data(), h.ctbs.size() * sizeof(CtbDev));
   st.tab = blob.put(h.luma_tab.data(), h.luma_tab.size() * sizeof(int32_t));
+  st.pack = blob.put(h.luma_packed.data(), h.luma_packed.size() * sizeof(uint32_t));
 }
 
 // Runs pass 2 (SAO and/or ALF) from `src` into the picture planes `dst`.
-int run_pass2(h266_ctx *ctx, Pass2Args a, bool do_sao, bool do_alf, const uint8_t *base, size_t off_ctb,
-              size_t off_tab, const DPlane src[3], const DPlane dst[3]) {
+int run_pass2(h266_ctx *ctx, Pass2Args a, bool do_sao, bool do_alf, bool packed, const uint8_t *base,
+              const Staged &st, const DPlane src[3], const DPlane dst[3]) {
   for (int i = 0; i < 3; ++i) {
     a.src[i] = src[i];
     a.dst[i] = dst[i];
   }
-  a.ctbs = reinterpret_cast<const CtbDev *>(base + off_ctb);
-  a.tables.luma_coeff = reinterpret_cast<const int32_t *>(base + off_tab);  // per slot: coeff[300], clip[300]
+  a.ctbs = reinterpret_cast<const CtbDev *>(base + st.ctb);
+  a.tables.luma_coeff = reinterpret_cast<const int32_t *>(base + st.tab);  // per slot: coeff[300], clip[300]
   a.tables.luma_clip = a.tables.luma_coeff + 300;
+  a.tables.luma_packed = reinterpret_cast<const uint32_t *>(base + st.pack);
   Prof pf(ctx, H266_PROF_SAO_ALF);
+  if (packed && !ctx->force_scalar) return launch_pass2_packed(ctx->stream, a, do_sao, do_alf, &ctx->launches);
   return launch_pass2(ctx->stream, a, do_sao, do_alf, &ctx->launches);
 }
 
@@ -570,7 +617,7 @@ int exec_chain(h266_ctx *ctx, const uint8_t *base, const Staged &st, const uint3
   }
   for (int i = 0; i < 3; ++i) H266_TRY(plane_map(ctx, S[i], P[i], i == 0 ? lut : nullptr));
   H266_TRY(run_deblock(ctx, base, st.seg, st.comp, n_comp, S, dbd));
-  return run_pass2(ctx, h.args, h.do_sao, h.do_alf, base, st.ctb, st.tab, S, P);
+  return run_pass2(ctx, h.args, h.do_sao, h.do_alf, h.packed, base, st, S, P);
 }
 
 // The chain for one picture whose planes are already device views `P`.
@@ -623,6 +670,8 @@ int h266_ctx_create(int device, h266_ctx **out) {
     return cuda_error(e, "h266_ctx_create");
   }
   c->stream = c->own;
+  const char *fs = std::getenv("H266_FORCE_SCALAR_ALF");
+  c->force_scalar = fs && fs[0] == '1';
   *out = c;
   return H266_OK;
 }
@@ -719,7 +768,7 @@ static int pass2_entry(h266_ctx *ctx, h266_picture *pic, const Pass2Inputs &in) 
     DPlane S[3];
     H266_TRY(ensure_scratch(ctx, P, S));
     for (int i = 0; i < 3; ++i) H266_TRY(plane_map(ctx, S[i], P[i], nullptr));
-    H266_TRY(run_pass2(ctx, h.args, h.do_sao, h.do_alf, st.base, st.ctb, st.tab, S, P));
+    H266_TRY(run_pass2(ctx, h.args, h.do_sao, h.do_alf, h.packed, st.base, st, S, P));
   }
   return picture_from_device(ctx, *pic);
 }
@@ -850,6 +899,8 @@ int h266_chain_plan_create(h266_ctx *ctx, const h266_picture *pic, const h266_in
   }
   pl->off_ctb = pr.st.ctb;
   pl->off_tab = pr.st.tab;
+  pl->off_pack = pr.st.pack;
+  pl->packed = pr.h.packed;
   pl->args = pr.h.args;
   pl->do_sao = pr.h.do_sao;
   pl->do_alf = pr.h.do_alf;
@@ -879,10 +930,12 @@ int h266_chain_plan_execute(h266_ctx *ctx, h266_chain_plan *plan, h266_picture *
   }
   st.ctb = plan->off_ctb;
   st.tab = plan->off_tab;
+  st.pack = plan->off_pack;
   Pass2Host h;
   h.args = plan->args;
   h.do_sao = plan->do_sao;
   h.do_alf = plan->do_alf;
+  h.packed = plan->packed;
   return exec_chain(ctx, st.base, st, plan->n_comp, h, plan->lmcs ? plan->lut.as<uint16_t>() : nullptr,
                     plan->deblock_bd, P, S);
 }

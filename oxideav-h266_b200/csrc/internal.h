@@ -114,6 +114,9 @@ struct AlfTablesDev {
   int32_t chroma_coeff[8][6];
   int32_t chroma_clip[8][6];
   int32_t cc_coeff[2][4][7];  // [cb/cr][filter][tap]
+  // packed-arithmetic form (sao_alf2.cu): per tap three words (c|c<<16, -c|-c<<16, coeff & 0xff)
+  const uint32_t *luma_packed;  // [slot][class * 4 + transposeIdx][12 taps][3], taps pre-permuted
+  uint32_t chroma_packed[8 * 18];  // [alt][6 taps][3]
 };
 
 struct Pass2Args {
@@ -137,5 +140,7 @@ struct Pass2Args {
 };
 
 int launch_pass2(cudaStream_t st, const Pass2Args &a, bool do_sao, bool do_alf, uint64_t *launches);
+// Packed 16x2 form; requires bit_depth <= 14, 4:2:0 or 4:0:0, coefficients in [-128, 127].
+int launch_pass2_packed(cudaStream_t st, const Pass2Args &a, bool do_sao, bool do_alf, uint64_t *launches);
 
 }  // namespace h266

@@ -1,0 +1,490 @@
+// SAO + ALF + CC-ALF tile pass, packed-arithmetic form (the default for
+// BitDepth <= 14, |coefficients| <= 127 and 4:2:0 / 4:0:0 chroma; other inputs
+// use the scalar pass in sao_alf.cu).
+//
+// Same semantics as the scalar pass (reads deblocked planes, writes final
+// planes; post-SAO samples clamped into the CTB's ALF fetch rectangle), with a
+// different organisation aimed at integer issue rate:
+//  * tiles of TW x 32 luma samples (TW = 64 when the CTB allows it);
+//  * SAO parameters of the 3x3 CTB neighbourhood cached in shared memory;
+//  * ALF classification from per-2x2-cell Laplacian sums shared by the four
+//    blocks whose windows contain the cell; only the two block rows next to
+//    the CTB's virtual boundary (their windows and padding differ, src/alf.rs:
+//    864-901) are summed directly;
+//  * the 7x7 and 5x5 diamonds work on pairs of horizontally adjacent samples
+//    packed in one 32-bit register: per tap the clipped differences of both
+//    pixels are formed with two 16x2 add-max / add-min operations, the two
+//    symmetric taps added as 16x2, and the coefficient applied per pixel with
+//    dp2a; coefficients, clip values and their negations are pre-permuted per
+//    (class, transposeIdx) on the host and held in registers per 4x4 block.
+#include <initializer_list>
+
+#include "internal.h"
+
+namespace h266 {
+namespace {
+
+constexpr int TH = 32;
+constexpr int NT = 256;
+
+__device__ __forceinline__ int clampd(int v, int lo, int hi) { return min(max(v, lo), hi); }
+__device__ __forceinline__ int sgn(int v) { return (v > 0) - (v < 0); }
+
+struct SaoLocal {  // one component's SAO parameters of one CTB, plus its clip rectangle
+  int type, cls, band, off[4];
+  int rect[4];
+};
+
+template <int W>
+struct Smem {
+  static constexpr int DLW = W + 12, DLH = TH + 8;  // deblocked luma [X0-6, X1+6) x [Y0-4, Y1+4)
+  static constexpr int SLW = W + 8, SLH = TH + 6;   // post-SAO luma [X0-4, X1+4) x [Y0-3, Y1+3)
+  static constexpr int CW = W / 2 + 2, CH = TH / 2 + 2;  // 2x2 Laplacian cells
+  static constexpr int DCW = W / 2 + 12, DCH = TH / 2 + 6;  // deblocked chroma [x-6, x+6) x [y-3, y+3)
+  static constexpr int SCW = W / 2 + 8, SCH = TH / 2 + 4;   // post-SAO chroma [x-4, x+4) x [y-2, y+2)
+  alignas(16) uint16_t dL[DLH * DLW];
+  alignas(16) uint16_t sL[SLH * SLW];
+  alignas(16) uint4 cell[CH * CW];  // sh, sv, sd0, sd1 over the cell's two checkerboard positions
+  alignas(16) uint16_t dC[DCH * DCW];
+  alignas(16) uint16_t sC[SCH * SCW];
+  uint8_t cls_f[(TH / 4) * (W / 4)], cls_t[(TH / 4) * (W / 4)];
+  SaoLocal sao[3][9];
+  int any_sao[3];
+};
+
+// §8.8.4.2 for one sample; `at(dx, dy)` reads the pre-SAO plane.
+template <class At>
+__device__ __forceinline__ int sao_one(const SaoLocal &p, int x, int y, int pw, int ph, int maxv, int bd, At at) {
+  const int c = at(0, 0);
+  if (p.type == 1) {
+    const int k = (((c >> (bd - 5)) & 31) - p.band) & 31;
+    return clampd(k < 4 ? c + p.off[k] : c, 0, maxv);
+  }
+  const int h0 = p.cls == 0 ? -1 : (p.cls == 1 ? 0 : (p.cls == 2 ? -1 : 1));
+  const int v0 = p.cls == 0 ? 0 : -1;
+  const int x0 = max(0, p.rect[0]), y0 = max(0, p.rect[1]), x1 = min(pw, p.rect[2]), y1 = min(ph, p.rect[3]);
+  if (x + h0 < x0 || x - h0 < x0 || y + v0 < y0 || y - v0 < y0 || x + h0 >= x1 || x - h0 >= x1 || y + v0 >= y1 ||
+      y - v0 >= y1)
+    return clampd(c, 0, maxv);
+  int e = 2 + sgn(c - at(h0, v0)) + sgn(c - at(-h0, -v0));
+  if (e <= 2) e = e == 2 ? 0 : e + 1;
+  return clampd(e ? c + p.off[e - 1] : c, 0, maxv);
+}
+
+// Pair of samples (col, col + 1) of a shared-memory row; DC fixes the parity
+// of col (col = even base + DC).
+template <int DC>
+__device__ __forceinline__ uint32_t pair_at(const uint16_t *row, int even_base) {
+  const int col = even_base + DC;
+  if constexpr ((DC & 1) == 0) {
+    return *reinterpret_cast<const uint32_t *>(row + col);
+  } else {
+    const uint32_t a = *reinterpret_cast<const uint32_t *>(row + col - 1);
+    const uint32_t b = *reinterpret_cast<const uint32_t *>(row + col + 1);
+    return __byte_perm(a, b, 0x5432);
+  }
+}
+
+// clip(n - cur, -c, c) for both 16-bit lanes
+__device__ __forceinline__ uint32_t clipd(uint32_t n, uint32_t ncur, uint32_t c2, uint32_t nc2) {
+  return __viaddmin_s16x2(__viaddmax_s16x2(n, ncur, nc2), 0u, c2);
+}
+__device__ __forceinline__ uint32_t add2(uint32_t a, uint32_t b) { return __viaddmax_s16x2(a, b, 0x80008000u); }
+__device__ __forceinline__ uint32_t neg2(uint32_t a) { return __viaddmax_s16x2(~a, 0x00010001u, 0x80008000u); }
+
+template <int DX>
+__device__ __forceinline__ void luma_tap(const uint16_t *up, const uint16_t *dn, int c0, const uint32_t ncur[2],
+                                         uint32_t c2, uint32_t nc2, uint32_t f, int acc[4]) {
+  // tap at (DX, +dy) on row `up`, mirrored tap at (-DX, -dy) on row `dn`
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const uint32_t a = clipd(pair_at<DX>(up, c0 + 2 * q), ncur[q], c2, nc2);
+    const uint32_t b = clipd(pair_at<-DX>(dn, c0 + 2 * q), ncur[q], c2, nc2);
+    const uint32_t s = add2(a, b);
+    acc[2 * q] = __dp2a_lo((int)s, (int)f, acc[2 * q]);
+    acc[2 * q + 1] = __dp2a_lo((int)s, (int)(f << 8), acc[2 * q + 1]);
+  }
+}
+
+template <int DX>
+__device__ __forceinline__ void chroma_tap(const uint16_t *up, const uint16_t *dn, int c0, uint32_t ncur, uint32_t c2,
+                                           uint32_t nc2, uint32_t f, int acc[2]) {
+  const uint32_t a = clipd(pair_at<DX>(up, c0), ncur, c2, nc2);
+  const uint32_t b = clipd(pair_at<-DX>(dn, c0), ncur, c2, nc2);
+  const uint32_t s = add2(a, b);
+  acc[0] = __dp2a_lo((int)s, (int)f, acc[0]);
+  acc[1] = __dp2a_lo((int)s, (int)(f << 8), acc[1]);
+}
+
+constexpr uint64_t pack4(std::initializer_list<int> v) {
+  uint64_t r = 0;
+  int i = 0;
+  for (int x : v) r |= (uint64_t)x << (4 * i++);
+  return r;
+}
+constexpr uint32_t pack2(std::initializer_list<int> v) {
+  uint32_t r = 0;
+  int i = 0;
+  for (int x : v) r |= (uint32_t)x << (2 * i++);
+  return r;
+}
+
+// Class of one block from its four direction sums (eqs. 1463-1482, src/alf.rs:954-1007).
+__device__ __forceinline__ void classify(int sh, int sv, int sd0, int sd1, int ac, int bd, uint8_t &f_out,
+                                         uint8_t &t_out) {
+  int hv1, hv0, dhv, d1, d0, dd;
+  if (sv > sh) { hv1 = sv; hv0 = sh; dhv = 1; } else { hv1 = sh; hv0 = sv; dhv = 3; }
+  if (sd0 > sd1) { d1 = sd0; d0 = sd1; dd = 0; } else { d1 = sd1; d0 = sd0; dd = 2; }
+  const bool pd = (long long)d1 * hv0 > (long long)hv1 * d0;
+  const int hvd1 = pd ? d1 : hv1, hvd0 = pd ? d0 : hv0;
+  const int dir1 = pd ? dd : dhv, dir2 = pd ? dhv : dd;
+  const int dir_s = hvd1 * 2 > 9 * hvd0 ? 2 : (hvd1 > 2 * hvd0 ? 1 : 0);
+  const long long act = ((long long)(sh + sv) * ac) >> (bd - 1);
+  const int avg = (int)(act > 15 ? 15 : act);
+  // varTab (eq. 1480) packed 4 bits per entry, transposeTable 2 bits per entry
+  constexpr uint64_t kVarTab = pack4({0, 1, 2, 2, 2, 2, 2, 3, 3, 3, 3, 3, 3, 3, 3, 4});
+  constexpr uint32_t kTransposeTable = pack2({0, 1, 0, 2, 2, 3, 1, 3});
+  int f = (int)((kVarTab >> (avg * 4)) & 0xF);
+  if (dir_s != 0) f += (((dir1 & 1) << 1) + dir_s) * 5;
+  f_out = (uint8_t)f;
+  t_out = (uint8_t)((kTransposeTable >> ((dir1 * 2 + (dir2 >> 1)) * 2)) & 3);
+}
+
+template <int W, bool DO_SAO, bool DO_ALF>
+__global__ void __launch_bounds__(NT) k_sao_alf_packed(const __grid_constant__ Pass2Args a) {
+  using S = Smem<W>;
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  S &sm = *reinterpret_cast<S *>(smem_raw);
+  const int tid = threadIdx.x;
+  const int tx = blockIdx.x % a.tiles_x, ty = blockIdx.x / a.tiles_x;
+  const int X0 = tx * W, Y0 = ty * TH;
+  const int bd = a.bit_depth, maxv = (1 << bd) - 1;
+  const int log2 = a.ctb_log2, ctb = 1 << log2;
+  const int rx = X0 >> log2, ry = Y0 >> log2;
+  const int y_ctb = ry << log2;
+  const int pw = a.pic_w, ph = a.pic_h;
+  const bool in_grid = rx < a.w_ctbs && ry < a.h_ctbs;
+  const CtbDev *me = in_grid ? &a.ctbs[ry * a.w_ctbs + rx] : nullptr;
+  int rect[4] = {0, 0, pw, ph};
+  if (me) {
+    rect[0] = me->rect[0];
+    rect[1] = me->rect[1];
+    rect[2] = me->rect[2];
+    rect[3] = me->rect[3];
+  }
+  const int rx0 = max(rect[0], 0), ry0 = max(rect[1], 0), rx1 = min(rect[2], pw), ry1 = min(rect[3], ph);
+
+  // ---- SAO parameters of the 3x3 CTB neighbourhood
+  if (tid < 27) {
+    const int comp = tid / 9, n = tid % 9;
+    const int nx = rx + n % 3 - 1, ny = ry + n / 3 - 1;
+    SaoLocal &s = sm.sao[comp][n];
+    s.type = 0;
+    const bool used = comp == 0 ? a.sao_luma : a.sao_chroma;
+    if (DO_SAO && used && nx >= 0 && ny >= 0 && nx < a.w_ctbs && ny < a.h_ctbs) {
+      const CtbDev &c = a.ctbs[ny * a.w_ctbs + nx];
+      const SaoCtbDev &p = c.sao[comp];
+      s.type = p.type;
+      s.cls = p.eo_class;
+      s.band = p.band_pos;
+      for (int k = 0; k < 4; ++k) s.off[k] = p.off[k];
+      const int sw = comp ? 2 : 1;
+      if (a.has_clip) {
+        s.rect[0] = c.rect[0] / sw;
+        s.rect[1] = c.rect[1] / sw;
+        s.rect[2] = (c.rect[2] + sw - 1) / sw;
+        s.rect[3] = (c.rect[3] + sw - 1) / sw;
+      } else {
+        s.rect[0] = s.rect[1] = 0;
+        s.rect[2] = s.rect[3] = 1 << 30;
+      }
+    }
+  }
+  __syncthreads();
+  if (tid < 3) {
+    int any = 0;
+    for (int n = 0; n < 9; ++n) any |= sm.sao[tid][n].type;
+    sm.any_sao[tid] = any;
+  }
+
+  // ---- luma: deblocked samples with halo
+  const DPlane LS = a.src[0], LD = a.dst[0];
+  for (int i = tid; i < S::DLH * S::DLW; i += NT) {
+    const int r = i / S::DLW, c = i - r * S::DLW;
+    const int gx = clampd(X0 - 6 + c, 0, LS.w - 1), gy = clampd(Y0 - 4 + r, 0, LS.h - 1);
+    sm.dL[i] = LS.s[(int64_t)gy * LS.stride + gx];
+  }
+  __syncthreads();
+  // ---- post-SAO luma, clamped into the fetch rectangle
+  {
+    const bool any = sm.any_sao[0] != 0;
+    for (int i = tid; i < S::SLH * S::SLW; i += NT) {
+      const int r = i / S::SLW, c = i - r * S::SLW;
+      const int ax = clampd(X0 - 4 + c, rx0, rx1 - 1), ay = clampd(Y0 - 3 + r, ry0, ry1 - 1);
+      const int lr = ay - (Y0 - 4), lc = ax - (X0 - 6);
+      const uint16_t *d = &sm.dL[lr * S::DLW + lc];
+      int v = *d;
+      if (any) {
+        const SaoLocal &p = sm.sao[0][((ay >> log2) - ry + 1) * 3 + ((ax >> log2) - rx + 1)];
+        if (p.type)
+          v = sao_one(p, ax, ay, LS.w, LS.h, maxv, bd, [&](int dx, int dy) { return (int)d[dy * S::DLW + dx]; });
+      }
+      sm.sL[i] = (uint16_t)v;
+    }
+  }
+  __syncthreads();
+
+  const bool luma_alf = DO_ALF && me && me->luma_set >= 0;
+  if (luma_alf) {
+    // ---- Laplacian sums per 2x2 cell (unpadded rows)
+    for (int i = tid; i < S::CH * S::CW; i += NT) {
+      const int cy = i / S::CW, cx = i - cy * S::CW;
+      uint4 g = make_uint4(0, 0, 0, 0);
+#pragma unroll
+      for (int d = 0; d < 2; ++d) {
+        const int r = 2 * cy + d + 1;      // sL row of the position: y = Y0 - 2 + 2cy + d
+        const int c = 2 * cx + d + 2;      // sL col: x = X0 - 2 + 2cx + d
+        const uint16_t *row = &sm.sL[r * S::SLW + c];
+        const int c2 = 2 * row[0];
+        g.x += abs(c2 - row[-1] - row[1]);
+        g.y += abs(c2 - row[-S::SLW] - row[S::SLW]);
+        g.z += abs(c2 - row[-S::SLW - 1] - row[S::SLW + 1]);
+        g.w += abs(c2 - row[-S::SLW + 1] - row[S::SLW - 1]);
+      }
+      sm.cell[i] = g;
+    }
+    __syncthreads();
+    // ---- classes
+    const bool bottom = y_ctb + ctb >= ph;
+    const bool carve = !bottom || (ph - y_ctb) > ctb - 4;
+    const int vb = y_ctb + ctb - 4;
+    constexpr int NB = (TH / 4) * (W / 4);
+    for (int b = tid; b < NB; b += NT) {
+      const int bx = b % (W / 4), by = b / (W / 4);
+      const int y4 = Y0 + 4 * by - y_ctb;
+      if (y4 == ctb - 8 || y4 == ctb - 4) {  // virtual-boundary rows: windows and padding differ
+        int min_y = -2, max_y = 5, ac = 2;
+        if (y4 == ctb - 8 && carve) { max_y = 3; ac = 3; }
+        else if (y4 == ctb - 4 && carve) { min_y = 0; ac = 3; }
+        const bool top_pad = y4 == ctb - 4, bot_pad = y4 == ctb - 8;
+        auto pad = [&](int gy) {
+          if (top_pad) gy = max(gy, vb);
+          if (bot_pad) gy = min(gy, vb - 1);
+          return gy - (Y0 - 3);
+        };
+        int sh = 0, sv = 0, sd0 = 0, sd1 = 0;
+        for (int j = min_y; j <= max_y; ++j) {
+          const int gy = y_ctb + y4 + j;
+          const uint16_t *rc = &sm.sL[pad(gy) * S::SLW], *ru = &sm.sL[pad(gy - 1) * S::SLW],
+                         *rd = &sm.sL[pad(gy + 1) * S::SLW];
+          for (int i = (j & 1) ? -1 : -2; i <= 5; i += 2) {
+            const int c = 4 * bx + i + 4;
+            const int c2 = 2 * rc[c];
+            sh += abs(c2 - rc[c - 1] - rc[c + 1]);
+            sv += abs(c2 - ru[c] - rd[c]);
+            sd0 += abs(c2 - ru[c - 1] - rd[c + 1]);
+            sd1 += abs(c2 - ru[c + 1] - rd[c - 1]);
+          }
+        }
+        classify(sh, sv, sd0, sd1, ac, bd, sm.cls_f[b], sm.cls_t[b]);
+      } else {
+        uint4 s = make_uint4(0, 0, 0, 0);
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            const uint4 g = sm.cell[(2 * by + r) * S::CW + 2 * bx + c];
+            s.x += g.x;
+            s.y += g.y;
+            s.z += g.z;
+            s.w += g.w;
+          }
+        classify((int)s.x, (int)s.y, (int)s.z, (int)s.w, 2, bd, sm.cls_f[b], sm.cls_t[b]);
+      }
+    }
+    __syncthreads();
+    // ---- 7x7 diamond, 4-pixel runs; every thread keeps one block's taps
+    constexpr int RUNS = TH * W / 4;
+    constexpr int RPT = RUNS / NT;  // runs per thread: 1 (W = 32) or 2 (W = 64)
+    constexpr int TPB = 4 / RPT;    // threads per 4x4 block
+    const int b = tid / TPB;
+    const int bx = b % (W / 4), by = b / (W / 4);
+    const uint32_t *tab = a.tables.luma_packed + ((size_t)me->luma_set * 100 + sm.cls_f[b] * 4 + sm.cls_t[b]) * 36;
+    uint32_t c2[12], nc2[12], f[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      c2[k] = __ldg(tab + 3 * k);
+      nc2[k] = __ldg(tab + 3 * k + 1);
+      f[k] = __ldg(tab + 3 * k + 2);
+    }
+#pragma unroll
+    for (int rr = 0; rr < RPT; ++rr) {
+      const int jr = (tid % TPB) * RPT + rr;  // row inside the block
+      const int j = 4 * by + jr;               // tile row
+      const int gy = Y0 + j;
+      const int yr = gy - y_ctb;
+      int shift = 7, y1 = 1, y2 = 2, y3 = 3;  // Table 45 (line-buffer arms always applied)
+      if (yr == ctb - 5 || yr == ctb - 4) { shift = 10; y1 = y2 = y3 = 0; }
+      else if (yr == ctb - 6 || yr == ctb - 3) { y2 = y3 = 1; }
+      else if (yr == ctb - 7 || yr == ctb - 2) { y3 = 2; }
+      const int r = j + 3;
+      const int c0 = 4 * bx + 4;
+      const uint16_t *R0 = &sm.sL[r * S::SLW];
+      const uint16_t *U1 = R0 - y1 * S::SLW, *D1 = R0 + y1 * S::SLW;
+      const uint16_t *U2 = R0 - y2 * S::SLW, *D2 = R0 + y2 * S::SLW;
+      const uint16_t *U3 = R0 - y3 * S::SLW, *D3 = R0 + y3 * S::SLW;
+      const uint32_t cur[2] = {pair_at<0>(R0, c0), pair_at<0>(R0, c0 + 2)};
+      const uint32_t ncur[2] = {neg2(cur[0]), neg2(cur[1])};
+      int acc[4] = {0, 0, 0, 0};
+      luma_tap<0>(D3, U3, c0, ncur, c2[0], nc2[0], f[0], acc);
+      luma_tap<1>(D2, U2, c0, ncur, c2[1], nc2[1], f[1], acc);
+      luma_tap<0>(D2, U2, c0, ncur, c2[2], nc2[2], f[2], acc);
+      luma_tap<-1>(D2, U2, c0, ncur, c2[3], nc2[3], f[3], acc);
+      luma_tap<2>(D1, U1, c0, ncur, c2[4], nc2[4], f[4], acc);
+      luma_tap<1>(D1, U1, c0, ncur, c2[5], nc2[5], f[5], acc);
+      luma_tap<0>(D1, U1, c0, ncur, c2[6], nc2[6], f[6], acc);
+      luma_tap<-1>(D1, U1, c0, ncur, c2[7], nc2[7], f[7], acc);
+      luma_tap<-2>(D1, U1, c0, ncur, c2[8], nc2[8], f[8], acc);
+      luma_tap<3>(R0, R0, c0, ncur, c2[9], nc2[9], f[9], acc);
+      luma_tap<2>(R0, R0, c0, ncur, c2[10], nc2[10], f[10], acc);
+      luma_tap<1>(R0, R0, c0, ncur, c2[11], nc2[11], f[11], acc);
+      if (gy < LD.h) {
+        const int round = 1 << (shift - 1);
+        uint16_t *out = LD.s + (int64_t)gy * LD.stride + X0 + 4 * bx;
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+          const int cv = (int)((cur[p >> 1] >> ((p & 1) * 16)) & 0xFFFF);
+          if (X0 + 4 * bx + p < LD.w) out[p] = (uint16_t)clampd(cv + ((acc[p] + round) >> shift), 0, maxv);
+        }
+      }
+    }
+  } else {
+    for (int p = tid; p < TH * W; p += NT) {
+      const int i = p % W, j = p / W;
+      const int gx = X0 + i, gy = Y0 + j;
+      if (gx < LD.w && gy < LD.h) LD.s[(int64_t)gy * LD.stride + gx] = sm.sL[(j + 3) * S::SLW + i + 4];
+    }
+  }
+
+  // ---- chroma (4:2:0)
+  if (!a.chroma) return;
+  constexpr int TWC = W / 2, THC = TH / 2;
+  const int xc0 = X0 / 2, yc0 = Y0 / 2;
+  const int ctb_c = ctb / 2, y_ctb_c = y_ctb / 2;
+  const int crx0 = rect[0] / 2, cry0 = rect[1] / 2, crx1 = (rect[2] + 1) / 2, cry1 = (rect[3] + 1) / 2;
+  for (int comp = 1; comp <= 2; ++comp) {
+    const DPlane CS = a.src[comp], CD = a.dst[comp];
+    if (CS.w <= 0 || CS.h <= 0 || xc0 >= CS.w || yc0 >= CS.h) continue;
+    const int cx0 = max(crx0, 0), cy0 = max(cry0, 0), cx1 = min(crx1, CS.w), cy1 = min(cry1, CS.h);
+    __syncthreads();
+    for (int i = tid; i < S::DCH * S::DCW; i += NT) {
+      const int r = i / S::DCW, c = i - r * S::DCW;
+      const int gx = clampd(xc0 - 6 + c, 0, CS.w - 1), gy = clampd(yc0 - 3 + r, 0, CS.h - 1);
+      sm.dC[i] = CS.s[(int64_t)gy * CS.stride + gx];
+    }
+    __syncthreads();
+    const bool any = sm.any_sao[comp] != 0;
+    for (int i = tid; i < S::SCH * S::SCW; i += NT) {
+      const int r = i / S::SCW, c = i - r * S::SCW;
+      const int ax = clampd(xc0 - 4 + c, cx0, cx1 - 1), ay = clampd(yc0 - 2 + r, cy0, cy1 - 1);
+      const uint16_t *d = &sm.dC[(ay - (yc0 - 3)) * S::DCW + ax - (xc0 - 6)];
+      int v = *d;
+      if (any) {
+        const SaoLocal &p = sm.sao[comp][(((ay * 2) >> log2) - ry + 1) * 3 + (((ax * 2) >> log2) - rx + 1)];
+        if (p.type)
+          v = sao_one(p, ax, ay, CS.w, CS.h, maxv, bd, [&](int dx, int dy) { return (int)d[dy * S::DCW + dx]; });
+      }
+      sm.sC[i] = (uint16_t)v;
+    }
+    __syncthreads();
+    const int cf = (DO_ALF && me) ? me->chroma_filt[comp - 1] : -1;
+    const int ccf = (DO_ALF && me) ? me->cc_filt[comp - 1] : -1;
+    // one pair of chroma samples per thread
+    const int i2 = (tid % (TWC / 2)) * 2, j = tid / (TWC / 2);
+    for (int jj = j; jj < THC; jj += NT / (TWC / 2)) {
+      const int gy = yc0 + jj, gx = xc0 + i2;
+      const int r = jj + 2, c0 = i2 + 4;
+      const uint16_t *R0 = &sm.sC[r * S::SCW];
+      const uint32_t cur = pair_at<0>(R0, c0);
+      int v[2] = {(int)(cur & 0xFFFF), (int)(cur >> 16)};
+      if (cf >= 0) {
+        const int jr = gy - y_ctb_c;
+        int s2 = 7, y1 = 1, y2 = 2;  // Table 46 (line-buffer arms always applied)
+        if (jr == ctb_c - 2 || jr == ctb_c - 3) { s2 = 10; y1 = y2 = 0; }
+        else if (jr == ctb_c - 1 || jr == ctb_c - 4) { y2 = 1; }
+        const uint32_t *ct = a.tables.chroma_packed + max(cf, 0) * 18;
+        const uint32_t ncur = neg2(cur);
+        int acc[2] = {0, 0};
+        const uint16_t *U1 = R0 - y1 * S::SCW, *D1 = R0 + y1 * S::SCW, *U2 = R0 - y2 * S::SCW, *D2 = R0 + y2 * S::SCW;
+        chroma_tap<0>(D2, U2, c0, ncur, ct[0], ct[1], ct[2], acc);
+        chroma_tap<1>(D1, U1, c0, ncur, ct[3], ct[4], ct[5], acc);
+        chroma_tap<0>(D1, U1, c0, ncur, ct[6], ct[7], ct[8], acc);
+        chroma_tap<-1>(D1, U1, c0, ncur, ct[9], ct[10], ct[11], acc);
+        chroma_tap<2>(R0, R0, c0, ncur, ct[12], ct[13], ct[14], acc);
+        chroma_tap<1>(R0, R0, c0, ncur, ct[15], ct[16], ct[17], acc);
+        const int round = 1 << (s2 - 1);
+        v[0] = clampd(v[0] + ((acc[0] + round) >> s2), 0, maxv);
+        v[1] = clampd(v[1] + ((acc[1] + round) >> s2), 0, maxv);
+      }
+      if (ccf >= 0) {  // CC-ALF from post-SAO luma (Table 47, src/alf.rs:447-523)
+        const int *cc = a.tables.cc_coeff[comp - 1][max(ccf, 0)];
+        const int half = 1 << (bd - 1);
+        const int yline = (gy - y_ctb_c) * 2;
+        const bool lbb = !(gy * 2 + ctb >= ph && (ph - y_ctb) <= ctb - 4);
+        int yp1 = 1, yp2 = 2;
+        if (lbb) {
+          if (yline == ctb - 5 || yline == ctb - 4) { yp1 = 0; yp2 = 0; }
+          else if (yline == ctb - 6 || yline == ctb - 3) { yp2 = 1; }
+        }
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+          const uint16_t *L = &sm.sL[(2 * jj + 3) * S::SLW + 2 * (i2 + p) + 4];
+          const int ctr = L[0];
+          int sum = cc[0] * ((int)L[-yp1 * S::SLW] - ctr);
+          sum += cc[1] * ((int)L[-1] - ctr);
+          sum += cc[2] * ((int)L[1] - ctr);
+          sum += cc[3] * ((int)L[yp1 * S::SLW - 1] - ctr);
+          sum += cc[4] * ((int)L[yp1 * S::SLW] - ctr);
+          sum += cc[5] * ((int)L[yp1 * S::SLW + 1] - ctr);
+          sum += cc[6] * ((int)L[yp2 * S::SLW] - ctr);
+          v[p] = clampd(v[p] + clampd((sum + 64) >> 7, -half, half - 1), 0, maxv);
+        }
+      }
+      if (gy < CD.h) {
+        uint16_t *out = CD.s + (int64_t)gy * CD.stride + gx;
+        if (gx < CD.w) out[0] = (uint16_t)v[0];
+        if (gx + 1 < CD.w) out[1] = (uint16_t)v[1];
+      }
+    }
+  }
+}
+
+template <int W>
+int launch_w(cudaStream_t st, const Pass2Args &in, bool do_sao, bool do_alf) {
+  static_assert(sizeof(Smem<W>) <= 48 * 1024, "fits the default dynamic shared-memory limit");
+  Pass2Args a = in;
+  a.tiles_x = (a.ext_w + W - 1) / W;
+  a.tiles_y = (a.ext_h + TH - 1) / TH;
+  const unsigned n = (unsigned)(a.tiles_x * a.tiles_y);
+  const size_t shm = sizeof(Smem<W>);
+  auto go = [&](auto kern) -> int {
+    kern<<<n, NT, shm, st>>>(a);
+    H266_CUDA(cudaGetLastError());
+    return H266_OK;
+  };
+  if (do_sao && do_alf) return go(k_sao_alf_packed<W, true, true>);
+  if (do_sao) return go(k_sao_alf_packed<W, true, false>);
+  if (do_alf) return go(k_sao_alf_packed<W, false, true>);
+  return go(k_sao_alf_packed<W, false, false>);
+}
+
+}  // namespace
+
+int launch_pass2_packed(cudaStream_t st, const Pass2Args &a, bool do_sao, bool do_alf, uint64_t *launches) {
+  if (a.ext_w <= 0 || a.ext_h <= 0) return H266_OK;
+  const int rc = a.ctb_log2 >= 6 ? launch_w<64>(st, a, do_sao, do_alf) : launch_w<32>(st, a, do_sao, do_alf);
+  if (rc == H266_OK) ++*launches;
+  return rc;
+}
+
+}  // namespace h266

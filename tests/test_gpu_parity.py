@@ -180,3 +180,32 @@ def test_profiling_counts_every_family(ctx):
     # one bracket per family call: deblock (both passes), SAO/ALF, LMCS LUT + LUT-mapped copy
     assert prof["deblock"][1] == 1 and prof["sao_alf"][1] == 1 and prof["lmcs"][1] == 2
     assert all(ms >= 0 for ms, _ in prof.values())
+
+
+@pytest.mark.parametrize("kind", ["c1", "c2_small", "stress", "stress_tiles", "odd_tail"])
+def test_scalar_sao_alf_kernel_parity(kind, monkeypatch):
+    """The scalar SAO/ALF kernel (used when the packed kernel's range
+    conditions fail) stays bit-exact too."""
+    monkeypatch.setenv("H266_FORCE_SCALAR_ALF", "1")
+    c = native.Context(0)
+    try:
+        pic, fa = WORKLOADS[kind](3)
+        got, want = pic.copy(), pic.copy()
+        c.apply_in_loop_filters(got, fa)
+        oracle.apply_in_loop_filters(want, fa)
+        assert_same(got, want, f"scalar chain {kind}")
+    finally:
+        c.close()
+
+
+def test_wide_coefficients_take_the_scalar_path(ctx):
+    """Coefficients outside int8 are legal input for the reference; they must
+    still filter bit-exactly (through the scalar kernel)."""
+    pic, fa = small_c2(31)
+    a = np.ctypeslib.as_array(fa.apses[0].luma_coeff)
+    a[0, 0] = 300
+    a[3, 5] = -250
+    got, want = pic.copy(), pic.copy()
+    ctx.apply_in_loop_filters(got, fa)
+    oracle.apply_in_loop_filters(want, fa)
+    assert_same(got, want, "wide coefficients")
