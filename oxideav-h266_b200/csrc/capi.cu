@@ -5,6 +5,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 
@@ -74,18 +75,62 @@ struct Staging {
 
 using namespace h266;
 
-struct h266_ctx {
-  int device = 0;
-  cudaStream_t own = nullptr, stream = nullptr;
+namespace h266 {
+// One stream's worth of chain resources.  The context's main lane runs the
+// single-picture calls on the context stream; batch calls spread pictures over
+// extra lanes with their own streams so that the uploads, kernels and
+// downloads of successive pictures overlap.
+struct Lane {
+  cudaStream_t stream = nullptr;
+  bool owns_stream = false;
   cudaEvent_t staged = nullptr;  // last side-information upload done reading the staging buffer
-  uint64_t launches = 0;
+  cudaEvent_t mark = nullptr;    // joins this lane with other streams
   DevBuf io[3];       // device copies of host pictures
   DevBuf scratch[3];  // deblocked planes read by the SAO / ALF pass
   DevBuf lut;         // LMCS inverse LUT
   DevBuf side;        // side information
   Staging stage;
-  DeblockPlan plan;
-  std::vector<uint8_t> blob;  // side information assembled on the host
+  int init(cudaStream_t s) {
+    if (!s) {
+      H266_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+      owns_stream = true;
+    } else {
+      stream = s;
+    }
+    H266_CUDA(cudaEventCreateWithFlags(&staged, cudaEventDisableTiming));
+    H266_CUDA(cudaEventCreateWithFlags(&mark, cudaEventDisableTiming));
+    H266_CUDA(cudaEventRecord(staged, stream));
+    return H266_OK;
+  }
+  void release() {
+    for (int i = 0; i < 3; ++i) {
+      io[i].release();
+      scratch[i].release();
+    }
+    lut.release();
+    side.release();
+    if (stage.ptr) cudaFreeHost(stage.ptr);
+    stage.ptr = nullptr;
+    stage.cap = 0;
+    if (staged) cudaEventDestroy(staged);
+    if (mark) cudaEventDestroy(mark);
+    staged = mark = nullptr;
+    if (owns_stream && stream) cudaStreamDestroy(stream);
+    stream = nullptr;
+  }
+};
+
+struct Prep;  // host-side preparation of one picture's chain call
+}  // namespace h266
+
+struct h266_ctx {
+  int device = 0;
+  cudaStream_t own = nullptr, stream = nullptr;
+  uint64_t launches = 0;
+  h266::Lane main;                                   // single-picture calls (stream = ctx->stream)
+  std::vector<std::unique_ptr<h266::Lane>> lanes;    // batch calls
+  std::unique_ptr<h266::TaskPool> pool;              // host side-information builders
+  std::vector<std::unique_ptr<h266::Prep>> preps;    // [0]: single-picture calls, [i]: batch picture i
   // profiling: CUDA events around every launch, resolved in h266_ctx_profile
   bool prof = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -126,6 +171,7 @@ struct Guard {  // makes the context's device current for the call
 // Brackets a launch with profiling events when profiling is on.
 struct Prof {
   h266_ctx *ctx;
+  cudaStream_t st;
   int fam;
   cudaEvent_t a = nullptr;
   static cudaEvent_t take(h266_ctx *c) {
@@ -138,16 +184,16 @@ struct Prof {
     cudaEventCreate(&e);
     return e;
   }
-  Prof(h266_ctx *c, int family) : ctx(c), fam(family) {
+  Prof(h266_ctx *c, cudaStream_t stream, int family) : ctx(c), st(stream), fam(family) {
     if (ctx->prof) {
       a = take(ctx);
-      cudaEventRecord(a, ctx->stream);
+      cudaEventRecord(a, st);
     }
   }
   ~Prof() {
     if (a) {
       cudaEvent_t b = take(ctx);
-      cudaEventRecord(b, ctx->stream);
+      cudaEventRecord(b, st);
       ctx->ev_pending.push_back({fam, {a, b}});
     }
   }
@@ -179,7 +225,7 @@ DPlane dplane(const h266_plane &p, uint16_t *ptr, int64_t stride) {
 
 // Device views of the picture: the caller's planes (device memory) or the
 // context's copies of them (host memory, uploaded here).
-int picture_to_device(h266_ctx *ctx, const h266_picture &pic, DPlane out[3]) {
+int picture_to_device(Lane &ln, const h266_picture &pic, DPlane out[3]) {
   const h266_plane *pl[3] = {&pic.luma, &pic.cb, &pic.cr};
   for (int i = 0; i < 3; ++i) {
     const h266_plane &p = *pl[i];
@@ -189,25 +235,27 @@ int picture_to_device(h266_ctx *ctx, const h266_picture &pic, DPlane out[3]) {
       continue;
     }
     const size_t row = (size_t)p.width * 2;
-    H266_TRY(ctx->io[i].ensure(row * p.height));
-    H266_CUDA(cudaMemcpy2DAsync(ctx->io[i].ptr, row, p.samples, (size_t)p.stride * 2, row, p.height,
-                                cudaMemcpyHostToDevice, ctx->stream));
-    out[i] = dplane(p, ctx->io[i].as<uint16_t>(), p.width);
+    H266_TRY(ln.io[i].ensure(row * p.height));
+    H266_CUDA(cudaMemcpy2DAsync(ln.io[i].ptr, row, p.samples, (size_t)p.stride * 2, row, p.height,
+                                cudaMemcpyHostToDevice, ln.stream));
+    out[i] = dplane(p, ln.io[i].as<uint16_t>(), p.width);
   }
   return H266_OK;
 }
 
-int picture_from_device(h266_ctx *ctx, const h266_picture &pic) {
+// Queues the copies of a host picture back from the lane; with `sync` waits
+// for them.
+int picture_from_device(Lane &ln, const h266_picture &pic, bool sync = true) {
   if (pic.mem == H266_MEM_DEVICE) return H266_OK;
   const h266_plane *pl[3] = {&pic.luma, &pic.cb, &pic.cr};
   for (int i = 0; i < 3; ++i) {
     const h266_plane &p = *pl[i];
     if ((uint64_t)p.width * p.height == 0) continue;
     const size_t row = (size_t)p.width * 2;
-    H266_CUDA(cudaMemcpy2DAsync(p.samples, (size_t)p.stride * 2, ctx->io[i].ptr, row, row, p.height,
-                                cudaMemcpyDeviceToHost, ctx->stream));
+    H266_CUDA(cudaMemcpy2DAsync(p.samples, (size_t)p.stride * 2, ln.io[i].ptr, row, row, p.height,
+                                cudaMemcpyDeviceToHost, ln.stream));
   }
-  H266_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (sync) H266_CUDA(cudaStreamSynchronize(ln.stream));
   return H266_OK;
 }
 
@@ -222,15 +270,15 @@ struct Blob {
   }
 };
 
-int upload_blob(h266_ctx *ctx, uint8_t **dev_base) {
-  const size_t n = ctx->blob.size();
-  H266_TRY(ctx->side.ensure(n));
-  H266_CUDA(cudaEventSynchronize(ctx->staged));  // previous upload finished reading the staging buffer
-  H266_TRY(ctx->stage.ensure(n));
-  std::memcpy(ctx->stage.ptr, ctx->blob.data(), n);
-  H266_CUDA(cudaMemcpyAsync(ctx->side.ptr, ctx->stage.ptr, n, cudaMemcpyHostToDevice, ctx->stream));
-  H266_CUDA(cudaEventRecord(ctx->staged, ctx->stream));
-  *dev_base = ctx->side.as<uint8_t>();
+int upload_blob(Lane &ln, const std::vector<uint8_t> &blob, uint8_t **dev_base) {
+  const size_t n = blob.size();
+  H266_TRY(ln.side.ensure(n));
+  H266_CUDA(cudaEventSynchronize(ln.staged));  // previous upload finished reading the staging buffer
+  H266_TRY(ln.stage.ensure(n));
+  std::memcpy(ln.stage.ptr, blob.data(), n);
+  H266_CUDA(cudaMemcpyAsync(ln.side.ptr, ln.stage.ptr, n, cudaMemcpyHostToDevice, ln.stream));
+  H266_CUDA(cudaEventRecord(ln.staged, ln.stream));
+  *dev_base = ln.side.as<uint8_t>();
   return H266_OK;
 }
 
@@ -500,31 +548,30 @@ int build_pass2(const h266_picture &pic, const Pass2Inputs &in, Pass2Host &h) {
   return H266_OK;
 }
 
-// Side information of one call, assembled into ctx->blob and uploaded once.
+// Side information of one call, assembled into one host blob and uploaded once.
 struct Staged {
   size_t ctb = 0, tab = 0, pack = 0, seg[2] = {0, 0}, comp[2] = {0, 0};
   uint8_t *base = nullptr;
 };
 
-void stage_deblock(h266_ctx *ctx, Staged &st) {
-  Blob blob{ctx->blob};
-  DeblockPlan &pl = ctx->plan;
+void stage_deblock(const DeblockPlan &pl, std::vector<uint8_t> &b, Staged &st) {
+  Blob blob{b};
   for (int d = 0; d < 2; ++d) {
     st.seg[d] = blob.put(pl.segs[d].data(), pl.segs[d].size() * sizeof(EdgeSeg));
     st.comp[d] = blob.put(pl.comp[d].data(), pl.comp[d].size() * sizeof(uint32_t));
   }
 }
 
-void stage_pass2(h266_ctx *ctx, const Pass2Host &h, Staged &st) {
-  Blob blob{ctx->blob};
+void stage_pass2(const Pass2Host &h, std::vector<uint8_t> &b, Staged &st) {
+  Blob blob{b};
   st.ctb = blob.put(h.ctbs.data(), h.ctbs.size() * sizeof(CtbDev));
   st.tab = blob.put(h.luma_tab.data(), h.luma_tab.size() * sizeof(int32_t));
   st.pack = blob.put(h.luma_packed.data(), h.luma_packed.size() * sizeof(uint32_t));
 }
 
 // Runs pass 2 (SAO and/or ALF) from `src` into the picture planes `dst`.
-int run_pass2(h266_ctx *ctx, Pass2Args a, bool do_sao, bool do_alf, bool packed, const uint8_t *base,
-              const Staged &st, const DPlane src[3], const DPlane dst[3]) {
+int run_pass2(h266_ctx *ctx, cudaStream_t stream, Pass2Args a, bool do_sao, bool do_alf, bool packed,
+              const uint8_t *base, const Staged &st, const DPlane src[3], const DPlane dst[3]) {
   for (int i = 0; i < 3; ++i) {
     a.src[i] = src[i];
     a.dst[i] = dst[i];
@@ -533,37 +580,38 @@ int run_pass2(h266_ctx *ctx, Pass2Args a, bool do_sao, bool do_alf, bool packed,
   a.tables.luma_coeff = reinterpret_cast<const int32_t *>(base + st.tab);  // per slot: coeff[300], clip[300]
   a.tables.luma_clip = a.tables.luma_coeff + 300;
   a.tables.luma_packed = reinterpret_cast<const uint32_t *>(base + st.pack);
-  Prof pf(ctx, H266_PROF_SAO_ALF);
-  if (packed && !ctx->force_scalar) return launch_pass2_packed(ctx->stream, a, do_sao, do_alf, &ctx->launches);
-  return launch_pass2(ctx->stream, a, do_sao, do_alf, &ctx->launches);
+  Prof pf(ctx, stream, H266_PROF_SAO_ALF);
+  if (packed && !ctx->force_scalar) return launch_pass2_packed(stream, a, do_sao, do_alf, &ctx->launches);
+  return launch_pass2(stream, a, do_sao, do_alf, &ctx->launches);
 }
 
-int ensure_scratch(h266_ctx *ctx, const DPlane p[3], DPlane s[3]) {
+int ensure_scratch(Lane &ln, const DPlane p[3], DPlane s[3]) {
   for (int i = 0; i < 3; ++i) {
     const size_t n = (size_t)std::max(p[i].w, 0) * std::max(p[i].h, 0);
-    H266_TRY(ctx->scratch[i].ensure(std::max<size_t>(n, 1) * 2));
-    s[i] = DPlane{ctx->scratch[i].as<uint16_t>(), std::max(p[i].w, 1), p[i].w, p[i].h};
+    H266_TRY(ln.scratch[i].ensure(std::max<size_t>(n, 1) * 2));
+    s[i] = DPlane{ln.scratch[i].as<uint16_t>(), std::max(p[i].w, 1), p[i].w, p[i].h};
   }
   return H266_OK;
 }
 
-int run_deblock(h266_ctx *ctx, const uint8_t *base, const size_t off_seg[2], const size_t off_comp[2],
-                const uint32_t n_comp[2], const DPlane planes[3], int bd) {
-  Prof pf(ctx, H266_PROF_DEBLOCK);
-  return launch_deblock(ctx->stream, planes, bd, reinterpret_cast<const EdgeSeg *>(base + off_seg[0]),
+int run_deblock(h266_ctx *ctx, cudaStream_t stream, const uint8_t *base, const size_t off_seg[2],
+                const size_t off_comp[2], const uint32_t n_comp[2], const DPlane planes[3], int bd) {
+  Prof pf(ctx, stream, H266_PROF_DEBLOCK);
+  return launch_deblock(stream, planes, bd, reinterpret_cast<const EdgeSeg *>(base + off_seg[0]),
                         reinterpret_cast<const uint32_t *>(base + off_comp[0]), n_comp[0],
                         reinterpret_cast<const EdgeSeg *>(base + off_seg[1]),
                         reinterpret_cast<const uint32_t *>(base + off_comp[1]), n_comp[1], &ctx->launches);
 }
 
-int plane_map(h266_ctx *ctx, DPlane dst, DPlane src, const uint16_t *lut) {
-  Prof pf(ctx, lut ? H266_PROF_LMCS : H266_PROF_COPY);
-  return launch_plane_map(ctx->stream, dst, src, lut, &ctx->launches);
+int plane_map(h266_ctx *ctx, cudaStream_t stream, DPlane dst, DPlane src, const uint16_t *lut) {
+  Prof pf(ctx, stream, lut ? H266_PROF_LMCS : H266_PROF_COPY);
+  return launch_plane_map(stream, dst, src, lut, &ctx->launches);
 }
 
-int build_lut(h266_ctx *ctx, uint16_t *lut, const h266_lmcs_derived &l, uint32_t mn, uint32_t mx) {
-  Prof pf(ctx, H266_PROF_LMCS);
-  return launch_lmcs_lut(ctx->stream, lut, l, mn, mx, &ctx->launches);
+int build_lut(h266_ctx *ctx, cudaStream_t stream, uint16_t *lut, const h266_lmcs_derived &l, uint32_t mn,
+              uint32_t mx) {
+  Prof pf(ctx, stream, H266_PROF_LMCS);
+  return launch_lmcs_lut(stream, lut, l, mn, mx, &ctx->launches);
 }
 
 int check_lmcs(const h266_lmcs_derived *l, uint32_t mn, uint32_t mx) {
@@ -573,22 +621,32 @@ int check_lmcs(const h266_lmcs_derived *l, uint32_t mn, uint32_t mx) {
   return H266_OK;
 }
 
-// Host-side preparation of one chain call: deblocking plan (ctx->plan), pass-2
-// tables, and the side-information blob (ctx->blob) with its section offsets.
-struct Prepared {
+}  // namespace
+
+// Host-side preparation of one chain call: the deblocking plan, the pass-2
+// tables and the side-information blob with its section offsets.  A failed
+// preparation keeps its status and message (it may run on a worker thread).
+struct h266::Prep {
+  DeblockPlan plan;
+  std::vector<uint8_t> blob;
   Pass2Host h;
   Staged st;
   uint32_t n_comp[2] = {0, 0};
+  int rc = H266_OK;
+  std::string msg;
 };
 
-int prepare_chain(h266_ctx *ctx, const h266_picture &pic, const h266_in_loop_filter_args &a, Prepared &pr) {
+namespace {
+
+int prepare_chain(Prep &pr, const h266_picture &pic, const h266_in_loop_filter_args &a, TaskPool *pool) {
+  pr.st = Staged{};
   H266_TRY(check_lmcs(a.lmcs, a.lmcs_min_bin_idx, a.lmcs_max_bin_idx));
   if ((a.n_cus && !a.cus) || (a.n_no_filter_cols && !a.no_filter_cols) || (a.n_no_filter_rows && !a.no_filter_rows))
     return set_error(H266_ERR_INVALID_ARGUMENT, "NULL list with nonzero length");
   if (a.clip_cols && !a.clip_rows) return set_error(H266_ERR_INVALID_ARGUMENT, "clip_rows is NULL while clip_cols is not");
   H266_TRY(build_deblock_plan(pic, a.cus, a.n_cus, a.chroma_cus, a.n_chroma_cus, a.mv_grid, a.deblock,
                               a.chroma_format_idc, a.no_filter_cols, a.n_no_filter_cols, a.no_filter_rows,
-                              a.n_no_filter_rows, ctx->plan));
+                              a.n_no_filter_rows, pr.plan, pool));
   Pass2Inputs in;
   in.sao = a.sao;
   in.sao_cfg = a.sao ? &a.sao_cfg : nullptr;
@@ -600,40 +658,63 @@ int prepare_chain(h266_ctx *ctx, const h266_picture &pic, const h266_in_loop_fil
   in.n_cols = a.n_clip_cols;
   in.n_rows = a.n_clip_rows;
   H266_TRY(build_pass2(pic, in, pr.h));
-  ctx->blob.clear();
-  stage_deblock(ctx, pr.st);
-  if (pr.h.do_sao || pr.h.do_alf) stage_pass2(ctx, pr.h, pr.st);
-  for (int d = 0; d < 2; ++d) pr.n_comp[d] = (uint32_t)ctx->plan.comp[d].size() - 1;
+  pr.blob.clear();
+  stage_deblock(pr.plan, pr.blob, pr.st);
+  if (pr.h.do_sao || pr.h.do_alf) stage_pass2(pr.h, pr.blob, pr.st);
+  for (int d = 0; d < 2; ++d) pr.n_comp[d] = (uint32_t)pr.plan.comp[d].size() - 1;
   return H266_OK;
 }
 
 // Launches the chain: LMCS (LUT already built) -> deblock -> SAO/ALF.  With a
 // pass 2 the deblocked planes go to the scratch planes S, else in place.
-int exec_chain(h266_ctx *ctx, const uint8_t *base, const Staged &st, const uint32_t n_comp[2], const Pass2Host &h,
-               const uint16_t *lut, int dbd, const DPlane P[3], const DPlane S[3]) {
+int exec_chain(h266_ctx *ctx, cudaStream_t stream, const uint8_t *base, const Staged &st, const uint32_t n_comp[2],
+               const Pass2Host &h, const uint16_t *lut, int dbd, const DPlane P[3], const DPlane S[3]) {
   if (!h.do_sao && !h.do_alf) {
-    if (lut) H266_TRY(plane_map(ctx, P[0], P[0], lut));
-    return run_deblock(ctx, base, st.seg, st.comp, n_comp, P, dbd);
+    if (lut) H266_TRY(plane_map(ctx, stream, P[0], P[0], lut));
+    return run_deblock(ctx, stream, base, st.seg, st.comp, n_comp, P, dbd);
   }
-  for (int i = 0; i < 3; ++i) H266_TRY(plane_map(ctx, S[i], P[i], i == 0 ? lut : nullptr));
-  H266_TRY(run_deblock(ctx, base, st.seg, st.comp, n_comp, S, dbd));
-  return run_pass2(ctx, h.args, h.do_sao, h.do_alf, h.packed, base, st, S, P);
+  for (int i = 0; i < 3; ++i) H266_TRY(plane_map(ctx, stream, S[i], P[i], i == 0 ? lut : nullptr));
+  H266_TRY(run_deblock(ctx, stream, base, st.seg, st.comp, n_comp, S, dbd));
+  return run_pass2(ctx, stream, h.args, h.do_sao, h.do_alf, h.packed, base, st, S, P);
 }
 
-// The chain for one picture whose planes are already device views `P`.
-int chain_on_device(h266_ctx *ctx, const h266_picture &pic, const DPlane P[3], const h266_in_loop_filter_args &a) {
-  Prepared pr;
-  H266_TRY(prepare_chain(ctx, pic, a, pr));
-  H266_TRY(upload_blob(ctx, &pr.st.base));
+// Queues the chain for one prepared picture whose planes are the device
+// views `P` on lane `ln`.
+int issue_chain(h266_ctx *ctx, Lane &ln, Prep &pr, const DPlane P[3], const h266_in_loop_filter_args &a) {
+  H266_TRY(upload_blob(ln, pr.blob, &pr.st.base));
   const uint16_t *lut = nullptr;
   if (a.lmcs) {
-    H266_TRY(ctx->lut.ensure(65536 * 2));
-    H266_TRY(build_lut(ctx, ctx->lut.as<uint16_t>(), *a.lmcs, a.lmcs_min_bin_idx, a.lmcs_max_bin_idx));
-    lut = ctx->lut.as<uint16_t>();
+    H266_TRY(ln.lut.ensure(65536 * 2));
+    H266_TRY(build_lut(ctx, ln.stream, ln.lut.as<uint16_t>(), *a.lmcs, a.lmcs_min_bin_idx, a.lmcs_max_bin_idx));
+    lut = ln.lut.as<uint16_t>();
   }
   DPlane S[3];
-  if (pr.h.do_sao || pr.h.do_alf) H266_TRY(ensure_scratch(ctx, P, S));
-  return exec_chain(ctx, pr.st.base, pr.st, pr.n_comp, pr.h, lut, (int)a.deblock.bit_depth, P, S);
+  if (pr.h.do_sao || pr.h.do_alf) H266_TRY(ensure_scratch(ln, P, S));
+  return exec_chain(ctx, ln.stream, pr.st.base, pr.st, pr.n_comp, pr.h, lut, (int)a.deblock.bit_depth, P, S);
+}
+
+// Worker pool of the context (created on first use): as many threads as the
+// host offers, at most 16.
+TaskPool *ctx_pool(h266_ctx *ctx) {
+  if (!ctx->pool) {
+    unsigned n = std::thread::hardware_concurrency();
+    n = std::max(1u, std::min(n, 16u));
+    ctx->pool.reset(new TaskPool(n));
+  }
+  return ctx->pool.get();
+}
+
+Prep &ctx_prep(h266_ctx *ctx, size_t i) {
+  while (ctx->preps.size() <= i) ctx->preps.emplace_back(new Prep());
+  return *ctx->preps[i];
+}
+
+// The chain for one picture whose planes are already device views `P`, on the
+// main lane; its deblocking plan is built with the worker pool.
+int chain_on_device(h266_ctx *ctx, const h266_picture &pic, const DPlane P[3], const h266_in_loop_filter_args &a) {
+  Prep &pr = ctx_prep(ctx, 0);
+  H266_TRY(prepare_chain(pr, pic, a, ctx_pool(ctx)));
+  return issue_chain(ctx, ctx->main, pr, P, a);
 }
 
 bool same_geometry(const h266_picture &a, const h266_picture &b) {
@@ -663,13 +744,18 @@ int h266_ctx_create(int device, h266_ctx **out) {
   h266_ctx *c = new h266_ctx();
   c->device = device;
   cudaError_t e = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->staged, cudaEventDisableTiming);
-  if (e == cudaSuccess) e = cudaEventRecord(c->staged, c->own);
   if (e != cudaSuccess) {
     delete c;
     return cuda_error(e, "h266_ctx_create");
   }
   c->stream = c->own;
+  const int rc = c->main.init(c->own);
+  if (rc != H266_OK) {
+    c->main.release();
+    cudaStreamDestroy(c->own);
+    delete c;
+    return rc;
+  }
   const char *fs = std::getenv("H266_FORCE_SCALAR_ALF");
   c->force_scalar = fs && fs[0] == '1';
   *out = c;
@@ -680,14 +766,17 @@ int h266_ctx_destroy(h266_ctx *ctx) {
   if (!ctx) return H266_OK;
   Guard g(ctx->device);
   cudaStreamSynchronize(ctx->stream);
-  for (int i = 0; i < 3; ++i) {
-    ctx->io[i].release();
-    ctx->scratch[i].release();
+  for (auto &l : ctx->lanes) {
+    cudaStreamSynchronize(l->stream);
+    l->release();
   }
-  ctx->lut.release();
-  ctx->side.release();
-  if (ctx->stage.ptr) cudaFreeHost(ctx->stage.ptr);
-  if (ctx->staged) cudaEventDestroy(ctx->staged);
+  ctx->main.release();
+  ctx->pool.reset();
+  for (auto &e : ctx->ev_pool) cudaEventDestroy(e);
+  for (auto &e : ctx->ev_pending) {
+    cudaEventDestroy(e.second.first);
+    cudaEventDestroy(e.second.second);
+  }
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
   return H266_OK;
@@ -696,6 +785,7 @@ int h266_ctx_destroy(h266_ctx *ctx) {
 int h266_ctx_set_stream(h266_ctx *ctx, void *stream) {
   H266_TRY(check_ctx(ctx));
   ctx->stream = stream ? (cudaStream_t)stream : ctx->own;
+  ctx->main.stream = ctx->stream;
   return H266_OK;
 }
 
@@ -719,12 +809,13 @@ int h266_lmcs_inverse_map_luma(h266_ctx *ctx, h266_picture *pic, const h266_lmcs
   if (!lmcs) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL lmcs");
   H266_TRY(check_lmcs(lmcs, mn, mx));
   Guard g(ctx->device);
+  Lane &ln = ctx->main;
   DPlane P[3];
-  H266_TRY(picture_to_device(ctx, *pic, P));
-  H266_TRY(ctx->lut.ensure(65536 * 2));
-  H266_TRY(build_lut(ctx, ctx->lut.as<uint16_t>(), *lmcs, mn, mx));
-  H266_TRY(plane_map(ctx, P[0], P[0], ctx->lut.as<uint16_t>()));
-  return picture_from_device(ctx, *pic);
+  H266_TRY(picture_to_device(ln, *pic, P));
+  H266_TRY(ln.lut.ensure(65536 * 2));
+  H266_TRY(build_lut(ctx, ln.stream, ln.lut.as<uint16_t>(), *lmcs, mn, mx));
+  H266_TRY(plane_map(ctx, ln.stream, P[0], P[0], ln.lut.as<uint16_t>()));
+  return picture_from_device(ln, *pic);
 }
 
 int h266_apply_deblocking_clipped(h266_ctx *ctx, h266_picture *pic, const h266_deblock_cu *cus, uint64_t n_cus,
@@ -738,17 +829,19 @@ int h266_apply_deblocking_clipped(h266_ctx *ctx, h266_picture *pic, const h266_d
   if ((n_cus && !cus) || (n_cols && !nf_cols) || (n_rows && !nf_rows))
     return set_error(H266_ERR_INVALID_ARGUMENT, "NULL list with nonzero length");
   Guard g(ctx->device);
+  Prep &pr = ctx_prep(ctx, 0);
   H266_TRY(build_deblock_plan(*pic, cus, n_cus, chroma_cus, n_chroma_cus, mv_grid, *params, cfi, nf_cols, n_cols,
-                              nf_rows, n_rows, ctx->plan));
+                              nf_rows, n_rows, pr.plan, ctx_pool(ctx)));
+  Lane &ln = ctx->main;
   DPlane P[3];
-  H266_TRY(picture_to_device(ctx, *pic, P));
+  H266_TRY(picture_to_device(ln, *pic, P));
   Staged st;
-  ctx->blob.clear();
-  stage_deblock(ctx, st);
-  H266_TRY(upload_blob(ctx, &st.base));
-  const uint32_t n_comp[2] = {(uint32_t)ctx->plan.comp[0].size() - 1, (uint32_t)ctx->plan.comp[1].size() - 1};
-  H266_TRY(run_deblock(ctx, st.base, st.seg, st.comp, n_comp, P, (int)params->bit_depth));
-  return picture_from_device(ctx, *pic);
+  pr.blob.clear();
+  stage_deblock(pr.plan, pr.blob, st);
+  H266_TRY(upload_blob(ln, pr.blob, &st.base));
+  const uint32_t n_comp[2] = {(uint32_t)pr.plan.comp[0].size() - 1, (uint32_t)pr.plan.comp[1].size() - 1};
+  H266_TRY(run_deblock(ctx, ln.stream, st.base, st.seg, st.comp, n_comp, P, (int)params->bit_depth));
+  return picture_from_device(ln, *pic);
 }
 
 static int pass2_entry(h266_ctx *ctx, h266_picture *pic, const Pass2Inputs &in) {
@@ -756,21 +849,23 @@ static int pass2_entry(h266_ctx *ctx, h266_picture *pic, const Pass2Inputs &in) 
   H266_TRY(check_picture(pic));
   if (in.cols && !in.rows) return set_error(H266_ERR_INVALID_ARGUMENT, "row bounds NULL while col bounds are not");
   Guard g(ctx->device);
-  Pass2Host h;
+  Prep &pr = ctx_prep(ctx, 0);
+  Pass2Host &h = pr.h;
   H266_TRY(build_pass2(*pic, in, h));
+  Lane &ln = ctx->main;
   DPlane P[3];
-  H266_TRY(picture_to_device(ctx, *pic, P));
+  H266_TRY(picture_to_device(ln, *pic, P));
   if (h.do_sao || h.do_alf) {
     Staged st;
-    ctx->blob.clear();
-    stage_pass2(ctx, h, st);
-    H266_TRY(upload_blob(ctx, &st.base));
+    pr.blob.clear();
+    stage_pass2(h, pr.blob, st);
+    H266_TRY(upload_blob(ln, pr.blob, &st.base));
     DPlane S[3];
-    H266_TRY(ensure_scratch(ctx, P, S));
-    for (int i = 0; i < 3; ++i) H266_TRY(plane_map(ctx, S[i], P[i], nullptr));
-    H266_TRY(run_pass2(ctx, h.args, h.do_sao, h.do_alf, h.packed, st.base, st, S, P));
+    H266_TRY(ensure_scratch(ln, P, S));
+    for (int i = 0; i < 3; ++i) H266_TRY(plane_map(ctx, ln.stream, S[i], P[i], nullptr));
+    H266_TRY(run_pass2(ctx, ln.stream, h.args, h.do_sao, h.do_alf, h.packed, st.base, st, S, P));
   }
-  return picture_from_device(ctx, *pic);
+  return picture_from_device(ln, *pic);
 }
 
 int h266_apply_sao_clipped(h266_ctx *ctx, h266_picture *pic, const h266_sao_picture *sao_pic,
@@ -808,17 +903,71 @@ int h266_apply_in_loop_filters(h266_ctx *ctx, h266_picture *pic, const h266_in_l
   if (!args) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL args");
   Guard g(ctx->device);
   DPlane P[3];
-  H266_TRY(picture_to_device(ctx, *pic, P));
+  H266_TRY(picture_to_device(ctx->main, *pic, P));  // the copy overlaps the host-side preparation
   H266_TRY(chain_on_device(ctx, *pic, P, *args));
-  return picture_from_device(ctx, *pic);
+  return picture_from_device(ctx->main, *pic);
 }
 
+// Pictures of a batch are prepared on the worker pool (one picture per worker,
+// in parallel) while this thread queues every prepared picture, in order, on
+// one of kBatchLanes streams: upload, side information, chain, download.  The
+// lanes start after the work already queued on the context stream, and the
+// context stream waits for all of them before the call returns; host pictures
+// are complete on return.
 int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *const *pics,
                                      const h266_in_loop_filter_args *const *args) {
+  constexpr uint32_t kBatchLanes = 4;
   H266_TRY(check_ctx(ctx));
   if (n && (!pics || !args)) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL batch arrays");
-  for (uint32_t i = 0; i < n; ++i) H266_TRY(h266_apply_in_loop_filters(ctx, pics[i], args[i]));
-  return H266_OK;
+  bool any_host = false;
+  for (uint32_t i = 0; i < n; ++i) {
+    H266_TRY(check_picture(pics[i]));
+    if (!args[i]) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL args in batch");
+    any_host |= pics[i]->mem == H266_MEM_HOST;
+  }
+  if (n <= 1) return n ? h266_apply_in_loop_filters(ctx, pics[0], args[0]) : H266_OK;
+  Guard g(ctx->device);
+  const uint32_t n_lanes = std::min(n, kBatchLanes);
+  while (ctx->lanes.size() < n_lanes) {
+    std::unique_ptr<Lane> l(new Lane());
+    const int rc = l->init(nullptr);
+    if (rc != H266_OK) {
+      l->release();
+      return rc;
+    }
+    ctx->lanes.push_back(std::move(l));
+  }
+  H266_CUDA(cudaEventRecord(ctx->main.mark, ctx->stream));
+  for (uint32_t l = 0; l < n_lanes; ++l) H266_CUDA(cudaStreamWaitEvent(ctx->lanes[l]->stream, ctx->main.mark, 0));
+  for (uint32_t i = 0; i < n; ++i) ctx_prep(ctx, i + 1);
+  TaskPool *pool = ctx_pool(ctx);
+  pool->start(n, [&](size_t i) {
+    Prep &pr = *ctx->preps[i + 1];
+    pr.rc = prepare_chain(pr, *pics[i], *args[i], nullptr);
+    if (pr.rc != H266_OK) pr.msg = h266_last_error();
+  });
+  int rc = H266_OK;
+  for (uint32_t i = 0; i < n && rc == H266_OK; ++i) {
+    pool->wait_item(i);
+    Prep &pr = *ctx->preps[i + 1];
+    if (pr.rc != H266_OK) {
+      rc = set_error(pr.rc, pr.msg);
+      break;
+    }
+    Lane &ln = *ctx->lanes[i % n_lanes];
+    DPlane P[3];
+    rc = picture_to_device(ln, *pics[i], P);
+    if (rc == H266_OK) rc = issue_chain(ctx, ln, pr, P, *args[i]);
+    if (rc == H266_OK) rc = picture_from_device(ln, *pics[i], false);
+  }
+  pool->wait_all();
+  for (uint32_t l = 0; l < n_lanes; ++l) {
+    Lane &ln = *ctx->lanes[l];
+    H266_CUDA(cudaEventRecord(ln.mark, ln.stream));
+    H266_CUDA(cudaStreamWaitEvent(ctx->stream, ln.mark, 0));
+    if (any_host || rc != H266_OK) H266_CUDA(cudaStreamSynchronize(ln.stream));
+  }
+  return rc;
 }
 
 int h266_ctx_set_profiling(h266_ctx *ctx, int on) {
@@ -864,8 +1013,8 @@ int h266_chain_plan_create(h266_ctx *ctx, const h266_picture *pic, const h266_in
   }
   H266_TRY(check_picture(&geom));
   Guard g(ctx->device);
-  Prepared pr;
-  H266_TRY(prepare_chain(ctx, geom, *args, pr));
+  Prep &pr = ctx_prep(ctx, 0);
+  H266_TRY(prepare_chain(pr, geom, *args, ctx_pool(ctx)));
   h266_chain_plan *pl = new h266_chain_plan();
   pl->device = ctx->device;
   pl->geom = geom;
@@ -873,15 +1022,15 @@ int h266_chain_plan_create(h266_ctx *ctx, const h266_picture *pic, const h266_in
     h266_chain_plan_destroy(pl);
     return rc;
   };
-  int rc = pl->side.ensure(ctx->blob.size());
+  int rc = pl->side.ensure(pr.blob.size());
   if (rc != H266_OK) return fail(rc);
-  cudaError_t e = cudaMemcpy(pl->side.ptr, ctx->blob.data(), ctx->blob.size(), cudaMemcpyHostToDevice);
+  cudaError_t e = cudaMemcpy(pl->side.ptr, pr.blob.data(), pr.blob.size(), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return fail(cuda_error(e, "plan upload"));
   pl->lmcs = args->lmcs != nullptr;
   if (pl->lmcs) {
     if ((rc = pl->lut.ensure(65536 * 2)) != H266_OK) return fail(rc);
-    if ((rc = build_lut(ctx, pl->lut.as<uint16_t>(), *args->lmcs, args->lmcs_min_bin_idx, args->lmcs_max_bin_idx)) !=
-        H266_OK)
+    if ((rc = build_lut(ctx, ctx->stream, pl->lut.as<uint16_t>(), *args->lmcs, args->lmcs_min_bin_idx,
+                        args->lmcs_max_bin_idx)) != H266_OK)
       return fail(rc);
   }
   pl->pass2 = pr.h.do_sao || pr.h.do_alf;
@@ -919,7 +1068,7 @@ int h266_chain_plan_execute(h266_ctx *ctx, h266_chain_plan *plan, h266_picture *
   if (plan->device != ctx->device) return set_error(H266_ERR_INVALID_ARGUMENT, "plan belongs to another device");
   Guard g(ctx->device);
   DPlane P[3], S[3];
-  H266_TRY(picture_to_device(ctx, *pic, P));
+  H266_TRY(picture_to_device(ctx->main, *pic, P));
   for (int i = 0; i < 3; ++i)
     S[i] = DPlane{plan->pass2 ? plan->scratch[i].as<uint16_t>() : nullptr, std::max(P[i].w, 1), P[i].w, P[i].h};
   Staged st;
@@ -936,7 +1085,7 @@ int h266_chain_plan_execute(h266_ctx *ctx, h266_chain_plan *plan, h266_picture *
   h.do_sao = plan->do_sao;
   h.do_alf = plan->do_alf;
   h.packed = plan->packed;
-  return exec_chain(ctx, st.base, st, plan->n_comp, h, plan->lmcs ? plan->lut.as<uint16_t>() : nullptr,
+  return exec_chain(ctx, ctx->stream, st.base, st, plan->n_comp, h, plan->lmcs ? plan->lut.as<uint16_t>() : nullptr,
                     plan->deblock_bd, P, S);
 }
 
@@ -1000,15 +1149,16 @@ extern "C" int h266_apply_in_loop_filters_noalloc(h266_picture *pic, const h266_
     return set_error(H266_ERR_INVALID_ARGUMENT, "the allocation-free chain takes device planes (H266_MEM_DEVICE)");
   uint8_t *scratch = nullptr;
   H266_TRY(noalloc_scratch(&scratch));
-  // A context object on the stack carries the stream and host-side staging
-  // vectors; it owns no device memory and no CUDA handles.
+  // A context object on the stack carries the stream and the launch counter;
+  // it owns no device memory and no CUDA handles.  The side information is
+  // built on this thread.
   h266_ctx local;
   H266_CUDA(cudaGetDevice(&local.device));
   local.stream = (cudaStream_t)cuda_stream;
-  Prepared pr;
-  H266_TRY(prepare_chain(&local, *pic, *args, pr));
+  Prep pr;
+  H266_TRY(prepare_chain(pr, *pic, *args, nullptr));
   // Scratch layout: [side information][LMCS LUT][three deblocked planes].
-  const size_t blob = align256(local.blob.size());
+  const size_t blob = align256(pr.blob.size());
   const size_t lut_off = blob, lut_bytes = args->lmcs ? align256(65536 * 2) : 0;
   size_t planes_off = lut_off + lut_bytes, need = planes_off;
   const bool pass2 = pr.h.do_sao || pr.h.do_alf;
@@ -1024,13 +1174,13 @@ extern "C" int h266_apply_in_loop_filters_noalloc(h266_picture *pic, const h266_
                                                std::to_string((size_t)H266_NOALLOC_SCRATCH_BYTES));
   // Every scratch region is written in full below before anything reads it,
   // so no region needs clearing.
-  if (!local.blob.empty())
-    H266_CUDA(cudaMemcpyAsync(scratch, local.blob.data(), local.blob.size(), cudaMemcpyHostToDevice, local.stream));
+  if (!pr.blob.empty())
+    H266_CUDA(cudaMemcpyAsync(scratch, pr.blob.data(), pr.blob.size(), cudaMemcpyHostToDevice, local.stream));
   pr.st.base = scratch;
   const uint16_t *lut = nullptr;
   if (args->lmcs) {
     uint16_t *l = reinterpret_cast<uint16_t *>(scratch + lut_off);
-    H266_TRY(build_lut(&local, l, *args->lmcs, args->lmcs_min_bin_idx, args->lmcs_max_bin_idx));
+    H266_TRY(build_lut(&local, local.stream, l, *args->lmcs, args->lmcs_min_bin_idx, args->lmcs_max_bin_idx));
     lut = l;
   }
   DPlane P[3], S[3];
@@ -1039,5 +1189,5 @@ extern "C" int h266_apply_in_loop_filters_noalloc(h266_picture *pic, const h266_
     S[i] = DPlane{reinterpret_cast<uint16_t *>(scratch + plane_off[i]), std::max<int>((int)pl[i]->width, 1),
                   (int)pl[i]->width, (int)pl[i]->height};
   }
-  return exec_chain(&local, scratch, pr.st, pr.n_comp, pr.h, lut, (int)args->deblock.bit_depth, P, S);
+  return exec_chain(&local, local.stream, scratch, pr.st, pr.n_comp, pr.h, lut, (int)args->deblock.bit_depth, P, S);
 }

@@ -19,6 +19,7 @@
 // reference's clamped reads and bounds-checked Clip1 writes on global memory.
 #include <algorithm>
 #include <cstring>
+#include <memory>
 #include <numeric>
 
 #include "internal.h"
@@ -295,41 +296,73 @@ void Walker::walk_cu(const PlaneCfg &pc, bool vert, const MvGrid &mv, const uint
 inline int reach(int m) { return m <= 3 ? 4 : m + 1; }
 
 // Groups one (pass, plane) segment list into components and appends them.
-void group(std::vector<Emitted> &segs, std::vector<EdgeSeg> &dst, std::vector<uint32_t> &comp, uint32_t &max_len) {
+// Components come out band by band, by footprint start inside a band, with
+// their members in emission (reference) order.  Segments are bucketed by band
+// in emission order; decode order visits the CUs crossing a band from its low
+// end to its high end (z-scan inside a CTB, raster / tile order between CTBs),
+// so a bucket is normally sorted by footprint start already and the pass is
+// linear.  A bucket that is not (CU lists in an unusual order) is sorted, and
+// its components' members are put back in emission order.
+struct GroupScratch {
+  std::vector<uint32_t> head, cursor, order, members;
+  std::vector<int32_t> start, end;
+};
+
+void group(const std::vector<Emitted> &segs, std::vector<EdgeSeg> &dst, std::vector<uint32_t> &comp,
+           uint32_t &max_len, GroupScratch &g) {
   const size_t n = segs.size();
   if (n == 0) return;
-  struct Key {
-    uint32_t band;
-    int32_t start, end;
-    uint32_t i;
-  };
-  std::vector<Key> keys(n);
+  g.start.resize(n);
+  g.end.resize(n);
+  uint32_t max_band = 0;
   for (size_t i = 0; i < n; ++i) {
     const EdgeSeg &s = segs[i].s;
     const bool vert = s.flags & 1;
     const int pos = vert ? s.x : s.y;
-    keys[i] = Key{vert ? s.y : s.x, pos - reach(s.mfl >> 4), pos + reach(s.mfl & 15), (uint32_t)i};
+    g.start[i] = pos - reach(s.mfl >> 4);
+    g.end[i] = pos + reach(s.mfl & 15);
+    max_band = std::max<uint32_t>(max_band, vert ? s.y : s.x);
   }
-  std::sort(keys.begin(), keys.end(), [](const Key &a, const Key &b) {
-    return a.band != b.band ? a.band < b.band : (a.start != b.start ? a.start < b.start : a.i < b.i);
-  });
-  std::vector<uint32_t> members;
-  size_t i = 0;
-  while (i < n) {
-    size_t j = i + 1;
-    int32_t end = keys[i].end;
-    while (j < n && keys[j].band == keys[i].band && keys[j].start < end) {
-      end = std::max(end, keys[j].end);
-      ++j;
+  g.head.assign((size_t)max_band + 2, 0);
+  for (size_t i = 0; i < n; ++i) {
+    const EdgeSeg &s = segs[i].s;
+    ++g.head[(size_t)((s.flags & 1) ? s.y : s.x) + 1];
+  }
+  for (size_t b = 1; b < g.head.size(); ++b) g.head[b] += g.head[b - 1];
+  g.cursor.assign(g.head.begin(), g.head.end() - 1);
+  g.order.resize(n);
+  for (size_t i = 0; i < n; ++i) {
+    const EdgeSeg &s = segs[i].s;
+    g.order[g.cursor[(s.flags & 1) ? s.y : s.x]++] = (uint32_t)i;
+  }
+  dst.reserve(dst.size() + n);
+  uint32_t longest = max_len;
+  auto by_start = [&](uint32_t a, uint32_t b) { return g.start[a] < g.start[b]; };
+  for (size_t b = 0; b + 1 < g.head.size(); ++b) {
+    uint32_t *lo = g.order.data() + g.head[b], *hi = g.order.data() + g.head[b + 1];
+    if (lo == hi) continue;
+    const bool sorted = std::is_sorted(lo, hi, by_start);
+    if (!sorted) std::stable_sort(lo, hi, by_start);  // ties keep emission order
+    for (uint32_t *i = lo; i < hi;) {
+      uint32_t *j = i + 1;
+      int32_t e = g.end[*i];
+      while (j < hi && g.start[*j] < e) {
+        e = std::max(e, g.end[*j]);
+        ++j;
+      }
+      comp.push_back((uint32_t)dst.size());
+      if (sorted) {
+        for (uint32_t *t = i; t < j; ++t) dst.push_back(segs[*t].s);
+      } else {
+        g.members.assign(i, j);
+        std::sort(g.members.begin(), g.members.end());  // indices are emission order
+        for (uint32_t m : g.members) dst.push_back(segs[m].s);
+      }
+      longest = std::max<uint32_t>(longest, (uint32_t)(j - i));
+      i = j;
     }
-    members.clear();
-    for (size_t t = i; t < j; ++t) members.push_back(keys[t].i);
-    std::sort(members.begin(), members.end(), [&](uint32_t a, uint32_t b) { return segs[a].order < segs[b].order; });
-    comp.push_back((uint32_t)dst.size());
-    for (uint32_t m : members) dst.push_back(segs[m].s);
-    max_len = std::max<uint32_t>(max_len, (uint32_t)(j - i));
-    i = j;
   }
+  max_len = longest;
 }
 
 }  // namespace
@@ -337,7 +370,7 @@ void group(std::vector<Emitted> &segs, std::vector<EdgeSeg> &dst, std::vector<ui
 int build_deblock_plan(const h266_picture &pic, const h266_deblock_cu *cus, uint64_t n_cus,
                        const h266_deblock_cu *chroma_cus, uint64_t n_chroma, const h266_deblock_mv_grid *mv,
                        const h266_deblock_params &params, uint32_t cfi, const uint32_t *nf_cols, uint64_t n_cols,
-                       const uint32_t *nf_rows, uint64_t n_rows, DeblockPlan &plan) {
+                       const uint32_t *nf_rows, uint64_t n_rows, DeblockPlan &plan, TaskPool *pool) {
   for (int d = 0; d < 2; ++d) {
     plan.segs[d].clear();
     plan.comp[d].assign(1, 0);  // component offsets end with the total count
@@ -364,29 +397,54 @@ int build_deblock_plan(const h266_picture &pic, const h266_deblock_cu *cus, uint
   const int bd = (int)params.bit_depth;
   const uint32_t ctb = 1u << params.ctb_log2_size_y;
   const int pw = (int)pic.luma.width, ph = (int)pic.luma.height;
-  MvGrid mvg{mv};
-  std::vector<Emitted> em;
+  MvGrid mvg{mv}, none{nullptr};
+  // Six independent lists: (luma, cb, cr) x (vertical, horizontal) pass.  Each
+  // is walked and grouped on its own (in parallel with a pool) and the lists
+  // are concatenated per pass in plane order.
+  const bool sep = chroma_cus != nullptr;
+  const int n_lists = cfi != 0 ? 6 : 2;
   Walker luma(cus, n_cus, pw, ph);
-  PlaneCfg lc{0, 1, 1, params.luma_beta_offset_div2, params.luma_tc_offset_div2, 0, bd, ctb};
-  for (int d = 0; d < 2; ++d) {
+  std::unique_ptr<Walker> cwalk;
+  if (cfi != 0 && sep) cwalk.reset(new Walker(chroma_cus, n_chroma, pw, ph));
+  const Walker &cw = sep && cfi != 0 ? *cwalk : luma;
+  const PlaneCfg cfg[3] = {
+      {0, 1, 1, params.luma_beta_offset_div2, params.luma_tc_offset_div2, 0, bd, ctb},
+      {1, 2, 2, params.cb_beta_offset_div2, params.cb_tc_offset_div2, params.chroma_qp_offset_cb, bd, ctb},
+      {2, 2, 2, params.cr_beta_offset_div2, params.cr_tc_offset_div2, params.chroma_qp_offset_cr, bd, ctb}};
+  auto one_list = [&](size_t l) {
+    thread_local std::vector<Emitted> em;
+    thread_local GroupScratch gs;
+    const int plane = (int)l / 2, d = (int)l % 2;
     em.clear();
-    luma.walk(lc, d == 0, mvg, d == 0 ? nf_cols : nf_rows, d == 0 ? n_cols : n_rows, em);
-    group(em, plan.segs[d], plan.comp[d], plan.max_comp_len[d]);
+    (plane == 0 ? luma : cw).walk(cfg[plane], d == 0, plane == 0 ? mvg : none, d == 0 ? nf_cols : nf_rows,
+                                  d == 0 ? n_cols : n_rows, em);
+    DeblockPlan::Part &part = plan.parts[l];
+    part.segs.clear();
+    part.comp.clear();
+    part.max_len = 0;
+    group(em, part.segs, part.comp, part.max_len, gs);
+  };
+  if (pool && pool->size() > 1)
+    pool->run((size_t)n_lists, one_list);
+  else
+    for (int l = 0; l < n_lists; ++l) one_list((size_t)l);
+  for (int d = 0; d < 2; ++d) {
+    size_t total = 0, total_c = 0;
+    for (int l = d; l < n_lists; l += 2) {
+      total += plan.parts[l].segs.size();
+      total_c += plan.parts[l].comp.size();
+    }
+    plan.segs[d].reserve(total);
+    plan.comp[d].reserve(total_c + 1);
+    for (int l = d; l < n_lists; l += 2) {
+      const uint32_t base = (uint32_t)plan.segs[d].size();
+      const DeblockPlan::Part &part = plan.parts[l];
+      plan.segs[d].insert(plan.segs[d].end(), part.segs.begin(), part.segs.end());
+      for (uint32_t c : part.comp) plan.comp[d].push_back(base + c);
+      plan.max_comp_len[d] = std::max(plan.max_comp_len[d], part.max_len);
+    }
+    plan.comp[d].push_back((uint32_t)plan.segs[d].size());
   }
-  if (cfi != 0) {
-    const bool sep = chroma_cus != nullptr;
-    Walker cwalk(sep ? chroma_cus : cus, sep ? n_chroma : n_cus, pw, ph);
-    PlaneCfg cc[2] = {{1, 2, 2, params.cb_beta_offset_div2, params.cb_tc_offset_div2, params.chroma_qp_offset_cb, bd, ctb},
-                      {2, 2, 2, params.cr_beta_offset_div2, params.cr_tc_offset_div2, params.chroma_qp_offset_cr, bd, ctb}};
-    MvGrid none{nullptr};
-    for (int c = 0; c < 2; ++c)
-      for (int d = 0; d < 2; ++d) {
-        em.clear();
-        cwalk.walk(cc[c], d == 0, none, d == 0 ? nf_cols : nf_rows, d == 0 ? n_cols : n_rows, em);
-        group(em, plan.segs[d], plan.comp[d], plan.max_comp_len[d]);
-      }
-  }
-  for (int d = 0; d < 2; ++d) plan.comp[d].push_back((uint32_t)plan.segs[d].size());
   return H266_OK;
 }
 

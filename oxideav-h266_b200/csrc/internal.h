@@ -4,8 +4,12 @@
 
 #include <cuda_runtime.h>
 
+#include <condition_variable>
 #include <cstdint>
+#include <functional>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "oxideav_h266_b200.h"
@@ -29,6 +33,37 @@ int cuda_error(cudaError_t e, const char *what);   // H266_ERR_CUDA (or OUT_OF_M
     int rc_ = (call);           \
     if (rc_ != H266_OK) return rc_; \
   } while (0)
+
+// ---------------------------------------------------------------- host worker pool
+// Fixed set of host threads that run the items of one job at a time
+// (fn(0) .. fn(n-1), in any order and in parallel).  The thread that starts a
+// job may wait for single items, so it can consume results in order while the
+// workers are still producing later ones.  One job at a time per pool.
+class TaskPool {
+ public:
+  explicit TaskPool(unsigned threads);
+  ~TaskPool();
+  TaskPool(const TaskPool &) = delete;
+  TaskPool &operator=(const TaskPool &) = delete;
+  unsigned size() const { return (unsigned)workers_.size(); }
+  void start(size_t n, std::function<void(size_t)> fn);  // returns at once
+  void wait_item(size_t i);                               // item i of the current job has finished
+  void wait_all();                                        // every item of the current job has finished
+  void run(size_t n, std::function<void(size_t)> fn) {    // start + wait_all
+    start(n, std::move(fn));
+    wait_all();
+  }
+
+ private:
+  void loop();
+  std::vector<std::thread> workers_;
+  std::mutex mu_;
+  std::condition_variable work_cv_, done_cv_;
+  std::function<void(size_t)> fn_;
+  std::vector<uint8_t> done_;
+  size_t n_ = 0, next_ = 0, finished_ = 0;
+  bool stop_ = false;
+};
 
 // ---------------------------------------------------------------- device buffers
 // A growable device allocation owned by a context.
@@ -71,12 +106,20 @@ struct DeblockPlan {
   std::vector<EdgeSeg> segs[2];      // [0] vertical pass, [1] horizontal pass
   std::vector<uint32_t> comp[2];     // component start offsets (+ final end)
   uint32_t max_comp_len[2] = {0, 0};
+  // per (plane, pass) lists before concatenation, index plane * 2 + pass; each
+  // on its own cache lines, as different threads fill them
+  struct alignas(64) Part {
+    std::vector<EdgeSeg> segs;
+    std::vector<uint32_t> comp;
+    uint32_t max_len = 0;
+  };
+  Part parts[6];
 };
 
 int build_deblock_plan(const h266_picture &pic, const h266_deblock_cu *cus, uint64_t n_cus,
                        const h266_deblock_cu *chroma_cus, uint64_t n_chroma, const h266_deblock_mv_grid *mv,
                        const h266_deblock_params &params, uint32_t cfi, const uint32_t *nf_cols, uint64_t n_cols,
-                       const uint32_t *nf_rows, uint64_t n_rows, DeblockPlan &plan);
+                       const uint32_t *nf_rows, uint64_t n_rows, DeblockPlan &plan, TaskPool *pool = nullptr);
 
 // Launches the two deblocking passes (vertical then horizontal) in place on
 // the three device planes.  seg/comp point at device copies of the plan.

@@ -139,6 +139,57 @@ def test_batch_mixed_sizes(ctx):
         assert_same(got, want, "batch")
 
 
+BATCH_MIX = [lambda s: W.stress_workload(7000 + s), lambda s: small_c2(7100 + s),
+             lambda s: W.config1(7200 + s), lambda s: W.stress_workload(7300 + s, dual_tree=True, bit_depth=8)]
+
+
+def test_batch_pipelined_host_pictures(ctx):
+    """More pictures than batch lanes, mixed sizes and formats: every lane is
+    reused and side information is prepared on the worker pool."""
+    items = [BATCH_MIX[i % len(BATCH_MIX)](i) for i in range(11)]
+    pics = [p.copy() for p, _ in items]
+    ctx.apply_in_loop_filters_batch(pics, [f for _, f in items])
+    for i, ((p, f), got) in enumerate(zip(items, pics)):
+        want = p.copy()
+        oracle.apply_in_loop_filters(want, f)
+        assert_same(got, want, f"batch picture {i}")
+
+
+def test_batch_device_pictures_follow_context_stream(ctx):
+    import torch
+
+    items = [BATCH_MIX[i % len(BATCH_MIX)](20 + i) for i in range(6)]
+    devs = [native.DevicePicture.from_host(p) for p, _ in items]
+    torch.cuda.synchronize()
+    ctx.apply_in_loop_filters_batch(devs, [f for _, f in items])
+    # a second chain on picture 0 queued on the context stream runs after the batch
+    p0, f0 = items[0]
+    ctx.apply_in_loop_filters(devs[0], f0)
+    ctx.synchronize()
+    for i, ((p, f), d) in enumerate(zip(items, devs)):
+        want = p.copy()
+        oracle.apply_in_loop_filters(want, f)
+        if i == 0:
+            oracle.apply_in_loop_filters(want, f)
+        assert_same(d.to_host(), want, f"device batch picture {i}")
+
+
+def test_batch_reports_a_failed_preparation(ctx):
+    items = [W.stress_workload(7400 + i) for i in range(5)]
+    bad = items[3][1]
+    bad.lmcs_max_bin = 16  # rejected while the side information is prepared
+    pics = [p.copy() for p, _ in items]
+    with pytest.raises(native.H266Error) as e:
+        ctx.apply_in_loop_filters_batch(pics, [f for _, f in items])
+    assert "LMCS bin index" in str(e.value)
+    # the context stays usable
+    p, f = items[0]
+    got, want = p.copy(), p.copy()
+    ctx.apply_in_loop_filters(got, f)
+    oracle.apply_in_loop_filters(want, f)
+    assert_same(got, want, "after failed batch")
+
+
 def test_repeat_calls_are_deterministic(ctx):
     pic, fa = W.stress_workload(99)
     a, b = pic.copy(), pic.copy()
