@@ -10,9 +10,10 @@ planes (199 MB for 32 pictures) exceed the 126 MB L2, so no flush is needed.
   value     device-resident throughput: side information resident in resident
             plans (h266_chain_plan_*), samples resident in HBM, CUDA-event
             timed on the stream the library launches on, max over ranks.
-  e2e       the same work through the reference-facing call
-            h266_apply_in_loop_filters with host (pinned) buffers: per picture
-            the side-information build, H2D copies, kernels and D2H copies.
+  e2e       the same work through the public batch call
+            h266_apply_in_loop_filters_batch with host (pinned) buffers: per
+            picture the side-information build from the CU lists (worker
+            pool), H2D copies, kernels and D2H copies, pipelined over lanes.
   roofline  the SAO/ALF tile kernel (the top kernel) timed per launch with
             CUDA events inside the run, against the measured HBM copy
             bandwidth.
@@ -125,26 +126,38 @@ def bad_clocks(c):
     return bool(sm and mx and sm < 0.5 * mx and "sw_power_cap" not in c.get("reasons", []))
 
 
+def workload_config(batch: int, world: int) -> dict:
+    return {"workload": f"c2_1080p10_x{batch}", "width": WIDTH, "height": HEIGHT, "bit_depth": BITDEPTH,
+            "pictures_per_step_per_gpu": batch, "chain": "LMCS-1 -> deblock -> SAO -> ALF -> CC-ALF",
+            "parallelism": f"replicas x{world}",
+            "l2": f"inputs larger than L2 ({batch * 6.2:.0f} MB per GPU)"}
+
+
 def make_batch(rank: int, n: int):
     from oxideav_h266_b200 import workloads as W
 
     return [W.config2(2000 + 1000 * rank + i, WIDTH, HEIGHT) for i in range(n)]
 
 
-def cpu_baseline(items, threads: int):
-    """Oracle chain on `threads` host threads over a bounded sample (each
-    picture of the batch twice)."""
+def cpu_baseline(items, threads: int, min_seconds: float = 10.0):
+    """Oracle chain on `threads` host threads over a bounded sample: the batch's
+    pictures, filtered again from their unfiltered copies until at least
+    `min_seconds` of wall time have been measured."""
     import oracle
 
-    pics = [p.copy() for p, _ in items] * 2
-    fas = [f for _, f in items] * 2
+    fas = [f for _, f in items]
     oracle.lib()
-    t0 = time.perf_counter()
-    used = oracle.apply_in_loop_filters_mt(pics, fas, threads)
-    dt = time.perf_counter() - t0
-    mpx = len(pics) * WIDTH * HEIGHT / 1e6
+    dt, n_pics, used = 0.0, 0, threads
+    while dt < min_seconds:
+        pics = [p.copy() for p, _ in items]
+        t0 = time.perf_counter()
+        used = oracle.apply_in_loop_filters_mt(pics, fas, threads)
+        dt += time.perf_counter() - t0
+        n_pics += len(pics)
+    mpx = n_pics * WIDTH * HEIGHT / 1e6
     return {"value": round(mpx / dt, 2), "unit": "Mpx/s", "cores": used, "kind": "port",
-            "sample": f"{len(pics)} pictures 1920x1080 10-bit (chain), one per thread, {dt:.1f} s wall"}
+            "sample": f"{n_pics} pictures 1920x1080 10-bit (chain; the step's {len(items)} pictures repeated), "
+                      f"one picture per thread, {dt:.1f} s wall"}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -263,7 +276,7 @@ def run_ours(args, rank, world, local_rank):
 
     cpu = None
     if rank == 0 and world == 1:
-        cpu = cpu_baseline(items[:16], os.cpu_count() or 1)
+        cpu = cpu_baseline(items, os.cpu_count() or 1)
 
     for pl in plans:
         pl.close()
@@ -272,10 +285,7 @@ def run_ours(args, rank, world, local_rank):
             "metric": METRIC, "value": round(value, 2), "unit": "Mpx/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic (seeded 1080p config generator)",
-            "config": {"workload": f"c2_1080p10_x{args.batch}", "width": WIDTH, "height": HEIGHT,
-                       "bit_depth": BITDEPTH, "pictures_per_step_per_gpu": args.batch,
-                       "chain": "LMCS-1 -> deblock -> SAO -> ALF -> CC-ALF", "parallelism": f"replicas x{world}",
-                       "l2": f"inputs larger than L2 ({args.batch * 6.2:.0f} MB per GPU)"},
+            "config": workload_config(args.batch, world),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clocks,
         }
@@ -294,7 +304,7 @@ def run_reference(args, rank, world):
     import oracle
 
     threads = os.cpu_count() or 1
-    per_step = max(threads, 4)
+    per_step = args.batch  # the same pictures per step as the GPU arm
     items = make_batch(0, per_step)
     oracle.lib()
     times = []
@@ -311,10 +321,11 @@ def run_reference(args, rank, world):
         "metric": METRIC, "value": round(value, 2), "unit": "Mpx/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total / len(times) * 1e3, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic (seeded 1080p config generator)",
-        "config": {"workload": f"c2_1080p10_x{per_step}", "width": WIDTH, "height": HEIGHT, "bit_depth": BITDEPTH},
+        "config": workload_config(per_step, world),
         "impl": "reference",
         "cpu_baseline": {"value": round(value, 2), "unit": "Mpx/s", "cores": threads, "kind": "port",
-                         "sample": f"{per_step} pictures per step, one per thread"},
+                         "sample": f"{per_step} pictures 1920x1080 10-bit per step, one picture per thread, "
+                                   f"{len(times)} timed steps"},
         "e2e": {"value": round(value, 2), "unit": "Mpx/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -323,7 +334,7 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])

@@ -138,19 +138,7 @@ struct h266_ctx {
   double prof_ms[H266_PROF_FAMILIES] = {0};
   uint64_t prof_n[H266_PROF_FAMILIES] = {0};
   bool force_scalar = false;  // H266_FORCE_SCALAR_ALF=1: scalar SAO/ALF kernel (cross-checks)
-};
-
-// A chain whose side information is resident on the device (h266_chain_plan_create).
-struct h266_chain_plan {
-  int device = 0;
-  h266_picture geom{};  // plane sizes / bit depths the plan was built for
-  h266::DevBuf side, lut, scratch[3];
-  bool lmcs = false, pass2 = false;
-  int deblock_bd = 8;
-  uint32_t n_comp[2] = {0, 0};
-  size_t off_seg[2] = {0, 0}, off_comp[2] = {0, 0}, off_ctb = 0, off_tab = 0, off_pack = 0;
-  h266::Pass2Args args{};
-  bool do_sao = false, do_alf = false, packed = false;
+  bool force_global_deblock = false;  // H266_FORCE_GLOBAL_DEBLOCK=1: deblocking on global memory (cross-checks)
 };
 
 namespace {
@@ -550,15 +538,28 @@ int build_pass2(const h266_picture &pic, const Pass2Inputs &in, Pass2Host &h) {
 
 // Side information of one call, assembled into one host blob and uploaded once.
 struct Staged {
-  size_t ctb = 0, tab = 0, pack = 0, seg[2] = {0, 0}, comp[2] = {0, 0};
+  size_t ctb = 0, tab = 0, pack = 0, seg[2] = {0, 0}, comp[2] = {0, 0}, band[2] = {0, 0};
   uint8_t *base = nullptr;
 };
 
-void stage_deblock(const DeblockPlan &pl, std::vector<uint8_t> &b, Staged &st) {
+// Sizes of the staged deblocking plan.
+struct DbSide {
+  uint32_t n_comp[2] = {0, 0};
+  uint32_t band_off[2][3] = {{0, 0, 0}, {0, 0, 0}};
+  uint32_t n_bands[2][3] = {{0, 0, 0}, {0, 0, 0}};
+};
+
+void stage_deblock(const DeblockPlan &pl, std::vector<uint8_t> &b, Staged &st, DbSide &db) {
   Blob blob{b};
   for (int d = 0; d < 2; ++d) {
     st.seg[d] = blob.put(pl.segs[d].data(), pl.segs[d].size() * sizeof(EdgeSeg));
     st.comp[d] = blob.put(pl.comp[d].data(), pl.comp[d].size() * sizeof(uint32_t));
+    st.band[d] = blob.put(pl.band_first[d].data(), pl.band_first[d].size() * sizeof(uint32_t));
+    db.n_comp[d] = (uint32_t)pl.comp[d].size() - 1;
+    for (int p = 0; p < 3; ++p) {
+      db.band_off[d][p] = pl.band_off[d][p];
+      db.n_bands[d][p] = pl.n_bands[d][p];
+    }
   }
 }
 
@@ -594,13 +595,32 @@ int ensure_scratch(Lane &ln, const DPlane p[3], DPlane s[3]) {
   return H266_OK;
 }
 
-int run_deblock(h266_ctx *ctx, cudaStream_t stream, const uint8_t *base, const size_t off_seg[2],
-                const size_t off_comp[2], const uint32_t n_comp[2], const DPlane planes[3], int bd) {
+int plane_map(h266_ctx *ctx, cudaStream_t stream, DPlane dst, DPlane src, const uint16_t *lut);
+
+// Deblocking of the planes `src` into `dst` (the same planes for in-place
+// filtering), luma mapped through the LMCS LUT `lut` first when given: the
+// shared-memory strip kernels when the planes fit them, else plane copies and
+// one thread per component on global memory.
+int run_deblock(h266_ctx *ctx, cudaStream_t stream, const uint8_t *base, const Staged &st, const DbSide &db,
+                const DPlane src[3], const DPlane dst[3], const uint16_t *lut, int bd) {
+  if (!ctx->force_global_deblock && deblock_strips_fit(dst)) {
+    Prof pf(ctx, stream, H266_PROF_DEBLOCK);
+    const StripSide v{reinterpret_cast<const EdgeSeg *>(base + st.seg[0]),
+                      reinterpret_cast<const uint32_t *>(base + st.comp[0]),
+                      reinterpret_cast<const uint32_t *>(base + st.band[0])};
+    const StripSide h{reinterpret_cast<const EdgeSeg *>(base + st.seg[1]),
+                      reinterpret_cast<const uint32_t *>(base + st.comp[1]),
+                      reinterpret_cast<const uint32_t *>(base + st.band[1])};
+    return launch_deblock_strips(stream, src, dst, lut, bd, v, h, db.band_off, db.n_bands, &ctx->launches);
+  }
+  for (int i = 0; i < 3; ++i)
+    if (src[i].s != dst[i].s || (i == 0 && lut))
+      H266_TRY(plane_map(ctx, stream, dst[i], src[i], i == 0 ? lut : nullptr));
   Prof pf(ctx, stream, H266_PROF_DEBLOCK);
-  return launch_deblock(stream, planes, bd, reinterpret_cast<const EdgeSeg *>(base + off_seg[0]),
-                        reinterpret_cast<const uint32_t *>(base + off_comp[0]), n_comp[0],
-                        reinterpret_cast<const EdgeSeg *>(base + off_seg[1]),
-                        reinterpret_cast<const uint32_t *>(base + off_comp[1]), n_comp[1], &ctx->launches);
+  return launch_deblock(stream, dst, bd, reinterpret_cast<const EdgeSeg *>(base + st.seg[0]),
+                        reinterpret_cast<const uint32_t *>(base + st.comp[0]), db.n_comp[0],
+                        reinterpret_cast<const EdgeSeg *>(base + st.seg[1]),
+                        reinterpret_cast<const uint32_t *>(base + st.comp[1]), db.n_comp[1], &ctx->launches);
 }
 
 int plane_map(h266_ctx *ctx, cudaStream_t stream, DPlane dst, DPlane src, const uint16_t *lut) {
@@ -631,9 +651,22 @@ struct h266::Prep {
   std::vector<uint8_t> blob;
   Pass2Host h;
   Staged st;
-  uint32_t n_comp[2] = {0, 0};
+  DbSide db;
   int rc = H266_OK;
   std::string msg;
+};
+
+// A chain whose side information is resident on the device (h266_chain_plan_create).
+struct h266_chain_plan {
+  int device = 0;
+  h266_picture geom{};  // plane sizes / bit depths the plan was built for
+  h266::DevBuf side, lut, scratch[3];
+  bool lmcs = false, pass2 = false;
+  int deblock_bd = 8;
+  Staged st;  // section offsets inside `side` (base unset)
+  DbSide db;
+  h266::Pass2Args args{};
+  bool do_sao = false, do_alf = false, packed = false;
 };
 
 namespace {
@@ -659,22 +692,17 @@ int prepare_chain(Prep &pr, const h266_picture &pic, const h266_in_loop_filter_a
   in.n_rows = a.n_clip_rows;
   H266_TRY(build_pass2(pic, in, pr.h));
   pr.blob.clear();
-  stage_deblock(pr.plan, pr.blob, pr.st);
+  stage_deblock(pr.plan, pr.blob, pr.st, pr.db);
   if (pr.h.do_sao || pr.h.do_alf) stage_pass2(pr.h, pr.blob, pr.st);
-  for (int d = 0; d < 2; ++d) pr.n_comp[d] = (uint32_t)pr.plan.comp[d].size() - 1;
   return H266_OK;
 }
 
 // Launches the chain: LMCS (LUT already built) -> deblock -> SAO/ALF.  With a
 // pass 2 the deblocked planes go to the scratch planes S, else in place.
-int exec_chain(h266_ctx *ctx, cudaStream_t stream, const uint8_t *base, const Staged &st, const uint32_t n_comp[2],
+int exec_chain(h266_ctx *ctx, cudaStream_t stream, const uint8_t *base, const Staged &st, const DbSide &db,
                const Pass2Host &h, const uint16_t *lut, int dbd, const DPlane P[3], const DPlane S[3]) {
-  if (!h.do_sao && !h.do_alf) {
-    if (lut) H266_TRY(plane_map(ctx, stream, P[0], P[0], lut));
-    return run_deblock(ctx, stream, base, st.seg, st.comp, n_comp, P, dbd);
-  }
-  for (int i = 0; i < 3; ++i) H266_TRY(plane_map(ctx, stream, S[i], P[i], i == 0 ? lut : nullptr));
-  H266_TRY(run_deblock(ctx, stream, base, st.seg, st.comp, n_comp, S, dbd));
+  if (!h.do_sao && !h.do_alf) return run_deblock(ctx, stream, base, st, db, P, P, lut, dbd);
+  H266_TRY(run_deblock(ctx, stream, base, st, db, P, S, lut, dbd));
   return run_pass2(ctx, stream, h.args, h.do_sao, h.do_alf, h.packed, base, st, S, P);
 }
 
@@ -690,7 +718,7 @@ int issue_chain(h266_ctx *ctx, Lane &ln, Prep &pr, const DPlane P[3], const h266
   }
   DPlane S[3];
   if (pr.h.do_sao || pr.h.do_alf) H266_TRY(ensure_scratch(ln, P, S));
-  return exec_chain(ctx, ln.stream, pr.st.base, pr.st, pr.n_comp, pr.h, lut, (int)a.deblock.bit_depth, P, S);
+  return exec_chain(ctx, ln.stream, pr.st.base, pr.st, pr.db, pr.h, lut, (int)a.deblock.bit_depth, P, S);
 }
 
 // Worker pool of the context (created on first use): as many threads as the
@@ -758,6 +786,8 @@ int h266_ctx_create(int device, h266_ctx **out) {
   }
   const char *fs = std::getenv("H266_FORCE_SCALAR_ALF");
   c->force_scalar = fs && fs[0] == '1';
+  const char *fg = std::getenv("H266_FORCE_GLOBAL_DEBLOCK");
+  c->force_global_deblock = fg && fg[0] == '1';
   *out = c;
   return H266_OK;
 }
@@ -836,11 +866,11 @@ int h266_apply_deblocking_clipped(h266_ctx *ctx, h266_picture *pic, const h266_d
   DPlane P[3];
   H266_TRY(picture_to_device(ln, *pic, P));
   Staged st;
+  DbSide db;
   pr.blob.clear();
-  stage_deblock(pr.plan, pr.blob, st);
+  stage_deblock(pr.plan, pr.blob, st, db);
   H266_TRY(upload_blob(ln, pr.blob, &st.base));
-  const uint32_t n_comp[2] = {(uint32_t)pr.plan.comp[0].size() - 1, (uint32_t)pr.plan.comp[1].size() - 1};
-  H266_TRY(run_deblock(ctx, ln.stream, st.base, st.seg, st.comp, n_comp, P, (int)params->bit_depth));
+  H266_TRY(run_deblock(ctx, ln.stream, st.base, st, db, P, P, nullptr, (int)params->bit_depth));
   return picture_from_device(ln, *pic);
 }
 
@@ -1041,14 +1071,9 @@ int h266_chain_plan_create(h266_ctx *ctx, const h266_picture *pic, const h266_in
         return fail(rc);
   }
   pl->deblock_bd = (int)args->deblock.bit_depth;
-  for (int d = 0; d < 2; ++d) {
-    pl->n_comp[d] = pr.n_comp[d];
-    pl->off_seg[d] = pr.st.seg[d];
-    pl->off_comp[d] = pr.st.comp[d];
-  }
-  pl->off_ctb = pr.st.ctb;
-  pl->off_tab = pr.st.tab;
-  pl->off_pack = pr.st.pack;
+  pl->db = pr.db;
+  pl->st = pr.st;
+  pl->st.base = nullptr;
   pl->packed = pr.h.packed;
   pl->args = pr.h.args;
   pl->do_sao = pr.h.do_sao;
@@ -1071,21 +1096,14 @@ int h266_chain_plan_execute(h266_ctx *ctx, h266_chain_plan *plan, h266_picture *
   H266_TRY(picture_to_device(ctx->main, *pic, P));
   for (int i = 0; i < 3; ++i)
     S[i] = DPlane{plan->pass2 ? plan->scratch[i].as<uint16_t>() : nullptr, std::max(P[i].w, 1), P[i].w, P[i].h};
-  Staged st;
+  Staged st = plan->st;
   st.base = plan->side.as<uint8_t>();
-  for (int d = 0; d < 2; ++d) {
-    st.seg[d] = plan->off_seg[d];
-    st.comp[d] = plan->off_comp[d];
-  }
-  st.ctb = plan->off_ctb;
-  st.tab = plan->off_tab;
-  st.pack = plan->off_pack;
   Pass2Host h;
   h.args = plan->args;
   h.do_sao = plan->do_sao;
   h.do_alf = plan->do_alf;
   h.packed = plan->packed;
-  return exec_chain(ctx, ctx->stream, st.base, st, plan->n_comp, h, plan->lmcs ? plan->lut.as<uint16_t>() : nullptr,
+  return exec_chain(ctx, ctx->stream, st.base, st, plan->db, h, plan->lmcs ? plan->lut.as<uint16_t>() : nullptr,
                     plan->deblock_bd, P, S);
 }
 
@@ -1189,5 +1207,5 @@ extern "C" int h266_apply_in_loop_filters_noalloc(h266_picture *pic, const h266_
     S[i] = DPlane{reinterpret_cast<uint16_t *>(scratch + plane_off[i]), std::max<int>((int)pl[i]->width, 1),
                   (int)pl[i]->width, (int)pl[i]->height};
   }
-  return exec_chain(&local, local.stream, scratch, pr.st, pr.n_comp, pr.h, lut, (int)args->deblock.bit_depth, P, S);
+  return exec_chain(&local, local.stream, scratch, pr.st, pr.db, pr.h, lut, (int)args->deblock.bit_depth, P, S);
 }

@@ -365,6 +365,32 @@ void group(const std::vector<Emitted> &segs, std::vector<EdgeSeg> &dst, std::vec
   max_len = longest;
 }
 
+// Fills the band index of both passes from the component lists.
+void index_bands(const h266_picture &pic, DeblockPlan &plan) {
+  const h266_plane *pl[3] = {&pic.luma, &pic.cb, &pic.cr};
+  for (int d = 0; d < 2; ++d) {
+    std::vector<uint32_t> &bf = plan.band_first[d];
+    bf.clear();
+    const std::vector<uint32_t> &comp = plan.comp[d];
+    const std::vector<EdgeSeg> &segs = plan.segs[d];
+    const uint32_t n_comp = (uint32_t)comp.size() - 1;
+    uint32_t c = 0;
+    for (int p = 0; p < 3; ++p) {
+      const uint32_t unit = p ? 2 : 4;
+      const uint32_t dim = d == 0 ? pl[p]->height : pl[p]->width;
+      const uint32_t nb = (uint64_t)pl[p]->width * pl[p]->height ? (dim + unit - 1) / unit : 0;
+      plan.band_off[d][p] = (uint32_t)bf.size();
+      plan.n_bands[d][p] = nb;
+      // components of plane p are contiguous, sorted by band coordinate
+      for (uint32_t b = 0; b <= nb; ++b) {
+        while (c < n_comp && segs[comp[c]].plane == p && (d == 0 ? segs[comp[c]].y : segs[comp[c]].x) / unit < b) ++c;
+        bf.push_back(c);
+      }
+      while (c < n_comp && segs[comp[c]].plane == p) ++c;  // bands beyond the plane
+    }
+  }
+}
+
 }  // namespace
 
 int build_deblock_plan(const h266_picture &pic, const h266_deblock_cu *cus, uint64_t n_cus,
@@ -376,7 +402,10 @@ int build_deblock_plan(const h266_picture &pic, const h266_deblock_cu *cus, uint
     plan.comp[d].assign(1, 0);  // component offsets end with the total count
     plan.max_comp_len[d] = 0;
   }
-  if (params.disabled) return H266_OK;
+  if (params.disabled) {
+    index_bands(pic, plan);
+    return H266_OK;
+  }
   for (int d = 0; d < 2; ++d) plan.comp[d].clear();
   if (params.bit_depth < 8 || params.bit_depth > 16)
     return set_error(H266_ERR_INVALID_ARGUMENT, "deblock: bit_depth must be 8..16");
@@ -445,99 +474,152 @@ int build_deblock_plan(const h266_picture &pic, const h266_deblock_cu *cus, uint
     }
     plan.comp[d].push_back((uint32_t)plan.segs[d].size());
   }
+  index_bands(pic, plan);
   return H266_OK;
 }
 
 // ===================================================================== device
 namespace {
 
-__device__ __forceinline__ int rdc(const DPlane &p, int x, int y) {
-  x = min(max(x, 0), p.w - 1);
-  y = min(max(y, 0), p.h - 1);
-  return p.s[(int64_t)y * p.stride + x];
+// Sample access of the segment filters: reads clamp into the plane (the
+// reference's clamped `sample()`), writes outside the plane are dropped and
+// written values are Clip1'd.
+struct GlobalView {  // a plane in global memory
+  DPlane p;
+  __host__ __device__ __forceinline__ int rd(int x, int y) const {
+    x = min(max(x, 0), p.w - 1);
+    y = min(max(y, 0), p.h - 1);
+    return p.s[(int64_t)y * p.stride + x];
+  }
+  __host__ __device__ __forceinline__ void wr(int x, int y, int v, int maxv) const {
+    if (x < 0 || y < 0 || x >= p.w || y >= p.h) return;
+    p.s[(int64_t)y * p.stride + x] = (uint16_t)min(max(v, 0), maxv);
+  }
+};
+
+// A window of a plane staged in shared memory: columns [ox, ox + ww) and rows
+// [oy, oy + wh) of a w x h plane, `ld` samples per row.  Every clamped
+// coordinate a segment of the window's bands touches lies inside the window
+// (bands are whole rows / full-height column strips); the window clamp below
+// only keeps shared-memory accesses in bounds whatever the input.
+struct SharedView {
+  uint16_t *s;
+  int ld, ox, oy, ww, wh, w, h;
+  __host__ __device__ __forceinline__ int rd(int x, int y) const {
+    x = min(max(min(max(x, 0), w - 1), ox), ox + ww - 1);
+    y = min(max(min(max(y, 0), h - 1), oy), oy + wh - 1);
+    return s[(y - oy) * ld + (x - ox)];
+  }
+  __host__ __device__ __forceinline__ void wr(int x, int y, int v, int maxv) const {
+    if (x < 0 || y < 0 || x >= w || y >= h) return;
+    if (x < ox || y < oy || x >= ox + ww || y >= oy + wh) return;
+    s[(y - oy) * ld + (x - ox)] = (uint16_t)min(max(v, 0), maxv);
+  }
+};
+
+__host__ __device__ __forceinline__ int clampd(int v, int lo, int hi) { return min(max(v, lo), hi); }
+
+// Long-filter weights of eqs. 1395-1408 as closed forms of the tables
+// F7 = {59, 50, 41, 32, 23, 14, 5}, F5 = {58, 45, 32, 19, 6}, F3 = {53, 32, 11}
+// and T7 = {6, 5, 4, 3, 2, 1, 1}, T5 = {6, 5, 4, 3, 2}, T3 = {6, 4, 2}, so that
+// a fully unrolled filter needs no indexed table.
+__host__ __device__ __forceinline__ int long_f(int m, int i) {
+  return m == 7 ? 59 - 9 * i : (m == 5 ? 58 - 13 * i : 53 - 21 * i);
 }
-__device__ __forceinline__ void wrc(const DPlane &p, int x, int y, int v, int maxv) {
-  if (x < 0 || y < 0 || x >= p.w || y >= p.h) return;
-  p.s[(int64_t)y * p.stride + x] = (uint16_t)min(max(v, 0), maxv);
+__host__ __device__ __forceinline__ int long_t(int m, int i) {
+  return m == 7 ? (i < 6 ? 6 - i : 1) : (m == 5 ? 6 - i : 6 - 2 * i);
 }
-__device__ __forceinline__ int clampd(int v, int lo, int hi) { return min(max(v, lo), hi); }
 
 // One luma edge segment: §8.8.3.6.2 decision + §8.8.3.6.7 / .8 filters
 // (luma_edge_decision / run_luma_filter / short_luma_apply / long_luma_apply,
 // src/deblock.rs:1224-1776).  The decision reads lines 0 and 3 before any
-// write and every line is filtered from its own samples, so the four lines
-// are loaded once: v[k][8 + d] holds the sample at distance d from q0.
-__device__ void luma_segment(const DPlane &P, const EdgeSeg &e, int maxv) {
+// write; every line is then filtered from its own samples and written back
+// before the next line is read (lines are disjoint; a line clamped onto
+// another one lies outside the plane, so its writes are dropped).  Every
+// array index is a compile-time constant after unrolling, so the samples stay
+// in registers.
+template <class View>
+__host__ __device__ void luma_segment(const View &P, const EdgeSeg &e, int maxv) {
   const bool vert = e.flags & 1;
   const int tc = e.tc, beta = e.beta;
   int mp = e.mfl >> 4, mq = e.mfl & 15;
   const int cx = e.x, cy = e.y;
-  int v[4][16];
+  const bool plt_p = e.flags & 4, plt_q = e.flags & 8;
+  // l0[8 + d], l3[8 + d]: lines 0 and 3 at distance d from q0
+  int l0[16], l3[16];
 #pragma unroll
-  for (int k = 0; k < 4; ++k)
-#pragma unroll
-    for (int d = -8; d < 8; ++d) v[k][8 + d] = vert ? rdc(P, cx + d, cy + k) : rdc(P, cx + k, cy + d);
-#define PS(i, k) v[k][7 - (i)]
-#define QS(j, k) v[k][8 + (j)]
-  const int dp0 = abs(PS(2, 0) - 2 * PS(1, 0) + PS(0, 0)), dp3 = abs(PS(2, 3) - 2 * PS(1, 3) + PS(0, 3));
-  const int dq0 = abs(QS(2, 0) - 2 * QS(1, 0) + QS(0, 0)), dq3 = abs(QS(2, 3) - 2 * QS(1, 3) + QS(0, 3));
-  const int sp0 = abs(PS(3, 0) - PS(0, 0)), sq0 = abs(QS(0, 0) - QS(3, 0)), spq0 = abs(PS(0, 0) - QS(0, 0));
-  const int sp3 = abs(PS(3, 3) - PS(0, 3)), sq3 = abs(QS(0, 3) - QS(3, 3)), spq3 = abs(PS(0, 3) - QS(0, 3));
+  for (int d = -8; d < 8; ++d) {
+    l0[8 + d] = vert ? P.rd(cx + d, cy) : P.rd(cx, cy + d);
+    l3[8 + d] = vert ? P.rd(cx + d, cy + 3) : P.rd(cx + 3, cy + d);
+  }
+#define P0(i) l0[7 - (i)]
+#define Q0(j) l0[8 + (j)]
+#define P3(i) l3[7 - (i)]
+#define Q3(j) l3[8 + (j)]
+  const int dp0 = abs(P0(2) - 2 * P0(1) + P0(0)), dp3 = abs(P3(2) - 2 * P3(1) + P3(0));
+  const int dq0 = abs(Q0(2) - 2 * Q0(1) + Q0(0)), dq3 = abs(Q3(2) - 2 * Q3(1) + Q3(0));
+  const int sp0 = abs(P0(3) - P0(0)), sq0 = abs(Q0(0) - Q0(3)), spq0 = abs(P0(0) - Q0(0));
+  const int sp3 = abs(P3(3) - P3(0)), sq3 = abs(Q3(0) - Q3(3)), spq3 = abs(P3(0) - Q3(0));
   const int tc_gate = (5 * tc + 1) >> 1;
-  bool p_large = mp > 3 && !(e.flags & 2);
+  const bool p_large = mp > 3 && !(e.flags & 2);
   const bool q_large = mq > 3;
   bool long_ok = false;
   if (p_large || q_large) {
     int dp0l = dp0, dp3l = dp3, dq0l = dq0, dq3l = dq3;
     if (p_large) {
-      dp0l = (dp0 + abs(PS(5, 0) - 2 * PS(4, 0) + PS(3, 0)) + 1) >> 1;
-      dp3l = (dp3 + abs(PS(5, 3) - 2 * PS(4, 3) + PS(3, 3)) + 1) >> 1;
+      dp0l = (dp0 + abs(P0(5) - 2 * P0(4) + P0(3)) + 1) >> 1;
+      dp3l = (dp3 + abs(P3(5) - 2 * P3(4) + P3(3)) + 1) >> 1;
     } else {
       mp = 3;
     }
     if (q_large) {
-      dq0l = (dq0 + abs(QS(5, 0) - 2 * QS(4, 0) + QS(3, 0)) + 1) >> 1;
-      dq3l = (dq3 + abs(QS(5, 3) - 2 * QS(4, 3) + QS(3, 3)) + 1) >> 1;
+      dq0l = (dq0 + abs(Q0(5) - 2 * Q0(4) + Q0(3)) + 1) >> 1;
+      dq3l = (dq3 + abs(Q3(5) - 2 * Q3(4) + Q3(3)) + 1) >> 1;
     }
     int sp0l = sp0, sp3l = sp3, sq0l = sq0, sq3l = sq3;
     if (mp == 7) {
-      sp0l += abs(PS(7, 0) - PS(6, 0) - PS(5, 0) + PS(4, 0));
-      sp3l += abs(PS(7, 3) - PS(6, 3) - PS(5, 3) + PS(4, 3));
+      sp0l += abs(P0(7) - P0(6) - P0(5) + P0(4));
+      sp3l += abs(P3(7) - P3(6) - P3(5) + P3(4));
     }
     if (mq == 7) {
-      sq0l += abs(QS(4, 0) - QS(5, 0) - QS(6, 0) + QS(7, 0));
-      sq3l += abs(QS(4, 3) - QS(5, 3) - QS(6, 3) + QS(7, 3));
+      sq0l += abs(Q0(4) - Q0(5) - Q0(6) + Q0(7));
+      sq3l += abs(Q3(4) - Q3(5) - Q3(6) + Q3(7));
     }
     if ((dp0l + dq0l) + (dp3l + dq3l) < beta) {
       const int t1 = (3 * beta) >> 5, t2 = beta >> 4;
-      bool ok = true;
-#pragma unroll
-      for (int r = 0; r < 2; ++r) {
-        const int k = r ? 3 : 0;
-        const int dpq = r ? dp3l + dq3l : dp0l + dq0l;
-        int spl = r ? sp3l : sp0l, sql = r ? sq3l : sq0l;
-        if (p_large) spl = (spl + abs(PS(3, k) - PS(mp, k)) + 1) >> 1;
-        if (q_large) sql = (sql + abs(QS(3, k) - QS(mq, k)) + 1) >> 1;
-        ok = ok && 2 * dpq < t2 && spl + sql < t1 && (r ? spq3 : spq0) < tc_gate;
+      // P(mp) / Q(mq) of lines 0 and 3 (mp, mq in {3, 5, 7})
+      const int pm0 = mp == 7 ? P0(7) : (mp == 5 ? P0(5) : P0(3)), pm3 = mp == 7 ? P3(7) : (mp == 5 ? P3(5) : P3(3));
+      const int qm0 = mq == 7 ? Q0(7) : (mq == 5 ? Q0(5) : Q0(3)), qm3 = mq == 7 ? Q3(7) : (mq == 5 ? Q3(5) : Q3(3));
+      int spl0 = sp0l, sql0 = sq0l, spl3 = sp3l, sql3 = sq3l;
+      if (p_large) {
+        spl0 = (spl0 + abs(P0(3) - pm0) + 1) >> 1;
+        spl3 = (spl3 + abs(P3(3) - pm3) + 1) >> 1;
       }
-      long_ok = ok;
+      if (q_large) {
+        sql0 = (sql0 + abs(Q0(3) - qm0) + 1) >> 1;
+        sql3 = (sql3 + abs(Q3(3) - qm3) + 1) >> 1;
+      }
+      long_ok = 2 * (dp0l + dq0l) < t2 && spl0 + sql0 < t1 && spq0 < tc_gate && 2 * (dp3l + dq3l) < t2 &&
+                spl3 + sql3 < t1 && spq3 < tc_gate;
     }
   }
-  int wp = 0, wq = 0;  // samples written on each side of every line
-  const bool plt_p = e.flags & 4, plt_q = e.flags & 8;
+#undef P0
+#undef Q0
+#undef P3
+#undef Q3
   if (long_ok) {
-    // refMiddle per (mflP, mflQ), eqs. 1389-1394; refP / refQ eqs. 1395-1396
-    const int F7[7] = {59, 50, 41, 32, 23, 14, 5}, F5[5] = {58, 45, 32, 19, 6}, F3[3] = {53, 32, 11};
-    const int T7[7] = {6, 5, 4, 3, 2, 1, 1}, T5[5] = {6, 5, 4, 3, 2}, T3[3] = {6, 4, 2};
-    const int *fp = mp == 7 ? F7 : (mp == 5 ? F5 : F3), *tp = mp == 7 ? T7 : (mp == 5 ? T5 : T3);
-    const int *fq = mq == 7 ? F7 : (mq == 5 ? F5 : F3), *tq = mq == 7 ? T7 : (mq == 5 ? T5 : T3);
+#pragma unroll
     for (int k = 0; k < 4; ++k) {
+      // p[i], q[j]: line k; entries beyond mflP / mflQ are zero as in the reference's arrays
       int p[8], q[8];
-      for (int i = 0; i < 8; ++i) {  // unread entries are zero in the reference's arrays
-        p[i] = i <= mp ? PS(i, k) : 0;
-        q[i] = i <= mq ? QS(i, k) : 0;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int pi = k == 0 ? l0[7 - i] : (k == 3 ? l3[7 - i] : (vert ? P.rd(cx - 1 - i, cy + k) : P.rd(cx + k, cy - 1 - i)));
+        const int qi = k == 0 ? l0[8 + i] : (k == 3 ? l3[8 + i] : (vert ? P.rd(cx + i, cy + k) : P.rd(cx + k, cy + i)));
+        p[i] = i <= mp ? pi : 0;
+        q[i] = i <= mq ? qi : 0;
       }
-      int mid;
+      int mid;  // refMiddle, eqs. 1389-1394
       if (mp == 5 && mq == 5)
         mid = (p[4] + p[3] + 2 * (p[2] + p[1] + p[0] + q[0] + q[1] + q[2]) + q[3] + q[4] + 8) >> 4;
       else if (mp == mq)
@@ -551,25 +633,24 @@ __device__ void luma_segment(const DPlane &P, const EdgeSeg &e, int maxv) {
         mid = (2 * (p[2] + p[1] + p[0] + q[0]) + p[0] + p[1] + q[1] + q[2] + q[3] + q[4] + q[5] + q[6] + 8) >> 4;
       else
         mid = (p[6] + p[5] + p[4] + p[3] + p[2] + p[1] + 2 * (q[2] + q[1] + q[0] + p[0]) + q[0] + q[1] + 8) >> 4;
-      const int rp = (p[mp] + p[mp - 1] + 1) >> 1, rq = (q[mq] + q[mq - 1] + 1) >> 1;
-      for (int i = 0; i < mp; ++i) {
-        const int lim = (tc * tp[i]) >> 1;
-        PS(i, k) = clampd((mid * fp[i] + rp * (64 - fp[i]) + 32) >> 6, p[i] - lim, p[i] + lim);
+      // refP / refQ, eqs. 1395-1396
+      const int rp = mp == 7 ? (p[7] + p[6] + 1) >> 1 : (mp == 5 ? (p[5] + p[4] + 1) >> 1 : (p[3] + p[2] + 1) >> 1);
+      const int rq = mq == 7 ? (q[7] + q[6] + 1) >> 1 : (mq == 5 ? (q[5] + q[4] + 1) >> 1 : (q[3] + q[2] + 1) >> 1);
+#pragma unroll
+      for (int i = 0; i < 7; ++i) {
+        if (i < mp && !plt_p) {
+          const int f = long_f(mp, i), lim = (tc * long_t(mp, i)) >> 1;
+          const int v = clampd((mid * f + rp * (64 - f) + 32) >> 6, p[i] - lim, p[i] + lim);
+          if (vert) P.wr(cx - i - 1, cy + k, v, maxv);
+          else P.wr(cx + k, cy - i - 1, v, maxv);
+        }
+        if (i < mq && !plt_q) {
+          const int f = long_f(mq, i), lim = (tc * long_t(mq, i)) >> 1;
+          const int v = clampd((mid * f + rq * (64 - f) + 32) >> 6, q[i] - lim, q[i] + lim);
+          if (vert) P.wr(cx + i, cy + k, v, maxv);
+          else P.wr(cx + k, cy + i, v, maxv);
+        }
       }
-      for (int j = 0; j < mq; ++j) {
-        const int lim = (tc * tq[j]) >> 1;
-        QS(j, k) = clampd((mid * fq[j] + rq * (64 - fq[j]) + 32) >> 6, q[j] - lim, q[j] + lim);
-      }
-    }
-    wp = plt_p ? 0 : mp;
-    wq = plt_q ? 0 : mq;
-    for (int k = 0; k < 4; ++k) {
-      for (int i = 0; i < wp; ++i)
-        if (vert) wrc(P, cx - i - 1, cy + k, PS(i, k), maxv);
-        else wrc(P, cx + k, cy - i - 1, PS(i, k), maxv);
-      for (int j = 0; j < wq; ++j)
-        if (vert) wrc(P, cx + j, cy + k, QS(j, k), maxv);
-        else wrc(P, cx + k, cy + j, QS(j, k), maxv);
     }
     return;
   }
@@ -585,52 +666,61 @@ __device__ void luma_segment(const DPlane &P, const EdgeSeg &e, int maxv) {
   const int side_gate = (beta + (beta >> 1)) >> 3;
   const bool dep = mp > 1 && mq > 1 && dp0 + dp3 < side_gate;
   const bool deq = mp > 1 && mq > 1 && dq0 + dq3 < side_gate;
+#pragma unroll
   for (int k = 0; k < 4; ++k) {
-    const int p3 = PS(3, k), p2 = PS(2, k), p1 = PS(1, k), p0 = PS(0, k);
-    const int q0 = QS(0, k), q1 = QS(1, k), q2 = QS(2, k), q3 = QS(3, k);
+    int s[8];  // p3 p2 p1 p0 q0 q1 q2 q3 of line k
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      s[t] = k == 0 ? l0[4 + t] : (k == 3 ? l3[4 + t] : (vert ? P.rd(cx - 4 + t, cy + k) : P.rd(cx + k, cy - 4 + t)));
+    const int p3 = s[0], p2 = s[1], p1 = s[2], p0 = s[3], q0 = s[4], q1 = s[5], q2 = s[6], q3 = s[7];
     int np = 0, nq = 0;  // samples written this line, from p0 / q0 outwards
-    int out_p[3], out_q[3];
+    int op0 = 0, op1 = 0, op2 = 0, oq0 = 0, oq1 = 0, oq2 = 0;
     if (strong) {
-      out_p[0] = clampd((p2 + 2 * p1 + 2 * p0 + 2 * q0 + q1 + 4) >> 3, p0 - 3 * tc, p0 + 3 * tc);
-      out_p[1] = clampd((p2 + p1 + p0 + q0 + 2) >> 2, p1 - 2 * tc, p1 + 2 * tc);
-      out_p[2] = clampd((2 * p3 + 3 * p2 + p1 + p0 + q0 + 4) >> 3, p2 - tc, p2 + tc);
-      out_q[0] = clampd((p1 + 2 * p0 + 2 * q0 + 2 * q1 + q2 + 4) >> 3, q0 - 3 * tc, q0 + 3 * tc);
-      out_q[1] = clampd((p0 + q0 + q1 + q2 + 2) >> 2, q1 - 2 * tc, q1 + 2 * tc);
-      out_q[2] = clampd((p0 + q0 + q1 + 3 * q2 + 2 * q3 + 4) >> 3, q2 - tc, q2 + tc);
+      op0 = clampd((p2 + 2 * p1 + 2 * p0 + 2 * q0 + q1 + 4) >> 3, p0 - 3 * tc, p0 + 3 * tc);
+      op1 = clampd((p2 + p1 + p0 + q0 + 2) >> 2, p1 - 2 * tc, p1 + 2 * tc);
+      op2 = clampd((2 * p3 + 3 * p2 + p1 + p0 + q0 + 4) >> 3, p2 - tc, p2 + tc);
+      oq0 = clampd((p1 + 2 * p0 + 2 * q0 + 2 * q1 + q2 + 4) >> 3, q0 - 3 * tc, q0 + 3 * tc);
+      oq1 = clampd((p0 + q0 + q1 + q2 + 2) >> 2, q1 - 2 * tc, q1 + 2 * tc);
+      oq2 = clampd((p0 + q0 + q1 + 3 * q2 + 2 * q3 + 4) >> 3, q2 - tc, q2 + tc);
       np = nq = 3;
     } else {
       const int raw = (9 * (q0 - p0) - 3 * (q1 - p1) + 8) >> 4;
       if (abs(raw) < tc * 10) {
         const int delta = clampd(raw, -tc, tc);
-        out_p[0] = p0 + delta;
-        out_q[0] = q0 - delta;
+        op0 = p0 + delta;
+        oq0 = q0 - delta;
         np = nq = 1;
         if (dep) {
-          out_p[1] = p1 + clampd((((p2 + p0 + 1) >> 1) - p1 + delta) >> 1, -(tc >> 1), tc >> 1);
+          op1 = p1 + clampd((((p2 + p0 + 1) >> 1) - p1 + delta) >> 1, -(tc >> 1), tc >> 1);
           np = 2;
         }
         if (deq) {
-          out_q[1] = q1 + clampd((((q2 + q0 + 1) >> 1) - q1 - delta) >> 1, -(tc >> 1), tc >> 1);
+          oq1 = q1 + clampd((((q2 + q0 + 1) >> 1) - q1 - delta) >> 1, -(tc >> 1), tc >> 1);
           nq = 2;
         }
       }
     }
     if (plt_p) np = 0;
     if (plt_q) nq = 0;
-    for (int i = 0; i < np; ++i)
-      if (vert) wrc(P, cx - i - 1, cy + k, out_p[i], maxv);
-      else wrc(P, cx + k, cy - i - 1, out_p[i], maxv);
-    for (int j = 0; j < nq; ++j)
-      if (vert) wrc(P, cx + j, cy + k, out_q[j], maxv);
-      else wrc(P, cx + k, cy + j, out_q[j], maxv);
+    const int op[3] = {op0, op1, op2}, oq[3] = {oq0, oq1, oq2};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      if (i < np) {
+        if (vert) P.wr(cx - i - 1, cy + k, op[i], maxv);
+        else P.wr(cx + k, cy - i - 1, op[i], maxv);
+      }
+      if (i < nq) {
+        if (vert) P.wr(cx + i, cy + k, oq[i], maxv);
+        else P.wr(cx + k, cy + i, oq[i], maxv);
+      }
+    }
   }
-#undef PS
-#undef QS
 }
 
 // One chroma edge segment (2 lines): run_chroma_filter_v / _h with the strong
-// decision and filters of src/deblock.rs:1803-2075.
-__device__ void chroma_segment(const DPlane &P, const EdgeSeg &e, int maxv) {
+// decision and filters of src/deblock.rs:1803-2075.  Constant indices only.
+template <class View>
+__host__ __device__ void chroma_segment(const View &P, const EdgeSeg &e, int maxv) {
   const bool vert = e.flags & 1;
   const int tc = e.tc, beta = e.beta, mp = e.mfl >> 4, mq = e.mfl & 15;
   const int cx = e.x, cy = e.y;
@@ -639,7 +729,7 @@ __device__ void chroma_segment(const DPlane &P, const EdgeSeg &e, int maxv) {
 #pragma unroll
   for (int k = 0; k < 2; ++k)
 #pragma unroll
-    for (int d = -4; d < 4; ++d) v[k][4 + d] = vert ? rdc(P, cx + d, cy + k) : rdc(P, cx + k, cy + d);
+    for (int d = -4; d < 4; ++d) v[k][4 + d] = vert ? P.rd(cx + d, cy + k) : P.rd(cx + k, cy + d);
   const bool eligible = vert ? (mp == 3 && mq == 3) : (mq == 3 && (mp == 3 || mp == 1));
   const bool short_p = !vert && mp == 1;
   if (eligible) {
@@ -652,10 +742,12 @@ __device__ void chroma_segment(const DPlane &P, const EdgeSeg &e, int maxv) {
       ok = ok && dpq < (beta >> 2) && abs(p3 - p0) + abs(q0 - q3) < (beta >> 3) && abs(p0 - q0) < ((5 * tc + 1) >> 1);
     }
     if (ok) {
+#pragma unroll
       for (int k = 0; k < 2; ++k) {
         const int p3 = v[k][0], p2 = v[k][1], p1 = v[k][2], p0 = v[k][3];
         const int q0 = v[k][4], q1 = v[k][5], q2 = v[k][6], q3 = v[k][7];
-        int op[3], oq[3], np;
+        int op[3] = {0, 0, 0}, oq[3];
+        int np;
         if (short_p) {
           op[0] = clampd((3 * p1 + 2 * p0 + q0 + q1 + q2 + 4) >> 3, p0 - tc, p0 + tc);
           oq[0] = clampd((2 * p1 + p0 + 2 * q0 + q1 + q2 + q3 + 4) >> 3, q0 - tc, q0 + tc);
@@ -669,28 +761,32 @@ __device__ void chroma_segment(const DPlane &P, const EdgeSeg &e, int maxv) {
         }
         oq[1] = clampd((p1 + p0 + q0 + 2 * q1 + q2 + 2 * q3 + 4) >> 3, q1 - tc, q1 + tc);
         oq[2] = clampd((p0 + q0 + q1 + 2 * q2 + 3 * q3 + 4) >> 3, q2 - tc, q2 + tc);
-        if (!plt_p)
-          for (int i = 0; i < np; ++i)
-            if (vert) wrc(P, cx - i - 1, cy + k, op[i], maxv);
-            else wrc(P, cx + k, cy - i - 1, op[i], maxv);
-        if (!plt_q)
-          for (int j = 0; j < 3; ++j)
-            if (vert) wrc(P, cx + j, cy + k, oq[j], maxv);
-            else wrc(P, cx + k, cy + j, oq[j], maxv);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          if (!plt_p && i < np) {
+            if (vert) P.wr(cx - i - 1, cy + k, op[i], maxv);
+            else P.wr(cx + k, cy - i - 1, op[i], maxv);
+          }
+          if (!plt_q) {
+            if (vert) P.wr(cx + i, cy + k, oq[i], maxv);
+            else P.wr(cx + k, cy + i, oq[i], maxv);
+          }
+        }
       }
       return;
     }
   }
+#pragma unroll
   for (int k = 0; k < 2; ++k) {  // weak filter, eqs. 1421-1423
     const int p1 = v[k][2], p0 = v[k][3], q0 = v[k][4], q1 = v[k][5];
     const int delta = clampd(((q0 - p0) * 4 + p1 - q1 + 4) >> 3, -tc, tc);
     if (!plt_p) {
-      if (vert) wrc(P, cx - 1, cy + k, p0 + delta, maxv);
-      else wrc(P, cx + k, cy - 1, p0 + delta, maxv);
+      if (vert) P.wr(cx - 1, cy + k, p0 + delta, maxv);
+      else P.wr(cx + k, cy - 1, p0 + delta, maxv);
     }
     if (!plt_q) {
-      if (vert) wrc(P, cx, cy + k, q0 - delta, maxv);
-      else wrc(P, cx + k, cy, q0 - delta, maxv);
+      if (vert) P.wr(cx, cy + k, q0 - delta, maxv);
+      else P.wr(cx + k, cy, q0 - delta, maxv);
     }
   }
 }
@@ -699,6 +795,7 @@ struct Planes3 {
   DPlane p[3];
 };
 
+// Global-memory deblocking: one thread per component.
 __global__ void __launch_bounds__(128) k_deblock_components(Planes3 planes, const EdgeSeg *__restrict__ segs,
                                                             const uint32_t *__restrict__ comp, uint32_t n_comp,
                                                             int maxv) {
@@ -707,12 +804,213 @@ __global__ void __launch_bounds__(128) k_deblock_components(Planes3 planes, cons
   const uint32_t b = comp[c], e = comp[c + 1];
   for (uint32_t i = b; i < e; ++i) {
     const EdgeSeg s = segs[i];
-    if (s.plane == 0) luma_segment(planes.p[0], s, maxv);
-    else chroma_segment(planes.p[s.plane], s, maxv);
+    if (s.plane == 0) luma_segment(GlobalView{planes.p[0]}, s, maxv);
+    else chroma_segment(GlobalView{planes.p[s.plane]}, s, maxv);
   }
 }
 
+// ------------------------------------------------------------ strip kernels
+// Every vertical-pass component lies in one band of 4 luma / 2 chroma rows
+// (its segments share the band) and every horizontal-pass component in one
+// band of 4 / 2 columns, so a CTA that holds whole rows (vertical pass) or a
+// full-height column strip (horizontal pass) in shared memory runs its
+// components without touching samples of other CTAs.  All clamped reads of a
+// segment stay inside the staged window: rows clamp into the plane, whose
+// whole width (rows kernel) or height (columns kernel) is staged.
+constexpr int kStripCols = 16;             // columns per horizontal-pass CTA
+constexpr int kMaxStripSmem = 200 * 1024;  // dynamic shared memory per CTA
+
+struct StripParams {
+  DPlane src[3], dst[3];
+  EdgeSeg const *segs;
+  uint32_t const *comp;
+  uint32_t const *band_first;
+  uint32_t band_off[3];
+  uint32_t n_bands[3];
+  uint32_t ctas[3];  // CTAs per plane
+  const uint16_t *lut;
+  int maxv;
+};
+
+__device__ __forceinline__ bool vec_ok(const DPlane &p) { return ((uintptr_t)p.s & 15) == 0 && (p.stride & 7) == 0; }
+
+__device__ __forceinline__ int plane_of(const StripParams &a, int &bid) {
+  int plane = 0;
+  while (plane < 2 && bid >= (int)a.ctas[plane]) {
+    bid -= (int)a.ctas[plane];
+    ++plane;
+  }
+  return plane;
+}
+
+__device__ __forceinline__ void run_components(const StripParams &a, const SharedView &v, int plane, uint32_t c0,
+                                               uint32_t c1) {
+  for (uint32_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+    const uint32_t e = a.comp[c + 1];
+    for (uint32_t i = a.comp[c]; i < e; ++i) {
+      const EdgeSeg s = a.segs[i];
+      if (plane == 0) luma_segment(v, s, a.maxv);
+      else chroma_segment(v, s, a.maxv);
+    }
+  }
+}
+
+// Vertical pass: one CTA per band of rows, all planes in one grid.  Loads the
+// rows from src (luma through the LMCS LUT), filters, stores them to dst.
+__global__ void __launch_bounds__(128) k_deblock_rows(StripParams a) {
+  extern __shared__ __align__(16) uint16_t sm[];
+  int band = blockIdx.x;
+  const int plane = plane_of(a, band);
+  const DPlane src = a.src[plane], dst = a.dst[plane];
+  const int unit = plane ? 2 : 4;
+  const int y0 = band * unit, rows = min(unit, src.h - y0), w = src.w;
+  const int ld = (w + 7) & ~7;
+  const uint16_t *lut = plane == 0 ? a.lut : nullptr;
+  const int nvec = vec_ok(src) ? w / 8 : 0;
+  for (int i = threadIdx.x; i < rows * nvec; i += blockDim.x) {
+    const int r = i / nvec, c = (i - r * nvec) * 8;
+    uint4 q = *reinterpret_cast<const uint4 *>(src.s + (int64_t)(y0 + r) * src.stride + c);
+    if (lut) {
+      uint32_t *u = reinterpret_cast<uint32_t *>(&q);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) u[k] = (uint32_t)lut[u[k] & 0xFFFF] | (uint32_t)lut[u[k] >> 16] << 16;
+    }
+    *reinterpret_cast<uint4 *>(sm + r * ld + c) = q;
+  }
+  const int tail = w - nvec * 8;
+  for (int i = threadIdx.x; i < rows * tail; i += blockDim.x) {
+    const int r = i / tail, c = nvec * 8 + (i - r * tail);
+    const uint16_t x = src.s[(int64_t)(y0 + r) * src.stride + c];
+    sm[r * ld + c] = lut ? lut[x] : x;
+  }
+  __syncthreads();
+  const uint32_t *bf = a.band_first + a.band_off[plane];
+  run_components(a, SharedView{sm, ld, 0, y0, w, rows, w, src.h}, plane, bf[band], bf[band + 1]);
+  __syncthreads();
+  const int nvo = vec_ok(dst) ? w / 8 : 0;
+  for (int i = threadIdx.x; i < rows * nvo; i += blockDim.x) {
+    const int r = i / nvo, c = (i - r * nvo) * 8;
+    *reinterpret_cast<uint4 *>(dst.s + (int64_t)(y0 + r) * dst.stride + c) =
+        *reinterpret_cast<const uint4 *>(sm + r * ld + c);
+  }
+  const int tail_o = w - nvo * 8;
+  for (int i = threadIdx.x; i < rows * tail_o; i += blockDim.x) {
+    const int r = i / tail_o, c = nvo * 8 + (i - r * tail_o);
+    dst.s[(int64_t)(y0 + r) * dst.stride + c] = sm[r * ld + c];
+  }
+}
+
+// Horizontal pass: one CTA per 16-column strip (full plane height), in place.
+__global__ void __launch_bounds__(256) k_deblock_cols(StripParams a) {
+  extern __shared__ __align__(16) uint16_t sm[];
+  int strip = blockIdx.x;
+  const int plane = plane_of(a, strip);
+  const DPlane p = a.dst[plane];
+  const int unit = plane ? 2 : 4;
+  const int x0 = strip * kStripCols, cols = min(kStripCols, p.w - x0), h = p.h;
+  const bool vec = cols == kStripCols && vec_ok(p);
+  if (vec) {
+    for (int i = threadIdx.x; i < h * 2; i += blockDim.x) {
+      const int r = i >> 1, c = (i & 1) * 8;
+      *reinterpret_cast<uint4 *>(sm + r * kStripCols + c) =
+          *reinterpret_cast<const uint4 *>(p.s + (int64_t)r * p.stride + x0 + c);
+    }
+  } else {
+    for (int i = threadIdx.x; i < h * cols; i += blockDim.x) {
+      const int r = i / cols, c = i - r * cols;
+      sm[r * kStripCols + c] = p.s[(int64_t)r * p.stride + x0 + c];
+    }
+  }
+  __syncthreads();
+  const uint32_t *bf = a.band_first + a.band_off[plane];
+  const uint32_t nb = a.n_bands[plane];
+  const uint32_t b0 = min((uint32_t)(x0 / unit), nb), b1 = min((uint32_t)((x0 + kStripCols) / unit), nb);
+  run_components(a, SharedView{sm, kStripCols, x0, 0, cols, h, p.w, h}, plane, bf[b0], bf[b1]);
+  __syncthreads();
+  if (vec) {
+    for (int i = threadIdx.x; i < h * 2; i += blockDim.x) {
+      const int r = i >> 1, c = (i & 1) * 8;
+      *reinterpret_cast<uint4 *>(p.s + (int64_t)r * p.stride + x0 + c) =
+          *reinterpret_cast<const uint4 *>(sm + r * kStripCols + c);
+    }
+  } else {
+    for (int i = threadIdx.x; i < h * cols; i += blockDim.x) {
+      const int r = i / cols, c = i - r * cols;
+      p.s[(int64_t)r * p.stride + x0 + c] = sm[r * kStripCols + c];
+    }
+  }
+}
+
+size_t rows_smem(const DPlane &p) { return (size_t)4 * ((p.w + 7) & ~7) * 2; }
+size_t cols_smem(const DPlane &p) { return (size_t)p.h * kStripCols * 2; }
+
 }  // namespace
+
+bool deblock_strips_fit(const DPlane planes[3]) {
+  for (int i = 0; i < 3; ++i) {
+    if ((int64_t)planes[i].w * planes[i].h == 0) continue;
+    if (rows_smem(planes[i]) > (size_t)kMaxStripSmem || cols_smem(planes[i]) > (size_t)kMaxStripSmem) return false;
+  }
+  return true;
+}
+
+int launch_deblock_strips(cudaStream_t st, const DPlane src[3], const DPlane dst[3], const uint16_t *lut,
+                          int bit_depth, const StripSide &v, const StripSide &h, const uint32_t band_off[2][3],
+                          const uint32_t n_bands[2][3], uint64_t *launches) {
+  StripParams a;
+  std::memset(&a, 0, sizeof a);
+  size_t smem_rows = 0, smem_cols = 0;
+  uint32_t ctas_rows = 0, ctas_cols = 0;
+  uint32_t strips[3];
+  for (int i = 0; i < 3; ++i) {
+    a.src[i] = src[i];
+    a.dst[i] = dst[i];
+    const bool empty = (int64_t)src[i].w * src[i].h == 0;
+    strips[i] = empty ? 0 : (uint32_t)((src[i].w + kStripCols - 1) / kStripCols);
+    if (!empty) {
+      smem_rows = std::max(smem_rows, rows_smem(src[i]));
+      smem_cols = std::max(smem_cols, cols_smem(src[i]));
+    }
+    ctas_rows += empty ? 0 : n_bands[0][i];
+    ctas_cols += strips[i];
+  }
+  a.lut = lut;
+  a.maxv = (1 << bit_depth) - 1;
+  // vertical pass
+  a.segs = v.segs;
+  a.comp = v.comp;
+  a.band_first = v.band_first;
+  for (int i = 0; i < 3; ++i) {
+    a.band_off[i] = band_off[0][i];
+    a.n_bands[i] = n_bands[0][i];
+    a.ctas[i] = (int64_t)src[i].w * src[i].h ? n_bands[0][i] : 0;
+  }
+  if (ctas_rows) {
+    if (smem_rows > 48 * 1024)
+      H266_CUDA(cudaFuncSetAttribute(k_deblock_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_rows));
+    k_deblock_rows<<<ctas_rows, 128, smem_rows, st>>>(a);
+    H266_CUDA(cudaGetLastError());
+    ++*launches;
+  }
+  // horizontal pass, in place on dst
+  a.segs = h.segs;
+  a.comp = h.comp;
+  a.band_first = h.band_first;
+  a.lut = nullptr;
+  for (int i = 0; i < 3; ++i) {
+    a.band_off[i] = band_off[1][i];
+    a.n_bands[i] = n_bands[1][i];
+    a.ctas[i] = strips[i];
+  }
+  if (ctas_cols) {
+    if (smem_cols > 48 * 1024)
+      H266_CUDA(cudaFuncSetAttribute(k_deblock_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cols));
+    k_deblock_cols<<<ctas_cols, 256, smem_cols, st>>>(a);
+    H266_CUDA(cudaGetLastError());
+    ++*launches;
+  }
+  return H266_OK;
+}
 
 int launch_deblock(cudaStream_t st, const DPlane planes[3], int bit_depth, const EdgeSeg *d_segs_v,
                    const uint32_t *d_comp_v, uint32_t n_comp_v, const EdgeSeg *d_segs_h, const uint32_t *d_comp_h,

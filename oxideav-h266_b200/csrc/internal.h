@@ -114,6 +114,14 @@ struct DeblockPlan {
     uint32_t max_len = 0;
   };
   Part parts[6];
+  // Band index of each pass for the strip kernels, planes concatenated:
+  // band_first[d][band_off[d][p] + b] is the first component of plane p's band
+  // b and the plane's n_bands[d][p] + 1-th entry ends its last band.  Bands
+  // are 4 luma / 2 chroma rows (vertical pass) or columns (horizontal pass);
+  // components of bands beyond the plane touch no sample and are left out.
+  std::vector<uint32_t> band_first[2];
+  uint32_t band_off[2][3] = {{0, 0, 0}, {0, 0, 0}};
+  uint32_t n_bands[2][3] = {{0, 0, 0}, {0, 0, 0}};
 };
 
 int build_deblock_plan(const h266_picture &pic, const h266_deblock_cu *cus, uint64_t n_cus,
@@ -123,6 +131,18 @@ int build_deblock_plan(const h266_picture &pic, const h266_deblock_cu *cus, uint
 
 // Launches the two deblocking passes (vertical then horizontal) in place on
 // the three device planes.  seg/comp point at device copies of the plan.
+// Strip kernels: the vertical pass on row bands read from `src` (luma mapped
+// through `lut` when given) and written to `dst` (which may be `src`), then the
+// horizontal pass on 16-column strips of `dst` in place.
+bool deblock_strips_fit(const DPlane planes[3]);
+struct StripSide {  // device pointers of one pass
+  const EdgeSeg *segs;
+  const uint32_t *comp;
+  const uint32_t *band_first;
+};
+int launch_deblock_strips(cudaStream_t st, const DPlane src[3], const DPlane dst[3], const uint16_t *lut,
+                          int bit_depth, const StripSide &v, const StripSide &h, const uint32_t band_off[2][3],
+                          const uint32_t n_bands[2][3], uint64_t *launches);
 int launch_deblock(cudaStream_t st, const DPlane planes[3], int bit_depth, const EdgeSeg *d_segs_v,
                    const uint32_t *d_comp_v, uint32_t n_comp_v, const EdgeSeg *d_segs_h, const uint32_t *d_comp_h,
                    uint32_t n_comp_h, uint64_t *launches);

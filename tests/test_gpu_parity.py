@@ -59,6 +59,9 @@ WORKLOADS = {
     "ctb64_8bit": lambda s: W.make_workload(6000 + s, 832, 480, 8, 6, ccalf=True, lmcs=True, n_luma_aps=2,
                                             alf_fixed_frac=0.5),
     "odd_tail": lambda s: W.make_workload(7000 + s, 200, 136, 10, 7, inter_frac=0.5, ccalf=True, lmcs=True),
+    # rows not a multiple of 8 samples (unaligned strip loads), height not a
+    # multiple of 4 (a partial last band)
+    "odd_stride": lambda s: W.make_workload(7500 + s, 202, 138, 10, 5, inter_frac=0.5, ccalf=True, lmcs=True),
 }
 
 
@@ -102,8 +105,9 @@ def test_chain_parity_host(ctx, kind):
     assert_same(got, want, f"chain {kind}")
 
 
-def test_chain_parity_device_planes(ctx):
-    pic, fa = small_c2(11)
+@pytest.mark.parametrize("kind", ["c2_small", "odd_stride", "stress_dual"])
+def test_chain_parity_device_planes(ctx, kind):
+    pic, fa = WORKLOADS[kind](11)
     want = pic.copy()
     oracle.apply_in_loop_filters(want, fa)
     dev = native.DevicePicture.from_host(pic)
@@ -228,8 +232,8 @@ def test_profiling_counts_every_family(ctx):
     ctx.apply_in_loop_filters(pic.copy(), fa)
     prof = ctx.profile()
     ctx.set_profiling(False)
-    # one bracket per family call: deblock (both passes), SAO/ALF, LMCS LUT + LUT-mapped copy
-    assert prof["deblock"][1] == 1 and prof["sao_alf"][1] == 1 and prof["lmcs"][1] == 2
+    # one bracket per family call: deblock (LMCS-mapped load, both passes), SAO/ALF, LMCS LUT
+    assert prof["deblock"][1] == 1 and prof["sao_alf"][1] == 1 and prof["lmcs"][1] == 1 and prof["copy"][1] == 0
     assert all(ms >= 0 for ms, _ in prof.values())
 
 
@@ -245,6 +249,26 @@ def test_scalar_sao_alf_kernel_parity(kind, monkeypatch):
         c.apply_in_loop_filters(got, fa)
         oracle.apply_in_loop_filters(want, fa)
         assert_same(got, want, f"scalar chain {kind}")
+    finally:
+        c.close()
+
+
+@pytest.mark.parametrize("kind", ["stress", "stress_dual", "odd_stride", "c2_small"])
+def test_global_memory_deblocking_parity(kind, monkeypatch):
+    """The global-memory deblocking path (planes too large for the strip
+    kernels' shared memory) stays bit-exact too."""
+    monkeypatch.setenv("H266_FORCE_GLOBAL_DEBLOCK", "1")
+    c = native.Context(0)
+    try:
+        pic, fa = WORKLOADS[kind](5)
+        got, want = pic.copy(), pic.copy()
+        c.apply_in_loop_filters(got, fa)
+        oracle.apply_in_loop_filters(want, fa)
+        assert_same(got, want, f"global deblocking chain {kind}")
+        got, want = pic.copy(), pic.copy()
+        c.apply_deblocking_clipped(got, fa)
+        oracle.apply_deblocking_clipped(want, fa)
+        assert_same(got, want, f"global deblocking {kind}")
     finally:
         c.close()
 
