@@ -176,7 +176,12 @@ def run_ours(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     items = make_batch(rank, args.batch)
     ctx = native.Context(local_rank)
-    stream = torch.cuda.current_stream()
+    # A dedicated stream: the library launches on it and the CUDA events below
+    # are recorded on it (the legacy default stream's handle is 0, which the
+    # library reads as "use the context's own stream").
+    stream = torch.cuda.Stream(device=local_rank)
+    assert stream.cuda_stream != 0
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
     dev = [native.DevicePicture.from_host(p, local_rank) for p, _ in items]
     plans = [ctx.plan(p, f) for p, f in items]

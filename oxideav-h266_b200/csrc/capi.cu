@@ -139,6 +139,7 @@ struct h266_ctx {
   uint64_t prof_n[H266_PROF_FAMILIES] = {0};
   bool force_scalar = false;  // H266_FORCE_SCALAR_ALF=1: scalar SAO/ALF kernel (cross-checks)
   bool force_global_deblock = false;  // H266_FORCE_GLOBAL_DEBLOCK=1: deblocking on global memory (cross-checks)
+  bool force_strip_deblock = false;   // H266_FORCE_STRIP_DEBLOCK=1: strip kernels instead of tiles (cross-checks)
 };
 
 namespace {
@@ -539,6 +540,7 @@ int build_pass2(const h266_picture &pic, const Pass2Inputs &in, Pass2Host &h) {
 // Side information of one call, assembled into one host blob and uploaded once.
 struct Staged {
   size_t ctb = 0, tab = 0, pack = 0, seg[2] = {0, 0}, comp[2] = {0, 0}, band[2] = {0, 0};
+  size_t tile_range = 0, tile_comps = 0;
   uint8_t *base = nullptr;
 };
 
@@ -547,6 +549,8 @@ struct DbSide {
   uint32_t n_comp[2] = {0, 0};
   uint32_t band_off[2][3] = {{0, 0, 0}, {0, 0, 0}};
   uint32_t n_bands[2][3] = {{0, 0, 0}, {0, 0, 0}};
+  bool tiles_ok = false;
+  uint32_t tiles_x = 0, tiles_y = 0;
 };
 
 void stage_deblock(const DeblockPlan &pl, std::vector<uint8_t> &b, Staged &st, DbSide &db) {
@@ -560,6 +564,13 @@ void stage_deblock(const DeblockPlan &pl, std::vector<uint8_t> &b, Staged &st, D
       db.band_off[d][p] = pl.band_off[d][p];
       db.n_bands[d][p] = pl.n_bands[d][p];
     }
+  }
+  db.tiles_ok = pl.tiles_ok;
+  db.tiles_x = pl.tiles_x;
+  db.tiles_y = pl.tiles_y;
+  if (pl.tiles_ok) {
+    st.tile_range = blob.put(pl.tile_range.data(), pl.tile_range.size() * sizeof(uint32_t));
+    st.tile_comps = blob.put(pl.tile_comps.data(), pl.tile_comps.size() * sizeof(uint32_t));
   }
 }
 
@@ -599,18 +610,26 @@ int plane_map(h266_ctx *ctx, cudaStream_t stream, DPlane dst, DPlane src, const 
 
 // Deblocking of the planes `src` into `dst` (the same planes for in-place
 // filtering), luma mapped through the LMCS LUT `lut` first when given: the
+// tile kernel when the plan has tile lists and dst is not src, else the
 // shared-memory strip kernels when the planes fit them, else plane copies and
 // one thread per component on global memory.
 int run_deblock(h266_ctx *ctx, cudaStream_t stream, const uint8_t *base, const Staged &st, const DbSide &db,
                 const DPlane src[3], const DPlane dst[3], const uint16_t *lut, int bd) {
+  const StripSide v{reinterpret_cast<const EdgeSeg *>(base + st.seg[0]),
+                    reinterpret_cast<const uint32_t *>(base + st.comp[0]),
+                    reinterpret_cast<const uint32_t *>(base + st.band[0])};
+  const StripSide h{reinterpret_cast<const EdgeSeg *>(base + st.seg[1]),
+                    reinterpret_cast<const uint32_t *>(base + st.comp[1]),
+                    reinterpret_cast<const uint32_t *>(base + st.band[1])};
+  const bool separate = src[0].s != dst[0].s && src[1].s != dst[1].s && src[2].s != dst[2].s;
+  if (!ctx->force_global_deblock && !ctx->force_strip_deblock && db.tiles_ok && separate) {
+    Prof pf(ctx, stream, H266_PROF_DEBLOCK);
+    return launch_deblock_tiles(stream, src, dst, lut, bd, v, h, reinterpret_cast<const uint32_t *>(base + st.tile_range),
+                                reinterpret_cast<const uint32_t *>(base + st.tile_comps), db.tiles_x, db.tiles_y,
+                                &ctx->launches);
+  }
   if (!ctx->force_global_deblock && deblock_strips_fit(dst)) {
     Prof pf(ctx, stream, H266_PROF_DEBLOCK);
-    const StripSide v{reinterpret_cast<const EdgeSeg *>(base + st.seg[0]),
-                      reinterpret_cast<const uint32_t *>(base + st.comp[0]),
-                      reinterpret_cast<const uint32_t *>(base + st.band[0])};
-    const StripSide h{reinterpret_cast<const EdgeSeg *>(base + st.seg[1]),
-                      reinterpret_cast<const uint32_t *>(base + st.comp[1]),
-                      reinterpret_cast<const uint32_t *>(base + st.band[1])};
     return launch_deblock_strips(stream, src, dst, lut, bd, v, h, db.band_off, db.n_bands, &ctx->launches);
   }
   for (int i = 0; i < 3; ++i)
@@ -788,6 +807,8 @@ int h266_ctx_create(int device, h266_ctx **out) {
   c->force_scalar = fs && fs[0] == '1';
   const char *fg = std::getenv("H266_FORCE_GLOBAL_DEBLOCK");
   c->force_global_deblock = fg && fg[0] == '1';
+  const char *fstrip = std::getenv("H266_FORCE_STRIP_DEBLOCK");
+  c->force_strip_deblock = fstrip && fstrip[0] == '1';
   *out = c;
   return H266_OK;
 }

@@ -391,6 +391,101 @@ void index_bands(const h266_picture &pic, DeblockPlan &plan) {
   }
 }
 
+// Fills the tile lists.  A vertical-pass component runs in every tile whose
+// columns its footprint reaches and whose rows widened by the halo hold its
+// band (the horizontal pass of those rows reads its output); a
+// horizontal-pass component runs in the tile holding its band whose rows its
+// footprint reaches.
+void index_tiles(const h266_picture &pic, uint32_t cfi, DeblockPlan &plan) {
+  plan.tiles_ok = false;
+  const int T = kDeblockTile;
+  const int w = (int)pic.luma.width, h = (int)pic.luma.height;
+  plan.tiles_x = (uint32_t)((w + T - 1) / T);
+  plan.tiles_y = (uint32_t)((h + T - 1) / T);
+  const bool chroma = (uint64_t)pic.cb.width * pic.cb.height != 0 || (uint64_t)pic.cr.width * pic.cr.height != 0;
+  if (cfi > 1 || (cfi == 0 && chroma)) return;
+  if (chroma && (pic.cb.width != (pic.luma.width + 1) / 2 || pic.cb.height != (pic.luma.height + 1) / 2 ||
+                 pic.cr.width != pic.cb.width || pic.cr.height != pic.cb.height))
+    return;
+  const int tiles_x = (int)plan.tiles_x, tiles_y = (int)plan.tiles_y;
+  const int cw = (int)pic.cb.width, ch = (int)pic.cb.height;
+  // Tile range of component c of pass d: false when it spans more than the
+  // halo; an empty range when it touches no sample of the plane.
+  auto range = [&](int d, size_t c, int &p, int &t0x, int &t1x, int &t0y, int &t1y) {
+    const std::vector<uint32_t> &comp = plan.comp[d];
+    const std::vector<EdgeSeg> &segs = plan.segs[d];
+    const EdgeSeg &f = segs[comp[c]];
+    p = f.plane;
+    const int shift = p ? 5 : 6, halo = p ? kDeblockHaloC : kDeblockHaloY, unit = p ? 2 : 4;
+    int s, e;
+    if (comp[c + 1] - comp[c] == 1) {
+      const int pos = (f.flags & 1) ? f.x : f.y;
+      s = pos - reach(f.mfl >> 4);
+      e = pos + reach(f.mfl & 15);
+    } else {
+      s = INT32_MAX;
+      e = INT32_MIN;
+      for (uint32_t i = comp[c]; i < comp[c + 1]; ++i) {
+        const EdgeSeg &g = segs[i];
+        const int pos = (g.flags & 1) ? g.x : g.y;
+        s = std::min(s, pos - reach(g.mfl >> 4));
+        e = std::max(e, pos + reach(g.mfl & 15));
+      }
+    }
+    if (e - s > halo) return false;
+    const int pw = p ? cw : w, ph = p ? ch : h;
+    const int band = d == 0 ? f.y : f.x, across = d == 0 ? ph : pw;
+    s = std::max(s, 0);
+    e = std::min(e, d == 0 ? pw : ph);
+    t0x = 1, t1x = 0, t0y = 1, t1y = 0;
+    if (s >= e || band >= across) return true;
+    if (d == 0) {  // footprint along x, band rows [band, band + unit)
+      t0x = s >> shift;
+      t1x = (e - 1) >> shift;
+      // tiles whose rows widened by the halo, [ty * tp - halo, (ty + 1) * tp + halo), hold the band
+      t0y = band - halo < 0 ? 0 : (band - halo) >> shift;
+      t1y = (band + unit + halo - 1) >> shift;
+    } else {  // band columns [band, band + unit), footprint along y
+      t0x = t1x = band >> shift;
+      t0y = s >> shift;
+      t1y = (e - 1) >> shift;
+    }
+    t1x = std::min(t1x, tiles_x - 1);
+    t1y = std::min(t1y, tiles_y - 1);
+    return true;
+  };
+  const size_t n_tiles = (size_t)tiles_x * tiles_y;
+  std::vector<uint32_t> &tr = plan.tile_range;
+  tr.assign(n_tiles * 12, 0);
+  // pass 1: counts in the odd entries
+  for (int d = 0; d < 2; ++d)
+    for (size_t c = 0; c + 1 < plan.comp[d].size(); ++c) {
+      int p, t0x, t1x, t0y, t1y;
+      if (!range(d, c, p, t0x, t1x, t0y, t1y)) return;
+      for (int ty = t0y; ty <= t1y; ++ty)
+        for (int tx = t0x; tx <= t1x; ++tx) ++tr[(((size_t)ty * tiles_x + tx) * 6 + d * 3 + p) * 2 + 1];
+    }
+  uint32_t total = 0;
+  for (size_t k = 0; k < n_tiles * 6; ++k) {
+    tr[2 * k] = total;
+    total += tr[2 * k + 1];
+    tr[2 * k + 1] = 0;
+  }
+  plan.tile_comps.resize(total);
+  // pass 2: fill, counting again
+  for (int d = 0; d < 2; ++d)
+    for (size_t c = 0; c + 1 < plan.comp[d].size(); ++c) {
+      int p, t0x, t1x, t0y, t1y;
+      range(d, c, p, t0x, t1x, t0y, t1y);
+      for (int ty = t0y; ty <= t1y; ++ty)
+        for (int tx = t0x; tx <= t1x; ++tx) {
+          const size_t k = ((size_t)ty * tiles_x + tx) * 6 + d * 3 + p;
+          plan.tile_comps[tr[2 * k] + tr[2 * k + 1]++] = (uint32_t)c;
+        }
+    }
+  plan.tiles_ok = true;
+}
+
 }  // namespace
 
 int build_deblock_plan(const h266_picture &pic, const h266_deblock_cu *cus, uint64_t n_cus,
@@ -404,6 +499,7 @@ int build_deblock_plan(const h266_picture &pic, const h266_deblock_cu *cus, uint
   }
   if (params.disabled) {
     index_bands(pic, plan);
+    index_tiles(pic, cfi, plan);
     return H266_OK;
   }
   for (int d = 0; d < 2; ++d) plan.comp[d].clear();
@@ -475,6 +571,7 @@ int build_deblock_plan(const h266_picture &pic, const h266_deblock_cu *cus, uint
     plan.comp[d].push_back((uint32_t)plan.segs[d].size());
   }
   index_bands(pic, plan);
+  index_tiles(pic, cfi, plan);
   return H266_OK;
 }
 
@@ -791,6 +888,292 @@ __host__ __device__ void chroma_segment(const View &P, const EdgeSeg &e, int max
   }
 }
 
+// ------------------------------------------------------------ line-parallel segments
+// The strip kernels filter a segment with one lane per line (4 luma, 2 chroma
+// lines): each lane loads its line, the decision terms of lines 0 and 3 (luma)
+// or of both lines (chroma) are exchanged between the lanes of the group, and
+// each lane filters and writes its own line.  The arithmetic is that of
+// luma_segment / chroma_segment above, split into per-line pieces; every line
+// is loaded before any line is written, as there.
+
+// Access to one line of a segment by distance d from its q0 sample (negative
+// on the P side): through a clamping view, or -- when the segment's samples
+// lie inside the staged window -- straight in shared memory with the step SN
+// between samples along the edge normal.
+template <class View>
+struct ClampLine {
+  const View &P;
+  int qx, qy;  // q0 of the line
+  bool vert;
+  __host__ __device__ __forceinline__ int rd(int d) const { return vert ? P.rd(qx + d, qy) : P.rd(qx, qy + d); }
+  __host__ __device__ __forceinline__ void wr(int d, int v, int maxv) const {
+    if (vert) P.wr(qx + d, qy, v, maxv);
+    else P.wr(qx, qy + d, v, maxv);
+  }
+};
+template <int SN>
+struct RawLine {
+  uint16_t *q;  // q0 of the line
+  __host__ __device__ __forceinline__ int rd(int d) const { return q[d * SN]; }
+  __host__ __device__ __forceinline__ void wr(int d, int v, int maxv) const { q[d * SN] = (uint16_t)min(max(v, 0), maxv); }
+};
+struct RawLineDyn {
+  uint16_t *q;
+  int sn;
+  __host__ __device__ __forceinline__ int rd(int d) const { return q[d * sn]; }
+  __host__ __device__ __forceinline__ void wr(int d, int v, int maxv) const { q[d * sn] = (uint16_t)min(max(v, 0), maxv); }
+};
+
+// Samples of a luma line: s[8 + d] at distance d from q0, d in [-8, 7].
+template <class Line>
+__host__ __device__ __forceinline__ void load_luma_line(const Line &L, int s[16]) {
+#pragma unroll
+  for (int d = -8; d < 8; ++d) s[8 + d] = L.rd(d);
+}
+
+// The decision terms of one luma line (§8.8.3.6.2, src/deblock.rs:1224-1410).
+struct LumaStats {
+  int dp, dq, sp, sq, spq;  // |p2-2p1+p0|, |q2-2q1+q0|, |p3-p0|, |q0-q3|, |p0-q0|
+  int dpx, dqx;             // |p5-2p4+p3|, |q5-2q4+q3|
+  int sp7, sq7;             // |p7-p6-p5+p4|, |q4-q5-q6+q7|
+  int pmd, qmd;             // |p3-p(mflP)|, |q3-q(mflQ)| for mfl 5 / 7
+};
+
+__host__ __device__ __forceinline__ LumaStats luma_stats(const EdgeSeg &e, const int s[16]) {
+#define PL(i) s[7 - (i)]
+#define QL(j) s[8 + (j)]
+  const int mp = e.mfl >> 4, mq = e.mfl & 15;
+  LumaStats t;
+  t.dp = abs(PL(2) - 2 * PL(1) + PL(0));
+  t.dq = abs(QL(2) - 2 * QL(1) + QL(0));
+  t.sp = abs(PL(3) - PL(0));
+  t.sq = abs(QL(0) - QL(3));
+  t.spq = abs(PL(0) - QL(0));
+  t.dpx = abs(PL(5) - 2 * PL(4) + PL(3));
+  t.dqx = abs(QL(5) - 2 * QL(4) + QL(3));
+  t.sp7 = abs(PL(7) - PL(6) - PL(5) + PL(4));
+  t.sq7 = abs(QL(4) - QL(5) - QL(6) + QL(7));
+  t.pmd = abs(PL(3) - (mp == 7 ? PL(7) : (mp == 5 ? PL(5) : PL(3))));
+  t.qmd = abs(QL(3) - (mq == 7 ? QL(7) : (mq == 5 ? QL(5) : QL(3))));
+#undef PL
+#undef QL
+  return t;
+}
+
+struct LumaDecision {
+  int mode;  // 0: no filtering (dE = 0), 1: long filter, 2: short filter
+  int mp, mq;
+  bool strong, dep, deq;
+};
+
+// The segment's decision from the terms of lines 0 (a) and 3 (b).
+__host__ __device__ __forceinline__ LumaDecision luma_decide(const EdgeSeg &e, const LumaStats &a,
+                                                             const LumaStats &b) {
+  const int tc = e.tc, beta = e.beta;
+  LumaDecision dc;
+  dc.mp = e.mfl >> 4;
+  dc.mq = e.mfl & 15;
+  dc.strong = dc.dep = dc.deq = false;
+  const int tc_gate = (5 * tc + 1) >> 1;
+  const bool p_large = dc.mp > 3 && !(e.flags & 2);
+  const bool q_large = dc.mq > 3;
+  if (p_large || q_large) {
+    int dp0l = a.dp, dp3l = b.dp, dq0l = a.dq, dq3l = b.dq;
+    if (p_large) {
+      dp0l = (a.dp + a.dpx + 1) >> 1;
+      dp3l = (b.dp + b.dpx + 1) >> 1;
+    } else {
+      dc.mp = 3;
+    }
+    if (q_large) {
+      dq0l = (a.dq + a.dqx + 1) >> 1;
+      dq3l = (b.dq + b.dqx + 1) >> 1;
+    }
+    int sp0l = a.sp, sp3l = b.sp, sq0l = a.sq, sq3l = b.sq;
+    if (dc.mp == 7) {
+      sp0l += a.sp7;
+      sp3l += b.sp7;
+    }
+    if (dc.mq == 7) {
+      sq0l += a.sq7;
+      sq3l += b.sq7;
+    }
+    if ((dp0l + dq0l) + (dp3l + dq3l) < beta) {
+      const int t1 = (3 * beta) >> 5, t2 = beta >> 4;
+      int spl0 = sp0l, sql0 = sq0l, spl3 = sp3l, sql3 = sq3l;
+      if (p_large) {
+        spl0 = (spl0 + a.pmd + 1) >> 1;
+        spl3 = (spl3 + b.pmd + 1) >> 1;
+      }
+      if (q_large) {
+        sql0 = (sql0 + a.qmd + 1) >> 1;
+        sql3 = (sql3 + b.qmd + 1) >> 1;
+      }
+      if (2 * (dp0l + dq0l) < t2 && spl0 + sql0 < t1 && a.spq < tc_gate && 2 * (dp3l + dq3l) < t2 &&
+          spl3 + sql3 < t1 && b.spq < tc_gate) {
+        dc.mode = 1;
+        return dc;
+      }
+    }
+  }
+  if (a.dp + a.dq + b.dp + b.dq >= beta) {
+    dc.mode = 0;  // dE = 0
+    return dc;
+  }
+  dc.mode = 2;
+  if (dc.mp > 2 && dc.mq > 2) {
+    const int t1 = beta >> 3, t2 = beta >> 2;
+    dc.strong = 2 * (a.dp + a.dq) < t2 && a.sp + a.sq < t1 && a.spq < tc_gate && 2 * (b.dp + b.dq) < t2 &&
+                b.sp + b.sq < t1 && b.spq < tc_gate;
+  }
+  if (dc.strong) dc.mp = dc.mq = 3;
+  const int side_gate = (beta + (beta >> 1)) >> 3;
+  dc.dep = dc.mp > 1 && dc.mq > 1 && a.dp + b.dp < side_gate;
+  dc.deq = dc.mp > 1 && dc.mq > 1 && a.dq + b.dq < side_gate;
+  return dc;
+}
+
+// Filters one luma line (samples s) of a segment after its decision.
+template <class Line>
+__host__ __device__ __forceinline__ void luma_filter_line(const Line &L, const EdgeSeg &e, const LumaDecision &dc,
+                                                          const int s[16], int maxv) {
+  const int tc = e.tc, mp = dc.mp, mq = dc.mq;
+  const bool plt_p = e.flags & 4, plt_q = e.flags & 8;
+  if (dc.mode == 1) {
+    int p[8], q[8];  // entries beyond mflP / mflQ are zero as in the reference's arrays
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      p[i] = i <= mp ? s[7 - i] : 0;
+      q[i] = i <= mq ? s[8 + i] : 0;
+    }
+    int mid;  // refMiddle, eqs. 1389-1394
+    if (mp == 5 && mq == 5)
+      mid = (p[4] + p[3] + 2 * (p[2] + p[1] + p[0] + q[0] + q[1] + q[2]) + q[3] + q[4] + 8) >> 4;
+    else if (mp == mq)
+      mid = (p[6] + p[5] + p[4] + p[3] + p[2] + p[1] + 2 * (p[0] + q[0]) + q[1] + q[2] + q[3] + q[4] + q[5] + q[6] +
+             8) >> 4;
+    else if ((mp == 7 && mq == 5) || (mp == 5 && mq == 7))
+      mid = (p[5] + p[4] + p[3] + p[2] + 2 * (p[1] + p[0] + q[0] + q[1]) + q[2] + q[3] + q[4] + q[5] + 8) >> 4;
+    else if ((mp == 5 && mq == 3) || (mp == 3 && mq == 5))
+      mid = (p[3] + p[2] + p[1] + p[0] + q[0] + q[1] + q[2] + q[3] + 4) >> 3;
+    else if (mp == 3 && mq == 7)
+      mid = (2 * (p[2] + p[1] + p[0] + q[0]) + p[0] + p[1] + q[1] + q[2] + q[3] + q[4] + q[5] + q[6] + 8) >> 4;
+    else
+      mid = (p[6] + p[5] + p[4] + p[3] + p[2] + p[1] + 2 * (q[2] + q[1] + q[0] + p[0]) + q[0] + q[1] + 8) >> 4;
+    const int rp = mp == 7 ? (p[7] + p[6] + 1) >> 1 : (mp == 5 ? (p[5] + p[4] + 1) >> 1 : (p[3] + p[2] + 1) >> 1);
+    const int rq = mq == 7 ? (q[7] + q[6] + 1) >> 1 : (mq == 5 ? (q[5] + q[4] + 1) >> 1 : (q[3] + q[2] + 1) >> 1);
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+      if (i < mp && !plt_p) {
+        const int f = long_f(mp, i), lim = (tc * long_t(mp, i)) >> 1;
+        L.wr(-i - 1, clampd((mid * f + rp * (64 - f) + 32) >> 6, p[i] - lim, p[i] + lim), maxv);
+      }
+      if (i < mq && !plt_q) {
+        const int f = long_f(mq, i), lim = (tc * long_t(mq, i)) >> 1;
+        L.wr(i, clampd((mid * f + rq * (64 - f) + 32) >> 6, q[i] - lim, q[i] + lim), maxv);
+      }
+    }
+    return;
+  }
+  if (dc.mode == 0) return;
+  const int p3 = s[4], p2 = s[5], p1 = s[6], p0 = s[7], q0 = s[8], q1 = s[9], q2 = s[10], q3 = s[11];
+  int np = 0, nq = 0;
+  int op0 = 0, op1 = 0, op2 = 0, oq0 = 0, oq1 = 0, oq2 = 0;
+  if (dc.strong) {
+    op0 = clampd((p2 + 2 * p1 + 2 * p0 + 2 * q0 + q1 + 4) >> 3, p0 - 3 * tc, p0 + 3 * tc);
+    op1 = clampd((p2 + p1 + p0 + q0 + 2) >> 2, p1 - 2 * tc, p1 + 2 * tc);
+    op2 = clampd((2 * p3 + 3 * p2 + p1 + p0 + q0 + 4) >> 3, p2 - tc, p2 + tc);
+    oq0 = clampd((p1 + 2 * p0 + 2 * q0 + 2 * q1 + q2 + 4) >> 3, q0 - 3 * tc, q0 + 3 * tc);
+    oq1 = clampd((p0 + q0 + q1 + q2 + 2) >> 2, q1 - 2 * tc, q1 + 2 * tc);
+    oq2 = clampd((p0 + q0 + q1 + 3 * q2 + 2 * q3 + 4) >> 3, q2 - tc, q2 + tc);
+    np = nq = 3;
+  } else {
+    const int raw = (9 * (q0 - p0) - 3 * (q1 - p1) + 8) >> 4;
+    if (abs(raw) < tc * 10) {
+      const int delta = clampd(raw, -tc, tc);
+      op0 = p0 + delta;
+      oq0 = q0 - delta;
+      np = nq = 1;
+      if (dc.dep) {
+        op1 = p1 + clampd((((p2 + p0 + 1) >> 1) - p1 + delta) >> 1, -(tc >> 1), tc >> 1);
+        np = 2;
+      }
+      if (dc.deq) {
+        oq1 = q1 + clampd((((q2 + q0 + 1) >> 1) - q1 - delta) >> 1, -(tc >> 1), tc >> 1);
+        nq = 2;
+      }
+    }
+  }
+  if (plt_p) np = 0;
+  if (plt_q) nq = 0;
+  const int op[3] = {op0, op1, op2}, oq[3] = {oq0, oq1, oq2};
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    if (i < np) L.wr(-i - 1, op[i], maxv);
+    if (i < nq) L.wr(i, oq[i], maxv);
+  }
+}
+
+// Samples of a chroma line: s[4 + d], d in [-4, 3].
+template <class Line>
+__host__ __device__ __forceinline__ void load_chroma_line(const Line &L, int s[8]) {
+#pragma unroll
+  for (int d = -4; d < 4; ++d) s[4 + d] = L.rd(d);
+}
+
+// Whether the segment may take the strong chroma filter (src/deblock.rs:1803-1890).
+__host__ __device__ __forceinline__ bool chroma_eligible(const EdgeSeg &e) {
+  const int mp = e.mfl >> 4, mq = e.mfl & 15;
+  return (e.flags & 1) ? (mp == 3 && mq == 3) : (mq == 3 && (mp == 3 || mp == 1));
+}
+
+// The strong-filter condition of one chroma line.
+__host__ __device__ __forceinline__ bool chroma_line_ok(const EdgeSeg &e, const int s[8]) {
+  const bool short_p = !(e.flags & 1) && (e.mfl >> 4) == 1;
+  const int tc = e.tc, beta = e.beta;
+  const int p1 = s[2], p0 = s[3], q0 = s[4], q1 = s[5], q2 = s[6], q3 = s[7];
+  const int p3 = short_p ? p1 : s[0], p2 = short_p ? p1 : s[1];
+  const int dpq = 2 * (abs(p2 - 2 * p1 + p0) + abs(q2 - 2 * q1 + q0));
+  return dpq < (beta >> 2) && abs(p3 - p0) + abs(q0 - q3) < (beta >> 3) && abs(p0 - q0) < ((5 * tc + 1) >> 1);
+}
+
+// Filters one chroma line: strong when `strong` (eligible and both lines ok), else weak.
+template <class Line>
+__host__ __device__ __forceinline__ void chroma_filter_line(const Line &L, const EdgeSeg &e, bool strong,
+                                                            const int s[8], int maxv) {
+  const bool vert = e.flags & 1;
+  const int tc = e.tc;
+  const bool plt_p = e.flags & 4, plt_q = e.flags & 8;
+  const int p3 = s[0], p2 = s[1], p1 = s[2], p0 = s[3], q0 = s[4], q1 = s[5], q2 = s[6], q3 = s[7];
+  if (strong) {
+    const bool short_p = !vert && (e.mfl >> 4) == 1;
+    int op[3] = {0, 0, 0}, oq[3];
+    int np;
+    if (short_p) {
+      op[0] = clampd((3 * p1 + 2 * p0 + q0 + q1 + q2 + 4) >> 3, p0 - tc, p0 + tc);
+      oq[0] = clampd((2 * p1 + p0 + 2 * q0 + q1 + q2 + q3 + 4) >> 3, q0 - tc, q0 + tc);
+      np = 1;
+    } else {
+      op[0] = clampd((p3 + p2 + p1 + 2 * p0 + q0 + q1 + q2 + 4) >> 3, p0 - tc, p0 + tc);
+      op[1] = clampd((2 * p3 + p2 + 2 * p1 + p0 + q0 + q1 + 4) >> 3, p1 - tc, p1 + tc);
+      op[2] = clampd((3 * p3 + 2 * p2 + p1 + p0 + q0 + 4) >> 3, p2 - tc, p2 + tc);
+      oq[0] = clampd((p2 + p1 + p0 + 2 * q0 + q1 + q2 + q3 + 4) >> 3, q0 - tc, q0 + tc);
+      np = 3;
+    }
+    oq[1] = clampd((p1 + p0 + q0 + 2 * q1 + q2 + 2 * q3 + 4) >> 3, q1 - tc, q1 + tc);
+    oq[2] = clampd((p0 + q0 + q1 + 2 * q2 + 3 * q3 + 4) >> 3, q2 - tc, q2 + tc);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      if (!plt_p && i < np) L.wr(-i - 1, op[i], maxv);
+      if (!plt_q) L.wr(i, oq[i], maxv);
+    }
+    return;
+  }
+  const int delta = clampd(((q0 - p0) * 4 + p1 - q1 + 4) >> 3, -tc, tc);  // weak filter, eqs. 1421-1423
+  if (!plt_p) L.wr(-1, p0 + delta, maxv);
+  if (!plt_q) L.wr(0, q0 - delta, maxv);
+}
+
 struct Planes3 {
   DPlane p[3];
 };
@@ -817,7 +1200,8 @@ __global__ void __launch_bounds__(128) k_deblock_components(Planes3 planes, cons
 // components without touching samples of other CTAs.  All clamped reads of a
 // segment stay inside the staged window: rows clamp into the plane, whose
 // whole width (rows kernel) or height (columns kernel) is staged.
-constexpr int kStripCols = 16;             // columns per horizontal-pass CTA
+constexpr int kStripCols = 8;              // columns per horizontal-pass CTA (two luma bands)
+constexpr int kStripVec = kStripCols / 8;  // 16-byte vectors per strip row
 constexpr int kMaxStripSmem = 200 * 1024;  // dynamic shared memory per CTA
 
 struct StripParams {
@@ -832,6 +1216,10 @@ struct StripParams {
   int maxv;
 };
 
+// Shared-memory row pitch of the rows kernel: whole 16-byte vectors plus one
+// more, so that the four rows of a band start in different banks.
+__host__ __device__ __forceinline__ int row_pitch(int w) { return ((w + 7) & ~7) + 8; }
+
 __device__ __forceinline__ bool vec_ok(const DPlane &p) { return ((uintptr_t)p.s & 15) == 0 && (p.stride & 7) == 0; }
 
 __device__ __forceinline__ int plane_of(const StripParams &a, int &bid) {
@@ -843,14 +1231,66 @@ __device__ __forceinline__ int plane_of(const StripParams &a, int &bid) {
   return plane;
 }
 
-__device__ __forceinline__ void run_components(const StripParams &a, const SharedView &v, int plane, uint32_t c0,
-                                               uint32_t c1) {
-  for (uint32_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+// One segment by a group of G lanes (G = 4 luma lines, 2 chroma lines); lane
+// k of the group owns line k.  `base` is the group's first lane in the warp.
+// PITCH is the window's row pitch when it is a compile-time constant (0:
+// v.ld), used for direct access along columns.
+template <int G, class Line>
+__device__ __forceinline__ void segment_lines(const Line &L, const EdgeSeg &e, int maxv, int base, unsigned mask) {
+  if (G == 4) {
+    int s[16];
+    load_luma_line(L, s);
+    const LumaStats t = luma_stats(e, s);
+    LumaStats a, b;  // lines 0 and 3
+#define XCHG(f)                       \
+  a.f = __shfl_sync(mask, t.f, base); \
+  b.f = __shfl_sync(mask, t.f, base + 3);
+    XCHG(dp) XCHG(dq) XCHG(sp) XCHG(sq) XCHG(spq) XCHG(dpx) XCHG(dqx) XCHG(sp7) XCHG(sq7) XCHG(pmd) XCHG(qmd)
+#undef XCHG
+    luma_filter_line(L, e, luma_decide(e, a, b), s, maxv);
+  } else {
+    int s[8];
+    load_chroma_line(L, s);
+    const bool ok = chroma_line_ok(e, s);
+    const bool both = __shfl_sync(mask, ok, base) && __shfl_sync(mask, ok, base + 1);
+    chroma_filter_line(L, e, chroma_eligible(e) && both, s, maxv);
+  }
+}
+
+template <int G, int PITCH>
+__device__ __forceinline__ void segment_group(const SharedView &v, const EdgeSeg &e, int maxv, int k, int base,
+                                              unsigned mask) {
+  const bool vert = e.flags & 1;
+  constexpr int R = G == 4 ? 8 : 4;  // samples read on each side of the edge
+  const int qx = vert ? e.x : e.x + k, qy = vert ? e.y + k : e.y;
+  // the segment's samples: R on each side across G lines
+  const int x0 = vert ? e.x - R : e.x, x1 = vert ? e.x + R : e.x + G;
+  const int y0 = vert ? e.y : e.y - R, y1 = vert ? e.y + G : e.y + R;
+  const bool inside = x0 >= v.ox && y0 >= v.oy && x1 <= v.ox + v.ww && y1 <= v.oy + v.wh;
+  if (inside) {  // uniform over the group: the window lies inside the plane, no clamping
+    uint16_t *q = v.s + (qy - v.oy) * v.ld + (qx - v.ox);
+    if (vert) segment_lines<G>(RawLine<1>{q}, e, maxv, base, mask);
+    else if (PITCH > 0) segment_lines<G>(RawLine<(PITCH > 0 ? PITCH : 1)>{q}, e, maxv, base, mask);
+    else segment_lines<G>(RawLineDyn{q, v.ld}, e, maxv, base, mask);
+  } else {
+    segment_lines<G>(ClampLine<SharedView>{v, qx, qy, vert}, e, maxv, base, mask);
+  }
+}
+
+// Components [c0, c1) of the window, one lane group per component.  All lanes
+// of a group walk the same segments; after each segment the group
+// synchronises, as the next segment may read samples another lane wrote
+// (a line clamped onto another at the plane edge).
+template <int G, int PITCH>
+__device__ __forceinline__ void run_components(const StripParams &a, const SharedView &v, uint32_t c0, uint32_t c1) {
+  const int lane = threadIdx.x & 31, k = lane % G, base = lane - k;
+  const unsigned mask = ((1u << G) - 1) << base;
+  const uint32_t groups = blockDim.x / G;
+  for (uint32_t c = c0 + threadIdx.x / G; c < c1; c += groups) {
     const uint32_t e = a.comp[c + 1];
     for (uint32_t i = a.comp[c]; i < e; ++i) {
-      const EdgeSeg s = a.segs[i];
-      if (plane == 0) luma_segment(v, s, a.maxv);
-      else chroma_segment(v, s, a.maxv);
+      segment_group<G, PITCH>(v, a.segs[i], a.maxv, k, base, mask);
+      __syncwarp(mask);
     }
   }
 }
@@ -864,7 +1304,7 @@ __global__ void __launch_bounds__(128) k_deblock_rows(StripParams a) {
   const DPlane src = a.src[plane], dst = a.dst[plane];
   const int unit = plane ? 2 : 4;
   const int y0 = band * unit, rows = min(unit, src.h - y0), w = src.w;
-  const int ld = (w + 7) & ~7;
+  const int ld = row_pitch(w);
   const uint16_t *lut = plane == 0 ? a.lut : nullptr;
   const int nvec = vec_ok(src) ? w / 8 : 0;
   for (int i = threadIdx.x; i < rows * nvec; i += blockDim.x) {
@@ -885,7 +1325,9 @@ __global__ void __launch_bounds__(128) k_deblock_rows(StripParams a) {
   }
   __syncthreads();
   const uint32_t *bf = a.band_first + a.band_off[plane];
-  run_components(a, SharedView{sm, ld, 0, y0, w, rows, w, src.h}, plane, bf[band], bf[band + 1]);
+  const SharedView view{sm, ld, 0, y0, w, rows, w, src.h};
+  if (plane == 0) run_components<4, 0>(a, view, bf[band], bf[band + 1]);
+  else run_components<2, 0>(a, view, bf[band], bf[band + 1]);
   __syncthreads();
   const int nvo = vec_ok(dst) ? w / 8 : 0;
   for (int i = threadIdx.x; i < rows * nvo; i += blockDim.x) {
@@ -900,8 +1342,8 @@ __global__ void __launch_bounds__(128) k_deblock_rows(StripParams a) {
   }
 }
 
-// Horizontal pass: one CTA per 16-column strip (full plane height), in place.
-__global__ void __launch_bounds__(256) k_deblock_cols(StripParams a) {
+// Horizontal pass: one CTA per 8-column strip (full plane height), in place.
+__global__ void __launch_bounds__(128, 8) k_deblock_cols(StripParams a) {
   extern __shared__ __align__(16) uint16_t sm[];
   int strip = blockIdx.x;
   const int plane = plane_of(a, strip);
@@ -910,8 +1352,8 @@ __global__ void __launch_bounds__(256) k_deblock_cols(StripParams a) {
   const int x0 = strip * kStripCols, cols = min(kStripCols, p.w - x0), h = p.h;
   const bool vec = cols == kStripCols && vec_ok(p);
   if (vec) {
-    for (int i = threadIdx.x; i < h * 2; i += blockDim.x) {
-      const int r = i >> 1, c = (i & 1) * 8;
+    for (int i = threadIdx.x; i < h * kStripVec; i += blockDim.x) {
+      const int r = i / kStripVec, c = (i % kStripVec) * 8;
       *reinterpret_cast<uint4 *>(sm + r * kStripCols + c) =
           *reinterpret_cast<const uint4 *>(p.s + (int64_t)r * p.stride + x0 + c);
     }
@@ -925,11 +1367,13 @@ __global__ void __launch_bounds__(256) k_deblock_cols(StripParams a) {
   const uint32_t *bf = a.band_first + a.band_off[plane];
   const uint32_t nb = a.n_bands[plane];
   const uint32_t b0 = min((uint32_t)(x0 / unit), nb), b1 = min((uint32_t)((x0 + kStripCols) / unit), nb);
-  run_components(a, SharedView{sm, kStripCols, x0, 0, cols, h, p.w, h}, plane, bf[b0], bf[b1]);
+  const SharedView view{sm, kStripCols, x0, 0, cols, h, p.w, h};
+  if (plane == 0) run_components<4, kStripCols>(a, view, bf[b0], bf[b1]);
+  else run_components<2, kStripCols>(a, view, bf[b0], bf[b1]);
   __syncthreads();
   if (vec) {
-    for (int i = threadIdx.x; i < h * 2; i += blockDim.x) {
-      const int r = i >> 1, c = (i & 1) * 8;
+    for (int i = threadIdx.x; i < h * kStripVec; i += blockDim.x) {
+      const int r = i / kStripVec, c = (i % kStripVec) * 8;
       *reinterpret_cast<uint4 *>(p.s + (int64_t)r * p.stride + x0 + c) =
           *reinterpret_cast<const uint4 *>(sm + r * kStripCols + c);
     }
@@ -941,7 +1385,154 @@ __global__ void __launch_bounds__(256) k_deblock_cols(StripParams a) {
   }
 }
 
-size_t rows_smem(const DPlane &p) { return (size_t)4 * ((p.w + 7) & ~7) * 2; }
+// ------------------------------------------------------------ tile kernel
+// One CTA per 64x64 luma tile and its 32x32 chroma tiles.  The tile's region
+// -- the tile widened by the halo, clipped to the plane -- is loaded once
+// (luma through the LMCS LUT), the vertical-pass components that reach the
+// tile's columns in the widened rows run, then the horizontal-pass components
+// that reach the tile, and the tile itself is stored.  A component that two
+// tiles need runs in both on the same samples, so no CTA reads another's
+// output.  Components span at most the halo (checked on the host), so every
+// clamped read of a listed component stays inside the region.
+constexpr int kTileThreads = 256;
+constexpr int kRegionY = kDeblockTile + 2 * kDeblockHaloY;      // 96
+constexpr int kRegionC = kDeblockTile / 2 + 2 * kDeblockHaloC;  // 48
+constexpr int kPitchY = kRegionY + 8;                           // smem row pitch, samples
+constexpr int kPitchC = kRegionC + 8;
+constexpr size_t kTileSmem = (size_t)(kRegionY * kPitchY + 2 * kRegionC * kPitchC) * 2;
+
+struct TileParams {
+  DPlane src[3], dst[3];
+  const EdgeSeg *segs[2];
+  const uint32_t *comp[2];
+  const uint32_t *range;  // 12 entries per tile
+  const uint32_t *comps;
+  const uint16_t *lut;
+  uint32_t tiles_x;
+  int maxv;
+};
+
+// Copies rows [oy, oy + wh) x columns [ox, ox + ww) of `src` (ox a multiple of
+// 8) to shared memory with row pitch `pitch`, mapping through `lut` if given.
+__device__ __forceinline__ void load_window(uint16_t *sm, int pitch, const DPlane &src, int ox, int oy, int ww,
+                                            int wh, const uint16_t *lut) {
+  const int nvec = vec_ok(src) ? ww / 8 : 0, tail = ww - nvec * 8;
+  for (int i = threadIdx.x; i < wh * nvec; i += blockDim.x) {
+    const int r = i / nvec, c = (i - r * nvec) * 8;
+    uint4 q = *reinterpret_cast<const uint4 *>(src.s + (int64_t)(oy + r) * src.stride + ox + c);
+    if (lut) {
+      uint32_t *u = reinterpret_cast<uint32_t *>(&q);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) u[k] = (uint32_t)lut[u[k] & 0xFFFF] | (uint32_t)lut[u[k] >> 16] << 16;
+    }
+    *reinterpret_cast<uint4 *>(sm + r * pitch + c) = q;
+  }
+  for (int i = threadIdx.x; i < wh * tail; i += blockDim.x) {
+    const int r = i / tail, c = nvec * 8 + (i - r * tail);
+    const uint16_t x = src.s[(int64_t)(oy + r) * src.stride + ox + c];
+    sm[r * pitch + c] = lut ? lut[x] : x;
+  }
+}
+
+// Stores rows [y0, y0 + ih) x columns [x0, x0 + iw) (x0 a multiple of 8) from
+// the window whose origin is (ox, oy).
+__device__ __forceinline__ void store_window(const uint16_t *sm, int pitch, const DPlane &dst, int ox, int oy,
+                                             int x0, int y0, int iw, int ih) {
+  const int nvec = vec_ok(dst) ? iw / 8 : 0, tail = iw - nvec * 8;
+  const uint16_t *s0 = sm + (y0 - oy) * pitch + (x0 - ox);
+  for (int i = threadIdx.x; i < ih * nvec; i += blockDim.x) {
+    const int r = i / nvec, c = (i - r * nvec) * 8;
+    *reinterpret_cast<uint4 *>(dst.s + (int64_t)(y0 + r) * dst.stride + x0 + c) =
+        *reinterpret_cast<const uint4 *>(s0 + r * pitch + c);
+  }
+  for (int i = threadIdx.x; i < ih * tail; i += blockDim.x) {
+    const int r = i / tail, c = nvec * 8 + (i - r * tail);
+    dst.s[(int64_t)(y0 + r) * dst.stride + x0 + c] = s0[r * pitch + c];
+  }
+}
+
+// The components of one pass of a tile, all three planes, spread over the
+// CTA's warps: a warp task is 8 luma components (groups of 4 lanes) or 16
+// chroma components (groups of 2), so no plane waits for another.
+template <int PITCH_Y, int PITCH_C>
+__device__ __forceinline__ void run_tile_pass(const EdgeSeg *segs, const uint32_t *comp, const uint32_t *comps,
+                                              const uint32_t *r, const SharedView &v0, const SharedView &v1,
+                                              const SharedView &v2, int maxv) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, n_warps = blockDim.x >> 5;
+  const uint32_t n[3] = {r[1], r[3], r[5]};
+  const uint32_t tasks[3] = {(n[0] + 7) / 8, (n[1] + 15) / 16, (n[2] + 15) / 16};
+  const uint32_t total = tasks[0] + tasks[1] + tasks[2];
+  for (uint32_t t = warp; t < total; t += n_warps) {
+    int p = 0;
+    uint32_t tt = t;
+    if (tt >= tasks[0]) {
+      tt -= tasks[0];
+      p = tt >= tasks[1] ? 2 : 1;
+      if (p == 2) tt -= tasks[1];
+    }
+    const uint32_t *list = comps + r[2 * p];
+    if (p == 0) {
+      const int k = lane & 3, base = lane - k;
+      const unsigned mask = 0xFu << base;
+      const uint32_t j = tt * 8 + (lane >> 2);
+      if (j < n[0]) {
+        const uint32_t c = list[j], e = comp[c + 1];
+        for (uint32_t i = comp[c]; i < e; ++i) {
+          segment_group<4, PITCH_Y>(v0, segs[i], maxv, k, base, mask);
+          __syncwarp(mask);
+        }
+      }
+    } else {
+      const int k = lane & 1, base = lane - k;
+      const unsigned mask = 0x3u << base;
+      const uint32_t j = tt * 16 + (lane >> 1);
+      if (j < n[p]) {
+        const SharedView vc = p == 1 ? v1 : v2;
+        const uint32_t c = list[j], e = comp[c + 1];
+        for (uint32_t i = comp[c]; i < e; ++i) {
+          segment_group<2, PITCH_C>(vc, segs[i], maxv, k, base, mask);
+          __syncwarp(mask);
+        }
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kTileThreads, 4) k_deblock_tiles(TileParams a) {
+  extern __shared__ __align__(16) uint16_t sm[];
+  const int t = blockIdx.x, tx = t % (int)a.tiles_x, ty = t / (int)a.tiles_x;
+  uint16_t *const base[3] = {sm, sm + kRegionY * kPitchY, sm + kRegionY * kPitchY + kRegionC * kPitchC};
+  SharedView v[3];
+  int x0[3], y0[3];
+#pragma unroll
+  for (int p = 0; p < 3; ++p) {
+    const DPlane &src = a.src[p];
+    const int tp = p ? kDeblockTile / 2 : kDeblockTile, halo = p ? kDeblockHaloC : kDeblockHaloY;
+    const int pitch = p ? kPitchC : kPitchY;
+    x0[p] = tx * tp;
+    y0[p] = ty * tp;
+    const int ox = max(x0[p] - halo, 0), oy = max(y0[p] - halo, 0);
+    const int ww = min(x0[p] + tp + halo, src.w) - ox, wh = min(y0[p] + tp + halo, src.h) - oy;
+    v[p] = SharedView{base[p], pitch, ox, oy, max(ww, 0), max(wh, 0), src.w, src.h};
+    if (ww > 0 && wh > 0) load_window(base[p], pitch, src, ox, oy, ww, wh, p == 0 ? a.lut : nullptr);
+  }
+  __syncthreads();
+  const uint32_t *r = a.range + (size_t)t * 12;
+#pragma unroll
+  for (int d = 0; d < 2; ++d) {
+    run_tile_pass<kPitchY, kPitchC>(a.segs[d], a.comp[d], a.comps, r + d * 6, v[0], v[1], v[2], a.maxv);
+    __syncthreads();
+  }
+#pragma unroll
+  for (int p = 0; p < 3; ++p) {
+    const int tp = p ? kDeblockTile / 2 : kDeblockTile;
+    const int iw = min(x0[p] + tp, a.dst[p].w) - x0[p], ih = min(y0[p] + tp, a.dst[p].h) - y0[p];
+    if (iw > 0 && ih > 0 && v[p].ww > 0 && v[p].wh > 0)
+      store_window(base[p], p ? kPitchC : kPitchY, a.dst[p], v[p].ox, v[p].oy, x0[p], y0[p], iw, ih);
+  }
+}
+
+size_t rows_smem(const DPlane &p) { return (size_t)4 * row_pitch(p.w) * 2; }
 size_t cols_smem(const DPlane &p) { return (size_t)p.h * kStripCols * 2; }
 
 }  // namespace
@@ -1005,10 +1596,36 @@ int launch_deblock_strips(cudaStream_t st, const DPlane src[3], const DPlane dst
   if (ctas_cols) {
     if (smem_cols > 48 * 1024)
       H266_CUDA(cudaFuncSetAttribute(k_deblock_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cols));
-    k_deblock_cols<<<ctas_cols, 256, smem_cols, st>>>(a);
+    k_deblock_cols<<<ctas_cols, 128, smem_cols, st>>>(a);
     H266_CUDA(cudaGetLastError());
     ++*launches;
   }
+  return H266_OK;
+}
+
+int launch_deblock_tiles(cudaStream_t st, const DPlane src[3], const DPlane dst[3], const uint16_t *lut,
+                         int bit_depth, const StripSide &v, const StripSide &h, const uint32_t *tile_range,
+                         const uint32_t *tile_comps, uint32_t tiles_x, uint32_t tiles_y, uint64_t *launches) {
+  TileParams a;
+  std::memset(&a, 0, sizeof a);
+  for (int i = 0; i < 3; ++i) {
+    a.src[i] = src[i];
+    a.dst[i] = dst[i];
+  }
+  a.segs[0] = v.segs;
+  a.comp[0] = v.comp;
+  a.segs[1] = h.segs;
+  a.comp[1] = h.comp;
+  a.range = tile_range;
+  a.comps = tile_comps;
+  a.lut = lut;
+  a.tiles_x = tiles_x;
+  a.maxv = (1 << bit_depth) - 1;
+  const uint64_t n = (uint64_t)tiles_x * tiles_y;
+  if (!n) return H266_OK;
+  k_deblock_tiles<<<(unsigned)n, kTileThreads, kTileSmem, st>>>(a);
+  H266_CUDA(cudaGetLastError());
+  ++*launches;
   return H266_OK;
 }
 

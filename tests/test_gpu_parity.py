@@ -273,6 +273,22 @@ def test_global_memory_deblocking_parity(kind, monkeypatch):
         c.close()
 
 
+@pytest.mark.parametrize("kind", ["c2_small", "odd_stride", "ctb64_8bit"])
+def test_strip_deblocking_parity(kind, monkeypatch):
+    """The strip deblocking kernels (used when a component spans more than the
+    tile halo) stay bit-exact on pictures the tile kernel takes too."""
+    monkeypatch.setenv("H266_FORCE_STRIP_DEBLOCK", "1")
+    c = native.Context(0)
+    try:
+        pic, fa = WORKLOADS[kind](6)
+        got, want = pic.copy(), pic.copy()
+        c.apply_in_loop_filters(got, fa)
+        oracle.apply_in_loop_filters(want, fa)
+        assert_same(got, want, f"strip deblocking chain {kind}")
+    finally:
+        c.close()
+
+
 def test_wide_coefficients_take_the_scalar_path(ctx):
     """Coefficients outside int8 are legal input for the reference; they must
     still filter bit-exactly (through the scalar kernel)."""
