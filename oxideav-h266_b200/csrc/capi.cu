@@ -540,7 +540,7 @@ int build_pass2(const h266_picture &pic, const Pass2Inputs &in, Pass2Host &h) {
 // Side information of one call, assembled into one host blob and uploaded once.
 struct Staged {
   size_t ctb = 0, tab = 0, pack = 0, seg[2] = {0, 0}, comp[2] = {0, 0}, band[2] = {0, 0};
-  size_t tile_range = 0, tile_comps = 0;
+  size_t tile_bounds = 0;
   uint8_t *base = nullptr;
 };
 
@@ -551,6 +551,7 @@ struct DbSide {
   uint32_t n_bands[2][3] = {{0, 0, 0}, {0, 0, 0}};
   bool tiles_ok = false;
   uint32_t tiles_x = 0, tiles_y = 0;
+  uint32_t tb_off[2][3] = {{0, 0, 0}, {0, 0, 0}};
 };
 
 void stage_deblock(const DeblockPlan &pl, std::vector<uint8_t> &b, Staged &st, DbSide &db) {
@@ -569,8 +570,9 @@ void stage_deblock(const DeblockPlan &pl, std::vector<uint8_t> &b, Staged &st, D
   db.tiles_x = pl.tiles_x;
   db.tiles_y = pl.tiles_y;
   if (pl.tiles_ok) {
-    st.tile_range = blob.put(pl.tile_range.data(), pl.tile_range.size() * sizeof(uint32_t));
-    st.tile_comps = blob.put(pl.tile_comps.data(), pl.tile_comps.size() * sizeof(uint32_t));
+    st.tile_bounds = blob.put(pl.tile_bounds.data(), pl.tile_bounds.size() * sizeof(uint32_t));
+    for (int d = 0; d < 2; ++d)
+      for (int p = 0; p < 3; ++p) db.tb_off[d][p] = pl.tb_off[d][p];
   }
 }
 
@@ -624,9 +626,9 @@ int run_deblock(h266_ctx *ctx, cudaStream_t stream, const uint8_t *base, const S
   const bool separate = src[0].s != dst[0].s && src[1].s != dst[1].s && src[2].s != dst[2].s;
   if (!ctx->force_global_deblock && !ctx->force_strip_deblock && db.tiles_ok && separate) {
     Prof pf(ctx, stream, H266_PROF_DEBLOCK);
-    return launch_deblock_tiles(stream, src, dst, lut, bd, v, h, reinterpret_cast<const uint32_t *>(base + st.tile_range),
-                                reinterpret_cast<const uint32_t *>(base + st.tile_comps), db.tiles_x, db.tiles_y,
-                                &ctx->launches);
+    return launch_deblock_tiles(stream, src, dst, lut, bd, v, h,
+                                reinterpret_cast<const uint32_t *>(base + st.tile_bounds), db.tb_off, db.n_bands,
+                                db.tiles_x, db.tiles_y, &ctx->launches);
   }
   if (!ctx->force_global_deblock && deblock_strips_fit(dst)) {
     Prof pf(ctx, stream, H266_PROF_DEBLOCK);

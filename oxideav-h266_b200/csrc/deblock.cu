@@ -146,7 +146,10 @@ struct Emitted {
 
 class Walker {
  public:
-  Walker(const h266_deblock_cu *cus, size_t n, int pw, int ph) : cus_(cus), n_(n) {
+  // `grid` is caller-owned storage for the 4x4 cell -> CU map, reused across
+  // calls so that no call allocates it anew.
+  Walker(const h266_deblock_cu *cus, size_t n, int pw, int ph, std::vector<int32_t> &grid)
+      : cus_(cus), n_(n), grid_(grid) {
     cw_ = (pw + 3) / 4;
     ch_ = (ph + 3) / 4;
     grid_.assign((size_t)cw_ * ch_, -1);
@@ -155,7 +158,7 @@ class Walker {
       int x0 = c.x / 4, y0 = c.y / 4;
       int x1 = std::min<int64_t>(((int64_t)c.x + c.w + 3) / 4, cw_), y1 = std::min<int64_t>(((int64_t)c.y + c.h + 3) / 4, ch_);
       for (int y = y0; y < y1; ++y)
-        for (int x = x0; x < x1; ++x) grid_[(size_t)y * cw_ + x] = (int64_t)i;
+        for (int x = x0; x < x1; ++x) grid_[(size_t)y * cw_ + x] = (int32_t)i;
     }
   }
   int64_t at(int x, int y) const {
@@ -174,7 +177,7 @@ class Walker {
   const h266_deblock_cu *cus_;
   size_t n_;
   int cw_, ch_;
-  std::vector<int64_t> grid_;
+  std::vector<int32_t> &grid_;
 };
 
 int bs_of(uint32_t comp, const h266_deblock_cu &p, const h266_deblock_cu &q, const MvGrid &mv, int px, int py,
@@ -391,11 +394,12 @@ void index_bands(const h266_picture &pic, DeblockPlan &plan) {
   }
 }
 
-// Fills the tile lists.  A vertical-pass component runs in every tile whose
-// columns its footprint reaches and whose rows widened by the halo hold its
-// band (the horizontal pass of those rows reads its output); a
-// horizontal-pass component runs in the tile holding its band whose rows its
-// footprint reaches.
+// Fills the component ranges of the tile kernel.  A vertical-pass component
+// runs in every tile whose columns its footprint reaches and whose rows
+// widened by the halo hold its band (the horizontal pass of those rows reads
+// its output); a horizontal-pass component runs in the tile holding its band
+// whose rows its footprint reaches.  Footprints are clipped to the plane, so
+// components touching no sample of it are in no range.
 void index_tiles(const h266_picture &pic, uint32_t cfi, DeblockPlan &plan) {
   plan.tiles_ok = false;
   const int T = kDeblockTile;
@@ -408,81 +412,70 @@ void index_tiles(const h266_picture &pic, uint32_t cfi, DeblockPlan &plan) {
                  pic.cr.width != pic.cb.width || pic.cr.height != pic.cb.height))
     return;
   const int tiles_x = (int)plan.tiles_x, tiles_y = (int)plan.tiles_y;
-  const int cw = (int)pic.cb.width, ch = (int)pic.cb.height;
-  // Tile range of component c of pass d: false when it spans more than the
-  // halo; an empty range when it touches no sample of the plane.
-  auto range = [&](int d, size_t c, int &p, int &t0x, int &t1x, int &t0y, int &t1y) {
+  std::vector<uint32_t> &tb = plan.tile_bounds;
+  tb.clear();
+  // per tile and pass: listed components per plane, checked against the shared lists
+  thread_local std::vector<uint32_t> load;
+  load.assign((size_t)tiles_x * tiles_y * 3, 0);
+  for (int d = 0; d < 2; ++d) {
+    std::fill(load.begin(), load.end(), 0);
     const std::vector<uint32_t> &comp = plan.comp[d];
     const std::vector<EdgeSeg> &segs = plan.segs[d];
-    const EdgeSeg &f = segs[comp[c]];
-    p = f.plane;
-    const int shift = p ? 5 : 6, halo = p ? kDeblockHaloC : kDeblockHaloY, unit = p ? 2 : 4;
-    int s, e;
-    if (comp[c + 1] - comp[c] == 1) {
-      const int pos = (f.flags & 1) ? f.x : f.y;
-      s = pos - reach(f.mfl >> 4);
-      e = pos + reach(f.mfl & 15);
-    } else {
-      s = INT32_MAX;
-      e = INT32_MIN;
-      for (uint32_t i = comp[c]; i < comp[c + 1]; ++i) {
-        const EdgeSeg &g = segs[i];
-        const int pos = (g.flags & 1) ? g.x : g.y;
-        s = std::min(s, pos - reach(g.mfl >> 4));
-        e = std::max(e, pos + reach(g.mfl & 15));
+    for (int p = 0; p < 3; ++p) {
+      plan.tb_off[d][p] = (uint32_t)tb.size();
+      const uint32_t nb = plan.n_bands[d][p];
+      if (!nb) continue;
+      const int tp = p ? T / 2 : T, halo = p ? kDeblockHaloC : kDeblockHaloY, unit = p ? 2 : 4;
+      const int along = d == 0 ? (p ? (int)pic.cb.width : w) : (p ? (int)pic.cb.height : h);
+      const int n_t = d == 0 ? tiles_x : tiles_y;  // tiles along the footprint axis
+      const uint32_t *bf = plan.band_first[d].data() + plan.band_off[d][p];
+      const size_t base = tb.size();
+      tb.resize(base + (size_t)nb * n_t * 2);
+      thread_local std::vector<int32_t> fs, fe;  // clipped footprints of one band's components
+      for (uint32_t b = 0; b < nb; ++b) {
+        const uint32_t c0 = bf[b], c1 = bf[b + 1];
+        fs.resize(c1 - c0);
+        fe.resize(c1 - c0);
+        for (uint32_t c = c0; c < c1; ++c) {
+          const EdgeSeg &f = segs[comp[c]];
+          const int pos = (f.flags & 1) ? f.x : f.y;
+          int s = pos - reach(f.mfl >> 4), e = pos + reach(f.mfl & 15);
+          for (uint32_t i = comp[c] + 1; i < comp[c + 1]; ++i) {
+            const EdgeSeg &g = segs[i];
+            const int q = (g.flags & 1) ? g.x : g.y;
+            s = std::min(s, q - reach(g.mfl >> 4));
+            e = std::max(e, q + reach(g.mfl & 15));
+          }
+          if (e - s > halo) return;  // longer than the halo: strip kernels
+          fs[c - c0] = std::max(s, 0);
+          fe[c - c0] = std::min(e, along);
+        }
+        uint32_t lo = c0, hi = c0;
+        for (int t = 0; t < n_t; ++t) {
+          const int t0 = t * tp, t1 = std::min((t + 1) * tp, along);
+          while (lo < c1 && fe[lo - c0] <= t0) ++lo;
+          if (hi < lo) hi = lo;
+          while (hi < c1 && fs[hi - c0] < t1) ++hi;
+          tb[base + ((size_t)b * n_t + t) * 2] = lo;
+          tb[base + ((size_t)b * n_t + t) * 2 + 1] = hi;
+          // count the entries of the tiles that take this band's range
+          const uint32_t n = hi - lo;
+          if (!n) continue;
+          if (d == 0) {
+            const int band = (int)b * unit;
+            const int ty0 = band - halo < 0 ? 0 : (band - halo) / tp;
+            const int ty1 = std::min(tiles_y - 1, (band + unit + halo - 1) / tp);
+            for (int ty = ty0; ty <= ty1; ++ty) load[((size_t)ty * tiles_x + t) * 3 + p] += n;
+          } else {
+            const int tx = (int)b * unit / tp;
+            if (tx < tiles_x) load[((size_t)t * tiles_x + tx) * 3 + p] += n;
+          }
+        }
       }
     }
-    if (e - s > halo) return false;
-    const int pw = p ? cw : w, ph = p ? ch : h;
-    const int band = d == 0 ? f.y : f.x, across = d == 0 ? ph : pw;
-    s = std::max(s, 0);
-    e = std::min(e, d == 0 ? pw : ph);
-    t0x = 1, t1x = 0, t0y = 1, t1y = 0;
-    if (s >= e || band >= across) return true;
-    if (d == 0) {  // footprint along x, band rows [band, band + unit)
-      t0x = s >> shift;
-      t1x = (e - 1) >> shift;
-      // tiles whose rows widened by the halo, [ty * tp - halo, (ty + 1) * tp + halo), hold the band
-      t0y = band - halo < 0 ? 0 : (band - halo) >> shift;
-      t1y = (band + unit + halo - 1) >> shift;
-    } else {  // band columns [band, band + unit), footprint along y
-      t0x = t1x = band >> shift;
-      t0y = s >> shift;
-      t1y = (e - 1) >> shift;
-    }
-    t1x = std::min(t1x, tiles_x - 1);
-    t1y = std::min(t1y, tiles_y - 1);
-    return true;
-  };
-  const size_t n_tiles = (size_t)tiles_x * tiles_y;
-  std::vector<uint32_t> &tr = plan.tile_range;
-  tr.assign(n_tiles * 12, 0);
-  // pass 1: counts in the odd entries
-  for (int d = 0; d < 2; ++d)
-    for (size_t c = 0; c + 1 < plan.comp[d].size(); ++c) {
-      int p, t0x, t1x, t0y, t1y;
-      if (!range(d, c, p, t0x, t1x, t0y, t1y)) return;
-      for (int ty = t0y; ty <= t1y; ++ty)
-        for (int tx = t0x; tx <= t1x; ++tx) ++tr[(((size_t)ty * tiles_x + tx) * 6 + d * 3 + p) * 2 + 1];
-    }
-  uint32_t total = 0;
-  for (size_t k = 0; k < n_tiles * 6; ++k) {
-    tr[2 * k] = total;
-    total += tr[2 * k + 1];
-    tr[2 * k + 1] = 0;
+    for (size_t k = 0; k < load.size(); ++k)
+      if (load[k] > (uint32_t)(k % 3 ? kTileListC : kTileListY)) return;
   }
-  plan.tile_comps.resize(total);
-  // pass 2: fill, counting again
-  for (int d = 0; d < 2; ++d)
-    for (size_t c = 0; c + 1 < plan.comp[d].size(); ++c) {
-      int p, t0x, t1x, t0y, t1y;
-      range(d, c, p, t0x, t1x, t0y, t1y);
-      for (int ty = t0y; ty <= t1y; ++ty)
-        for (int tx = t0x; tx <= t1x; ++tx) {
-          const size_t k = ((size_t)ty * tiles_x + tx) * 6 + d * 3 + p;
-          plan.tile_comps[tr[2 * k] + tr[2 * k + 1]++] = (uint32_t)c;
-        }
-    }
   plan.tiles_ok = true;
 }
 
@@ -506,6 +499,8 @@ int build_deblock_plan(const h266_picture &pic, const h266_deblock_cu *cus, uint
   if (params.bit_depth < 8 || params.bit_depth > 16)
     return set_error(H266_ERR_INVALID_ARGUMENT, "deblock: bit_depth must be 8..16");
   if (params.ctb_log2_size_y > 16) return set_error(H266_ERR_INVALID_ARGUMENT, "deblock: ctb_log2_size_y too large");
+  if (n_cus > (uint64_t)INT32_MAX || n_chroma > (uint64_t)INT32_MAX)
+    return set_error(H266_ERR_UNSUPPORTED, "deblock: more than 2^31 - 1 CUs");
   const h266_deblock_cu *lists[2] = {cus, chroma_cus};
   const uint64_t counts[2] = {n_cus, n_chroma};
   for (int l = 0; l < 2; ++l)
@@ -528,9 +523,10 @@ int build_deblock_plan(const h266_picture &pic, const h266_deblock_cu *cus, uint
   // are concatenated per pass in plane order.
   const bool sep = chroma_cus != nullptr;
   const int n_lists = cfi != 0 ? 6 : 2;
-  Walker luma(cus, n_cus, pw, ph);
+  thread_local std::vector<int32_t> grid_luma, grid_chroma;
+  Walker luma(cus, n_cus, pw, ph, grid_luma);
   std::unique_ptr<Walker> cwalk;
-  if (cfi != 0 && sep) cwalk.reset(new Walker(chroma_cus, n_chroma, pw, ph));
+  if (cfi != 0 && sep) cwalk.reset(new Walker(chroma_cus, n_chroma, pw, ph, grid_chroma));
   const Walker &cw = sep && cfi != 0 ? *cwalk : luma;
   const PlaneCfg cfg[3] = {
       {0, 1, 1, params.luma_beta_offset_div2, params.luma_tc_offset_div2, 0, bd, ctb},
@@ -1405,12 +1401,15 @@ struct TileParams {
   DPlane src[3], dst[3];
   const EdgeSeg *segs[2];
   const uint32_t *comp[2];
-  const uint32_t *range;  // 12 entries per tile
-  const uint32_t *comps;
+  const uint32_t *bounds;  // component ranges per (band, tile), see DeblockPlan::tile_bounds
+  uint32_t tb_off[2][3];
+  uint32_t n_bands[2][3];
   const uint16_t *lut;
-  uint32_t tiles_x;
+  uint32_t tiles_x, tiles_y;
   int maxv;
 };
+
+constexpr int kTileBands = 32;  // bands of one tile and pass that a plane can have (at most 24)
 
 // Copies rows [oy, oy + wh) x columns [ox, ox + ww) of `src` (ox a multiple of
 // 8) to shared memory with row pitch `pitch`, mapping through `lut` if given.
@@ -1455,11 +1454,12 @@ __device__ __forceinline__ void store_window(const uint16_t *sm, int pitch, cons
 // CTA's warps: a warp task is 8 luma components (groups of 4 lanes) or 16
 // chroma components (groups of 2), so no plane waits for another.
 template <int PITCH_Y, int PITCH_C>
-__device__ __forceinline__ void run_tile_pass(const EdgeSeg *segs, const uint32_t *comp, const uint32_t *comps,
-                                              const uint32_t *r, const SharedView &v0, const SharedView &v1,
+__device__ __forceinline__ void run_tile_pass(const EdgeSeg *segs, const uint32_t *comp, const uint32_t *list0,
+                                              const uint32_t *list1, const uint32_t *list2, uint32_t n0, uint32_t n1,
+                                              uint32_t n2, const SharedView &v0, const SharedView &v1,
                                               const SharedView &v2, int maxv) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, n_warps = blockDim.x >> 5;
-  const uint32_t n[3] = {r[1], r[3], r[5]};
+  const uint32_t n[3] = {n0, n1, n2};
   const uint32_t tasks[3] = {(n[0] + 7) / 8, (n[1] + 15) / 16, (n[2] + 15) / 16};
   const uint32_t total = tasks[0] + tasks[1] + tasks[2];
   for (uint32_t t = warp; t < total; t += n_warps) {
@@ -1470,12 +1470,12 @@ __device__ __forceinline__ void run_tile_pass(const EdgeSeg *segs, const uint32_
       p = tt >= tasks[1] ? 2 : 1;
       if (p == 2) tt -= tasks[1];
     }
-    const uint32_t *list = comps + r[2 * p];
+    const uint32_t *list = p == 0 ? list0 : (p == 1 ? list1 : list2);
     if (p == 0) {
       const int k = lane & 3, base = lane - k;
       const unsigned mask = 0xFu << base;
       const uint32_t j = tt * 8 + (lane >> 2);
-      if (j < n[0]) {
+      if (j < n0) {
         const uint32_t c = list[j], e = comp[c + 1];
         for (uint32_t i = comp[c]; i < e; ++i) {
           segment_group<4, PITCH_Y>(v0, segs[i], maxv, k, base, mask);
@@ -1486,7 +1486,7 @@ __device__ __forceinline__ void run_tile_pass(const EdgeSeg *segs, const uint32_
       const int k = lane & 1, base = lane - k;
       const unsigned mask = 0x3u << base;
       const uint32_t j = tt * 16 + (lane >> 1);
-      if (j < n[p]) {
+      if (j < (p == 1 ? n1 : n2)) {
         const SharedView vc = p == 1 ? v1 : v2;
         const uint32_t c = list[j], e = comp[c + 1];
         for (uint32_t i = comp[c]; i < e; ++i) {
@@ -1498,8 +1498,59 @@ __device__ __forceinline__ void run_tile_pass(const EdgeSeg *segs, const uint32_
   }
 }
 
+// Expands the tile's component ranges of pass d into the shared lists.
+__device__ __forceinline__ void tile_lists(const TileParams &a, int d, int tx, int ty, uint32_t *list0,
+                                           uint32_t *list1, uint32_t *list2, uint32_t (*s_off)[kTileBands + 1],
+                                           uint32_t (*s_lo)[kTileBands]) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp < 3) {  // one warp per plane: band counts and their prefix sums
+    const int p = warp;
+    const int tp = p ? kDeblockTile / 2 : kDeblockTile, halo = p ? kDeblockHaloC : kDeblockHaloY, unit = p ? 2 : 4;
+    const int nb = (int)a.n_bands[d][p];
+    int b0, b1, n_t, t;
+    if (d == 0) {  // row bands of the tile's rows widened by the halo
+      b0 = max(ty * tp - halo, 0) / unit;
+      b1 = min((ty * tp + tp + halo) / unit, nb);
+      n_t = (int)a.tiles_x;
+      t = tx;
+    } else {  // column bands of the tile
+      b0 = tx * tp / unit;
+      b1 = min((tx * tp + tp) / unit, nb);
+      n_t = (int)a.tiles_y;
+      t = ty;
+    }
+    const int j = lane, b = b0 + j;
+    uint32_t lo = 0, cnt = 0;
+    if (b < b1) {
+      const uint32_t *e = a.bounds + a.tb_off[d][p] + ((size_t)b * n_t + t) * 2;
+      lo = e[0];
+      cnt = e[1] - e[0];
+    }
+    uint32_t incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    s_lo[p][j] = lo;
+    s_off[p][j + 1] = incl;
+    if (lane == 0) s_off[p][0] = 0;
+  }
+  __syncthreads();
+  const int n_warps = blockDim.x >> 5;
+  for (int task = warp; task < 3 * kTileBands; task += n_warps) {  // one warp per (plane, band)
+    const int p = task / kTileBands, j = task % kTileBands;
+    const uint32_t o = s_off[p][j], cnt = s_off[p][j + 1] - o, lo = s_lo[p][j];
+    uint32_t *list = p == 0 ? list0 : (p == 1 ? list1 : list2);
+    for (uint32_t i = lane; i < cnt; i += 32) list[o + i] = lo + i;
+  }
+  __syncthreads();
+}
+
 __global__ void __launch_bounds__(kTileThreads, 4) k_deblock_tiles(TileParams a) {
   extern __shared__ __align__(16) uint16_t sm[];
+  __shared__ uint32_t s_list_y[kTileListY], s_list_c[2][kTileListC];
+  __shared__ uint32_t s_off[3][kTileBands + 1], s_lo[3][kTileBands];
   const int t = blockIdx.x, tx = t % (int)a.tiles_x, ty = t / (int)a.tiles_x;
   uint16_t *const base[3] = {sm, sm + kRegionY * kPitchY, sm + kRegionY * kPitchY + kRegionC * kPitchC};
   SharedView v[3];
@@ -1516,11 +1567,11 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_deblock_tiles(TileParams a)
     v[p] = SharedView{base[p], pitch, ox, oy, max(ww, 0), max(wh, 0), src.w, src.h};
     if (ww > 0 && wh > 0) load_window(base[p], pitch, src, ox, oy, ww, wh, p == 0 ? a.lut : nullptr);
   }
-  __syncthreads();
-  const uint32_t *r = a.range + (size_t)t * 12;
 #pragma unroll
   for (int d = 0; d < 2; ++d) {
-    run_tile_pass<kPitchY, kPitchC>(a.segs[d], a.comp[d], a.comps, r + d * 6, v[0], v[1], v[2], a.maxv);
+    tile_lists(a, d, tx, ty, s_list_y, s_list_c[0], s_list_c[1], s_off, s_lo);  // its barriers also order the loads
+    run_tile_pass<kPitchY, kPitchC>(a.segs[d], a.comp[d], s_list_y, s_list_c[0], s_list_c[1], s_off[0][kTileBands],
+                                    s_off[1][kTileBands], s_off[2][kTileBands], v[0], v[1], v[2], a.maxv);
     __syncthreads();
   }
 #pragma unroll
@@ -1604,22 +1655,27 @@ int launch_deblock_strips(cudaStream_t st, const DPlane src[3], const DPlane dst
 }
 
 int launch_deblock_tiles(cudaStream_t st, const DPlane src[3], const DPlane dst[3], const uint16_t *lut,
-                         int bit_depth, const StripSide &v, const StripSide &h, const uint32_t *tile_range,
-                         const uint32_t *tile_comps, uint32_t tiles_x, uint32_t tiles_y, uint64_t *launches) {
+                         int bit_depth, const StripSide &v, const StripSide &h, const uint32_t *tile_bounds,
+                         const uint32_t tb_off[2][3], const uint32_t n_bands[2][3], uint32_t tiles_x,
+                         uint32_t tiles_y, uint64_t *launches) {
   TileParams a;
   std::memset(&a, 0, sizeof a);
   for (int i = 0; i < 3; ++i) {
     a.src[i] = src[i];
     a.dst[i] = dst[i];
+    for (int d = 0; d < 2; ++d) {
+      a.tb_off[d][i] = tb_off[d][i];
+      a.n_bands[d][i] = n_bands[d][i];
+    }
   }
   a.segs[0] = v.segs;
   a.comp[0] = v.comp;
   a.segs[1] = h.segs;
   a.comp[1] = h.comp;
-  a.range = tile_range;
-  a.comps = tile_comps;
+  a.bounds = tile_bounds;
   a.lut = lut;
   a.tiles_x = tiles_x;
+  a.tiles_y = tiles_y;
   a.maxv = (1 << bit_depth) - 1;
   const uint64_t n = (uint64_t)tiles_x * tiles_y;
   if (!n) return H266_OK;

@@ -122,20 +122,26 @@ struct DeblockPlan {
   std::vector<uint32_t> band_first[2];
   uint32_t band_off[2][3] = {{0, 0, 0}, {0, 0, 0}};
   uint32_t n_bands[2][3] = {{0, 0, 0}, {0, 0, 0}};
-  // Tile lists of the tile kernel (kDeblockTile x kDeblockTile luma tiles and
-  // the co-located chroma tiles): tile_range[t * 12 + (pass * 3 + plane) * 2]
-  // is the first entry in tile_comps and the next one the count of the
-  // components of that pass and plane the tile runs.  tiles_ok is false when
-  // a component spans more than the tile halo or the chroma format is not
-  // 4:2:0 / 4:0:0; the strip kernels run then.
+  // Component ranges of the tile kernel (kDeblockTile x kDeblockTile luma
+  // tiles and the co-located chroma tiles).  Inside a band the components are
+  // sorted and disjoint, so those reaching one tile form a range: for the
+  // vertical pass tile_bounds[tb_off[0][p] + (band * tiles_x + tx) * 2] and the
+  // next entry are the first and end component of the band reaching tile
+  // column tx; for the horizontal pass the same with (column band * tiles_y +
+  // ty).  tiles_ok is false when a component spans more than the tile halo, a
+  // tile would list more components than the kernel's shared list holds, or
+  // the chroma format is not 4:2:0 / 4:0:0; the strip kernels run then.
   bool tiles_ok = false;
   uint32_t tiles_x = 0, tiles_y = 0;
-  std::vector<uint32_t> tile_range, tile_comps;
+  std::vector<uint32_t> tile_bounds;
+  uint32_t tb_off[2][3] = {{0, 0, 0}, {0, 0, 0}};
 };
 
 constexpr int kDeblockTile = 64;      // luma tile edge of the tile kernel
 constexpr int kDeblockHaloY = 16;     // luma halo (a component's footprint is at most 16 samples)
 constexpr int kDeblockHaloC = 8;      // chroma halo (footprints of at most 8 samples)
+constexpr int kTileListY = 320;       // shared list entries per pass: luma components of a tile
+constexpr int kTileListC = 176;       // chroma components of a tile, per plane
 
 int build_deblock_plan(const h266_picture &pic, const h266_deblock_cu *cus, uint64_t n_cus,
                        const h266_deblock_cu *chroma_cus, uint64_t n_chroma, const h266_deblock_mv_grid *mv,
@@ -159,8 +165,9 @@ int launch_deblock_strips(cudaStream_t st, const DPlane src[3], const DPlane dst
 // Tile kernel: both passes per tile, from `src` (luma through `lut` when
 // given) into `dst`, which must not overlap `src`.
 int launch_deblock_tiles(cudaStream_t st, const DPlane src[3], const DPlane dst[3], const uint16_t *lut,
-                         int bit_depth, const StripSide &v, const StripSide &h, const uint32_t *tile_range,
-                         const uint32_t *tile_comps, uint32_t tiles_x, uint32_t tiles_y, uint64_t *launches);
+                         int bit_depth, const StripSide &v, const StripSide &h, const uint32_t *tile_bounds,
+                         const uint32_t tb_off[2][3], const uint32_t n_bands[2][3], uint32_t tiles_x,
+                         uint32_t tiles_y, uint64_t *launches);
 int launch_deblock(cudaStream_t st, const DPlane planes[3], int bit_depth, const EdgeSeg *d_segs_v,
                    const uint32_t *d_comp_v, uint32_t n_comp_v, const EdgeSeg *d_segs_h, const uint32_t *d_comp_h,
                    uint32_t n_comp_h, uint64_t *launches);
