@@ -1450,47 +1450,89 @@ __device__ __forceinline__ void store_window(const uint16_t *sm, int pitch, cons
   }
 }
 
+// Band counts and prefix sums of the tile's component ranges for (pass d,
+// plane p), by one warp.
+__device__ __forceinline__ void tile_prefix(const TileParams &a, int d, int p, int tx, int ty,
+                                            uint32_t *s_off /* kTileBands + 1 */, uint32_t *s_lo /* kTileBands */) {
+  const int lane = threadIdx.x & 31;
+  const int tp = p ? kDeblockTile / 2 : kDeblockTile, halo = p ? kDeblockHaloC : kDeblockHaloY, unit = p ? 2 : 4;
+  const int nb = (int)a.n_bands[d][p];
+  int b0, b1, n_t, t;
+  if (d == 0) {  // row bands of the tile's rows widened by the halo
+    b0 = max(ty * tp - halo, 0) / unit;
+    b1 = min((ty * tp + tp + halo) / unit, nb);
+    n_t = (int)a.tiles_x;
+    t = tx;
+  } else {  // column bands of the tile
+    b0 = tx * tp / unit;
+    b1 = min((tx * tp + tp) / unit, nb);
+    n_t = (int)a.tiles_y;
+    t = ty;
+  }
+  const int b = b0 + lane;
+  uint32_t lo = 0, cnt = 0;
+  if (b < b1) {
+    const uint32_t *e = a.bounds + a.tb_off[d][p] + ((size_t)b * n_t + t) * 2;
+    lo = e[0];
+    cnt = e[1] - e[0];
+  }
+  uint32_t incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  s_lo[lane] = lo;
+  s_off[lane + 1] = incl;
+  if (lane == 0) s_off[0] = 0;
+}
+
+// The staged window of plane p of tile (tx, ty): the tile widened by the
+// halo, clipped to the plane.  Recomputed where needed rather than kept live.
+__device__ __forceinline__ SharedView tile_view(const TileParams &a, uint16_t *sm, int p, int tx, int ty) {
+  const DPlane &src = a.src[p];
+  const int tp = p ? kDeblockTile / 2 : kDeblockTile, halo = p ? kDeblockHaloC : kDeblockHaloY;
+  uint16_t *base = p == 0 ? sm : sm + kRegionY * kPitchY + (p - 1) * kRegionC * kPitchC;
+  const int ox = max(tx * tp - halo, 0), oy = max(ty * tp - halo, 0);
+  const int ww = min(tx * tp + tp + halo, src.w) - ox, wh = min(ty * tp + tp + halo, src.h) - oy;
+  return SharedView{base, p ? kPitchC : kPitchY, ox, oy, max(ww, 0), max(wh, 0), src.w, src.h};
+}
+
 // The components of one pass of a tile, all three planes, spread over the
 // CTA's warps: a warp task is 8 luma components (groups of 4 lanes) or 16
 // chroma components (groups of 2), so no plane waits for another.
-template <int PITCH_Y, int PITCH_C>
-__device__ __forceinline__ void run_tile_pass(const EdgeSeg *segs, const uint32_t *comp, const uint32_t *list0,
-                                              const uint32_t *list1, const uint32_t *list2, uint32_t n0, uint32_t n1,
-                                              uint32_t n2, const SharedView &v0, const SharedView &v1,
-                                              const SharedView &v2, int maxv) {
+__device__ __forceinline__ void run_tile_pass(const TileParams &a, uint16_t *sm, int tx, int ty, int d,
+                                              const uint32_t *list0, const uint32_t *list1, const uint32_t *list2,
+                                              uint32_t n0, uint32_t n1, uint32_t n2) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, n_warps = blockDim.x >> 5;
-  const uint32_t n[3] = {n0, n1, n2};
-  const uint32_t tasks[3] = {(n[0] + 7) / 8, (n[1] + 15) / 16, (n[2] + 15) / 16};
-  const uint32_t total = tasks[0] + tasks[1] + tasks[2];
+  const EdgeSeg *segs = a.segs[d];
+  const uint32_t *comp = a.comp[d];
+  const uint32_t tasks0 = (n0 + 7) / 8, tasks1 = (n1 + 15) / 16, tasks2 = (n2 + 15) / 16;
+  const uint32_t total = tasks0 + tasks1 + tasks2;
   for (uint32_t t = warp; t < total; t += n_warps) {
-    int p = 0;
-    uint32_t tt = t;
-    if (tt >= tasks[0]) {
-      tt -= tasks[0];
-      p = tt >= tasks[1] ? 2 : 1;
-      if (p == 2) tt -= tasks[1];
-    }
-    const uint32_t *list = p == 0 ? list0 : (p == 1 ? list1 : list2);
-    if (p == 0) {
+    if (t < tasks0) {
       const int k = lane & 3, base = lane - k;
       const unsigned mask = 0xFu << base;
-      const uint32_t j = tt * 8 + (lane >> 2);
+      const uint32_t j = t * 8 + (lane >> 2);
       if (j < n0) {
-        const uint32_t c = list[j], e = comp[c + 1];
+        const SharedView v = tile_view(a, sm, 0, tx, ty);
+        const uint32_t c = list0[j], e = comp[c + 1];
         for (uint32_t i = comp[c]; i < e; ++i) {
-          segment_group<4, PITCH_Y>(v0, segs[i], maxv, k, base, mask);
+          segment_group<4, kPitchY>(v, segs[i], a.maxv, k, base, mask);
           __syncwarp(mask);
         }
       }
     } else {
+      const bool cr = t >= tasks0 + tasks1;
+      const uint32_t tt = t - tasks0 - (cr ? tasks1 : 0);
       const int k = lane & 1, base = lane - k;
       const unsigned mask = 0x3u << base;
       const uint32_t j = tt * 16 + (lane >> 1);
-      if (j < (p == 1 ? n1 : n2)) {
-        const SharedView vc = p == 1 ? v1 : v2;
-        const uint32_t c = list[j], e = comp[c + 1];
+      if (j < (cr ? n2 : n1)) {
+        const SharedView v = tile_view(a, sm, cr ? 2 : 1, tx, ty);
+        const uint32_t c = (cr ? list2 : list1)[j], e = comp[c + 1];
         for (uint32_t i = comp[c]; i < e; ++i) {
-          segment_group<2, PITCH_C>(vc, segs[i], maxv, k, base, mask);
+          segment_group<2, kPitchC>(v, segs[i], a.maxv, k, base, mask);
           __syncwarp(mask);
         }
       }
@@ -1498,88 +1540,41 @@ __device__ __forceinline__ void run_tile_pass(const EdgeSeg *segs, const uint32_
   }
 }
 
-// Expands the tile's component ranges of pass d into the shared lists.
-__device__ __forceinline__ void tile_lists(const TileParams &a, int d, int tx, int ty, uint32_t *list0,
-                                           uint32_t *list1, uint32_t *list2, uint32_t (*s_off)[kTileBands + 1],
-                                           uint32_t (*s_lo)[kTileBands]) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (warp < 3) {  // one warp per plane: band counts and their prefix sums
-    const int p = warp;
-    const int tp = p ? kDeblockTile / 2 : kDeblockTile, halo = p ? kDeblockHaloC : kDeblockHaloY, unit = p ? 2 : 4;
-    const int nb = (int)a.n_bands[d][p];
-    int b0, b1, n_t, t;
-    if (d == 0) {  // row bands of the tile's rows widened by the halo
-      b0 = max(ty * tp - halo, 0) / unit;
-      b1 = min((ty * tp + tp + halo) / unit, nb);
-      n_t = (int)a.tiles_x;
-      t = tx;
-    } else {  // column bands of the tile
-      b0 = tx * tp / unit;
-      b1 = min((tx * tp + tp) / unit, nb);
-      n_t = (int)a.tiles_y;
-      t = ty;
-    }
-    const int j = lane, b = b0 + j;
-    uint32_t lo = 0, cnt = 0;
-    if (b < b1) {
-      const uint32_t *e = a.bounds + a.tb_off[d][p] + ((size_t)b * n_t + t) * 2;
-      lo = e[0];
-      cnt = e[1] - e[0];
-    }
-    uint32_t incl = cnt;
+__global__ void __launch_bounds__(kTileThreads, 4) k_deblock_tiles(TileParams a) {
+  extern __shared__ __align__(16) uint16_t sm[];
+  __shared__ uint32_t s_list_y[2][kTileListY], s_list_c[2][2][kTileListC];
+  __shared__ uint32_t s_off[2][3][kTileBands + 1], s_lo[2][3][kTileBands];
+  const int t = blockIdx.x, tx = t % (int)a.tiles_x, ty = t / (int)a.tiles_x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, n_warps = blockDim.x >> 5;
+  // Warps 0-5 first read the component ranges of both passes (one warp per
+  // pass and plane), then every thread loads the planes' regions.
+  if (warp < 6) tile_prefix(a, warp / 3, warp % 3, tx, ty, s_off[warp / 3][warp % 3], s_lo[warp / 3][warp % 3]);
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-      if (lane >= o) incl += y;
-    }
-    s_lo[p][j] = lo;
-    s_off[p][j + 1] = incl;
-    if (lane == 0) s_off[p][0] = 0;
+  for (int p = 0; p < 3; ++p) {
+    const SharedView v = tile_view(a, sm, p, tx, ty);
+    if (v.ww > 0 && v.wh > 0) load_window(v.s, v.ld, a.src[p], v.ox, v.oy, v.ww, v.wh, p == 0 ? a.lut : nullptr);
   }
   __syncthreads();
-  const int n_warps = blockDim.x >> 5;
-  for (int task = warp; task < 3 * kTileBands; task += n_warps) {  // one warp per (plane, band)
-    const int p = task / kTileBands, j = task % kTileBands;
-    const uint32_t o = s_off[p][j], cnt = s_off[p][j + 1] - o, lo = s_lo[p][j];
-    uint32_t *list = p == 0 ? list0 : (p == 1 ? list1 : list2);
+  // expand the ranges into the lists: one warp per (pass, plane, band)
+  for (int task = warp; task < 6 * kTileBands; task += n_warps) {
+    const int dp = task / kTileBands, j = task % kTileBands, d = dp / 3, p = dp % 3;
+    const uint32_t o = s_off[d][p][j], cnt = s_off[d][p][j + 1] - o, lo = s_lo[d][p][j];
+    uint32_t *list = p == 0 ? s_list_y[d] : s_list_c[d][p - 1];
     for (uint32_t i = lane; i < cnt; i += 32) list[o + i] = lo + i;
   }
   __syncthreads();
-}
-
-__global__ void __launch_bounds__(kTileThreads, 4) k_deblock_tiles(TileParams a) {
-  extern __shared__ __align__(16) uint16_t sm[];
-  __shared__ uint32_t s_list_y[kTileListY], s_list_c[2][kTileListC];
-  __shared__ uint32_t s_off[3][kTileBands + 1], s_lo[3][kTileBands];
-  const int t = blockIdx.x, tx = t % (int)a.tiles_x, ty = t / (int)a.tiles_x;
-  uint16_t *const base[3] = {sm, sm + kRegionY * kPitchY, sm + kRegionY * kPitchY + kRegionC * kPitchC};
-  SharedView v[3];
-  int x0[3], y0[3];
-#pragma unroll
-  for (int p = 0; p < 3; ++p) {
-    const DPlane &src = a.src[p];
-    const int tp = p ? kDeblockTile / 2 : kDeblockTile, halo = p ? kDeblockHaloC : kDeblockHaloY;
-    const int pitch = p ? kPitchC : kPitchY;
-    x0[p] = tx * tp;
-    y0[p] = ty * tp;
-    const int ox = max(x0[p] - halo, 0), oy = max(y0[p] - halo, 0);
-    const int ww = min(x0[p] + tp + halo, src.w) - ox, wh = min(y0[p] + tp + halo, src.h) - oy;
-    v[p] = SharedView{base[p], pitch, ox, oy, max(ww, 0), max(wh, 0), src.w, src.h};
-    if (ww > 0 && wh > 0) load_window(base[p], pitch, src, ox, oy, ww, wh, p == 0 ? a.lut : nullptr);
-  }
 #pragma unroll
   for (int d = 0; d < 2; ++d) {
-    tile_lists(a, d, tx, ty, s_list_y, s_list_c[0], s_list_c[1], s_off, s_lo);  // its barriers also order the loads
-    run_tile_pass<kPitchY, kPitchC>(a.segs[d], a.comp[d], s_list_y, s_list_c[0], s_list_c[1], s_off[0][kTileBands],
-                                    s_off[1][kTileBands], s_off[2][kTileBands], v[0], v[1], v[2], a.maxv);
+    run_tile_pass(a, sm, tx, ty, d, s_list_y[d], s_list_c[d][0], s_list_c[d][1], s_off[d][0][kTileBands],
+                  s_off[d][1][kTileBands], s_off[d][2][kTileBands]);
     __syncthreads();
   }
 #pragma unroll
   for (int p = 0; p < 3; ++p) {
-    const int tp = p ? kDeblockTile / 2 : kDeblockTile;
-    const int iw = min(x0[p] + tp, a.dst[p].w) - x0[p], ih = min(y0[p] + tp, a.dst[p].h) - y0[p];
-    if (iw > 0 && ih > 0 && v[p].ww > 0 && v[p].wh > 0)
-      store_window(base[p], p ? kPitchC : kPitchY, a.dst[p], v[p].ox, v[p].oy, x0[p], y0[p], iw, ih);
+    const SharedView v = tile_view(a, sm, p, tx, ty);
+    const int tp = p ? kDeblockTile / 2 : kDeblockTile, x0 = tx * tp, y0 = ty * tp;
+    const int iw = min(x0 + tp, a.dst[p].w) - x0, ih = min(y0 + tp, a.dst[p].h) - y0;
+    if (iw > 0 && ih > 0 && v.ww > 0 && v.wh > 0) store_window(v.s, v.ld, a.dst[p], v.ox, v.oy, x0, y0, iw, ih);
   }
 }
 
