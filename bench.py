@@ -40,8 +40,9 @@ import time
 ROOT = pathlib.Path(__file__).resolve().parent
 WIDTH, HEIGHT, BITDEPTH = 1920, 1080, 10
 METRIC = "filter-chain Mpx/s 1080p/2160p 10-bit bit-exact"
-# DRAM bytes per luma pixel of the SAO/ALF kernel from `ncu` (profiles/); None until captured
-SAO_ALF_TRAFFIC_PER_PX = None
+# DRAM bytes (read + write) per luma pixel of one k_sao_alf_packed launch, from the
+# ncu capture in profiles/k_sao_alf_packed_c2_1080p10.md (6 288 384 B / 1920x1080)
+SAO_ALF_TRAFFIC_PER_PX = 6288384 / (1920 * 1080)
 
 
 def _import_pkg():
@@ -238,7 +239,7 @@ def run_ours(args, rank, world, local_rank):
     achieved = alg_bytes / per_launch_s / 1e9
     total_ms = sum(v[0] for v in prof.values())
     roofline = {
-        "kernel": "k_sao_alf (SAO + ALF classification + 7x7/5x5 + CC-ALF tile pass)",
+        "kernel": "k_sao_alf_packed (SAO + ALF classification + 7x7/5x5 + CC-ALF tile pass)",
         "bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
         "frac": round(achieved / peaks["hbm_gbs"], 4), "peak_source": peak_kind,
         "traffic": (round(SAO_ALF_TRAFFIC_PER_PX * WIDTH * HEIGHT) if SAO_ALF_TRAFFIC_PER_PX else None),
