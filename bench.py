@@ -7,9 +7,12 @@ pictures generated like the 1080p benchmark config (50 % inter CUs with a
 motion grid, 4 luma ALF APSs switched per CTU, CC-ALF, LMCS).  The batch's
 planes (199 MB for 32 pictures) exceed the 126 MB L2, so no flush is needed.
 
-  value     device-resident throughput: side information resident in resident
-            plans (h266_chain_plan_*), samples resident in HBM, CUDA-event
-            timed on the stream the library launches on, max over ranks.
+  value     device-resident throughput: side information resident in plans
+            (h266_chain_plan_*), samples resident in HBM, the batch executed
+            by h266_chain_plan_execute_batch (one deblocking and one SAO/ALF
+            launch over every picture's tiles), CUDA-event timed on the stream
+            the library launches on, max over ranks.
+  plain     the same plans executed picture by picture (two launches each).
   e2e       the same work through the public batch call
             h266_apply_in_loop_filters_batch with host (pinned) buffers: per
             picture the side-information build from the CU lists (worker
@@ -188,9 +191,21 @@ def run_ours(args, rank, world, local_rank):
     plans = [ctx.plan(p, f) for p, f in items]
     torch.cuda.synchronize()
 
-    def step():
+    def step():  # the whole batch: one deblocking and one SAO/ALF launch over all pictures' tiles
+        ctx.execute_plans(plans, dev)
+
+    def step_plain():  # the same work as per-picture launches
         for pl, d in zip(plans, dev):
             pl.execute(d)
+
+    def device_ms(fn, steps):
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(steps):
+            fn()
+        end.record(stream)
+        torch.cuda.synchronize()
+        return start.elapsed_time(end)
 
     def barrier():
         if dist:
@@ -225,7 +240,21 @@ def run_ours(args, rank, world, local_rank):
     px_per_step = args.batch * WIDTH * HEIGHT
     value = world * px_per_step * args.steps / (ms_max / 1e3) / 1e6
 
-    # roofline of the SAO/ALF tile kernel: per-launch CUDA-event durations in a profiled run
+    # the same pictures as plain per-picture launches, for comparison
+    for _ in range(args.warmup):
+        step_plain()
+    barrier()
+    torch.cuda.synchronize()
+    plain_steps = max(1, min(args.steps, 20))
+    tp = torch.tensor([device_ms(step_plain, plain_steps)], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(tp, op=dist.ReduceOp.MAX)
+    plain = {"value": round(world * px_per_step * plain_steps / (float(tp.item()) / 1e3) / 1e6, 2), "unit": "Mpx/s",
+             "ms_per_step": round(float(tp.item()) / plain_steps, 4), "steps": plain_steps,
+             "path": "h266_chain_plan_execute per picture (2 launches per picture)"}
+
+    # roofline of the SAO/ALF tile kernel: CUDA-event durations of its launches
+    # (one per step, covering the batch's pictures) in a profiled run
     ctx.set_profiling(True)
     prof_steps = min(args.steps, 5)
     for _ in range(prof_steps):
@@ -233,7 +262,7 @@ def run_ours(args, rank, world, local_rank):
     prof = ctx.profile()
     ctx.set_profiling(False)
     ms_sa, n_sa = prof["sao_alf"]
-    alg_bytes = 6 * WIDTH * HEIGHT  # u16 4:2:0 planes read once + written once per launch (one picture)
+    alg_bytes = 6 * WIDTH * HEIGHT * args.batch  # u16 4:2:0 planes read once + written once, per launch
     per_launch_s = ms_sa / max(n_sa, 1) / 1e3
     peaks, peak_kind = measured_peaks()
     achieved = alg_bytes / per_launch_s / 1e9
@@ -242,8 +271,9 @@ def run_ours(args, rank, world, local_rank):
         "kernel": "k_sao_alf_packed (SAO + ALF classification + 7x7/5x5 + CC-ALF tile pass)",
         "bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
         "frac": round(achieved / peaks["hbm_gbs"], 4), "peak_source": peak_kind,
-        "traffic": (round(SAO_ALF_TRAFFIC_PER_PX * WIDTH * HEIGHT) if SAO_ALF_TRAFFIC_PER_PX else None),
+        "traffic": (round(SAO_ALF_TRAFFIC_PER_PX * WIDTH * HEIGHT * args.batch) if SAO_ALF_TRAFFIC_PER_PX else None),
         "algorithmic_bytes_per_launch": alg_bytes, "launch_us": round(per_launch_s * 1e6, 2),
+        "pictures_per_launch": args.batch,
         "share_of_device_time": {k: round(v[0] / total_ms, 3) for k, v in prof.items() if total_ms > 0},
     }
 
@@ -292,7 +322,7 @@ def run_ours(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic (seeded 1080p config generator)",
             "config": workload_config(args.batch, world),
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "roofline": roofline, "plain": plain, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

@@ -330,6 +330,14 @@ typedef struct h266_chain_plan h266_chain_plan;
 int h266_chain_plan_create(h266_ctx *ctx, const h266_picture *pic, const h266_in_loop_filter_args *args,
                            h266_chain_plan **out);
 int h266_chain_plan_execute(h266_ctx *ctx, h266_chain_plan *plan, h266_picture *pic);
+/* Executes n plans on n device pictures (pics[i] with plans[i]; sizes may
+ * differ) as one batch: one deblocking launch and one SAO / ALF launch per
+ * kernel variant cover the tiles of every picture, so the GPU's tail between
+ * pictures disappears.  No counterpart in the crate.  Asynchronous on the
+ * context's stream, like h266_chain_plan_execute; results are bit-identical
+ * to executing the plans one by one.  A picture must not appear twice. */
+int h266_chain_plan_execute_batch(h266_ctx *ctx, uint32_t n, h266_chain_plan *const *plans,
+                                  h266_picture *const *pics);
 int h266_chain_plan_destroy(h266_chain_plan *plan);
 
 /* ---- allocation-free chain ---------------------------------------------------

@@ -137,6 +137,12 @@ struct h266_ctx {
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
   double prof_ms[H266_PROF_FAMILIES] = {0};
   uint64_t prof_n[H266_PROF_FAMILIES] = {0};
+  // batched plan executions: per-picture kernel parameters, uploaded per call
+  std::vector<uint8_t> batch_blob;
+  h266::DevBuf batch_side;
+  h266::Staging batch_stage;
+  cudaEvent_t batch_staged = nullptr;
+  cudaEvent_t batch_done = nullptr;  // last batched launch that reads batch_side
   bool force_scalar = false;  // H266_FORCE_SCALAR_ALF=1: scalar SAO/ALF kernel (cross-checks)
   bool force_global_deblock = false;  // H266_FORCE_GLOBAL_DEBLOCK=1: deblocking on global memory (cross-checks)
   bool force_strip_deblock = false;   // H266_FORCE_STRIP_DEBLOCK=1: strip kernels instead of tiles (cross-checks)
@@ -584,8 +590,8 @@ void stage_pass2(const Pass2Host &h, std::vector<uint8_t> &b, Staged &st) {
 }
 
 // Runs pass 2 (SAO and/or ALF) from `src` into the picture planes `dst`.
-int run_pass2(h266_ctx *ctx, cudaStream_t stream, Pass2Args a, bool do_sao, bool do_alf, bool packed,
-              const uint8_t *base, const Staged &st, const DPlane src[3], const DPlane dst[3]) {
+// Completes the pass-2 arguments with the planes and the staged tables.
+void bind_pass2(Pass2Args &a, const uint8_t *base, const Staged &st, const DPlane src[3], const DPlane dst[3]) {
   for (int i = 0; i < 3; ++i) {
     a.src[i] = src[i];
     a.dst[i] = dst[i];
@@ -594,6 +600,11 @@ int run_pass2(h266_ctx *ctx, cudaStream_t stream, Pass2Args a, bool do_sao, bool
   a.tables.luma_coeff = reinterpret_cast<const int32_t *>(base + st.tab);  // per slot: coeff[300], clip[300]
   a.tables.luma_clip = a.tables.luma_coeff + 300;
   a.tables.luma_packed = reinterpret_cast<const uint32_t *>(base + st.pack);
+}
+
+int run_pass2(h266_ctx *ctx, cudaStream_t stream, Pass2Args a, bool do_sao, bool do_alf, bool packed,
+              const uint8_t *base, const Staged &st, const DPlane src[3], const DPlane dst[3]) {
+  bind_pass2(a, base, st, src, dst);
   Prof pf(ctx, stream, H266_PROF_SAO_ALF);
   if (packed && !ctx->force_scalar) return launch_pass2_packed(stream, a, do_sao, do_alf, &ctx->launches);
   return launch_pass2(stream, a, do_sao, do_alf, &ctx->launches);
@@ -830,6 +841,10 @@ int h266_ctx_destroy(h266_ctx *ctx) {
     cudaEventDestroy(e.second.first);
     cudaEventDestroy(e.second.second);
   }
+  ctx->batch_side.release();
+  if (ctx->batch_stage.ptr) cudaFreeHost(ctx->batch_stage.ptr);
+  if (ctx->batch_staged) cudaEventDestroy(ctx->batch_staged);
+  if (ctx->batch_done) cudaEventDestroy(ctx->batch_done);
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
   return H266_OK;
@@ -1128,6 +1143,124 @@ int h266_chain_plan_execute(h266_ctx *ctx, h266_chain_plan *plan, h266_picture *
   h.packed = plan->packed;
   return exec_chain(ctx, ctx->stream, st.base, st, plan->db, h, plan->lmcs ? plan->lut.as<uint16_t>() : nullptr,
                     plan->deblock_bd, P, S);
+}
+
+int h266_chain_plan_execute_batch(h266_ctx *ctx, uint32_t n, h266_chain_plan *const *plans,
+                                  h266_picture *const *pics) {
+  H266_TRY(check_ctx(ctx));
+  if (n && (!plans || !pics)) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL batch arrays");
+  for (uint32_t i = 0; i < n; ++i) {
+    if (!plans[i]) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL plan in batch");
+    H266_TRY(check_picture(pics[i]));
+    if (pics[i]->mem != H266_MEM_DEVICE) return set_error(H266_ERR_INVALID_ARGUMENT, "plans execute on device pictures");
+    if (!same_geometry(*pics[i], plans[i]->geom))
+      return set_error(H266_ERR_INVALID_ARGUMENT, "picture geometry differs from its plan");
+    if (plans[i]->device != ctx->device) return set_error(H266_ERR_INVALID_ARGUMENT, "plan belongs to another device");
+  }
+  if (!n) return H266_OK;
+  Guard g(ctx->device);
+  cudaStream_t stream = ctx->stream;
+  if (!ctx->batch_staged) H266_CUDA(cudaEventCreateWithFlags(&ctx->batch_staged, cudaEventDisableTiming));
+  if (!ctx->batch_done) H266_CUDA(cudaEventCreateWithFlags(&ctx->batch_done, cudaEventDisableTiming));
+  // Per picture: device views, and which part runs batched.
+  struct Item {
+    DPlane P[3], S[3];
+    Staged st;
+    bool tile, packed;
+    int variant;
+  };
+  std::vector<Item> items(n);
+  std::vector<uint8_t> tile_params;
+  std::vector<uint32_t> tile_first(1, 0);
+  std::vector<Pass2Args> p2[8];
+  std::vector<uint32_t> p2_first[8];
+  const size_t tps = deblock_tile_params_size();
+  for (uint32_t i = 0; i < n; ++i) {
+    const h266_chain_plan &pl = *plans[i];
+    Item &it = items[i];
+    H266_TRY(picture_to_device(ctx->main, *pics[i], it.P));
+    for (int k = 0; k < 3; ++k)
+      it.S[k] = DPlane{pl.pass2 ? pl.scratch[k].as<uint16_t>() : nullptr, std::max(it.P[k].w, 1), it.P[k].w, it.P[k].h};
+    it.st = pl.st;
+    it.st.base = pl.side.as<uint8_t>();
+    const uint8_t *base = it.st.base;
+    it.tile = pl.pass2 && pl.db.tiles_ok && !ctx->force_global_deblock && !ctx->force_strip_deblock;
+    if (it.tile) {
+      const StripSide v{reinterpret_cast<const EdgeSeg *>(base + it.st.seg[0]),
+                        reinterpret_cast<const uint32_t *>(base + it.st.comp[0]),
+                        reinterpret_cast<const uint32_t *>(base + it.st.band[0])};
+      const StripSide h{reinterpret_cast<const EdgeSeg *>(base + it.st.seg[1]),
+                        reinterpret_cast<const uint32_t *>(base + it.st.comp[1]),
+                        reinterpret_cast<const uint32_t *>(base + it.st.band[1])};
+      tile_params.resize(tile_params.size() + tps);
+      const uint32_t c = fill_deblock_tile_params(tile_params.data() + tile_params.size() - tps, it.P, it.S,
+                                                  pl.lmcs ? pl.lut.as<uint16_t>() : nullptr, pl.deblock_bd, v, h,
+                                                  reinterpret_cast<const uint32_t *>(base + it.st.tile_bounds),
+                                                  pl.db.tb_off, pl.db.n_bands, pl.db.tiles_x, pl.db.tiles_y);
+      tile_first.push_back(tile_first.back() + c);
+    }
+    it.packed = pl.pass2 && pl.packed && !ctx->force_scalar;
+    it.variant = -1;
+    if (it.packed) {
+      Pass2Args a = pl.args;
+      bind_pass2(a, base, it.st, it.S, it.P);
+      uint32_t c = 0;
+      it.variant = pass2_packed_variant(a, pl.do_sao, pl.do_alf, &c);
+      if (p2_first[it.variant].empty()) p2_first[it.variant].push_back(0);
+      p2[it.variant].push_back(a);
+      p2_first[it.variant].push_back(p2_first[it.variant].back() + c);
+    }
+  }
+  // one upload of every batched launch's parameter table
+  std::vector<uint8_t> &b = ctx->batch_blob;
+  b.clear();
+  Blob blob{b};
+  const size_t off_tp = blob.put(tile_params.data(), tile_params.size());
+  const size_t off_tf = blob.put(tile_first.data(), tile_first.size() * sizeof(uint32_t));
+  size_t off_p2[8] = {0}, off_p2f[8] = {0};
+  for (int v = 0; v < 8; ++v)
+    if (!p2[v].empty()) {
+      off_p2[v] = blob.put(p2[v].data(), p2[v].size() * sizeof(Pass2Args));
+      off_p2f[v] = blob.put(p2_first[v].data(), p2_first[v].size() * sizeof(uint32_t));
+    }
+  H266_TRY(ctx->batch_side.ensure(b.size()));
+  H266_CUDA(cudaStreamWaitEvent(stream, ctx->batch_done, 0));  // earlier batches read batch_side (any stream)
+  H266_CUDA(cudaEventSynchronize(ctx->batch_staged));         // the previous upload has read the staging buffer
+  H266_TRY(ctx->batch_stage.ensure(b.size()));
+  std::memcpy(ctx->batch_stage.ptr, b.data(), b.size());
+  H266_CUDA(cudaMemcpyAsync(ctx->batch_side.ptr, ctx->batch_stage.ptr, b.size(), cudaMemcpyHostToDevice, stream));
+  H266_CUDA(cudaEventRecord(ctx->batch_staged, stream));
+  const uint8_t *dside = ctx->batch_side.as<uint8_t>();
+  // deblocking: per picture where the tile kernel does not apply, then one batched launch
+  for (uint32_t i = 0; i < n; ++i) {
+    const h266_chain_plan &pl = *plans[i];
+    Item &it = items[i];
+    if (it.tile) continue;
+    const uint16_t *lut = pl.lmcs ? pl.lut.as<uint16_t>() : nullptr;
+    if (pl.pass2) H266_TRY(run_deblock(ctx, stream, it.st.base, it.st, pl.db, it.P, it.S, lut, pl.deblock_bd));
+    else H266_TRY(run_deblock(ctx, stream, it.st.base, it.st, pl.db, it.P, it.P, lut, pl.deblock_bd));
+  }
+  if (tile_first.size() > 1) {
+    Prof pf(ctx, stream, H266_PROF_DEBLOCK);
+    H266_TRY(launch_deblock_tiles_batch(stream, dside + off_tp, reinterpret_cast<const uint32_t *>(dside + off_tf),
+                                        (int)tile_first.size() - 1, tile_first.back(), &ctx->launches));
+  }
+  // SAO / ALF: per picture where the packed kernel does not apply, then one launch per variant
+  for (uint32_t i = 0; i < n; ++i) {
+    const h266_chain_plan &pl = *plans[i];
+    Item &it = items[i];
+    if (!pl.pass2 || it.packed) continue;
+    H266_TRY(run_pass2(ctx, stream, pl.args, pl.do_sao, pl.do_alf, pl.packed, it.st.base, it.st, it.S, it.P));
+  }
+  for (int v = 0; v < 8; ++v)
+    if (!p2[v].empty()) {
+      Prof pf(ctx, stream, H266_PROF_SAO_ALF);
+      H266_TRY(launch_pass2_packed_batch(stream, v, reinterpret_cast<const Pass2Args *>(dside + off_p2[v]),
+                                         reinterpret_cast<const uint32_t *>(dside + off_p2f[v]), (int)p2[v].size(),
+                                         p2_first[v].back(), &ctx->launches));
+    }
+  H266_CUDA(cudaEventRecord(ctx->batch_done, stream));
+  return H266_OK;
 }
 
 int h266_chain_plan_destroy(h266_chain_plan *plan) {

@@ -1540,11 +1540,20 @@ __device__ __forceinline__ void run_tile_pass(const TileParams &a, uint16_t *sm,
   }
 }
 
-__global__ void __launch_bounds__(kTileThreads, 4) k_deblock_tiles(TileParams a) {
+struct TileShared {
+  uint32_t list_y[2][kTileListY], list_c[2][2][kTileListC];
+  uint32_t off[2][3][kTileBands + 1], lo[2][3][kTileBands];
+};
+
+// Tile t of the picture whose parameters are `a`.
+__device__ __forceinline__ void deblock_tile(const TileParams &a, int t) {
   extern __shared__ __align__(16) uint16_t sm[];
-  __shared__ uint32_t s_list_y[2][kTileListY], s_list_c[2][2][kTileListC];
-  __shared__ uint32_t s_off[2][3][kTileBands + 1], s_lo[2][3][kTileBands];
-  const int t = blockIdx.x, tx = t % (int)a.tiles_x, ty = t / (int)a.tiles_x;
+  __shared__ TileShared ts;
+  auto &s_list_y = ts.list_y;
+  auto &s_list_c = ts.list_c;
+  auto &s_off = ts.off;
+  auto &s_lo = ts.lo;
+  const int tx = t % (int)a.tiles_x, ty = t / (int)a.tiles_x;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, n_warps = blockDim.x >> 5;
   // Warps 0-5 first read the component ranges of both passes (one warp per
   // pass and plane), then every thread loads the planes' regions.
@@ -1576,6 +1585,29 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_deblock_tiles(TileParams a)
     const int iw = min(x0 + tp, a.dst[p].w) - x0, ih = min(y0 + tp, a.dst[p].h) - y0;
     if (iw > 0 && ih > 0 && v.ww > 0 && v.wh > 0) store_window(v.s, v.ld, a.dst[p], v.ox, v.oy, x0, y0, iw, ih);
   }
+}
+
+__global__ void __launch_bounds__(kTileThreads, 4) k_deblock_tiles(const __grid_constant__ TileParams a) {
+  deblock_tile(a, blockIdx.x);
+}
+
+// Many pictures in one grid: CTAs [first[i], first[i + 1]) are the tiles of
+// picture i, whose parameters are params[i].
+__global__ void __launch_bounds__(kTileThreads, 4) k_deblock_tiles_batch(const TileParams *__restrict__ params,
+                                                                         const uint32_t *__restrict__ first, int n) {
+  __shared__ TileParams s_params;  // the picture's parameters, read once per CTA
+  int lo = 0, hi = n;               // first[lo] <= blockIdx.x < first[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (first[mid] <= blockIdx.x) lo = mid;
+    else hi = mid;
+  }
+  static_assert(sizeof(TileParams) % 4 == 0, "word copy");
+  const uint32_t *src = reinterpret_cast<const uint32_t *>(params + lo);
+  uint32_t *dst = reinterpret_cast<uint32_t *>(&s_params);
+  for (int i = threadIdx.x; i < (int)(sizeof(TileParams) / 4); i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+  deblock_tile(s_params, (int)(blockIdx.x - first[lo]));
 }
 
 size_t rows_smem(const DPlane &p) { return (size_t)4 * row_pitch(p.w) * 2; }
@@ -1649,10 +1681,12 @@ int launch_deblock_strips(cudaStream_t st, const DPlane src[3], const DPlane dst
   return H266_OK;
 }
 
-int launch_deblock_tiles(cudaStream_t st, const DPlane src[3], const DPlane dst[3], const uint16_t *lut,
-                         int bit_depth, const StripSide &v, const StripSide &h, const uint32_t *tile_bounds,
-                         const uint32_t tb_off[2][3], const uint32_t n_bands[2][3], uint32_t tiles_x,
-                         uint32_t tiles_y, uint64_t *launches) {
+size_t deblock_tile_params_size() { return sizeof(TileParams); }
+
+uint32_t fill_deblock_tile_params(void *out, const DPlane src[3], const DPlane dst[3], const uint16_t *lut,
+                                  int bit_depth, const StripSide &v, const StripSide &h, const uint32_t *tile_bounds,
+                                  const uint32_t tb_off[2][3], const uint32_t n_bands[2][3], uint32_t tiles_x,
+                                  uint32_t tiles_y) {
   TileParams a;
   std::memset(&a, 0, sizeof a);
   for (int i = 0; i < 3; ++i) {
@@ -1672,9 +1706,28 @@ int launch_deblock_tiles(cudaStream_t st, const DPlane src[3], const DPlane dst[
   a.tiles_x = tiles_x;
   a.tiles_y = tiles_y;
   a.maxv = (1 << bit_depth) - 1;
-  const uint64_t n = (uint64_t)tiles_x * tiles_y;
+  std::memcpy(out, &a, sizeof a);
+  return tiles_x * tiles_y;
+}
+
+int launch_deblock_tiles(cudaStream_t st, const DPlane src[3], const DPlane dst[3], const uint16_t *lut,
+                         int bit_depth, const StripSide &v, const StripSide &h, const uint32_t *tile_bounds,
+                         const uint32_t tb_off[2][3], const uint32_t n_bands[2][3], uint32_t tiles_x,
+                         uint32_t tiles_y, uint64_t *launches) {
+  TileParams a;
+  const uint32_t n = fill_deblock_tile_params(&a, src, dst, lut, bit_depth, v, h, tile_bounds, tb_off, n_bands,
+                                              tiles_x, tiles_y);
   if (!n) return H266_OK;
-  k_deblock_tiles<<<(unsigned)n, kTileThreads, kTileSmem, st>>>(a);
+  k_deblock_tiles<<<n, kTileThreads, kTileSmem, st>>>(a);
+  H266_CUDA(cudaGetLastError());
+  ++*launches;
+  return H266_OK;
+}
+
+int launch_deblock_tiles_batch(cudaStream_t st, const void *d_params, const uint32_t *d_first, int n, uint32_t ctas,
+                               uint64_t *launches) {
+  if (!ctas || n <= 0) return H266_OK;
+  k_deblock_tiles_batch<<<ctas, kTileThreads, kTileSmem, st>>>(static_cast<const TileParams *>(d_params), d_first, n);
   H266_CUDA(cudaGetLastError());
   ++*launches;
   return H266_OK;

@@ -168,6 +168,16 @@ int launch_deblock_tiles(cudaStream_t st, const DPlane src[3], const DPlane dst[
                          int bit_depth, const StripSide &v, const StripSide &h, const uint32_t *tile_bounds,
                          const uint32_t tb_off[2][3], const uint32_t n_bands[2][3], uint32_t tiles_x,
                          uint32_t tiles_y, uint64_t *launches);
+// Batched tile kernel: fill_deblock_tile_params writes one picture's kernel
+// parameters (deblock_tile_params_size() bytes) to `out` and returns its CTA
+// count; CTAs [first[i], first[i + 1]) of the batched launch are picture i's.
+size_t deblock_tile_params_size();
+uint32_t fill_deblock_tile_params(void *out, const DPlane src[3], const DPlane dst[3], const uint16_t *lut,
+                                  int bit_depth, const StripSide &v, const StripSide &h, const uint32_t *tile_bounds,
+                                  const uint32_t tb_off[2][3], const uint32_t n_bands[2][3], uint32_t tiles_x,
+                                  uint32_t tiles_y);
+int launch_deblock_tiles_batch(cudaStream_t st, const void *d_params, const uint32_t *d_first, int n, uint32_t ctas,
+                               uint64_t *launches);
 int launch_deblock(cudaStream_t st, const DPlane planes[3], int bit_depth, const EdgeSeg *d_segs_v,
                    const uint32_t *d_comp_v, uint32_t n_comp_v, const EdgeSeg *d_segs_h, const uint32_t *d_comp_h,
                    uint32_t n_comp_h, uint64_t *launches);
@@ -230,5 +240,10 @@ struct Pass2Args {
 int launch_pass2(cudaStream_t st, const Pass2Args &a, bool do_sao, bool do_alf, uint64_t *launches);
 // Packed 16x2 form; requires bit_depth <= 14, 4:2:0 or 4:0:0, coefficients in [-128, 127].
 int launch_pass2_packed(cudaStream_t st, const Pass2Args &a, bool do_sao, bool do_alf, uint64_t *launches);
+// Batched packed pass: fills a's tile grid, returns the kernel variant (0..7)
+// and the picture's CTA count; pictures of one variant share a launch.
+int pass2_packed_variant(Pass2Args &a, bool do_sao, bool do_alf, uint32_t *ctas);
+int launch_pass2_packed_batch(cudaStream_t st, int variant, const Pass2Args *d_args, const uint32_t *d_first, int n,
+                              uint32_t ctas, uint64_t *launches);
 
 }  // namespace h266

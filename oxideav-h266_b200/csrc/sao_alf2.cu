@@ -150,13 +150,14 @@ __device__ __forceinline__ void classify(int sh, int sv, int sd0, int sd1, int a
   t_out = (uint8_t)((kTransposeTable >> ((dir1 * 2 + (dir2 >> 1)) * 2)) & 3);
 }
 
+// One tile (index `tile` of the picture's tile grid) of the pass.
 template <int W, bool DO_SAO, bool DO_ALF>
-__global__ void __launch_bounds__(NT) k_sao_alf_packed(const __grid_constant__ Pass2Args a) {
+__device__ __forceinline__ void sao_alf_tile(const Pass2Args &a, int tile) {
   using S = Smem<W>;
   extern __shared__ __align__(16) uint8_t smem_raw[];
   S &sm = *reinterpret_cast<S *>(smem_raw);
   const int tid = threadIdx.x;
-  const int tx = blockIdx.x % a.tiles_x, ty = blockIdx.x / a.tiles_x;
+  const int tx = tile % a.tiles_x, ty = tile / a.tiles_x;
   const int X0 = tx * W, Y0 = ty * TH;
   const int bd = a.bit_depth, maxv = (1 << bd) - 1;
   const int log2 = a.ctb_log2, ctb = 1 << log2;
@@ -459,6 +460,31 @@ __global__ void __launch_bounds__(NT) k_sao_alf_packed(const __grid_constant__ P
   }
 }
 
+template <int W, bool DO_SAO, bool DO_ALF>
+__global__ void __launch_bounds__(NT) k_sao_alf_packed(const __grid_constant__ Pass2Args a) {
+  sao_alf_tile<W, DO_SAO, DO_ALF>(a, blockIdx.x);
+}
+
+// Many pictures in one grid: CTAs [first[i], first[i + 1]) are the tiles of
+// picture i, whose parameters are args[i].
+template <int W, bool DO_SAO, bool DO_ALF>
+__global__ void __launch_bounds__(NT, 3) k_sao_alf_packed_batch(const Pass2Args *__restrict__ args,
+                                                             const uint32_t *__restrict__ first, int n) {
+  __shared__ Pass2Args s_args;  // the picture's parameters, read once per CTA
+  int lo = 0, hi = n;            // first[lo] <= blockIdx.x < first[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (first[mid] <= blockIdx.x) lo = mid;
+    else hi = mid;
+  }
+  static_assert(sizeof(Pass2Args) % 4 == 0, "word copy");
+  const uint32_t *src = reinterpret_cast<const uint32_t *>(args + lo);
+  uint32_t *dst = reinterpret_cast<uint32_t *>(&s_args);
+  for (int i = threadIdx.x; i < (int)(sizeof(Pass2Args) / 4); i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+  sao_alf_tile<W, DO_SAO, DO_ALF>(s_args, (int)(blockIdx.x - first[lo]));
+}
+
 template <int W>
 int launch_w(cudaStream_t st, const Pass2Args &in, bool do_sao, bool do_alf) {
   static_assert(sizeof(Smem<W>) <= 48 * 1024, "fits the default dynamic shared-memory limit");
@@ -479,6 +505,35 @@ int launch_w(cudaStream_t st, const Pass2Args &in, bool do_sao, bool do_alf) {
 }
 
 }  // namespace
+
+int pass2_packed_variant(Pass2Args &a, bool do_sao, bool do_alf, uint32_t *ctas) {
+  const int W = a.ctb_log2 >= 6 ? 64 : 32;
+  a.tiles_x = (a.ext_w + W - 1) / W;
+  a.tiles_y = (a.ext_h + TH - 1) / TH;
+  *ctas = a.ext_w > 0 && a.ext_h > 0 ? (uint32_t)(a.tiles_x * a.tiles_y) : 0;
+  return (W == 64 ? 4 : 0) + (do_sao ? 2 : 0) + (do_alf ? 1 : 0);
+}
+
+int launch_pass2_packed_batch(cudaStream_t st, int variant, const Pass2Args *d_args, const uint32_t *d_first, int n,
+                              uint32_t ctas, uint64_t *launches) {
+  if (!ctas || n <= 0) return H266_OK;
+  auto go = [&](auto kern, size_t shm) -> int {
+    kern<<<ctas, NT, shm, st>>>(d_args, d_first, n);
+    H266_CUDA(cudaGetLastError());
+    ++*launches;
+    return H266_OK;
+  };
+  switch (variant) {
+    case 7: return go(k_sao_alf_packed_batch<64, true, true>, sizeof(Smem<64>));
+    case 6: return go(k_sao_alf_packed_batch<64, true, false>, sizeof(Smem<64>));
+    case 5: return go(k_sao_alf_packed_batch<64, false, true>, sizeof(Smem<64>));
+    case 4: return go(k_sao_alf_packed_batch<64, false, false>, sizeof(Smem<64>));
+    case 3: return go(k_sao_alf_packed_batch<32, true, true>, sizeof(Smem<32>));
+    case 2: return go(k_sao_alf_packed_batch<32, true, false>, sizeof(Smem<32>));
+    case 1: return go(k_sao_alf_packed_batch<32, false, true>, sizeof(Smem<32>));
+    default: return go(k_sao_alf_packed_batch<32, false, false>, sizeof(Smem<32>));
+  }
+}
 
 int launch_pass2_packed(cudaStream_t st, const Pass2Args &a, bool do_sao, bool do_alf, uint64_t *launches) {
   if (a.ext_w <= 0 || a.ext_h <= 0) return H266_OK;

@@ -32,7 +32,8 @@ EXPORTS = [
     "h266_ctx_kernel_launches", "h266_derive_lmcs", "h266_lmcs_inverse_map_luma", "h266_apply_deblocking_clipped",
     "h266_apply_sao_clipped", "h266_apply_alf_clipped", "h266_apply_in_loop_filters",
     "h266_apply_in_loop_filters_batch", "h266_ctx_set_profiling", "h266_ctx_profile", "h266_chain_plan_create",
-    "h266_chain_plan_execute", "h266_chain_plan_destroy", "h266_apply_in_loop_filters_noalloc",
+    "h266_chain_plan_execute", "h266_chain_plan_execute_batch", "h266_chain_plan_destroy",
+    "h266_apply_in_loop_filters_noalloc",
 ]
 PROF_FAMILIES = ("lmcs", "deblock", "sao_alf", "copy")
 
@@ -68,6 +69,7 @@ def lib():
         L.h266_ctx_profile.argtypes = [vp, vp, vp]
         L.h266_chain_plan_create.argtypes = [vp, vp, vp, C.POINTER(vp)]
         L.h266_chain_plan_execute.argtypes = [vp, vp, vp]
+        L.h266_chain_plan_execute_batch.argtypes = [vp, u32, vp, vp]
         L.h266_chain_plan_destroy.argtypes = [vp]
         L.h266_apply_in_loop_filters_noalloc.argtypes = [vp, vp, vp]
         _LIB = L
@@ -179,6 +181,13 @@ class Context:
         cp = pic.to_ctypes()
         a, keep = fa.to_ctypes()
         _check(lib().h266_apply_in_loop_filters(self._h, C.byref(cp), C.byref(a)))
+
+    def execute_plans(self, plans, pics):
+        """h266_chain_plan_execute_batch: plans[i] on device picture pics[i], batched launches."""
+        cps = [p.to_ctypes() for p in pics]
+        P = (C.c_void_p * len(plans))(*[pl._h.value for pl in plans])
+        Q = (C.c_void_p * len(pics))(*[C.addressof(c) for c in cps])
+        _check(lib().h266_chain_plan_execute_batch(self._h, len(plans), P, Q))
 
     def apply_in_loop_filters_batch(self, pics, fas):
         cps = [p.to_ctypes() for p in pics]

@@ -226,6 +226,42 @@ def test_resident_plan_matches_direct_chain(ctx):
     plan.close()
 
 
+def _deblock_only(seed):
+    pic, fa = W.stress_workload(seed)
+    fa.sao = None
+    fa.alf = None
+    return pic, fa
+
+
+def test_plan_batch_matches_oracle_on_mixed_pictures(ctx):
+    """One batched execution over pictures of different sizes, CTB sizes, bit
+    depths and deblocking paths (tile kernel, strip kernels for chained
+    edges, in place without SAO / ALF), twice in a row on fresh samples."""
+    makers = [lambda: small_c2(40), lambda: WORKLOADS["ctb64_8bit"](41), lambda: WORKLOADS["c1"](42),
+              lambda: WORKLOADS["odd_stride"](43), lambda: WORKLOADS["stress"](44),
+              lambda: WORKLOADS["stress_dual"](45), lambda: _deblock_only(46), lambda: small_c2(47)]
+    items = [m() for m in makers]
+    plans = [ctx.plan(p, f) for p, f in items]
+    wants = []
+    for p, f in items:
+        w = p.copy()
+        oracle.apply_in_loop_filters(w, f)
+        wants.append(w)
+    try:
+        for rnd in range(2):
+            devs = [native.DevicePicture.from_host(p) for p, _ in items]
+            import torch
+
+            torch.cuda.synchronize()
+            ctx.execute_plans(plans, devs)
+            ctx.synchronize()
+            for i, (d, w) in enumerate(zip(devs, wants)):
+                assert_same(d.to_host(), w, f"plan batch round {rnd} picture {i}")
+    finally:
+        for pl in plans:
+            pl.close()
+
+
 def test_profiling_counts_every_family(ctx):
     pic, fa = small_c2(22)
     ctx.set_profiling(True)
