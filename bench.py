@@ -164,6 +164,85 @@ def cpu_baseline(items, threads: int, min_seconds: float = 10.0):
                       f"one picture per thread, {dt:.1f} s wall"}
 
 
+# Served mix: (width, height, ctb_log2, fps, streams), 10-bit 4:2:0, config-1 content
+SERVED_MIX = ((832, 480, 6, 60, 12), (1920, 1080, 7, 60, 14), (3840, 2160, 7, 30, 6))
+SERVED_RING = 3  # pictures (each with its own plan) in flight per stream at most
+
+
+def run_served(ctx, local_rank, seconds: float, rates=(1, 4)):
+    """Continuous-batching server vs plain per-picture launches on Poisson
+    arrivals from the stream mix; latency from each picture's scheduled
+    arrival to its completion."""
+    import random
+
+    import numpy as np
+    import torch
+
+    from oxideav_h266_b200 import native
+    from oxideav_h266_b200 import workloads as W
+
+    streams = []
+    for k, (w, h, ctb, fps, n) in enumerate(SERVED_MIX):
+        for j in range(n):
+            pic, fa = W.make_workload(9000 + 100 * k + j, w, h, 10, ctb)
+            ring = []
+            for r in range(SERVED_RING):
+                plan, dev = ctx.plan(pic, fa), native.DevicePicture.from_host(pic, local_rank)
+                ring.append((plan, dev, dev.to_ctypes()))  # ctypes picture built once
+            streams.append({"fps": fps, "px": w * h, "ring": ring})
+    torch.cuda.synchronize()
+    L = native.lib()
+
+    def serve_once(srv, x, dur):
+        """Poisson arrivals at x times the nominal rates for `dur` seconds,
+        replayed by the library's native trace player."""
+        rng = random.Random(1234 + x)
+        arrivals = []
+        for si, st in enumerate(streams):
+            t = rng.expovariate(st["fps"] * x)
+            while t < dur:
+                arrivals.append((t, si))
+                t += rng.expovariate(st["fps"] * x)
+        arrivals.sort()
+        plans, pics, times, after, px = [], [], [], [], 0
+        last = [[-1] * SERVED_RING for _ in streams]  # request that last used each ring slot
+        nxt = [0] * len(streams)
+        for i, (t, si) in enumerate(arrivals):
+            k = nxt[si]
+            nxt[si] = (k + 1) % SERVED_RING
+            plan, _, cp = streams[si]["ring"][k]
+            plans.append(plan)
+            pics.append(cp)
+            times.append(t)
+            after.append(last[si][k])  # that picture buffer must be free again
+            last[si][k] = i
+            px += streams[si]["px"]
+        r0, b0 = srv.stats()
+        t0 = time.perf_counter()
+        lat = srv.replay(plans, pics, times, after)
+        wall = time.perf_counter() - t0
+        r1, b1 = srv.stats()
+        return {"requests": len(plans), "batches": int(b1 - b0),
+                "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                "max_ms": round(float(lat.max()), 3), "mpx_per_s": round(px / wall / 1e6, 1)}
+
+    nominal_mpx = sum(st["fps"] * st["px"] for st in streams) / 1e6
+    out = {"streams": len(streams), "mix": "12x 832x480@60, 14x 1920x1080@60, 6x 3840x2160@30, 10-bit",
+           "nominal_mpx_per_s": round(nominal_mpx, 1), "seconds": seconds, "ring_per_stream": SERVED_RING,
+           "latency": "scheduled arrival to completion"}
+    for mode, max_batch in (("batched", 64), ("plain", 1)):
+        with native.Server(local_rank, max_batch=max_batch, memory_budget=40 << 30) as srv:
+            warm = [srv.submit(plan, dev) for st in streams for plan, dev, _ in st["ring"]]
+            for tk in warm:
+                srv.wait(tk)
+            serve_once(srv, rates[0], 0.5)  # discarded warm-up run
+            out[mode] = {f"{x}x": serve_once(srv, x, seconds) for x in rates}
+    for st in streams:
+        for plan, _, _ in st["ring"]:
+            plan.close()
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -310,6 +389,10 @@ def run_ours(args, rank, world, local_rank):
                "path": "h266_apply_in_loop_filters_batch per step, H266_MEM_HOST pinned planes, side information "
                        "built from the CU lists in every call"}
 
+    served = None
+    if rank == 0 and world == 1 and args.served_seconds > 0:
+        served = run_served(ctx, local_rank, args.served_seconds)
+
     cpu = None
     if rank == 0 and world == 1:
         cpu = cpu_baseline(items, os.cpu_count() or 1)
@@ -322,7 +405,8 @@ def run_ours(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic (seeded 1080p config generator)",
             "config": workload_config(args.batch, world),
-            "roofline": roofline, "plain": plain, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "roofline": roofline, "plain": plain, "served": served, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": int(launches),
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
@@ -374,6 +458,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--served-seconds", type=float, default=2.0,
+                    help="seconds of Poisson arrivals per served measurement (0: skip)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

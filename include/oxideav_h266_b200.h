@@ -340,6 +340,33 @@ int h266_chain_plan_execute_batch(h266_ctx *ctx, uint32_t n, h266_chain_plan *co
                                   h266_picture *const *pics);
 int h266_chain_plan_destroy(h266_chain_plan *plan);
 
+/* Served filter chain: a request loop for many concurrent streams.  No
+ * counterpart in the crate, which filters one picture per call on the
+ * decoding thread (src/stream.rs:768).  Callers (any thread) submit a plan and
+ * a device picture of its geometry; the server admits queued requests into a
+ * batch whenever one of its three batch slots is free and the requests in
+ * flight fit `memory_budget` (a request counts its picture's planes plus its
+ * plan's scratch planes; an idle server always admits one), and runs the
+ * batch as h266_chain_plan_execute_batch does on the slot's own stream, so
+ * batches overlap on the GPU.  max_batch = 1 gives plain per-picture launches.
+ * The server owns a context on `device`.  A picture must not be submitted
+ * again before its request completed.  wait blocks until the request is done
+ * and returns its status and its latency from submission to completion. */
+typedef struct h266_server h266_server;
+int h266_server_create(int device, uint32_t max_batch, uint64_t memory_budget, h266_server **out);
+int h266_server_submit(h266_server *server, h266_chain_plan *plan, h266_picture *pic, uint64_t *ticket);
+int h266_server_wait(h266_server *server, uint64_t ticket, double *latency_ms);
+int h266_server_stats(h266_server *server, uint64_t *requests, uint64_t *batches);
+/* Replays a request trace against the server from native threads: request i
+ * (plans[i] on pics[i]) is submitted arrival_s[i] seconds after the call
+ * starts (non-decreasing), and not before request after[i] (< i, or -1; NULL
+ * for none) has completed -- the caller's picture-buffer reuse.  Returns when
+ * every request is done, with latency_ms[i] = completion - scheduled arrival.
+ * For load tests of a serving configuration. */
+int h266_server_replay(h266_server *server, uint32_t n, h266_chain_plan *const *plans, h266_picture *const *pics,
+                       const double *arrival_s, const int32_t *after, double *latency_ms);
+int h266_server_destroy(h266_server *server); /* drains the queue first */
+
 /* ---- allocation-free chain ---------------------------------------------------
  * No counterpart in the reference.  The whole chain (as h266_apply_in_loop_filters)
  * on device planes, for callers that cannot call cudaMalloc at run time: code

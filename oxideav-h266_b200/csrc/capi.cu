@@ -2,12 +2,18 @@
 // packing and the per-filter / whole-chain entry points declared in
 // include/oxideav_h266_b200.h.
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
+#include <unordered_map>
+#include <unordered_set>
 
 #include "fixed_filters.h"
 #include "internal.h"
@@ -121,6 +127,30 @@ struct Lane {
 };
 
 struct Prep;  // host-side preparation of one picture's chain call
+
+// Parameter tables of batched plan executions: assembled on the host,
+// uploaded once per batch through pinned staging.
+struct BatchBufs {
+  std::vector<uint8_t> blob;
+  DevBuf side;
+  Staging stage;
+  cudaEvent_t staged = nullptr;  // the last upload has read the staging buffer
+  cudaEvent_t done = nullptr;    // the last batch that reads `side` has finished its launches
+  int init() {
+    if (!staged) H266_CUDA(cudaEventCreateWithFlags(&staged, cudaEventDisableTiming));
+    if (!done) H266_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+    return H266_OK;
+  }
+  void release() {
+    side.release();
+    if (stage.ptr) cudaFreeHost(stage.ptr);
+    stage.ptr = nullptr;
+    stage.cap = 0;
+    if (staged) cudaEventDestroy(staged);
+    if (done) cudaEventDestroy(done);
+    staged = done = nullptr;
+  }
+};
 }  // namespace h266
 
 struct h266_ctx {
@@ -137,12 +167,7 @@ struct h266_ctx {
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
   double prof_ms[H266_PROF_FAMILIES] = {0};
   uint64_t prof_n[H266_PROF_FAMILIES] = {0};
-  // batched plan executions: per-picture kernel parameters, uploaded per call
-  std::vector<uint8_t> batch_blob;
-  h266::DevBuf batch_side;
-  h266::Staging batch_stage;
-  cudaEvent_t batch_staged = nullptr;
-  cudaEvent_t batch_done = nullptr;  // last batched launch that reads batch_side
+  h266::BatchBufs batch;  // parameter tables of h266_chain_plan_execute_batch
   bool force_scalar = false;  // H266_FORCE_SCALAR_ALF=1: scalar SAO/ALF kernel (cross-checks)
   bool force_global_deblock = false;  // H266_FORCE_GLOBAL_DEBLOCK=1: deblocking on global memory (cross-checks)
   bool force_strip_deblock = false;   // H266_FORCE_STRIP_DEBLOCK=1: strip kernels instead of tiles (cross-checks)
@@ -841,10 +866,7 @@ int h266_ctx_destroy(h266_ctx *ctx) {
     cudaEventDestroy(e.second.first);
     cudaEventDestroy(e.second.second);
   }
-  ctx->batch_side.release();
-  if (ctx->batch_stage.ptr) cudaFreeHost(ctx->batch_stage.ptr);
-  if (ctx->batch_staged) cudaEventDestroy(ctx->batch_staged);
-  if (ctx->batch_done) cudaEventDestroy(ctx->batch_done);
+  ctx->batch.release();
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
   return H266_OK;
@@ -1145,9 +1167,10 @@ int h266_chain_plan_execute(h266_ctx *ctx, h266_chain_plan *plan, h266_picture *
                     plan->deblock_bd, P, S);
 }
 
-int h266_chain_plan_execute_batch(h266_ctx *ctx, uint32_t n, h266_chain_plan *const *plans,
-                                  h266_picture *const *pics) {
-  H266_TRY(check_ctx(ctx));
+}  // extern "C"
+
+namespace h266 {
+int check_plan_batch(h266_ctx *ctx, uint32_t n, h266_chain_plan *const *plans, h266_picture *const *pics) {
   if (n && (!plans || !pics)) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL batch arrays");
   for (uint32_t i = 0; i < n; ++i) {
     if (!plans[i]) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL plan in batch");
@@ -1157,11 +1180,15 @@ int h266_chain_plan_execute_batch(h266_ctx *ctx, uint32_t n, h266_chain_plan *co
       return set_error(H266_ERR_INVALID_ARGUMENT, "picture geometry differs from its plan");
     if (plans[i]->device != ctx->device) return set_error(H266_ERR_INVALID_ARGUMENT, "plan belongs to another device");
   }
+  return H266_OK;
+}
+
+// Queues a batch of plan executions on `stream` with its parameter tables in
+// `bb`; the caller has checked the batch and made the device current.
+int exec_plan_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, uint32_t n, h266_chain_plan *const *plans,
+                    h266_picture *const *pics) {
   if (!n) return H266_OK;
-  Guard g(ctx->device);
-  cudaStream_t stream = ctx->stream;
-  if (!ctx->batch_staged) H266_CUDA(cudaEventCreateWithFlags(&ctx->batch_staged, cudaEventDisableTiming));
-  if (!ctx->batch_done) H266_CUDA(cudaEventCreateWithFlags(&ctx->batch_done, cudaEventDisableTiming));
+  H266_TRY(bb.init());
   // Per picture: device views, and which part runs batched.
   struct Item {
     DPlane P[3], S[3];
@@ -1212,7 +1239,7 @@ int h266_chain_plan_execute_batch(h266_ctx *ctx, uint32_t n, h266_chain_plan *co
     }
   }
   // one upload of every batched launch's parameter table
-  std::vector<uint8_t> &b = ctx->batch_blob;
+  std::vector<uint8_t> &b = bb.blob;
   b.clear();
   Blob blob{b};
   const size_t off_tp = blob.put(tile_params.data(), tile_params.size());
@@ -1223,14 +1250,14 @@ int h266_chain_plan_execute_batch(h266_ctx *ctx, uint32_t n, h266_chain_plan *co
       off_p2[v] = blob.put(p2[v].data(), p2[v].size() * sizeof(Pass2Args));
       off_p2f[v] = blob.put(p2_first[v].data(), p2_first[v].size() * sizeof(uint32_t));
     }
-  H266_TRY(ctx->batch_side.ensure(b.size()));
-  H266_CUDA(cudaStreamWaitEvent(stream, ctx->batch_done, 0));  // earlier batches read batch_side (any stream)
-  H266_CUDA(cudaEventSynchronize(ctx->batch_staged));         // the previous upload has read the staging buffer
-  H266_TRY(ctx->batch_stage.ensure(b.size()));
-  std::memcpy(ctx->batch_stage.ptr, b.data(), b.size());
-  H266_CUDA(cudaMemcpyAsync(ctx->batch_side.ptr, ctx->batch_stage.ptr, b.size(), cudaMemcpyHostToDevice, stream));
-  H266_CUDA(cudaEventRecord(ctx->batch_staged, stream));
-  const uint8_t *dside = ctx->batch_side.as<uint8_t>();
+  H266_TRY(bb.side.ensure(b.size()));
+  H266_CUDA(cudaStreamWaitEvent(stream, bb.done, 0));  // earlier batches read bb.side (any stream)
+  H266_CUDA(cudaEventSynchronize(bb.staged));         // the previous upload has read the staging buffer
+  H266_TRY(bb.stage.ensure(b.size()));
+  std::memcpy(bb.stage.ptr, b.data(), b.size());
+  H266_CUDA(cudaMemcpyAsync(bb.side.ptr, bb.stage.ptr, b.size(), cudaMemcpyHostToDevice, stream));
+  H266_CUDA(cudaEventRecord(bb.staged, stream));
+  const uint8_t *dside = bb.side.as<uint8_t>();
   // deblocking: per picture where the tile kernel does not apply, then one batched launch
   for (uint32_t i = 0; i < n; ++i) {
     const h266_chain_plan &pl = *plans[i];
@@ -1259,8 +1286,20 @@ int h266_chain_plan_execute_batch(h266_ctx *ctx, uint32_t n, h266_chain_plan *co
                                          reinterpret_cast<const uint32_t *>(dside + off_p2f[v]), (int)p2[v].size(),
                                          p2_first[v].back(), &ctx->launches));
     }
-  H266_CUDA(cudaEventRecord(ctx->batch_done, stream));
+  H266_CUDA(cudaEventRecord(bb.done, stream));
   return H266_OK;
+}
+}  // namespace h266
+
+extern "C" {
+
+int h266_chain_plan_execute_batch(h266_ctx *ctx, uint32_t n, h266_chain_plan *const *plans,
+                                  h266_picture *const *pics) {
+  H266_TRY(check_ctx(ctx));
+  H266_TRY(check_plan_batch(ctx, n, plans, pics));
+  if (!n) return H266_OK;
+  Guard g(ctx->device);
+  return exec_plan_batch(ctx, ctx->batch, ctx->stream, n, plans, pics);
 }
 
 int h266_chain_plan_destroy(h266_chain_plan *plan) {
@@ -1270,6 +1309,317 @@ int h266_chain_plan_destroy(h266_chain_plan *plan) {
   plan->lut.release();
   for (auto &b : plan->scratch) b.release();
   delete plan;
+  return H266_OK;
+}
+
+}  // extern "C"
+
+// ======================================================================= served filter chain
+//
+// A request loop for many concurrent streams: callers submit (plan, device
+// picture) requests from any thread; a dispatcher thread admits the queued
+// requests into a batch as soon as one of kServerSlots batch slots is free and
+// the device-memory budget allows, and queues the batch (one batched
+// execution, h266_chain_plan_execute_batch's path) on that slot's stream.
+// Batches of different slots overlap on the GPU, so requests that arrive while
+// others are running start without waiting for them (continuous batching).
+// A completion thread waits for the batches in order and records each
+// request's latency from submission to completion.  max_batch = 1 gives plain
+// per-picture launches of the same kernels.
+namespace {
+
+constexpr int kServerSlots = 3;
+using Clock = std::chrono::steady_clock;
+
+struct ServerReq {
+  uint64_t ticket;
+  h266_chain_plan *plan;
+  h266_picture pic;
+  uint64_t bytes;
+  Clock::time_point t0;
+};
+
+struct ServerSlot {
+  h266::BatchBufs bb;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  bool busy = false;
+};
+
+struct ServerFlight {
+  std::vector<ServerReq> reqs;
+  int slot;
+  uint64_t bytes;
+  int rc;
+  std::string msg;
+};
+
+struct ServerResult {
+  int rc;
+  double ms;
+  std::string msg;
+};
+
+}  // namespace
+
+struct h266_server {
+  h266_ctx *ctx = nullptr;  // the server's own context, used by the dispatcher thread only
+  uint32_t max_batch = 1;
+  uint64_t budget = 0;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_flight, cv_done;
+  std::deque<ServerReq> queue;
+  std::deque<ServerFlight> flights;
+  ServerSlot slots[kServerSlots];
+  std::unordered_map<uint64_t, ServerResult> results;
+  std::unordered_set<uint64_t> pending;
+  uint64_t next_ticket = 1, inflight = 0, batches = 0, requests = 0;
+  bool stop = false, dispatcher_done = false;
+  std::thread dispatcher, completer;
+};
+
+namespace {
+
+int free_slot(const h266_server *s) {
+  for (int i = 0; i < kServerSlots; ++i)
+    if (!s->slots[i].busy) return i;
+  return -1;
+}
+
+void server_dispatch(h266_server *s) {
+  cudaSetDevice(s->ctx->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  for (;;) {
+    s->cv_work.wait(lk, [&] { return (s->stop && s->queue.empty()) || (!s->queue.empty() && free_slot(s) >= 0); });
+    if (s->queue.empty()) break;  // stopping and drained
+    const int slot = free_slot(s);
+    // admit in arrival order up to max_batch and the memory budget (an idle
+    // server always admits the first request)
+    std::vector<ServerReq> take;
+    uint64_t bytes = 0;
+    while (!s->queue.empty() && take.size() < s->max_batch) {
+      const ServerReq &r = s->queue.front();
+      if ((s->inflight > 0 || !take.empty()) && s->inflight + bytes + r.bytes > s->budget) break;
+      bytes += r.bytes;
+      take.push_back(r);
+      s->queue.pop_front();
+    }
+    if (take.empty()) {  // over budget: wait for a completion
+      s->cv_work.wait(lk);
+      continue;
+    }
+    s->slots[slot].busy = true;
+    s->inflight += bytes;
+    lk.unlock();
+    std::vector<h266_chain_plan *> plans(take.size());
+    std::vector<h266_picture *> pics(take.size());
+    for (size_t i = 0; i < take.size(); ++i) {
+      plans[i] = take[i].plan;
+      pics[i] = &take[i].pic;
+    }
+    ServerSlot &sl = s->slots[slot];
+    int rc = exec_plan_batch(s->ctx, sl.bb, sl.stream, (uint32_t)take.size(), plans.data(), pics.data());
+    std::string msg = rc == H266_OK ? std::string() : std::string(h266_last_error());
+    if (cudaEventRecord(sl.done, sl.stream) != cudaSuccess && rc == H266_OK) {
+      rc = H266_ERR_CUDA;
+      msg = "cudaEventRecord";
+    }
+    lk.lock();
+    s->flights.push_back(ServerFlight{std::move(take), slot, bytes, rc, msg});
+    ++s->batches;
+    s->cv_flight.notify_one();
+  }
+  s->dispatcher_done = true;
+  s->cv_flight.notify_all();
+}
+
+void server_complete(h266_server *s) {
+  cudaSetDevice(s->ctx->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  for (;;) {
+    s->cv_flight.wait(lk, [&] { return !s->flights.empty() || s->dispatcher_done; });
+    if (s->flights.empty()) break;
+    ServerFlight f = std::move(s->flights.front());
+    s->flights.pop_front();
+    lk.unlock();
+    const cudaError_t e = cudaEventSynchronize(s->slots[f.slot].done);
+    const Clock::time_point t1 = Clock::now();
+    lk.lock();
+    for (const ServerReq &r : f.reqs) {
+      ServerResult res{f.rc, std::chrono::duration<double, std::milli>(t1 - r.t0).count(), f.msg};
+      if (res.rc == H266_OK && e != cudaSuccess) {
+        res.rc = H266_ERR_CUDA;
+        res.msg = std::string("batch: ") + cudaGetErrorString(e);
+      }
+      s->results[r.ticket] = res;
+      s->pending.erase(r.ticket);
+    }
+    s->requests += f.reqs.size();
+    s->slots[f.slot].busy = false;
+    s->inflight -= f.bytes;
+    s->cv_done.notify_all();
+    s->cv_work.notify_one();
+  }
+}
+
+uint64_t request_bytes(const h266_picture &p, const h266_chain_plan &pl) {
+  const h266_plane *q[3] = {&p.luma, &p.cb, &p.cr};
+  uint64_t b = 0;
+  for (const h266_plane *x : q) b += (uint64_t)x->width * x->height * 2;
+  return pl.pass2 ? 2 * b : b;  // the picture's planes, plus the plan's scratch planes
+}
+
+}  // namespace
+
+extern "C" {
+
+int h266_server_create(int device, uint32_t max_batch, uint64_t memory_budget, h266_server **out) {
+  if (!out) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL out");
+  *out = nullptr;
+  if (max_batch == 0) return set_error(H266_ERR_INVALID_ARGUMENT, "max_batch must be at least 1");
+  h266_ctx *ctx = nullptr;
+  H266_TRY(h266_ctx_create(device, &ctx));
+  h266_server *s = new h266_server();
+  s->ctx = ctx;
+  s->max_batch = max_batch;
+  s->budget = memory_budget;
+  Guard g(device);
+  // Parameter tables sized for a full batch up front: growing them later
+  // would synchronise the device (and allocate pinned memory) mid-run.
+  const size_t reserve = std::max<size_t>((size_t)max_batch * (deblock_tile_params_size() + sizeof(Pass2Args) + 64),
+                                          256 * 1024);
+  for (ServerSlot &sl : s->slots) {
+    cudaError_t e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
+    int rc = e == cudaSuccess ? sl.bb.init() : H266_OK;
+    if (e == cudaSuccess && rc == H266_OK) rc = sl.bb.side.ensure(reserve);
+    if (e == cudaSuccess && rc == H266_OK) rc = sl.bb.stage.ensure(reserve);
+    if (e != cudaSuccess || rc != H266_OK) {
+      h266_server_destroy(s);
+      return e != cudaSuccess ? cuda_error(e, "h266_server_create") : rc;
+    }
+    sl.bb.blob.reserve(reserve);
+  }
+  s->dispatcher = std::thread(server_dispatch, s);
+  s->completer = std::thread(server_complete, s);
+  *out = s;
+  return H266_OK;
+}
+
+int h266_server_submit(h266_server *s, h266_chain_plan *plan, h266_picture *pic, uint64_t *ticket) {
+  if (!s || !ticket) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL server or ticket");
+  H266_TRY(check_plan_batch(s->ctx, 1, &plan, &pic));
+  ServerReq r{0, plan, *pic, request_bytes(*pic, *plan), Clock::now()};
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->stop) return set_error(H266_ERR_INVALID_ARGUMENT, "server is stopping");
+  r.ticket = s->next_ticket++;
+  s->pending.insert(r.ticket);
+  s->queue.push_back(r);
+  *ticket = r.ticket;
+  s->cv_work.notify_one();
+  return H266_OK;
+}
+
+int h266_server_wait(h266_server *s, uint64_t ticket, double *latency_ms) {
+  if (!s) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL server");
+  std::unique_lock<std::mutex> lk(s->mu);
+  s->cv_done.wait(lk, [&] { return s->results.count(ticket) || !s->pending.count(ticket); });
+  auto it = s->results.find(ticket);
+  if (it == s->results.end()) return set_error(H266_ERR_INVALID_ARGUMENT, "unknown or already collected ticket");
+  const ServerResult r = it->second;
+  s->results.erase(it);
+  if (latency_ms) *latency_ms = r.ms;
+  if (r.rc != H266_OK) return set_error(r.rc, r.msg);
+  return H266_OK;
+}
+
+int h266_server_stats(h266_server *s, uint64_t *requests, uint64_t *batches) {
+  if (!s) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (requests) *requests = s->requests;
+  if (batches) *batches = s->batches;
+  return H266_OK;
+}
+
+int h266_server_replay(h266_server *s, uint32_t n, h266_chain_plan *const *plans, h266_picture *const *pics,
+                       const double *arrival_s, const int32_t *after, double *latency_ms) {
+  if (!s || (n && (!plans || !pics || !arrival_s || !latency_ms)))
+    return set_error(H266_ERR_INVALID_ARGUMENT, "NULL argument");
+  for (uint32_t i = 0; i < n; ++i) {
+    if (i && arrival_s[i] < arrival_s[i - 1]) return set_error(H266_ERR_INVALID_ARGUMENT, "arrivals not in order");
+    if (after && after[i] >= (int32_t)i) return set_error(H266_ERR_INVALID_ARGUMENT, "after[i] must precede i");
+  }
+  std::vector<uint64_t> tickets(n, 0);
+  std::vector<std::atomic<int>> state(n);  // 0 not submitted, 1 submitted, 2 done
+  for (auto &x : state) x.store(0);
+  std::vector<Clock::time_point> due(n);
+  std::atomic<uint32_t> submitted{0};
+  std::atomic<int> first_rc{H266_OK};
+  std::string first_msg;
+  std::mutex msg_mu;
+  // completions in submission order on a second thread
+  std::thread collector([&] {
+    for (uint32_t i = 0; i < n; ++i) {
+      while (submitted.load(std::memory_order_acquire) <= i) {
+        if (first_rc.load() != H266_OK && submitted.load() <= i) return;
+        std::this_thread::yield();
+      }
+      double ms = 0;
+      const int rc = h266_server_wait(s, tickets[i], &ms);
+      latency_ms[i] = std::chrono::duration<double, std::milli>(Clock::now() - due[i]).count();
+      if (rc != H266_OK && first_rc.load() == H266_OK) {
+        std::lock_guard<std::mutex> lk(msg_mu);
+        first_msg = h266_last_error();
+        first_rc.store(rc);
+      }
+      state[i].store(2, std::memory_order_release);
+    }
+  });
+  const Clock::time_point t0 = Clock::now();
+  int rc = H266_OK;
+  for (uint32_t i = 0; i < n; ++i) {
+    due[i] = t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(arrival_s[i]));
+    while (Clock::now() < due[i]) {
+    }
+    if (after && after[i] >= 0)
+      while (state[after[i]].load(std::memory_order_acquire) != 2) std::this_thread::yield();
+    rc = h266_server_submit(s, plans[i], pics[i], &tickets[i]);
+    if (rc != H266_OK) {
+      std::lock_guard<std::mutex> lk(msg_mu);
+      if (first_rc.load() == H266_OK) {
+        first_msg = h266_last_error();
+        first_rc.store(rc);
+      }
+      break;
+    }
+    state[i].store(1);
+    submitted.store(i + 1, std::memory_order_release);
+  }
+  collector.join();
+  if (first_rc.load() != H266_OK) return set_error(first_rc.load(), first_msg);
+  return H266_OK;
+}
+
+int h266_server_destroy(h266_server *s) {
+  if (!s) return H266_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  if (s->dispatcher.joinable()) s->dispatcher.join();
+  if (s->completer.joinable()) s->completer.join();
+  if (s->ctx) {
+    Guard g(s->ctx->device);
+    for (ServerSlot &sl : s->slots) {
+      if (sl.stream) cudaStreamSynchronize(sl.stream);
+      sl.bb.release();
+      if (sl.done) cudaEventDestroy(sl.done);
+      if (sl.stream) cudaStreamDestroy(sl.stream);
+    }
+    h266_ctx_destroy(s->ctx);
+  }
+  delete s;
   return H266_OK;
 }
 

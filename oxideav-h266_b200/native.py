@@ -33,7 +33,8 @@ EXPORTS = [
     "h266_apply_sao_clipped", "h266_apply_alf_clipped", "h266_apply_in_loop_filters",
     "h266_apply_in_loop_filters_batch", "h266_ctx_set_profiling", "h266_ctx_profile", "h266_chain_plan_create",
     "h266_chain_plan_execute", "h266_chain_plan_execute_batch", "h266_chain_plan_destroy",
-    "h266_apply_in_loop_filters_noalloc",
+    "h266_apply_in_loop_filters_noalloc", "h266_server_create", "h266_server_submit", "h266_server_wait",
+    "h266_server_stats", "h266_server_replay", "h266_server_destroy",
 ]
 PROF_FAMILIES = ("lmcs", "deblock", "sao_alf", "copy")
 
@@ -70,6 +71,12 @@ def lib():
         L.h266_chain_plan_create.argtypes = [vp, vp, vp, C.POINTER(vp)]
         L.h266_chain_plan_execute.argtypes = [vp, vp, vp]
         L.h266_chain_plan_execute_batch.argtypes = [vp, u32, vp, vp]
+        L.h266_server_create.argtypes = [i32, u32, u64, C.POINTER(vp)]
+        L.h266_server_submit.argtypes = [vp, vp, vp, C.POINTER(u64)]
+        L.h266_server_wait.argtypes = [vp, u64, C.POINTER(C.c_double)]
+        L.h266_server_stats.argtypes = [vp, C.POINTER(u64), C.POINTER(u64)]
+        L.h266_server_replay.argtypes = [vp, u32, vp, vp, vp, vp, vp]
+        L.h266_server_destroy.argtypes = [vp]
         L.h266_chain_plan_destroy.argtypes = [vp]
         L.h266_apply_in_loop_filters_noalloc.argtypes = [vp, vp, vp]
         _LIB = L
@@ -250,6 +257,74 @@ class ChainPlan:
         if self._h:
             lib().h266_chain_plan_destroy(self._h)
             self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """h266_server: continuous-batching request loop over resident plans.
+
+    submit() takes a ChainPlan and a DevicePicture of its geometry and returns
+    a ticket; wait(ticket) blocks until that request is done and returns its
+    latency in ms (submission to completion).  max_batch=1 gives plain
+    per-picture launches."""
+
+    def __init__(self, device: int = 0, max_batch: int = 32, memory_budget: int = 40 << 30):
+        h = C.c_void_p()
+        _check(lib().h266_server_create(device, max_batch, memory_budget, C.byref(h)))
+        self._h = h
+        self._keep = {}
+
+    def submit(self, plan: "ChainPlan", pic: "DevicePicture") -> int:
+        cp = pic.to_ctypes()
+        t = C.c_uint64()
+        _check(lib().h266_server_submit(self._h, plan._h, C.byref(cp), C.byref(t)))
+        self._keep[t.value] = (plan, pic)
+        return t.value
+
+    def wait(self, ticket: int) -> float:
+        ms = C.c_double()
+        try:
+            _check(lib().h266_server_wait(self._h, ticket, C.byref(ms)))
+        finally:
+            self._keep.pop(ticket, None)
+        return ms.value
+
+    def replay(self, plans, pics, arrival_s, after=None):
+        """h266_server_replay: submit request i at arrival_s[i] seconds (after
+        request after[i] completed, -1 for none) from native threads; returns
+        latency_ms per request (completion - scheduled arrival)."""
+        n = len(plans)
+        cps = [p.to_ctypes() if hasattr(p, "to_ctypes") else p for p in pics]
+        P = (C.c_void_p * n)(*[pl._h.value for pl in plans])
+        Q = (C.c_void_p * n)(*[C.addressof(c) for c in cps])
+        arr = np.ascontiguousarray(arrival_s, dtype=np.float64)
+        aft = None if after is None else np.ascontiguousarray(after, dtype=np.int32)
+        lat = np.zeros(n, dtype=np.float64)
+        _check(lib().h266_server_replay(self._h, n, P, Q, arr.ctypes.data, None if aft is None else aft.ctypes.data,
+                                        lat.ctypes.data))
+        return lat
+
+    def stats(self) -> tuple:
+        r, b = C.c_uint64(), C.c_uint64()
+        _check(lib().h266_server_stats(self._h, C.byref(r), C.byref(b)))
+        return r.value, b.value
+
+    def close(self):
+        if self._h:
+            lib().h266_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
     def __del__(self):
         try:
