@@ -169,7 +169,7 @@ SERVED_MIX = ((832, 480, 6, 60, 12), (1920, 1080, 7, 60, 14), (3840, 2160, 7, 30
 SERVED_RING = 3  # pictures (each with its own plan) in flight per stream at most
 
 
-def run_served(ctx, local_rank, seconds: float, rates=(1, 4)):
+def run_served(ctx, local_rank, seconds: float, rates=(1, 4, 8, 12)):
     """Continuous-batching server vs plain per-picture launches on Poisson
     arrivals from the stream mix; latency from each picture's scheduled
     arrival to its completion."""

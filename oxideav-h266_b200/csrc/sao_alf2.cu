@@ -30,17 +30,25 @@ constexpr int NT = 256;
 __device__ __forceinline__ int clampd(int v, int lo, int hi) { return min(max(v, lo), hi); }
 __device__ __forceinline__ int sgn(int v) { return (v > 0) - (v < 0); }
 
-struct SaoLocal {  // one component's SAO parameters of one CTB, plus its clip rectangle
-  int type, cls, band, off[4];
-  int rect[4];
+// One component's SAO parameters of one CTB in the form the per-sample step
+// needs: band offsets; for edge offset the offset per 2 + sign + sign (the
+// edgeIdx remap of eq. 154 folded in), the shared-memory offset of the first
+// neighbour (the second is its negation), and the rectangle of samples whose
+// two neighbours lie inside the picture and the clip rectangle.
+struct SaoLocal {
+  int type, band, bd_shift;
+  int off[4];   // band offset per band index 0..3 after the band position
+  int eo[5];    // edge offset per 2 + sign(c - a) + sign(c - b)
+  int nb;       // smem offset of the first neighbour (row pitch of the component's window)
+  int ex0, ey0, ex1, ey1;  // [ex0, ex1) x [ey0, ey1): both neighbours available
 };
 
 template <int W>
 struct Smem {
-  static constexpr int DLW = W + 12, DLH = TH + 8;  // deblocked luma [X0-6, X1+6) x [Y0-4, Y1+4)
+  static constexpr int DLW = W + 16, DLH = TH + 8;  // deblocked luma [X0-8, X1+8) x [Y0-4, Y1+4)
   static constexpr int SLW = W + 8, SLH = TH + 6;   // post-SAO luma [X0-4, X1+4) x [Y0-3, Y1+3)
   static constexpr int CW = W / 2 + 2, CH = TH / 2 + 2;  // 2x2 Laplacian cells
-  static constexpr int DCW = W / 2 + 12, DCH = TH / 2 + 6;  // deblocked chroma [x-6, x+6) x [y-3, y+3)
+  static constexpr int DCW = W / 2 + 16, DCH = TH / 2 + 6;  // deblocked chroma [x-8, x+8) x [y-3, y+3)
   static constexpr int SCW = W / 2 + 8, SCH = TH / 2 + 4;   // post-SAO chroma [x-4, x+4) x [y-2, y+2)
   alignas(16) uint16_t dL[DLH * DLW];
   alignas(16) uint16_t sL[SLH * SLW];
@@ -52,23 +60,63 @@ struct Smem {
   int any_sao[3];
 };
 
-// §8.8.4.2 for one sample; `at(dx, dy)` reads the pre-SAO plane.
-template <class At>
-__device__ __forceinline__ int sao_one(const SaoLocal &p, int x, int y, int pw, int ph, int maxv, int bd, At at) {
-  const int c = at(0, 0);
+// Fills one SaoLocal from the CTB's SAO parameters (src/sao.rs:504-626):
+// hPos / vPos of eq. 152 per class, and the clip rectangle `rect` (component
+// samples) intersected with the picture.
+__device__ __forceinline__ void sao_local(SaoLocal &s, const SaoCtbDev &p, int pitch, int rx0, int ry0, int rx1,
+                                          int ry1, int bd) {
+  s.type = p.type;
+  s.band = p.band_pos;
+  s.bd_shift = bd - 5;
+  for (int k = 0; k < 4; ++k) s.off[k] = p.off[k];
+  // edgeIdx = 2 + sign + sign, remapped 0 -> 1, 1 -> 2, 2 -> 0 (eq. 154); offset edgeIdx - 1
+  s.eo[0] = p.off[0];
+  s.eo[1] = p.off[1];
+  s.eo[2] = 0;
+  s.eo[3] = p.off[2];
+  s.eo[4] = p.off[3];
+  const int h0 = p.eo_class == 0 ? -1 : (p.eo_class == 1 ? 0 : (p.eo_class == 2 ? -1 : 1));
+  const int v0 = p.eo_class == 0 ? 0 : -1;
+  s.nb = v0 * pitch + h0;
+  const int ah = h0 < 0 ? -h0 : h0, av = v0 < 0 ? -v0 : v0;
+  s.ex0 = rx0 + ah;
+  s.ex1 = rx1 - ah;
+  s.ey0 = ry0 + av;
+  s.ey1 = ry1 - av;
+}
+
+// §8.8.4.2 for one sample at (x, y) whose pre-SAO value is *d (shared memory).
+__device__ __forceinline__ int sao_one(const SaoLocal &p, int x, int y, int maxv, const uint16_t *d) {
+  const int c = *d;
   if (p.type == 1) {
-    const int k = (((c >> (bd - 5)) & 31) - p.band) & 31;
+    const int k = ((c >> p.bd_shift) - p.band) & 31;
     return clampd(k < 4 ? c + p.off[k] : c, 0, maxv);
   }
-  const int h0 = p.cls == 0 ? -1 : (p.cls == 1 ? 0 : (p.cls == 2 ? -1 : 1));
-  const int v0 = p.cls == 0 ? 0 : -1;
-  const int x0 = max(0, p.rect[0]), y0 = max(0, p.rect[1]), x1 = min(pw, p.rect[2]), y1 = min(ph, p.rect[3]);
-  if (x + h0 < x0 || x - h0 < x0 || y + v0 < y0 || y - v0 < y0 || x + h0 >= x1 || x - h0 >= x1 || y + v0 >= y1 ||
-      y - v0 >= y1)
-    return clampd(c, 0, maxv);
-  int e = 2 + sgn(c - at(h0, v0)) + sgn(c - at(-h0, -v0));
-  if (e <= 2) e = e == 2 ? 0 : e + 1;
-  return clampd(e ? c + p.off[e - 1] : c, 0, maxv);
+  if (x < p.ex0 || x >= p.ex1 || y < p.ey0 || y >= p.ey1) return clampd(c, 0, maxv);
+  return clampd(c + p.eo[2 + sgn(c - d[p.nb]) + sgn(c - d[-p.nb])], 0, maxv);
+}
+
+// Copies the HH x WW window at (x0, y0) of plane P (coordinates clamped into
+// the plane) to dst with row pitch WW; whole 16-byte vectors when the window's
+// columns lie inside the plane and the plane is aligned.
+template <int WW, int HH>
+__device__ __forceinline__ void load_window(uint16_t *dst, const DPlane &P, int x0, int y0) {
+  static_assert(WW % 8 == 0, "whole vectors per row");
+  const bool vec = x0 >= 0 && x0 + WW <= P.w && (x0 & 7) == 0 && ((uintptr_t)P.s & 15) == 0 && (P.stride & 7) == 0;
+  if (vec) {
+    constexpr int NV = WW / 8;
+    for (int i = threadIdx.x; i < HH * NV; i += NT) {
+      const int r = i / NV, c = (i - r * NV) * 8;
+      const int gy = clampd(y0 + r, 0, P.h - 1);
+      *reinterpret_cast<uint4 *>(dst + r * WW + c) = *reinterpret_cast<const uint4 *>(P.s + (int64_t)gy * P.stride + x0 + c);
+    }
+  } else {
+    for (int i = threadIdx.x; i < HH * WW; i += NT) {
+      const int r = i / WW, c = i - r * WW;
+      const int gx = clampd(x0 + c, 0, P.w - 1), gy = clampd(y0 + r, 0, P.h - 1);
+      dst[i] = P.s[(int64_t)gy * P.stride + gx];
+    }
+  }
 }
 
 // Pair of samples (col, col + 1) of a shared-memory row; DC fixes the parity
@@ -184,21 +232,16 @@ __device__ __forceinline__ void sao_alf_tile(const Pass2Args &a, int tile) {
     const bool used = comp == 0 ? a.sao_luma : a.sao_chroma;
     if (DO_SAO && used && nx >= 0 && ny >= 0 && nx < a.w_ctbs && ny < a.h_ctbs) {
       const CtbDev &c = a.ctbs[ny * a.w_ctbs + nx];
-      const SaoCtbDev &p = c.sao[comp];
-      s.type = p.type;
-      s.cls = p.eo_class;
-      s.band = p.band_pos;
-      for (int k = 0; k < 4; ++k) s.off[k] = p.off[k];
       const int sw = comp ? 2 : 1;
+      const int cw = comp ? a.src[comp].w : a.src[0].w, ch = comp ? a.src[comp].h : a.src[0].h;
+      int q0 = 0, q1 = 0, q2 = cw, q3 = ch;  // clip rectangle in component samples, within the picture
       if (a.has_clip) {
-        s.rect[0] = c.rect[0] / sw;
-        s.rect[1] = c.rect[1] / sw;
-        s.rect[2] = (c.rect[2] + sw - 1) / sw;
-        s.rect[3] = (c.rect[3] + sw - 1) / sw;
-      } else {
-        s.rect[0] = s.rect[1] = 0;
-        s.rect[2] = s.rect[3] = 1 << 30;
+        q0 = max(q0, c.rect[0] / sw);
+        q1 = max(q1, c.rect[1] / sw);
+        q2 = min(q2, (c.rect[2] + sw - 1) / sw);
+        q3 = min(q3, (c.rect[3] + sw - 1) / sw);
       }
+      sao_local(s, c.sao[comp], comp ? S::DCW : S::DLW, q0, q1, q2, q3, bd);
     }
   }
   __syncthreads();
@@ -210,11 +253,7 @@ __device__ __forceinline__ void sao_alf_tile(const Pass2Args &a, int tile) {
 
   // ---- luma: deblocked samples with halo
   const DPlane LS = a.src[0], LD = a.dst[0];
-  for (int i = tid; i < S::DLH * S::DLW; i += NT) {
-    const int r = i / S::DLW, c = i - r * S::DLW;
-    const int gx = clampd(X0 - 6 + c, 0, LS.w - 1), gy = clampd(Y0 - 4 + r, 0, LS.h - 1);
-    sm.dL[i] = LS.s[(int64_t)gy * LS.stride + gx];
-  }
+  load_window<S::DLW, S::DLH>(sm.dL, LS, X0 - 8, Y0 - 4);
   __syncthreads();
   // ---- post-SAO luma, clamped into the fetch rectangle
   {
@@ -222,13 +261,12 @@ __device__ __forceinline__ void sao_alf_tile(const Pass2Args &a, int tile) {
     for (int i = tid; i < S::SLH * S::SLW; i += NT) {
       const int r = i / S::SLW, c = i - r * S::SLW;
       const int ax = clampd(X0 - 4 + c, rx0, rx1 - 1), ay = clampd(Y0 - 3 + r, ry0, ry1 - 1);
-      const int lr = ay - (Y0 - 4), lc = ax - (X0 - 6);
+      const int lr = ay - (Y0 - 4), lc = ax - (X0 - 8);
       const uint16_t *d = &sm.dL[lr * S::DLW + lc];
       int v = *d;
       if (any) {
         const SaoLocal &p = sm.sao[0][((ay >> log2) - ry + 1) * 3 + ((ax >> log2) - rx + 1)];
-        if (p.type)
-          v = sao_one(p, ax, ay, LS.w, LS.h, maxv, bd, [&](int dx, int dy) { return (int)d[dy * S::DLW + dx]; });
+        if (p.type) v = sao_one(p, ax, ay, maxv, d);
       }
       sm.sL[i] = (uint16_t)v;
     }
@@ -378,22 +416,17 @@ __device__ __forceinline__ void sao_alf_tile(const Pass2Args &a, int tile) {
     if (CS.w <= 0 || CS.h <= 0 || xc0 >= CS.w || yc0 >= CS.h) continue;
     const int cx0 = max(crx0, 0), cy0 = max(cry0, 0), cx1 = min(crx1, CS.w), cy1 = min(cry1, CS.h);
     __syncthreads();
-    for (int i = tid; i < S::DCH * S::DCW; i += NT) {
-      const int r = i / S::DCW, c = i - r * S::DCW;
-      const int gx = clampd(xc0 - 6 + c, 0, CS.w - 1), gy = clampd(yc0 - 3 + r, 0, CS.h - 1);
-      sm.dC[i] = CS.s[(int64_t)gy * CS.stride + gx];
-    }
+    load_window<S::DCW, S::DCH>(sm.dC, CS, xc0 - 8, yc0 - 3);
     __syncthreads();
     const bool any = sm.any_sao[comp] != 0;
     for (int i = tid; i < S::SCH * S::SCW; i += NT) {
       const int r = i / S::SCW, c = i - r * S::SCW;
       const int ax = clampd(xc0 - 4 + c, cx0, cx1 - 1), ay = clampd(yc0 - 2 + r, cy0, cy1 - 1);
-      const uint16_t *d = &sm.dC[(ay - (yc0 - 3)) * S::DCW + ax - (xc0 - 6)];
+      const uint16_t *d = &sm.dC[(ay - (yc0 - 3)) * S::DCW + ax - (xc0 - 8)];
       int v = *d;
       if (any) {
         const SaoLocal &p = sm.sao[comp][(((ay * 2) >> log2) - ry + 1) * 3 + (((ax * 2) >> log2) - rx + 1)];
-        if (p.type)
-          v = sao_one(p, ax, ay, CS.w, CS.h, maxv, bd, [&](int dx, int dy) { return (int)d[dy * S::DCW + dx]; });
+        if (p.type) v = sao_one(p, ax, ay, maxv, d);
       }
       sm.sC[i] = (uint16_t)v;
     }
@@ -461,14 +494,14 @@ __device__ __forceinline__ void sao_alf_tile(const Pass2Args &a, int tile) {
 }
 
 template <int W, bool DO_SAO, bool DO_ALF>
-__global__ void __launch_bounds__(NT) k_sao_alf_packed(const __grid_constant__ Pass2Args a) {
+__global__ void __launch_bounds__(NT, 4) k_sao_alf_packed(const __grid_constant__ Pass2Args a) {
   sao_alf_tile<W, DO_SAO, DO_ALF>(a, blockIdx.x);
 }
 
 // Many pictures in one grid: CTAs [first[i], first[i + 1]) are the tiles of
 // picture i, whose parameters are args[i].
 template <int W, bool DO_SAO, bool DO_ALF>
-__global__ void __launch_bounds__(NT, 3) k_sao_alf_packed_batch(const Pass2Args *__restrict__ args,
+__global__ void __launch_bounds__(NT, 4) k_sao_alf_packed_batch(const Pass2Args *__restrict__ args,
                                                              const uint32_t *__restrict__ first, int n) {
   __shared__ Pass2Args s_args;  // the picture's parameters, read once per CTA
   int lo = 0, hi = n;            // first[lo] <= blockIdx.x < first[hi]
