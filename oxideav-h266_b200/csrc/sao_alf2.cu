@@ -53,11 +53,10 @@ struct Smem {
   alignas(16) uint16_t dL[DLH * DLW];
   alignas(16) uint16_t sL[SLH * SLW];
   alignas(16) uint4 cell[CH * CW];  // sh, sv, sd0, sd1 over the cell's two checkerboard positions
-  alignas(16) uint16_t dC[DCH * DCW];
-  alignas(16) uint16_t sC[SCH * SCW];
+  alignas(16) uint16_t dC[2][DCH * DCW];
+  alignas(16) uint16_t sC[2][SCH * SCW];
   uint8_t cls_f[(TH / 4) * (W / 4)], cls_t[(TH / 4) * (W / 4)];
   SaoLocal sao[3][9];
-  int any_sao[3];
 };
 
 // Fills one SaoLocal from the CTB's SAO parameters (src/sao.rs:504-626):
@@ -198,7 +197,74 @@ __device__ __forceinline__ void classify(int sh, int sv, int sd0, int sd1, int a
   t_out = (uint8_t)((kTransposeTable >> ((dir1 * 2 + (dir2 >> 1)) * 2)) & 3);
 }
 
-// One tile (index `tile` of the picture's tile grid) of the pass.
+// Chroma ALF (5x5 diamond, Table 46) and CC-ALF (Table 47) of one pair of
+// chroma samples (tile column i2, i2 + 1, tile row jj) of plane `comp`.
+template <int W>
+__device__ __forceinline__ void chroma_pair(const Pass2Args &a, const Smem<W> &sm, int comp, int i2, int jj, int cf,
+                                            int ccf, int xc0, int yc0, int y_ctb, int ctb, int ph, int bd, int maxv) {
+  using S = Smem<W>;
+  const DPlane CD = a.dst[comp];
+  const int ctb_c = ctb / 2, y_ctb_c = y_ctb / 2;
+  const int gy = yc0 + jj, gx = xc0 + i2;
+  const int r = jj + 2, c0 = i2 + 4;
+  const uint16_t *R0 = &sm.sC[comp - 1][r * S::SCW];
+  const uint32_t cur = pair_at<0>(R0, c0);
+  int v[2] = {(int)(cur & 0xFFFF), (int)(cur >> 16)};
+  if (cf >= 0) {
+    const int jr = gy - y_ctb_c;
+    int s2 = 7, y1 = 1, y2 = 2;  // Table 46 (line-buffer arms always applied)
+    if (jr == ctb_c - 2 || jr == ctb_c - 3) { s2 = 10; y1 = y2 = 0; }
+    else if (jr == ctb_c - 1 || jr == ctb_c - 4) { y2 = 1; }
+    const uint32_t *ct = a.tables.chroma_packed + max(cf, 0) * 18;
+    const uint32_t ncur = neg2(cur);
+    int acc[2] = {0, 0};
+    const uint16_t *U1 = R0 - y1 * S::SCW, *D1 = R0 + y1 * S::SCW, *U2 = R0 - y2 * S::SCW, *D2 = R0 + y2 * S::SCW;
+    chroma_tap<0>(D2, U2, c0, ncur, ct[0], ct[1], ct[2], acc);
+    chroma_tap<1>(D1, U1, c0, ncur, ct[3], ct[4], ct[5], acc);
+    chroma_tap<0>(D1, U1, c0, ncur, ct[6], ct[7], ct[8], acc);
+    chroma_tap<-1>(D1, U1, c0, ncur, ct[9], ct[10], ct[11], acc);
+    chroma_tap<2>(R0, R0, c0, ncur, ct[12], ct[13], ct[14], acc);
+    chroma_tap<1>(R0, R0, c0, ncur, ct[15], ct[16], ct[17], acc);
+    const int round = 1 << (s2 - 1);
+    v[0] = clampd(v[0] + ((acc[0] + round) >> s2), 0, maxv);
+    v[1] = clampd(v[1] + ((acc[1] + round) >> s2), 0, maxv);
+  }
+  if (ccf >= 0) {  // CC-ALF from post-SAO luma (Table 47, src/alf.rs:447-523)
+    const int *cc = a.tables.cc_coeff[comp - 1][max(ccf, 0)];
+    const int half = 1 << (bd - 1);
+    const int yline = (gy - y_ctb_c) * 2;
+    const bool lbb = !(gy * 2 + ctb >= ph && (ph - y_ctb) <= ctb - 4);
+    int yp1 = 1, yp2 = 2;
+    if (lbb) {
+      if (yline == ctb - 5 || yline == ctb - 4) { yp1 = 0; yp2 = 0; }
+      else if (yline == ctb - 6 || yline == ctb - 3) { yp2 = 1; }
+    }
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      const uint16_t *L = &sm.sL[(2 * jj + 3) * S::SLW + 2 * (i2 + p) + 4];
+      const int ctr = L[0];
+      int sum = cc[0] * ((int)L[-yp1 * S::SLW] - ctr);
+      sum += cc[1] * ((int)L[-1] - ctr);
+      sum += cc[2] * ((int)L[1] - ctr);
+      sum += cc[3] * ((int)L[yp1 * S::SLW - 1] - ctr);
+      sum += cc[4] * ((int)L[yp1 * S::SLW] - ctr);
+      sum += cc[5] * ((int)L[yp1 * S::SLW + 1] - ctr);
+      sum += cc[6] * ((int)L[yp2 * S::SLW] - ctr);
+      v[p] = clampd(v[p] + clampd((sum + 64) >> 7, -half, half - 1), 0, maxv);
+    }
+  }
+  if (gy < CD.h) {
+    uint16_t *out = CD.s + (int64_t)gy * CD.stride + gx;
+    if (gx < CD.w) out[0] = (uint16_t)v[0];
+    if (gx + 1 < CD.w) out[1] = (uint16_t)v[1];
+  }
+}
+
+// One tile (index `tile` of the picture's tile grid) of the pass.  Phases,
+// each ended by one barrier: (1) SAO parameters and every plane's deblocked
+// window; (2) post-SAO windows of all planes; (3) luma Laplacian cells and
+// the chroma planes' ALF / CC-ALF (their inputs are complete after 2);
+// (4) luma classes; (5) the 7x7 luma filter.
 template <int W, bool DO_SAO, bool DO_ALF>
 __device__ __forceinline__ void sao_alf_tile(const Pass2Args &a, int tile) {
   using S = Smem<W>;
@@ -222,8 +288,16 @@ __device__ __forceinline__ void sao_alf_tile(const Pass2Args &a, int tile) {
     rect[3] = me->rect[3];
   }
   const int rx0 = max(rect[0], 0), ry0 = max(rect[1], 0), rx1 = min(rect[2], pw), ry1 = min(rect[3], ph);
+  constexpr int TWC = W / 2, THC = TH / 2;
+  const int xc0 = X0 / 2, yc0 = Y0 / 2;
+  bool chroma_on[2] = {false, false};  // the tile has chroma samples of that plane
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    const DPlane &CS = a.src[c + 1];
+    chroma_on[c] = a.chroma && CS.w > 0 && CS.h > 0 && xc0 < CS.w && yc0 < CS.h;
+  }
 
-  // ---- SAO parameters of the 3x3 CTB neighbourhood
+  // ---- (1) SAO parameters of the 3x3 CTB neighbourhood; deblocked windows
   if (tid < 27) {
     const int comp = tid / 9, n = tid % 9;
     const int nx = rx + n % 3 - 1, ny = ry + n / 3 - 1;
@@ -244,45 +318,62 @@ __device__ __forceinline__ void sao_alf_tile(const Pass2Args &a, int tile) {
       sao_local(s, c.sao[comp], comp ? S::DCW : S::DLW, q0, q1, q2, q3, bd);
     }
   }
-  __syncthreads();
-  if (tid < 3) {
-    int any = 0;
-    for (int n = 0; n < 9; ++n) any |= sm.sao[tid][n].type;
-    sm.any_sao[tid] = any;
-  }
-
-  // ---- luma: deblocked samples with halo
   const DPlane LS = a.src[0], LD = a.dst[0];
   load_window<S::DLW, S::DLH>(sm.dL, LS, X0 - 8, Y0 - 4);
+#pragma unroll
+  for (int c = 0; c < 2; ++c)
+    if (chroma_on[c]) load_window<S::DCW, S::DCH>(sm.dC[c], a.src[c + 1], xc0 - 8, yc0 - 3);
   __syncthreads();
-  // ---- post-SAO luma, clamped into the fetch rectangle
-  {
-    const bool any = sm.any_sao[0] != 0;
-    for (int i = tid; i < S::SLH * S::SLW; i += NT) {
-      const int r = i / S::SLW, c = i - r * S::SLW;
-      const int ax = clampd(X0 - 4 + c, rx0, rx1 - 1), ay = clampd(Y0 - 3 + r, ry0, ry1 - 1);
-      const int lr = ay - (Y0 - 4), lc = ax - (X0 - 8);
-      const uint16_t *d = &sm.dL[lr * S::DLW + lc];
+  int any_sao[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    int any = 0;
+    for (int n = 0; n < 9; ++n) any |= sm.sao[c][n].type;
+    any_sao[c] = any;
+  }
+
+  // ---- (2) post-SAO windows, clamped into the fetch rectangle
+  for (int i = tid; i < S::SLH * S::SLW; i += NT) {
+    const int r = i / S::SLW, c = i - r * S::SLW;
+    const int ax = clampd(X0 - 4 + c, rx0, rx1 - 1), ay = clampd(Y0 - 3 + r, ry0, ry1 - 1);
+    const uint16_t *d = &sm.dL[(ay - (Y0 - 4)) * S::DLW + ax - (X0 - 8)];
+    int v = *d;
+    if (any_sao[0]) {
+      const SaoLocal &p = sm.sao[0][((ay >> log2) - ry + 1) * 3 + ((ax >> log2) - rx + 1)];
+      if (p.type) v = sao_one(p, ax, ay, maxv, d);
+    }
+    sm.sL[i] = (uint16_t)v;
+  }
+  const int crx0 = rect[0] / 2, cry0 = rect[1] / 2, crx1 = (rect[2] + 1) / 2, cry1 = (rect[3] + 1) / 2;
+#pragma unroll
+  for (int cc = 0; cc < 2; ++cc) {
+    if (!chroma_on[cc]) continue;
+    const DPlane &CS = a.src[cc + 1];
+    const int cx0 = max(crx0, 0), cy0 = max(cry0, 0), cx1 = min(crx1, CS.w), cy1 = min(cry1, CS.h);
+    for (int i = tid; i < S::SCH * S::SCW; i += NT) {
+      const int r = i / S::SCW, c = i - r * S::SCW;
+      const int ax = clampd(xc0 - 4 + c, cx0, cx1 - 1), ay = clampd(yc0 - 2 + r, cy0, cy1 - 1);
+      const uint16_t *d = &sm.dC[cc][(ay - (yc0 - 3)) * S::DCW + ax - (xc0 - 8)];
       int v = *d;
-      if (any) {
-        const SaoLocal &p = sm.sao[0][((ay >> log2) - ry + 1) * 3 + ((ax >> log2) - rx + 1)];
+      if (any_sao[cc + 1]) {
+        const SaoLocal &p = sm.sao[cc + 1][(((ay * 2) >> log2) - ry + 1) * 3 + (((ax * 2) >> log2) - rx + 1)];
         if (p.type) v = sao_one(p, ax, ay, maxv, d);
       }
-      sm.sL[i] = (uint16_t)v;
+      sm.sC[cc][i] = (uint16_t)v;
     }
   }
   __syncthreads();
 
+  // ---- (3) luma Laplacian sums per 2x2 cell (unpadded rows); chroma ALF / CC-ALF
   const bool luma_alf = DO_ALF && me && me->luma_set >= 0;
   if (luma_alf) {
-    // ---- Laplacian sums per 2x2 cell (unpadded rows)
     for (int i = tid; i < S::CH * S::CW; i += NT) {
       const int cy = i / S::CW, cx = i - cy * S::CW;
       uint4 g = make_uint4(0, 0, 0, 0);
 #pragma unroll
       for (int d = 0; d < 2; ++d) {
-        const int r = 2 * cy + d + 1;      // sL row of the position: y = Y0 - 2 + 2cy + d
-        const int c = 2 * cx + d + 2;      // sL col: x = X0 - 2 + 2cx + d
+        const int r = 2 * cy + d + 1;  // sL row of the position: y = Y0 - 2 + 2cy + d
+        const int c = 2 * cx + d + 2;  // sL col: x = X0 - 2 + 2cx + d
         const uint16_t *row = &sm.sL[r * S::SLW + c];
         const int c2 = 2 * row[0];
         g.x += abs(c2 - row[-1] - row[1]);
@@ -292,8 +383,30 @@ __device__ __forceinline__ void sao_alf_tile(const Pass2Args &a, int tile) {
       }
       sm.cell[i] = g;
     }
-    __syncthreads();
-    // ---- classes
+  }
+  {
+    // both chroma planes, one pair of samples per (plane, pair) item
+    constexpr int PAIRS = (TWC / 2) * THC;  // per plane
+    for (int it = tid; it < 2 * PAIRS; it += NT) {
+      const int cc = it / PAIRS, q = it - cc * PAIRS;
+      if (!chroma_on[cc]) continue;
+      const int cf = (DO_ALF && me) ? me->chroma_filt[cc] : -1;
+      const int ccf = (DO_ALF && me) ? me->cc_filt[cc] : -1;
+      chroma_pair<W>(a, sm, cc + 1, (q % (TWC / 2)) * 2, q / (TWC / 2), cf, ccf, xc0, yc0, y_ctb, ctb, ph, bd, maxv);
+    }
+  }
+  if (!luma_alf) {
+    for (int p = tid; p < TH * W; p += NT) {
+      const int i = p % W, j = p / W;
+      const int gx = X0 + i, gy = Y0 + j;
+      if (gx < LD.w && gy < LD.h) LD.s[(int64_t)gy * LD.stride + gx] = sm.sL[(j + 3) * S::SLW + i + 4];
+    }
+    return;
+  }
+  __syncthreads();
+
+  // ---- (4) classes
+  {
     const bool bottom = y_ctb + ctb >= ph;
     const bool carve = !bottom || (ph - y_ctb) > ctb - 4;
     const int vb = y_ctb + ctb - 4;
@@ -341,153 +454,61 @@ __device__ __forceinline__ void sao_alf_tile(const Pass2Args &a, int tile) {
         classify((int)s.x, (int)s.y, (int)s.z, (int)s.w, 2, bd, sm.cls_f[b], sm.cls_t[b]);
       }
     }
-    __syncthreads();
-    // ---- 7x7 diamond, 4-pixel runs; every thread keeps one block's taps
-    constexpr int RUNS = TH * W / 4;
-    constexpr int RPT = RUNS / NT;  // runs per thread: 1 (W = 32) or 2 (W = 64)
-    constexpr int TPB = 4 / RPT;    // threads per 4x4 block
-    const int b = tid / TPB;
-    const int bx = b % (W / 4), by = b / (W / 4);
-    const uint32_t *tab = a.tables.luma_packed + ((size_t)me->luma_set * 100 + sm.cls_f[b] * 4 + sm.cls_t[b]) * 36;
-    uint32_t c2[12], nc2[12], f[12];
-#pragma unroll
-    for (int k = 0; k < 12; ++k) {
-      c2[k] = __ldg(tab + 3 * k);
-      nc2[k] = __ldg(tab + 3 * k + 1);
-      f[k] = __ldg(tab + 3 * k + 2);
-    }
-#pragma unroll
-    for (int rr = 0; rr < RPT; ++rr) {
-      const int jr = (tid % TPB) * RPT + rr;  // row inside the block
-      const int j = 4 * by + jr;               // tile row
-      const int gy = Y0 + j;
-      const int yr = gy - y_ctb;
-      int shift = 7, y1 = 1, y2 = 2, y3 = 3;  // Table 45 (line-buffer arms always applied)
-      if (yr == ctb - 5 || yr == ctb - 4) { shift = 10; y1 = y2 = y3 = 0; }
-      else if (yr == ctb - 6 || yr == ctb - 3) { y2 = y3 = 1; }
-      else if (yr == ctb - 7 || yr == ctb - 2) { y3 = 2; }
-      const int r = j + 3;
-      const int c0 = 4 * bx + 4;
-      const uint16_t *R0 = &sm.sL[r * S::SLW];
-      const uint16_t *U1 = R0 - y1 * S::SLW, *D1 = R0 + y1 * S::SLW;
-      const uint16_t *U2 = R0 - y2 * S::SLW, *D2 = R0 + y2 * S::SLW;
-      const uint16_t *U3 = R0 - y3 * S::SLW, *D3 = R0 + y3 * S::SLW;
-      const uint32_t cur[2] = {pair_at<0>(R0, c0), pair_at<0>(R0, c0 + 2)};
-      const uint32_t ncur[2] = {neg2(cur[0]), neg2(cur[1])};
-      int acc[4] = {0, 0, 0, 0};
-      luma_tap<0>(D3, U3, c0, ncur, c2[0], nc2[0], f[0], acc);
-      luma_tap<1>(D2, U2, c0, ncur, c2[1], nc2[1], f[1], acc);
-      luma_tap<0>(D2, U2, c0, ncur, c2[2], nc2[2], f[2], acc);
-      luma_tap<-1>(D2, U2, c0, ncur, c2[3], nc2[3], f[3], acc);
-      luma_tap<2>(D1, U1, c0, ncur, c2[4], nc2[4], f[4], acc);
-      luma_tap<1>(D1, U1, c0, ncur, c2[5], nc2[5], f[5], acc);
-      luma_tap<0>(D1, U1, c0, ncur, c2[6], nc2[6], f[6], acc);
-      luma_tap<-1>(D1, U1, c0, ncur, c2[7], nc2[7], f[7], acc);
-      luma_tap<-2>(D1, U1, c0, ncur, c2[8], nc2[8], f[8], acc);
-      luma_tap<3>(R0, R0, c0, ncur, c2[9], nc2[9], f[9], acc);
-      luma_tap<2>(R0, R0, c0, ncur, c2[10], nc2[10], f[10], acc);
-      luma_tap<1>(R0, R0, c0, ncur, c2[11], nc2[11], f[11], acc);
-      if (gy < LD.h) {
-        const int round = 1 << (shift - 1);
-        uint16_t *out = LD.s + (int64_t)gy * LD.stride + X0 + 4 * bx;
-#pragma unroll
-        for (int p = 0; p < 4; ++p) {
-          const int cv = (int)((cur[p >> 1] >> ((p & 1) * 16)) & 0xFFFF);
-          if (X0 + 4 * bx + p < LD.w) out[p] = (uint16_t)clampd(cv + ((acc[p] + round) >> shift), 0, maxv);
-        }
-      }
-    }
-  } else {
-    for (int p = tid; p < TH * W; p += NT) {
-      const int i = p % W, j = p / W;
-      const int gx = X0 + i, gy = Y0 + j;
-      if (gx < LD.w && gy < LD.h) LD.s[(int64_t)gy * LD.stride + gx] = sm.sL[(j + 3) * S::SLW + i + 4];
-    }
   }
+  __syncthreads();
 
-  // ---- chroma (4:2:0)
-  if (!a.chroma) return;
-  constexpr int TWC = W / 2, THC = TH / 2;
-  const int xc0 = X0 / 2, yc0 = Y0 / 2;
-  const int ctb_c = ctb / 2, y_ctb_c = y_ctb / 2;
-  const int crx0 = rect[0] / 2, cry0 = rect[1] / 2, crx1 = (rect[2] + 1) / 2, cry1 = (rect[3] + 1) / 2;
-  for (int comp = 1; comp <= 2; ++comp) {
-    const DPlane CS = a.src[comp], CD = a.dst[comp];
-    if (CS.w <= 0 || CS.h <= 0 || xc0 >= CS.w || yc0 >= CS.h) continue;
-    const int cx0 = max(crx0, 0), cy0 = max(cry0, 0), cx1 = min(crx1, CS.w), cy1 = min(cry1, CS.h);
-    __syncthreads();
-    load_window<S::DCW, S::DCH>(sm.dC, CS, xc0 - 8, yc0 - 3);
-    __syncthreads();
-    const bool any = sm.any_sao[comp] != 0;
-    for (int i = tid; i < S::SCH * S::SCW; i += NT) {
-      const int r = i / S::SCW, c = i - r * S::SCW;
-      const int ax = clampd(xc0 - 4 + c, cx0, cx1 - 1), ay = clampd(yc0 - 2 + r, cy0, cy1 - 1);
-      const uint16_t *d = &sm.dC[(ay - (yc0 - 3)) * S::DCW + ax - (xc0 - 8)];
-      int v = *d;
-      if (any) {
-        const SaoLocal &p = sm.sao[comp][(((ay * 2) >> log2) - ry + 1) * 3 + (((ax * 2) >> log2) - rx + 1)];
-        if (p.type) v = sao_one(p, ax, ay, maxv, d);
-      }
-      sm.sC[i] = (uint16_t)v;
-    }
-    __syncthreads();
-    const int cf = (DO_ALF && me) ? me->chroma_filt[comp - 1] : -1;
-    const int ccf = (DO_ALF && me) ? me->cc_filt[comp - 1] : -1;
-    // one pair of chroma samples per thread
-    const int i2 = (tid % (TWC / 2)) * 2, j = tid / (TWC / 2);
-    for (int jj = j; jj < THC; jj += NT / (TWC / 2)) {
-      const int gy = yc0 + jj, gx = xc0 + i2;
-      const int r = jj + 2, c0 = i2 + 4;
-      const uint16_t *R0 = &sm.sC[r * S::SCW];
-      const uint32_t cur = pair_at<0>(R0, c0);
-      int v[2] = {(int)(cur & 0xFFFF), (int)(cur >> 16)};
-      if (cf >= 0) {
-        const int jr = gy - y_ctb_c;
-        int s2 = 7, y1 = 1, y2 = 2;  // Table 46 (line-buffer arms always applied)
-        if (jr == ctb_c - 2 || jr == ctb_c - 3) { s2 = 10; y1 = y2 = 0; }
-        else if (jr == ctb_c - 1 || jr == ctb_c - 4) { y2 = 1; }
-        const uint32_t *ct = a.tables.chroma_packed + max(cf, 0) * 18;
-        const uint32_t ncur = neg2(cur);
-        int acc[2] = {0, 0};
-        const uint16_t *U1 = R0 - y1 * S::SCW, *D1 = R0 + y1 * S::SCW, *U2 = R0 - y2 * S::SCW, *D2 = R0 + y2 * S::SCW;
-        chroma_tap<0>(D2, U2, c0, ncur, ct[0], ct[1], ct[2], acc);
-        chroma_tap<1>(D1, U1, c0, ncur, ct[3], ct[4], ct[5], acc);
-        chroma_tap<0>(D1, U1, c0, ncur, ct[6], ct[7], ct[8], acc);
-        chroma_tap<-1>(D1, U1, c0, ncur, ct[9], ct[10], ct[11], acc);
-        chroma_tap<2>(R0, R0, c0, ncur, ct[12], ct[13], ct[14], acc);
-        chroma_tap<1>(R0, R0, c0, ncur, ct[15], ct[16], ct[17], acc);
-        const int round = 1 << (s2 - 1);
-        v[0] = clampd(v[0] + ((acc[0] + round) >> s2), 0, maxv);
-        v[1] = clampd(v[1] + ((acc[1] + round) >> s2), 0, maxv);
-      }
-      if (ccf >= 0) {  // CC-ALF from post-SAO luma (Table 47, src/alf.rs:447-523)
-        const int *cc = a.tables.cc_coeff[comp - 1][max(ccf, 0)];
-        const int half = 1 << (bd - 1);
-        const int yline = (gy - y_ctb_c) * 2;
-        const bool lbb = !(gy * 2 + ctb >= ph && (ph - y_ctb) <= ctb - 4);
-        int yp1 = 1, yp2 = 2;
-        if (lbb) {
-          if (yline == ctb - 5 || yline == ctb - 4) { yp1 = 0; yp2 = 0; }
-          else if (yline == ctb - 6 || yline == ctb - 3) { yp2 = 1; }
-        }
+  // ---- (5) 7x7 diamond, 4-pixel runs; every thread keeps one block's taps
+  constexpr int RUNS = TH * W / 4;
+  constexpr int RPT = RUNS / NT;  // runs per thread: 1 (W = 32) or 2 (W = 64)
+  constexpr int TPB = 4 / RPT;    // threads per 4x4 block
+  const int b = tid / TPB;
+  const int bx = b % (W / 4), by = b / (W / 4);
+  const uint32_t *tab = a.tables.luma_packed + ((size_t)me->luma_set * 100 + sm.cls_f[b] * 4 + sm.cls_t[b]) * 36;
+  uint32_t c2[12], nc2[12], f[12];
 #pragma unroll
-        for (int p = 0; p < 2; ++p) {
-          const uint16_t *L = &sm.sL[(2 * jj + 3) * S::SLW + 2 * (i2 + p) + 4];
-          const int ctr = L[0];
-          int sum = cc[0] * ((int)L[-yp1 * S::SLW] - ctr);
-          sum += cc[1] * ((int)L[-1] - ctr);
-          sum += cc[2] * ((int)L[1] - ctr);
-          sum += cc[3] * ((int)L[yp1 * S::SLW - 1] - ctr);
-          sum += cc[4] * ((int)L[yp1 * S::SLW] - ctr);
-          sum += cc[5] * ((int)L[yp1 * S::SLW + 1] - ctr);
-          sum += cc[6] * ((int)L[yp2 * S::SLW] - ctr);
-          v[p] = clampd(v[p] + clampd((sum + 64) >> 7, -half, half - 1), 0, maxv);
-        }
-      }
-      if (gy < CD.h) {
-        uint16_t *out = CD.s + (int64_t)gy * CD.stride + gx;
-        if (gx < CD.w) out[0] = (uint16_t)v[0];
-        if (gx + 1 < CD.w) out[1] = (uint16_t)v[1];
+  for (int k = 0; k < 12; ++k) {
+    c2[k] = __ldg(tab + 3 * k);
+    nc2[k] = __ldg(tab + 3 * k + 1);
+    f[k] = __ldg(tab + 3 * k + 2);
+  }
+#pragma unroll
+  for (int rr = 0; rr < RPT; ++rr) {
+    const int jr = (tid % TPB) * RPT + rr;  // row inside the block
+    const int j = 4 * by + jr;               // tile row
+    const int gy = Y0 + j;
+    const int yr = gy - y_ctb;
+    int shift = 7, y1 = 1, y2 = 2, y3 = 3;  // Table 45 (line-buffer arms always applied)
+    if (yr == ctb - 5 || yr == ctb - 4) { shift = 10; y1 = y2 = y3 = 0; }
+    else if (yr == ctb - 6 || yr == ctb - 3) { y2 = y3 = 1; }
+    else if (yr == ctb - 7 || yr == ctb - 2) { y3 = 2; }
+    const int r = j + 3;
+    const int c0 = 4 * bx + 4;
+    const uint16_t *R0 = &sm.sL[r * S::SLW];
+    const uint16_t *U1 = R0 - y1 * S::SLW, *D1 = R0 + y1 * S::SLW;
+    const uint16_t *U2 = R0 - y2 * S::SLW, *D2 = R0 + y2 * S::SLW;
+    const uint16_t *U3 = R0 - y3 * S::SLW, *D3 = R0 + y3 * S::SLW;
+    const uint32_t cur[2] = {pair_at<0>(R0, c0), pair_at<0>(R0, c0 + 2)};
+    const uint32_t ncur[2] = {neg2(cur[0]), neg2(cur[1])};
+    int acc[4] = {0, 0, 0, 0};
+    luma_tap<0>(D3, U3, c0, ncur, c2[0], nc2[0], f[0], acc);
+    luma_tap<1>(D2, U2, c0, ncur, c2[1], nc2[1], f[1], acc);
+    luma_tap<0>(D2, U2, c0, ncur, c2[2], nc2[2], f[2], acc);
+    luma_tap<-1>(D2, U2, c0, ncur, c2[3], nc2[3], f[3], acc);
+    luma_tap<2>(D1, U1, c0, ncur, c2[4], nc2[4], f[4], acc);
+    luma_tap<1>(D1, U1, c0, ncur, c2[5], nc2[5], f[5], acc);
+    luma_tap<0>(D1, U1, c0, ncur, c2[6], nc2[6], f[6], acc);
+    luma_tap<-1>(D1, U1, c0, ncur, c2[7], nc2[7], f[7], acc);
+    luma_tap<-2>(D1, U1, c0, ncur, c2[8], nc2[8], f[8], acc);
+    luma_tap<3>(R0, R0, c0, ncur, c2[9], nc2[9], f[9], acc);
+    luma_tap<2>(R0, R0, c0, ncur, c2[10], nc2[10], f[10], acc);
+    luma_tap<1>(R0, R0, c0, ncur, c2[11], nc2[11], f[11], acc);
+    if (gy < LD.h) {
+      const int round = 1 << (shift - 1);
+      uint16_t *out = LD.s + (int64_t)gy * LD.stride + X0 + 4 * bx;
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        const int cv = (int)((cur[p >> 1] >> ((p & 1) * 16)) & 0xFFFF);
+        if (X0 + 4 * bx + p < LD.w) out[p] = (uint16_t)clampd(cv + ((acc[p] + round) >> shift), 0, maxv);
       }
     }
   }
