@@ -711,6 +711,25 @@ struct h266::Prep {
   DbSide db;
   int rc = H266_OK;
   std::string msg;
+  // Batch pictures: the blob copied to pinned memory by the worker that built
+  // it, uploaded from there; `uploaded` marks the end of the last upload.
+  Staging pinned;
+  cudaEvent_t uploaded = nullptr;
+  bool staged_pinned = false;
+  ~Prep() {
+    if (pinned.ptr) cudaFreeHost(pinned.ptr);
+    if (uploaded) cudaEventDestroy(uploaded);
+  }
+  // Copies the blob to `pinned` (waiting for the previous upload from it).
+  int stage() {
+    staged_pinned = false;
+    if (!uploaded) H266_CUDA(cudaEventCreateWithFlags(&uploaded, cudaEventDisableTiming));
+    H266_CUDA(cudaEventSynchronize(uploaded));
+    H266_TRY(pinned.ensure(blob.size()));
+    std::memcpy(pinned.ptr, blob.data(), blob.size());
+    staged_pinned = true;
+    return H266_OK;
+  }
 };
 
 // A chain whose side information is resident on the device (h266_chain_plan_create).
@@ -730,6 +749,7 @@ namespace {
 
 int prepare_chain(Prep &pr, const h266_picture &pic, const h266_in_loop_filter_args &a, TaskPool *pool) {
   pr.st = Staged{};
+  pr.staged_pinned = false;
   H266_TRY(check_lmcs(a.lmcs, a.lmcs_min_bin_idx, a.lmcs_max_bin_idx));
   if ((a.n_cus && !a.cus) || (a.n_no_filter_cols && !a.no_filter_cols) || (a.n_no_filter_rows && !a.no_filter_rows))
     return set_error(H266_ERR_INVALID_ARGUMENT, "NULL list with nonzero length");
@@ -766,7 +786,14 @@ int exec_chain(h266_ctx *ctx, cudaStream_t stream, const uint8_t *base, const St
 // Queues the chain for one prepared picture whose planes are the device
 // views `P` on lane `ln`.
 int issue_chain(h266_ctx *ctx, Lane &ln, Prep &pr, const DPlane P[3], const h266_in_loop_filter_args &a) {
-  H266_TRY(upload_blob(ln, pr.blob, &pr.st.base));
+  if (pr.staged_pinned) {  // staged by the worker: copy straight from its pinned buffer
+    H266_TRY(ln.side.ensure(pr.blob.size()));
+    H266_CUDA(cudaMemcpyAsync(ln.side.ptr, pr.pinned.ptr, pr.blob.size(), cudaMemcpyHostToDevice, ln.stream));
+    H266_CUDA(cudaEventRecord(pr.uploaded, ln.stream));
+    pr.st.base = ln.side.as<uint8_t>();
+  } else {
+    H266_TRY(upload_blob(ln, pr.blob, &pr.st.base));
+  }
   const uint16_t *lut = nullptr;
   if (a.lmcs) {
     H266_TRY(ln.lut.ensure(65536 * 2));
@@ -1031,9 +1058,12 @@ int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *co
   for (uint32_t l = 0; l < n_lanes; ++l) H266_CUDA(cudaStreamWaitEvent(ctx->lanes[l]->stream, ctx->main.mark, 0));
   for (uint32_t i = 0; i < n; ++i) ctx_prep(ctx, i + 1);
   TaskPool *pool = ctx_pool(ctx);
+  const int device = ctx->device;
   pool->start(n, [&](size_t i) {
     Prep &pr = *ctx->preps[i + 1];
+    pr.staged_pinned = false;
     pr.rc = prepare_chain(pr, *pics[i], *args[i], nullptr);
+    if (pr.rc == H266_OK && cudaSetDevice(device) == cudaSuccess) pr.rc = pr.stage();
     if (pr.rc != H266_OK) pr.msg = h266_last_error();
   });
   int rc = H266_OK;

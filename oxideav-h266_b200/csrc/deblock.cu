@@ -100,14 +100,14 @@ struct Cu {
   }
 };
 
+const h266_deblock_mv_cell kNoMotion = {};  // DeblockMvCell::default()
+
 struct MvGrid {
   const h266_deblock_mv_grid *g;
-  h266_deblock_mv_cell at(int x, int y) const {  // DeblockMvGrid::at_luma
-    h266_deblock_mv_cell d;
-    std::memset(&d, 0, sizeof d);
-    if (!g || x < 0 || y < 0) return d;
+  const h266_deblock_mv_cell &at(int x, int y) const {  // DeblockMvGrid::at_luma
+    if (!g || x < 0 || y < 0) return kNoMotion;
     uint64_t cx = (uint64_t)x / 4, cy = (uint64_t)y / 4;
-    if (cx >= g->cells_w || cy >= g->cells_h) return d;
+    if (cx >= g->cells_w || cy >= g->cells_h) return kNoMotion;
     return g->cells[cy * g->cells_w + cx];
   }
 };
@@ -216,6 +216,12 @@ void Walker::walk_cu(const PlaneCfg &pc, bool vert, const MvGrid &mv, const uint
     const bool is_tb = off == 0 ? filter_edge : q_geo.tb_boundary(off, vert, chroma);
     const bool is_sb = !chroma && off % sb == 0 && off / sb <= last_sb && (off > 0 || filter_edge);
     if (!is_tb && !is_sb) continue;
+    // Along one edge only the P-side CU and the bS inputs change; the
+    // maxFilterLengths, qP and flags that depend on the P-side CU are kept
+    // while it stays the same.
+    int64_t memo_pi = -2;
+    uint32_t memo_mp = 0, memo_mq = 0;
+    int memo_qp = 0;
     for (uint32_t k = 0; k < n_other; k += seg) {
       const int qx = (int)(vert ? cu.x + off : cu.x + k), qy = (int)(vert ? cu.y + k : cu.y + off);
       const int px = vert ? qx - 1 : qx, py = vert ? qy : qy - 1;
@@ -226,8 +232,12 @@ void Walker::walk_cu(const PlaneCfg &pc, bool vert, const MvGrid &mv, const uint
       if (bs == 0) continue;
       uint32_t mp, mq;
       int qp;
-      bool ctb_row = false;
-      if (!chroma) {
+      const bool ctb_row = !chroma && !vert && off == 0 && pc.ctb > 0 && cu.y % pc.ctb == 0;
+      if (pi == memo_pi) {
+        mp = memo_mp;
+        mq = memo_mq;
+        qp = memo_qp;
+      } else if (!chroma) {
         mp = mq = 0;
         if (is_tb) {
           uint32_t wq = q_geo.tb_len(qx, qy, vert, false), wp = Cu{p}.tb_len(px, py, vert, false);
@@ -258,7 +268,6 @@ void Walker::walk_cu(const PlaneCfg &pc, bool vert, const MvGrid &mv, const uint
             }
           }
         }
-        ctb_row = !vert && off == 0 && pc.ctb > 0 && cu.y % pc.ctb == 0;
         qp = (p.qp_y + cu.qp_y + 1) >> 1;  // eq. 1274 (no LADF)
       } else {
         const uint32_t sub = vert ? pc.sub_w : pc.sub_h;
@@ -277,6 +286,10 @@ void Walker::walk_cu(const PlaneCfg &pc, bool vert, const MvGrid &mv, const uint
         };
         qp = (pick(p) + pick(cu) + 1) >> 1;  // eq. 1343
       }
+      memo_pi = pi;
+      memo_mp = mp;
+      memo_mq = mq;
+      memo_qp = qp;
       const int beta = beta_of(qp + pc.beta_off * 2, pc.bd);
       const int tc = tc_of(qp + 2 * (bs - 1) + pc.tc_off * 2, pc.bd);
       if (tc == 0) continue;  // every filter arm is a no-op at tC = 0
