@@ -139,9 +139,8 @@ struct PlaneCfg {
   uint32_t ctb;
 };
 
-struct Emitted {
+struct Emitted {  // a segment in emission (reference) order: its index in the list
   EdgeSeg s;
-  uint32_t order;
 };
 
 class Walker {
@@ -303,7 +302,6 @@ void Walker::walk_cu(const PlaneCfg &pc, bool vert, const MvGrid &mv, const uint
       e.s.bs = (uint8_t)bs;
       e.s.mfl = (uint8_t)(mp << 4 | mq);
       e.s.flags = (uint8_t)((vert ? 1 : 0) | (ctb_row ? 2 : 0) | (p.plt ? 4 : 0) | (cu.plt ? 8 : 0));
-      e.order = (uint32_t)out.size();
       out.push_back(e);
     }
   }
@@ -320,24 +318,23 @@ inline int reach(int m) { return m <= 3 ? 4 : m + 1; }
 // linear.  A bucket that is not (CU lists in an unusual order) is sorted, and
 // its components' members are put back in emission order.
 struct GroupScratch {
-  std::vector<uint32_t> head, cursor, order, members;
-  std::vector<int32_t> start, end;
+  struct Item {  // a segment with its footprint and emission index, bucketed by band
+    EdgeSeg s;
+    int32_t start, end;
+    uint32_t i;
+  };
+  std::vector<uint32_t> head;
+  std::vector<Item> items, members;
 };
 
 void group(const std::vector<Emitted> &segs, std::vector<EdgeSeg> &dst, std::vector<uint32_t> &comp,
            uint32_t &max_len, GroupScratch &g) {
   const size_t n = segs.size();
   if (n == 0) return;
-  g.start.resize(n);
-  g.end.resize(n);
   uint32_t max_band = 0;
   for (size_t i = 0; i < n; ++i) {
     const EdgeSeg &s = segs[i].s;
-    const bool vert = s.flags & 1;
-    const int pos = vert ? s.x : s.y;
-    g.start[i] = pos - reach(s.mfl >> 4);
-    g.end[i] = pos + reach(s.mfl & 15);
-    max_band = std::max<uint32_t>(max_band, vert ? s.y : s.x);
+    max_band = std::max<uint32_t>(max_band, (s.flags & 1) ? s.y : s.x);
   }
   g.head.assign((size_t)max_band + 2, 0);
   for (size_t i = 0; i < n; ++i) {
@@ -345,34 +342,45 @@ void group(const std::vector<Emitted> &segs, std::vector<EdgeSeg> &dst, std::vec
     ++g.head[(size_t)((s.flags & 1) ? s.y : s.x) + 1];
   }
   for (size_t b = 1; b < g.head.size(); ++b) g.head[b] += g.head[b - 1];
-  g.cursor.assign(g.head.begin(), g.head.end() - 1);
-  g.order.resize(n);
-  for (size_t i = 0; i < n; ++i) {
-    const EdgeSeg &s = segs[i].s;
-    g.order[g.cursor[(s.flags & 1) ? s.y : s.x]++] = (uint32_t)i;
+  g.items.resize(n);
+  {
+    std::vector<uint32_t> &cur = g.head;  // used as the fill cursor, restored below
+    for (size_t i = 0; i < n; ++i) {
+      const EdgeSeg &s = segs[i].s;
+      const bool vert = s.flags & 1;
+      const int pos = vert ? s.x : s.y;
+      g.items[cur[vert ? s.y : s.x]++] =
+          GroupScratch::Item{s, pos - reach(s.mfl >> 4), pos + reach(s.mfl & 15), (uint32_t)i};
+    }
+    for (size_t b = g.head.size() - 1; b > 0; --b) g.head[b] = g.head[b - 1];  // cursor[b] ended at start[b + 1]
+    g.head[0] = 0;
   }
-  dst.reserve(dst.size() + n);
+  const size_t d0 = dst.size();
+  dst.resize(d0 + n);
+  EdgeSeg *out = dst.data() + d0;
+  size_t o = 0;
   uint32_t longest = max_len;
-  auto by_start = [&](uint32_t a, uint32_t b) { return g.start[a] < g.start[b]; };
+  auto by_start = [](const GroupScratch::Item &a, const GroupScratch::Item &b) { return a.start < b.start; };
   for (size_t b = 0; b + 1 < g.head.size(); ++b) {
-    uint32_t *lo = g.order.data() + g.head[b], *hi = g.order.data() + g.head[b + 1];
+    GroupScratch::Item *lo = g.items.data() + g.head[b], *hi = g.items.data() + g.head[b + 1];
     if (lo == hi) continue;
     const bool sorted = std::is_sorted(lo, hi, by_start);
     if (!sorted) std::stable_sort(lo, hi, by_start);  // ties keep emission order
-    for (uint32_t *i = lo; i < hi;) {
-      uint32_t *j = i + 1;
-      int32_t e = g.end[*i];
-      while (j < hi && g.start[*j] < e) {
-        e = std::max(e, g.end[*j]);
+    for (GroupScratch::Item *i = lo; i < hi;) {
+      GroupScratch::Item *j = i + 1;
+      int32_t e = i->end;
+      while (j < hi && j->start < e) {
+        e = std::max(e, j->end);
         ++j;
       }
-      comp.push_back((uint32_t)dst.size());
-      if (sorted) {
-        for (uint32_t *t = i; t < j; ++t) dst.push_back(segs[*t].s);
+      comp.push_back((uint32_t)(d0 + o));
+      if (sorted || j - i == 1) {
+        for (GroupScratch::Item *t = i; t < j; ++t) out[o++] = t->s;
       } else {
         g.members.assign(i, j);
-        std::sort(g.members.begin(), g.members.end());  // indices are emission order
-        for (uint32_t m : g.members) dst.push_back(segs[m].s);
+        std::sort(g.members.begin(), g.members.end(),
+                  [](const GroupScratch::Item &a, const GroupScratch::Item &b) { return a.i < b.i; });
+        for (const GroupScratch::Item &m : g.members) out[o++] = m.s;
       }
       longest = std::max<uint32_t>(longest, (uint32_t)(j - i));
       i = j;
