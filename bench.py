@@ -43,9 +43,10 @@ import time
 ROOT = pathlib.Path(__file__).resolve().parent
 WIDTH, HEIGHT, BITDEPTH = 1920, 1080, 10
 METRIC = "filter-chain Mpx/s 1080p/2160p 10-bit bit-exact"
-# DRAM bytes (read + write) per luma pixel of one k_sao_alf_packed launch, from the
-# ncu capture in profiles/k_sao_alf_packed_c2_1080p10.md (6 288 384 B / 1920x1080)
-SAO_ALF_TRAFFIC_PER_PX = 6288384 / (1920 * 1080)
+# DRAM bytes (read + write) per luma pixel of the batched SAO/ALF launch, from the
+# ncu capture in profiles/k_sao_alf_packed_c2_1080p10.md (16 pictures per launch:
+# 100 803 840 + 63 711 232 B)
+SAO_ALF_TRAFFIC_PER_PX = (100803840 + 63711232) / (16 * 1920 * 1080)
 
 
 def _import_pkg():
