@@ -131,6 +131,20 @@ def bad_clocks(c):
     return bool(sm and mx and sm < 0.5 * mx and "sw_power_cap" not in c.get("reasons", []))
 
 
+def replica_value(px_per_step: float, steps: int, ms_local: float, dist=None, device=None):
+    """Whole-job Mpx/s of replicas: every rank filters its own batch, the
+    elapsed time is the maximum over ranks.  Returns (Mpx/s, max ms)."""
+    import torch
+
+    t = torch.tensor([ms_local], dtype=torch.float64, device=device)
+    world = 1
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        world = dist.get_world_size()
+    ms = float(t.item())
+    return world * px_per_step * steps / (ms / 1e3) / 1e6, ms
+
+
 def workload_config(batch: int, world: int) -> dict:
     return {"workload": f"c2_1080p10_x{batch}", "width": WIDTH, "height": HEIGHT, "bit_depth": BITDEPTH,
             "pictures_per_step_per_gpu": batch, "chain": "LMCS-1 -> deblock -> SAO -> ALF -> CC-ALF",
@@ -313,12 +327,8 @@ def run_ours(args, rank, world, local_rank):
         clocks = cs.summary()
         if not bad_clocks(clocks):
             break
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
     px_per_step = args.batch * WIDTH * HEIGHT
-    value = world * px_per_step * args.steps / (ms_max / 1e3) / 1e6
+    value, ms_max = replica_value(px_per_step, args.steps, ms, dist, "cuda")
 
     # the same pictures as plain per-picture launches, for comparison
     for _ in range(args.warmup):
