@@ -258,6 +258,48 @@ def run_served(ctx, local_rank, seconds: float, rates=(1, 4, 8, 12)):
     return out
 
 
+def run_configs(ctx, local_rank, stream, steps: int):
+    """The benchmark's batched configs on device-resident pictures: one
+    batched execution per step vs per-picture launches of the same plans."""
+    import torch
+
+    from oxideav_h266_b200 import native
+    from oxideav_h266_b200 import workloads as W
+
+    out = {}
+    specs = (("c3_2160p10_tiles4x2_x16", lambda: [W.config3(3000 + i) for i in range(16)]),
+             ("c4_mixed_x64", lambda: [W.config4(4000 + i) for i in range(64)]))
+    for name, make in specs:
+        items = make()
+        devs = [native.DevicePicture.from_host(p, local_rank) for p, _ in items]
+        plans = [ctx.plan(p, f) for p, f in items]
+        px = sum(p.planes()[0].shape[0] * p.planes()[0].shape[1] for p, _ in items)
+        torch.cuda.synchronize()
+
+        def timed(fn):
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize()
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            for _ in range(steps):
+                fn()
+            s1.record(stream)
+            torch.cuda.synchronize()
+            return s0.elapsed_time(s1) / steps
+
+        ms_b = timed(lambda: ctx.execute_plans(plans, devs))
+        ms_p = timed(lambda: [pl.execute(d) for pl, d in zip(plans, devs)])
+        out[name] = {"pictures": len(items), "mpx_per_step": round(px / 1e6, 2),
+                     "batched": {"ms_per_step": round(ms_b, 4), "mpx_per_s": round(px / ms_b / 1e3, 1)},
+                     "plain": {"ms_per_step": round(ms_p, 4), "mpx_per_s": round(px / ms_p / 1e3, 1)}}
+        for pl in plans:
+            pl.close()
+        del devs
+        torch.cuda.synchronize()
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -403,6 +445,9 @@ def run_ours(args, rank, world, local_rank):
     served = None
     if rank == 0 and world == 1 and args.served_seconds > 0:
         served = run_served(ctx, local_rank, args.served_seconds)
+    configs = None
+    if rank == 0 and world == 1 and args.configs:
+        configs = run_configs(ctx, local_rank, stream, max(1, min(args.steps, 10)))
 
     cpu = None
     if rank == 0 and world == 1:
@@ -416,7 +461,7 @@ def run_ours(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic (seeded 1080p config generator)",
             "config": workload_config(args.batch, world),
-            "roofline": roofline, "plain": plain, "served": served, "cpu_baseline": cpu, "e2e": e2e,
+            "roofline": roofline, "plain": plain, "served": served, "configs": configs, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches),
             "clocks": clocks,
         }
@@ -469,6 +514,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--configs", type=int, default=1, help="measure the 2160p-tiles and mixed-size batches (0: skip)")
     ap.add_argument("--served-seconds", type=float, default=2.0,
                     help="seconds of Poisson arrivals per served measurement (0: skip)")
     args = ap.parse_args()
