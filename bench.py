@@ -428,17 +428,19 @@ def run_ours(args, rank, world, local_rank):
         for _ in range(2):  # warm-up: lanes, worker pool, device buffers
             ctx.apply_in_loop_filters_batch(hps, hfs)
         barrier()
+        b0 = ctx.transfer_bytes()
         t0 = time.perf_counter()
         for _ in range(e_steps):
             ctx.apply_in_loop_filters_batch(hps, hfs)  # returns with the results in host memory
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
+        b1 = ctx.transfer_bytes()
         te = torch.tensor([dt], dtype=torch.float64, device="cuda")
         if dist:
             dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        plane_bytes = sum(a.nbytes for p, _ in items for a in p.planes())
         e2e = {"value": round(world * px_per_step * e_steps / float(te.item()) / 1e6, 2), "unit": "Mpx/s",
-               "h2d_bytes_per_step": plane_bytes, "d2h_bytes_per_step": plane_bytes,
+               "h2d_bytes_per_step": (b1[0] - b0[0]) // e_steps, "d2h_bytes_per_step": (b1[1] - b0[1]) // e_steps,
+               "bytes": "planes and side information, from the context's transfer counters",
                "path": "h266_apply_in_loop_filters_batch per step, H266_MEM_HOST pinned planes, side information "
                        "built from the CU lists in every call"}
 

@@ -260,6 +260,10 @@ int h266_ctx_synchronize(h266_ctx *ctx);
 const char *h266_last_error(void);
 /* Number of kernels this context has launched since creation. */
 uint64_t h266_ctx_kernel_launches(const h266_ctx *ctx);
+/* Bytes of host -> device and device -> host copies the context has queued
+ * for the chain calls (host picture planes and side information).  No
+ * counterpart in the crate. */
+int h266_ctx_transfer_bytes(const h266_ctx *ctx, uint64_t *h2d, uint64_t *d2h);
 
 /* Per-kernel-family device time, for metrics and roofline accounting.  No
  * counterpart in the crate.  While profiling is on, every launch is bracketed

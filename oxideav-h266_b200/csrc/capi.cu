@@ -95,6 +95,7 @@ struct Lane {
   DevBuf scratch[3];  // deblocked planes read by the SAO / ALF pass
   DevBuf lut;         // LMCS inverse LUT
   DevBuf side;        // side information
+  DevBuf walk;        // CU maps and segment grids of device-built side information
   Staging stage;
   int init(cudaStream_t s) {
     if (!s) {
@@ -115,6 +116,7 @@ struct Lane {
     }
     lut.release();
     side.release();
+    walk.release();
     if (stage.ptr) cudaFreeHost(stage.ptr);
     stage.ptr = nullptr;
     stage.cap = 0;
@@ -157,6 +159,7 @@ struct h266_ctx {
   int device = 0;
   cudaStream_t own = nullptr, stream = nullptr;
   uint64_t launches = 0;
+  uint64_t h2d_bytes = 0, d2h_bytes = 0;  // host <-> device copies queued by the context
   h266::Lane main;                                   // single-picture calls (stream = ctx->stream)
   std::vector<std::unique_ptr<h266::Lane>> lanes;    // batch calls
   std::unique_ptr<h266::TaskPool> pool;              // host side-information builders
@@ -171,6 +174,7 @@ struct h266_ctx {
   bool force_scalar = false;  // H266_FORCE_SCALAR_ALF=1: scalar SAO/ALF kernel (cross-checks)
   bool force_global_deblock = false;  // H266_FORCE_GLOBAL_DEBLOCK=1: deblocking on global memory (cross-checks)
   bool force_strip_deblock = false;   // H266_FORCE_STRIP_DEBLOCK=1: strip kernels instead of tiles (cross-checks)
+  bool force_host_sideinfo = false;   // H266_FORCE_HOST_SIDEINFO=1: never build side information on the device
 };
 
 namespace {
@@ -245,6 +249,14 @@ DPlane dplane(const h266_plane &p, uint16_t *ptr, int64_t stride) {
 
 // Device views of the picture: the caller's planes (device memory) or the
 // context's copies of them (host memory, uploaded here).
+uint64_t host_plane_bytes(const h266_picture &pic) {  // bytes of the planes of a host picture
+  if (pic.mem != H266_MEM_HOST) return 0;
+  const h266_plane *pl[3] = {&pic.luma, &pic.cb, &pic.cr};
+  uint64_t b = 0;
+  for (const h266_plane *p : pl) b += (uint64_t)p->width * p->height * 2;
+  return b;
+}
+
 int picture_to_device(Lane &ln, const h266_picture &pic, DPlane out[3]) {
   const h266_plane *pl[3] = {&pic.luma, &pic.cb, &pic.cr};
   for (int i = 0; i < 3; ++i) {
@@ -572,6 +584,7 @@ int build_pass2(const h266_picture &pic, const Pass2Inputs &in, Pass2Host &h) {
 struct Staged {
   size_t ctb = 0, tab = 0, pack = 0, seg[2] = {0, 0}, comp[2] = {0, 0}, band[2] = {0, 0};
   size_t tile_bounds = 0;
+  size_t dw_cus = 0, dw_ccus = 0, dw_mv = 0, dw_cols = 0, dw_rows = 0;  // device-walk inputs
   uint8_t *base = nullptr;
 };
 
@@ -583,6 +596,10 @@ struct DbSide {
   bool tiles_ok = false;
   uint32_t tiles_x = 0, tiles_y = 0;
   uint32_t tb_off[2][3] = {{0, 0, 0}, {0, 0, 0}};
+  // side information built on the device: the walk's inputs (pointers are
+  // rebased onto the uploaded blob when the chain runs)
+  bool device_walk = false, dw_sep = false, dw_mv = false, dw_mv_cu = false;
+  DeviceWalkIn dw{};
 };
 
 void stage_deblock(const DeblockPlan &pl, std::vector<uint8_t> &b, Staged &st, DbSide &db) {
@@ -651,8 +668,17 @@ int plane_map(h266_ctx *ctx, cudaStream_t stream, DPlane dst, DPlane src, const 
 // tile kernel when the plan has tile lists and dst is not src, else the
 // shared-memory strip kernels when the planes fit them, else plane copies and
 // one thread per component on global memory.
+DeviceWalkIn device_walk_in(const uint8_t *base, const Staged &st, const DbSide &db);
+
 int run_deblock(h266_ctx *ctx, cudaStream_t stream, const uint8_t *base, const Staged &st, const DbSide &db,
-                const DPlane src[3], const DPlane dst[3], const uint16_t *lut, int bd) {
+                const DPlane src[3], const DPlane dst[3], const uint16_t *lut, int bd, uint8_t *walk = nullptr) {
+  if (db.device_walk) {  // side information built on the device, then the tile kernel on its grids
+    if (!walk) return set_error(H266_ERR_INVALID_ARGUMENT, "device-built side information without walk scratch");
+    Prof pf(ctx, stream, H266_PROF_DEBLOCK);
+    DeviceWalkOut out;
+    H266_TRY(launch_device_walk(stream, device_walk_in(base, st, db), walk, out, &ctx->launches));
+    return launch_deblock_tiles_grid(stream, src, dst, lut, bd, out, &ctx->launches);
+  }
   const StripSide v{reinterpret_cast<const EdgeSeg *>(base + st.seg[0]),
                     reinterpret_cast<const uint32_t *>(base + st.comp[0]),
                     reinterpret_cast<const uint32_t *>(base + st.band[0])};
@@ -747,16 +773,19 @@ struct h266_chain_plan {
 
 namespace {
 
-int prepare_chain(Prep &pr, const h266_picture &pic, const h266_in_loop_filter_args &a, TaskPool *pool) {
+// `allow_device`: a picture eligible for the device-built side information
+// (device_walk_eligible, and SAO or ALF on, so that deblocking runs out of
+// place) skips the host walk; its CU lists, motion grid and gate lists are
+// staged instead.
+int prepare_chain(Prep &pr, const h266_picture &pic, const h266_in_loop_filter_args &a, TaskPool *pool,
+                  bool allow_device = false) {
   pr.st = Staged{};
+  pr.db = DbSide{};
   pr.staged_pinned = false;
   H266_TRY(check_lmcs(a.lmcs, a.lmcs_min_bin_idx, a.lmcs_max_bin_idx));
   if ((a.n_cus && !a.cus) || (a.n_no_filter_cols && !a.no_filter_cols) || (a.n_no_filter_rows && !a.no_filter_rows))
     return set_error(H266_ERR_INVALID_ARGUMENT, "NULL list with nonzero length");
   if (a.clip_cols && !a.clip_rows) return set_error(H266_ERR_INVALID_ARGUMENT, "clip_rows is NULL while clip_cols is not");
-  H266_TRY(build_deblock_plan(pic, a.cus, a.n_cus, a.chroma_cus, a.n_chroma_cus, a.mv_grid, a.deblock,
-                              a.chroma_format_idc, a.no_filter_cols, a.n_no_filter_cols, a.no_filter_rows,
-                              a.n_no_filter_rows, pr.plan, pool));
   Pass2Inputs in;
   in.sao = a.sao;
   in.sao_cfg = a.sao ? &a.sao_cfg : nullptr;
@@ -769,23 +798,93 @@ int prepare_chain(Prep &pr, const h266_picture &pic, const h266_in_loop_filter_a
   in.n_rows = a.n_clip_rows;
   H266_TRY(build_pass2(pic, in, pr.h));
   pr.blob.clear();
-  stage_deblock(pr.plan, pr.blob, pr.st, pr.db);
+  const bool dev = allow_device && (pr.h.do_sao || pr.h.do_alf) &&
+                   device_walk_eligible(pic, a.cus, a.n_cus, a.chroma_cus, a.n_chroma_cus, a.deblock,
+                                        a.chroma_format_idc);
+  if (dev) {
+    Blob blob{pr.blob};
+    DbSide &db = pr.db;
+    db.device_walk = true;
+    db.dw_sep = a.chroma_cus != nullptr;
+    db.dw_mv = a.mv_grid && a.mv_grid->cells && a.mv_grid->cells_w * a.mv_grid->cells_h;
+    DeviceWalkIn &w = db.dw;
+    w.n_cus = a.n_cus;
+    w.n_chroma = db.dw_sep ? a.n_chroma_cus : 0;
+    w.mv_w = db.dw_mv ? a.mv_grid->cells_w : 0;
+    w.mv_h = db.dw_mv ? a.mv_grid->cells_h : 0;
+    w.n_cols = a.n_no_filter_cols;
+    w.n_rows = a.n_no_filter_rows;
+    w.params = a.deblock;
+    w.cfi = a.chroma_format_idc;
+    w.w = (int)pic.luma.width;
+    w.h = (int)pic.luma.height;
+    w.cw = (int)pic.cb.width;
+    w.ch = (int)pic.cb.height;
+    pr.st.dw_cus = blob.put(a.cus, a.n_cus * sizeof(h266_deblock_cu));
+    if (db.dw_sep) pr.st.dw_ccus = blob.put(a.chroma_cus, a.n_chroma_cus * sizeof(h266_deblock_cu));
+    if (db.dw_mv) {
+      // Motion by CU when the grid covers the picture and every luma CU's
+      // cells agree (the walk reads motion only inside CUs): one record per
+      // CU instead of one per 4x4 cell.
+      const h266_deblock_mv_grid &g = *a.mv_grid;
+      bool per_cu = g.cells_w >= (uint64_t)(w.w + 3) / 4 && g.cells_h >= (uint64_t)(w.h + 3) / 4;
+      thread_local std::vector<h266_deblock_mv_cell> rec;
+      rec.resize(a.n_cus);
+      for (uint64_t i = 0; i < a.n_cus && per_cu; ++i) {
+        const h266_deblock_cu &c = a.cus[i];
+        const h266_deblock_mv_cell *first = &g.cells[(c.y / 4) * g.cells_w + c.x / 4];
+        for (uint32_t y = c.y / 4; y < (c.y + c.h) / 4 && per_cu; ++y) {
+          const h266_deblock_mv_cell *row = &g.cells[y * g.cells_w];
+          for (uint32_t x = c.x / 4; x < (c.x + c.w) / 4; ++x)
+            if (std::memcmp(&row[x], first, sizeof *first) != 0) {
+              per_cu = false;
+              break;
+            }
+        }
+        rec[i] = *first;
+      }
+      db.dw_mv_cu = per_cu;
+      if (per_cu) pr.st.dw_mv = blob.put(rec.data(), a.n_cus * sizeof(h266_deblock_mv_cell));
+      else pr.st.dw_mv = blob.put(a.mv_grid->cells, w.mv_w * w.mv_h * sizeof(h266_deblock_mv_cell));
+    }
+    pr.st.dw_cols = blob.put(a.no_filter_cols, a.n_no_filter_cols * sizeof(uint32_t));
+    pr.st.dw_rows = blob.put(a.no_filter_rows, a.n_no_filter_rows * sizeof(uint32_t));
+  } else {
+    H266_TRY(build_deblock_plan(pic, a.cus, a.n_cus, a.chroma_cus, a.n_chroma_cus, a.mv_grid, a.deblock,
+                                a.chroma_format_idc, a.no_filter_cols, a.n_no_filter_cols, a.no_filter_rows,
+                                a.n_no_filter_rows, pr.plan, pool));
+    stage_deblock(pr.plan, pr.blob, pr.st, pr.db);
+  }
   if (pr.h.do_sao || pr.h.do_alf) stage_pass2(pr.h, pr.blob, pr.st);
   return H266_OK;
+}
+
+// The device walk's inputs rebased onto the uploaded blob at `base`.
+DeviceWalkIn device_walk_in(const uint8_t *base, const Staged &st, const DbSide &db) {
+  DeviceWalkIn in = db.dw;
+  in.cus = reinterpret_cast<const h266_deblock_cu *>(base + st.dw_cus);
+  in.chroma_cus = db.dw_sep ? reinterpret_cast<const h266_deblock_cu *>(base + st.dw_ccus) : in.cus;
+  in.mv_cells = db.dw_mv && !db.dw_mv_cu ? reinterpret_cast<const h266_deblock_mv_cell *>(base + st.dw_mv) : nullptr;
+  in.mv_per_cu = db.dw_mv && db.dw_mv_cu ? reinterpret_cast<const h266_deblock_mv_cell *>(base + st.dw_mv) : nullptr;
+  in.nf_cols = reinterpret_cast<const uint32_t *>(base + st.dw_cols);
+  in.nf_rows = reinterpret_cast<const uint32_t *>(base + st.dw_rows);
+  return in;
 }
 
 // Launches the chain: LMCS (LUT already built) -> deblock -> SAO/ALF.  With a
 // pass 2 the deblocked planes go to the scratch planes S, else in place.
 int exec_chain(h266_ctx *ctx, cudaStream_t stream, const uint8_t *base, const Staged &st, const DbSide &db,
-               const Pass2Host &h, const uint16_t *lut, int dbd, const DPlane P[3], const DPlane S[3]) {
+               const Pass2Host &h, const uint16_t *lut, int dbd, const DPlane P[3], const DPlane S[3],
+               uint8_t *walk = nullptr) {
   if (!h.do_sao && !h.do_alf) return run_deblock(ctx, stream, base, st, db, P, P, lut, dbd);
-  H266_TRY(run_deblock(ctx, stream, base, st, db, P, S, lut, dbd));
+  H266_TRY(run_deblock(ctx, stream, base, st, db, P, S, lut, dbd, walk));
   return run_pass2(ctx, stream, h.args, h.do_sao, h.do_alf, h.packed, base, st, S, P);
 }
 
 // Queues the chain for one prepared picture whose planes are the device
 // views `P` on lane `ln`.
 int issue_chain(h266_ctx *ctx, Lane &ln, Prep &pr, const DPlane P[3], const h266_in_loop_filter_args &a) {
+  ctx->h2d_bytes += pr.blob.size();
   if (pr.staged_pinned) {  // staged by the worker: copy straight from its pinned buffer
     H266_TRY(ln.side.ensure(pr.blob.size()));
     H266_CUDA(cudaMemcpyAsync(ln.side.ptr, pr.pinned.ptr, pr.blob.size(), cudaMemcpyHostToDevice, ln.stream));
@@ -802,7 +901,17 @@ int issue_chain(h266_ctx *ctx, Lane &ln, Prep &pr, const DPlane P[3], const h266
   }
   DPlane S[3];
   if (pr.h.do_sao || pr.h.do_alf) H266_TRY(ensure_scratch(ln, P, S));
-  return exec_chain(ctx, ln.stream, pr.st.base, pr.st, pr.db, pr.h, lut, (int)a.deblock.bit_depth, P, S);
+  uint8_t *walk = nullptr;
+  if (pr.db.device_walk) {
+    H266_TRY(ln.walk.ensure(device_walk_bytes(pr.db.dw)));
+    walk = ln.walk.as<uint8_t>();
+  }
+  return exec_chain(ctx, ln.stream, pr.st.base, pr.st, pr.db, pr.h, lut, (int)a.deblock.bit_depth, P, S, walk);
+}
+
+// Device-built side information unless a cross-check switch selects another path.
+bool device_sideinfo_allowed(const h266_ctx *ctx) {
+  return !ctx->force_host_sideinfo && !ctx->force_global_deblock && !ctx->force_strip_deblock;
 }
 
 // Worker pool of the context (created on first use): as many threads as the
@@ -825,7 +934,7 @@ Prep &ctx_prep(h266_ctx *ctx, size_t i) {
 // main lane; its deblocking plan is built with the worker pool.
 int chain_on_device(h266_ctx *ctx, const h266_picture &pic, const DPlane P[3], const h266_in_loop_filter_args &a) {
   Prep &pr = ctx_prep(ctx, 0);
-  H266_TRY(prepare_chain(pr, pic, a, ctx_pool(ctx)));
+  H266_TRY(prepare_chain(pr, pic, a, ctx_pool(ctx), device_sideinfo_allowed(ctx)));
   return issue_chain(ctx, ctx->main, pr, P, a);
 }
 
@@ -874,6 +983,8 @@ int h266_ctx_create(int device, h266_ctx **out) {
   c->force_global_deblock = fg && fg[0] == '1';
   const char *fstrip = std::getenv("H266_FORCE_STRIP_DEBLOCK");
   c->force_strip_deblock = fstrip && fstrip[0] == '1';
+  const char *fhost = std::getenv("H266_FORCE_HOST_SIDEINFO");
+  c->force_host_sideinfo = fhost && fhost[0] == '1';
   *out = c;
   return H266_OK;
 }
@@ -914,6 +1025,13 @@ int h266_ctx_synchronize(h266_ctx *ctx) {
 }
 
 uint64_t h266_ctx_kernel_launches(const h266_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+int h266_ctx_transfer_bytes(const h266_ctx *ctx, uint64_t *h2d, uint64_t *d2h) {
+  H266_TRY(check_ctx(const_cast<h266_ctx *>(ctx)));
+  if (h2d) *h2d = ctx->h2d_bytes;
+  if (d2h) *d2h = ctx->d2h_bytes;
+  return H266_OK;
+}
 
 int h266_derive_lmcs(const h266_lmcs_data *data, uint32_t bit_depth, h266_lmcs_derived *out) {
   return derive_lmcs(data, bit_depth, out);
@@ -1021,7 +1139,9 @@ int h266_apply_in_loop_filters(h266_ctx *ctx, h266_picture *pic, const h266_in_l
   Guard g(ctx->device);
   DPlane P[3];
   H266_TRY(picture_to_device(ctx->main, *pic, P));  // the copy overlaps the host-side preparation
+  ctx->h2d_bytes += host_plane_bytes(*pic);
   H266_TRY(chain_on_device(ctx, *pic, P, *args));
+  ctx->d2h_bytes += host_plane_bytes(*pic);
   return picture_from_device(ctx->main, *pic);
 }
 
@@ -1062,7 +1182,7 @@ int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *co
   pool->start(n, [&](size_t i) {
     Prep &pr = *ctx->preps[i + 1];
     pr.staged_pinned = false;
-    pr.rc = prepare_chain(pr, *pics[i], *args[i], nullptr);
+    pr.rc = prepare_chain(pr, *pics[i], *args[i], nullptr, device_sideinfo_allowed(ctx));
     if (pr.rc == H266_OK && cudaSetDevice(device) == cudaSuccess) pr.rc = pr.stage();
     if (pr.rc != H266_OK) pr.msg = h266_last_error();
   });
@@ -1079,6 +1199,8 @@ int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *co
     rc = picture_to_device(ln, *pics[i], P);
     if (rc == H266_OK) rc = issue_chain(ctx, ln, pr, P, *args[i]);
     if (rc == H266_OK) rc = picture_from_device(ln, *pics[i], false);
+    ctx->h2d_bytes += host_plane_bytes(*pics[i]);
+    ctx->d2h_bytes += host_plane_bytes(*pics[i]);
   }
   pool->wait_all();
   for (uint32_t l = 0; l < n_lanes; ++l) {

@@ -27,21 +27,44 @@
 namespace h266 {
 namespace {
 
+// The edge derivation below runs on the host (the general plan) and on the
+// device (the side-information builder for pictures without chained edges):
+// the same functions, compiled for both.
+#define H266_HD __host__ __device__
+
 // ---------------------------------------------------------------- tables
 // Table 43 (β′, tC′) as in src/deblock.rs:401-418.
-const int kBeta[64] = {0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  6,  7,  8,  9,  10, 11,
-                       12, 13, 14, 15, 16, 17, 18, 20, 22, 24, 26, 28, 30, 32, 34, 36, 38, 40, 42, 44, 46, 48,
-                       50, 52, 54, 56, 58, 60, 62, 64, 66, 68, 70, 72, 74, 76, 78, 80, 82, 84, 86, 88};
-const int kTc[66] = {0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,   0,   0,   0,   0,   0,   0,   0,   3,   4,   4,   4,
-                     4,  5,  5,  5,  5,  7,  7,  8,  9,  10, 10,  11,  13,  14,  15,  17,  19,  21,  24,  25,  29,  33,
-                     36, 41, 45, 51, 57, 64, 71, 80, 89, 100, 112, 125, 141, 157, 177, 198, 222, 250, 280, 314, 352, 395};
+#define H266_BETA_TABLE \
+  0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 6, 7, 8, 9, 10, 11,  \
+  12, 13, 14, 15, 16, 17, 18, 20, 22, 24, 26, 28, 30, 32, 34, 36, 38, 40, 42, 44, 46, 48,  \
+  50, 52, 54, 56, 58, 60, 62, 64, 66, 68, 70, 72, 74, 76, 78, 80, 82, 84, 86, 88
+#define H266_TC_TABLE \
+  0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 3, 4, 4, 4,  \
+  4, 5, 5, 5, 5, 7, 7, 8, 9, 10, 10, 11, 13, 14, 15, 17, 19, 21, 24, 25, 29, 33,  \
+  36, 41, 45, 51, 57, 64, 71, 80, 89, 100, 112, 125, 141, 157, 177, 198, 222, 250, 280, 314, 352, 395
+#ifndef __CUDA_ARCH__
+const int kBeta[64] = {H266_BETA_TABLE};
+const int kTc[66] = {H266_TC_TABLE};
+#endif
+__constant__ int kBetaDev[64] = {H266_BETA_TABLE};  // the same tables for device code
+__constant__ int kTcDev[66] = {H266_TC_TABLE};
 
-inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+H266_HD inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
 // eqs. 1276-1279 (src/deblock.rs:424-452)
-inline int beta_of(int q, int bd) { return kBeta[clampi(q, 0, 63)] * (1 << (bd - 8)); }
-inline int tc_of(int q, int bd) {
+H266_HD inline int beta_of(int q, int bd) {
+#ifdef __CUDA_ARCH__
+  return kBetaDev[clampi(q, 0, 63)] * (1 << (bd - 8));
+#else
+  return kBeta[clampi(q, 0, 63)] * (1 << (bd - 8));
+#endif
+}
+H266_HD inline int tc_of(int q, int bd) {
+#ifdef __CUDA_ARCH__
+  int t = kTcDev[clampi(q, 0, 65)];
+#else
   int t = kTc[clampi(q, 0, 65)];
+#endif
   if (bd < 10) return (t + (1 << (9 - bd))) >> (10 - bd);
   return t * (1 << (bd - 10));
 }
@@ -50,16 +73,16 @@ inline int tc_of(int q, int bd) {
 // The per-CU transform-block queries of src/deblock.rs:163-320, for one CU.
 struct Cu {
   const h266_deblock_cu &c;
-  uint32_t rel(int lx, int ly, bool vert) const {
+  H266_HD uint32_t rel(int lx, int ly, bool vert) const {
     return vert ? (uint32_t)clampi(lx - (int)c.x, 0, (int)c.w - 1) : (uint32_t)clampi(ly - (int)c.y, 0, (int)c.h - 1);
   }
-  int split_index(uint32_t r) const {
+  H266_HD int split_index(uint32_t r) const {
     int idx = 0;
     for (int i = 0; i < c.tb_split.n_bounds; ++i)
       if (r >= c.tb_split.bounds[i]) idx = i + 1;
     return idx;
   }
-  uint32_t split_len(uint32_t r, uint32_t dim) const {
+  H266_HD uint32_t split_len(uint32_t r, uint32_t dim) const {
     uint32_t lo = 0, hi = dim;
     for (int i = 0; i < c.tb_split.n_bounds; ++i) {
       if (r < c.tb_split.bounds[i]) {
@@ -70,7 +93,7 @@ struct Cu {
     }
     return hi - lo;
   }
-  bool coded(uint32_t comp, int lx, int ly) const {  // tu_coded_at
+  H266_HD bool coded(uint32_t comp, int lx, int ly) const {  // tu_coded_at
     if (c.has_tu64) {
       uint32_t tx = std::min(rel(lx, ly, true) / 64, 1u), ty = std::min(rel(lx, ly, false) / 64, 1u);
       return comp == 0 ? c.tu64.y[ty][tx] : (comp == 1 ? c.tu64.cb[ty][tx] : c.tu64.cr[ty][tx]);
@@ -81,14 +104,14 @@ struct Cu {
     }
     return comp == 0 ? c.tu_y_coded : (comp == 1 ? c.tu_cb_coded : c.tu_cr_coded);
   }
-  uint32_t tb_len(int lx, int ly, bool vert, bool chroma) const {  // luma_tb_len / chroma_tb_len (luma units)
+  H266_HD uint32_t tb_len(int lx, int ly, bool vert, bool chroma) const {  // luma_tb_len / chroma_tb_len (luma units)
     uint32_t dim = vert ? c.w : c.h;
     if (c.has_tu64 && dim > 64) return std::min(dim - (rel(lx, ly, vert) / 64) * 64, 64u);
     if (c.has_tb_split && (c.tb_split.vertical != 0) == vert && !(chroma && c.tb_split.luma_only))
       return split_len(rel(lx, ly, vert), dim);
     return dim;
   }
-  bool tb_boundary(uint32_t off, bool vert, bool chroma) const {  // is_{luma,chroma}_tb_boundary
+  H266_HD bool tb_boundary(uint32_t off, bool vert, bool chroma) const {  // is_{luma,chroma}_tb_boundary
     uint32_t dim = vert ? c.w : c.h;
     if (off == 0 || off >= dim) return false;
     if (c.has_tu64 && dim > 64) return off % 64 == 0;
@@ -100,22 +123,30 @@ struct Cu {
   }
 };
 
+#ifndef __CUDA_ARCH__
 const h266_deblock_mv_cell kNoMotion = {};  // DeblockMvCell::default()
+#endif
+__device__ const h266_deblock_mv_cell kNoMotionDev = {};
 
-struct MvGrid {
+struct MvGrid {  // `g` points to a grid descriptor whose cells are reachable by the caller's side
   const h266_deblock_mv_grid *g;
-  const h266_deblock_mv_cell &at(int x, int y) const {  // DeblockMvGrid::at_luma
-    if (!g || x < 0 || y < 0) return kNoMotion;
+  H266_HD const h266_deblock_mv_cell &at(int x, int y) const {  // DeblockMvGrid::at_luma
+#ifdef __CUDA_ARCH__
+    const h266_deblock_mv_cell &none = kNoMotionDev;
+#else
+    const h266_deblock_mv_cell &none = kNoMotion;
+#endif
+    if (!g || x < 0 || y < 0) return none;
     uint64_t cx = (uint64_t)x / 4, cy = (uint64_t)y / 4;
-    if (cx >= g->cells_w || cy >= g->cells_h) return kNoMotion;
+    if (cx >= g->cells_w || cy >= g->cells_h) return none;
     return g->cells[cy * g->cells_w + cx];
   }
 };
 
-bool mv_far(const int32_t *a, const int32_t *b) { return std::abs(a[0] - b[0]) >= 8 || std::abs(a[1] - b[1]) >= 8; }
+H266_HD inline bool mv_far(const int32_t *a, const int32_t *b) { return abs(a[0] - b[0]) >= 8 || abs(a[1] - b[1]) >= 8; }
 
 // §8.8.3.5 motion arm, src/deblock.rs:992-1045
-bool motion_differs(const h266_deblock_mv_cell &p, const h266_deblock_mv_cell &q) {
+H266_HD inline bool motion_differs(const h266_deblock_mv_cell &p, const h266_deblock_mv_cell &q) {
   int np = (p.pred_l0 != 0) + (p.pred_l1 != 0), nq = (q.pred_l0 != 0) + (q.pred_l1 != 0);
   if (np != nq) return true;
   if (np == 0) return false;
@@ -166,21 +197,21 @@ class Walker {
   }
   // deblock_cu_dir (src/deblock.rs:707-983) for every CU, recording segments.
   void walk(const PlaneCfg &pc, bool vert, const MvGrid &mv, const uint32_t *nf, uint64_t n_nf,
-            std::vector<Emitted> &out) const {
-    for (size_t idx = 0; idx < n_; ++idx) walk_cu(pc, vert, mv, nf, n_nf, idx, out);
-  }
+            std::vector<Emitted> &out) const;
 
  private:
-  void walk_cu(const PlaneCfg &pc, bool vert, const MvGrid &mv, const uint32_t *nf, uint64_t n_nf, size_t idx,
-               std::vector<Emitted> &out) const;
   const h266_deblock_cu *cus_;
   size_t n_;
   int cw_, ch_;
   std::vector<int32_t> &grid_;
 };
 
-int bs_of(uint32_t comp, const h266_deblock_cu &p, const h266_deblock_cu &q, const MvGrid &mv, int px, int py,
-          int qx, int qy, bool is_tb, bool idc2) {  // derive_bs, src/deblock.rs:1055-1119
+// `mv`: the motion lookup (MvGrid, or per-CU motion on the device); mv.g
+// non-null when the picture has a motion grid.
+#pragma nv_exec_check_disable
+template <class Mv>
+H266_HD inline int bs_of(uint32_t comp, const h266_deblock_cu &p, const h266_deblock_cu &q, const Mv &mv, int px,
+                         int py, int qx, int qy, bool is_tb, bool idc2) {  // derive_bs, src/deblock.rs:1055-1119
   if (comp == 0 ? (p.bdpcm_luma && q.bdpcm_luma) : (p.bdpcm_chroma && q.bdpcm_chroma)) return 0;
   if (p.intra || q.intra || p.ciip || q.ciip) return 2;
   if (is_tb && (Cu{p}.coded(comp, px, py) || Cu{q}.coded(comp, qx, qy))) return 1;
@@ -194,8 +225,13 @@ int bs_of(uint32_t comp, const h266_deblock_cu &p, const h266_deblock_cu &q, con
   return 0;
 }
 
-void Walker::walk_cu(const PlaneCfg &pc, bool vert, const MvGrid &mv, const uint32_t *nf, uint64_t n_nf, size_t idx,
-                     std::vector<Emitted> &out) const {
+// deblock_cu_dir (src/deblock.rs:707-983) for CU `idx`: every edge segment it
+// owns, in the reference's order, passed to `emit`.  `grid.at(x, y)` is the
+// CU covering luma sample (x, y) (CuGrid::cu_at), -1 for none.
+#pragma nv_exec_check_disable
+template <class Grid, class Mv, class Emit>
+H266_HD void walk_cu(const h266_deblock_cu *cus_, const Grid &grid, const PlaneCfg &pc, bool vert, const Mv &mv,
+                     const uint32_t *nf, uint64_t n_nf, size_t idx, Emit &emit) {
   const h266_deblock_cu &cu = cus_[idx];
   const bool chroma = pc.comp != 0;
   if (chroma && ((vert ? cu.x / pc.sub_w : cu.y / pc.sub_h) % 8) != 0) return;
@@ -224,7 +260,7 @@ void Walker::walk_cu(const PlaneCfg &pc, bool vert, const MvGrid &mv, const uint
     for (uint32_t k = 0; k < n_other; k += seg) {
       const int qx = (int)(vert ? cu.x + off : cu.x + k), qy = (int)(vert ? cu.y + k : cu.y + off);
       const int px = vert ? qx - 1 : qx, py = vert ? qy : qy - 1;
-      int64_t pi = off == 0 ? at(px, py) : (int64_t)idx;
+      int64_t pi = off == 0 ? grid.at(px, py) : (int64_t)idx;
       if (pi < 0 || (off == 0 && pi == (int64_t)idx)) continue;
       const h266_deblock_cu &p = cus_[pi];
       const int bs = bs_of(pc.comp, p, cu, mv, px, py, qx, qy, is_tb, is_sb);
@@ -302,12 +338,24 @@ void Walker::walk_cu(const PlaneCfg &pc, bool vert, const MvGrid &mv, const uint
       e.s.bs = (uint8_t)bs;
       e.s.mfl = (uint8_t)(mp << 4 | mq);
       e.s.flags = (uint8_t)((vert ? 1 : 0) | (ctb_row ? 2 : 0) | (p.plt ? 4 : 0) | (cu.plt ? 8 : 0));
-      out.push_back(e);
+      emit(e.s);
     }
   }
 }
 
+struct VectorEmit {  // host: the segment list in emission order
+  std::vector<Emitted> &out;
+  void operator()(const EdgeSeg &s) { out.push_back(Emitted{s}); }
+};
+
+void Walker::walk(const PlaneCfg &pc, bool vert, const MvGrid &mv, const uint32_t *nf, uint64_t n_nf,
+                  std::vector<Emitted> &out) const {
+  VectorEmit emit{out};
+  for (size_t idx = 0; idx < n_; ++idx) walk_cu(cus_, *this, pc, vert, mv, nf, n_nf, idx, emit);
+}
+
 inline int reach(int m) { return m <= 3 ? 4 : m + 1; }
+__device__ __forceinline__ int reach_d(int m) { return m <= 3 ? 4 : m + 1; }
 
 // Groups one (pass, plane) segment list into components and appends them.
 // Components come out band by band, by footprint start inside a band, with
@@ -1428,6 +1476,12 @@ struct TileParams {
   const uint16_t *lut;
   uint32_t tiles_x, tiles_y;
   int maxv;
+  // Grid mode (side information built on the device): every component is one
+  // segment, stored in grid[d][p][band * grid_slots[d][p] + pos / unit] (bs 0:
+  // none), unit 4 luma / 8 chroma samples along the edge normal.
+  int grid_mode;
+  const EdgeSeg *grid[2][3];
+  uint32_t grid_slots[2][3];
 };
 
 constexpr int kTileBands = 32;  // bands of one tile and pass that a plane can have (at most 24)
@@ -1473,6 +1527,55 @@ __device__ __forceinline__ void store_window(const uint16_t *sm, int pitch, cons
 
 // Band counts and prefix sums of the tile's component ranges for (pass d,
 // plane p), by one warp.
+// Grid mode: the list of (pass d, plane p) of tile (tx, ty) by one warp,
+// scanning the grid cells of the tile's bands whose footprint reaches the
+// tile; s_off[kTileBands] receives the count.
+__device__ __forceinline__ void tile_grid_list(const TileParams &a, int d, int p, int tx, int ty, uint32_t *list,
+                                               uint32_t cap, uint32_t *s_off) {
+  const int lane = threadIdx.x & 31;
+  const int tp = p ? kDeblockTile / 2 : kDeblockTile, halo = p ? kDeblockHaloC : kDeblockHaloY, unit = p ? 2 : 4;
+  const int pu = p ? 8 : 4;  // grid positions along the edge normal
+  const int nb = (int)a.n_bands[d][p], ns = (int)a.grid_slots[d][p];
+  const EdgeSeg *g = a.grid[d][p];
+  const DPlane &pl = a.src[p];
+  const int along = d == 0 ? pl.w : pl.h;
+  int b0, b1, t0, t1;  // bands; tile extent along the normal
+  if (d == 0) {
+    b0 = max(ty * tp - halo, 0) / unit;
+    b1 = min((ty * tp + tp + halo) / unit, nb);
+    t0 = tx * tp;
+    t1 = min(t0 + tp, along);
+  } else {
+    b0 = tx * tp / unit;
+    b1 = min((tx * tp + tp) / unit, nb);
+    t0 = ty * tp;
+    t1 = min(t0 + tp, along);
+  }
+  const int s0 = max(t0 - halo, 0) / pu, s1 = min((t1 + halo + pu - 1) / pu, ns);
+  uint32_t n = 0;
+  for (int b = b0; b < b1; ++b) {
+    for (int sb = s0; sb < s1; sb += 32) {
+      const int sl = sb + lane;
+      bool take = false;
+      uint32_t cell = 0;
+      if (sl < s1) {
+        cell = (uint32_t)b * ns + sl;
+        const EdgeSeg e = g[cell];
+        if (e.bs) {
+          const int pos = d == 0 ? e.x : e.y;
+          const int fs = max(pos - reach_d(e.mfl >> 4), 0), fe = min(pos + reach_d(e.mfl & 15), along);
+          take = fs < t1 && fe > t0;
+        }
+      }
+      const unsigned m = __ballot_sync(0xFFFFFFFFu, take);
+      const uint32_t rank = __popc(m & ((1u << lane) - 1));
+      if (take && n + rank < cap) list[n + rank] = cell;
+      n += __popc(m);
+    }
+  }
+  if (lane == 0) s_off[kTileBands] = min(n, cap);
+}
+
 __device__ __forceinline__ void tile_prefix(const TileParams &a, int d, int p, int tx, int ty,
                                             uint32_t *s_off /* kTileBands + 1 */, uint32_t *s_lo /* kTileBands */) {
   const int lane = threadIdx.x & 31;
@@ -1537,10 +1640,14 @@ __device__ __forceinline__ void run_tile_pass(const TileParams &a, uint16_t *sm,
       const uint32_t j = t * 8 + (lane >> 2);
       if (j < n0) {
         const SharedView v = tile_view(a, sm, 0, tx, ty);
-        const uint32_t c = list0[j], e = comp[c + 1];
-        for (uint32_t i = comp[c]; i < e; ++i) {
-          segment_group<4, kPitchY>(v, segs[i], a.maxv, k, base, mask);
-          __syncwarp(mask);
+        if (a.grid_mode) {
+          segment_group<4, kPitchY>(v, a.grid[d][0][list0[j]], a.maxv, k, base, mask);
+        } else {
+          const uint32_t c = list0[j], e = comp[c + 1];
+          for (uint32_t i = comp[c]; i < e; ++i) {
+            segment_group<4, kPitchY>(v, segs[i], a.maxv, k, base, mask);
+            __syncwarp(mask);
+          }
         }
       }
     } else {
@@ -1551,10 +1658,14 @@ __device__ __forceinline__ void run_tile_pass(const TileParams &a, uint16_t *sm,
       const uint32_t j = tt * 16 + (lane >> 1);
       if (j < (cr ? n2 : n1)) {
         const SharedView v = tile_view(a, sm, cr ? 2 : 1, tx, ty);
-        const uint32_t c = (cr ? list2 : list1)[j], e = comp[c + 1];
-        for (uint32_t i = comp[c]; i < e; ++i) {
-          segment_group<2, kPitchC>(v, segs[i], a.maxv, k, base, mask);
-          __syncwarp(mask);
+        if (a.grid_mode) {
+          segment_group<2, kPitchC>(v, a.grid[d][cr ? 2 : 1][(cr ? list2 : list1)[j]], a.maxv, k, base, mask);
+        } else {
+          const uint32_t c = (cr ? list2 : list1)[j], e = comp[c + 1];
+          for (uint32_t i = comp[c]; i < e; ++i) {
+            segment_group<2, kPitchC>(v, segs[i], a.maxv, k, base, mask);
+            __syncwarp(mask);
+          }
         }
       }
     }
@@ -1577,8 +1688,16 @@ __device__ __forceinline__ void deblock_tile(const TileParams &a, int t) {
   const int tx = t % (int)a.tiles_x, ty = t / (int)a.tiles_x;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, n_warps = blockDim.x >> 5;
   // Warps 0-5 first read the component ranges of both passes (one warp per
-  // pass and plane), then every thread loads the planes' regions.
-  if (warp < 6) tile_prefix(a, warp / 3, warp % 3, tx, ty, s_off[warp / 3][warp % 3], s_lo[warp / 3][warp % 3]);
+  // pass and plane) -- in grid mode they build the lists outright -- then
+  // every thread loads the planes' regions.
+  if (warp < 6) {
+    const int d = warp / 3, p = warp % 3;
+    if (a.grid_mode)
+      tile_grid_list(a, d, p, tx, ty, p == 0 ? s_list_y[d] : s_list_c[d][p - 1], p == 0 ? kTileListY : kTileListC,
+                     s_off[d][p]);
+    else
+      tile_prefix(a, d, p, tx, ty, s_off[d][p], s_lo[d][p]);
+  }
 #pragma unroll
   for (int p = 0; p < 3; ++p) {
     const SharedView v = tile_view(a, sm, p, tx, ty);
@@ -1586,7 +1705,7 @@ __device__ __forceinline__ void deblock_tile(const TileParams &a, int t) {
   }
   __syncthreads();
   // expand the ranges into the lists: one warp per (pass, plane, band)
-  for (int task = warp; task < 6 * kTileBands; task += n_warps) {
+  for (int task = warp; task < (a.grid_mode ? 0 : 6 * kTileBands); task += n_warps) {
     const int dp = task / kTileBands, j = task % kTileBands, d = dp / 3, p = dp % 3;
     const uint32_t o = s_off[d][p][j], cnt = s_off[d][p][j + 1] - o, lo = s_lo[d][p][j];
     uint32_t *list = p == 0 ? s_list_y[d] : s_list_c[d][p - 1];
@@ -1769,6 +1888,251 @@ int launch_deblock(cudaStream_t st, const DPlane planes[3], int bit_depth, const
     H266_CUDA(cudaGetLastError());
     ++*launches;
   }
+  return H266_OK;
+}
+
+// ===================================================================== device-built side information
+bool device_walk_eligible(const h266_picture &pic, const h266_deblock_cu *cus, uint64_t n_cus,
+                          const h266_deblock_cu *chroma_cus, uint64_t n_chroma, const h266_deblock_params &params,
+                          uint32_t cfi) {
+  if (params.disabled || params.bit_depth < 8 || params.bit_depth > 16 || params.ctb_log2_size_y > 16) return false;
+  const int w = (int)pic.luma.width, h = (int)pic.luma.height;
+  const bool chroma = (uint64_t)pic.cb.width * pic.cb.height != 0 || (uint64_t)pic.cr.width * pic.cr.height != 0;
+  if (cfi > 1 || (cfi == 0 && chroma)) return false;
+  if (chroma && (pic.cb.width != (pic.luma.width + 1) / 2 || pic.cb.height != (pic.luma.height + 1) / 2 ||
+                 pic.cr.width != pic.cb.width || pic.cr.height != pic.cb.height))
+    return false;
+  if (n_cus > (uint64_t)INT32_MAX || n_chroma > (uint64_t)INT32_MAX) return false;
+  // no CU overlaps another (the walk's emissions then never collide)
+  const int cw4 = (w + 3) / 4, ch4 = (h + 3) / 4;
+  thread_local std::vector<uint8_t> seen;
+  const h266_deblock_cu *lists[2] = {cus, chroma_cus};
+  const uint64_t counts[2] = {n_cus, chroma_cus ? n_chroma : 0};
+  for (int l = 0; l < 2; ++l) {
+    if (!lists[l]) continue;
+    seen.assign((size_t)cw4 * ch4, 0);
+    for (uint64_t i = 0; i < counts[l]; ++i) {
+      const h266_deblock_cu &c = lists[l][i];
+      if ((c.x | c.y | c.w | c.h) & 3 || c.w < 8 || c.h < 8) return false;  // 4-sample edges chain
+      if ((uint64_t)c.x + c.w > (uint64_t)w || (uint64_t)c.y + c.h > (uint64_t)h) return false;
+      if (c.has_num_sb) return false;  // sub-block edges (maxFilterLength 5 next to 8-spaced edges)
+      if (c.has_tb_split) {
+        const uint32_t dim = c.tb_split.vertical ? c.w : c.h;
+        if (c.tb_split.n_bounds < 1 || c.tb_split.n_bounds > 3) return false;
+        uint32_t prev = 0;
+        for (int k = 0; k < c.tb_split.n_bounds; ++k) {
+          const uint32_t b = c.tb_split.bounds[k];
+          if (b < prev + 8) return false;  // transform blocks narrower than 8
+          prev = b;
+        }
+        if (dim < prev + 8) return false;
+      }
+      for (uint32_t y = c.y / 4; y < (c.y + c.h) / 4; ++y)
+        for (uint32_t x = c.x / 4; x < (c.x + c.w) / 4; ++x) {
+          uint8_t &o = seen[(size_t)y * cw4 + x];
+          if (o) return false;
+          o = 1;
+        }
+    }
+  }
+  return true;
+}
+
+namespace {
+
+struct DevCuGrid {  // CuGrid::cu_at on device memory
+  const int32_t *cells;
+  int cw, ch;
+  __device__ int64_t at(int x, int y) const {
+    if (x < 0 || y < 0 || x / 4 >= cw || y / 4 >= ch) return -1;
+    return cells[(size_t)(y / 4) * cw + x / 4];
+  }
+};
+
+struct GridEmit {  // a segment into its grid cell
+  EdgeSeg *g;
+  uint32_t slots, bands;
+  int unit, pu;
+  __device__ void operator()(const EdgeSeg &s) {
+    const bool vert = s.flags & 1;
+    const uint32_t band = (uint32_t)((vert ? s.y : s.x) / unit), pos = (uint32_t)((vert ? s.x : s.y) / pu);
+    if (band < bands && pos < slots) g[(size_t)band * slots + pos] = s;
+  }
+};
+
+// Motion by CU: every 4x4 cell of a CU carries the same motion (checked on
+// the host), so the cell's motion is its CU's record.
+struct CuMotion {
+  const h266_deblock_mv_grid *g;  // presence only
+  const h266_deblock_mv_cell *per_cu;
+  DevCuGrid grid;
+  __device__ const h266_deblock_mv_cell &at(int x, int y) const {
+    const int64_t i = grid.at(x, y);
+    return i < 0 ? kNoMotionDev : per_cu[i];
+  }
+};
+
+struct WalkParams {
+  const h266_deblock_cu *cus[2];  // luma list, chroma list
+  uint32_t n[2];
+  int32_t *cu_grid[2];
+  int cw4, ch4;
+  h266_deblock_mv_grid mv;
+  int has_mv;
+  const h266_deblock_mv_cell *mv_per_cu;  // non-null: motion by luma CU instead of the grid
+  const uint32_t *nf[2];  // columns (vertical pass), rows (horizontal pass)
+  uint32_t n_nf[2];
+  PlaneCfg cfg[3];
+  EdgeSeg *grid[2][3];
+  uint32_t slots[2][3], bands[2][3];
+};
+
+// CuGrid::build: cell -> CU covering it, the later CU winning (here: the larger index).
+__global__ void k_cu_grid(const __grid_constant__ WalkParams a, int list) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n[list]) return;
+  const h266_deblock_cu &c = a.cus[list][i];
+  const int x0 = c.x / 4, y0 = c.y / 4;
+  const int x1 = min((int)((c.x + c.w + 3) / 4), a.cw4), y1 = min((int)((c.y + c.h + 3) / 4), a.ch4);
+  for (int y = y0; y < y1; ++y)
+    for (int x = x0; x < x1; ++x) atomicMax(&a.cu_grid[list][(size_t)y * a.cw4 + x], (int32_t)i);
+}
+
+// The edge walk of one CU for one (plane, pass) list: blockIdx.y = plane * 2 + pass.
+__global__ void __launch_bounds__(128) k_walk(const __grid_constant__ WalkParams a) {
+  const int l = blockIdx.y, plane = l / 2, d = l % 2;
+  const int list = plane ? 1 : 0;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n[list]) return;
+  const DevCuGrid grid{a.cu_grid[list], a.cw4, a.ch4};
+  GridEmit emit{a.grid[d][plane], a.slots[d][plane], a.bands[d][plane], plane ? 2 : 4, plane ? 8 : 4};
+  if (plane == 0 && a.has_mv && a.mv_per_cu) {
+    const CuMotion mv{&a.mv, a.mv_per_cu, DevCuGrid{a.cu_grid[0], a.cw4, a.ch4}};
+    walk_cu(a.cus[list], grid, a.cfg[plane], d == 0, mv, a.nf[d], a.n_nf[d], i, emit);
+  } else {
+    const MvGrid mv{plane == 0 && a.has_mv ? &a.mv : nullptr};
+    walk_cu(a.cus[list], grid, a.cfg[plane], d == 0, mv, a.nf[d], a.n_nf[d], i, emit);
+  }
+}
+
+size_t align_up(size_t n) { return (n + 255) & ~(size_t)255; }
+
+struct WalkLayout {
+  size_t cu_grid[2], grid[2][3], total;
+  uint32_t slots[2][3], bands[2][3];
+};
+
+WalkLayout walk_layout(const DeviceWalkIn &in) {
+  WalkLayout L{};
+  const size_t cells = (size_t)((in.w + 3) / 4) * ((in.h + 3) / 4);
+  size_t off = 0;
+  for (int l = 0; l < 2; ++l) {
+    L.cu_grid[l] = off;
+    if (l == 0 || in.chroma_cus != in.cus) off += align_up(cells * 4);
+  }
+  if (in.chroma_cus == in.cus) L.cu_grid[1] = L.cu_grid[0];
+  for (int d = 0; d < 2; ++d)
+    for (int p = 0; p < 3; ++p) {
+      const bool has = p == 0 || in.cfi != 0;
+      const int pw = p ? in.cw : in.w, ph = p ? in.ch : in.h;
+      const int unit = p ? 2 : 4, pu = p ? 8 : 4;
+      L.bands[d][p] = has && pw > 0 && ph > 0 ? (uint32_t)(((d == 0 ? ph : pw) + unit - 1) / unit) : 0;
+      L.slots[d][p] = has && pw > 0 && ph > 0 ? (uint32_t)(((d == 0 ? pw : ph) + pu - 1) / pu) : 0;
+      L.grid[d][p] = off;
+      off += align_up((size_t)L.bands[d][p] * L.slots[d][p] * sizeof(EdgeSeg));
+    }
+  L.total = off;
+  return L;
+}
+
+}  // namespace
+
+size_t device_walk_bytes(const DeviceWalkIn &in) { return walk_layout(in).total; }
+
+int launch_device_walk(cudaStream_t st, const DeviceWalkIn &in, uint8_t *scratch, DeviceWalkOut &out,
+                       uint64_t *launches) {
+  const WalkLayout L = walk_layout(in);
+  WalkParams a;
+  std::memset(&a, 0, sizeof a);
+  const bool sep = in.chroma_cus != in.cus;
+  a.cus[0] = in.cus;
+  a.cus[1] = in.chroma_cus;
+  a.n[0] = (uint32_t)in.n_cus;
+  a.n[1] = (uint32_t)(sep ? in.n_chroma : in.n_cus);
+  a.cw4 = (in.w + 3) / 4;
+  a.ch4 = (in.h + 3) / 4;
+  a.cu_grid[0] = reinterpret_cast<int32_t *>(scratch + L.cu_grid[0]);
+  a.cu_grid[1] = reinterpret_cast<int32_t *>(scratch + L.cu_grid[1]);
+  a.has_mv = in.mv_cells != nullptr || in.mv_per_cu != nullptr;
+  a.mv_per_cu = in.mv_per_cu;
+  a.mv.cells = in.mv_cells;
+  a.mv.cells_w = in.mv_w;
+  a.mv.cells_h = in.mv_h;
+  a.nf[0] = in.nf_cols;
+  a.nf[1] = in.nf_rows;
+  a.n_nf[0] = (uint32_t)in.n_cols;
+  a.n_nf[1] = (uint32_t)in.n_rows;
+  const h266_deblock_params &pr = in.params;
+  const int bd = (int)pr.bit_depth;
+  const uint32_t ctb = 1u << pr.ctb_log2_size_y;
+  a.cfg[0] = PlaneCfg{0, 1, 1, pr.luma_beta_offset_div2, pr.luma_tc_offset_div2, 0, bd, ctb};
+  a.cfg[1] = PlaneCfg{1, 2, 2, pr.cb_beta_offset_div2, pr.cb_tc_offset_div2, pr.chroma_qp_offset_cb, bd, ctb};
+  a.cfg[2] = PlaneCfg{2, 2, 2, pr.cr_beta_offset_div2, pr.cr_tc_offset_div2, pr.chroma_qp_offset_cr, bd, ctb};
+  for (int d = 0; d < 2; ++d)
+    for (int p = 0; p < 3; ++p) {
+      a.grid[d][p] = reinterpret_cast<EdgeSeg *>(scratch + L.grid[d][p]);
+      a.slots[d][p] = L.slots[d][p];
+      a.bands[d][p] = L.bands[d][p];
+      out.grid[d][p] = a.grid[d][p];
+      out.slots[d][p] = L.slots[d][p];
+      out.bands[d][p] = L.bands[d][p];
+    }
+  out.tiles_x = (uint32_t)((in.w + kDeblockTile - 1) / kDeblockTile);
+  out.tiles_y = (uint32_t)((in.h + kDeblockTile - 1) / kDeblockTile);
+  // CU maps to -1 (no CU), segment grids to bS 0 (no segment)
+  const size_t cells = (size_t)a.cw4 * a.ch4;
+  H266_CUDA(cudaMemsetAsync(a.cu_grid[0], 0xFF, cells * 4, st));
+  if (sep) H266_CUDA(cudaMemsetAsync(a.cu_grid[1], 0xFF, cells * 4, st));
+  H266_CUDA(cudaMemsetAsync(scratch + L.grid[0][0], 0, L.total - L.grid[0][0], st));
+  const int lists = in.cfi != 0 ? 6 : 2;
+  for (int l = 0; l < (sep && in.cfi != 0 ? 2 : 1); ++l) {
+    if (!a.n[l]) continue;
+    k_cu_grid<<<(a.n[l] + 127) / 128, 128, 0, st>>>(a, l);
+    H266_CUDA(cudaGetLastError());
+    ++*launches;
+  }
+  const uint32_t nmax = std::max(a.n[0], a.n[1]);
+  if (nmax) {
+    k_walk<<<dim3((nmax + 127) / 128, lists), 128, 0, st>>>(a);
+    H266_CUDA(cudaGetLastError());
+    ++*launches;
+  }
+  return H266_OK;
+}
+
+int launch_deblock_tiles_grid(cudaStream_t st, const DPlane src[3], const DPlane dst[3], const uint16_t *lut,
+                              int bit_depth, const DeviceWalkOut &g, uint64_t *launches) {
+  TileParams a;
+  std::memset(&a, 0, sizeof a);
+  for (int i = 0; i < 3; ++i) {
+    a.src[i] = src[i];
+    a.dst[i] = dst[i];
+    for (int d = 0; d < 2; ++d) {
+      a.n_bands[d][i] = g.bands[d][i];
+      a.grid[d][i] = g.grid[d][i];
+      a.grid_slots[d][i] = g.slots[d][i];
+    }
+  }
+  a.grid_mode = 1;
+  a.lut = lut;
+  a.tiles_x = g.tiles_x;
+  a.tiles_y = g.tiles_y;
+  a.maxv = (1 << bit_depth) - 1;
+  const uint64_t n = (uint64_t)g.tiles_x * g.tiles_y;
+  if (!n) return H266_OK;
+  k_deblock_tiles<<<(unsigned)n, kTileThreads, kTileSmem, st>>>(a);
+  H266_CUDA(cudaGetLastError());
+  ++*launches;
   return H266_OK;
 }
 

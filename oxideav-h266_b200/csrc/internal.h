@@ -178,6 +178,37 @@ uint32_t fill_deblock_tile_params(void *out, const DPlane src[3], const DPlane d
                                   uint32_t tiles_y);
 int launch_deblock_tiles_batch(cudaStream_t st, const void *d_params, const uint32_t *d_first, int n, uint32_t ctas,
                                uint64_t *launches);
+// ---------------------------------------------------------------- device-built side information
+// For pictures whose deblocking has no chained edges (every component one
+// segment: luma CUs and transform blocks at least 8x8, no sub-block edges,
+// no overlapping CUs, CUs inside the picture, 4:2:0 or 4:0:0), the edge walk
+// runs on the device from the CU list and the motion grid and writes each
+// segment to a dense per-band grid that the tile kernel scans.
+bool device_walk_eligible(const h266_picture &pic, const h266_deblock_cu *cus, uint64_t n_cus,
+                          const h266_deblock_cu *chroma_cus, uint64_t n_chroma, const h266_deblock_params &params,
+                          uint32_t cfi);
+struct DeviceWalkIn {  // device pointers
+  const h266_deblock_cu *cus, *chroma_cus;  // chroma_cus == cus for a single tree
+  uint64_t n_cus, n_chroma;
+  const h266_deblock_mv_cell *mv_cells;  // nullptr: no motion grid (or motion by CU)
+  uint64_t mv_w, mv_h;
+  const h266_deblock_mv_cell *mv_per_cu;  // motion by luma CU when every CU's cells agree
+  const uint32_t *nf_cols, *nf_rows;
+  uint64_t n_cols, n_rows;
+  h266_deblock_params params;
+  uint32_t cfi;
+  int w, h, cw, ch;  // luma and chroma plane sizes
+};
+size_t device_walk_bytes(const DeviceWalkIn &in);  // scratch for the CU maps and segment grids
+struct DeviceWalkOut {
+  EdgeSeg *grid[2][3];
+  uint32_t slots[2][3], bands[2][3];
+  uint32_t tiles_x, tiles_y;
+};
+int launch_device_walk(cudaStream_t st, const DeviceWalkIn &in, uint8_t *scratch, DeviceWalkOut &out,
+                       uint64_t *launches);
+int launch_deblock_tiles_grid(cudaStream_t st, const DPlane src[3], const DPlane dst[3], const uint16_t *lut,
+                              int bit_depth, const DeviceWalkOut &g, uint64_t *launches);
 int launch_deblock(cudaStream_t st, const DPlane planes[3], int bit_depth, const EdgeSeg *d_segs_v,
                    const uint32_t *d_comp_v, uint32_t n_comp_v, const EdgeSeg *d_segs_h, const uint32_t *d_comp_h,
                    uint32_t n_comp_h, uint64_t *launches);

@@ -29,7 +29,8 @@ _LIB = None
 # Every symbol declared in include/oxideav_h266_b200.h.
 EXPORTS = [
     "h266_ctx_create", "h266_ctx_destroy", "h266_ctx_set_stream", "h266_ctx_synchronize", "h266_last_error",
-    "h266_ctx_kernel_launches", "h266_derive_lmcs", "h266_lmcs_inverse_map_luma", "h266_apply_deblocking_clipped",
+    "h266_ctx_kernel_launches", "h266_ctx_transfer_bytes", "h266_derive_lmcs", "h266_lmcs_inverse_map_luma",
+    "h266_apply_deblocking_clipped",
     "h266_apply_sao_clipped", "h266_apply_alf_clipped", "h266_apply_in_loop_filters",
     "h266_apply_in_loop_filters_batch", "h266_ctx_set_profiling", "h266_ctx_profile", "h266_chain_plan_create",
     "h266_chain_plan_execute", "h266_chain_plan_execute_batch", "h266_chain_plan_destroy",
@@ -59,6 +60,7 @@ def lib():
         L.h266_last_error.restype = C.c_char_p
         L.h266_ctx_kernel_launches.argtypes = [vp]
         L.h266_ctx_kernel_launches.restype = u64
+        L.h266_ctx_transfer_bytes.argtypes = [vp, C.POINTER(u64), C.POINTER(u64)]
         L.h266_derive_lmcs.argtypes = [vp, u32, vp]
         L.h266_lmcs_inverse_map_luma.argtypes = [vp, vp, vp, u32, u32]
         L.h266_apply_deblocking_clipped.argtypes = [vp, vp, vp, u64, vp, u64, vp, vp, u32, vp, u64, vp, u64]
@@ -163,6 +165,12 @@ class Context:
     @property
     def kernel_launches(self) -> int:
         return lib().h266_ctx_kernel_launches(self._h)
+
+    def transfer_bytes(self) -> tuple:
+        """(host -> device, device -> host) bytes the context has queued."""
+        a, b = C.c_uint64(), C.c_uint64()
+        _check(lib().h266_ctx_transfer_bytes(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def synchronize(self):
         _check(lib().h266_ctx_synchronize(self._h))

@@ -325,6 +325,55 @@ def test_strip_deblocking_parity(kind, monkeypatch):
         c.close()
 
 
+@pytest.mark.parametrize("kind", ["c1", "c2_small", "ctb64_8bit", "odd_tail"])
+def test_device_built_side_information(ctx, kind):
+    """Pictures without chained edges build their deblocking side information
+    on the device (CU map, edge walk into per-band grids, grid-mode tiles):
+    bit-exact, and the builder's kernels are the ones that ran."""
+    pic, fa = WORKLOADS[kind](8)
+    got, want = pic.copy(), pic.copy()
+    l0 = ctx.kernel_launches
+    ctx.apply_in_loop_filters(got, fa)
+    launches = ctx.kernel_launches - l0
+    oracle.apply_in_loop_filters(want, fa)
+    assert_same(got, want, f"device-built side information {kind}")
+    lut = 1 if fa.lmcs is not None else 0
+    assert launches == lut + 2 + 1 + 1  # LUT, CU map + walk, tiles, SAO/ALF
+
+
+def test_device_built_side_information_with_per_cell_motion(ctx):
+    """A motion grid whose cells differ inside a CU is uploaded whole (not as
+    one record per CU); the device walk reads it cell by cell."""
+    pic, fa = small_c2(12)
+    cus = fa.cus
+    inter = [i for i in range(len(cus)) if not cus["intra"][i] and cus["w"][i] >= 16 and cus["h"][i] >= 16]
+    assert inter
+    for i in inter[::3]:
+        cy, cx = (int(cus["y"][i]) + 4) // 4, (int(cus["x"][i]) + 8) // 4
+        fa.mv["mv_l0"][cy, cx, 0] += 96  # a sub-CU motion difference
+    got, want = pic.copy(), pic.copy()
+    ctx.apply_in_loop_filters(got, fa)
+    oracle.apply_in_loop_filters(want, fa)
+    assert_same(got, want, "per-cell motion")
+
+
+@pytest.mark.parametrize("kind", ["c2_small", "ctb64_8bit"])
+def test_host_built_side_information_on_eligible_pictures(kind, monkeypatch):
+    monkeypatch.setenv("H266_FORCE_HOST_SIDEINFO", "1")
+    c = native.Context(0)
+    try:
+        pic, fa = WORKLOADS[kind](9)
+        got, want = pic.copy(), pic.copy()
+        l0 = c.kernel_launches
+        c.apply_in_loop_filters(got, fa)
+        launches = c.kernel_launches - l0
+        oracle.apply_in_loop_filters(want, fa)
+        assert_same(got, want, f"host-built side information {kind}")
+        assert launches == (1 if fa.lmcs is not None else 0) + 1 + 1
+    finally:
+        c.close()
+
+
 def test_wide_coefficients_take_the_scalar_path(ctx):
     """Coefficients outside int8 are legal input for the reference; they must
     still filter bit-exactly (through the scalar kernel)."""
