@@ -818,6 +818,10 @@ int prepare_chain(Prep &pr, const h266_picture &pic, const h266_in_loop_filter_a
     w.cfi = a.chroma_format_idc;
     w.w = (int)pic.luma.width;
     w.h = (int)pic.luma.height;
+    w.max_cu_dim = 4;
+    for (uint64_t i = 0; i < a.n_cus; ++i) w.max_cu_dim = std::max(w.max_cu_dim, std::max(a.cus[i].w, a.cus[i].h));
+    for (uint64_t i = 0; db.dw_sep && i < a.n_chroma_cus; ++i)
+      w.max_cu_dim = std::max(w.max_cu_dim, std::max(a.chroma_cus[i].w, a.chroma_cus[i].h));
     w.cw = (int)pic.cb.width;
     w.ch = (int)pic.cb.height;
     pr.st.dw_cus = blob.put(a.cus, a.n_cus * sizeof(h266_deblock_cu));

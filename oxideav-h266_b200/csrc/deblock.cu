@@ -229,9 +229,11 @@ H266_HD inline int bs_of(uint32_t comp, const h266_deblock_cu &p, const h266_deb
 // owns, in the reference's order, passed to `emit`.  `grid.at(x, y)` is the
 // CU covering luma sample (x, y) (CuGrid::cu_at), -1 for none.
 #pragma nv_exec_check_disable
+// `only_off` >= 0 restricts the walk to the edge at that offset inside the CU
+// (the device runs one thread per offset).
 template <class Grid, class Mv, class Emit>
 H266_HD void walk_cu(const h266_deblock_cu *cus_, const Grid &grid, const PlaneCfg &pc, bool vert, const Mv &mv,
-                     const uint32_t *nf, uint64_t n_nf, size_t idx, Emit &emit) {
+                     const uint32_t *nf, uint64_t n_nf, size_t idx, Emit &emit, int only_off = -1) {
   const h266_deblock_cu &cu = cus_[idx];
   const bool chroma = pc.comp != 0;
   if (chroma && ((vert ? cu.x / pc.sub_w : cu.y / pc.sub_h) % 8) != 0) return;
@@ -247,7 +249,8 @@ H266_HD void walk_cu(const h266_deblock_cu *cus_, const Grid &grid, const PlaneC
   const uint32_t last_sb = std::min(n8 - 1, nsb - 1);
   const uint32_t ctb_h_c = pc.ctb / std::max(pc.sub_h, 1u);
   Cu q_geo{cu};
-  for (uint32_t off = 0; off < n_cb; off += step) {
+  for (uint32_t off = only_off >= 0 ? (uint32_t)only_off : 0; off < n_cb; off += step) {
+    if (only_off >= 0 && off != (uint32_t)only_off) break;
     const bool is_tb = off == 0 ? filter_edge : q_geo.tb_boundary(off, vert, chroma);
     const bool is_sb = !chroma && off % sb == 0 && off / sb <= last_sb && (off > 0 || filter_edge);
     if (!is_tb && !is_sb) continue;
@@ -1998,20 +2001,26 @@ __global__ void k_cu_grid(const __grid_constant__ WalkParams a, int list) {
     for (int x = x0; x < x1; ++x) atomicMax(&a.cu_grid[list][(size_t)y * a.cw4 + x], (int32_t)i);
 }
 
-// The edge walk of one CU for one (plane, pass) list: blockIdx.y = plane * 2 + pass.
+// The edge walk of one CU for one (plane, pass) list (blockIdx.y = plane * 2 +
+// pass) at one edge offset (blockIdx.z: offset / step; offsets beyond the CU
+// return at once).
 __global__ void __launch_bounds__(128) k_walk(const __grid_constant__ WalkParams a) {
   const int l = blockIdx.y, plane = l / 2, d = l % 2;
   const int list = plane ? 1 : 0;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.n[list]) return;
+  const h266_deblock_cu &cu = a.cus[list][i];
+  const uint32_t step = plane ? 8 * (d == 0 ? a.cfg[plane].sub_w : a.cfg[plane].sub_h) : 4;
+  const uint32_t off = blockIdx.z * step;
+  if (off >= (d == 0 ? cu.w : cu.h)) return;
   const DevCuGrid grid{a.cu_grid[list], a.cw4, a.ch4};
   GridEmit emit{a.grid[d][plane], a.slots[d][plane], a.bands[d][plane], plane ? 2 : 4, plane ? 8 : 4};
   if (plane == 0 && a.has_mv && a.mv_per_cu) {
     const CuMotion mv{&a.mv, a.mv_per_cu, DevCuGrid{a.cu_grid[0], a.cw4, a.ch4}};
-    walk_cu(a.cus[list], grid, a.cfg[plane], d == 0, mv, a.nf[d], a.n_nf[d], i, emit);
+    walk_cu(a.cus[list], grid, a.cfg[plane], d == 0, mv, a.nf[d], a.n_nf[d], i, emit, (int)off);
   } else {
     const MvGrid mv{plane == 0 && a.has_mv ? &a.mv : nullptr};
-    walk_cu(a.cus[list], grid, a.cfg[plane], d == 0, mv, a.nf[d], a.n_nf[d], i, emit);
+    walk_cu(a.cus[list], grid, a.cfg[plane], d == 0, mv, a.nf[d], a.n_nf[d], i, emit, (int)off);
   }
 }
 
@@ -2102,8 +2111,11 @@ int launch_device_walk(cudaStream_t st, const DeviceWalkIn &in, uint8_t *scratch
     ++*launches;
   }
   const uint32_t nmax = std::max(a.n[0], a.n[1]);
+  // offsets per CU: at most max dimension / 4 (luma; chroma has fewer)
+  uint32_t max_dim = 4;
+  max_dim = std::max(max_dim, in.max_cu_dim);
   if (nmax) {
-    k_walk<<<dim3((nmax + 127) / 128, lists), 128, 0, st>>>(a);
+    k_walk<<<dim3((nmax + 127) / 128, lists, (max_dim + 3) / 4), 128, 0, st>>>(a);
     H266_CUDA(cudaGetLastError());
     ++*launches;
   }

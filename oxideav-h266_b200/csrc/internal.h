@@ -197,7 +197,8 @@ struct DeviceWalkIn {  // device pointers
   uint64_t n_cols, n_rows;
   h266_deblock_params params;
   uint32_t cfi;
-  int w, h, cw, ch;  // luma and chroma plane sizes
+  int w, h, cw, ch;      // luma and chroma plane sizes
+  uint32_t max_cu_dim;   // largest CU width or height of both lists
 };
 size_t device_walk_bytes(const DeviceWalkIn &in);  // scratch for the CU maps and segment grids
 struct DeviceWalkOut {
