@@ -300,6 +300,141 @@ def run_configs(ctx, local_rank, stream, steps: int):
     return out
 
 
+def run_encoder_trials(ctx, local_rank, stream, steps: int, n_pics: int = 4):
+    """Encoder luma ALF decision (src/alf_enc.rs:352-528: 16 fixed sets + one
+    APS set per CTB, commit of the winners) on device-resident 1920x1080 10-bit
+    pictures: per call one trial pass over all 17 sets, the decision and the
+    commit.  The original is the picture plus seeded noise in [-6, 6].  The
+    oracle's restatement runs the reference's 17 full apply_alf passes."""
+    import numpy as np
+    import torch
+
+    import oracle
+    from oxideav_h266_b200 import abi, native
+    from oxideav_h266_b200 import workloads as W
+
+    items = []
+    for i in range(n_pics):
+        rec, fa = W.config2(5000 + i)
+        rng = np.random.Generator(np.random.PCG64(5100 + i))
+        src = rec.copy()
+        src.luma = np.clip(rec.luma.astype(np.int64) + rng.integers(-6, 7, size=rec.luma.shape), 0, 1023).astype(
+            np.uint16)
+        items.append((src, rec, fa.apses[0]))
+    devs = [(native.DevicePicture.from_host(s_, local_rank), native.DevicePicture.from_host(r_, local_rank),
+             native.DevicePicture.from_host(r_, local_rank), a) for s_, r_, a in items]
+    px = 1920 * 1080
+
+    def restore(d):
+        for dst, src_ in zip((d[2].luma, d[2].cb, d[2].cr), (d[1].luma, d[1].cb, d[1].cr)):
+            dst.copy_(src_)
+
+    for d in devs:  # warm-up
+        for _ in range(3):
+            restore(d)
+            native.alf_decide_and_apply(ctx, d[0], d[2], d[3], ctb_log2=7, bit_depth=10)
+    torch.cuda.synchronize()
+    ctx.set_profiling(True)
+    ctx.profile()
+    total, calls = 0.0, 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(max(1, steps)):
+        for d in devs:
+            restore(d)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            native.alf_decide_and_apply(ctx, d[0], d[2], d[3], ctb_log2=7, bit_depth=10)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            total += e0.elapsed_time(e1)
+            calls += 1
+    prof = ctx.profile()
+    ctx.set_profiling(False)
+    ms = total / calls
+    dev_ms = prof["sao_alf"][0] / calls
+    s_, r_, a = items[0]
+    r2 = r_.copy()
+    t0 = time.perf_counter()
+    oracle.alf_decide_and_apply(s_, r2, a, ctb_log2=7, bit_depth=10, alf_ctb_dtype=abi.ALF_CTB)
+    cpu_ms = (time.perf_counter() - t0) * 1e3
+    del devs
+    torch.cuda.synchronize()
+    return {"workload": "encoder luma ALF decision, 1920x1080 10-bit CTU 128, 16 fixed sets + 1 APS set",
+            "pictures": n_pics, "calls": calls, "ms_per_picture": round(ms, 4), "mpx_per_s": round(px / ms / 1e3, 1),
+            "kernel_ms_per_picture": round(dev_ms, 4),
+            "path": "h266_alf_decide_and_apply_clipped on H266_MEM_DEVICE pictures (trials, decision, commit, "
+                    "decisions copied back)",
+            "cpu_oracle": {"ms_per_picture": round(cpu_ms, 1), "mpx_per_s": round(px / cpu_ms / 1e3, 2), "cores": 1,
+                           "kind": "port", "sample": "one picture, the reference's 17 apply_alf trial passes"}}
+
+
+def run_recon_io(ctx, local_rank, stream, steps: int, peak_gbs: float):
+    """The steps either side of the chain on device-resident 1920x1080 10-bit
+    pictures: the forward LMCS map over every CU of the picture (disjoint
+    rectangles covering it), the chroma residual add of every chroma TB with
+    LMCS scaling, and the cropped 16-bit planar dump into device memory.
+    Kernel time from the context's per-family CUDA events; bandwidth from the
+    algorithmic bytes (read + write of every touched sample)."""
+    import numpy as np
+    import torch
+
+    from oxideav_h266_b200 import abi, native
+    from oxideav_h266_b200 import workloads as W
+
+    pic, fa = W.config2(6000)
+    dp = native.DevicePicture.from_host(pic, local_rank)
+    cus = fa.cus
+    rects = np.zeros(len(cus), dtype=abi.RECT)
+    rects["x"], rects["y"], rects["w"], rects["h"] = cus["x"], cus["y"], cus["w"], cus["h"]
+    rng = np.random.Generator(np.random.PCG64(6001))
+    blocks = np.zeros(2 * len(cus), dtype=abi.RES_BLOCK)
+    blocks["x"] = np.repeat(cus["x"] // 2, 2)
+    blocks["y"] = np.repeat(cus["y"] // 2, 2)
+    blocks["w"] = np.repeat(cus["w"] // 2, 2)
+    blocks["h"] = np.repeat(cus["h"] // 2, 2)
+    blocks["plane"] = np.tile([1, 2], len(cus))
+    blocks["var_scale"] = rng.integers(1024, 4096, len(blocks))
+    area = (blocks["w"].astype(np.uint64) * blocks["h"])
+    blocks["res_offset"] = np.concatenate([[0], np.cumsum(area)[:-1]])
+    res = torch.tensor(rng.integers(-64, 65, int(area.sum()), dtype=np.int32), device=f"cuda:{local_rank}")
+    crop = (0, 0, 1920, 1080)
+    dst = torch.zeros(1920 * 1080 * 3, dtype=torch.uint8, device=f"cuda:{local_rank}")
+    legs = {
+        "lmcs_forward_map": (lambda: native.lmcs_forward_map_luma_rects(ctx, dp, fa.lmcs, rects), "lmcs",
+                             4 * int((rects["w"].astype(np.int64) * rects["h"]).sum())),
+        "chroma_residual_add": (lambda: native.lmcs_add_chroma_residual(ctx, dp, 10, res, blocks), "lmcs",
+                                8 * int(area.sum())),
+        "output_dump_16bit": (lambda: native.output_convert(ctx, dp, crop, 1, 10, dst=dst), "copy",
+                              4 * 1920 * 1080 * 3 // 2),
+    }
+    out = {}
+    for name, (fn, fam, bytes_) in legs.items():
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        ctx.set_profiling(True)
+        ctx.profile()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        prof = ctx.profile()
+        ctx.set_profiling(False)
+        k_ms = prof[fam][0] / steps
+        gbs = bytes_ / k_ms / 1e6
+        out[name] = {"ms_per_call": round(e0.elapsed_time(e1) / steps, 4), "kernel_ms": round(k_ms, 4),
+                     "algorithmic_bytes": bytes_, "achieved_gbs": round(gbs, 1),
+                     "frac_of_measured_hbm": round(gbs / peak_gbs, 3)}
+    out["workload"] = ("1920x1080 10-bit: forward map over the picture's CUs (disjoint, covering it); chroma "
+                       "residual add with LMCS scaling over every chroma TB; cropped 16-bit planar dump to device "
+                       "memory")
+    del dp, res, dst
+    torch.cuda.synchronize()
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -451,6 +586,11 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and world == 1 and args.configs:
         configs = run_configs(ctx, local_rank, stream, max(1, min(args.steps, 10)))
 
+    trials = recon = None
+    if rank == 0 and world == 1 and args.trials:
+        trials = run_encoder_trials(ctx, local_rank, stream, max(1, min(args.steps, 5)))
+        recon = run_recon_io(ctx, local_rank, stream, max(3, min(args.steps, 20)), peaks["hbm_gbs"])
+
     cpu = None
     if rank == 0 and world == 1:
         cpu = cpu_baseline(items, os.cpu_count() or 1)
@@ -463,7 +603,8 @@ def run_ours(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic (seeded 1080p config generator)",
             "config": workload_config(args.batch, world),
-            "roofline": roofline, "plain": plain, "served": served, "configs": configs, "cpu_baseline": cpu, "e2e": e2e,
+            "roofline": roofline, "plain": plain, "served": served, "configs": configs, "encoder_alf_trials": trials, "recon_io": recon,
+            "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches),
             "clocks": clocks,
         }
@@ -517,6 +658,7 @@ def main():
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--configs", type=int, default=1, help="measure the 2160p-tiles and mixed-size batches (0: skip)")
+    ap.add_argument("--trials", type=int, default=1, help="measure the encoder ALF trial decision (0: skip)")
     ap.add_argument("--served-seconds", type=float, default=2.0,
                     help="seconds of Poisson arrivals per served measurement (0: skip)")
     args = ap.parse_args()

@@ -290,6 +290,70 @@ int h266_derive_lmcs(const h266_lmcs_data *data, uint32_t bit_depth, h266_lmcs_d
 int h266_lmcs_inverse_map_luma(h266_ctx *ctx, h266_picture *pic, const h266_lmcs_derived *lmcs,
                                uint32_t lmcs_min_bin_idx, uint32_t lmcs_max_bin_idx);
 
+/* ---- recon-side LMCS (src/lmcs.rs:169-290, src/ctu.rs:734-742, 1701-1815) */
+typedef struct h266_rect {
+    uint32_t x, y, w, h;
+} h266_rect;
+
+/* CtuWalker::lmcs_forward_map_luma_rect (src/ctu.rs:1701-1727) over a list of
+ * rectangles, in list order: every luma sample of each rectangle (clipped to
+ * the plane) becomes Clip1(forward_map_luma_sample(s)) (src/lmcs.rs:186-194,
+ * eq. 1213).  A sample inside k rectangles is mapped k times, as in the
+ * crate's loop.  The crate has no bin for a sample above (1 << BitDepth) - 1
+ * (its table index runs out of bounds): such a sample makes the call return
+ * H266_ERR_INVALID_ARGUMENT.  Waits for the context stream. */
+int h266_lmcs_forward_map_luma_rects(h266_ctx *ctx, h266_picture *pic, const h266_lmcs_derived *lmcs,
+                                     const h266_rect *rects, uint64_t n_rects);
+
+typedef struct h266_lmcs_cvs_block { /* one CU's eq. 1216 inputs (src/ctu.rs:1752-1815) */
+    uint32_t x_cu_cb, y_cu_cb; /* luma origin of the CU holding the sizeY-aligned corner */
+    uint8_t avail_l, avail_t;  /* nb_in_region() of the left / top neighbour; the
+                                  picture-edge tests x_cu_cb > 0, y_cu_cb > 0 are applied here */
+    uint8_t reserved[2];
+} h266_lmcs_cvs_block;
+
+/* CtuWalker::lmcs_chroma_var_scale_for_cu (src/ctu.rs:1752-1815) from the CU
+ * origin and neighbour availability on, for n CUs: invAvgLuma over the left
+ * column / top row of the (mapped) luma plane, sizeY = min(ctb_size_y, 64)
+ * samples each with the crate's edge clamps (eqs. 1216/1217), idx_y_inv
+ * (src/lmcs.rs:209-221) and ChromaScaleCoeff (eq. 1218).  var_scale: n
+ * entries in host memory. */
+int h266_lmcs_chroma_var_scale(h266_ctx *ctx, const h266_picture *pic, const h266_lmcs_derived *lmcs,
+                               uint32_t lmcs_min_bin_idx, uint32_t lmcs_max_bin_idx, uint32_t ctb_size_y,
+                               const h266_lmcs_cvs_block *blocks, uint64_t n, uint32_t *var_scale);
+
+#define H266_NO_VAR_SCALE 0xFFFFFFFFu
+typedef struct h266_chroma_res_block { /* one chroma TB of the inter residual add */
+    uint32_t x, y, w, h;  /* chroma samples; x + w <= width, y + h <= height */
+    uint32_t plane;       /* 1 = Cb, 2 = Cr */
+    uint32_t var_scale;   /* eq. 1218 varScale, H266_NO_VAR_SCALE = none (the crate's None) */
+    uint64_t res_offset;  /* index of the TB's first residual in `res` (row-major, w per row) */
+} h266_chroma_res_block;
+
+/* The inter chroma residual add (src/ctu.rs:9912-9945): each TB's residual,
+ * folded by lmcs_scale_chroma_residuals (src/ctu.rs:734-742, eqs. 1219/1220)
+ * when it has a varScale, is added to the plane with Clip1, TB by TB in list
+ * order (overlapping TBs add in order).  `res` is host memory for
+ * H266_MEM_HOST pictures and device memory for H266_MEM_DEVICE ones. */
+int h266_lmcs_add_chroma_residual(h266_ctx *ctx, h266_picture *pic, uint32_t bit_depth, const int32_t *res,
+                                  uint64_t n_res, const h266_chroma_res_block *blocks, uint64_t n);
+
+/* ---- output conversion (examples/decode_dump.rs, src/stream.rs:47-66) ---- */
+typedef struct h266_crop_window { /* DecodedPicture::crop (src/stream.rs:59-61), luma samples */
+    uint32_t left, top, width, height;
+} h266_crop_window;
+
+/* The cropped planar dump of a decoded picture as examples/decode_dump.rs:
+ * 24-40 writes it (the bytes tests/jvet_conformance.rs:402-427 hash per
+ * plane): luma rows, then, when chroma_format_idc != 0, Cb and Cr rows with
+ * the crop window halved; one byte per sample (`v as u8`) when bit_depth <= 8,
+ * else two bytes little-endian.  dst (dst_mem: H266_MEM_HOST or
+ * H266_MEM_DEVICE) must hold the whole dump; *written receives its size
+ * (dst == NULL: only the size, nothing is converted). */
+int h266_output_convert(h266_ctx *ctx, const h266_picture *pic, const h266_crop_window *crop,
+                        uint32_t chroma_format_idc, uint32_t bit_depth, void *dst, uint64_t dst_capacity,
+                        uint32_t dst_mem, uint64_t *written);
+
 /* apply_deblocking_clipped (src/deblock.rs:497-617). chroma_cus may be NULL
  * (None), mv_grid may be NULL (None). */
 int h266_apply_deblocking_clipped(h266_ctx *ctx, h266_picture *pic, const h266_deblock_cu *cus,
@@ -309,6 +373,25 @@ int h266_apply_alf_clipped(h266_ctx *ctx, h266_picture *pic, const h266_alf_pict
                            const h266_alf_config *cfg, const h266_alf_aps_binding *binding,
                            const uint32_t *col_bd, uint64_t n_col_bd, const uint32_t *row_bd,
                            uint64_t n_row_bd);
+
+/* Encoder luma ALF decision: alf_decide_and_apply_clipped (src/alf_enc.rs:
+ * 185-322) when aps == NULL, alf_decide_and_apply_with_aps_clipped
+ * (src/alf_enc.rs:352-528) otherwise.  Trials 0..15 are the fixed filter sets
+ * and trial 16 the APS set (APS slot 0); for every CTB the option of lowest
+ * luma SSE against `src` among {off, trial 0, ...} is kept (earlier options win
+ * ties), its samples are written into rec's luma plane (chroma untouched) and
+ * decisions[] receives the returned AlfPicture (wc * hc entries, wc/hc =
+ * rec luma size / CTB size rounded up; only luma_on and luma_filt_set_idx are
+ * set).  sse, when not NULL, receives the per-CTB table
+ * [off, trial 0, ..., trial T-1] (T = 16, or 17 with an APS) of uint64 sums.
+ * Supported: BitDepth 8..14, CtbLog2SizeY 5..7, APS coefficients in
+ * [-128, 127] (H266_ERR_UNSUPPORTED otherwise). */
+int h266_alf_decide_and_apply_clipped(h266_ctx *ctx, const h266_picture *src, h266_picture *rec,
+                                      const h266_alf_aps_data *aps, uint32_t ctb_log2_size_y,
+                                      uint32_t bit_depth, uint32_t chroma_format_idc,
+                                      const uint32_t *col_bd, uint64_t n_col_bd, const uint32_t *row_bd,
+                                      uint64_t n_row_bd, h266_alf_ctb *decisions, uint64_t n_decisions,
+                                      uint64_t *sse);
 
 /* CtuWalker::apply_in_loop_filters_with_alf (src/ctu.rs:11822-12065) after its
  * gate lists are built: LMCS inverse -> deblock -> SAO -> ALF in one call. */

@@ -70,6 +70,14 @@ def lib():
         L.oracle_class_to_filt_map.argtypes = [C.c_uint32, C.c_uint32]
         L.oracle_derive_luma_classification.argtypes = [vp, C.c_uint64, C.c_int, vp, C.c_uint32, C.c_uint32,
                                                         C.c_uint32, C.c_uint32, vp, vp]
+        L.oracle_alf_decide_and_apply.argtypes = [vp, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, C.c_uint64, vp,
+                                                  C.c_uint64, vp, vp]
+        L.oracle_lmcs_forward_map_rects.argtypes = [vp, vp, vp, C.c_uint64]
+        L.oracle_lmcs_forward_map_rects.restype = C.c_int
+        L.oracle_lmcs_chroma_var_scale.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, C.c_uint64, vp]
+        L.oracle_lmcs_add_chroma_residual.argtypes = [vp, C.c_uint32, vp, vp, C.c_uint64]
+        L.oracle_output_convert.argtypes = [vp, vp, C.c_uint32, C.c_uint32, vp]
+        L.oracle_output_convert.restype = C.c_uint64
         _LIB = L
     return _LIB
 
@@ -163,3 +171,52 @@ def derive_lmcs(data, bit_depth: int, derived_type):
     out = derived_type()
     rc = lib().oracle_derive_lmcs(C.byref(data), bit_depth, C.byref(out))
     return rc, out
+
+
+def alf_decide_and_apply(src, rec, aps=None, *, ctb_log2: int, bit_depth: int, chroma_format_idc: int = 1,
+                         clip_cols=None, clip_rows=None, alf_ctb_dtype=None):
+    """alf_decide_and_apply[_with_aps]_clipped (src/alf_enc.rs:185-528) on host
+    pictures: `rec` filtered in place; returns (decisions, SSE table [n, 1 + T])."""
+    ctb = 1 << ctb_log2
+    wc, hc = -(-rec.luma.shape[1] // ctb), -(-rec.luma.shape[0] // ctb)
+    n = wc * hc
+    dec = np.zeros(n, dtype=alf_ctb_dtype)
+    sse = np.zeros((n, 18 if aps is not None else 17), dtype=np.uint64)
+    s_c, r_c = src.to_ctypes(), rec.to_ctypes()
+    c1, nc, k1 = _u32(clip_cols)
+    c2, nr, k2 = _u32(clip_rows)
+    lib().oracle_alf_decide_and_apply(C.byref(s_c), C.byref(r_c), _ref(aps), ctb_log2, bit_depth, chroma_format_idc,
+                                      c1, nc, c2, nr, dec.ctypes.data, sse.ctypes.data)
+    return dec, sse
+
+
+def lmcs_forward_map_luma_rects(pic, lmcs, rects) -> int:
+    """CtuWalker::lmcs_forward_map_luma_rect per rectangle (src/ctu.rs:1701-1727); -1 where the crate panics."""
+    cp = pic.to_ctypes()
+    r = np.ascontiguousarray(rects)
+    return lib().oracle_lmcs_forward_map_rects(C.byref(cp), C.byref(lmcs), r.ctypes.data if len(r) else None, len(r))
+
+
+def lmcs_chroma_var_scale(pic, lmcs, mn, mx, ctb_size_y, blocks) -> np.ndarray:
+    cp = pic.to_ctypes()
+    b = np.ascontiguousarray(blocks)
+    out = np.zeros(max(len(b), 1), dtype=np.uint32)
+    lib().oracle_lmcs_chroma_var_scale(C.byref(cp), C.byref(lmcs), mn, mx, ctb_size_y, b.ctypes.data, len(b),
+                                       out.ctypes.data)
+    return out[: len(b)]
+
+
+def lmcs_add_chroma_residual(pic, bit_depth, res, blocks) -> None:
+    cp = pic.to_ctypes()
+    b = np.ascontiguousarray(blocks)
+    r = np.ascontiguousarray(res, dtype=np.int32)
+    lib().oracle_lmcs_add_chroma_residual(C.byref(cp), bit_depth, r.ctypes.data, b.ctypes.data, len(b))
+
+
+def output_convert(pic, crop, chroma_format_idc, bit_depth, crop_type) -> np.ndarray:
+    """The cropped planar dump of examples/decode_dump.rs:24-40."""
+    cp = pic.to_ctypes()
+    cw = crop_type(*crop)
+    out = np.zeros(pic.luma.size * 2 * 2 + 16, dtype=np.uint8)
+    n = lib().oracle_output_convert(C.byref(cp), C.byref(cw), chroma_format_idc, bit_depth, out.ctypes.data)
+    return out[:n]

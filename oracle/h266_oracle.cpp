@@ -1339,6 +1339,196 @@ static void chain(h266_picture *pic, const h266_in_loop_filter_args *a) {
                       a->n_clip_rows);
 }
 
+// CtuWalker::lmcs_forward_map_luma_rect (src/ctu.rs:1701-1727), one call per
+// rectangle in list order.  Returns false where the crate would index past its
+// 16 bins (a sample above 2^BitDepth - 1), leaving the rest unmapped.
+static bool lmcs_forward_map_rects(h266_plane &pl, const h266_lmcs_derived *l, const h266_rect *rects, size_t n) {
+  const int64_t hi = ((int64_t)1 << l->bit_depth) - 1;
+  for (size_t r = 0; r < n; ++r) {
+    const uint64_t y1 = std::min<uint64_t>((uint64_t)rects[r].y + rects[r].h, pl.height);
+    const uint64_t x1 = std::min<uint64_t>((uint64_t)rects[r].x + rects[r].w, pl.width);
+    for (uint64_t row = rects[r].y; row < y1; ++row)
+      for (uint64_t col = rects[r].x; col < x1; ++col) {
+        uint16_t &v = pl.samples[row * pl.stride + col];
+        if ((v >> (l->bit_depth - 4)) > 15) return false;
+        v = (uint16_t)clampl(forward_map(l, v), 0, hi);
+      }
+  }
+  return true;
+}
+
+// CtuWalker::lmcs_chroma_var_scale_for_cu (src/ctu.rs:1752-1815) from
+// (xCuCb, yCuCb) and the neighbour availability on.
+static uint32_t lmcs_chroma_var_scale(const h266_plane &luma, const h266_lmcs_derived *l, uint32_t mn, uint32_t mx,
+                                      uint32_t size_y, const h266_lmcs_cvs_block &b) {
+  const bool avail_l = b.x_cu_cb > 0 && b.avail_l, avail_t = b.y_cu_cb > 0 && b.avail_t;
+  uint64_t sum = 0, cnt = 0;
+  if (avail_l) {
+    for (uint32_t i = 0; i < size_y; ++i) {
+      const uint64_t yy = std::min<uint64_t>((uint64_t)b.y_cu_cb + i, luma.height - 1);
+      sum += luma.samples[yy * luma.stride + (b.x_cu_cb - 1)];
+    }
+    cnt += size_y;
+  }
+  if (avail_t) {
+    for (uint32_t i = 0; i < size_y; ++i) {
+      const uint64_t xx = std::min<uint64_t>((uint64_t)b.x_cu_cb + i, luma.width - 1);
+      sum += luma.samples[(uint64_t)(b.y_cu_cb - 1) * luma.stride + xx];
+    }
+    cnt += size_y;
+  }
+  uint32_t avg;
+  if (cnt > 0) {
+    int tz = 0;
+    while (!((cnt >> tz) & 1)) ++tz;
+    avg = (uint32_t)((sum + (cnt >> 1)) >> tz);
+  } else {
+    avg = 1u << (l->bit_depth - 1);
+  }
+  return l->chroma_scale_coeff[idx_y_inv(l, avg, mn, mx)];
+}
+
+// The inter chroma residual add (src/ctu.rs:9912-9945) with the optional
+// lmcs_scale_chroma_residuals fold (src/ctu.rs:734-742).
+static void add_chroma_residual(h266_picture *pic, uint32_t bd, const int32_t *res, const h266_chroma_res_block &b) {
+  h266_plane &pl = b.plane == 1 ? pic->cb : pic->cr;
+  const int64_t lo = -((int64_t)1 << bd), hi = ((int64_t)1 << bd) - 1;
+  for (uint32_t row = 0; row < b.h; ++row)
+    for (uint32_t col = 0; col < b.w; ++col) {
+      int64_t r = res[b.res_offset + (uint64_t)row * b.w + col];
+      if (b.var_scale != H266_NO_VAR_SCALE) {
+        const int64_t v = clampl(r, lo, hi);
+        const int64_t mag = (int64_t)(((uint64_t)(v < 0 ? -v : v) * b.var_scale + 1024) >> 11);
+        r = v < 0 ? -mag : mag;
+      }
+      uint16_t &s = pl.samples[(uint64_t)(b.y + row) * pl.stride + b.x + col];
+      s = (uint16_t)clampl((int64_t)s + r, 0, hi);
+    }
+}
+
+// The cropped planar dump of examples/decode_dump.rs:24-40 (and the per-plane
+// serialisation hashed by tests/jvet_conformance.rs:402-427): luma, then Cb and
+// Cr with the crop halved when chroma_format_idc != 0; one byte per sample
+// (`v as u8`) for BitDepth <= 8, else two bytes little-endian.
+static uint64_t output_convert(const h266_picture *pic, const h266_crop_window &c, uint32_t cfi, uint32_t bd,
+                               uint8_t *out) {
+  const bool wide = bd > 8;
+  struct P { const h266_plane *p; uint32_t x0, y0, w, h; };
+  P planes[3] = {{&pic->luma, c.left, c.top, c.width, c.height},
+                 {&pic->cb, c.left / 2, c.top / 2, c.width / 2, c.height / 2},
+                 {&pic->cr, c.left / 2, c.top / 2, c.width / 2, c.height / 2}};
+  uint64_t o = 0;
+  for (int i = 0; i < (cfi != 0 ? 3 : 1); ++i) {
+    const P &q = planes[i];
+    for (uint64_t y = q.y0; y < (uint64_t)q.y0 + q.h; ++y)
+      for (uint64_t x = q.x0; x < (uint64_t)q.x0 + q.w; ++x) {
+        const uint16_t v = q.p->samples[y * q.p->stride + x];
+        if (wide) {
+          out[o++] = (uint8_t)(v & 0xFF);
+          out[o++] = (uint8_t)(v >> 8);
+        } else {
+          out[o++] = (uint8_t)v;
+        }
+      }
+  }
+  return o;
+}
+
+// ctb_sse_y, src/alf_enc.rs:79-105: SSE over the CTB rectangle inside both planes.
+static uint64_t ctb_sse_y(const h266_plane &src, const h266_plane &rec, size_t x0, size_t y0, size_t w, size_t h) {
+  uint64_t sse = 0;
+  for (size_t y = 0; y < h; ++y) {
+    const size_t yi = y0 + y;
+    if (yi >= src.height || yi >= rec.height) break;
+    for (size_t x = 0; x < w; ++x) {
+      const size_t xi = x0 + x;
+      if (xi >= src.width || xi >= rec.width) break;
+      const int64_t d = (int64_t)src.samples[yi * src.stride + xi] - (int64_t)rec.samples[yi * rec.stride + xi];
+      sse += (uint64_t)(d * d);
+    }
+  }
+  return sse;
+}
+
+// alf_decide_and_apply_clipped (src/alf_enc.rs:185-322) when `aps` is NULL,
+// alf_decide_and_apply_with_aps_clipped (src/alf_enc.rs:352-528) otherwise:
+// trials 0..15 are the fixed sets (every CTB on), trial 16 the APS set
+// (luma_filt_set_idx 16, APS slot 0); per CTB the lowest SSE_Y among
+// {off, trial 0, ...} wins (strict <, so earlier options win ties) and its
+// luma samples are copied into `rec`.  `decisions` receives the returned
+// AlfPicture; `sse` (optional) the per-CTB table [off, trial 0, ...].
+static void alf_decide_and_apply(const h266_picture *src, h266_picture *rec, const h266_alf_aps_data *aps,
+                                 uint32_t log2, uint32_t bd, uint32_t cfi, const uint32_t *cols, size_t n_cols,
+                                 const uint32_t *rows, size_t n_rows, h266_alf_ctb *decisions, uint64_t *sse) {
+  const uint32_t ctb = 1u << log2;
+  const uint32_t wc = (rec->luma.width + ctb - 1) / ctb, hc = (rec->luma.height + ctb - 1) / ctb;
+  const size_t n = (size_t)wc * hc;
+  const size_t trials = aps ? 17 : 16;
+  std::vector<uint64_t> pre(n);
+  for (uint32_t ry = 0; ry < hc; ++ry)
+    for (uint32_t rx = 0; rx < wc; ++rx)
+      pre[(size_t)ry * wc + rx] = ctb_sse_y(src->luma, rec->luma, (size_t)rx * ctb, (size_t)ry * ctb, ctb, ctb);
+  h266_alf_config cfg{};
+  cfg.alf_enabled = 1;
+  cfg.bit_depth = bd;
+  cfg.ctb_log2_size_y = log2;
+  cfg.chroma_format_idc = cfi;
+  const h266_alf_aps_data *slot[1] = {aps};
+  h266_alf_aps_binding binding{};
+  if (aps) {
+    binding.luma_apses = slot;
+    binding.n_luma_apses = 1;
+  }
+  const size_t lum = (size_t)rec->luma.stride * rec->luma.height;
+  std::vector<uint64_t> per(n * trials);
+  std::vector<std::vector<uint16_t>> per_luma(trials);
+  std::vector<h266_alf_ctb> trial(n);
+  for (size_t t = 0; t < trials; ++t) {
+    std::vector<uint16_t> y(rec->luma.samples, rec->luma.samples + lum);  // rec.clone() (luma; chroma is untouched)
+    h266_picture pic = *rec;
+    pic.luma.samples = y.data();
+    pic.cb.width = pic.cb.height = 0;
+    pic.cr.width = pic.cr.height = 0;
+    for (size_t i = 0; i < n; ++i) {
+      trial[i] = h266_alf_ctb{};
+      trial[i].luma_on = 1;
+      trial[i].luma_filt_set_idx = (uint8_t)(t < 16 ? t : 16);
+    }
+    h266_alf_picture ap{wc, hc, trial.data()};
+    apply_alf_clipped(&pic, &ap, &cfg, t < 16 ? nullptr : &binding, cols, n_cols, rows, n_rows);
+    for (uint32_t ry = 0; ry < hc; ++ry)
+      for (uint32_t rx = 0; rx < wc; ++rx)
+        per[((size_t)ry * wc + rx) * trials + t] =
+            ctb_sse_y(src->luma, pic.luma, (size_t)rx * ctb, (size_t)ry * ctb, ctb, ctb);
+    per_luma[t] = std::move(y);
+  }
+  const size_t st = rec->luma.stride;
+  for (uint32_t ry = 0; ry < hc; ++ry)
+    for (uint32_t rx = 0; rx < wc; ++rx) {
+      const size_t idx = (size_t)ry * wc + rx;
+      uint64_t best = pre[idx];
+      int pick = -1;
+      for (size_t t = 0; t < trials; ++t)
+        if (per[idx * trials + t] < best) {
+          best = per[idx * trials + t];
+          pick = (int)t;
+        }
+      decisions[idx] = h266_alf_ctb{};
+      if (sse) {
+        sse[idx * (trials + 1)] = pre[idx];
+        for (size_t t = 0; t < trials; ++t) sse[idx * (trials + 1) + 1 + t] = per[idx * trials + t];
+      }
+      if (pick < 0) continue;
+      const size_t x0 = (size_t)rx * ctb, y0 = (size_t)ry * ctb;
+      const size_t w = std::min<size_t>(ctb, rec->luma.width > x0 ? rec->luma.width - x0 : 0);
+      const size_t h = std::min<size_t>(ctb, rec->luma.height > y0 ? rec->luma.height - y0 : 0);
+      for (size_t y = 0; y < h; ++y)
+        std::memcpy(rec->luma.samples + (y0 + y) * st + x0, per_luma[pick].data() + (y0 + y) * st + x0, w * 2);
+      decisions[idx].luma_on = 1;
+      decisions[idx].luma_filt_set_idx = (uint8_t)(pick < 16 ? pick : 16);
+    }
+}
+
 }  // namespace oracle
 
 // ---------------------------------------------------------------------------
@@ -1435,6 +1625,29 @@ void oracle_apply_alf_clipped(h266_picture *pic, const h266_alf_picture *ap, con
 }
 
 void oracle_apply_in_loop_filters(h266_picture *pic, const h266_in_loop_filter_args *a) { oracle::chain(pic, a); }
+
+int oracle_lmcs_forward_map_rects(h266_picture *pic, const h266_lmcs_derived *l, const h266_rect *rects, uint64_t n) {
+  return oracle::lmcs_forward_map_rects(pic->luma, l, rects, n) ? 0 : -1;
+}
+void oracle_lmcs_chroma_var_scale(const h266_picture *pic, const h266_lmcs_derived *l, uint32_t mn, uint32_t mx,
+                                  uint32_t ctb_size_y, const h266_lmcs_cvs_block *b, uint64_t n, uint32_t *out) {
+  const uint32_t size_y = std::min<uint32_t>(ctb_size_y, 64);
+  for (uint64_t i = 0; i < n; ++i) out[i] = oracle::lmcs_chroma_var_scale(pic->luma, l, mn, mx, size_y, b[i]);
+}
+void oracle_lmcs_add_chroma_residual(h266_picture *pic, uint32_t bd, const int32_t *res,
+                                     const h266_chroma_res_block *b, uint64_t n) {
+  for (uint64_t i = 0; i < n; ++i) oracle::add_chroma_residual(pic, bd, res, b[i]);
+}
+uint64_t oracle_output_convert(const h266_picture *pic, const h266_crop_window *c, uint32_t cfi, uint32_t bd,
+                               uint8_t *out) {
+  return oracle::output_convert(pic, *c, cfi, bd, out);
+}
+
+void oracle_alf_decide_and_apply(const h266_picture *src, h266_picture *rec, const h266_alf_aps_data *aps,
+                                 uint32_t log2, uint32_t bd, uint32_t cfi, const uint32_t *cols, uint64_t n_cols,
+                                 const uint32_t *rows, uint64_t n_rows, h266_alf_ctb *decisions, uint64_t *sse) {
+  oracle::alf_decide_and_apply(src, rec, aps, log2, bd, cfi, cols, n_cols, rows, n_rows, decisions, sse);
+}
 
 // CPU baseline: n pictures spread over `threads` std::threads (one picture per
 // task).  Returns the thread count used.

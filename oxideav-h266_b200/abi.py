@@ -292,6 +292,20 @@ class InLoopFilterArgs(C.Structure):
     ]
 
 
+# h266_rect (16 bytes), h266_lmcs_cvs_block (12), h266_chroma_res_block (32)
+RECT = np.dtype({"names": ["x", "y", "w", "h"], "formats": ["<u4"] * 4, "offsets": [0, 4, 8, 12], "itemsize": 16})
+CVS_BLOCK = np.dtype({"names": ["x_cu_cb", "y_cu_cb", "avail_l", "avail_t"], "formats": ["<u4", "<u4", "u1", "u1"],
+                      "offsets": [0, 4, 8, 9], "itemsize": 12})
+RES_BLOCK = np.dtype({"names": ["x", "y", "w", "h", "plane", "var_scale", "res_offset"],
+                      "formats": ["<u4"] * 6 + ["<u8"], "offsets": [0, 4, 8, 12, 16, 20, 24], "itemsize": 32})
+NO_VAR_SCALE = 0xFFFFFFFF
+
+
+class CropWindow(C.Structure):
+    """DecodedPicture::crop, src/stream.rs:59-61 (luma samples)."""
+
+    _fields_ = [("left", C.c_uint32), ("top", C.c_uint32), ("width", C.c_uint32), ("height", C.c_uint32)]
+
 # Sizes of the C structs on x86-64 / aarch64; the library static_asserts the
 # same numbers and the CPU tests compare them with the mirrors above.
 SIZES = {

@@ -952,6 +952,67 @@ bool same_geometry(const h266_picture &a, const h266_picture &b) {
 }  // namespace
 
 // ======================================================================= C ABI
+// ---------------------------------------------------------------- recon-side LMCS, output dump
+namespace {
+
+// Samples of a plane already covered by the rectangles of the current launch
+// group: a rectangle meeting one of them starts the next group, so every
+// launch works on disjoint rectangles and groups run in list order.
+// Cells are g x g samples, g the coarsest grid every rectangle edge lies on
+// (CU and TB edges: 4 luma / 2 chroma), so the test stays exact.
+struct Coverage {
+  uint32_t w = 0, h = 0, wpr = 0, g = 1;
+  std::vector<uint64_t> bits;
+  void reset(uint32_t w_, uint32_t h_, uint32_t g_) {
+    g = g_;
+    w = (w_ + g - 1) / g;
+    h = (h_ + g - 1) / g;
+    wpr = (w + 63) / 64;
+    bits.assign((size_t)wpr * h, 0);
+  }
+  void clear() { std::fill(bits.begin(), bits.end(), 0); }
+  template <class F>
+  bool each(uint32_t x, uint32_t y, uint32_t rw, uint32_t rh, F f) {  // f(word, mask) until it returns true
+    for (uint32_t r = y; r < y + rh; ++r)
+      for (uint32_t wi = x / 64; wi <= (x + rw - 1) / 64; ++wi) {
+        const uint32_t lo = std::max(x, wi * 64) - wi * 64, hi = std::min(x + rw, wi * 64 + 64) - wi * 64;
+        const uint64_t m = (hi - lo == 64 ? ~0ull : (((1ull << (hi - lo)) - 1) << lo));
+        if (f(bits[(size_t)r * wpr + wi], m)) return true;
+      }
+    return false;
+  }
+  bool meets(uint32_t x, uint32_t y, uint32_t rw, uint32_t rh) {  // sample coordinates on the g grid
+    return each(x / g, y / g, (rw + g - 1) / g, (rh + g - 1) / g, [](uint64_t &b, uint64_t m) { return (b & m) != 0; });
+  }
+  void mark(uint32_t x, uint32_t y, uint32_t rw, uint32_t rh) {
+    each(x / g, y / g, (rw + g - 1) / g, (rh + g - 1) / g, [](uint64_t &b, uint64_t m) {
+      b |= m;
+      return false;
+    });
+  }
+};
+
+// The coarsest of 4, 2, 1 dividing every value folded into `acc` (an OR).
+uint32_t grid_of(uint32_t acc) { return (acc & 3) == 0 ? 4 : ((acc & 1) == 0 ? 2 : 1); }
+
+constexpr uint32_t kPieceSamples = 4096;
+
+h266_picture plane_view(const h266_picture &pic, int keep) {  // the picture with only plane `keep` (-1: chroma)
+  h266_picture v = pic;
+  h266_plane *pl[3] = {&v.luma, &v.cb, &v.cr};
+  for (int i = 0; i < 3; ++i)
+    if (keep >= 0 ? i != keep : i == 0) pl[i]->width = pl[i]->height = 0;
+  return v;
+}
+
+int sync_read(Lane &ln, void *host, const void *dev, size_t n) {
+  H266_CUDA(cudaMemcpyAsync(host, dev, n, cudaMemcpyDeviceToHost, ln.stream));
+  H266_CUDA(cudaStreamSynchronize(ln.stream));
+  return H266_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 const char *h266_last_error(void) { return g_last_error.c_str(); }
@@ -1134,6 +1195,352 @@ int h266_apply_alf_clipped(h266_ctx *ctx, h266_picture *pic, const h266_alf_pict
   in.n_cols = n_col;
   in.n_rows = n_row;
   return pass2_entry(ctx, pic, in);
+}
+
+int h266_lmcs_forward_map_luma_rects(h266_ctx *ctx, h266_picture *pic, const h266_lmcs_derived *lmcs,
+                                     const h266_rect *rects, uint64_t n) {
+  H266_TRY(check_ctx(ctx));
+  H266_TRY(check_picture(pic));
+  if (!lmcs) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL lmcs");
+  H266_TRY(check_lmcs(lmcs, 0, 0));
+  if (n && !rects) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL rects with nonzero length");
+  const uint32_t W = pic->luma.width, H = pic->luma.height;
+  std::vector<RectPiece> pieces;
+  std::vector<uint32_t> group_end;
+  auto clipped = [&](const h266_rect &r, uint32_t &rw, uint32_t &rh) {  // clipped as src/ctu.rs:1718-1719
+    if (r.x >= W || r.y >= H || !r.w || !r.h) return false;
+    rw = (uint32_t)std::min<uint64_t>((uint64_t)r.x + r.w, W) - r.x;
+    rh = (uint32_t)std::min<uint64_t>((uint64_t)r.y + r.h, H) - r.y;
+    return true;
+  };
+  uint32_t acc = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    uint32_t rw, rh;
+    if (clipped(rects[i], rw, rh)) acc |= rects[i].x | rects[i].y | (rects[i].x + rw) | (rects[i].y + rh);
+  }
+  Coverage cov;
+  cov.reset(W, H, grid_of(acc));
+  for (uint64_t i = 0; i < n; ++i) {
+    const h266_rect &r = rects[i];
+    uint32_t rw, rh;
+    if (!clipped(r, rw, rh)) continue;
+    if (cov.meets(r.x, r.y, rw, rh)) {
+      group_end.push_back((uint32_t)pieces.size());
+      cov.clear();
+    }
+    cov.mark(r.x, r.y, rw, rh);
+    const uint32_t rows = std::max<uint32_t>(1, kPieceSamples / rw);
+    for (uint32_t y = 0; y < rh; y += rows) pieces.push_back(RectPiece{r.x, r.y + y, rw, std::min(rows, rh - y)});
+  }
+  group_end.push_back((uint32_t)pieces.size());
+  Guard g(ctx->device);
+  Lane &ln = ctx->main;
+  const h266_picture lv = plane_view(*pic, 0);
+  DPlane P[3];
+  H266_TRY(picture_to_device(ln, lv, P));
+  ctx->h2d_bytes += host_plane_bytes(lv);
+  H266_TRY(ln.lut.ensure(65536 * 2));
+  H266_TRY(launch_lmcs_fwd_lut(ln.stream, ln.lut.as<uint16_t>(), *lmcs, &ctx->launches));
+  Prep &pr = ctx_prep(ctx, 0);
+  pr.blob.clear();
+  Blob blob{pr.blob};
+  const size_t off = blob.put(pieces.data(), pieces.size() * sizeof(RectPiece));
+  uint8_t *base = nullptr;
+  H266_TRY(upload_blob(ln, pr.blob, &base));
+  ctx->h2d_bytes += pr.blob.size();
+  H266_TRY(ln.walk.ensure(16));
+  uint32_t *d_err = ln.walk.as<uint32_t>();
+  H266_CUDA(cudaMemsetAsync(d_err, 0, 4, ln.stream));
+  {
+    Prof pf(ctx, ln.stream, H266_PROF_LMCS);
+    uint32_t g0 = 0;
+    for (uint32_t ge : group_end) {
+      H266_TRY(launch_lmcs_fwd_rects(ln.stream, P[0], ln.lut.as<uint16_t>(),
+                                     reinterpret_cast<const RectPiece *>(base + off) + g0, ge - g0,
+                                     lmcs->bit_depth < 16, d_err, &ctx->launches));
+      g0 = ge;
+    }
+  }
+  H266_TRY(picture_from_device(ln, lv, false));
+  ctx->d2h_bytes += host_plane_bytes(lv);
+  uint32_t err = 0;
+  H266_TRY(sync_read(ln, &err, d_err, 4));
+  if (err) return set_error(H266_ERR_INVALID_ARGUMENT, "forward LMCS: a sample above (1 << BitDepth) - 1 has no bin");
+  return H266_OK;
+}
+
+int h266_lmcs_chroma_var_scale(h266_ctx *ctx, const h266_picture *pic, const h266_lmcs_derived *lmcs, uint32_t mn,
+                               uint32_t mx, uint32_t ctb_size_y, const h266_lmcs_cvs_block *blocks, uint64_t n,
+                               uint32_t *var_scale) {
+  H266_TRY(check_ctx(ctx));
+  H266_TRY(check_picture(pic));
+  if (!lmcs) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL lmcs");
+  H266_TRY(check_lmcs(lmcs, mn, mx));
+  if (n && (!blocks || !var_scale)) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL blocks / output");
+  if (n > (1u << 26)) return set_error(H266_ERR_UNSUPPORTED, "too many blocks");
+  const uint32_t size_y = std::min<uint32_t>(ctb_size_y, 64);
+  if (!size_y || (size_y & (size_y - 1)))
+    return set_error(H266_ERR_INVALID_ARGUMENT, "ctb_size_y must be a power of two");
+  for (uint64_t i = 0; i < n; ++i) {  // the crate's reads stay inside the plane (src/ctu.rs:1789-1806)
+    const h266_lmcs_cvs_block &b = blocks[i];
+    if ((b.x_cu_cb > 0 && b.avail_l && b.x_cu_cb - 1 >= pic->luma.width) ||
+        (b.y_cu_cb > 0 && b.avail_t && b.y_cu_cb - 1 >= pic->luma.height))
+      return set_error(H266_ERR_INVALID_ARGUMENT, "CU origin outside the luma plane");
+  }
+  Guard g(ctx->device);
+  Lane &ln = ctx->main;
+  const h266_picture lv = plane_view(*pic, 0);
+  DPlane P[3];
+  H266_TRY(picture_to_device(ln, lv, P));
+  ctx->h2d_bytes += host_plane_bytes(lv);
+  Prep &pr = ctx_prep(ctx, 0);
+  pr.blob.clear();
+  Blob blob{pr.blob};
+  const size_t off = blob.put(blocks, n * sizeof(h266_lmcs_cvs_block));
+  uint8_t *base = nullptr;
+  H266_TRY(upload_blob(ln, pr.blob, &base));
+  ctx->h2d_bytes += pr.blob.size();
+  H266_TRY(ln.walk.ensure(std::max<uint64_t>(n, 1) * 4));
+  CvsTables t;
+  for (int i = 0; i < 17; ++i) t.pivot[i] = lmcs->lmcs_pivot[i];
+  for (int i = 0; i < 16; ++i) t.chroma_scale[i] = lmcs->chroma_scale_coeff[i];
+  t.mn = mn;
+  t.mx = mx;
+  t.bd = lmcs->bit_depth;
+  {
+    Prof pf(ctx, ln.stream, H266_PROF_LMCS);
+    H266_TRY(launch_lmcs_cvs(ln.stream, P[0], reinterpret_cast<const h266_lmcs_cvs_block *>(base + off), (uint32_t)n,
+                             (int)size_y, t, ln.walk.as<uint32_t>(), &ctx->launches));
+  }
+  if (n) H266_TRY(sync_read(ln, var_scale, ln.walk.as<uint32_t>(), n * 4));
+  ctx->d2h_bytes += n * 4;
+  return H266_OK;
+}
+
+int h266_lmcs_add_chroma_residual(h266_ctx *ctx, h266_picture *pic, uint32_t bd, const int32_t *res, uint64_t n_res,
+                                  const h266_chroma_res_block *blocks, uint64_t n) {
+  H266_TRY(check_ctx(ctx));
+  H266_TRY(check_picture(pic));
+  if (bd < 8 || bd > 16) return set_error(H266_ERR_INVALID_ARGUMENT, "bit_depth must be 8..16");
+  if (n && (!blocks || !res)) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL blocks / residuals");
+  const h266_plane *cp[2] = {&pic->cb, &pic->cr};
+  uint32_t acc = 0;
+  for (uint64_t i = 0; i < n; ++i) acc |= blocks[i].x | blocks[i].y | blocks[i].w | blocks[i].h;
+  Coverage cov[2];
+  cov[0].reset(pic->cb.width, pic->cb.height, grid_of(acc));
+  cov[1].reset(pic->cr.width, pic->cr.height, grid_of(acc));
+  std::vector<ResPiece> pieces;
+  std::vector<uint32_t> group_end;
+  for (uint64_t i = 0; i < n; ++i) {
+    const h266_chroma_res_block &b = blocks[i];
+    if (b.plane != 1 && b.plane != 2) return set_error(H266_ERR_INVALID_ARGUMENT, "residual block plane must be 1 or 2");
+    const h266_plane &pl = *cp[b.plane - 1];
+    // src/ctu.rs:9931-9937 (the crate's planes have stride == width)
+    if ((uint64_t)b.x + b.w > pl.width || (uint64_t)b.y + b.h > pl.height)
+      return set_error(H266_ERR_INVALID_ARGUMENT, "chroma TB does not fit in the plane");
+    if (b.res_offset > n_res || (uint64_t)b.w * b.h > n_res - b.res_offset)
+      return set_error(H266_ERR_INVALID_ARGUMENT, "chroma TB residuals run past n_res");
+    if (!b.w || !b.h) continue;
+    Coverage &c = cov[b.plane - 1];
+    if (c.meets(b.x, b.y, b.w, b.h)) {
+      group_end.push_back((uint32_t)pieces.size());
+      cov[0].clear();
+      cov[1].clear();
+    }
+    c.mark(b.x, b.y, b.w, b.h);
+    const uint32_t rows = std::max<uint32_t>(1, kPieceSamples / b.w);
+    for (uint32_t y = 0; y < b.h; y += rows)
+      pieces.push_back(ResPiece{b.x, b.y + y, b.w, std::min(rows, b.h - y), b.plane, b.var_scale,
+                                b.res_offset + (uint64_t)y * b.w, b.w, 0});
+  }
+  group_end.push_back((uint32_t)pieces.size());
+  Guard g(ctx->device);
+  Lane &ln = ctx->main;
+  const h266_picture cv = plane_view(*pic, -1);
+  DPlane P[3];
+  H266_TRY(picture_to_device(ln, cv, P));
+  ctx->h2d_bytes += host_plane_bytes(cv);
+  const int32_t *d_res = res;
+  if (pic->mem == H266_MEM_HOST && n_res) {
+    H266_TRY(ln.scratch[0].ensure(n_res * 4));
+    H266_CUDA(cudaMemcpyAsync(ln.scratch[0].ptr, res, n_res * 4, cudaMemcpyHostToDevice, ln.stream));
+    d_res = ln.scratch[0].as<int32_t>();
+    ctx->h2d_bytes += n_res * 4;
+  }
+  Prep &pr = ctx_prep(ctx, 0);
+  pr.blob.clear();
+  Blob blob{pr.blob};
+  const size_t off = blob.put(pieces.data(), pieces.size() * sizeof(ResPiece));
+  uint8_t *base = nullptr;
+  H266_TRY(upload_blob(ln, pr.blob, &base));
+  ctx->h2d_bytes += pr.blob.size();
+  {
+    Prof pf(ctx, ln.stream, H266_PROF_LMCS);
+    uint32_t g0 = 0;
+    for (uint32_t ge : group_end) {
+      H266_TRY(launch_chroma_residual(ln.stream, P[1], P[2], reinterpret_cast<const ResPiece *>(base + off) + g0,
+                                      ge - g0, d_res, (int)bd, &ctx->launches));
+      g0 = ge;
+    }
+  }
+  H266_TRY(picture_from_device(ln, cv));
+  ctx->d2h_bytes += host_plane_bytes(cv);
+  if (pic->mem == H266_MEM_DEVICE) H266_CUDA(cudaStreamSynchronize(ln.stream));
+  return H266_OK;
+}
+
+int h266_output_convert(h266_ctx *ctx, const h266_picture *pic, const h266_crop_window *crop, uint32_t cfi,
+                        uint32_t bd, void *dst, uint64_t cap, uint32_t dst_mem, uint64_t *written) {
+  H266_TRY(check_ctx(ctx));
+  H266_TRY(check_picture(pic));
+  if (!crop) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL crop");
+  if (dst_mem != H266_MEM_HOST && dst_mem != H266_MEM_DEVICE)
+    return set_error(H266_ERR_INVALID_ARGUMENT, "dst_mem must be H266_MEM_HOST or H266_MEM_DEVICE");
+  if (bd < 8 || bd > 16) return set_error(H266_ERR_INVALID_ARGUMENT, "bit_depth must be 8..16");
+  const bool wide = bd > 8;
+  OutPlanes o{};
+  const uint32_t x0[3] = {crop->left, crop->left / 2, crop->left / 2}, y0[3] = {crop->top, crop->top / 2, crop->top / 2};
+  const uint32_t w[3] = {crop->width, crop->width / 2, crop->width / 2};
+  const uint32_t h[3] = {crop->height, crop->height / 2, crop->height / 2};
+  const h266_plane *pl[3] = {&pic->luma, &pic->cb, &pic->cr};
+  const int planes = cfi != 0 ? 3 : 1;
+  for (int i = 0; i < planes; ++i) {  // the crate slices these rows (examples/decode_dump.rs:34)
+    if ((uint64_t)x0[i] + w[i] > pl[i]->width || (uint64_t)y0[i] + h[i] > pl[i]->height)
+      return set_error(H266_ERR_INVALID_ARGUMENT, "crop window outside the plane");
+    o.x0[i] = x0[i];
+    o.y0[i] = y0[i];
+    o.w[i] = w[i];
+    o.n[i] = (uint64_t)w[i] * h[i];
+    o.total += o.n[i];
+  }
+  const uint64_t bytes = o.total * (wide ? 2 : 1);
+  if (written) *written = bytes;
+  if (!dst) return H266_OK;  // size query
+  if (cap < bytes) return set_error(H266_ERR_INVALID_ARGUMENT, "dst smaller than the cropped dump");
+  if (wide && dst_mem == H266_MEM_DEVICE && (reinterpret_cast<uintptr_t>(dst) & 1))
+    return set_error(H266_ERR_INVALID_ARGUMENT, "device dst of a 16-bit dump must be 2-byte aligned");
+  Guard g(ctx->device);
+  Lane &ln = ctx->main;
+  h266_picture v = *pic;
+  if (planes == 1) v.cb.width = v.cb.height = v.cr.width = v.cr.height = 0;
+  DPlane P[3];
+  H266_TRY(picture_to_device(ln, v, P));
+  ctx->h2d_bytes += host_plane_bytes(v);
+  for (int i = 0; i < 3; ++i) o.p[i] = P[i];
+  uint8_t *d_dst = static_cast<uint8_t *>(dst);
+  if (dst_mem == H266_MEM_HOST) {
+    H266_TRY(ln.walk.ensure(std::max<uint64_t>(bytes, 16)));
+    d_dst = ln.walk.as<uint8_t>();
+  }
+  {
+    Prof pf(ctx, ln.stream, H266_PROF_COPY);
+    H266_TRY(launch_output_dump(ln.stream, o, d_dst, wide, &ctx->launches));
+  }
+  if (dst_mem == H266_MEM_HOST) {
+    H266_TRY(sync_read(ln, dst, d_dst, bytes));
+    ctx->d2h_bytes += bytes;
+  }
+  return H266_OK;
+}
+
+int h266_alf_decide_and_apply_clipped(h266_ctx *ctx, const h266_picture *src, h266_picture *rec,
+                                      const h266_alf_aps_data *aps, uint32_t log2, uint32_t bd, uint32_t cfi,
+                                      const uint32_t *col_bd, uint64_t n_col, const uint32_t *row_bd, uint64_t n_row,
+                                      h266_alf_ctb *decisions, uint64_t n_decisions, uint64_t *sse) {
+  H266_TRY(check_ctx(ctx));
+  H266_TRY(check_picture(src));
+  H266_TRY(check_picture(rec));
+  if (!decisions) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL decisions");
+  if (col_bd && !row_bd) return set_error(H266_ERR_INVALID_ARGUMENT, "row bounds NULL while col bounds are not");
+  if (bd < 8 || bd > 14) return set_error(H266_ERR_UNSUPPORTED, "ALF trials need BitDepth 8..14");
+  if (log2 < 5 || log2 > 7) return set_error(H266_ERR_UNSUPPORTED, "ALF trials need CtbLog2SizeY in 5..7");
+  const uint32_t ctb = 1u << log2;
+  const uint32_t wc = (rec->luma.width + ctb - 1) / ctb, hc = (rec->luma.height + ctb - 1) / ctb;
+  const size_t n = (size_t)wc * hc;
+  if (n_decisions != n) return set_error(H266_ERR_GRID_MISMATCH, "decisions size != CTB grid of rec");
+  const bool aps_ok = aps && aps->alf_luma_filter_signal_flag;
+  if (aps_ok && aps->n_luma_filters < 25)
+    return set_error(H266_ERR_INVALID_ARGUMENT, "luma APS signals fewer than 25 filters");
+  const int cols = aps ? 18 : 17, run = aps_ok ? 17 : 16;
+  Guard g(ctx->device);
+  Prep &pr = ctx_prep(ctx, 0);
+  Pass2Host &h = pr.h;
+  // The commit pass is apply_alf with luma only (the trial configuration,
+  // src/alf_enc.rs:226-235); its CTB records get their sets from the decision.
+  std::vector<h266_alf_ctb> all(n, h266_alf_ctb{});
+  for (h266_alf_ctb &c : all) c.luma_on = 1;
+  const h266_alf_picture ap{wc, hc, all.data()};
+  const h266_alf_config cfg{1, 0, 0, 0, 0, bd, log2, cfi};
+  h266_picture rl = *rec;  // luma only: chroma is neither read nor written
+  rl.cb.width = rl.cb.height = rl.cr.width = rl.cr.height = 0;
+  Pass2Inputs in;
+  in.alf = &ap;
+  in.alf_cfg = &cfg;
+  in.cols = col_bd;
+  in.rows = row_bd;
+  in.n_cols = n_col;
+  in.n_rows = n_row;
+  H266_TRY(build_pass2(rl, in, h));
+  // trial slots: fixed sets 0..15 (clipIdx 0), then the APS set
+  h.luma_tab.assign((size_t)run * 600, 0);
+  for (int t = 0; t < run; ++t)
+    for (int c = 0; c < 25; ++c)
+      for (int j = 0; j < 12; ++j) {
+        int32_t *e = &h.luma_tab[(size_t)t * 600];
+        e[c * 12 + j] = t < 16 ? kFixedSetCoeff[(t * 25 + c) * 12 + j] : aps->luma_coeff[c][j];
+        e[300 + c * 12 + j] = alf_clip_value((int)bd, t < 16 ? 0 : aps->luma_clip_idx[c][j]);
+      }
+  if (!build_packed(h, (int)bd, 0, nullptr))
+    return set_error(H266_ERR_UNSUPPORTED, "ALF trials: APS luma coefficients outside [-128, 127]");
+  h.packed = true;
+  Lane &ln = ctx->main;
+  DPlane P[3], S[3];
+  H266_TRY(picture_to_device(ln, rl, P));
+  DPlane O;
+  if (src->mem == H266_MEM_DEVICE) {
+    O = dplane(src->luma, src->luma.samples, (int64_t)src->luma.stride);
+  } else {
+    const size_t row = (size_t)src->luma.width * 2;
+    H266_TRY(ln.io[1].ensure(row * src->luma.height));
+    H266_CUDA(cudaMemcpy2DAsync(ln.io[1].ptr, row, src->luma.samples, (size_t)src->luma.stride * 2, row,
+                                src->luma.height, cudaMemcpyHostToDevice, ln.stream));
+    O = dplane(src->luma, ln.io[1].as<uint16_t>(), src->luma.width);
+    ctx->h2d_bytes += row * src->luma.height;
+  }
+  ctx->h2d_bytes += host_plane_bytes(rl);
+  H266_TRY(ensure_scratch(ln, P, S));
+  H266_TRY(plane_map(ctx, ln.stream, S[0], P[0], nullptr));  // the pre-ALF snapshot
+  Staged st;
+  pr.blob.clear();
+  stage_pass2(h, pr.blob, st);
+  H266_TRY(upload_blob(ln, pr.blob, &st.base));
+  ctx->h2d_bytes += pr.blob.size();
+  const size_t sse_bytes = n * cols * sizeof(unsigned long long);
+  H266_TRY(ln.walk.ensure(sse_bytes + n * sizeof(int16_t)));
+  auto *d_sse = ln.walk.as<unsigned long long>();
+  auto *d_dec = reinterpret_cast<int16_t *>(ln.walk.as<uint8_t>() + sse_bytes);
+  H266_CUDA(cudaMemsetAsync(d_sse, 0, sse_bytes, ln.stream));
+  {
+    Pass2Args a = h.args;
+    bind_pass2(a, st.base, st, S, P);
+    Prof pf(ctx, ln.stream, H266_PROF_SAO_ALF);
+    H266_TRY(launch_alf_luma_trials(ln.stream, a, O, run, cols, d_sse, &ctx->launches));
+    H266_TRY(launch_alf_luma_decide(ln.stream, reinterpret_cast<CtbDev *>(st.base + st.ctb), (int)n, d_sse, cols, run,
+                                    d_dec, &ctx->launches));
+  }
+  H266_TRY(run_pass2(ctx, ln.stream, h.args, false, true, true, st.base, st, S, P));
+  std::vector<int16_t> dec(n);
+  H266_CUDA(cudaMemcpyAsync(dec.data(), d_dec, n * sizeof(int16_t), cudaMemcpyDeviceToHost, ln.stream));
+  if (sse) H266_CUDA(cudaMemcpyAsync(sse, d_sse, sse_bytes, cudaMemcpyDeviceToHost, ln.stream));
+  H266_TRY(picture_from_device(ln, rl));
+  ctx->d2h_bytes += host_plane_bytes(rl) + n * sizeof(int16_t) + (sse ? sse_bytes : 0);
+  for (size_t i = 0; i < n; ++i) {
+    decisions[i] = h266_alf_ctb{};
+    if (dec[i] < 0) continue;
+    decisions[i].luma_on = 1;
+    decisions[i].luma_filt_set_idx = (uint8_t)(dec[i] < 16 ? dec[i] : 16);
+  }
+  return H266_OK;
 }
 
 int h266_apply_in_loop_filters(h266_ctx *ctx, h266_picture *pic, const h266_in_loop_filter_args *args) {

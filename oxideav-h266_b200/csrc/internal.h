@@ -272,6 +272,45 @@ struct Pass2Args {
 int launch_pass2(cudaStream_t st, const Pass2Args &a, bool do_sao, bool do_alf, uint64_t *launches);
 // Packed 16x2 form; requires bit_depth <= 14, 4:2:0 or 4:0:0, coefficients in [-128, 127].
 int launch_pass2_packed(cudaStream_t st, const Pass2Args &a, bool do_sao, bool do_alf, uint64_t *launches);
+
+// ---------------------------------------------------------------- recon-side LMCS, output dump (recon.cu)
+struct RectPiece {  // a piece of a forward-map rectangle: <= 4096 samples, inside the plane
+  uint32_t x, y, w, h;
+};
+struct ResPiece {  // a piece of a chroma TB's residual add
+  uint32_t x, y, w, h;
+  uint32_t plane, var_scale;
+  uint64_t res_offset;  // residual of (x, y)
+  uint32_t res_pitch, pad;
+};
+struct CvsTables {
+  uint32_t pivot[17], chroma_scale[16];
+  uint32_t mn, mx, bd;
+};
+struct OutPlanes {
+  DPlane p[3];
+  uint32_t x0[3], y0[3], w[3];
+  uint64_t n[3], total;  // output samples per plane, and in all
+};
+int launch_lmcs_fwd_lut(cudaStream_t st, uint16_t *d_lut, const h266_lmcs_derived &l, uint64_t *launches);
+int launch_lmcs_fwd_rects(cudaStream_t st, DPlane p, const uint16_t *d_lut, const RectPiece *d_pieces, uint32_t n,
+                          bool check, uint32_t *d_err, uint64_t *launches);
+int launch_lmcs_cvs(cudaStream_t st, DPlane luma, const h266_lmcs_cvs_block *d_blocks, uint32_t n, int size_y,
+                    const CvsTables &t, uint32_t *d_out, uint64_t *launches);
+int launch_chroma_residual(cudaStream_t st, DPlane cb, DPlane cr, const ResPiece *d_pieces, uint32_t n,
+                           const int32_t *d_res, int bd, uint64_t *launches);
+int launch_output_dump(cudaStream_t st, const OutPlanes &o, uint8_t *d_dst, bool wide, uint64_t *launches);
+
+// Encoder luma ALF trials (packed form): `trials` filter-set slots of
+// a.tables.luma_packed evaluated on the pre-ALF luma a.src[0] against the
+// original `orig`; d_sse[ctb * cols + 0] += pre-ALF SSE, [.. + 1 + t] += SSE
+// of trial t (d_sse zeroed by the caller).  Then per CTB the decision, written
+// into d_ctbs[].luma_set (slot or -1) and d_decision[].
+constexpr int kAlfMaxTrials = 17;
+int launch_alf_luma_trials(cudaStream_t st, const Pass2Args &a, const DPlane &orig, int trials, int cols,
+                           unsigned long long *d_sse, uint64_t *launches);
+int launch_alf_luma_decide(cudaStream_t st, CtbDev *d_ctbs, int n, unsigned long long *d_sse, int cols, int trials_run,
+                           int16_t *d_decision, uint64_t *launches);
 // Batched packed pass: fills a's tile grid, returns the kernel variant (0..7)
 // and the picture's CTA count; pictures of one variant share a launch.
 int pass2_packed_variant(Pass2Args &a, bool do_sao, bool do_alf, uint32_t *ctas);

@@ -265,6 +265,158 @@ __device__ __forceinline__ void chroma_pair(const Pass2Args &a, const Smem<W> &s
 // window; (2) post-SAO windows of all planes; (3) luma Laplacian cells and
 // the chroma planes' ALF / CC-ALF (their inputs are complete after 2);
 // (4) luma classes; (5) the 7x7 luma filter.
+// Laplacian sums per 2x2 cell of the luma window `sm.sL` (unpadded rows).
+template <class S>
+__device__ __forceinline__ void luma_cells(S &sm) {
+  for (int i = threadIdx.x; i < S::CH * S::CW; i += NT) {
+    const int cy = i / S::CW, cx = i - cy * S::CW;
+    uint4 g = make_uint4(0, 0, 0, 0);
+#pragma unroll
+    for (int d = 0; d < 2; ++d) {
+      const int r = 2 * cy + d + 1;  // sL row of the position: y = Y0 - 2 + 2cy + d
+      const int c = 2 * cx + d + 2;  // sL col: x = X0 - 2 + 2cx + d
+      const uint16_t *row = &sm.sL[r * S::SLW + c];
+      const int c2 = 2 * row[0];
+      g.x += abs(c2 - row[-1] - row[1]);
+      g.y += abs(c2 - row[-S::SLW] - row[S::SLW]);
+      g.z += abs(c2 - row[-S::SLW - 1] - row[S::SLW + 1]);
+      g.w += abs(c2 - row[-S::SLW + 1] - row[S::SLW - 1]);
+    }
+    sm.cell[i] = g;
+  }
+}
+
+// Class and transposeIdx of every 4x4 block of the tile (src/alf.rs:750-1008).
+template <int W, class S>
+__device__ __forceinline__ void luma_classes(S &sm, int Y0, int y_ctb, int ctb, int ph, int bd) {
+  const bool bottom = y_ctb + ctb >= ph;
+  const bool carve = !bottom || (ph - y_ctb) > ctb - 4;
+  const int vb = y_ctb + ctb - 4;
+  constexpr int NB = (TH / 4) * (W / 4);
+  for (int b = threadIdx.x; b < NB; b += NT) {
+    const int bx = b % (W / 4), by = b / (W / 4);
+    const int y4 = Y0 + 4 * by - y_ctb;
+    if (y4 == ctb - 8 || y4 == ctb - 4) {  // virtual-boundary rows: windows and padding differ
+      int min_y = -2, max_y = 5, ac = 2;
+      if (y4 == ctb - 8 && carve) { max_y = 3; ac = 3; }
+      else if (y4 == ctb - 4 && carve) { min_y = 0; ac = 3; }
+      const bool top_pad = y4 == ctb - 4, bot_pad = y4 == ctb - 8;
+      auto pad = [&](int gy) {
+        if (top_pad) gy = max(gy, vb);
+        if (bot_pad) gy = min(gy, vb - 1);
+        return gy - (Y0 - 3);
+      };
+      int sh = 0, sv = 0, sd0 = 0, sd1 = 0;
+      for (int j = min_y; j <= max_y; ++j) {
+        const int gy = y_ctb + y4 + j;
+        const uint16_t *rc = &sm.sL[pad(gy) * S::SLW], *ru = &sm.sL[pad(gy - 1) * S::SLW],
+                       *rd = &sm.sL[pad(gy + 1) * S::SLW];
+        for (int i = (j & 1) ? -1 : -2; i <= 5; i += 2) {
+          const int c = 4 * bx + i + 4;
+          const int c2 = 2 * rc[c];
+          sh += abs(c2 - rc[c - 1] - rc[c + 1]);
+          sv += abs(c2 - ru[c] - rd[c]);
+          sd0 += abs(c2 - ru[c - 1] - rd[c + 1]);
+          sd1 += abs(c2 - ru[c + 1] - rd[c - 1]);
+        }
+      }
+      classify(sh, sv, sd0, sd1, ac, bd, sm.cls_f[b], sm.cls_t[b]);
+    } else {
+      uint4 s = make_uint4(0, 0, 0, 0);
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const uint4 g = sm.cell[(2 * by + r) * S::CW + 2 * bx + c];
+          s.x += g.x;
+          s.y += g.y;
+          s.z += g.z;
+          s.w += g.w;
+        }
+      classify((int)s.x, (int)s.y, (int)s.z, (int)s.w, 2, bd, sm.cls_f[b], sm.cls_t[b]);
+    }
+  }
+}
+
+// The 7x7 diamond on one run of 4 samples (tile row j, block column bx) with
+// one block's packed taps; `yr` is the row inside its CTB.  out[] receives the
+// filtered samples (src/alf.rs:652-743, Table 45 arms always applied).
+template <class S>
+__device__ __forceinline__ void luma_run(const S &sm, int j, int bx, int yr, int ctb, const uint32_t c2[12],
+                                         const uint32_t nc2[12], const uint32_t f[12], int maxv, int out[4]) {
+  int shift = 7, y1 = 1, y2 = 2, y3 = 3;
+  if (yr == ctb - 5 || yr == ctb - 4) { shift = 10; y1 = y2 = y3 = 0; }
+  else if (yr == ctb - 6 || yr == ctb - 3) { y2 = y3 = 1; }
+  else if (yr == ctb - 7 || yr == ctb - 2) { y3 = 2; }
+  const int r = j + 3;
+  const int c0 = 4 * bx + 4;
+  const uint16_t *R0 = &sm.sL[r * S::SLW];
+  const uint16_t *U1 = R0 - y1 * S::SLW, *D1 = R0 + y1 * S::SLW;
+  const uint16_t *U2 = R0 - y2 * S::SLW, *D2 = R0 + y2 * S::SLW;
+  const uint16_t *U3 = R0 - y3 * S::SLW, *D3 = R0 + y3 * S::SLW;
+  const uint32_t cur[2] = {pair_at<0>(R0, c0), pair_at<0>(R0, c0 + 2)};
+  const uint32_t ncur[2] = {neg2(cur[0]), neg2(cur[1])};
+  int acc[4] = {0, 0, 0, 0};
+  luma_tap<0>(D3, U3, c0, ncur, c2[0], nc2[0], f[0], acc);
+  luma_tap<1>(D2, U2, c0, ncur, c2[1], nc2[1], f[1], acc);
+  luma_tap<0>(D2, U2, c0, ncur, c2[2], nc2[2], f[2], acc);
+  luma_tap<-1>(D2, U2, c0, ncur, c2[3], nc2[3], f[3], acc);
+  luma_tap<2>(D1, U1, c0, ncur, c2[4], nc2[4], f[4], acc);
+  luma_tap<1>(D1, U1, c0, ncur, c2[5], nc2[5], f[5], acc);
+  luma_tap<0>(D1, U1, c0, ncur, c2[6], nc2[6], f[6], acc);
+  luma_tap<-1>(D1, U1, c0, ncur, c2[7], nc2[7], f[7], acc);
+  luma_tap<-2>(D1, U1, c0, ncur, c2[8], nc2[8], f[8], acc);
+  luma_tap<3>(R0, R0, c0, ncur, c2[9], nc2[9], f[9], acc);
+  luma_tap<2>(R0, R0, c0, ncur, c2[10], nc2[10], f[10], acc);
+  luma_tap<1>(R0, R0, c0, ncur, c2[11], nc2[11], f[11], acc);
+  const int round = 1 << (shift - 1);
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    const int cv = (int)((cur[p >> 1] >> ((p & 1) * 16)) & 0xFFFF);
+    out[p] = clampd(cv + ((acc[p] + round) >> shift), 0, maxv);
+  }
+}
+
+// The 12 symmetric tap sums (n+ - cur) + (n- - cur) of one 4-sample run,
+// packed per pixel pair, without clipping: the form every filter set whose
+// clip values never bind shares (clipIdx 0 gives 2^BitDepth, above any
+// |n - cur| of in-range samples).  Same taps and Table 45 rows as luma_run.
+template <class S>
+__device__ __forceinline__ void luma_sums(const S &sm, int j, int bx, int yr, int ctb, uint32_t sum[2][12],
+                                          uint32_t cur[2], int &shift) {
+  int y1 = 1, y2 = 2, y3 = 3;
+  shift = 7;
+  if (yr == ctb - 5 || yr == ctb - 4) { shift = 10; y1 = y2 = y3 = 0; }
+  else if (yr == ctb - 6 || yr == ctb - 3) { y2 = y3 = 1; }
+  else if (yr == ctb - 7 || yr == ctb - 2) { y3 = 2; }
+  const int c0 = 4 * bx + 4;
+  const uint16_t *R0 = &sm.sL[(j + 3) * S::SLW];
+  const uint16_t *U1 = R0 - y1 * S::SLW, *D1 = R0 + y1 * S::SLW;
+  const uint16_t *U2 = R0 - y2 * S::SLW, *D2 = R0 + y2 * S::SLW;
+  const uint16_t *U3 = R0 - y3 * S::SLW, *D3 = R0 + y3 * S::SLW;
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int c = c0 + 2 * q;
+    cur[q] = pair_at<0>(R0, c);
+    const uint32_t nc = neg2(cur[q]);
+    auto tap = [&](uint32_t up, uint32_t dn) {
+      return add2(__viaddmax_s16x2(up, nc, 0x80008000u), __viaddmax_s16x2(dn, nc, 0x80008000u));
+    };
+    sum[q][0] = tap(pair_at<0>(D3, c), pair_at<0>(U3, c));
+    sum[q][1] = tap(pair_at<1>(D2, c), pair_at<-1>(U2, c));
+    sum[q][2] = tap(pair_at<0>(D2, c), pair_at<0>(U2, c));
+    sum[q][3] = tap(pair_at<-1>(D2, c), pair_at<1>(U2, c));
+    sum[q][4] = tap(pair_at<2>(D1, c), pair_at<-2>(U1, c));
+    sum[q][5] = tap(pair_at<1>(D1, c), pair_at<-1>(U1, c));
+    sum[q][6] = tap(pair_at<0>(D1, c), pair_at<0>(U1, c));
+    sum[q][7] = tap(pair_at<-1>(D1, c), pair_at<1>(U1, c));
+    sum[q][8] = tap(pair_at<-2>(D1, c), pair_at<2>(U1, c));
+    sum[q][9] = tap(pair_at<3>(R0, c), pair_at<-3>(R0, c));
+    sum[q][10] = tap(pair_at<2>(R0, c), pair_at<-2>(R0, c));
+    sum[q][11] = tap(pair_at<1>(R0, c), pair_at<-1>(R0, c));
+  }
+}
+
 template <int W, bool DO_SAO, bool DO_ALF>
 __device__ __forceinline__ void sao_alf_tile(const Pass2Args &a, int tile) {
   using S = Smem<W>;
@@ -366,24 +518,7 @@ __device__ __forceinline__ void sao_alf_tile(const Pass2Args &a, int tile) {
 
   // ---- (3) luma Laplacian sums per 2x2 cell (unpadded rows); chroma ALF / CC-ALF
   const bool luma_alf = DO_ALF && me && me->luma_set >= 0;
-  if (luma_alf) {
-    for (int i = tid; i < S::CH * S::CW; i += NT) {
-      const int cy = i / S::CW, cx = i - cy * S::CW;
-      uint4 g = make_uint4(0, 0, 0, 0);
-#pragma unroll
-      for (int d = 0; d < 2; ++d) {
-        const int r = 2 * cy + d + 1;  // sL row of the position: y = Y0 - 2 + 2cy + d
-        const int c = 2 * cx + d + 2;  // sL col: x = X0 - 2 + 2cx + d
-        const uint16_t *row = &sm.sL[r * S::SLW + c];
-        const int c2 = 2 * row[0];
-        g.x += abs(c2 - row[-1] - row[1]);
-        g.y += abs(c2 - row[-S::SLW] - row[S::SLW]);
-        g.z += abs(c2 - row[-S::SLW - 1] - row[S::SLW + 1]);
-        g.w += abs(c2 - row[-S::SLW + 1] - row[S::SLW - 1]);
-      }
-      sm.cell[i] = g;
-    }
-  }
+  if (luma_alf) luma_cells(sm);
   {
     // both chroma planes, one pair of samples per (plane, pair) item
     constexpr int PAIRS = (TWC / 2) * THC;  // per plane
@@ -406,55 +541,7 @@ __device__ __forceinline__ void sao_alf_tile(const Pass2Args &a, int tile) {
   __syncthreads();
 
   // ---- (4) classes
-  {
-    const bool bottom = y_ctb + ctb >= ph;
-    const bool carve = !bottom || (ph - y_ctb) > ctb - 4;
-    const int vb = y_ctb + ctb - 4;
-    constexpr int NB = (TH / 4) * (W / 4);
-    for (int b = tid; b < NB; b += NT) {
-      const int bx = b % (W / 4), by = b / (W / 4);
-      const int y4 = Y0 + 4 * by - y_ctb;
-      if (y4 == ctb - 8 || y4 == ctb - 4) {  // virtual-boundary rows: windows and padding differ
-        int min_y = -2, max_y = 5, ac = 2;
-        if (y4 == ctb - 8 && carve) { max_y = 3; ac = 3; }
-        else if (y4 == ctb - 4 && carve) { min_y = 0; ac = 3; }
-        const bool top_pad = y4 == ctb - 4, bot_pad = y4 == ctb - 8;
-        auto pad = [&](int gy) {
-          if (top_pad) gy = max(gy, vb);
-          if (bot_pad) gy = min(gy, vb - 1);
-          return gy - (Y0 - 3);
-        };
-        int sh = 0, sv = 0, sd0 = 0, sd1 = 0;
-        for (int j = min_y; j <= max_y; ++j) {
-          const int gy = y_ctb + y4 + j;
-          const uint16_t *rc = &sm.sL[pad(gy) * S::SLW], *ru = &sm.sL[pad(gy - 1) * S::SLW],
-                         *rd = &sm.sL[pad(gy + 1) * S::SLW];
-          for (int i = (j & 1) ? -1 : -2; i <= 5; i += 2) {
-            const int c = 4 * bx + i + 4;
-            const int c2 = 2 * rc[c];
-            sh += abs(c2 - rc[c - 1] - rc[c + 1]);
-            sv += abs(c2 - ru[c] - rd[c]);
-            sd0 += abs(c2 - ru[c - 1] - rd[c + 1]);
-            sd1 += abs(c2 - ru[c + 1] - rd[c - 1]);
-          }
-        }
-        classify(sh, sv, sd0, sd1, ac, bd, sm.cls_f[b], sm.cls_t[b]);
-      } else {
-        uint4 s = make_uint4(0, 0, 0, 0);
-#pragma unroll
-        for (int r = 0; r < 4; ++r)
-#pragma unroll
-          for (int c = 0; c < 4; ++c) {
-            const uint4 g = sm.cell[(2 * by + r) * S::CW + 2 * bx + c];
-            s.x += g.x;
-            s.y += g.y;
-            s.z += g.z;
-            s.w += g.w;
-          }
-        classify((int)s.x, (int)s.y, (int)s.z, (int)s.w, 2, bd, sm.cls_f[b], sm.cls_t[b]);
-      }
-    }
-  }
+  luma_classes<W>(sm, Y0, y_ctb, ctb, ph, bd);
   __syncthreads();
 
   // ---- (5) 7x7 diamond, 4-pixel runs; every thread keeps one block's taps
@@ -476,40 +563,13 @@ __device__ __forceinline__ void sao_alf_tile(const Pass2Args &a, int tile) {
     const int jr = (tid % TPB) * RPT + rr;  // row inside the block
     const int j = 4 * by + jr;               // tile row
     const int gy = Y0 + j;
-    const int yr = gy - y_ctb;
-    int shift = 7, y1 = 1, y2 = 2, y3 = 3;  // Table 45 (line-buffer arms always applied)
-    if (yr == ctb - 5 || yr == ctb - 4) { shift = 10; y1 = y2 = y3 = 0; }
-    else if (yr == ctb - 6 || yr == ctb - 3) { y2 = y3 = 1; }
-    else if (yr == ctb - 7 || yr == ctb - 2) { y3 = 2; }
-    const int r = j + 3;
-    const int c0 = 4 * bx + 4;
-    const uint16_t *R0 = &sm.sL[r * S::SLW];
-    const uint16_t *U1 = R0 - y1 * S::SLW, *D1 = R0 + y1 * S::SLW;
-    const uint16_t *U2 = R0 - y2 * S::SLW, *D2 = R0 + y2 * S::SLW;
-    const uint16_t *U3 = R0 - y3 * S::SLW, *D3 = R0 + y3 * S::SLW;
-    const uint32_t cur[2] = {pair_at<0>(R0, c0), pair_at<0>(R0, c0 + 2)};
-    const uint32_t ncur[2] = {neg2(cur[0]), neg2(cur[1])};
-    int acc[4] = {0, 0, 0, 0};
-    luma_tap<0>(D3, U3, c0, ncur, c2[0], nc2[0], f[0], acc);
-    luma_tap<1>(D2, U2, c0, ncur, c2[1], nc2[1], f[1], acc);
-    luma_tap<0>(D2, U2, c0, ncur, c2[2], nc2[2], f[2], acc);
-    luma_tap<-1>(D2, U2, c0, ncur, c2[3], nc2[3], f[3], acc);
-    luma_tap<2>(D1, U1, c0, ncur, c2[4], nc2[4], f[4], acc);
-    luma_tap<1>(D1, U1, c0, ncur, c2[5], nc2[5], f[5], acc);
-    luma_tap<0>(D1, U1, c0, ncur, c2[6], nc2[6], f[6], acc);
-    luma_tap<-1>(D1, U1, c0, ncur, c2[7], nc2[7], f[7], acc);
-    luma_tap<-2>(D1, U1, c0, ncur, c2[8], nc2[8], f[8], acc);
-    luma_tap<3>(R0, R0, c0, ncur, c2[9], nc2[9], f[9], acc);
-    luma_tap<2>(R0, R0, c0, ncur, c2[10], nc2[10], f[10], acc);
-    luma_tap<1>(R0, R0, c0, ncur, c2[11], nc2[11], f[11], acc);
     if (gy < LD.h) {
-      const int round = 1 << (shift - 1);
+      int o[4];
+      luma_run(sm, j, bx, gy - y_ctb, ctb, c2, nc2, f, maxv, o);
       uint16_t *out = LD.s + (int64_t)gy * LD.stride + X0 + 4 * bx;
 #pragma unroll
-      for (int p = 0; p < 4; ++p) {
-        const int cv = (int)((cur[p >> 1] >> ((p & 1) * 16)) & 0xFFFF);
-        if (X0 + 4 * bx + p < LD.w) out[p] = (uint16_t)clampd(cv + ((acc[p] + round) >> shift), 0, maxv);
-      }
+      for (int p = 0; p < 4; ++p)
+        if (X0 + 4 * bx + p < LD.w) out[p] = (uint16_t)o[p];
     }
   }
 }
@@ -537,6 +597,192 @@ __global__ void __launch_bounds__(NT, 4) k_sao_alf_packed_batch(const Pass2Args 
   for (int i = threadIdx.x; i < (int)(sizeof(Pass2Args) / 4); i += blockDim.x) dst[i] = src[i];
   __syncthreads();
   sao_alf_tile<W, DO_SAO, DO_ALF>(s_args, (int)(blockIdx.x - first[lo]));
+}
+
+// ---- encoder luma ALF trials (src/alf_enc.rs:185-528)
+//
+// The reference runs one full apply_alf per candidate filter set (16 fixed
+// sets, plus the APS set) on a copy of the picture and sums SSE_Y per CTB
+// against the original.  Luma ALF output depends only on the pre-ALF samples
+// and the CTB's own filter set, so one tile pass serves every trial: it
+// stages the pre-ALF window once, classifies the 4x4 blocks once, then
+// filters the tile with each trial's taps and adds the squared errors of its
+// samples into per-(CTB, trial) sums; nothing is written back.  Column 0 of a
+// CTB's row is the pre-ALF SSE (the "off" option).
+template <int W>
+struct TrialSmem {
+  static constexpr int SLW = W + 8, SLH = TH + 6;        // pre-ALF luma [X0-4, X1+4) x [Y0-3, Y1+3)
+  static constexpr int CW = W / 2 + 2, CH = TH / 2 + 2;  // 2x2 Laplacian cells
+  alignas(16) uint16_t sL[SLH * SLW];
+  alignas(16) uint4 cell[CH * CW];
+  uint8_t cls_f[(TH / 4) * (W / 4)], cls_t[(TH / 4) * (W / 4)];
+  alignas(8) unsigned long long sse[kAlfMaxTrials + 1];
+};
+
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <int W>
+__global__ void __launch_bounds__(NT, 2) k_alf_luma_trials(const __grid_constant__ Pass2Args a, const DPlane orig,
+                                                           int trials, int cols, unsigned long long *__restrict__ sse) {
+  using S = TrialSmem<W>;
+  __shared__ S sm;
+  const int tid = threadIdx.x, tile = blockIdx.x;
+  const int tx = tile % a.tiles_x, ty = tile / a.tiles_x;
+  const int X0 = tx * W, Y0 = ty * TH;
+  const int bd = a.bit_depth, maxv = (1 << bd) - 1;
+  const int log2 = a.ctb_log2, ctb = 1 << log2;
+  const int rx = X0 >> log2, ry = Y0 >> log2;
+  if (rx >= a.w_ctbs || ry >= a.h_ctbs) return;  // uniform per CTA
+  const int y_ctb = ry << log2;
+  const int pw = a.pic_w, ph = a.pic_h;
+  const CtbDev &me = a.ctbs[ry * a.w_ctbs + rx];
+  const int rx0 = max((int)me.rect[0], 0), ry0 = max((int)me.rect[1], 0);
+  const int rx1 = min((int)me.rect[2], pw), ry1 = min((int)me.rect[3], ph);
+  const DPlane LS = a.src[0];
+  int wide = 0;  // a sample above 2^BitDepth - 1 (outside the picture format): clips may bind for every set
+  for (int i = tid; i < S::SLH * S::SLW; i += NT) {  // clamped into the fetch rectangle (sample(), src/alf.rs:1093-1110)
+    const int r = i / S::SLW, c = i - r * S::SLW;
+    const int ax = clampd(X0 - 4 + c, rx0, rx1 - 1), ay = clampd(Y0 - 3 + r, ry0, ry1 - 1);
+    const uint16_t v = LS.s[(int64_t)ay * LS.stride + ax];
+    wide |= v > maxv;
+    sm.sL[i] = v;
+  }
+  if (tid <= trials) sm.sse[tid] = 0;
+  wide = __syncthreads_or(wide);
+  luma_cells(sm);
+  __syncthreads();
+  luma_classes<W>(sm, Y0, y_ctb, ctb, ph, bd);
+  __syncthreads();
+
+  constexpr int RUNS = TH * W / 4;
+  constexpr int RPT = RUNS / NT;
+  constexpr int TPB = 4 / RPT;
+  const int b = tid / TPB;
+  const int bx = b % (W / 4), by = b / (W / 4);
+  // the SSE window is the CTB inside both planes (ctb_sse_y, src/alf_enc.rs:79-105)
+  const int vw = min(orig.w, pw), vh = min(orig.h, ph);
+  int org[RPT][4];
+  unsigned long long e0 = 0;
+#pragma unroll
+  for (int rr = 0; rr < RPT; ++rr) {
+    const int j = 4 * by + (tid % TPB) * RPT + rr, gy = Y0 + j;
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      const int gx = X0 + 4 * bx + p;
+      const bool in = gx < vw && gy < vh;
+      org[rr][p] = in ? (int)orig.s[(int64_t)gy * orig.stride + gx] : -1;
+      if (in) {
+        const int d = org[rr][p] - (int)sm.sL[(j + 3) * S::SLW + 4 * bx + p + 4];
+        e0 += (unsigned long long)(d * d);
+      }
+    }
+  }
+  e0 = warp_sum(e0);
+  if ((tid & 31) == 0) atomicAdd(&sm.sse[0], e0);
+  const int cls = sm.cls_f[b] * 4 + sm.cls_t[b];
+  int first = 0;  // first trial of the clipped path
+  if (!wide) {
+    // fixed sets 0..15 (clipIdx 0): tap sums once, then 12 dp2a per pixel pair per set
+    first = min(trials, 16);
+    uint32_t sum[RPT][2][12], cur[RPT][2];
+    int shift[RPT];
+#pragma unroll
+    for (int rr = 0; rr < RPT; ++rr) {
+      const int j = 4 * by + (tid % TPB) * RPT + rr;
+      luma_sums(sm, j, bx, Y0 + j - y_ctb, ctb, sum[rr], cur[rr], shift[rr]);
+    }
+    const uint32_t *tab0 = a.tables.luma_packed + (size_t)cls * 36 + 2;  // coefficient words of trial t at + t * 3600
+    uint32_t fn[12];  // the next trial's coefficients, loaded while the current trial runs
+#pragma unroll
+    for (int k = 0; k < 12; ++k) fn[k] = first > 0 ? __ldg(tab0 + 3 * k) : 0u;
+    for (int t = 0; t < first; ++t) {
+      uint32_t f[12];
+#pragma unroll
+      for (int k = 0; k < 12; ++k) f[k] = fn[k];
+      if (t + 1 < first) {
+#pragma unroll
+        for (int k = 0; k < 12; ++k) fn[k] = __ldg(tab0 + (size_t)(t + 1) * 3600 + 3 * k);
+      }
+      unsigned long long e = 0;
+#pragma unroll
+      for (int rr = 0; rr < RPT; ++rr) {
+        const int round = 1 << (shift[rr] - 1);
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          int lo = 0, hi = 0;
+#pragma unroll
+          for (int k = 0; k < 12; ++k) {
+            lo = __dp2a_lo((int)sum[rr][q][k], (int)f[k], lo);
+            hi = __dp2a_lo((int)sum[rr][q][k], (int)(f[k] << 8), hi);
+          }
+          const int v0 = clampd((int)(cur[rr][q] & 0xFFFF) + ((lo + round) >> shift[rr]), 0, maxv);
+          const int v1 = clampd((int)(cur[rr][q] >> 16) + ((hi + round) >> shift[rr]), 0, maxv);
+          if (org[rr][2 * q] >= 0) {
+            const int d = org[rr][2 * q] - v0;
+            e += (unsigned long long)(d * d);
+          }
+          if (org[rr][2 * q + 1] >= 0) {
+            const int d = org[rr][2 * q + 1] - v1;
+            e += (unsigned long long)(d * d);
+          }
+        }
+      }
+      e = warp_sum(e);
+      if ((tid & 31) == 0) atomicAdd(&sm.sse[1 + t], e);
+    }
+  }
+  for (int t = first; t < trials; ++t) {
+    const uint32_t *tab = a.tables.luma_packed + ((size_t)t * 100 + cls) * 36;
+    uint32_t c2[12], nc2[12], f[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      c2[k] = __ldg(tab + 3 * k);
+      nc2[k] = __ldg(tab + 3 * k + 1);
+      f[k] = __ldg(tab + 3 * k + 2);
+    }
+    unsigned long long e = 0;
+#pragma unroll
+    for (int rr = 0; rr < RPT; ++rr) {
+      const int j = 4 * by + (tid % TPB) * RPT + rr;
+      int o[4];
+      luma_run(sm, j, bx, Y0 + j - y_ctb, ctb, c2, nc2, f, maxv, o);
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+        if (org[rr][p] >= 0) {
+          const int d = org[rr][p] - o[p];
+          e += (unsigned long long)(d * d);
+        }
+    }
+    e = warp_sum(e);
+    if ((tid & 31) == 0) atomicAdd(&sm.sse[1 + t], e);
+  }
+  __syncthreads();
+  if (tid <= trials) atomicAdd(&sse[(size_t)(ry * a.w_ctbs + rx) * cols + tid], sm.sse[tid]);
+}
+
+// Per CTB the lowest SSE among {off, trial 0, ...} (strict <: earlier options
+// win ties, src/alf_enc.rs:276-292, 482-498); the commit pass then filters
+// the chosen CTBs with their sets.  Trials not run (an APS without luma
+// filters leaves the samples as they are) take the pre-ALF SSE.
+__global__ void k_alf_luma_decide(CtbDev *__restrict__ ctbs, int n, unsigned long long *__restrict__ sse, int cols,
+                                  int trials_run, int16_t *__restrict__ decision) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  unsigned long long *row = sse + (size_t)i * cols;
+  for (int t = trials_run; t < cols - 1; ++t) row[1 + t] = row[0];
+  unsigned long long best = row[0];
+  int pick = -1;
+  for (int t = 0; t < cols - 1; ++t)
+    if (row[1 + t] < best) {
+      best = row[1 + t];
+      pick = t;
+    }
+  ctbs[i].luma_set = (int16_t)pick;
+  decision[i] = (int16_t)pick;
 }
 
 template <int W>
@@ -587,6 +833,32 @@ int launch_pass2_packed_batch(cudaStream_t st, int variant, const Pass2Args *d_a
     case 1: return go(k_sao_alf_packed_batch<32, false, true>, sizeof(Smem<32>));
     default: return go(k_sao_alf_packed_batch<32, false, false>, sizeof(Smem<32>));
   }
+}
+
+int launch_alf_luma_trials(cudaStream_t st, const Pass2Args &in, const DPlane &orig, int trials, int cols,
+                           unsigned long long *d_sse, uint64_t *launches) {
+  if (in.ext_w <= 0 || in.ext_h <= 0) return H266_OK;
+  if (trials < 0 || trials > kAlfMaxTrials || cols < trials + 1)
+    return set_error(H266_ERR_INVALID_ARGUMENT, "ALF trials: bad trial count");
+  Pass2Args a = in;
+  const int W = a.ctb_log2 >= 6 ? 64 : 32;
+  a.tiles_x = (a.ext_w + W - 1) / W;
+  a.tiles_y = (a.ext_h + TH - 1) / TH;
+  const unsigned n = (unsigned)(a.tiles_x * a.tiles_y);
+  if (W == 64) k_alf_luma_trials<64><<<n, NT, 0, st>>>(a, orig, trials, cols, d_sse);
+  else k_alf_luma_trials<32><<<n, NT, 0, st>>>(a, orig, trials, cols, d_sse);
+  H266_CUDA(cudaGetLastError());
+  ++*launches;
+  return H266_OK;
+}
+
+int launch_alf_luma_decide(cudaStream_t st, CtbDev *d_ctbs, int n, unsigned long long *d_sse, int cols, int trials_run,
+                           int16_t *d_decision, uint64_t *launches) {
+  if (n <= 0) return H266_OK;
+  k_alf_luma_decide<<<(n + 127) / 128, 128, 0, st>>>(d_ctbs, n, d_sse, cols, trials_run, d_decision);
+  H266_CUDA(cudaGetLastError());
+  ++*launches;
+  return H266_OK;
 }
 
 int launch_pass2_packed(cudaStream_t st, const Pass2Args &a, bool do_sao, bool do_alf, uint64_t *launches) {

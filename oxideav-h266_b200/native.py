@@ -35,7 +35,9 @@ EXPORTS = [
     "h266_apply_in_loop_filters_batch", "h266_ctx_set_profiling", "h266_ctx_profile", "h266_chain_plan_create",
     "h266_chain_plan_execute", "h266_chain_plan_execute_batch", "h266_chain_plan_destroy",
     "h266_apply_in_loop_filters_noalloc", "h266_server_create", "h266_server_submit", "h266_server_wait",
-    "h266_server_stats", "h266_server_replay", "h266_server_destroy",
+    "h266_server_stats", "h266_server_replay", "h266_server_destroy", "h266_alf_decide_and_apply_clipped",
+    "h266_lmcs_forward_map_luma_rects", "h266_lmcs_chroma_var_scale", "h266_lmcs_add_chroma_residual",
+    "h266_output_convert",
 ]
 PROF_FAMILIES = ("lmcs", "deblock", "sao_alf", "copy")
 
@@ -81,6 +83,12 @@ def lib():
         L.h266_server_destroy.argtypes = [vp]
         L.h266_chain_plan_destroy.argtypes = [vp]
         L.h266_apply_in_loop_filters_noalloc.argtypes = [vp, vp, vp]
+        L.h266_alf_decide_and_apply_clipped.argtypes = [vp, vp, vp, vp, u32, u32, u32, vp, u64, vp, u64, vp, u64,
+                                                         vp]
+        L.h266_lmcs_forward_map_luma_rects.argtypes = [vp, vp, vp, vp, u64]
+        L.h266_lmcs_chroma_var_scale.argtypes = [vp, vp, vp, u32, u32, u32, vp, u64, vp]
+        L.h266_lmcs_add_chroma_residual.argtypes = [vp, vp, u32, vp, u64, vp, u64]
+        L.h266_output_convert.argtypes = [vp, vp, vp, u32, u32, vp, u64, u32, C.POINTER(u64)]
         _LIB = L
     return _LIB
 
@@ -339,3 +347,71 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def alf_decide_and_apply(ctx: Context, src, rec, aps=None, *, ctb_log2: int, bit_depth: int,
+                         chroma_format_idc: int = 1, clip_cols=None, clip_rows=None, want_sse: bool = False):
+    """h266_alf_decide_and_apply_clipped: the encoder's per-CTB luma ALF choice
+    among {off, fixed sets 0..15[, the APS set]} applied to `rec` in place.
+    Returns (decisions as an ALF_CTB array of the rec CTB grid, SSE table or None)."""
+    ctb = 1 << ctb_log2
+    wc, hc = -(-rec.luma.shape[1] // ctb), -(-rec.luma.shape[0] // ctb)
+    n = wc * hc
+    dec = np.zeros(n, dtype=abi.ALF_CTB)
+    cols = 18 if aps is not None else 17
+    sse = np.zeros((n, cols), dtype=np.uint64) if want_sse else None
+    s_c, r_c = src.to_ctypes(), rec.to_ctypes()
+    c1, nc, k1 = _u32(clip_cols)
+    c2, nr, k2 = _u32(clip_rows)
+    _check(lib().h266_alf_decide_and_apply_clipped(
+        ctx._h, C.byref(s_c), C.byref(r_c), C.byref(aps) if aps is not None else None, ctb_log2, bit_depth,
+        chroma_format_idc, c1, nc, c2, nr, dec.ctypes.data, n, sse.ctypes.data if sse is not None else None))
+    return dec, sse
+
+
+def _ptr(x):
+    """Address of a numpy array or a torch tensor."""
+    return x.data_ptr() if hasattr(x, "data_ptr") else x.ctypes.data
+
+
+def lmcs_forward_map_luma_rects(ctx: Context, pic, lmcs, rects):
+    """h266_lmcs_forward_map_luma_rects: rects is an abi.RECT array, in order."""
+    cp = pic.to_ctypes()
+    r = np.ascontiguousarray(rects, dtype=abi.RECT)
+    _check(lib().h266_lmcs_forward_map_luma_rects(ctx._h, C.byref(cp), C.byref(lmcs), r.ctypes.data if len(r) else None,
+                                                  len(r)))
+
+
+def lmcs_chroma_var_scale(ctx: Context, pic, lmcs, mn: int, mx: int, ctb_size_y: int, blocks) -> np.ndarray:
+    cp = pic.to_ctypes()
+    b = np.ascontiguousarray(blocks, dtype=abi.CVS_BLOCK)
+    out = np.zeros(max(len(b), 1), dtype=np.uint32)
+    _check(lib().h266_lmcs_chroma_var_scale(ctx._h, C.byref(cp), C.byref(lmcs), mn, mx, ctb_size_y,
+                                            b.ctypes.data if len(b) else None, len(b), out.ctypes.data))
+    return out[: len(b)]
+
+
+def lmcs_add_chroma_residual(ctx: Context, pic, bit_depth: int, res, blocks):
+    """res: int32 numpy array (host pictures) or int32 CUDA tensor (device pictures)."""
+    cp = pic.to_ctypes()
+    b = np.ascontiguousarray(blocks, dtype=abi.RES_BLOCK)
+    n_res = res.numel() if hasattr(res, "numel") else res.size
+    _check(lib().h266_lmcs_add_chroma_residual(ctx._h, C.byref(cp), bit_depth, _ptr(res) if n_res else None, n_res,
+                                               b.ctypes.data if len(b) else None, len(b)))
+
+
+def output_convert(ctx: Context, pic, crop, chroma_format_idc: int, bit_depth: int, dst=None) -> np.ndarray:
+    """h266_output_convert into a new host byte array (or `dst`, a uint8 CUDA tensor)."""
+    cp = pic.to_ctypes()
+    cw = abi.CropWindow(*crop)
+    n = C.c_uint64()
+    _check(lib().h266_output_convert(ctx._h, C.byref(cp), C.byref(cw), chroma_format_idc, bit_depth, None, 0,
+                                     abi.MEM_HOST, C.byref(n)))  # size query
+    if dst is not None:
+        _check(lib().h266_output_convert(ctx._h, C.byref(cp), C.byref(cw), chroma_format_idc, bit_depth,
+                                         dst.data_ptr(), dst.numel(), abi.MEM_DEVICE, C.byref(n)))
+        return dst
+    out = np.zeros(max(n.value, 1), dtype=np.uint8)
+    _check(lib().h266_output_convert(ctx._h, C.byref(cp), C.byref(cw), chroma_format_idc, bit_depth,
+                                     out.ctypes.data, out.size, abi.MEM_HOST, C.byref(n)))
+    return out[: n.value]

@@ -116,3 +116,17 @@ def check(case, before: PictureData, after: PictureData):
             assert got == e["v"], f"{tag} got {got}"
         else:
             raise ValueError(c)
+
+
+def lmcs_data(c):
+    """LmcsData of one transcribed LMCS case (tests/golden/kats.json "lmcs")."""
+    d = abi.LmcsData()
+    d.lmcs_min_bin_idx = c["min"]
+    d.lmcs_delta_max_bin_idx = c["dmax"]
+    d.lmcs_delta_cw_prec_minus1 = c["prec"]
+    for k, v in c["deltas"].items():
+        d.lmcs_delta_abs_cw[int(k)] = abs(v)
+        d.lmcs_delta_sign_cw_flag[int(k)] = 1 if v < 0 else 0
+    d.lmcs_delta_abs_crs = abs(c["crs"])
+    d.lmcs_delta_sign_crs_flag = 1 if c["crs"] < 0 else 0
+    return d

@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 import oracle
-from kat_util import KATS, build_args, build_picture, check
+from kat_util import KATS, build_args, build_picture, check, lmcs_data
 from oxideav_h266_b200 import abi
 
 CASES = KATS["cases"]
@@ -126,19 +126,6 @@ def test_classification_kats():
         ctb = 1 << log2
         f, _ = _classify(np.full((ctb, ctb), 100), ctb=ctb)
         assert f.shape == (ctb // 4, ctb // 4)
-
-
-def lmcs_data(c):
-    d = abi.LmcsData()
-    d.lmcs_min_bin_idx = c["min"]
-    d.lmcs_delta_max_bin_idx = c["dmax"]
-    d.lmcs_delta_cw_prec_minus1 = c["prec"]
-    for k, v in c["deltas"].items():
-        d.lmcs_delta_abs_cw[int(k)] = abs(v)
-        d.lmcs_delta_sign_cw_flag[int(k)] = 1 if v < 0 else 0
-    d.lmcs_delta_abs_crs = abs(c["crs"])
-    d.lmcs_delta_sign_crs_flag = 1 if c["crs"] < 0 else 0
-    return d
 
 
 def lmcs_field(derived, key):
