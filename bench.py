@@ -357,6 +357,34 @@ def run_encoder_trials(ctx, local_rank, stream, steps: int, n_pics: int = 4):
     t0 = time.perf_counter()
     oracle.alf_decide_and_apply(s_, r2, a, ctb_log2=7, bit_depth=10, alf_ctb_dtype=abi.ALF_CTB)
     cpu_ms = (time.perf_counter() - t0) * 1e3
+
+    # SAO decision (src/sao_enc.rs:385-487) on the same device pictures: statistics + decision kernels
+    for d in devs:
+        native.sao_decide_picture(ctx, d[0], d[1], ctb_log2=7, bit_depth=10)
+    torch.cuda.synchronize()
+    ctx.set_profiling(True)
+    ctx.profile()
+    s_total, s_calls = 0.0, 0
+    for _ in range(max(1, steps)):
+        for d in devs:
+            e0.record(stream)
+            native.sao_decide_picture(ctx, d[0], d[1], ctb_log2=7, bit_depth=10)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            s_total += e0.elapsed_time(e1)
+            s_calls += 1
+    sprof = ctx.profile()
+    ctx.set_profiling(False)
+    t0 = time.perf_counter()
+    oracle.sao_decide_picture(s_, r_, ctb_log2=7, bit_depth=10, params_dtype=abi.SAO_CTB_PARAMS)
+    sao_cpu_ms = (time.perf_counter() - t0) * 1e3
+    sao = {"workload": "encoder SAO decision, 1920x1080 10-bit CTU 128, luma + chroma",
+           "ms_per_picture": round(s_total / s_calls, 4),
+           "kernel_ms_per_picture": round(sprof["sao_alf"][0] / s_calls, 4),
+           "mpx_per_s": round(px / (s_total / s_calls) / 1e3, 1),
+           "path": "h266_sao_decide_picture on H266_MEM_DEVICE pictures (statistics, decision, records copied back)",
+           "cpu_oracle": {"ms_per_picture": round(sao_cpu_ms, 1), "cores": 1, "kind": "port",
+                          "sample": "one picture"}}
     del devs
     torch.cuda.synchronize()
     return {"workload": "encoder luma ALF decision, 1920x1080 10-bit CTU 128, 16 fixed sets + 1 APS set",
@@ -365,7 +393,8 @@ def run_encoder_trials(ctx, local_rank, stream, steps: int, n_pics: int = 4):
             "path": "h266_alf_decide_and_apply_clipped on H266_MEM_DEVICE pictures (trials, decision, commit, "
                     "decisions copied back)",
             "cpu_oracle": {"ms_per_picture": round(cpu_ms, 1), "mpx_per_s": round(px / cpu_ms / 1e3, 2), "cores": 1,
-                           "kind": "port", "sample": "one picture, the reference's 17 apply_alf trial passes"}}
+                           "kind": "port", "sample": "one picture, the reference's 17 apply_alf trial passes"},
+            "sao_decide": sao}
 
 
 def run_recon_io(ctx, local_rank, stream, steps: int, peak_gbs: float):

@@ -290,6 +290,18 @@ int h266_derive_lmcs(const h266_lmcs_data *data, uint32_t bit_depth, h266_lmcs_d
 int h266_lmcs_inverse_map_luma(h266_ctx *ctx, h266_picture *pic, const h266_lmcs_derived *lmcs,
                                uint32_t lmcs_min_bin_idx, uint32_t lmcs_max_bin_idx);
 
+/* Encoder SAO decision: sao_decide_picture (src/sao_enc.rs:385-487).  For
+ * every CTB of rec's grid (luma size / CTB size rounded up), luma (when
+ * sao_luma), Cb and Cr (when sao_chroma; Cr within Cb's type and class) get
+ * the crate's band-offset / edge-offset choice from the src - rec statistics
+ * of the CTB (4:2:0 chroma at half the luma CTB).  out: n_out = wc * hc
+ * records in host memory; the pictures are not modified.  A sample above
+ * (1 << bit_depth) - 1 has no band in the crate (its index runs out of
+ * bounds) and makes the call return H266_ERR_INVALID_ARGUMENT. */
+int h266_sao_decide_picture(h266_ctx *ctx, const h266_picture *src, const h266_picture *rec,
+                            uint32_t ctb_log2_size_y, uint32_t bit_depth, uint32_t sao_luma, uint32_t sao_chroma,
+                            h266_sao_ctb_params *out, uint64_t n_out);
+
 /* ---- recon-side LMCS (src/lmcs.rs:169-290, src/ctu.rs:734-742, 1701-1815) */
 typedef struct h266_rect {
     uint32_t x, y, w, h;

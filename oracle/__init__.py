@@ -78,6 +78,8 @@ def lib():
         L.oracle_lmcs_add_chroma_residual.argtypes = [vp, C.c_uint32, vp, vp, C.c_uint64]
         L.oracle_output_convert.argtypes = [vp, vp, C.c_uint32, C.c_uint32, vp]
         L.oracle_output_convert.restype = C.c_uint64
+        L.oracle_sao_eo_category.argtypes = [C.c_int, C.c_int, C.c_int]
+        L.oracle_sao_decide_picture.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_int, C.c_int, vp]
         _LIB = L
     return _LIB
 
@@ -220,3 +222,15 @@ def output_convert(pic, crop, chroma_format_idc, bit_depth, crop_type) -> np.nda
     out = np.zeros(pic.luma.size * 2 * 2 + 16, dtype=np.uint8)
     n = lib().oracle_output_convert(C.byref(cp), C.byref(cw), chroma_format_idc, bit_depth, out.ctypes.data)
     return out[:n]
+
+
+def sao_decide_picture(src, rec, *, ctb_log2: int, bit_depth: int, luma: bool = True, chroma: bool = True,
+                       params_dtype=None) -> np.ndarray:
+    """sao_decide_picture (src/sao_enc.rs:385-487): one SaoCtbParams per CTB of rec's grid."""
+    ctb = 1 << ctb_log2
+    n = (-(-rec.luma.shape[1] // ctb)) * (-(-rec.luma.shape[0] // ctb))
+    out = np.zeros(n, dtype=params_dtype)
+    s_c, r_c = src.to_ctypes(), rec.to_ctypes()
+    lib().oracle_sao_decide_picture(C.byref(s_c), C.byref(r_c), ctb_log2, bit_depth, int(luma), int(chroma),
+                                    out.ctypes.data)
+    return out

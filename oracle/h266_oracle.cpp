@@ -1434,6 +1434,175 @@ static uint64_t output_convert(const h266_picture *pic, const h266_crop_window &
   return o;
 }
 
+// ---- encoder SAO decision (src/sao_enc.rs:44-487)
+static bool pget(const h266_plane &p, int64_t x, int64_t y, uint16_t &v) {  // PicturePlane::get
+  if (x < 0 || y < 0 || x >= (int64_t)p.width || y >= (int64_t)p.height) return false;
+  v = p.samples[(size_t)y * p.stride + (size_t)x];
+  return true;
+}
+
+// derive_offset_val, src/sao.rs:356-365
+static void sao_offsets(h266_sao_ctb &c, const uint32_t abs_[4], const uint32_t sign[4], uint32_t bd) {
+  const int shift = (int)bd - (int)std::min<uint32_t>(bd, 10);
+  c.offset_val[0] = 0;
+  for (int i = 0; i < 4; ++i) c.offset_val[i + 1] = (1 - 2 * (int)(sign[i] & 1)) * (int)(abs_[i] << shift);
+}
+
+// try_band_offset, src/sao_enc.rs:77-171
+static bool try_band_offset(const h266_plane &src, const h266_plane &rec, size_t cx, size_t cy, size_t cw, size_t ch,
+                            uint32_t bd, h266_sao_ctb &out) {
+  int64_t cnt[32] = {0}, dif[32] = {0};
+  const uint32_t shift = bd - 5;
+  const size_t xe = std::min<size_t>(cx + cw, rec.width), ye = std::min<size_t>(cy + ch, rec.height);
+  for (size_t y = cy; y < ye; ++y)
+    for (size_t x = cx; x < xe; ++x) {
+      uint16_t r, s;
+      if (pget(rec, x, y, r) && pget(src, x, y, s)) {
+        cnt[r >> shift] += 1;
+        dif[r >> shift] += (int64_t)s - r;
+      }
+    }
+  int64_t best_delta = 0;
+  int best_start = 0, best_off[4] = {0, 0, 0, 0};
+  for (int start = 0; start < 28; ++start) {
+    int64_t delta = 0;
+    int off[4] = {0, 0, 0, 0};
+    for (int i = 0; i < 4; ++i) {
+      const int b = start + i;
+      if (cnt[b] > 0) {
+        const int64_t cmax = ((int64_t)1 << (std::min<uint32_t>(bd, 10) - 5)) - 1;
+        const int64_t opt = (dif[b] + cnt[b] / 2) / cnt[b];
+        off[i] = (int)clampl(opt, -cmax, cmax);
+        delta -= dif[b] * off[i];
+      }
+    }
+    if (delta < best_delta) {
+      best_delta = delta;
+      best_start = start;
+      std::memcpy(best_off, off, sizeof off);
+    }
+  }
+  if (best_delta >= 0) return false;
+  uint32_t a[4], sg[4];
+  for (int i = 0; i < 4; ++i) {
+    a[i] = (uint32_t)(best_off[i] < 0 ? -best_off[i] : best_off[i]);
+    sg[i] = best_off[i] < 0 ? 1 : 0;
+  }
+  out = h266_sao_ctb{};
+  out.sao_type_idx = 1;
+  out.band_position = (uint8_t)(best_start & 31);
+  sao_offsets(out, a, sg, bd);
+  return true;
+}
+
+// eo_category, src/sao_enc.rs:349-373
+static int eo_category(int r, int n0, int n1) {
+  const int s = (r > n0 ? 1 : (r < n0 ? -1 : 0)) + (r > n1 ? 1 : (r < n1 ? -1 : 0));
+  switch (s) {
+    case 2: return 4;
+    case 1: return 3;
+    case -1: return 2;
+    case -2: return 1;
+    default: return 0;
+  }
+}
+
+// try_edge_offset_class, src/sao_enc.rs:211-284 (the delta uses |diff|, as there)
+static void try_edge_offset_class(const h266_plane &src, const h266_plane &rec, size_t cx, size_t cy, size_t cw,
+                                  size_t ch, uint32_t bd, int cls, h266_sao_ctb &out, int64_t &delta) {
+  static const int kDirs[4][4] = {{-1, 0, 1, 0}, {0, -1, 0, 1}, {-1, -1, 1, 1}, {1, -1, -1, 1}};
+  const int *d = kDirs[cls];
+  int64_t cnt[5] = {0}, dif[5] = {0};
+  const size_t xe = std::min<size_t>(cx + cw, rec.width), ye = std::min<size_t>(cy + ch, rec.height);
+  for (size_t y = cy; y < ye; ++y)
+    for (size_t x = cx; x < xe; ++x) {
+      uint16_t r, a, b, s;
+      if (!pget(rec, x, y, r)) continue;
+      if (!pget(rec, (int64_t)x + d[0], (int64_t)y + d[1], a) || !pget(rec, (int64_t)x + d[2], (int64_t)y + d[3], b))
+        continue;
+      const int cat = eo_category(r, a, b);
+      if (pget(src, x, y, s)) {
+        cnt[cat] += 1;
+        dif[cat] += (int64_t)s - r;
+      }
+    }
+  uint32_t off[4] = {0, 0, 0, 0};
+  delta = 0;
+  for (int i = 0; i < 4; ++i) {
+    const int cat = i + 1;
+    if (cnt[cat] > 0) {
+      const int64_t ad = dif[cat] < 0 ? -dif[cat] : dif[cat];
+      off[i] = (uint32_t)clampl((ad + cnt[cat] / 2) / cnt[cat], 0, 7);
+      delta -= ad * (int64_t)off[i];
+    }
+  }
+  static const uint32_t kSign[4] = {0, 0, 1, 1};  // SaoCtb::edge_offset, src/sao.rs:169-180
+  out = h266_sao_ctb{};
+  out.sao_type_idx = 2;
+  out.eo_class = (uint8_t)cls;
+  sao_offsets(out, off, kSign, bd);
+}
+
+// sao_decide_ctb, src/sao_enc.rs:44-70 (with try_best_edge_offset, :175-209)
+static h266_sao_ctb sao_decide_ctb(const h266_plane &src, const h266_plane &rec, size_t cx, size_t cy, size_t cw,
+                                   size_t ch, uint32_t bd) {
+  h266_sao_ctb bo{}, eo{}, t{};
+  const bool has_bo = try_band_offset(src, rec, cx, cy, cw, ch, bd, bo);
+  int64_t best = 0, delta;
+  bool has_eo = false;
+  for (int c = 0; c < 4; ++c) {
+    try_edge_offset_class(src, rec, cx, cy, cw, ch, bd, c, t, delta);
+    if (delta < best) {
+      best = delta;
+      eo = t;
+      has_eo = true;
+    }
+  }
+  if (has_eo) return eo;
+  if (has_bo) return bo;
+  return h266_sao_ctb{};
+}
+
+// sao_decide_ctb_constrained, src/sao_enc.rs:286-347
+static h266_sao_ctb sao_decide_ctb_constrained(const h266_plane &src, const h266_plane &rec, size_t cx, size_t cy,
+                                               size_t cw, size_t ch, uint32_t bd, const h266_sao_ctb &shared) {
+  h266_sao_ctb out{};
+  if (shared.sao_type_idx == 1) {
+    if (!try_band_offset(src, rec, cx, cy, cw, ch, bd, out)) {
+      out = h266_sao_ctb{};
+      out.sao_type_idx = 1;
+    }
+  } else if (shared.sao_type_idx == 2) {
+    int64_t delta;
+    try_edge_offset_class(src, rec, cx, cy, cw, ch, bd, shared.eo_class, out, delta);
+    if (delta >= 0) {
+      out = h266_sao_ctb{};
+      out.sao_type_idx = 2;
+      out.eo_class = shared.eo_class;
+    }
+  }
+  return out;
+}
+
+// sao_decide_picture, src/sao_enc.rs:385-487
+static void sao_decide_picture(const h266_picture *src, const h266_picture *rec, uint32_t log2, uint32_t bd,
+                               bool luma_on, bool chroma_on, h266_sao_ctb_params *out) {
+  const size_t ctb = (size_t)1 << log2, pw = rec->luma.width, ph = rec->luma.height;
+  const size_t wc = (pw + ctb - 1) / ctb, hc = (ph + ctb - 1) / ctb;
+  for (size_t ry = 0; ry < hc; ++ry)
+    for (size_t rx = 0; rx < wc; ++rx) {
+      const size_t cx = rx * ctb, cy = ry * ctb, cw = std::min(ctb, pw - cx), ch = std::min(ctb, ph - cy);
+      h266_sao_ctb_params &p = out[ry * wc + rx];
+      p = h266_sao_ctb_params{};
+      if (luma_on) p.luma = sao_decide_ctb(src->luma, rec->luma, cx, cy, cw, ch, bd);
+      const size_t x2 = cx / 2, y2 = cy / 2, w2 = cw / 2, h2 = ch / 2;
+      if (chroma_on && w2 > 0 && h2 > 0) {
+        p.cb = sao_decide_ctb(src->cb, rec->cb, x2, y2, w2, h2, bd);
+        p.cr = sao_decide_ctb_constrained(src->cr, rec->cr, x2, y2, w2, h2, bd, p.cb);
+      }
+    }
+}
+
 // ctb_sse_y, src/alf_enc.rs:79-105: SSE over the CTB rectangle inside both planes.
 static uint64_t ctb_sse_y(const h266_plane &src, const h266_plane &rec, size_t x0, size_t y0, size_t w, size_t h) {
   uint64_t sse = 0;
@@ -1641,6 +1810,13 @@ void oracle_lmcs_add_chroma_residual(h266_picture *pic, uint32_t bd, const int32
 uint64_t oracle_output_convert(const h266_picture *pic, const h266_crop_window *c, uint32_t cfi, uint32_t bd,
                                uint8_t *out) {
   return oracle::output_convert(pic, *c, cfi, bd, out);
+}
+
+int oracle_sao_eo_category(int r, int n0, int n1) { return oracle::eo_category(r, n0, n1); }
+
+void oracle_sao_decide_picture(const h266_picture *src, const h266_picture *rec, uint32_t log2, uint32_t bd,
+                               int luma_on, int chroma_on, h266_sao_ctb_params *out) {
+  oracle::sao_decide_picture(src, rec, log2, bd, luma_on != 0, chroma_on != 0, out);
 }
 
 void oracle_alf_decide_and_apply(const h266_picture *src, h266_picture *rec, const h266_alf_aps_data *aps,

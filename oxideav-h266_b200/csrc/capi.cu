@@ -1197,6 +1197,58 @@ int h266_apply_alf_clipped(h266_ctx *ctx, h266_picture *pic, const h266_alf_pict
   return pass2_entry(ctx, pic, in);
 }
 
+int h266_sao_decide_picture(h266_ctx *ctx, const h266_picture *src, const h266_picture *rec, uint32_t log2,
+                            uint32_t bd, uint32_t sao_luma, uint32_t sao_chroma, h266_sao_ctb_params *out,
+                            uint64_t n_out) {
+  H266_TRY(check_ctx(ctx));
+  H266_TRY(check_picture(src));
+  H266_TRY(check_picture(rec));
+  if (!out) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL out");
+  if (bd < 8 || bd > 16) return set_error(H266_ERR_INVALID_ARGUMENT, "bit_depth must be 8..16");
+  if (log2 < 4 || log2 > 7) return set_error(H266_ERR_UNSUPPORTED, "CtbLog2SizeY must be 4..7");
+  const uint32_t ctb = 1u << log2;
+  const uint32_t wc = (rec->luma.width + ctb - 1) / ctb, hc = (rec->luma.height + ctb - 1) / ctb;
+  const uint64_t n = (uint64_t)wc * hc;
+  if (n_out != n) return set_error(H266_ERR_GRID_MISMATCH, "out size != CTB grid of rec");
+  if (n > (1u << 22)) return set_error(H266_ERR_UNSUPPORTED, "CTB grid too large");
+  Guard g(ctx->device);
+  Lane &ln = ctx->main;
+  DPlane R[3], S[3];
+  H266_TRY(picture_to_device(ln, *rec, R));
+  ctx->h2d_bytes += host_plane_bytes(*rec);
+  const h266_plane *sp[3] = {&src->luma, &src->cb, &src->cr};
+  for (int i = 0; i < 3; ++i) {  // the original: caller memory or a copy in the lane's scratch planes
+    const h266_plane &p = *sp[i];
+    if (src->mem == H266_MEM_DEVICE || (uint64_t)p.width * p.height == 0) {
+      S[i] = dplane(p, p.samples, (int64_t)std::max<uint64_t>(p.stride, 1));
+      continue;
+    }
+    const size_t row = (size_t)p.width * 2;
+    H266_TRY(ln.scratch[i].ensure(row * p.height));
+    H266_CUDA(cudaMemcpy2DAsync(ln.scratch[i].ptr, row, p.samples, (size_t)p.stride * 2, row, p.height,
+                                cudaMemcpyHostToDevice, ln.stream));
+    S[i] = dplane(p, ln.scratch[i].as<uint16_t>(), p.width);
+    ctx->h2d_bytes += row * p.height;
+  }
+  const size_t st_bytes = sao_stats_bytes((int)n), out_bytes = n * sizeof(h266_sao_ctb_params);
+  H266_TRY(ln.walk.ensure(st_bytes + out_bytes + 256));
+  uint8_t *w = ln.walk.as<uint8_t>();
+  auto *d_out = reinterpret_cast<h266_sao_ctb_params *>(w + st_bytes);
+  auto *d_err = reinterpret_cast<uint32_t *>(w + st_bytes + ((out_bytes + 15) & ~(size_t)15));
+  H266_CUDA(cudaMemsetAsync(d_err, 0, 4, ln.stream));
+  {
+    Prof pf(ctx, ln.stream, H266_PROF_SAO_ALF);
+    H266_TRY(launch_sao_decide(ln.stream, S, R, (int)bd, (int)log2, (int)wc, (int)hc, sao_luma != 0, sao_chroma != 0,
+                               w, d_err, d_out, &ctx->launches));
+  }
+  uint32_t err = 0;
+  H266_CUDA(cudaMemcpyAsync(out, d_out, out_bytes, cudaMemcpyDeviceToHost, ln.stream));
+  H266_TRY(sync_read(ln, &err, d_err, 4));
+  ctx->d2h_bytes += out_bytes;
+  if (err) return set_error(H266_ERR_INVALID_ARGUMENT, "SAO decision: a sample above (1 << bit_depth) - 1 has no band");
+  return H266_OK;
+}
+
 int h266_lmcs_forward_map_luma_rects(h266_ctx *ctx, h266_picture *pic, const h266_lmcs_derived *lmcs,
                                      const h266_rect *rects, uint64_t n) {
   H266_TRY(check_ctx(ctx));

@@ -301,6 +301,13 @@ int launch_chroma_residual(cudaStream_t st, DPlane cb, DPlane cr, const ResPiece
                            const int32_t *d_res, int bd, uint64_t *launches);
 int launch_output_dump(cudaStream_t st, const OutPlanes &o, uint8_t *d_dst, bool wide, uint64_t *launches);
 
+// Encoder SAO decision (sao_enc.cu): statistics per (CTB, component) into
+// d_stats (sao_stats_bytes), then the per-CTB decision into d_out.
+size_t sao_stats_bytes(int n_ctbs);
+int launch_sao_decide(cudaStream_t st, const DPlane src[3], const DPlane rec[3], int bd, int log2, int w_ctbs,
+                      int h_ctbs, bool luma_on, bool chroma_on, void *d_stats, uint32_t *d_err,
+                      h266_sao_ctb_params *d_out, uint64_t *launches);
+
 // Encoder luma ALF trials (packed form): `trials` filter-set slots of
 // a.tables.luma_packed evaluated on the pre-ALF luma a.src[0] against the
 // original `orig`; d_sse[ctb * cols + 0] += pre-ALF SSE, [.. + 1 + t] += SSE

@@ -37,7 +37,7 @@ EXPORTS = [
     "h266_apply_in_loop_filters_noalloc", "h266_server_create", "h266_server_submit", "h266_server_wait",
     "h266_server_stats", "h266_server_replay", "h266_server_destroy", "h266_alf_decide_and_apply_clipped",
     "h266_lmcs_forward_map_luma_rects", "h266_lmcs_chroma_var_scale", "h266_lmcs_add_chroma_residual",
-    "h266_output_convert",
+    "h266_output_convert", "h266_sao_decide_picture",
 ]
 PROF_FAMILIES = ("lmcs", "deblock", "sao_alf", "copy")
 
@@ -89,6 +89,7 @@ def lib():
         L.h266_lmcs_chroma_var_scale.argtypes = [vp, vp, vp, u32, u32, u32, vp, u64, vp]
         L.h266_lmcs_add_chroma_residual.argtypes = [vp, vp, u32, vp, u64, vp, u64]
         L.h266_output_convert.argtypes = [vp, vp, vp, u32, u32, vp, u64, u32, C.POINTER(u64)]
+        L.h266_sao_decide_picture.argtypes = [vp, vp, vp, u32, u32, u32, u32, vp, u64]
         _LIB = L
     return _LIB
 
@@ -415,3 +416,15 @@ def output_convert(ctx: Context, pic, crop, chroma_format_idc: int, bit_depth: i
     _check(lib().h266_output_convert(ctx._h, C.byref(cp), C.byref(cw), chroma_format_idc, bit_depth,
                                      out.ctypes.data, out.size, abi.MEM_HOST, C.byref(n)))
     return out[: n.value]
+
+
+def sao_decide_picture(ctx: Context, src, rec, *, ctb_log2: int, bit_depth: int, luma: bool = True,
+                       chroma: bool = True) -> np.ndarray:
+    """h266_sao_decide_picture: one abi.SAO_CTB_PARAMS record per CTB of rec's grid."""
+    ctb = 1 << ctb_log2
+    n = (-(-rec.luma.shape[1] // ctb)) * (-(-rec.luma.shape[0] // ctb))
+    out = np.zeros(n, dtype=abi.SAO_CTB_PARAMS)
+    s_c, r_c = src.to_ctypes(), rec.to_ctypes()
+    _check(lib().h266_sao_decide_picture(ctx._h, C.byref(s_c), C.byref(r_c), ctb_log2, bit_depth, int(luma),
+                                         int(chroma), out.ctypes.data, n))
+    return out

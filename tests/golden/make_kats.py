@@ -312,11 +312,17 @@ lmcs_maps = dict(
     chroma_scale_crs_0=[[5, 2048], [200, 1000, 255], [50, -1000, 0], [0, 300, 255]],
 )
 
+sao_enc = dict(
+    source="src/sao_enc.rs:808-840",
+    # eo_category(r, n0, n1) -> category
+    eo_category=[[10, 20, 30, 1], [50, 20, 10, 4], [50, 50, 50, 0], [10, 20, 10, 2], [10, 20, 5, 0]],
+)
+
 out = dict(
     reference="oxideav-h266 v0.0.8",
     note="Transcribed known-answer tests of the reference crate's filter path; expected values are the "
          "literals of the cited asserts.",
-    cases=cases, scalars=scalars, lmcs=lmcs, lmcs_maps=lmcs_maps)
+    cases=cases, scalars=scalars, lmcs=lmcs, lmcs_maps=lmcs_maps, sao_enc=sao_enc)
 path = pathlib.Path(__file__).with_name("kats.json")
 path.write_text(json.dumps(out, indent=1))
 print(f"wrote {path} ({len(cases)} picture cases, {len(lmcs)} LMCS cases)")
