@@ -290,6 +290,35 @@ int h266_derive_lmcs(const h266_lmcs_data *data, uint32_t bit_depth, h266_lmcs_d
 int h266_lmcs_inverse_map_luma(h266_ctx *ctx, h266_picture *pic, const h266_lmcs_derived *lmcs,
                                uint32_t lmcs_min_bin_idx, uint32_t lmcs_max_bin_idx);
 
+/* Encoder chroma ALF decision: chroma_alf_decide_and_apply_clipped
+ * (src/alf_enc.rs:628-821) for `component` 1 (Cb) or 2 (Cr).  One trial per
+ * alternative filter of `aps` (every CTB on with that filter); per CTB the
+ * option of lowest chroma SSE against `src` among {off, filter 0, ...} is kept
+ * (earlier options win ties), its samples are written into rec's component
+ * plane and apply_pic (the caller's AlfPicture records, n_apply = wc * hc,
+ * host memory) gets cb_on / cb_alt_idx (or cr_*) for the chosen CTBs; other
+ * records are left as they are.  No-op for chroma_format_idc 0 or an APS
+ * without chroma filters, as in the crate.  Supported: 4:2:0, BitDepth
+ * 8..14, coefficients in [-128, 127] (H266_ERR_UNSUPPORTED otherwise). */
+int h266_chroma_alf_decide_and_apply_clipped(h266_ctx *ctx, const h266_picture *src, h266_picture *rec,
+                                             h266_alf_ctb *apply_pic, uint64_t n_apply,
+                                             const h266_alf_aps_data *aps, uint32_t component,
+                                             uint32_t ctb_log2_size_y, uint32_t bit_depth,
+                                             uint32_t chroma_format_idc, const uint32_t *col_bd,
+                                             uint64_t n_col_bd, const uint32_t *row_bd, uint64_t n_row_bd);
+
+/* Encoder CC-ALF decision: cc_alf_decide_and_apply_clipped (src/alf_enc.rs:
+ * 935-1138).  As above with one trial per CC filter of `aps` for the
+ * component (idc = filter + 1), each reading `pre_luma_alf` (the luma before
+ * luma ALF, laid out as rec's luma plane, in rec->mem memory) and adding the
+ * correction into rec's chroma; apply_pic gets cc_cb_idc (or cc_cr_idc). */
+int h266_cc_alf_decide_and_apply_clipped(h266_ctx *ctx, const h266_picture *src, h266_picture *rec,
+                                         const uint16_t *pre_luma_alf, h266_alf_ctb *apply_pic, uint64_t n_apply,
+                                         const h266_alf_aps_data *aps, uint32_t component,
+                                         uint32_t ctb_log2_size_y, uint32_t bit_depth, uint32_t chroma_format_idc,
+                                         const uint32_t *col_bd, uint64_t n_col_bd, const uint32_t *row_bd,
+                                         uint64_t n_row_bd);
+
 /* Encoder SAO decision: sao_decide_picture (src/sao_enc.rs:385-487).  For
  * every CTB of rec's grid (luma size / CTB size rounded up), luma (when
  * sao_luma), Cb and Cr (when sao_chroma; Cr within Cb's type and class) get

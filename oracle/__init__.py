@@ -80,6 +80,8 @@ def lib():
         L.oracle_output_convert.restype = C.c_uint64
         L.oracle_sao_eo_category.argtypes = [C.c_int, C.c_int, C.c_int]
         L.oracle_sao_decide_picture.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_int, C.c_int, vp]
+        L.oracle_chroma_alf_decide.argtypes = [vp, vp, vp, vp, vp, C.c_int, C.c_int, C.c_uint32, C.c_uint32,
+                                               C.c_uint32, vp, C.c_uint64, vp, C.c_uint64]
         _LIB = L
     return _LIB
 
@@ -234,3 +236,16 @@ def sao_decide_picture(src, rec, *, ctb_log2: int, bit_depth: int, luma: bool = 
     lib().oracle_sao_decide_picture(C.byref(s_c), C.byref(r_c), ctb_log2, bit_depth, int(luma), int(chroma),
                                     out.ctypes.data)
     return out
+
+
+def chroma_alf_decide(src, rec, apply_pic, aps, *, component: int, cc: bool, ctb_log2: int, bit_depth: int,
+                      chroma_format_idc: int = 1, pre_luma=None, clip_cols=None, clip_rows=None) -> None:
+    """chroma_alf_decide_and_apply_clipped / cc_alf_decide_and_apply_clipped (src/alf_enc.rs:628-1138):
+    rec's component filtered in place, apply_pic (an ALF_CTB array of rec's CTB grid) updated."""
+    s_c, r_c = src.to_ctypes(), rec.to_ctypes()
+    pl = np.ascontiguousarray(pre_luma, dtype=np.uint16) if pre_luma is not None else None
+    c1, nc, k1 = _u32(clip_cols)
+    c2, nr, k2 = _u32(clip_rows)
+    lib().oracle_chroma_alf_decide(C.byref(s_c), C.byref(r_c), pl.ctypes.data if pl is not None else None,
+                                   apply_pic.ctypes.data, C.byref(aps), component, int(cc), ctb_log2, bit_depth,
+                                   chroma_format_idc, c1, nc, c2, nr)

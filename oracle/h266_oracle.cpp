@@ -1698,6 +1698,104 @@ static void alf_decide_and_apply(const h266_picture *src, h266_picture *rec, con
     }
 }
 
+// chroma_alf_decide_and_apply_clipped (src/alf_enc.rs:628-821) when cc is
+// false, cc_alf_decide_and_apply_clipped (src/alf_enc.rs:935-1138) when true:
+// per candidate (alt filter k, or CC filter k with idc k + 1) one apply_alf of
+// the whole picture with that candidate on every CTB for component `comp`
+// (1 = Cb, 2 = Cr), the CC trials on a copy whose luma is `pre_luma` (rec's
+// luma layout); per CTB the lowest chroma SSE among {off, candidates} wins
+// (strict <), its samples are copied into rec and `apply` records it.
+static void chroma_decide(const h266_picture *src, h266_picture *rec, const uint16_t *pre_luma, h266_alf_ctb *apply,
+                          const h266_alf_aps_data *aps, int comp, bool cc, uint32_t log2, uint32_t bd, uint32_t cfi,
+                          const uint32_t *cols, size_t n_cols, const uint32_t *rows, size_t n_rows) {
+  if (cfi == 0) return;
+  size_t n_cand;
+  if (!cc) {
+    if (!aps->alf_chroma_filter_signal_flag) return;
+    n_cand = aps->n_chroma_filters;
+  } else {
+    n_cand = comp == 1 ? aps->n_cc_cb_filters : aps->n_cc_cr_filters;
+  }
+  if (n_cand == 0) return;
+  const uint32_t ctb = 1u << log2;
+  const uint32_t wc = (rec->luma.width + ctb - 1) / ctb, hc = (rec->luma.height + ctb - 1) / ctb;
+  const size_t n = (size_t)wc * hc;
+  const uint32_t sw = cfi == 1 || cfi == 2 ? 2 : 1, sh = cfi == 1 ? 2 : 1;
+  const size_t cw = ctb / sw, chh = ctb / sh;
+  const h266_plane &sp = comp == 1 ? src->cb : src->cr;
+  h266_plane &rp = comp == 1 ? rec->cb : rec->cr;
+  std::vector<uint64_t> pre(n), per(n * n_cand);
+  for (uint32_t ry = 0; ry < hc; ++ry)
+    for (uint32_t rx = 0; rx < wc; ++rx)
+      pre[(size_t)ry * wc + rx] = ctb_sse_y(sp, rp, (size_t)rx * ctb / sw, (size_t)ry * ctb / sh, cw, chh);
+  h266_alf_aps_binding binding{};
+  if (!cc) binding.chroma_aps = aps;
+  else if (comp == 1) binding.cc_cb_aps = aps;
+  else binding.cc_cr_aps = aps;
+  h266_alf_config cfg{};
+  cfg.alf_enabled = 1;
+  cfg.cb_enabled = cfg.cc_cb_enabled = comp == 1;
+  cfg.cr_enabled = cfg.cc_cr_enabled = comp == 2;
+  cfg.bit_depth = bd;
+  cfg.ctb_log2_size_y = log2;
+  cfg.chroma_format_idc = cfi;
+  const size_t nl = (size_t)rec->luma.stride * rec->luma.height, nb = (size_t)rec->cb.stride * rec->cb.height,
+               nr = (size_t)rec->cr.stride * rec->cr.height;
+  std::vector<std::vector<uint16_t>> kept(n_cand);
+  std::vector<h266_alf_ctb> trial(n);
+  for (size_t k = 0; k < n_cand; ++k) {
+    std::vector<uint16_t> L(cc ? pre_luma : rec->luma.samples, (cc ? pre_luma : rec->luma.samples) + nl);
+    std::vector<uint16_t> B(rec->cb.samples, rec->cb.samples + nb), Rr(rec->cr.samples, rec->cr.samples + nr);
+    h266_picture t = *rec;
+    t.luma.samples = L.data();
+    t.cb.samples = B.data();
+    t.cr.samples = Rr.data();
+    for (size_t i = 0; i < n; ++i) {
+      trial[i] = h266_alf_ctb{};
+      if (!cc) {
+        if (comp == 1) trial[i].cb_on = 1, trial[i].cb_alt_idx = (uint8_t)k;
+        else trial[i].cr_on = 1, trial[i].cr_alt_idx = (uint8_t)k;
+      } else {
+        if (comp == 1) trial[i].cc_cb_idc = (uint8_t)(k + 1);
+        else trial[i].cc_cr_idc = (uint8_t)(k + 1);
+      }
+    }
+    h266_alf_picture ap{wc, hc, trial.data()};
+    apply_alf_clipped(&t, &ap, &cfg, &binding, cols, n_cols, rows, n_rows);
+    const h266_plane &tp = comp == 1 ? t.cb : t.cr;
+    for (uint32_t ry = 0; ry < hc; ++ry)
+      for (uint32_t rx = 0; rx < wc; ++rx)
+        per[((size_t)ry * wc + rx) * n_cand + k] =
+            ctb_sse_y(sp, tp, (size_t)rx * ctb / sw, (size_t)ry * ctb / sh, cw, chh);
+    kept[k] = comp == 1 ? std::move(B) : std::move(Rr);
+  }
+  for (uint32_t ry = 0; ry < hc; ++ry)
+    for (uint32_t rx = 0; rx < wc; ++rx) {
+      const size_t idx = (size_t)ry * wc + rx;
+      uint64_t best = pre[idx];
+      int pick = -1;
+      for (size_t k = 0; k < n_cand; ++k)
+        if (per[idx * n_cand + k] < best) {
+          best = per[idx * n_cand + k];
+          pick = (int)k;
+        }
+      if (pick < 0) continue;
+      const size_t x0 = (size_t)rx * ctb / sw, y0 = (size_t)ry * ctb / sh;
+      const size_t w = std::min<size_t>(cw, rp.width > x0 ? rp.width - x0 : 0);
+      const size_t h = std::min<size_t>(chh, rp.height > y0 ? rp.height - y0 : 0);
+      for (size_t y = 0; y < h; ++y)
+        std::memcpy(rp.samples + (y0 + y) * rp.stride + x0, kept[pick].data() + (y0 + y) * rp.stride + x0, w * 2);
+      h266_alf_ctb &e = apply[idx];
+      if (!cc) {
+        if (comp == 1) e.cb_on = 1, e.cb_alt_idx = (uint8_t)pick;
+        else e.cr_on = 1, e.cr_alt_idx = (uint8_t)pick;
+      } else {
+        if (comp == 1) e.cc_cb_idc = (uint8_t)(pick + 1);
+        else e.cc_cr_idc = (uint8_t)(pick + 1);
+      }
+    }
+}
+
 }  // namespace oracle
 
 // ---------------------------------------------------------------------------
@@ -1817,6 +1915,13 @@ int oracle_sao_eo_category(int r, int n0, int n1) { return oracle::eo_category(r
 void oracle_sao_decide_picture(const h266_picture *src, const h266_picture *rec, uint32_t log2, uint32_t bd,
                                int luma_on, int chroma_on, h266_sao_ctb_params *out) {
   oracle::sao_decide_picture(src, rec, log2, bd, luma_on != 0, chroma_on != 0, out);
+}
+
+void oracle_chroma_alf_decide(const h266_picture *src, h266_picture *rec, const uint16_t *pre_luma,
+                              h266_alf_ctb *apply, const h266_alf_aps_data *aps, int comp, int cc, uint32_t log2,
+                              uint32_t bd, uint32_t cfi, const uint32_t *cols, uint64_t n_cols, const uint32_t *rows,
+                              uint64_t n_rows) {
+  oracle::chroma_decide(src, rec, pre_luma, apply, aps, comp, cc != 0, log2, bd, cfi, cols, n_cols, rows, n_rows);
 }
 
 void oracle_alf_decide_and_apply(const h266_picture *src, h266_picture *rec, const h266_alf_aps_data *aps,

@@ -1197,6 +1197,169 @@ int h266_apply_alf_clipped(h266_ctx *ctx, h266_picture *pic, const h266_alf_pict
   return pass2_entry(ctx, pic, in);
 }
 
+// The chroma ALF (cc = false) and CC-ALF (cc = true) decisions: one chain
+// SAO/ALF pass per candidate into its own chroma plane (the other chroma
+// plane left out, luma written to a throw-away plane), per-CTB SSE, pick,
+// commit.
+static int chroma_trials(h266_ctx *ctx, const h266_picture *src, h266_picture *rec, const uint16_t *pre_luma,
+                         h266_alf_ctb *apply, uint64_t n_apply, const h266_alf_aps_data *aps, uint32_t comp, bool cc,
+                         uint32_t log2, uint32_t bd, uint32_t cfi, const uint32_t *col_bd, uint64_t n_col,
+                         const uint32_t *row_bd, uint64_t n_row) {
+  H266_TRY(check_ctx(ctx));
+  H266_TRY(check_picture(src));
+  H266_TRY(check_picture(rec));
+  if (!apply || !aps) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL apply_pic / aps");
+  if (comp != 1 && comp != 2) return set_error(H266_ERR_INVALID_ARGUMENT, "component must be 1 (Cb) or 2 (Cr)");
+  if (cc && !pre_luma) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL pre_luma_alf");
+  if (col_bd && !row_bd) return set_error(H266_ERR_INVALID_ARGUMENT, "row bounds NULL while col bounds are not");
+  if (cfi > 3) return set_error(H266_ERR_INVALID_ARGUMENT, "chroma_format_idc must be 0..3");
+  if (cfi == 0) return H266_OK;  // monochrome (src/alf_enc.rs:639-641, 946-948)
+  uint32_t n_cand;
+  if (!cc) {
+    if (!aps->alf_chroma_filter_signal_flag) return H266_OK;  // src/alf_enc.rs:642-648
+    n_cand = aps->n_chroma_filters;
+    if (n_cand > 8) return set_error(H266_ERR_INVALID_ARGUMENT, "chroma APS: more than 8 filters");
+  } else {
+    n_cand = comp == 1 ? aps->n_cc_cb_filters : aps->n_cc_cr_filters;  // src/alf_enc.rs:949-955
+    if (n_cand > 4) return set_error(H266_ERR_INVALID_ARGUMENT, "CC-ALF: more than 4 filters");
+  }
+  if (n_cand == 0) return H266_OK;
+  if (cfi != 1) return set_error(H266_ERR_UNSUPPORTED, "chroma ALF trials need 4:2:0");
+  if (bd < 8 || bd > 14) return set_error(H266_ERR_UNSUPPORTED, "chroma ALF trials need BitDepth 8..14");
+  if (log2 < 5 || log2 > 7) return set_error(H266_ERR_UNSUPPORTED, "chroma ALF trials need CtbLog2SizeY in 5..7");
+  const uint32_t ctb = 1u << log2;
+  const uint32_t wc = (rec->luma.width + ctb - 1) / ctb, hc = (rec->luma.height + ctb - 1) / ctb;
+  const int n = (int)((uint64_t)wc * hc);
+  if (n_apply != (uint64_t)n) return set_error(H266_ERR_GRID_MISMATCH, "apply_pic size != CTB grid of rec");
+  const h266_plane &rp = comp == 1 ? rec->cb : rec->cr, &sp = comp == 1 ? src->cb : src->cr;
+  if ((uint64_t)rp.width * rp.height == 0) return H266_OK;  // nothing to filter: every trial ties "off"
+  Guard g(ctx->device);
+  Lane &ln = ctx->main;
+  Prep &pr = ctx_prep(ctx, 0);
+  Pass2Host &h = pr.h;
+  DPlane R[3];
+  H266_TRY(picture_to_device(ln, *rec, R));
+  ctx->h2d_bytes += host_plane_bytes(*rec);
+  DPlane S{}, PL = R[0];
+  if (src->mem == H266_MEM_DEVICE || (uint64_t)sp.width * sp.height == 0) {
+    S = dplane(sp, sp.samples, (int64_t)std::max<uint64_t>(sp.stride, 1));
+  } else {
+    const size_t row = (size_t)sp.width * 2;
+    H266_TRY(ln.scratch[1].ensure(row * sp.height));
+    H266_CUDA(cudaMemcpy2DAsync(ln.scratch[1].ptr, row, sp.samples, (size_t)sp.stride * 2, row, sp.height,
+                                cudaMemcpyHostToDevice, ln.stream));
+    S = dplane(sp, ln.scratch[1].as<uint16_t>(), sp.width);
+    ctx->h2d_bytes += row * sp.height;
+  }
+  if (cc) {  // the trials' luma: the samples before luma ALF, rec's luma layout
+    if (rec->mem == H266_MEM_DEVICE) {
+      PL = dplane(rec->luma, const_cast<uint16_t *>(pre_luma), (int64_t)rec->luma.stride);
+    } else {
+      const size_t row = (size_t)rec->luma.width * 2;
+      H266_TRY(ln.scratch[0].ensure(row * rec->luma.height));
+      H266_CUDA(cudaMemcpy2DAsync(ln.scratch[0].ptr, row, pre_luma, (size_t)rec->luma.stride * 2, row,
+                                  rec->luma.height, cudaMemcpyHostToDevice, ln.stream));
+      PL = dplane(rec->luma, ln.scratch[0].as<uint16_t>(), rec->luma.width);
+      ctx->h2d_bytes += row * rec->luma.height;
+    }
+  }
+  // scratch: SSE table, picks, one chroma plane per candidate, a throw-away luma plane
+  const int cols = (int)n_cand + 1;
+  const size_t cw = rp.width, chh = rp.height, lw = rec->luma.width, lh = rec->luma.height;
+  const size_t sse_b = (size_t)n * cols * 8, pick_b = ((size_t)n + 255) & ~(size_t)255;
+  const size_t plane_b = ((cw * chh * 2) + 255) & ~(size_t)255, luma_b = lw * lh * 2;
+  H266_TRY(ln.walk.ensure(sse_b + pick_b + plane_b * n_cand + luma_b + 256));
+  uint8_t *w = ln.walk.as<uint8_t>();
+  auto *d_sse = reinterpret_cast<unsigned long long *>(w);
+  auto *d_pick = reinterpret_cast<int8_t *>(w + sse_b);
+  auto *d_trials = reinterpret_cast<uint16_t *>(w + sse_b + pick_b);
+  auto *d_luma = reinterpret_cast<uint16_t *>(w + sse_b + pick_b + plane_b * n_cand);
+  const int cwc = (int)(ctb / 2), chc = (int)(ctb / 2);
+  Prof pf(ctx, ln.stream, H266_PROF_SAO_ALF);
+  H266_TRY(launch_ctb_sse(ln.stream, S, R[comp], cwc, chc, (int)wc, n, d_sse, cols, 0, &ctx->launches));
+  std::vector<h266_alf_ctb> trial((size_t)n);
+  h266_alf_config cfg{1, comp == 1, comp == 2, comp == 1, comp == 2, bd, log2, cfi};
+  h266_alf_aps_binding binding{};
+  if (!cc) binding.chroma_aps = aps;
+  else if (comp == 1) binding.cc_cb_aps = aps;
+  else binding.cc_cr_aps = aps;
+  for (uint32_t k = 0; k < n_cand; ++k) {
+    for (h266_alf_ctb &c : trial) {
+      c = h266_alf_ctb{};
+      if (!cc) {
+        (comp == 1 ? c.cb_on : c.cr_on) = 1;
+        (comp == 1 ? c.cb_alt_idx : c.cr_alt_idx) = (uint8_t)k;
+      } else {
+        (comp == 1 ? c.cc_cb_idc : c.cc_cr_idc) = (uint8_t)(k + 1);
+      }
+    }
+    const h266_alf_picture ap{wc, hc, trial.data()};
+    Pass2Inputs in;
+    in.alf = &ap;
+    in.alf_cfg = &cfg;
+    in.binding = &binding;
+    in.cols = col_bd;
+    in.rows = row_bd;
+    in.n_cols = n_col;
+    in.n_rows = n_row;
+    H266_TRY(build_pass2(*rec, in, h));
+    if (!h.packed) return set_error(H266_ERR_UNSUPPORTED, "chroma ALF trials: coefficients outside [-128, 127]");
+    Staged st;
+    pr.blob.clear();
+    stage_pass2(h, pr.blob, st);
+    H266_TRY(upload_blob(ln, pr.blob, &st.base));
+    ctx->h2d_bytes += pr.blob.size();
+    const DPlane none{nullptr, 1, 0, 0};
+    DPlane SRC[3] = {cc ? PL : R[0], none, none}, DST[3] = {DPlane{d_luma, (int64_t)lw, (int)lw, (int)lh}, none, none};
+    SRC[comp] = R[comp];
+    DST[comp] = DPlane{d_trials + (size_t)k * (plane_b / 2), (int64_t)cw, (int)cw, (int)chh};
+    Pass2Args a = h.args;
+    bind_pass2(a, st.base, st, SRC, DST);
+    H266_TRY(launch_pass2_packed(ln.stream, a, false, true, &ctx->launches));
+    H266_TRY(launch_ctb_sse(ln.stream, S, DST[comp], cwc, chc, (int)wc, n, d_sse, cols, 1 + (int)k, &ctx->launches));
+  }
+  H266_TRY(launch_trial_pick_commit(ln.stream, d_sse, cols, n, d_pick, R[comp], d_trials, (int64_t)(plane_b / 2),
+                                    (int)cw, cwc, chc, (int)wc, &ctx->launches));
+  std::vector<int8_t> pick((size_t)n);
+  H266_CUDA(cudaMemcpyAsync(pick.data(), d_pick, (size_t)n, cudaMemcpyDeviceToHost, ln.stream));
+  h266_picture one = *rec;  // copy back only the decided plane
+  h266_plane *pl[3] = {&one.luma, &one.cb, &one.cr};
+  for (int i = 0; i < 3; ++i)
+    if (i != (int)comp) pl[i]->width = pl[i]->height = 0;
+  H266_TRY(picture_from_device(ln, one));
+  if (rec->mem == H266_MEM_DEVICE) H266_CUDA(cudaStreamSynchronize(ln.stream));
+  ctx->d2h_bytes += host_plane_bytes(one) + (size_t)n;
+  for (int i = 0; i < n; ++i) {
+    if (pick[i] < 0) continue;
+    h266_alf_ctb &e = apply[i];
+    if (!cc) {
+      (comp == 1 ? e.cb_on : e.cr_on) = 1;
+      (comp == 1 ? e.cb_alt_idx : e.cr_alt_idx) = (uint8_t)pick[i];
+    } else {
+      (comp == 1 ? e.cc_cb_idc : e.cc_cr_idc) = (uint8_t)(pick[i] + 1);
+    }
+  }
+  return H266_OK;
+}
+
+int h266_chroma_alf_decide_and_apply_clipped(h266_ctx *ctx, const h266_picture *src, h266_picture *rec,
+                                             h266_alf_ctb *apply_pic, uint64_t n_apply, const h266_alf_aps_data *aps,
+                                             uint32_t component, uint32_t log2, uint32_t bd, uint32_t cfi,
+                                             const uint32_t *col_bd, uint64_t n_col, const uint32_t *row_bd,
+                                             uint64_t n_row) {
+  return chroma_trials(ctx, src, rec, nullptr, apply_pic, n_apply, aps, component, false, log2, bd, cfi, col_bd, n_col,
+                       row_bd, n_row);
+}
+
+int h266_cc_alf_decide_and_apply_clipped(h266_ctx *ctx, const h266_picture *src, h266_picture *rec,
+                                         const uint16_t *pre_luma_alf, h266_alf_ctb *apply_pic, uint64_t n_apply,
+                                         const h266_alf_aps_data *aps, uint32_t component, uint32_t log2, uint32_t bd,
+                                         uint32_t cfi, const uint32_t *col_bd, uint64_t n_col, const uint32_t *row_bd,
+                                         uint64_t n_row) {
+  return chroma_trials(ctx, src, rec, pre_luma_alf, apply_pic, n_apply, aps, component, true, log2, bd, cfi, col_bd,
+                       n_col, row_bd, n_row);
+}
+
 int h266_sao_decide_picture(h266_ctx *ctx, const h266_picture *src, const h266_picture *rec, uint32_t log2,
                             uint32_t bd, uint32_t sao_luma, uint32_t sao_chroma, h266_sao_ctb_params *out,
                             uint64_t n_out) {

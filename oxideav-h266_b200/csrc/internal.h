@@ -301,6 +301,15 @@ int launch_chroma_residual(cudaStream_t st, DPlane cb, DPlane cr, const ResPiece
                            const int32_t *d_res, int bd, uint64_t *launches);
 int launch_output_dump(cudaStream_t st, const OutPlanes &o, uint8_t *d_dst, bool wide, uint64_t *launches);
 
+// Encoder chroma ALF / CC-ALF trials (alf_enc.cu): per-CTB chroma SSE of a
+// against b into d_sse[ctb * cols + col]; then the first-minimum pick per CTB
+// and the copy of the chosen trial plane's CTB region into dst.
+int launch_ctb_sse(cudaStream_t st, DPlane a, DPlane b, int cw, int ch, int w_ctbs, int n, unsigned long long *d_sse,
+                   int cols, int col, uint64_t *launches);
+int launch_trial_pick_commit(cudaStream_t st, const unsigned long long *d_sse, int cols, int n, int8_t *d_pick,
+                             DPlane dst, const uint16_t *d_trials, int64_t trial_samples, int trial_pitch, int cw,
+                             int ch, int w_ctbs, uint64_t *launches);
+
 // Encoder SAO decision (sao_enc.cu): statistics per (CTB, component) into
 // d_stats (sao_stats_bytes), then the per-CTB decision into d_out.
 size_t sao_stats_bytes(int n_ctbs);

@@ -37,7 +37,8 @@ EXPORTS = [
     "h266_apply_in_loop_filters_noalloc", "h266_server_create", "h266_server_submit", "h266_server_wait",
     "h266_server_stats", "h266_server_replay", "h266_server_destroy", "h266_alf_decide_and_apply_clipped",
     "h266_lmcs_forward_map_luma_rects", "h266_lmcs_chroma_var_scale", "h266_lmcs_add_chroma_residual",
-    "h266_output_convert", "h266_sao_decide_picture",
+    "h266_output_convert", "h266_sao_decide_picture", "h266_chroma_alf_decide_and_apply_clipped",
+    "h266_cc_alf_decide_and_apply_clipped",
 ]
 PROF_FAMILIES = ("lmcs", "deblock", "sao_alf", "copy")
 
@@ -90,6 +91,10 @@ def lib():
         L.h266_lmcs_add_chroma_residual.argtypes = [vp, vp, u32, vp, u64, vp, u64]
         L.h266_output_convert.argtypes = [vp, vp, vp, u32, u32, vp, u64, u32, C.POINTER(u64)]
         L.h266_sao_decide_picture.argtypes = [vp, vp, vp, u32, u32, u32, u32, vp, u64]
+        L.h266_chroma_alf_decide_and_apply_clipped.argtypes = [vp, vp, vp, vp, u64, vp, u32, u32, u32, u32, vp, u64,
+                                                               vp, u64]
+        L.h266_cc_alf_decide_and_apply_clipped.argtypes = [vp, vp, vp, vp, vp, u64, vp, u32, u32, u32, u32, vp, u64,
+                                                           vp, u64]
         _LIB = L
     return _LIB
 
@@ -428,3 +433,22 @@ def sao_decide_picture(ctx: Context, src, rec, *, ctb_log2: int, bit_depth: int,
     _check(lib().h266_sao_decide_picture(ctx._h, C.byref(s_c), C.byref(r_c), ctb_log2, bit_depth, int(luma),
                                          int(chroma), out.ctypes.data, n))
     return out
+
+
+def chroma_alf_decide(ctx: Context, src, rec, apply_pic, aps, *, component: int, cc: bool, ctb_log2: int,
+                      bit_depth: int, chroma_format_idc: int = 1, pre_luma=None, clip_cols=None, clip_rows=None):
+    """h266_chroma_alf_decide_and_apply_clipped (cc False) / h266_cc_alf_decide_and_apply_clipped (cc True):
+    rec's component filtered in place, apply_pic (an abi.ALF_CTB array of rec's CTB grid) updated.
+    pre_luma: rec's luma before luma ALF (numpy for host pictures, a CUDA tensor for device ones)."""
+    s_c, r_c = src.to_ctypes(), rec.to_ctypes()
+    c1, nc, k1 = _u32(clip_cols)
+    c2, nr, k2 = _u32(clip_rows)
+    if cc:
+        pl = pre_luma if hasattr(pre_luma, "data_ptr") else np.ascontiguousarray(pre_luma, dtype=np.uint16)
+        _check(lib().h266_cc_alf_decide_and_apply_clipped(
+            ctx._h, C.byref(s_c), C.byref(r_c), _ptr(pl), apply_pic.ctypes.data, len(apply_pic), C.byref(aps),
+            component, ctb_log2, bit_depth, chroma_format_idc, c1, nc, c2, nr))
+    else:
+        _check(lib().h266_chroma_alf_decide_and_apply_clipped(
+            ctx._h, C.byref(s_c), C.byref(r_c), apply_pic.ctypes.data, len(apply_pic), C.byref(aps), component,
+            ctb_log2, bit_depth, chroma_format_idc, c1, nc, c2, nr))
