@@ -385,6 +385,37 @@ def run_encoder_trials(ctx, local_rank, stream, steps: int, n_pics: int = 4):
            "path": "h266_sao_decide_picture on H266_MEM_DEVICE pictures (statistics, decision, records copied back)",
            "cpu_oracle": {"ms_per_picture": round(sao_cpu_ms, 1), "cores": 1, "kind": "port",
                           "sample": "one picture"}}
+    # chroma ALF / CC-ALF decisions (src/alf_enc.rs:628-1138), Cb, the picture's APS
+    chroma = {}
+    for cc in (False, True):
+        d = devs[0]
+        n_ctb = 15 * 9
+        for _ in range(3):
+            restore(d)
+            native.chroma_alf_decide(ctx, d[0], d[2], np.zeros(n_ctb, dtype=abi.ALF_CTB), d[3], component=1, cc=cc,
+                                     ctb_log2=7, bit_depth=10, pre_luma=d[1].luma if cc else None)
+        torch.cuda.synchronize()
+        c_total, c_calls = 0.0, 0
+        for _ in range(max(1, steps)):
+            restore(d)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            native.chroma_alf_decide(ctx, d[0], d[2], np.zeros(n_ctb, dtype=abi.ALF_CTB), d[3], component=1, cc=cc,
+                                     ctb_log2=7, bit_depth=10, pre_luma=d[1].luma if cc else None)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            c_total += e0.elapsed_time(e1)
+            c_calls += 1
+        r3 = r_.copy()
+        t0 = time.perf_counter()
+        oracle.chroma_alf_decide(s_, r3, np.zeros(n_ctb, dtype=abi.ALF_CTB), a, component=1, cc=cc, ctb_log2=7,
+                                 bit_depth=10, pre_luma=r_.luma if cc else None)
+        c_cpu = (time.perf_counter() - t0) * 1e3
+        n_cand = (a.n_cc_cb_filters if cc else a.n_chroma_filters)
+        chroma["cc_alf_cb" if cc else "chroma_alf_cb"] = {
+            "candidates": int(n_cand), "ms_per_picture": round(c_total / c_calls, 4),
+            "cpu_oracle_ms_per_picture": round(c_cpu, 1)}
+    sao["chroma_trials"] = chroma
     del devs
     torch.cuda.synchronize()
     return {"workload": "encoder luma ALF decision, 1920x1080 10-bit CTU 128, 16 fixed sets + 1 APS set",
