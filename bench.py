@@ -68,6 +68,12 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0}, "fallback"
 
 
+def torch_sync():
+    import torch
+
+    torch.cuda.synchronize()
+
+
 class ClockSampler:
     """nvidia-smi clock / throttle sampling during the timed region."""
 
@@ -85,7 +91,7 @@ class ClockSampler:
             self.path.parent.mkdir(exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                          "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -100,11 +106,29 @@ class ClockSampler:
                 self.proc.kill()
             self.f.close()
 
+    def _lines(self):
+        try:
+            return self.path.read_text().splitlines()
+        except Exception:
+            return []
+
+    def prime(self, step, max_steps: int):
+        """Runs untimed steps until the sampler has written its first line
+        (nvidia-smi starts slowly), so the timed region is sampled under load;
+        returns the line count at that point (samples before it are dropped)."""
+        for _ in range(max_steps if self.proc else 0):
+            if len(self._lines()) >= 1:
+                break
+            step()
+            torch_sync()
+        self.skip = len(self._lines())
+        return self.skip
+
     def summary(self):
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         rows = []
-        lines = self.path.read_text().splitlines()
+        lines = self._lines()[getattr(self, "skip", 0):]
         uuids = {l.split(",")[0].strip() for l in lines if l.count(",") >= 8}
         mine = self.gpu_id if self.gpu_id in uuids else (sorted(uuids)[0] if len(uuids) == 1 else None)
         for line in lines:
@@ -548,11 +572,12 @@ def run_ours(args, rank, world, local_rank):
         step()
     torch.cuda.synchronize()
     for attempt in range(2):
-        barrier()
-        torch.cuda.synchronize()
-        l0 = ctx.kernel_launches
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with ClockSampler(gpu_id) as cs:
+            cs.prime(step, 400)  # untimed steps until the clock sampler runs (no collectives inside a step)
+            barrier()
+            torch.cuda.synchronize()
+            l0 = ctx.kernel_launches
             start.record(stream)
             for _ in range(args.steps):
                 step()
@@ -713,7 +738,7 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
