@@ -331,6 +331,20 @@ int h266_sao_decide_picture(h266_ctx *ctx, const h266_picture *src, const h266_p
                             uint32_t ctb_log2_size_y, uint32_t bit_depth, uint32_t sao_luma, uint32_t sao_chroma,
                             h266_sao_ctb_params *out, uint64_t n_out);
 
+/* Encoder chroma SAO merge: apply_chroma_sao_merge (src/sao_enc.rs:500-668).
+ * In raster order every CTB of the independent SaoPicture (w_ctbs x
+ * h_ctbs, raster records) keeps its own Cb/Cr parameters or takes those of
+ * the already merged left / above CTB, whichever costs least (Cb + Cr SSE of
+ * SAO on rec_pre_sao against src, plus 8 x the crate's bit estimate; earlier
+ * options win ties).  merged: the resulting records (luma as given); map:
+ * 0 independent, 1 merge left, 2 merge above.  Both outputs in host memory.
+ * rec_pre_sao's Cb and Cr planes must have the same size and src's chroma
+ * planes at least that size (the crate indexes them alike). */
+int h266_sao_chroma_merge(h266_ctx *ctx, const h266_picture *src, const h266_picture *rec_pre_sao,
+                          const h266_sao_ctb_params *independent, uint32_t w_ctbs, uint32_t h_ctbs,
+                          uint32_t bit_depth, uint32_t ctb_log2_size_y, h266_sao_ctb_params *merged,
+                          uint8_t *merge_map);
+
 /* ---- recon-side LMCS (src/lmcs.rs:169-290, src/ctu.rs:734-742, 1701-1815) */
 typedef struct h266_rect {
     uint32_t x, y, w, h;

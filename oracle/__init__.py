@@ -80,6 +80,7 @@ def lib():
         L.oracle_output_convert.restype = C.c_uint64
         L.oracle_sao_eo_category.argtypes = [C.c_int, C.c_int, C.c_int]
         L.oracle_sao_decide_picture.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_int, C.c_int, vp]
+        L.oracle_sao_chroma_merge.argtypes = [vp, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp]
         L.oracle_chroma_alf_decide.argtypes = [vp, vp, vp, vp, vp, C.c_int, C.c_int, C.c_uint32, C.c_uint32,
                                                C.c_uint32, vp, C.c_uint64, vp, C.c_uint64]
         _LIB = L
@@ -249,3 +250,14 @@ def chroma_alf_decide(src, rec, apply_pic, aps, *, component: int, cc: bool, ctb
     lib().oracle_chroma_alf_decide(C.byref(s_c), C.byref(r_c), pl.ctypes.data if pl is not None else None,
                                    apply_pic.ctypes.data, C.byref(aps), component, int(cc), ctb_log2, bit_depth,
                                    chroma_format_idc, c1, nc, c2, nr)
+
+
+def sao_chroma_merge(src, pre, indep, w_ctbs: int, h_ctbs: int, *, bit_depth: int, ctb_log2: int):
+    """apply_chroma_sao_merge (src/sao_enc.rs:500-668): (merged SaoCtbParams array, merge map u8 array)."""
+    s_c, p_c = src.to_ctypes(), pre.to_ctypes()
+    ind = np.ascontiguousarray(indep)
+    merged = np.zeros_like(ind)
+    m = np.zeros(len(ind), dtype=np.uint8)
+    lib().oracle_sao_chroma_merge(C.byref(s_c), C.byref(p_c), ind.ctypes.data, w_ctbs, h_ctbs, bit_depth, ctb_log2,
+                                  merged.ctypes.data, m.ctypes.data)
+    return merged, m

@@ -1698,6 +1698,77 @@ static void alf_decide_and_apply(const h266_picture *src, h266_picture *rec, con
     }
 }
 
+// chroma_independent_bit_cost, src/sao_enc.rs:670-696
+static int64_t sao_chroma_bits(const h266_sao_ctb_params &p) {
+  int64_t bits = 1;
+  for (const h266_sao_ctb *c : {&p.cb, &p.cr}) bits += c->sao_type_idx == 0 ? 1 : (c->sao_type_idx == 1 ? 16 : 10);
+  return bits;
+}
+
+// chroma_ctb_sse_with, src/sao_enc.rs:698-749: SAO of one CTB with the given
+// chroma parameters on a copy of the pre-SAO picture, Cb + Cr SSE over the
+// CTB's chroma region (Cb's extent for both planes, as there).
+static uint64_t chroma_ctb_sse_with(const h266_picture *src, const h266_picture *pre, uint32_t rx, uint32_t ry,
+                                    size_t chr_ctb, uint32_t bd, const h266_sao_ctb &cb, const h266_sao_ctb &cr) {
+  std::vector<uint16_t> L = clone_plane(pre->luma), B = clone_plane(pre->cb), Cr = clone_plane(pre->cr);
+  h266_picture tmp = *pre;
+  tmp.luma.samples = L.data();
+  tmp.cb.samples = B.data();
+  tmp.cr.samples = Cr.data();
+  std::vector<h266_sao_ctb_params> one((size_t)(rx + 1) * (ry + 1));
+  one[(size_t)ry * (rx + 1) + rx].cb = cb;
+  one[(size_t)ry * (rx + 1) + rx].cr = cr;
+  const h266_sao_picture sp{rx + 1, ry + 1, one.data()};
+  uint32_t log2 = 0;
+  while (((size_t)1 << log2) < chr_ctb * 2) ++log2;
+  const h266_sao_config cfg{0, 1, bd, log2, 1};
+  apply_sao_clipped(&tmp, &sp, &cfg, nullptr, 0, nullptr, 0);
+  const size_t cx = (size_t)rx * chr_ctb, cy = (size_t)ry * chr_ctb;
+  const size_t cw = std::min(chr_ctb, tmp.cb.width > cx ? tmp.cb.width - cx : 0);
+  const size_t ch = std::min(chr_ctb, tmp.cb.height > cy ? tmp.cb.height - cy : 0);
+  uint64_t sse = 0;
+  for (size_t y = 0; y < ch; ++y)
+    for (size_t x = 0; x < cw; ++x) {
+      const int64_t dcb = (int64_t)src->cb.samples[(cy + y) * src->cb.stride + cx + x] -
+                          (int64_t)tmp.cb.samples[(cy + y) * tmp.cb.stride + cx + x];
+      const int64_t dcr = (int64_t)src->cr.samples[(cy + y) * src->cr.stride + cx + x] -
+                          (int64_t)tmp.cr.samples[(cy + y) * tmp.cr.stride + cx + x];
+      sse += (uint64_t)(dcb * dcb + dcr * dcr);
+    }
+  return sse;
+}
+
+// apply_chroma_sao_merge, src/sao_enc.rs:500-668: raster order; per CTB the
+// lowest cost (SSE + 8 * bits) among independent, merge-left (1 bit) and
+// merge-above (2 bits), strict < in that order; map: 0 independent, 1 left,
+// 2 above.
+static void sao_chroma_merge(const h266_picture *src, const h266_picture *pre, const h266_sao_ctb_params *indep,
+                             uint32_t pw, uint32_t ph, uint32_t bd, uint32_t log2, h266_sao_ctb_params *merged,
+                             uint8_t *map) {
+  const size_t chr = ((size_t)1 << log2) / 2;
+  for (size_t i = 0; i < (size_t)pw * ph; ++i) merged[i] = indep[i];
+  for (uint32_t ry = 0; ry < ph; ++ry)
+    for (uint32_t rx = 0; rx < pw; ++rx) {
+      const h266_sao_ctb_params in = merged[(size_t)ry * pw + rx];
+      int64_t best = (int64_t)chroma_ctb_sse_with(src, pre, rx, ry, chr, bd, in.cb, in.cr) + 8 * sao_chroma_bits(in);
+      uint8_t choice = 0;
+      h266_sao_ctb bcb = in.cb, bcr = in.cr;
+      if (rx > 0) {
+        const h266_sao_ctb_params &l = merged[(size_t)ry * pw + rx - 1];
+        const int64_t c = (int64_t)chroma_ctb_sse_with(src, pre, rx, ry, chr, bd, l.cb, l.cr) + 8 * 1;
+        if (c < best) best = c, choice = 1, bcb = l.cb, bcr = l.cr;
+      }
+      if (ry > 0) {
+        const h266_sao_ctb_params &u = merged[(size_t)(ry - 1) * pw + rx];
+        const int64_t c = (int64_t)chroma_ctb_sse_with(src, pre, rx, ry, chr, bd, u.cb, u.cr) + 8 * 2;
+        if (c < best) best = c, choice = 2, bcb = u.cb, bcr = u.cr;
+      }
+      map[(size_t)ry * pw + rx] = choice;
+      merged[(size_t)ry * pw + rx].cb = bcb;
+      merged[(size_t)ry * pw + rx].cr = bcr;
+    }
+}
+
 // chroma_alf_decide_and_apply_clipped (src/alf_enc.rs:628-821) when cc is
 // false, cc_alf_decide_and_apply_clipped (src/alf_enc.rs:935-1138) when true:
 // per candidate (alt filter k, or CC filter k with idc k + 1) one apply_alf of
@@ -1915,6 +1986,12 @@ int oracle_sao_eo_category(int r, int n0, int n1) { return oracle::eo_category(r
 void oracle_sao_decide_picture(const h266_picture *src, const h266_picture *rec, uint32_t log2, uint32_t bd,
                                int luma_on, int chroma_on, h266_sao_ctb_params *out) {
   oracle::sao_decide_picture(src, rec, log2, bd, luma_on != 0, chroma_on != 0, out);
+}
+
+void oracle_sao_chroma_merge(const h266_picture *src, const h266_picture *pre, const h266_sao_ctb_params *indep,
+                             uint32_t pw, uint32_t ph, uint32_t bd, uint32_t log2, h266_sao_ctb_params *merged,
+                             uint8_t *map) {
+  oracle::sao_chroma_merge(src, pre, indep, pw, ph, bd, log2, merged, map);
 }
 
 void oracle_chroma_alf_decide(const h266_picture *src, h266_picture *rec, const uint16_t *pre_luma,

@@ -1360,6 +1360,68 @@ int h266_cc_alf_decide_and_apply_clipped(h266_ctx *ctx, const h266_picture *src,
                        n_col, row_bd, n_row);
 }
 
+int h266_sao_chroma_merge(h266_ctx *ctx, const h266_picture *src, const h266_picture *pre,
+                          const h266_sao_ctb_params *indep, uint32_t wc, uint32_t hc, uint32_t bd, uint32_t log2,
+                          h266_sao_ctb_params *merged, uint8_t *map) {
+  H266_TRY(check_ctx(ctx));
+  H266_TRY(check_picture(src));
+  H266_TRY(check_picture(pre));
+  const uint64_t n = (uint64_t)wc * hc;
+  if (n && (!indep || !merged || !map)) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL records / map");
+  if (bd < 8 || bd > 16) return set_error(H266_ERR_INVALID_ARGUMENT, "bit_depth must be 8..16");
+  if (log2 < 1 || log2 > 7) return set_error(H266_ERR_INVALID_ARGUMENT, "ctb_log2_size_y must be 1..7");
+  if (n > (1u << 22)) return set_error(H266_ERR_UNSUPPORTED, "CTB grid too large");
+  if (pre->cb.width != pre->cr.width || pre->cb.height != pre->cr.height)
+    return set_error(H266_ERR_INVALID_ARGUMENT, "Cb and Cr planes differ in size");
+  if (src->cb.width < pre->cb.width || src->cb.height < pre->cb.height || src->cr.width < pre->cb.width ||
+      src->cr.height < pre->cb.height)
+    return set_error(H266_ERR_INVALID_ARGUMENT, "original chroma planes smaller than the reconstruction's");
+  if (!n) return H266_OK;
+  Guard g(ctx->device);
+  Lane &ln = ctx->main;
+  h266_picture cv = *pre;  // chroma only
+  cv.luma.width = cv.luma.height = 0;
+  DPlane P[3];
+  H266_TRY(picture_to_device(ln, cv, P));
+  ctx->h2d_bytes += host_plane_bytes(cv);
+  const h266_plane *sp[2] = {&src->cb, &src->cr};
+  DPlane S[2], Q[2] = {P[1], P[2]};
+  for (int i = 0; i < 2; ++i) {
+    const h266_plane &p = *sp[i];
+    if (src->mem == H266_MEM_DEVICE || (uint64_t)p.width * p.height == 0) {
+      S[i] = dplane(p, p.samples, (int64_t)std::max<uint64_t>(p.stride, 1));
+      continue;
+    }
+    const size_t row = (size_t)p.width * 2;
+    H266_TRY(ln.scratch[1 + i].ensure(row * p.height));
+    H266_CUDA(cudaMemcpy2DAsync(ln.scratch[1 + i].ptr, row, p.samples, (size_t)p.stride * 2, row, p.height,
+                                cudaMemcpyHostToDevice, ln.stream));
+    S[i] = dplane(p, ln.scratch[1 + i].as<uint16_t>(), p.width);
+    ctx->h2d_bytes += row * p.height;
+  }
+  Prep &pr = ctx_prep(ctx, 0);
+  pr.blob.clear();
+  Blob blob{pr.blob};
+  const size_t off = blob.put(indep, n * sizeof(h266_sao_ctb_params));
+  uint8_t *base = nullptr;
+  H266_TRY(upload_blob(ln, pr.blob, &base));
+  ctx->h2d_bytes += pr.blob.size();
+  const size_t rec_b = n * sizeof(h266_sao_ctb_params);
+  H266_TRY(ln.walk.ensure(rec_b + n + 256));
+  auto *d_merged = ln.walk.as<h266_sao_ctb_params>();
+  auto *d_map = ln.walk.as<uint8_t>() + rec_b;
+  {
+    Prof pf(ctx, ln.stream, H266_PROF_SAO_ALF);
+    H266_TRY(launch_sao_chroma_merge(ln.stream, S, Q, (int)bd, (1 << log2) / 2, (int)wc, (int)hc,
+                                     reinterpret_cast<const h266_sao_ctb_params *>(base + off), d_merged, d_map,
+                                     &ctx->launches));
+  }
+  H266_CUDA(cudaMemcpyAsync(merged, d_merged, rec_b, cudaMemcpyDeviceToHost, ln.stream));
+  H266_TRY(sync_read(ln, map, d_map, n));
+  ctx->d2h_bytes += rec_b + n;
+  return H266_OK;
+}
+
 int h266_sao_decide_picture(h266_ctx *ctx, const h266_picture *src, const h266_picture *rec, uint32_t log2,
                             uint32_t bd, uint32_t sao_luma, uint32_t sao_chroma, h266_sao_ctb_params *out,
                             uint64_t n_out) {

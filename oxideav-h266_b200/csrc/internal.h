@@ -313,6 +313,11 @@ int launch_trial_pick_commit(cudaStream_t st, const unsigned long long *d_sse, i
 // Encoder SAO decision (sao_enc.cu): statistics per (CTB, component) into
 // d_stats (sao_stats_bytes), then the per-CTB decision into d_out.
 size_t sao_stats_bytes(int n_ctbs);
+// Chroma SAO merge (sao_enc.cu): one launch per CTB anti-diagonal; d_merged
+// is written CTB by CTB (each launch reads the previous diagonal's records).
+int launch_sao_chroma_merge(cudaStream_t st, const DPlane src[2], const DPlane pre[2], int bd, int chr_ctb,
+                            int w_ctbs, int h_ctbs, const h266_sao_ctb_params *d_indep, h266_sao_ctb_params *d_merged,
+                            uint8_t *d_map, uint64_t *launches);
 int launch_sao_decide(cudaStream_t st, const DPlane src[3], const DPlane rec[3], int bd, int log2, int w_ctbs,
                       int h_ctbs, bool luma_on, bool chroma_on, void *d_stats, uint32_t *d_err,
                       h266_sao_ctb_params *d_out, uint64_t *launches);

@@ -292,7 +292,130 @@ __global__ void k_sao_decide(const __grid_constant__ SaoEncArgs a, const SaoStat
   if (lane == 0) out[i] = p;
 }
 
+// ---- chroma SAO merge (apply_chroma_sao_merge, src/sao_enc.rs:500-668)
+//
+// Raster-order dependency: a CTB weighs its own parameters against the
+// already merged left and above CTBs, so CTBs run one anti-diagonal per
+// launch (both neighbours lie on the previous diagonal).  One CTA per CTB:
+// for each candidate the SAO of this CTB alone on the pre-SAO planes
+// (apply_sao_ctb, src/sao.rs:504-626, no clip rectangle) and the Cb + Cr SSE
+// against the original (chroma_ctb_sse_with, src/sao_enc.rs:698-749), then
+// the decision by cost SSE + 8 * bits (strict <: independent, left, above).
+struct MergeArgs {
+  DPlane src[2], pre[2];  // Cb, Cr
+  int bd, chr_ctb, w_ctbs, diag, first_ry;
+  const h266_sao_ctb_params *indep;
+  h266_sao_ctb_params *merged;
+  uint8_t *map;
+};
+
+__device__ __forceinline__ int sao_value(const DPlane &P, int x, int y, const h266_sao_ctb &p, int maxv, int bd) {
+  const int v = P.s[(int64_t)y * P.stride + x];
+  if (p.sao_type_idx == 2) {
+    const int c = p.eo_class & 3;
+    const int hx = c == 1 ? 0 : (c == 3 ? 1 : -1), vy = c == 0 ? 0 : -1;  // hPos / vPos of neighbour 0
+    const int ax = x + hx, ay = y + vy, bx = x - hx, by = y - vy;
+    if (ax < 0 || ay < 0 || bx < 0 || by < 0 || ax >= P.w || ay >= P.h || bx >= P.w || by >= P.h)
+      return min(max(v, 0), maxv);
+    const int n0 = P.s[(int64_t)ay * P.stride + ax], n1 = P.s[(int64_t)by * P.stride + bx];
+    int e = 2 + ((v > n0) - (v < n0)) + ((v > n1) - (v < n1));
+    if (e <= 2) e = e == 2 ? 0 : e + 1;
+    const int off = (e >= 1 && e <= 4) ? p.offset_val[e] : 0;
+    return min(max(v + off, 0), maxv);
+  }
+  if (p.sao_type_idx == 1) {
+    const int band = (v >> (bd - 5)) & 31;
+    const int k = (band - p.band_position) & 31;
+    const int off = k < 4 ? p.offset_val[k + 1] : 0;
+    return min(max(v + off, 0), maxv);
+  }
+  return v;  // not applied: the sample as it is
+}
+
+__global__ void __launch_bounds__(kStatThreads) k_sao_merge_diag(const __grid_constant__ MergeArgs a) {
+  const int ry = a.first_ry + blockIdx.x, rx = a.diag - ry;
+  const int i = ry * a.w_ctbs + rx;
+  const int tid = threadIdx.x, maxv = (1 << a.bd) - 1;
+  const int cx = rx * a.chr_ctb, cy = ry * a.chr_ctb;
+  const int cw = max(0, min(a.chr_ctb, a.pre[0].w - cx)), ch = max(0, min(a.chr_ctb, a.pre[0].h - cy));
+  __shared__ unsigned long long part[kStatThreads / 32];
+  __shared__ unsigned long long sse[3];
+  const h266_sao_ctb_params in = a.indep[i];
+  const h266_sao_ctb_params *cand[3] = {&in, rx > 0 ? &a.merged[i - 1] : nullptr,
+                                        ry > 0 ? &a.merged[i - a.w_ctbs] : nullptr};
+  for (int k = 0; k < 3; ++k) {
+    if (!cand[k]) continue;  // uniform per CTA
+    const h266_sao_ctb pc[2] = {cand[k]->cb, cand[k]->cr};
+    unsigned long long e = 0;
+    for (int y = cy + tid / 32; y < cy + ch; y += kStatThreads / 32)
+      for (int x = cx + (tid & 31); x < cx + cw; x += 32)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const int d = (int)a.src[c].s[(int64_t)y * a.src[c].stride + x] - sao_value(a.pre[c], x, y, pc[c], maxv, a.bd);
+          e += (unsigned long long)(d * d);
+        }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
+    if ((tid & 31) == 0) part[tid / 32] = e;
+    __syncthreads();
+    if (tid == 0) {
+      unsigned long long t = 0;
+      for (int w = 0; w < kStatThreads / 32; ++w) t += part[w];
+      sse[k] = t;
+    }
+    __syncthreads();
+  }
+  if (tid) return;
+  auto bits = [](const h266_sao_ctb_params &p) {  // chroma_independent_bit_cost, src/sao_enc.rs:670-696
+    long long b = 1;
+    b += p.cb.sao_type_idx == 0 ? 1 : (p.cb.sao_type_idx == 1 ? 16 : 10);
+    b += p.cr.sao_type_idx == 0 ? 1 : (p.cr.sao_type_idx == 1 ? 16 : 10);
+    return b;
+  };
+  long long best = (long long)sse[0] + 8 * bits(in);
+  int choice = 0;
+  h266_sao_ctb_params out = in;
+  if (cand[1] && (long long)sse[1] + 8 < best) {
+    best = (long long)sse[1] + 8;
+    choice = 1;
+    out.cb = cand[1]->cb;
+    out.cr = cand[1]->cr;
+  }
+  if (cand[2] && (long long)sse[2] + 16 < best) {
+    choice = 2;
+    out.cb = cand[2]->cb;
+    out.cr = cand[2]->cr;
+  }
+  a.merged[i] = out;
+  a.map[i] = (uint8_t)choice;
+}
+
 }  // namespace
+
+int launch_sao_chroma_merge(cudaStream_t st, const DPlane src[2], const DPlane pre[2], int bd, int chr_ctb,
+                            int w_ctbs, int h_ctbs, const h266_sao_ctb_params *d_indep, h266_sao_ctb_params *d_merged,
+                            uint8_t *d_map, uint64_t *launches) {
+  MergeArgs a{};
+  for (int c = 0; c < 2; ++c) {
+    a.src[c] = src[c];
+    a.pre[c] = pre[c];
+  }
+  a.bd = bd;
+  a.chr_ctb = chr_ctb;
+  a.w_ctbs = w_ctbs;
+  a.indep = d_indep;
+  a.merged = d_merged;
+  a.map = d_map;
+  for (int d = 0; d <= w_ctbs + h_ctbs - 2; ++d) {
+    const int ry0 = max(0, d - (w_ctbs - 1)), ry1 = min(h_ctbs - 1, d);
+    a.diag = d;
+    a.first_ry = ry0;
+    k_sao_merge_diag<<<ry1 - ry0 + 1, kStatThreads, 0, st>>>(a);
+    H266_CUDA(cudaGetLastError());
+    ++*launches;
+  }
+  return H266_OK;
+}
 
 size_t sao_stats_bytes(int n_ctbs) { return (size_t)n_ctbs * 3 * sizeof(SaoStats); }
 

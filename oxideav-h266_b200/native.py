@@ -38,7 +38,7 @@ EXPORTS = [
     "h266_server_stats", "h266_server_replay", "h266_server_destroy", "h266_alf_decide_and_apply_clipped",
     "h266_lmcs_forward_map_luma_rects", "h266_lmcs_chroma_var_scale", "h266_lmcs_add_chroma_residual",
     "h266_output_convert", "h266_sao_decide_picture", "h266_chroma_alf_decide_and_apply_clipped",
-    "h266_cc_alf_decide_and_apply_clipped",
+    "h266_cc_alf_decide_and_apply_clipped", "h266_sao_chroma_merge",
 ]
 PROF_FAMILIES = ("lmcs", "deblock", "sao_alf", "copy")
 
@@ -91,6 +91,7 @@ def lib():
         L.h266_lmcs_add_chroma_residual.argtypes = [vp, vp, u32, vp, u64, vp, u64]
         L.h266_output_convert.argtypes = [vp, vp, vp, u32, u32, vp, u64, u32, C.POINTER(u64)]
         L.h266_sao_decide_picture.argtypes = [vp, vp, vp, u32, u32, u32, u32, vp, u64]
+        L.h266_sao_chroma_merge.argtypes = [vp, vp, vp, vp, u32, u32, u32, u32, vp, vp]
         L.h266_chroma_alf_decide_and_apply_clipped.argtypes = [vp, vp, vp, vp, u64, vp, u32, u32, u32, u32, vp, u64,
                                                                vp, u64]
         L.h266_cc_alf_decide_and_apply_clipped.argtypes = [vp, vp, vp, vp, vp, u64, vp, u32, u32, u32, u32, vp, u64,
@@ -452,3 +453,14 @@ def chroma_alf_decide(ctx: Context, src, rec, apply_pic, aps, *, component: int,
         _check(lib().h266_chroma_alf_decide_and_apply_clipped(
             ctx._h, C.byref(s_c), C.byref(r_c), apply_pic.ctypes.data, len(apply_pic), C.byref(aps), component,
             ctb_log2, bit_depth, chroma_format_idc, c1, nc, c2, nr))
+
+
+def sao_chroma_merge(ctx: Context, src, pre, indep, w_ctbs: int, h_ctbs: int, *, bit_depth: int, ctb_log2: int):
+    """h266_sao_chroma_merge: (merged abi.SAO_CTB_PARAMS records, merge map: 0 own, 1 left, 2 above)."""
+    s_c, p_c = src.to_ctypes(), pre.to_ctypes()
+    ind = np.ascontiguousarray(indep, dtype=abi.SAO_CTB_PARAMS)
+    merged = np.zeros_like(ind)
+    m = np.zeros(max(len(ind), 1), dtype=np.uint8)
+    _check(lib().h266_sao_chroma_merge(ctx._h, C.byref(s_c), C.byref(p_c), ind.ctypes.data, w_ctbs, h_ctbs,
+                                       bit_depth, ctb_log2, merged.ctypes.data, m.ctypes.data))
+    return merged, m[: len(ind)]

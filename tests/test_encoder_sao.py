@@ -111,3 +111,69 @@ def test_gpu_sao_decide_rejects_out_of_range_sample():
     with native.Context(0) as ctx:
         with pytest.raises(native.H266Error):
             native.sao_decide_picture(ctx, src, rec, ctb_log2=6, bit_depth=8)
+
+
+# ---------------------------------------------------------------- chroma merge (src/sao_enc.rs:500-668)
+def merge(src, rec, indep, log2, bd):
+    ctb = 1 << log2
+    return oracle.sao_chroma_merge(src, rec, indep, -(-rec.width // ctb), -(-rec.height // ctb), bit_depth=bd,
+                                   ctb_log2=log2)
+
+
+def test_merge_single_ctb_no_merge():  # chroma_sao_merge_single_ctb_no_merge, src/sao_enc.rs:845-855
+    src = flat(64, 64, 100)
+    rec = src.copy()
+    rec.cb.reshape(-1)[0] ^= 0x10
+    indep = decide(src, rec, 7, 8)
+    merged, m = merge(src, rec, indep, 7, 8)
+    assert merged.shape == (1,) and int((m != 0).sum()) == 0
+
+
+def test_merge_flat_picture_fires_on_neighbours():  # src/sao_enc.rs:862-895
+    src = flat(128, 128, 100)
+    rec = src.copy()
+    rec.cb[:] = 110
+    rec.cr[:] = 90
+    indep = decide(src, rec, 5, 8, luma=False, chroma=True)
+    merged, m = merge(src, rec, indep, 5, 8)
+    assert int((m != 0).sum()) * 2 > len(m)
+
+
+def test_merge_keeps_luma_and_costs():
+    name, src, rec, log2, bd = cases()[2]
+    indep = decide(src, rec, log2, bd)
+    merged, m = merge(src, rec, indep, log2, bd)
+    assert merged["luma"].tobytes() == indep["luma"].tobytes()
+    assert set(np.unique(m)) <= {0, 1, 2}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k", range(4))
+def test_gpu_sao_merge_matches_oracle(k):
+    from oxideav_h266_b200 import native
+    name, src, rec, log2, bd = cases()[k]
+    indep = decide(src, rec, log2, bd)
+    want, wm = merge(src, rec, indep, log2, bd)
+    ctb = 1 << log2
+    with native.Context(0) as ctx:
+        got, gm = native.sao_chroma_merge(ctx, src, rec, indep, -(-rec.width // ctb), -(-rec.height // ctb),
+                                          bit_depth=bd, ctb_log2=log2)
+    assert np.array_equal(gm, wm), name
+    assert got.tobytes() == want.tobytes(), name
+
+
+@pytest.mark.gpu
+def test_gpu_sao_merge_flat_and_device():
+    import torch
+    from oxideav_h266_b200 import native
+    src = flat(128, 128, 100)
+    rec = src.copy()
+    rec.cb[:] = 110
+    rec.cr[:] = 90
+    indep = decide(src, rec, 5, 8, luma=False, chroma=True)
+    want, wm = merge(src, rec, indep, 5, 8)
+    with native.Context(0) as ctx:
+        ds, dr = native.DevicePicture.from_host(src), native.DevicePicture.from_host(rec)
+        got, gm = native.sao_chroma_merge(ctx, ds, dr, indep, 4, 4, bit_depth=8, ctb_log2=5)
+        torch.cuda.synchronize()
+    assert np.array_equal(gm, wm) and got.tobytes() == want.tobytes()
