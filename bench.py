@@ -440,6 +440,24 @@ def run_encoder_trials(ctx, local_rank, stream, steps: int, n_pics: int = 4):
             "candidates": int(n_cand), "ms_per_picture": round(c_total / c_calls, 4),
             "cpu_oracle_ms_per_picture": round(c_cpu, 1)}
     sao["chroma_trials"] = chroma
+    # chroma SAO merge (src/sao_enc.rs:500-668) on the first picture's independent decision
+    d = devs[0]
+    indep = native.sao_decide_picture(ctx, d[0], d[1], ctb_log2=7, bit_depth=10)
+    for _ in range(3):
+        native.sao_chroma_merge(ctx, d[0], d[1], indep, 15, 9, bit_depth=10, ctb_log2=7)
+    torch.cuda.synchronize()
+    m_total, m_calls = 0.0, 0
+    for _ in range(max(1, steps)):
+        e0.record(stream)
+        native.sao_chroma_merge(ctx, d[0], d[1], indep, 15, 9, bit_depth=10, ctb_log2=7)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        m_total += e0.elapsed_time(e1)
+        m_calls += 1
+    t0 = time.perf_counter()
+    oracle.sao_chroma_merge(s_, r_, indep, 15, 9, bit_depth=10, ctb_log2=7)
+    sao["chroma_merge"] = {"ms_per_picture": round(m_total / m_calls, 4), "launches": 23,
+                           "cpu_oracle_ms_per_picture": round((time.perf_counter() - t0) * 1e3, 1)}
     del devs
     torch.cuda.synchronize()
     return {"workload": "encoder luma ALF decision, 1920x1080 10-bit CTU 128, 16 fixed sets + 1 APS set",
