@@ -1406,15 +1406,16 @@ int h266_sao_chroma_merge(h266_ctx *ctx, const h266_picture *src, const h266_pic
   uint8_t *base = nullptr;
   H266_TRY(upload_blob(ln, pr.blob, &base));
   ctx->h2d_bytes += pr.blob.size();
-  const size_t rec_b = n * sizeof(h266_sao_ctb_params);
-  H266_TRY(ln.walk.ensure(rec_b + n + 256));
+  const size_t rec_b = n * sizeof(h266_sao_ctb_params), map_b = (n + 255) & ~(uint64_t)255;
+  H266_TRY(ln.walk.ensure(rec_b + map_b + sao_merge_work_bytes(n) + 256));
   auto *d_merged = ln.walk.as<h266_sao_ctb_params>();
   auto *d_map = ln.walk.as<uint8_t>() + rec_b;
+  void *d_work = ln.walk.as<uint8_t>() + ((rec_b + map_b + 255) & ~(size_t)255);
   {
     Prof pf(ctx, ln.stream, H266_PROF_SAO_ALF);
     H266_TRY(launch_sao_chroma_merge(ln.stream, S, Q, (int)bd, (1 << log2) / 2, (int)wc, (int)hc,
                                      reinterpret_cast<const h266_sao_ctb_params *>(base + off), d_merged, d_map,
-                                     &ctx->launches));
+                                     d_work, &ctx->launches));
   }
   H266_CUDA(cudaMemcpyAsync(merged, d_merged, rec_b, cudaMemcpyDeviceToHost, ln.stream));
   H266_TRY(sync_read(ln, map, d_map, n));

@@ -317,7 +317,8 @@ size_t sao_stats_bytes(int n_ctbs);
 // is written CTB by CTB (each launch reads the previous diagonal's records).
 int launch_sao_chroma_merge(cudaStream_t st, const DPlane src[2], const DPlane pre[2], int bd, int chr_ctb,
                             int w_ctbs, int h_ctbs, const h266_sao_ctb_params *d_indep, h266_sao_ctb_params *d_merged,
-                            uint8_t *d_map, uint64_t *launches);
+                            uint8_t *d_map, void *d_work, uint64_t *launches);
+inline size_t sao_merge_work_bytes(size_t n_ctbs) { return n_ctbs * 3 * 8 + n_ctbs * 4; }
 int launch_sao_decide(cudaStream_t st, const DPlane src[3], const DPlane rec[3], int bd, int log2, int w_ctbs,
                       int h_ctbs, bool luma_on, bool chroma_on, void *d_stats, uint32_t *d_err,
                       h266_sao_ctb_params *d_out, uint64_t *launches);

@@ -296,8 +296,8 @@ __global__ void k_sao_decide(const __grid_constant__ SaoEncArgs a, const SaoStat
 //
 // Raster-order dependency: a CTB weighs its own parameters against the
 // already merged left and above CTBs, so CTBs run one anti-diagonal per
-// launch (both neighbours lie on the previous diagonal).  One CTA per CTB:
-// for each candidate the SAO of this CTB alone on the pre-SAO planes
+// launch (both neighbours lie on the previous diagonal).  Per CTB and
+// candidate: the SAO of this CTB alone on the pre-SAO planes
 // (apply_sao_ctb, src/sao.rs:504-626, no clip rectangle) and the Cb + Cr SSE
 // against the original (chroma_ctb_sse_with, src/sao_enc.rs:698-749), then
 // the decision by cost SSE + 8 * bits (strict <: independent, left, above).
@@ -307,6 +307,8 @@ struct MergeArgs {
   const h266_sao_ctb_params *indep;
   h266_sao_ctb_params *merged;
   uint8_t *map;
+  unsigned long long *sse;  // [ctb][3]
+  unsigned int *count;      // per CTB, zero at the start
 };
 
 __device__ __forceinline__ int sao_value(const DPlane &P, int x, int y, const h266_sao_ctb &p, int maxv, int bd) {
@@ -332,59 +334,64 @@ __device__ __forceinline__ int sao_value(const DPlane &P, int x, int y, const h2
   return v;  // not applied: the sample as it is
 }
 
-__global__ void __launch_bounds__(kStatThreads) k_sao_merge_diag(const __grid_constant__ MergeArgs a) {
-  const int ry = a.first_ry + blockIdx.x, rx = a.diag - ry;
+constexpr int kMergeThreads = 512;
+
+// One CTA per (CTB of the diagonal, candidate): the candidate's Cb + Cr SSE,
+// stored per CTB; the CTA that completes a CTB's set of candidates (per-CTB
+// arrival counter, zeroed by the host; no CTA waits for another) makes the
+// decision.
+__global__ void __launch_bounds__(kMergeThreads) k_sao_merge_diag(const __grid_constant__ MergeArgs a) {
+  const int ry = a.first_ry + blockIdx.x, rx = a.diag - ry, k = blockIdx.y;
+  if ((k == 1 && rx == 0) || (k == 2 && ry == 0)) return;  // no such neighbour (uniform per CTA)
   const int i = ry * a.w_ctbs + rx;
   const int tid = threadIdx.x, maxv = (1 << a.bd) - 1;
   const int cx = rx * a.chr_ctb, cy = ry * a.chr_ctb;
   const int cw = max(0, min(a.chr_ctb, a.pre[0].w - cx)), ch = max(0, min(a.chr_ctb, a.pre[0].h - cy));
-  __shared__ unsigned long long part[kStatThreads / 32];
-  __shared__ unsigned long long sse[3];
-  const h266_sao_ctb_params in = a.indep[i];
-  const h266_sao_ctb_params *cand[3] = {&in, rx > 0 ? &a.merged[i - 1] : nullptr,
-                                        ry > 0 ? &a.merged[i - a.w_ctbs] : nullptr};
-  for (int k = 0; k < 3; ++k) {
-    if (!cand[k]) continue;  // uniform per CTA
-    const h266_sao_ctb pc[2] = {cand[k]->cb, cand[k]->cr};
-    unsigned long long e = 0;
-    for (int y = cy + tid / 32; y < cy + ch; y += kStatThreads / 32)
-      for (int x = cx + (tid & 31); x < cx + cw; x += 32)
+  const h266_sao_ctb_params &cand = k == 0 ? a.indep[i] : (k == 1 ? a.merged[i - 1] : a.merged[i - a.w_ctbs]);
+  const h266_sao_ctb pc[2] = {cand.cb, cand.cr};
+  unsigned long long e = 0;
+  for (int y = cy + tid / 32; y < cy + ch; y += kMergeThreads / 32)
+    for (int x = cx + (tid & 31); x < cx + cw; x += 32)
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
-          const int d = (int)a.src[c].s[(int64_t)y * a.src[c].stride + x] - sao_value(a.pre[c], x, y, pc[c], maxv, a.bd);
-          e += (unsigned long long)(d * d);
-        }
+      for (int c = 0; c < 2; ++c) {
+        const int d = (int)a.src[c].s[(int64_t)y * a.src[c].stride + x] - sao_value(a.pre[c], x, y, pc[c], maxv, a.bd);
+        e += (unsigned long long)(d * d);
+      }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
-    if ((tid & 31) == 0) part[tid / 32] = e;
-    __syncthreads();
-    if (tid == 0) {
-      unsigned long long t = 0;
-      for (int w = 0; w < kStatThreads / 32; ++w) t += part[w];
-      sse[k] = t;
-    }
-    __syncthreads();
-  }
+  for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
+  __shared__ unsigned long long part[kMergeThreads / 32];
+  if ((tid & 31) == 0) part[tid / 32] = e;
+  __syncthreads();
   if (tid) return;
+  unsigned long long t = 0;
+  for (int w = 0; w < kMergeThreads / 32; ++w) t += part[w];
+  a.sse[(size_t)i * 3 + k] = t;
+  __threadfence();
+  const unsigned n_cand = 1u + (rx > 0) + (ry > 0);
+  if (atomicAdd(&a.count[i], 1u) != n_cand - 1) return;
+  __threadfence();
+  unsigned long long sse[3];
+  for (int q = 0; q < 3; ++q) sse[q] = __ldcg(&a.sse[(size_t)i * 3 + q]);
   auto bits = [](const h266_sao_ctb_params &p) {  // chroma_independent_bit_cost, src/sao_enc.rs:670-696
     long long b = 1;
     b += p.cb.sao_type_idx == 0 ? 1 : (p.cb.sao_type_idx == 1 ? 16 : 10);
     b += p.cr.sao_type_idx == 0 ? 1 : (p.cr.sao_type_idx == 1 ? 16 : 10);
     return b;
   };
+  const h266_sao_ctb_params in = a.indep[i];
   long long best = (long long)sse[0] + 8 * bits(in);
   int choice = 0;
   h266_sao_ctb_params out = in;
-  if (cand[1] && (long long)sse[1] + 8 < best) {
+  if (rx > 0 && (long long)sse[1] + 8 < best) {
     best = (long long)sse[1] + 8;
     choice = 1;
-    out.cb = cand[1]->cb;
-    out.cr = cand[1]->cr;
+    out.cb = a.merged[i - 1].cb;
+    out.cr = a.merged[i - 1].cr;
   }
-  if (cand[2] && (long long)sse[2] + 16 < best) {
+  if (ry > 0 && (long long)sse[2] + 16 < best) {
     choice = 2;
-    out.cb = cand[2]->cb;
-    out.cr = cand[2]->cr;
+    out.cb = a.merged[i - a.w_ctbs].cb;
+    out.cr = a.merged[i - a.w_ctbs].cr;
   }
   a.merged[i] = out;
   a.map[i] = (uint8_t)choice;
@@ -394,8 +401,11 @@ __global__ void __launch_bounds__(kStatThreads) k_sao_merge_diag(const __grid_co
 
 int launch_sao_chroma_merge(cudaStream_t st, const DPlane src[2], const DPlane pre[2], int bd, int chr_ctb,
                             int w_ctbs, int h_ctbs, const h266_sao_ctb_params *d_indep, h266_sao_ctb_params *d_merged,
-                            uint8_t *d_map, uint64_t *launches) {
+                            uint8_t *d_map, void *d_work, uint64_t *launches) {
   MergeArgs a{};
+  a.sse = static_cast<unsigned long long *>(d_work);
+  a.count = reinterpret_cast<unsigned int *>(a.sse + (size_t)w_ctbs * h_ctbs * 3);
+  H266_CUDA(cudaMemsetAsync(a.count, 0, (size_t)w_ctbs * h_ctbs * sizeof(unsigned int), st));
   for (int c = 0; c < 2; ++c) {
     a.src[c] = src[c];
     a.pre[c] = pre[c];
@@ -410,7 +420,7 @@ int launch_sao_chroma_merge(cudaStream_t st, const DPlane src[2], const DPlane p
     const int ry0 = max(0, d - (w_ctbs - 1)), ry1 = min(h_ctbs - 1, d);
     a.diag = d;
     a.first_ry = ry0;
-    k_sao_merge_diag<<<ry1 - ry0 + 1, kStatThreads, 0, st>>>(a);
+    k_sao_merge_diag<<<dim3(ry1 - ry0 + 1, 3), kMergeThreads, 0, st>>>(a);
     H266_CUDA(cudaGetLastError());
     ++*launches;
   }
