@@ -38,14 +38,15 @@ import pathlib
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = pathlib.Path(__file__).resolve().parent
 WIDTH, HEIGHT, BITDEPTH = 1920, 1080, 10
 METRIC = "filter-chain Mpx/s 1080p/2160p 10-bit bit-exact"
-# DRAM bytes (read + write) per luma pixel of the batched SAO/ALF launch, from the
-# ncu capture in profiles/k_sao_alf_packed_c2_1080p10.md (16 pictures per launch:
-# 100 803 840 + 63 711 232 B)
+# DRAM bytes (read + write) per luma pixel of the batched SAO/ALF launch, from one
+# ncu capture of that launch over 16 pictures of this workload (100 803 840 +
+# 63 711 232 B); the bench line scales it to its own batch and labels it so.
 SAO_ALF_TRAFFIC_PER_PX = (100803840 + 63711232) / (16 * 1920 * 1080)
 
 
@@ -84,11 +85,12 @@ class ClockSampler:
     def __init__(self, gpu_id: str):
         self.gpu_id = gpu_id
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+        fd, name = tempfile.mkstemp(prefix="h266_clocks_", suffix=".csv")
+        os.close(fd)
+        self.path = pathlib.Path(name)
 
     def __enter__(self):
         try:
-            self.path.parent.mkdir(exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
@@ -112,12 +114,14 @@ class ClockSampler:
         except Exception:
             return []
 
-    def prime(self, step, max_steps: int):
+    def prime(self, step, max_seconds: float = 20.0):
         """Runs untimed steps until the sampler has written its first line
-        (nvidia-smi starts slowly), so the timed region is sampled under load;
-        returns the line count at that point (samples before it are dropped)."""
-        for _ in range(max_steps if self.proc else 0):
-            if len(self._lines()) >= 1:
+        (nvidia-smi can take seconds to start), so the timed region is sampled
+        under load; gives up after `max_seconds` of wall time.  Returns the line
+        count at that point (samples before it are dropped)."""
+        t0 = time.perf_counter()
+        while self.proc and time.perf_counter() - t0 < max_seconds:
+            if len(self._lines()) >= 1 or self.proc.poll() is not None:
                 break
             step()
             torch_sync()
@@ -182,6 +186,60 @@ def make_batch(rank: int, n: int):
     return [W.config2(2000 + 1000 * rank + i, WIDTH, HEIGHT) for i in range(n)]
 
 
+def plane_digests(pic) -> tuple:
+    """SHA-256 (first 16 hex digits) of each plane's samples, row-major u16."""
+    import hashlib
+
+    import numpy as np
+
+    return tuple(hashlib.sha256(np.ascontiguousarray(a, dtype=np.uint16).tobytes()).hexdigest()[:16]
+                 for a in pic.planes())
+
+
+def oracle_digests(items, threads: int) -> list:
+    """Per-picture plane digests of the oracle's chain output for `items`
+    ((picture, filter args) pairs; the pictures are not modified)."""
+    import oracle
+
+    pics = [p.copy() for p, _ in items]
+    oracle.apply_in_loop_filters_mt(pics, [f for _, f in items], threads)
+    return [plane_digests(p) for p in pics]
+
+
+def parity_record(got_pics, want: list) -> dict:
+    """Compares the digests of the pictures a timed path produced with the
+    oracle's; `got_pics` are host pictures in the order of `want`."""
+    bad = [i for i, (g, w) in enumerate(zip(got_pics, want)) if plane_digests(g) != w]
+    rec = {"checked_pictures": len(want), "mismatches": len(bad), "hash": "sha256 per plane"}
+    if bad:
+        rec["first_mismatch"] = bad[0]
+    return rec
+
+
+def parity_summary(parity: dict, served, configs) -> dict:
+    """All legs' parity records in one object, with the totals first."""
+    legs = dict(parity)
+    for name, rec in (configs or {}).items():
+        if isinstance(rec, dict) and "parity" in rec:
+            for mode, r in rec["parity"].items():
+                legs[f"{name}_{mode}"] = r
+    if served and "parity" in served:
+        legs["served_mix"] = served["parity"]
+    return {"checked_pictures": sum(r["checked_pictures"] for r in legs.values()),
+            "mismatches": sum(r["mismatches"] for r in legs.values()), "legs": legs}
+
+
+def restore_device(devs, items):
+    """Puts the unfiltered samples back into the device pictures (the chain
+    filters in place, so every timed step re-filters the previous output)."""
+    import numpy as np
+    import torch
+
+    for d, (p, _) in zip(devs, items):
+        for t, a in zip((d.luma, d.cb, d.cr), p.planes()):
+            t.copy_(torch.from_numpy(np.ascontiguousarray(a).view(np.int16)))
+
+
 def cpu_baseline(items, threads: int, min_seconds: float = 10.0):
     """Oracle chain on `threads` host threads over a bounded sample: the batch's
     pictures, filtered again from their unfiltered copies until at least
@@ -228,7 +286,7 @@ def run_served(ctx, local_rank, seconds: float, rates=(1, 4, 8, 12)):
             for r in range(SERVED_RING):
                 plan, dev = ctx.plan(pic, fa), native.DevicePicture.from_host(pic, local_rank)
                 ring.append((plan, dev, dev.to_ctypes()))  # ctypes picture built once
-            streams.append({"fps": fps, "px": w * h, "ring": ring})
+            streams.append({"fps": fps, "px": w * h, "ring": ring, "item": (pic, fa)})
     torch.cuda.synchronize()
     L = native.lib()
 
@@ -276,6 +334,17 @@ def run_served(ctx, local_rank, seconds: float, rates=(1, 4, 8, 12)):
                 srv.wait(tk)
             serve_once(srv, rates[0], 0.5)  # discarded warm-up run
             out[mode] = {f"{x}x": serve_once(srv, x, seconds) for x in rates}
+            if mode == "batched":  # every ring picture of every stream submitted at once, checked
+                items = [st["item"] for st in streams]
+                want = oracle_digests(items, os.cpu_count() or 1)
+                devs = [dev for st in streams for _, dev, _ in st["ring"]]
+                restore_device(devs, [it for it in items for _ in range(SERVED_RING)])
+                torch.cuda.synchronize()
+                tickets = [srv.submit(plan, dev) for st in streams for plan, dev, _ in st["ring"]]
+                for tk in tickets:
+                    srv.wait(tk)
+                out["parity"] = parity_record([d.to_host() for d in devs],
+                                              [w_ for w_ in want for _ in range(SERVED_RING)])
     for st in streams:
         for plan, _, _ in st["ring"]:
             plan.close()
@@ -314,9 +383,18 @@ def run_configs(ctx, local_rank, stream, steps: int):
 
         ms_b = timed(lambda: ctx.execute_plans(plans, devs))
         ms_p = timed(lambda: [pl.execute(d) for pl, d in zip(plans, devs)])
+        want = oracle_digests(items, os.cpu_count() or 1)
+        par = {}
+        for mode, fn in (("batched", lambda: ctx.execute_plans(plans, devs)),
+                         ("plain", lambda: [pl.execute(d) for pl, d in zip(plans, devs)])):
+            restore_device(devs, items)
+            fn()
+            torch.cuda.synchronize()
+            par[mode] = parity_record([d.to_host() for d in devs], want)
         out[name] = {"pictures": len(items), "mpx_per_step": round(px / 1e6, 2),
                      "batched": {"ms_per_step": round(ms_b, 4), "mpx_per_s": round(px / ms_b / 1e3, 1)},
-                     "plain": {"ms_per_step": round(ms_p, 4), "mpx_per_s": round(px / ms_p / 1e3, 1)}}
+                     "plain": {"ms_per_step": round(ms_p, 4), "mpx_per_s": round(px / ms_p / 1e3, 1)},
+                     "parity": par}
         for pl in plans:
             pl.close()
         del devs
@@ -592,7 +670,7 @@ def run_ours(args, rank, world, local_rank):
     for attempt in range(2):
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with ClockSampler(gpu_id) as cs:
-            cs.prime(step, 400)  # untimed steps until the clock sampler runs (no collectives inside a step)
+            cs.prime(step)  # untimed steps until the clock sampler runs (no collectives inside a step)
             barrier()
             torch.cuda.synchronize()
             l0 = ctx.kernel_launches
@@ -623,6 +701,17 @@ def run_ours(args, rank, world, local_rank):
              "ms_per_step": round(float(tp.item()) / plain_steps, 4), "steps": plain_steps,
              "path": "h266_chain_plan_execute per picture (2 launches per picture)"}
 
+    # parity of the timed paths: one step of each on the unfiltered pictures,
+    # every plane hashed and compared with the oracle's output
+    threads = os.cpu_count() or 1
+    want = oracle_digests(items, threads)
+    parity = {}
+    for name, fn in (("batched", step), ("plain", step_plain)):
+        restore_device(dev, items)
+        fn()
+        torch.cuda.synchronize()
+        parity[name] = parity_record([d.to_host() for d in dev], want)
+
     # roofline of the SAO/ALF tile kernel: CUDA-event durations of its launches
     # (one per step, covering the batch's pictures) in a profiled run
     ctx.set_profiling(True)
@@ -642,6 +731,8 @@ def run_ours(args, rank, world, local_rank):
         "bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
         "frac": round(achieved / peaks["hbm_gbs"], 4), "peak_source": peak_kind,
         "traffic": (round(SAO_ALF_TRAFFIC_PER_PX * WIDTH * HEIGHT * args.batch) if SAO_ALF_TRAFFIC_PER_PX else None),
+        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 16-picture launch, scaled to "
+                          "this launch's pictures",
         "algorithmic_bytes_per_launch": alg_bytes, "launch_us": round(per_launch_s * 1e6, 2),
         "pictures_per_launch": args.batch,
         "share_of_device_time": {k: round(v[0] / total_ms, 3) for k, v in prof.items() if total_ms > 0},
@@ -676,6 +767,11 @@ def run_ours(args, rank, world, local_rank):
         te = torch.tensor([dt], dtype=torch.float64, device="cuda")
         if dist:
             dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        for (_, planes, _), (p, _) in zip(host, items):  # one more call on the unfiltered pictures, checked
+            for (_, arr), a in zip(planes, p.planes()):
+                arr[...] = a
+        ctx.apply_in_loop_filters_batch(hps, hfs)
+        parity["e2e"] = parity_record(hps, want)
         e2e = {"value": round(world * px_per_step * e_steps / float(te.item()) / 1e6, 2), "unit": "Mpx/s",
                "h2d_bytes_per_step": (b1[0] - b0[0]) // e_steps, "d2h_bytes_per_step": (b1[1] - b0[1]) // e_steps,
                "bytes": "planes and side information, from the context's transfer counters",
@@ -707,7 +803,7 @@ def run_ours(args, rank, world, local_rank):
             "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic (seeded 1080p config generator)",
             "config": workload_config(args.batch, world),
             "roofline": roofline, "plain": plain, "served": served, "configs": configs, "encoder_alf_trials": trials, "recon_io": recon,
-            "cpu_baseline": cpu, "e2e": e2e,
+            "cpu_baseline": cpu, "e2e": e2e, "parity": parity_summary(parity, served, configs),
             "gpu_launches": int(launches),
             "clocks": clocks,
         }

@@ -511,19 +511,22 @@ int h266_server_destroy(h266_server *server); /* drains the queue first */
 
 /* ---- allocation-free chain ---------------------------------------------------
  * No counterpart in the reference.  The whole chain (as h266_apply_in_loop_filters)
- * on device planes, for callers that cannot call cudaMalloc at run time: code
- * running inside CUDA-graph stream capture, real-time decode loops that ban
- * allocator calls once streaming starts, hosts whose device memory belongs to
- * their own pool.  The call allocates nothing: its scratch (side information,
- * LMCS LUT, deblocked planes) lives in one fixed device array of
+ * on device planes, for callers that cannot call cudaMalloc at run time:
+ * real-time decode loops that ban allocator calls (and their unbounded latency)
+ * once streaming starts, and hosts whose device memory all belongs to their own
+ * pool, so a library allocation would fail or break their accounting.  The call
+ * allocates no device memory: its scratch (side information, LMCS LUT,
+ * deblocked planes) lives in one fixed device array of
  * H266_NOALLOC_SCRATCH_BYTES that every GPU loading the library keeps until the
  * process exits.  The caller passes the picture (H266_MEM_DEVICE planes,
  * filtered in place) and the stream (NULL = legacy default stream).
  *   - Pictures whose scratch need exceeds the array are rejected with
  *     H266_ERR_UNSUPPORTED and a message naming both sizes (1920x1080 4:2:0
  *     fits; 3840x2160 does not).
- *   - The first call on a device looks up the array's device address; make that
- *     first call before any stream capture begins.
+ *   - Every call looks up the array's device address on the current device
+ *     (cudaGetSymbolAddress, which allocates nothing).  The first call on a
+ *     device also loads the library's device code there, so make that first
+ *     call before any stream capture begins.
  *   - All calls share the one array and every call overwrites it: calls whose
  *     work overlaps on the GPU (other streams, other threads) race.  Serialize
  *     them on one stream.

@@ -25,7 +25,7 @@ __global__ void __launch_bounds__(kSseThreads) k_ctb_sse(DPlane a, DPlane b, int
     for (int y = y0 + threadIdx.x / 32; y < y1; y += kSseThreads / 32)
       for (int x = x0 + (threadIdx.x & 31); x < x0 + w; x += 32) {
         const int d = (int)a.s[(int64_t)y * a.stride + x] - (int)b.s[(int64_t)y * b.stride + x];
-        e += (unsigned long long)(d * d);
+        e += (unsigned long long)((long long)d * d);
       }
   }
 #pragma unroll

@@ -2468,10 +2468,11 @@ int h266_server_destroy(h266_server *s) {
 
 // ======================================================================= allocation-free chain
 //
-// For callers that must not allocate device memory at run time: code running
-// while a CUDA graph is being captured, real-time decode loops that forbid
-// allocator calls (and their latency) once streaming has started, and hosts
-// that hand the whole device budget to their own pool.  The chain's scratch --
+// For callers that must not allocate device memory at run time: real-time
+// decode loops that forbid allocator calls (and their latency) once streaming
+// has started, and hosts that hand the whole device budget to their own pool,
+// where a library allocation would fail or escape their accounting.  The
+// chain's scratch --
 // the side information of the call, the LMCS LUT and the deblocked planes the
 // SAO / ALF pass reads -- lives in this fixed device array instead of in a
 // context.  Every GPU that loads the library holds the array until the process
@@ -2480,25 +2481,16 @@ namespace {
 
 static __device__ __align__(256) uint8_t g_noalloc_scratch[H266_NOALLOC_SCRATCH_BYTES];
 
-constexpr int kMaxDevices = 256;
-std::mutex g_noalloc_mu;
-uint8_t *g_noalloc_ptr[kMaxDevices] = {nullptr};
-
 // Device address of g_noalloc_scratch on the current device.  In host code the
-// symbol is only a host-side stand-in, so the address is looked up once per
-// device with that device current.
+// symbol is only a host-side stand-in, so the address is looked up with the
+// device current -- on every call, not cached: a cached address would outlive
+// a cudaDeviceReset or a recreated primary context.  The lookup allocates
+// nothing; the first one on a device also loads this library's device code.
 int noalloc_scratch(uint8_t **out) {
-  int dev = -1;
-  H266_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) return set_error(H266_ERR_UNSUPPORTED, "device ordinal beyond 255");
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void *p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-    g_noalloc_ptr[dev] = static_cast<uint8_t *>(p);
-  }
-  *out = g_noalloc_ptr[dev];
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+  *out = static_cast<uint8_t *>(p);
   return H266_OK;
 }
 

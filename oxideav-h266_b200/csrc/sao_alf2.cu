@@ -677,7 +677,7 @@ __global__ void __launch_bounds__(NT, 2) k_alf_luma_trials(const __grid_constant
       org[rr][p] = in ? (int)orig.s[(int64_t)gy * orig.stride + gx] : -1;
       if (in) {
         const int d = org[rr][p] - (int)sm.sL[(j + 3) * S::SLW + 4 * bx + p + 4];
-        e0 += (unsigned long long)(d * d);
+        e0 += (unsigned long long)((long long)d * d);
       }
     }
   }
@@ -723,11 +723,11 @@ __global__ void __launch_bounds__(NT, 2) k_alf_luma_trials(const __grid_constant
           const int v1 = clampd((int)(cur[rr][q] >> 16) + ((hi + round) >> shift[rr]), 0, maxv);
           if (org[rr][2 * q] >= 0) {
             const int d = org[rr][2 * q] - v0;
-            e += (unsigned long long)(d * d);
+            e += (unsigned long long)((long long)d * d);
           }
           if (org[rr][2 * q + 1] >= 0) {
             const int d = org[rr][2 * q + 1] - v1;
-            e += (unsigned long long)(d * d);
+            e += (unsigned long long)((long long)d * d);
           }
         }
       }
@@ -754,7 +754,7 @@ __global__ void __launch_bounds__(NT, 2) k_alf_luma_trials(const __grid_constant
       for (int p = 0; p < 4; ++p)
         if (org[rr][p] >= 0) {
           const int d = org[rr][p] - o[p];
-          e += (unsigned long long)(d * d);
+          e += (unsigned long long)((long long)d * d);
         }
     }
     e = warp_sum(e);

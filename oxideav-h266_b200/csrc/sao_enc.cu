@@ -355,7 +355,7 @@ __global__ void __launch_bounds__(kMergeThreads) k_sao_merge_diag(const __grid_c
 #pragma unroll
       for (int c = 0; c < 2; ++c) {
         const int d = (int)a.src[c].s[(int64_t)y * a.src[c].stride + x] - sao_value(a.pre[c], x, y, pc[c], maxv, a.bd);
-        e += (unsigned long long)(d * d);
+        e += (unsigned long long)((long long)d * d);
       }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);

@@ -177,3 +177,35 @@ def test_gpu_sao_merge_flat_and_device():
         got, gm = native.sao_chroma_merge(ctx, ds, dr, indep, 4, 4, bit_depth=8, ctb_log2=5)
         torch.cuda.synchronize()
     assert np.array_equal(gm, wm) and got.tobytes() == want.tobytes()
+
+
+def merge_16bit_case():
+    """A 16-bit picture whose chroma differences reach 50 000 and more, so a
+    squared difference no longer fits in 32 bits (46 341^2 > 2^31)."""
+    rec, _ = W.make_workload(8300, 256, 192, 8, 6)
+    rng = np.random.Generator(np.random.PCG64(8301))
+    rec = W.PictureData(*(np.asarray(p, np.uint16) * np.uint16(64) for p in (rec.luma, rec.cb, rec.cr)), 16)
+    src = rec.copy()
+    for name in ("cb", "cr"):
+        p = getattr(rec, name)
+        setattr(src, name, np.clip(65535 - p.astype(np.int64) + rng.integers(-300, 301, size=p.shape), 0,
+                                   65535).astype(np.uint16))
+    return src, rec
+
+
+def test_merge_16bit_case_exceeds_32_bit_squares():
+    src, rec = merge_16bit_case()
+    d = np.abs(src.cb.astype(np.int64) - rec.cb.astype(np.int64))
+    assert int(d.max()) > 46341
+
+
+@pytest.mark.gpu
+def test_gpu_sao_merge_16bit_large_differences():
+    from oxideav_h266_b200 import native
+    src, rec = merge_16bit_case()
+    indep = decide(src, rec, 6, 16, luma=False, chroma=True)
+    want, wm = merge(src, rec, indep, 6, 16)
+    with native.Context(0) as ctx:
+        got, gm = native.sao_chroma_merge(ctx, src, rec, indep, 4, 3, bit_depth=16, ctb_log2=6)
+    assert np.array_equal(gm, wm)
+    assert got.tobytes() == want.tobytes()

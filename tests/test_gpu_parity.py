@@ -262,6 +262,53 @@ def test_plan_batch_matches_oracle_on_mixed_pictures(ctx):
             pl.close()
 
 
+def _batched_plans_match_oracle(ctx, items, what):
+    """One batched execution of resident plans over `items` (the bench's
+    value path), then per-picture launches of the same plans, each on fresh
+    samples, every picture compared with the oracle bit for bit."""
+    import os
+
+    import torch
+
+    wants = [p.copy() for p, _ in items]
+    oracle.apply_in_loop_filters_mt(wants, [f for _, f in items], os.cpu_count() or 1)
+    plans = [ctx.plan(p, f) for p, f in items]
+    try:
+        for mode in ("batched", "plain"):
+            devs = [native.DevicePicture.from_host(p) for p, _ in items]
+            torch.cuda.synchronize()
+            if mode == "batched":
+                ctx.execute_plans(plans, devs)
+            else:
+                for pl, d in zip(plans, devs):
+                    pl.execute(d)
+            ctx.synchronize()
+            for i, (d, w) in enumerate(zip(devs, wants)):
+                assert_same(d.to_host(), w, f"{what} {mode} picture {i}")
+            del devs
+    finally:
+        for pl in plans:
+            pl.close()
+
+
+def test_plan_batch_full_size_1080p_x4(ctx):
+    """Four full-size pictures of the 1080p benchmark config (1920x1080
+    10-bit, inter CUs, 4 luma APSs, CC-ALF, LMCS) in one batched launch."""
+    _batched_plans_match_oracle(ctx, [W.config2(2000 + i) for i in range(4)], "1080p x4")
+
+
+def test_plan_batch_2160p_tiles_x16(ctx):
+    """The 16-picture 3840x2160 10-bit batch with a 4x2 tile grid and
+    filtering across tiles off, in one batched launch."""
+    _batched_plans_match_oracle(ctx, [W.config3(3000 + i) for i in range(16)], "2160p tiles x16")
+
+
+def test_plan_batch_mixed_sizes_x12(ctx):
+    """Mixed sizes as in the 64-picture batch (832x480 CTU 64 8-bit, 1080p and
+    2160p 10-bit, each picture with its own ALF / CC-ALF / LMCS tables)."""
+    _batched_plans_match_oracle(ctx, [W.config4(4000 + i) for i in range(12)], "mixed x12")
+
+
 def test_profiling_counts_every_family(ctx):
     pic, fa = small_c2(22)
     ctx.set_profiling(True)

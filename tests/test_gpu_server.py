@@ -119,3 +119,40 @@ def test_native_replay_honours_order_and_matches_oracle(requests):
             pl.close()
     finally:
         ctx.close()
+
+
+def test_served_stream_mix_with_waiting_admission():
+    """The served stream mix's resolutions (832x480, 1920x1080 and 3840x2160,
+    10-bit, config-1 content), two streams each with two pictures in flight,
+    all submitted at once to a server whose memory budget holds one 2160p
+    request: admission must wait for completions, and every result must still
+    equal the oracle's."""
+    import os
+
+    import torch
+
+    sizes = ((832, 480, 6), (1920, 1080, 7), (3840, 2160, 7))
+    items = [W.make_workload(9500 + 10 * k + j, w, h, 10, ctb) for k, (w, h, ctb) in enumerate(sizes)
+             for j in range(2)]
+    wants = [p.copy() for p, _ in items]
+    oracle.apply_in_loop_filters_mt(wants, [f for _, f in items], os.cpu_count() or 1)
+    # request bytes: the picture's planes and the plan's scratch planes (u16, 4:2:0)
+    budget = 2 * 2 * 3840 * 2160 * 3 // 2
+    ctx = native.Context(0)
+    try:
+        plans = [ctx.plan(p, f) for p, f in items for _ in range(2)]
+        devs = [native.DevicePicture.from_host(p) for p, _ in items for _ in range(2)]
+        torch.cuda.synchronize()
+        with native.Server(0, max_batch=64, memory_budget=budget) as srv:
+            tickets = [srv.submit(pl, d) for pl, d in zip(plans, devs)]
+            lat = [srv.wait(t) for t in tickets]
+            n_req, n_batches = srv.stats()
+        assert n_req == len(plans) and all(ms > 0 for ms in lat)
+        assert n_batches >= 4  # each 2160p request filled the budget on its own
+        torch.cuda.synchronize()
+        for i, d in enumerate(devs):
+            assert d.to_host().equal(wants[i // 2]), f"request {i} differs from the oracle"
+        for pl in plans:
+            pl.close()
+    finally:
+        ctx.close()

@@ -1,9 +1,9 @@
 """The allocation-free chain entry point, h266_apply_in_loop_filters_noalloc.
 
-It exists for callers that cannot allocate device memory while they run --
-work recorded under CUDA-graph stream capture, real-time decode loops that ban
-allocator calls once streaming starts, hosts whose device memory belongs to
-their own pool.  Its scratch is a fixed device array inside the library.
+It exists for callers that cannot allocate device memory while they run:
+real-time decode loops that ban allocator calls (and their latency) once
+streaming starts, and hosts whose device memory all belongs to their own pool.
+Its scratch is a fixed device array inside the library.
 
 These checks call it through the C ABI twice in a row and compare each output
 with the allocating entry point, h266_apply_in_loop_filters, bit for bit
