@@ -173,6 +173,36 @@ def replica_value(px_per_step: float, steps: int, ms_local: float, dist=None, de
     return world * px_per_step * steps / (ms / 1e3) / 1e6, ms
 
 
+def replica_parity(rec: dict, dist=None, device=None) -> dict:
+    """Sums one leg's parity record over the replicas (every rank checked its
+    own pictures), so rank 0's line covers the whole job."""
+    import torch
+
+    t = torch.tensor([rec["checked_pictures"], rec["mismatches"], int(rec["mismatches"] > 0)], dtype=torch.int64,
+                     device=device)
+    if dist is None:
+        return dict(rec)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return {"checked_pictures": int(t[0]), "mismatches": int(t[1]), "hash": rec["hash"],
+            "ranks": dist.get_world_size(), "ranks_with_mismatches": int(t[2])}
+
+
+def replica_job(items, step, check, steps: int, timer, dist=None, device=None):
+    """The replica structure of the multi-GPU run: every rank filters its own
+    pictures (`items`, seeded per rank): `steps` calls of `step` timed by
+    `timer` (a function of a callable, returning elapsed ms), then `check()`,
+    one step on the unfiltered pictures returning the filtered host pictures.
+    Returns the whole-job Mpx/s, the slowest rank's ms and the parity record
+    against the oracle, both aggregated over ranks; no collective runs inside
+    a step."""
+    want = oracle_digests(items, os.cpu_count() or 1)
+    ms = timer(lambda: [step() for _ in range(steps)])
+    px = sum(p.width * p.height for p, _ in items)
+    value, ms_max = replica_value(px, steps, ms, dist, device)
+    par = replica_parity(parity_record(check(), want), dist, device)
+    return value, ms_max, par
+
+
 def workload_config(batch: int, world: int) -> dict:
     return {"workload": f"c2_1080p10_x{batch}", "width": WIDTH, "height": HEIGHT, "bit_depth": BITDEPTH,
             "pictures_per_step_per_gpu": batch, "chain": "LMCS-1 -> deblock -> SAO -> ALF -> CC-ALF",
@@ -667,26 +697,37 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    for attempt in range(2):
-        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        with ClockSampler(gpu_id) as cs:
-            cs.prime(step)  # untimed steps until the clock sampler runs (no collectives inside a step)
+    run = {}
+
+    def timed(fn):  # CUDA events on the library's stream, clocks sampled meanwhile; one retake on bad clocks
+        for attempt in range(2):
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with ClockSampler(gpu_id) as cs:
+                cs.prime(step)  # untimed steps until the clock sampler runs (no collectives inside a step)
+                barrier()
+                torch.cuda.synchronize()
+                l0 = ctx.kernel_launches
+                start.record(stream)
+                fn()
+                end.record(stream)
+                torch.cuda.synchronize()
             barrier()
-            torch.cuda.synchronize()
-            l0 = ctx.kernel_launches
-            start.record(stream)
-            for _ in range(args.steps):
-                step()
-            end.record(stream)
-            torch.cuda.synchronize()
-        barrier()
-        ms = start.elapsed_time(end)
-        launches = ctx.kernel_launches - l0
-        clocks = cs.summary()
-        if not bad_clocks(clocks):
-            break
+            run["launches"] = ctx.kernel_launches - l0
+            run["clocks"] = cs.summary()
+            if not bad_clocks(run["clocks"]):
+                break
+        return start.elapsed_time(end)
+
+    def check_batched():  # one batched step on the unfiltered pictures, read back
+        restore_device(dev, items)
+        step()
+        torch.cuda.synchronize()
+        return [d.to_host() for d in dev]
+
     px_per_step = args.batch * WIDTH * HEIGHT
-    value, ms_max = replica_value(px_per_step, args.steps, ms, dist, "cuda")
+    parity = {}
+    value, ms_max, parity["batched"] = replica_job(items, step, check_batched, args.steps, timed, dist, "cuda")
+    launches, clocks = run["launches"], run["clocks"]
 
     # the same pictures as plain per-picture launches, for comparison
     for _ in range(args.warmup):
@@ -703,14 +744,11 @@ def run_ours(args, rank, world, local_rank):
 
     # parity of the timed paths: one step of each on the unfiltered pictures,
     # every plane hashed and compared with the oracle's output
-    threads = os.cpu_count() or 1
-    want = oracle_digests(items, threads)
-    parity = {}
-    for name, fn in (("batched", step), ("plain", step_plain)):
-        restore_device(dev, items)
-        fn()
-        torch.cuda.synchronize()
-        parity[name] = parity_record([d.to_host() for d in dev], want)
+    want = oracle_digests(items, os.cpu_count() or 1)
+    restore_device(dev, items)
+    step_plain()
+    torch.cuda.synchronize()
+    parity["plain"] = replica_parity(parity_record([d.to_host() for d in dev], want), dist, "cuda")
 
     # roofline of the SAO/ALF tile kernel: CUDA-event durations of its launches
     # (one per step, covering the batch's pictures) in a profiled run
@@ -771,7 +809,7 @@ def run_ours(args, rank, world, local_rank):
             for (_, arr), a in zip(planes, p.planes()):
                 arr[...] = a
         ctx.apply_in_loop_filters_batch(hps, hfs)
-        parity["e2e"] = parity_record(hps, want)
+        parity["e2e"] = replica_parity(parity_record(hps, want), dist, "cuda")
         e2e = {"value": round(world * px_per_step * e_steps / float(te.item()) / 1e6, 2), "unit": "Mpx/s",
                "h2d_bytes_per_step": (b1[0] - b0[0]) // e_steps, "d2h_bytes_per_step": (b1[1] - b0[1]) // e_steps,
                "bytes": "planes and side information, from the context's transfer counters",
@@ -864,8 +902,18 @@ def main():
     ap.add_argument("--served-seconds", type=float, default=2.0,
                     help="seconds of Poisson arrivals per served measurement (0: skip)")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: relaunch this command under torch.distributed.run
+        import random
+
+        port = 29500 + random.Random(os.getpid()).randrange(2000)
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+               "--master-addr", "127.0.0.1", "--master-port", str(port), str(pathlib.Path(__file__).resolve())]
+        os.execvp(sys.executable, cmd + sys.argv[1:])
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
+    if world != args.gpus and rank == 0:
+        print(f"bench: --gpus {args.gpus} but WORLD_SIZE={world}; running {world} replicas", file=sys.stderr)
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     _import_pkg()
     if args.impl == "reference":
