@@ -380,7 +380,7 @@ bool build_packed(Pass2Host &h, int bd, uint32_t cfi, const h266_alf_aps_data *c
           uint32_t *w = &h.luma_packed[((s * 100) + c * 4 + t) * 36 + 3 * k];
           w[0] = ((uint32_t)clip & 0xFFFF) | ((uint32_t)clip << 16);
           w[1] = ((uint32_t)(-clip) & 0xFFFF) | ((uint32_t)(-clip) << 16);
-          w[2] = (uint32_t)coef & 0xFF;
+          w[2] = ((uint32_t)coef & 0xFF) | ((uint32_t)coef & 0xFF) << 24;  // dp2a_lo: low lane, dp2a_hi: high lane
         }
   if (caps)
     for (uint32_t f = 0; f < caps->n_chroma_filters; ++f)
@@ -390,8 +390,13 @@ bool build_packed(Pass2Host &h, int bd, uint32_t cfi, const h266_alf_aps_data *c
         uint32_t *w = &h.args.tables.chroma_packed[f * 18 + 3 * k];
         w[0] = ((uint32_t)clip & 0xFFFF) | ((uint32_t)clip << 16);
         w[1] = ((uint32_t)(-clip) & 0xFFFF) | ((uint32_t)(-clip) << 16);
-        w[2] = (uint32_t)coef & 0xFF;
+        w[2] = ((uint32_t)coef & 0xFF) | ((uint32_t)coef & 0xFF) << 24;
       }
+  // CC-ALF taps are applied as signed-byte dp2a weights
+  for (int c = 0; c < 2; ++c)
+    for (int f = 0; f < 4; ++f)
+      for (int k = 0; k < 7; ++k)
+        if (!in8(h.args.tables.cc_coeff[c][f][k])) return false;
   return true;
 }
 
@@ -575,6 +580,11 @@ int build_pass2(const h266_picture &pic, const Pass2Inputs &in, Pass2Host &h) {
   a.has_clip = in.cols != nullptr;
   a.sao_luma = sao_on && in.sao_cfg->luma_used;
   a.sao_chroma = sao_on && in.sao_cfg->chroma_used && cfi != 0;
+  a.sao_i8 = 1;  // the packed SAO step looks offsets up as signed bytes
+  for (const CtbDev &d : h.ctbs)
+    for (int c = 0; c < 3; ++c)
+      for (int k = 0; k < 4; ++k)
+        if (d.sao[c].off[k] < -128 || d.sao[c].off[k] > 127) a.sao_i8 = 0;
   h.packed = build_packed(h, (int)bd, cfi, caps);
   if (!h.packed) h.luma_packed.clear();
   return H266_OK;
@@ -642,6 +652,7 @@ void bind_pass2(Pass2Args &a, const uint8_t *base, const Staged &st, const DPlan
   a.tables.luma_coeff = reinterpret_cast<const int32_t *>(base + st.tab);  // per slot: coeff[300], clip[300]
   a.tables.luma_clip = a.tables.luma_coeff + 300;
   a.tables.luma_packed = reinterpret_cast<const uint32_t *>(base + st.pack);
+  pass2_tma_maps(a);
 }
 
 int run_pass2(h266_ctx *ctx, cudaStream_t stream, Pass2Args a, bool do_sao, bool do_alf, bool packed,
@@ -1086,6 +1097,11 @@ int h266_ctx_synchronize(h266_ctx *ctx) {
   H266_TRY(check_ctx(ctx));
   Guard g(ctx->device);
   H266_CUDA(cudaStreamSynchronize(ctx->stream));
+  uint32_t timeouts = 0;
+  H266_TRY(pass2_wait_timeouts(&timeouts));
+  if (timeouts)
+    return set_error(H266_ERR_TIMEOUT, std::to_string(timeouts) +
+                                           " SAO/ALF tiles gave up waiting for their window copies (left unfiltered)");
   return H266_OK;
 }
 

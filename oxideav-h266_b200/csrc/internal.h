@@ -2,6 +2,7 @@
 // chain library (not part of the C ABI).
 #pragma once
 
+#include <cuda.h>  // CUtensorMap (the driver entry point is fetched at run time; nothing links libcuda)
 #include <cuda_runtime.h>
 
 #include <condition_variable>
@@ -250,6 +251,12 @@ struct AlfTablesDev {
 };
 
 struct Pass2Args {
+  // TMA descriptors of the three input planes (2-D u16 tensors, the tile
+  // kernel's window boxes); valid when `tma` is set.  First, for the 64-byte
+  // alignment the TMA unit needs.
+  CUtensorMap tmap[3];
+  int tma;        // windows staged by TMA (else 16-byte vector loads)
+  int sao_i8;     // every SAO offset of the picture fits a signed byte (the packed offset tables)
   DPlane src[3];  // input planes (post-deblock)
   DPlane dst[3];  // output planes
   int bit_depth;
@@ -270,6 +277,13 @@ struct Pass2Args {
 };
 
 int launch_pass2(cudaStream_t st, const Pass2Args &a, bool do_sao, bool do_alf, uint64_t *launches);
+// Fills a.tmap / a.tma for the packed tile kernel's windows of a.src (plane
+// bases 16-byte aligned, strides multiples of 8 samples; otherwise a.tma = 0
+// and the kernel loads its windows itself).  Host only, allocates nothing.
+void pass2_tma_maps(Pass2Args &a);
+// Timeouts of the tile kernels' bounded waits since the last call (the
+// kernels leave such a tile unfiltered and count it): 0 when none.
+int pass2_wait_timeouts(uint32_t *count);
 // Packed 16x2 form; requires bit_depth <= 14, 4:2:0 or 4:0:0, coefficients in [-128, 127].
 int launch_pass2_packed(cudaStream_t st, const Pass2Args &a, bool do_sao, bool do_alf, uint64_t *launches);
 
