@@ -472,6 +472,21 @@ typedef struct h266_chain_plan h266_chain_plan;
 int h266_chain_plan_create(h266_ctx *ctx, const h266_picture *pic, const h266_in_loop_filter_args *args,
                            h266_chain_plan **out);
 int h266_chain_plan_execute(h266_ctx *ctx, h266_chain_plan *plan, h266_picture *pic);
+/* As h266_chain_plan_create, with flags.  H266_PLAN_DEVICE_SIDEINFO: the plan
+ * keeps the CU lists, motion and no-filter lines instead of the derived edge
+ * segments, and every execution derives the deblocking side information on
+ * the device first (the CU map and edge walk of apply_deblocking_clipped,
+ * src/deblock.rs:630-983, the work the crate does on every call), batched
+ * over the pictures of h266_chain_plan_execute_batch.  Pictures the device
+ * walk does not cover (4-sample CUs or transform blocks, sub-block grids,
+ * overlapping CUs, 4:2:2 / 4:4:4, no SAO / ALF) keep host-derived segments,
+ * as without the flag. */
+#define H266_PLAN_DEVICE_SIDEINFO 1u
+int h266_chain_plan_create_ex(h266_ctx *ctx, const h266_picture *pic, const h266_in_loop_filter_args *args,
+                              uint32_t flags, h266_chain_plan **out);
+/* 1 when the plan derives its side information on the device at every
+ * execution, 0 when it holds host-derived segments. */
+int h266_chain_plan_device_sideinfo(const h266_chain_plan *plan);
 /* Executes n plans on n device pictures (pics[i] with plans[i]; sizes may
  * differ) as one batch: one deblocking launch and one SAO / ALF launch per
  * kernel variant cover the tiles of every picture, so the GPU's tail between

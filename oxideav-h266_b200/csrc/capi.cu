@@ -153,6 +153,45 @@ struct BatchBufs {
     staged = done = nullptr;
   }
 };
+
+// One stream of the end-to-end batch pipeline (h266_apply_in_loop_filters_batch):
+// device buffers for a group of pictures -- copies of host planes, deblocked
+// planes, LMCS LUT, side information, walk scratch -- and the parameter tables
+// of the group's batched launches.  Groups rotate over the lanes, so one
+// group's uploads, another's kernels and a third one's downloads overlap.
+struct GroupSlot {
+  DevBuf io[3], scratch[3], lut, side, walk;
+  void release() {
+    for (int i = 0; i < 3; ++i) {
+      io[i].release();
+      scratch[i].release();
+    }
+    lut.release();
+    side.release();
+    walk.release();
+  }
+};
+struct GroupLane {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t mark = nullptr;
+  std::vector<GroupSlot> slots;
+  BatchBufs bb;
+  int init(size_t n_slots) {
+    H266_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    H266_CUDA(cudaEventCreateWithFlags(&mark, cudaEventDisableTiming));
+    slots.resize(n_slots);
+    return bb.init();
+  }
+  void release() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (GroupSlot &sl : slots) sl.release();
+    bb.release();
+    if (mark) cudaEventDestroy(mark);
+    if (stream) cudaStreamDestroy(stream);
+    mark = nullptr;
+    stream = nullptr;
+  }
+};
 }  // namespace h266
 
 struct h266_ctx {
@@ -171,6 +210,7 @@ struct h266_ctx {
   double prof_ms[H266_PROF_FAMILIES] = {0};
   uint64_t prof_n[H266_PROF_FAMILIES] = {0};
   h266::BatchBufs batch;  // parameter tables of h266_chain_plan_execute_batch
+  std::vector<std::unique_ptr<h266::GroupLane>> glanes;  // the end-to-end batch pipeline
   bool force_scalar = false;  // H266_FORCE_SCALAR_ALF=1: scalar SAO/ALF kernel (cross-checks)
   bool force_global_deblock = false;  // H266_FORCE_GLOBAL_DEBLOCK=1: deblocking on global memory (cross-checks)
   bool force_strip_deblock = false;   // H266_FORCE_STRIP_DEBLOCK=1: strip kernels instead of tiles (cross-checks)
@@ -774,6 +814,7 @@ struct h266_chain_plan {
   int device = 0;
   h266_picture geom{};  // plane sizes / bit depths the plan was built for
   h266::DevBuf side, lut, scratch[3];
+  h266::DevBuf walk;  // CU maps and segment grids of the device walk (db.device_walk)
   bool lmcs = false, pass2 = false;
   int deblock_bd = 8;
   Staged st;  // section offsets inside `side` (base unset)
@@ -781,6 +822,24 @@ struct h266_chain_plan {
   h266::Pass2Args args{};
   bool do_sao = false, do_alf = false, packed = false;
 };
+
+namespace h266 {
+// One picture of a batched chain execution: device planes P (filtered in
+// place), scratch planes S, its staged side information (st.base set), the
+// pass-2 arguments before binding, LUT and walk scratch.
+struct BatchItem {
+  DPlane P[3], S[3];
+  Staged st;
+  DbSide db;
+  Pass2Args args;
+  bool pass2 = false, do_sao = false, do_alf = false, packed = false;
+  const uint16_t *lut = nullptr;
+  int bd = 8;
+  uint8_t *walk = nullptr;
+};
+int exec_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, std::vector<BatchItem> &items);
+}  // namespace h266
+
 
 namespace {
 
@@ -1073,6 +1132,7 @@ int h266_ctx_destroy(h266_ctx *ctx) {
     cudaStreamSynchronize(l->stream);
     l->release();
   }
+  for (auto &l : ctx->glanes) l->release();
   ctx->main.release();
   ctx->pool.reset();
   for (auto &e : ctx->ev_pool) cudaEventDestroy(e);
@@ -1858,7 +1918,11 @@ int h266_apply_in_loop_filters(h266_ctx *ctx, h266_picture *pic, const h266_in_l
 // are complete on return.
 int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *const *pics,
                                      const h266_in_loop_filter_args *const *args) {
-  constexpr uint32_t kBatchLanes = 4;
+  // Groups of kGroup pictures rotate over kGroupLanes streams: per group the
+  // uploads (planes of host pictures, side information staged in pinned
+  // memory by the worker that prepared the picture), the LUTs, one batched
+  // execution (device walks, tile deblocking, SAO / ALF) and the downloads.
+  constexpr uint32_t kGroup = 4, kGroupLanes = 3;
   H266_TRY(check_ctx(ctx));
   if (n && (!pics || !args)) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL batch arrays");
   bool any_host = false;
@@ -1869,50 +1933,111 @@ int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *co
   }
   if (n <= 1) return n ? h266_apply_in_loop_filters(ctx, pics[0], args[0]) : H266_OK;
   Guard g(ctx->device);
-  const uint32_t n_lanes = std::min(n, kBatchLanes);
-  while (ctx->lanes.size() < n_lanes) {
-    std::unique_ptr<Lane> l(new Lane());
-    const int rc = l->init(nullptr);
+  const uint32_t n_groups = (n + kGroup - 1) / kGroup, n_lanes = std::min(n_groups, kGroupLanes);
+  while (ctx->glanes.size() < n_lanes) {
+    std::unique_ptr<GroupLane> l(new GroupLane());
+    const int rc = l->init(kGroup);
     if (rc != H266_OK) {
       l->release();
       return rc;
     }
-    ctx->lanes.push_back(std::move(l));
+    ctx->glanes.push_back(std::move(l));
   }
   H266_CUDA(cudaEventRecord(ctx->main.mark, ctx->stream));
-  for (uint32_t l = 0; l < n_lanes; ++l) H266_CUDA(cudaStreamWaitEvent(ctx->lanes[l]->stream, ctx->main.mark, 0));
+  for (uint32_t l = 0; l < n_lanes; ++l) H266_CUDA(cudaStreamWaitEvent(ctx->glanes[l]->stream, ctx->main.mark, 0));
   for (uint32_t i = 0; i < n; ++i) ctx_prep(ctx, i + 1);
   TaskPool *pool = ctx_pool(ctx);
   const int device = ctx->device;
+  const bool allow_dev = device_sideinfo_allowed(ctx);
   pool->start(n, [&](size_t i) {
     Prep &pr = *ctx->preps[i + 1];
     pr.staged_pinned = false;
-    pr.rc = prepare_chain(pr, *pics[i], *args[i], nullptr, device_sideinfo_allowed(ctx));
+    pr.rc = prepare_chain(pr, *pics[i], *args[i], nullptr, allow_dev);
     if (pr.rc == H266_OK && cudaSetDevice(device) == cudaSuccess) pr.rc = pr.stage();
     if (pr.rc != H266_OK) pr.msg = h266_last_error();
   });
-  int rc = H266_OK;
-  for (uint32_t i = 0; i < n && rc == H266_OK; ++i) {
-    pool->wait_item(i);
-    Prep &pr = *ctx->preps[i + 1];
-    if (pr.rc != H266_OK) {
-      rc = set_error(pr.rc, pr.msg);
-      break;
+  auto run_group = [&](uint32_t gi) -> int {
+    GroupLane &L = *ctx->glanes[gi % n_lanes];
+    std::vector<BatchItem> items;
+    const uint32_t i0 = gi * kGroup, i1 = std::min(n, i0 + kGroup);
+    for (uint32_t i = i0; i < i1; ++i) {
+      pool->wait_item(i);
+      Prep &pr = *ctx->preps[i + 1];
+      if (pr.rc != H266_OK) return set_error(pr.rc, pr.msg);
+      GroupSlot &sl = L.slots[i - i0];
+      const h266_picture &pic = *pics[i];
+      const h266_in_loop_filter_args &a = *args[i];
+      BatchItem it;
+      const h266_plane *pl[3] = {&pic.luma, &pic.cb, &pic.cr};
+      for (int k = 0; k < 3; ++k) {
+        const h266_plane &q = *pl[k];
+        if (pic.mem == H266_MEM_DEVICE || (uint64_t)q.width * q.height == 0) {
+          it.P[k] = dplane(q, q.samples, (int64_t)std::max<uint64_t>(q.stride, 1));
+          continue;
+        }
+        const size_t row = (size_t)q.width * 2;
+        H266_TRY(sl.io[k].ensure(row * q.height));
+        H266_CUDA(cudaMemcpy2DAsync(sl.io[k].ptr, row, q.samples, (size_t)q.stride * 2, row, q.height,
+                                    cudaMemcpyHostToDevice, L.stream));
+        it.P[k] = dplane(q, sl.io[k].as<uint16_t>(), q.width);
+      }
+      H266_TRY(sl.side.ensure(pr.blob.size()));
+      H266_CUDA(cudaMemcpyAsync(sl.side.ptr, pr.pinned.ptr, pr.blob.size(), cudaMemcpyHostToDevice, L.stream));
+      H266_CUDA(cudaEventRecord(pr.uploaded, L.stream));
+      ctx->h2d_bytes += pr.blob.size() + host_plane_bytes(pic);
+      it.st = pr.st;
+      it.st.base = sl.side.as<uint8_t>();
+      it.db = pr.db;
+      it.args = pr.h.args;
+      it.pass2 = pr.h.do_sao || pr.h.do_alf;
+      it.do_sao = pr.h.do_sao;
+      it.do_alf = pr.h.do_alf;
+      it.packed = pr.h.packed;
+      it.bd = (int)a.deblock.bit_depth;
+      if (a.lmcs) {
+        H266_TRY(sl.lut.ensure(65536 * 2));
+        H266_TRY(build_lut(ctx, L.stream, sl.lut.as<uint16_t>(), *a.lmcs, a.lmcs_min_bin_idx, a.lmcs_max_bin_idx));
+        it.lut = sl.lut.as<uint16_t>();
+      }
+      for (int k = 0; k < 3; ++k) {
+        if (it.pass2) {
+          const size_t np = (size_t)std::max(it.P[k].w, 0) * std::max(it.P[k].h, 0);
+          H266_TRY(sl.scratch[k].ensure(std::max<size_t>(np, 1) * 2));
+        }
+        it.S[k] = DPlane{it.pass2 ? sl.scratch[k].as<uint16_t>() : nullptr, std::max(it.P[k].w, 1), it.P[k].w,
+                         it.P[k].h};
+      }
+      if (pr.db.device_walk) {
+        H266_TRY(sl.walk.ensure(device_walk_bytes(pr.db.dw)));
+        it.walk = sl.walk.as<uint8_t>();
+      }
+      items.push_back(it);
     }
-    Lane &ln = *ctx->lanes[i % n_lanes];
-    DPlane P[3];
-    rc = picture_to_device(ln, *pics[i], P);
-    if (rc == H266_OK) rc = issue_chain(ctx, ln, pr, P, *args[i]);
-    if (rc == H266_OK) rc = picture_from_device(ln, *pics[i], false);
-    ctx->h2d_bytes += host_plane_bytes(*pics[i]);
-    ctx->d2h_bytes += host_plane_bytes(*pics[i]);
-  }
+    H266_TRY(exec_batch(ctx, L.bb, L.stream, items));
+    for (uint32_t i = i0; i < i1; ++i) {
+      const h266_picture &pic = *pics[i];
+      if (pic.mem == H266_MEM_DEVICE) continue;
+      GroupSlot &sl = L.slots[i - i0];
+      const h266_plane *pl[3] = {&pic.luma, &pic.cb, &pic.cr};
+      for (int k = 0; k < 3; ++k) {
+        const h266_plane &q = *pl[k];
+        if ((uint64_t)q.width * q.height == 0) continue;
+        const size_t row = (size_t)q.width * 2;
+        H266_CUDA(cudaMemcpy2DAsync(q.samples, (size_t)q.stride * 2, sl.io[k].ptr, row, row, q.height,
+                                    cudaMemcpyDeviceToHost, L.stream));
+      }
+      ctx->d2h_bytes += host_plane_bytes(pic);
+    }
+    return H266_OK;
+  };
+  int rc = H266_OK;
+  for (uint32_t gi = 0; gi < n_groups && rc == H266_OK; ++gi) rc = run_group(gi);
   pool->wait_all();
   for (uint32_t l = 0; l < n_lanes; ++l) {
-    Lane &ln = *ctx->lanes[l];
-    H266_CUDA(cudaEventRecord(ln.mark, ln.stream));
-    H266_CUDA(cudaStreamWaitEvent(ctx->stream, ln.mark, 0));
-    if (any_host || rc != H266_OK) H266_CUDA(cudaStreamSynchronize(ln.stream));
+    GroupLane &L = *ctx->glanes[l];
+    H266_CUDA(cudaEventRecord(L.mark, L.stream));
+    H266_CUDA(cudaStreamWaitEvent(ctx->stream, L.mark, 0));
+    if (any_host || rc != H266_OK) H266_CUDA(cudaStreamSynchronize(L.stream));
   }
   return rc;
 }
@@ -1947,7 +2072,15 @@ int h266_ctx_profile(h266_ctx *ctx, double ms[H266_PROF_FAMILIES], uint64_t laun
 
 int h266_chain_plan_create(h266_ctx *ctx, const h266_picture *pic, const h266_in_loop_filter_args *args,
                            h266_chain_plan **out) {
+  return h266_chain_plan_create_ex(ctx, pic, args, 0, out);
+}
+
+int h266_chain_plan_device_sideinfo(const h266_chain_plan *plan) { return plan && plan->db.device_walk ? 1 : 0; }
+
+int h266_chain_plan_create_ex(h266_ctx *ctx, const h266_picture *pic, const h266_in_loop_filter_args *args,
+                              uint32_t flags, h266_chain_plan **out) {
   H266_TRY(check_ctx(ctx));
+  if (flags & ~H266_PLAN_DEVICE_SIDEINFO) return set_error(H266_ERR_INVALID_ARGUMENT, "unknown plan flags");
   if (!out || !args) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL argument");
   *out = nullptr;
   if (!pic) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL picture");
@@ -1961,7 +2094,8 @@ int h266_chain_plan_create(h266_ctx *ctx, const h266_picture *pic, const h266_in
   H266_TRY(check_picture(&geom));
   Guard g(ctx->device);
   Prep &pr = ctx_prep(ctx, 0);
-  H266_TRY(prepare_chain(pr, geom, *args, ctx_pool(ctx)));
+  H266_TRY(prepare_chain(pr, geom, *args, ctx_pool(ctx),
+                         (flags & H266_PLAN_DEVICE_SIDEINFO) != 0 && device_sideinfo_allowed(ctx)));
   h266_chain_plan *pl = new h266_chain_plan();
   pl->device = ctx->device;
   pl->geom = geom;
@@ -1987,6 +2121,7 @@ int h266_chain_plan_create(h266_ctx *ctx, const h266_picture *pic, const h266_in
       if ((rc = pl->scratch[i].ensure(std::max<size_t>((size_t)sp[i]->width * sp[i]->height, 1) * 2)) != H266_OK)
         return fail(rc);
   }
+  if (pr.db.device_walk && (rc = pl->walk.ensure(device_walk_bytes(pr.db.dw))) != H266_OK) return fail(rc);
   pl->deblock_bd = (int)args->deblock.bit_depth;
   pl->db = pr.db;
   pl->st = pr.st;
@@ -2021,7 +2156,7 @@ int h266_chain_plan_execute(h266_ctx *ctx, h266_chain_plan *plan, h266_picture *
   h.do_alf = plan->do_alf;
   h.packed = plan->packed;
   return exec_chain(ctx, ctx->stream, st.base, st, plan->db, h, plan->lmcs ? plan->lut.as<uint16_t>() : nullptr,
-                    plan->deblock_bd, P, S);
+                    plan->deblock_bd, P, S, plan->walk.as<uint8_t>());
 }
 
 }  // extern "C"
@@ -2040,36 +2175,49 @@ int check_plan_batch(h266_ctx *ctx, uint32_t n, h266_chain_plan *const *plans, h
   return H266_OK;
 }
 
-// Queues a batch of plan executions on `stream` with its parameter tables in
-// `bb`; the caller has checked the batch and made the device current.
-int exec_plan_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, uint32_t n, h266_chain_plan *const *plans,
-                    h266_picture *const *pics) {
+
+// Queues a batch of chain executions on `stream` with its parameter tables in
+// `bb`: the device walks of the pictures that derive their side information
+// on the device (three launches for all of them), one tile-deblocking launch
+// and one SAO/ALF launch per kernel variant over every picture's tiles, and
+// per picture whatever the batched kernels do not take.
+int exec_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, std::vector<BatchItem> &items) {
+  const uint32_t n = (uint32_t)items.size();
   if (!n) return H266_OK;
   H266_TRY(bb.init());
-  // Per picture: device views, and which part runs batched.
-  struct Item {
-    DPlane P[3], S[3];
-    Staged st;
+  struct Run {
     bool tile, packed;
     int variant;
   };
-  std::vector<Item> items(n);
-  std::vector<uint8_t> tile_params;
-  std::vector<uint32_t> tile_first(1, 0);
+  std::vector<Run> runs(n);
+  std::vector<uint8_t> tile_params, walk_items;
+  std::vector<uint32_t> tile_first(1, 0), walk_first[3] = {{0}, {0}, {0}};  // clear, CU map, walk CTAs
+  WalkBatchCounts walk_total;
+  const size_t wis = walk_batch_item_size();
   std::vector<Pass2Args> p2[8];
   std::vector<uint32_t> p2_first[8];
   const size_t tps = deblock_tile_params_size();
   for (uint32_t i = 0; i < n; ++i) {
-    const h266_chain_plan &pl = *plans[i];
-    Item &it = items[i];
-    H266_TRY(picture_to_device(ctx->main, *pics[i], it.P));
-    for (int k = 0; k < 3; ++k)
-      it.S[k] = DPlane{pl.pass2 ? pl.scratch[k].as<uint16_t>() : nullptr, std::max(it.P[k].w, 1), it.P[k].w, it.P[k].h};
-    it.st = pl.st;
-    it.st.base = pl.side.as<uint8_t>();
+    BatchItem &it = items[i];
+    Run &r = runs[i];
     const uint8_t *base = it.st.base;
-    it.tile = pl.pass2 && pl.db.tiles_ok && !ctx->force_global_deblock && !ctx->force_strip_deblock;
-    if (it.tile) {
+    r.tile = it.pass2 && (it.db.tiles_ok || it.db.device_walk) && !ctx->force_global_deblock &&
+             !ctx->force_strip_deblock;
+    if (r.tile && it.db.device_walk) {  // the side information is derived on the device first, batched
+      DeviceWalkOut g;
+      WalkBatchCounts c;
+      walk_items.resize(walk_items.size() + wis);
+      fill_walk_batch_item(walk_items.data() + walk_items.size() - wis, device_walk_in(base, it.st, it.db), it.walk, g,
+                           c);
+      walk_first[0].push_back(walk_first[0].back() + c.clear_ctas);
+      walk_first[1].push_back(walk_first[1].back() + c.grid_ctas);
+      walk_first[2].push_back(walk_first[2].back() + c.walk_ctas);
+      walk_total.offsets = std::max(walk_total.offsets, c.offsets);
+      tile_params.resize(tile_params.size() + tps);
+      const uint32_t tc =
+          fill_deblock_tile_params_grid(tile_params.data() + tile_params.size() - tps, it.P, it.S, it.lut, it.bd, g);
+      tile_first.push_back(tile_first.back() + tc);
+    } else if (r.tile) {
       const StripSide v{reinterpret_cast<const EdgeSeg *>(base + it.st.seg[0]),
                         reinterpret_cast<const uint32_t *>(base + it.st.comp[0]),
                         reinterpret_cast<const uint32_t *>(base + it.st.band[0])};
@@ -2077,22 +2225,21 @@ int exec_plan_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, uint32_t 
                         reinterpret_cast<const uint32_t *>(base + it.st.comp[1]),
                         reinterpret_cast<const uint32_t *>(base + it.st.band[1])};
       tile_params.resize(tile_params.size() + tps);
-      const uint32_t c = fill_deblock_tile_params(tile_params.data() + tile_params.size() - tps, it.P, it.S,
-                                                  pl.lmcs ? pl.lut.as<uint16_t>() : nullptr, pl.deblock_bd, v, h,
-                                                  reinterpret_cast<const uint32_t *>(base + it.st.tile_bounds),
-                                                  pl.db.tb_off, pl.db.n_bands, pl.db.tiles_x, pl.db.tiles_y);
+      const uint32_t c = fill_deblock_tile_params(tile_params.data() + tile_params.size() - tps, it.P, it.S, it.lut,
+                                                  it.bd, v, h, reinterpret_cast<const uint32_t *>(base + it.st.tile_bounds),
+                                                  it.db.tb_off, it.db.n_bands, it.db.tiles_x, it.db.tiles_y);
       tile_first.push_back(tile_first.back() + c);
     }
-    it.packed = pl.pass2 && pl.packed && !ctx->force_scalar;
-    it.variant = -1;
-    if (it.packed) {
-      Pass2Args a = pl.args;
+    r.packed = it.pass2 && it.packed && !ctx->force_scalar;
+    r.variant = -1;
+    if (r.packed) {
+      Pass2Args a = it.args;
       bind_pass2(a, base, it.st, it.S, it.P);
       uint32_t c = 0;
-      it.variant = pass2_packed_variant(a, pl.do_sao, pl.do_alf, &c);
-      if (p2_first[it.variant].empty()) p2_first[it.variant].push_back(0);
-      p2[it.variant].push_back(a);
-      p2_first[it.variant].push_back(p2_first[it.variant].back() + c);
+      r.variant = pass2_packed_variant(a, it.do_sao, it.do_alf, &c);
+      if (p2_first[r.variant].empty()) p2_first[r.variant].push_back(0);
+      p2[r.variant].push_back(a);
+      p2_first[r.variant].push_back(p2_first[r.variant].back() + c);
     }
   }
   // one upload of every batched launch's parameter table
@@ -2101,6 +2248,9 @@ int exec_plan_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, uint32_t 
   Blob blob{b};
   const size_t off_tp = blob.put(tile_params.data(), tile_params.size());
   const size_t off_tf = blob.put(tile_first.data(), tile_first.size() * sizeof(uint32_t));
+  const size_t off_wi = blob.put(walk_items.data(), walk_items.size());
+  size_t off_wf[3];
+  for (int k = 0; k < 3; ++k) off_wf[k] = blob.put(walk_first[k].data(), walk_first[k].size() * sizeof(uint32_t));
   size_t off_p2[8] = {0}, off_p2f[8] = {0};
   for (int v = 0; v < 8; ++v)
     if (!p2[v].empty()) {
@@ -2115,14 +2265,22 @@ int exec_plan_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, uint32_t 
   H266_CUDA(cudaMemcpyAsync(bb.side.ptr, bb.stage.ptr, b.size(), cudaMemcpyHostToDevice, stream));
   H266_CUDA(cudaEventRecord(bb.staged, stream));
   const uint8_t *dside = bb.side.as<uint8_t>();
-  // deblocking: per picture where the tile kernel does not apply, then one batched launch
+  // deblocking: per picture where the tile kernel does not apply, then the batched walks and tiles
   for (uint32_t i = 0; i < n; ++i) {
-    const h266_chain_plan &pl = *plans[i];
-    Item &it = items[i];
-    if (it.tile) continue;
-    const uint16_t *lut = pl.lmcs ? pl.lut.as<uint16_t>() : nullptr;
-    if (pl.pass2) H266_TRY(run_deblock(ctx, stream, it.st.base, it.st, pl.db, it.P, it.S, lut, pl.deblock_bd));
-    else H266_TRY(run_deblock(ctx, stream, it.st.base, it.st, pl.db, it.P, it.P, lut, pl.deblock_bd));
+    BatchItem &it = items[i];
+    if (runs[i].tile) continue;
+    if (it.pass2) H266_TRY(run_deblock(ctx, stream, it.st.base, it.st, it.db, it.P, it.S, it.lut, it.bd, it.walk));
+    else H266_TRY(run_deblock(ctx, stream, it.st.base, it.st, it.db, it.P, it.P, it.lut, it.bd, it.walk));
+  }
+  if (walk_first[0].size() > 1) {
+    walk_total.clear_ctas = walk_first[0].back();
+    walk_total.grid_ctas = walk_first[1].back();
+    walk_total.walk_ctas = walk_first[2].back();
+    Prof pf(ctx, stream, H266_PROF_DEBLOCK);
+    H266_TRY(launch_walk_batch(stream, dside + off_wi, reinterpret_cast<const uint32_t *>(dside + off_wf[0]),
+                               reinterpret_cast<const uint32_t *>(dside + off_wf[1]),
+                               reinterpret_cast<const uint32_t *>(dside + off_wf[2]), (int)walk_first[0].size() - 1,
+                               walk_total, &ctx->launches));
   }
   if (tile_first.size() > 1) {
     Prof pf(ctx, stream, H266_PROF_DEBLOCK);
@@ -2131,10 +2289,9 @@ int exec_plan_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, uint32_t 
   }
   // SAO / ALF: per picture where the packed kernel does not apply, then one launch per variant
   for (uint32_t i = 0; i < n; ++i) {
-    const h266_chain_plan &pl = *plans[i];
-    Item &it = items[i];
-    if (!pl.pass2 || it.packed) continue;
-    H266_TRY(run_pass2(ctx, stream, pl.args, pl.do_sao, pl.do_alf, pl.packed, it.st.base, it.st, it.S, it.P));
+    BatchItem &it = items[i];
+    if (!it.pass2 || runs[i].packed) continue;
+    H266_TRY(run_pass2(ctx, stream, it.args, it.do_sao, it.do_alf, it.packed, it.st.base, it.st, it.S, it.P));
   }
   for (int v = 0; v < 8; ++v)
     if (!p2[v].empty()) {
@@ -2145,6 +2302,33 @@ int exec_plan_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, uint32_t 
     }
   H266_CUDA(cudaEventRecord(bb.done, stream));
   return H266_OK;
+}
+
+// Queues a batch of plan executions on `stream` with its parameter tables in
+// `bb`; the caller has checked the batch and made the device current.
+int exec_plan_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, uint32_t n, h266_chain_plan *const *plans,
+                    h266_picture *const *pics) {
+  if (!n) return H266_OK;
+  std::vector<BatchItem> items(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    const h266_chain_plan &pl = *plans[i];
+    BatchItem &it = items[i];
+    H266_TRY(picture_to_device(ctx->main, *pics[i], it.P));
+    for (int k = 0; k < 3; ++k)
+      it.S[k] = DPlane{pl.pass2 ? pl.scratch[k].as<uint16_t>() : nullptr, std::max(it.P[k].w, 1), it.P[k].w, it.P[k].h};
+    it.st = pl.st;
+    it.st.base = pl.side.as<uint8_t>();
+    it.db = pl.db;
+    it.args = pl.args;
+    it.pass2 = pl.pass2;
+    it.do_sao = pl.do_sao;
+    it.do_alf = pl.do_alf;
+    it.packed = pl.packed;
+    it.lut = pl.lmcs ? pl.lut.as<uint16_t>() : nullptr;
+    it.bd = pl.deblock_bd;
+    it.walk = pl.walk.as<uint8_t>();
+  }
+  return exec_batch(ctx, bb, stream, items);
 }
 }  // namespace h266
 
@@ -2164,6 +2348,7 @@ int h266_chain_plan_destroy(h266_chain_plan *plan) {
   Guard g(plan->device);
   plan->side.release();
   plan->lut.release();
+  plan->walk.release();
   for (auto &b : plan->scratch) b.release();
   delete plan;
   return H266_OK;

@@ -2058,10 +2058,12 @@ WalkLayout walk_layout(const DeviceWalkIn &in) {
 
 size_t device_walk_bytes(const DeviceWalkIn &in) { return walk_layout(in).total; }
 
-int launch_device_walk(cudaStream_t st, const DeviceWalkIn &in, uint8_t *scratch, DeviceWalkOut &out,
-                       uint64_t *launches) {
-  const WalkLayout L = walk_layout(in);
-  WalkParams a;
+namespace {
+
+// The walk's parameters of one picture (CU maps and segment grids in
+// `scratch`, laid out by walk_layout) and the grids the tile kernel scans.
+void fill_walk(const DeviceWalkIn &in, uint8_t *scratch, WalkParams &a, DeviceWalkOut &out, WalkLayout &L) {
+  L = walk_layout(in);
   std::memset(&a, 0, sizeof a);
   const bool sep = in.chroma_cus != in.cus;
   a.cus[0] = in.cus;
@@ -2098,6 +2100,16 @@ int launch_device_walk(cudaStream_t st, const DeviceWalkIn &in, uint8_t *scratch
     }
   out.tiles_x = (uint32_t)((in.w + kDeblockTile - 1) / kDeblockTile);
   out.tiles_y = (uint32_t)((in.h + kDeblockTile - 1) / kDeblockTile);
+}
+
+}  // namespace
+
+int launch_device_walk(cudaStream_t st, const DeviceWalkIn &in, uint8_t *scratch, DeviceWalkOut &out,
+                       uint64_t *launches) {
+  WalkParams a;
+  WalkLayout L;
+  fill_walk(in, scratch, a, out, L);
+  const bool sep = in.chroma_cus != in.cus;
   // CU maps to -1 (no CU), segment grids to bS 0 (no segment)
   const size_t cells = (size_t)a.cw4 * a.ch4;
   H266_CUDA(cudaMemsetAsync(a.cu_grid[0], 0xFF, cells * 4, st));
@@ -2120,6 +2132,160 @@ int launch_device_walk(cudaStream_t st, const DeviceWalkIn &in, uint8_t *scratch
     ++*launches;
   }
   return H266_OK;
+}
+
+// ---------------------------------------------------------------- batched device walk
+//
+// The walks of many pictures in three launches: the clearing of every
+// picture's CU maps (-1) and segment grids (bS 0), the CU maps, and the edge
+// walk.  Per picture a WalkBatchItem (parameters, clear extents, the walk's
+// list count and offsets); CTAs find their picture by binary search over
+// per-launch prefix tables of CTA counts.
+struct WalkBatchItem {
+  WalkParams p;
+  uint4 *clear;            // the picture's walk scratch
+  uint32_t ff_vec, zero_vec;  // 16-byte words set to all ones, then to zero
+  uint32_t lists;          // (plane, pass) lists of the walk: 6, or 2 without chroma
+  uint32_t cu_lists;       // CU maps built: 1, or 2 for a separate chroma tree
+};
+
+namespace {
+
+__device__ __forceinline__ int batch_pick(const uint32_t *first, int n, uint32_t b) {
+  int lo = 0, hi = n;  // first[lo] <= b < first[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (first[mid] <= b) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+constexpr int kClearVecPerCta = 256 * 8;
+
+__global__ void __launch_bounds__(256) k_walk_clear_batch(const WalkBatchItem *__restrict__ items,
+                                                          const uint32_t *__restrict__ first, int n) {
+  const int p = batch_pick(first, n, blockIdx.x);
+  const WalkBatchItem &it = items[p];
+  const uint32_t base = (blockIdx.x - first[p]) * kClearVecPerCta, total = it.ff_vec + it.zero_vec;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const uint32_t i = base + k * 256 + threadIdx.x;
+    if (i < total) it.clear[i] = i < it.ff_vec ? make_uint4(~0u, ~0u, ~0u, ~0u) : make_uint4(0, 0, 0, 0);
+  }
+}
+
+__global__ void __launch_bounds__(128) k_cu_grid_batch(const WalkBatchItem *__restrict__ items,
+                                                       const uint32_t *__restrict__ first, int n) {
+  const int p = batch_pick(first, n, blockIdx.x);
+  const WalkParams &a = items[p].p;
+  const uint32_t lb = blockIdx.x - first[p], b0 = (a.n[0] + 127) / 128;
+  const int list = lb < b0 ? 0 : 1;
+  const uint32_t i = (lb - (list ? b0 : 0)) * 128 + threadIdx.x;
+  if (i >= a.n[list]) return;
+  const h266_deblock_cu &c = a.cus[list][i];
+  const int x0 = c.x / 4, y0 = c.y / 4;
+  const int x1 = min((int)((c.x + c.w + 3) / 4), a.cw4), y1 = min((int)((c.y + c.h + 3) / 4), a.ch4);
+  for (int y = y0; y < y1; ++y)
+    for (int x = x0; x < x1; ++x) atomicMax(&a.cu_grid[list][(size_t)y * a.cw4 + x], (int32_t)i);
+}
+
+// blockIdx.y = plane * 2 + pass, blockIdx.z = edge offset / step, as k_walk.
+__global__ void __launch_bounds__(128) k_walk_batch(const WalkBatchItem *__restrict__ items,
+                                                    const uint32_t *__restrict__ first, int n) {
+  __shared__ WalkParams s;
+  const int p = batch_pick(first, n, blockIdx.x);
+  if (blockIdx.y >= items[p].lists) return;  // uniform per CTA
+  static_assert(sizeof(WalkParams) % 4 == 0, "word copy");
+  const uint32_t *src = reinterpret_cast<const uint32_t *>(&items[p].p);
+  uint32_t *dst = reinterpret_cast<uint32_t *>(&s);
+  for (int i = threadIdx.x; i < (int)(sizeof(WalkParams) / 4); i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+  const WalkParams &a = s;
+  const int l = blockIdx.y, plane = l / 2, d = l % 2;
+  const int list = plane ? 1 : 0;
+  const uint32_t i = (blockIdx.x - first[p]) * blockDim.x + threadIdx.x;
+  if (i >= a.n[list]) return;
+  const h266_deblock_cu &cu = a.cus[list][i];
+  const uint32_t step = plane ? 8 * (d == 0 ? a.cfg[plane].sub_w : a.cfg[plane].sub_h) : 4;
+  const uint32_t off = blockIdx.z * step;
+  if (off >= (d == 0 ? cu.w : cu.h)) return;
+  const DevCuGrid grid{a.cu_grid[list], a.cw4, a.ch4};
+  GridEmit emit{a.grid[d][plane], a.slots[d][plane], a.bands[d][plane], plane ? 2 : 4, plane ? 8 : 4};
+  if (plane == 0 && a.has_mv && a.mv_per_cu) {
+    const CuMotion mv{&a.mv, a.mv_per_cu, DevCuGrid{a.cu_grid[0], a.cw4, a.ch4}};
+    walk_cu(a.cus[list], grid, a.cfg[plane], d == 0, mv, a.nf[d], a.n_nf[d], i, emit, (int)off);
+  } else {
+    const MvGrid mv{plane == 0 && a.has_mv ? &a.mv : nullptr};
+    walk_cu(a.cus[list], grid, a.cfg[plane], d == 0, mv, a.nf[d], a.n_nf[d], i, emit, (int)off);
+  }
+}
+
+}  // namespace
+
+size_t walk_batch_item_size() { return sizeof(WalkBatchItem); }
+
+void fill_walk_batch_item(void *out, const DeviceWalkIn &in, uint8_t *scratch, DeviceWalkOut &g, WalkBatchCounts &c) {
+  WalkBatchItem it;
+  std::memset(&it, 0, sizeof it);
+  WalkLayout L;
+  fill_walk(in, scratch, it.p, g, L);
+  const bool sep = in.chroma_cus != in.cus;
+  it.clear = reinterpret_cast<uint4 *>(scratch);
+  it.ff_vec = (uint32_t)(L.grid[0][0] / 16);  // the CU maps precede the grids (256-byte sections)
+  it.zero_vec = (uint32_t)((L.total - L.grid[0][0]) / 16);
+  it.lists = in.cfi != 0 ? 6 : 2;
+  it.cu_lists = sep && in.cfi != 0 ? 2 : 1;
+  c.clear_ctas = (it.ff_vec + it.zero_vec + kClearVecPerCta - 1) / kClearVecPerCta;
+  c.grid_ctas = (it.p.n[0] + 127) / 128 + (it.cu_lists == 2 ? (it.p.n[1] + 127) / 128 : 0);
+  c.walk_ctas = (std::max(it.p.n[0], it.p.n[1]) + 127) / 128;
+  c.offsets = (std::max<uint32_t>(4, in.max_cu_dim) + 3) / 4;
+  std::memcpy(out, &it, sizeof it);
+}
+
+int launch_walk_batch(cudaStream_t st, const void *d_items, const uint32_t *d_first_clear,
+                      const uint32_t *d_first_grid, const uint32_t *d_first_walk, int n, const WalkBatchCounts &total,
+                      uint64_t *launches) {
+  if (n <= 0) return H266_OK;
+  const WalkBatchItem *items = static_cast<const WalkBatchItem *>(d_items);
+  if (total.clear_ctas) {
+    k_walk_clear_batch<<<total.clear_ctas, 256, 0, st>>>(items, d_first_clear, n);
+    H266_CUDA(cudaGetLastError());
+    ++*launches;
+  }
+  if (total.grid_ctas) {
+    k_cu_grid_batch<<<total.grid_ctas, 128, 0, st>>>(items, d_first_grid, n);
+    H266_CUDA(cudaGetLastError());
+    ++*launches;
+  }
+  if (total.walk_ctas) {
+    k_walk_batch<<<dim3(total.walk_ctas, 6, total.offsets), 128, 0, st>>>(items, d_first_walk, n);
+    H266_CUDA(cudaGetLastError());
+    ++*launches;
+  }
+  return H266_OK;
+}
+
+uint32_t fill_deblock_tile_params_grid(void *out, const DPlane src[3], const DPlane dst[3], const uint16_t *lut,
+                                       int bit_depth, const DeviceWalkOut &g) {
+  TileParams a;
+  std::memset(&a, 0, sizeof a);
+  for (int i = 0; i < 3; ++i) {
+    a.src[i] = src[i];
+    a.dst[i] = dst[i];
+    for (int d = 0; d < 2; ++d) {
+      a.n_bands[d][i] = g.bands[d][i];
+      a.grid[d][i] = g.grid[d][i];
+      a.grid_slots[d][i] = g.slots[d][i];
+    }
+  }
+  a.grid_mode = 1;
+  a.lut = lut;
+  a.tiles_x = g.tiles_x;
+  a.tiles_y = g.tiles_y;
+  a.maxv = (1 << bit_depth) - 1;
+  std::memcpy(out, &a, sizeof a);
+  return g.tiles_x * g.tiles_y;
 }
 
 int launch_deblock_tiles_grid(cudaStream_t st, const DPlane src[3], const DPlane dst[3], const uint16_t *lut,

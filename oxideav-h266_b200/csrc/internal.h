@@ -211,6 +211,22 @@ int launch_device_walk(cudaStream_t st, const DeviceWalkIn &in, uint8_t *scratch
                        uint64_t *launches);
 int launch_deblock_tiles_grid(cudaStream_t st, const DPlane src[3], const DPlane dst[3], const uint16_t *lut,
                               int bit_depth, const DeviceWalkOut &g, uint64_t *launches);
+// Batched device walk: fill_walk_batch_item writes one picture's item
+// (walk_batch_item_size() bytes) and its CTA counts per launch; the prefix
+// sums of those counts over the batch's pictures (n + 1 entries each) select
+// the picture of a CTA.  The three launches clear the pictures' scratch, build
+// the CU maps and walk the edges; the grid-mode tile parameters of each
+// picture then go into a batched tile launch like any other.
+struct WalkBatchCounts {
+  uint32_t clear_ctas = 0, grid_ctas = 0, walk_ctas = 0, offsets = 0;  // offsets: the largest, over the batch
+};
+size_t walk_batch_item_size();
+void fill_walk_batch_item(void *out, const DeviceWalkIn &in, uint8_t *scratch, DeviceWalkOut &g, WalkBatchCounts &c);
+int launch_walk_batch(cudaStream_t st, const void *d_items, const uint32_t *d_first_clear,
+                      const uint32_t *d_first_grid, const uint32_t *d_first_walk, int n, const WalkBatchCounts &total,
+                      uint64_t *launches);
+uint32_t fill_deblock_tile_params_grid(void *out, const DPlane src[3], const DPlane dst[3], const uint16_t *lut,
+                                       int bit_depth, const DeviceWalkOut &g);
 int launch_deblock(cudaStream_t st, const DPlane planes[3], int bit_depth, const EdgeSeg *d_segs_v,
                    const uint32_t *d_comp_v, uint32_t n_comp_v, const EdgeSeg *d_segs_h, const uint32_t *d_comp_h,
                    uint32_t n_comp_h, uint64_t *launches);

@@ -668,11 +668,11 @@ __device__ __forceinline__ void sao_alf_tile3(const Pass2Args &a, const Pass2Arg
   const int b = tid / TPB;
   const int bx = b % (W / 4), by = b / (W / 4);
   const uint32_t *tab = a.tables.luma_packed + ((size_t)me->luma_set * 100 + sm.cls_f[b] * 4 + sm.cls_t[b]) * 36;
-  uint32_t c2[12], nc2[12], f[12];
+  // clip values and coefficients in registers (the negated clips are formed per use: fewer live registers)
+  uint32_t c2[12], f[12];
 #pragma unroll
   for (int k = 0; k < 12; ++k) {
     c2[k] = __ldg(tab + 3 * k);
-    nc2[k] = __ldg(tab + 3 * k + 1);
     f[k] = __ldg(tab + 3 * k + 2);
   }
   const int gx = X0 + 4 * bx;
@@ -690,10 +690,11 @@ __device__ __forceinline__ void sao_alf_tile3(const Pass2Args &a, const Pass2Arg
     Words<6, 2> ru, rd;
     auto tap = [&](const Words<6, 2> &up, const Words<6, 2> &dn, auto dx, int k) {
       constexpr int DX = decltype(dx)::value;
+      const uint32_t nc = neg2(c2[k]);
       static_for<2>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
-        const uint32_t x = clipd(up.template pair<DX + 2 * q>(), ncur[q], c2[k], nc2[k]);
-        const uint32_t y = clipd(dn.template pair<-DX + 2 * q>(), ncur[q], c2[k], nc2[k]);
+        const uint32_t x = clipd(up.template pair<DX + 2 * q>(), ncur[q], c2[k], nc);
+        const uint32_t y = clipd(dn.template pair<-DX + 2 * q>(), ncur[q], c2[k], nc);
         const uint32_t s = add2(x, y);
         acc[2 * q] = __dp2a_lo((int)s, (int)f[k], acc[2 * q]);
         acc[2 * q + 1] = __dp2a_hi((int)s, (int)f[k], acc[2 * q + 1]);

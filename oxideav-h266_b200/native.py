@@ -33,6 +33,7 @@ EXPORTS = [
     "h266_apply_deblocking_clipped",
     "h266_apply_sao_clipped", "h266_apply_alf_clipped", "h266_apply_in_loop_filters",
     "h266_apply_in_loop_filters_batch", "h266_ctx_set_profiling", "h266_ctx_profile", "h266_chain_plan_create",
+    "h266_chain_plan_create_ex", "h266_chain_plan_device_sideinfo",
     "h266_chain_plan_execute", "h266_chain_plan_execute_batch", "h266_chain_plan_destroy",
     "h266_apply_in_loop_filters_noalloc", "h266_server_create", "h266_server_submit", "h266_server_wait",
     "h266_server_stats", "h266_server_replay", "h266_server_destroy", "h266_alf_decide_and_apply_clipped",
@@ -41,6 +42,7 @@ EXPORTS = [
     "h266_cc_alf_decide_and_apply_clipped", "h266_sao_chroma_merge",
 ]
 PROF_FAMILIES = ("lmcs", "deblock", "sao_alf", "copy")
+PLAN_DEVICE_SIDEINFO = 1  # H266_PLAN_DEVICE_SIDEINFO
 
 
 class H266Error(RuntimeError):
@@ -74,6 +76,8 @@ def lib():
         L.h266_ctx_set_profiling.argtypes = [vp, i32]
         L.h266_ctx_profile.argtypes = [vp, vp, vp]
         L.h266_chain_plan_create.argtypes = [vp, vp, vp, C.POINTER(vp)]
+        L.h266_chain_plan_create_ex.argtypes = [vp, vp, vp, u32, C.POINTER(vp)]
+        L.h266_chain_plan_device_sideinfo.argtypes = [vp]
         L.h266_chain_plan_execute.argtypes = [vp, vp, vp]
         L.h266_chain_plan_execute_batch.argtypes = [vp, u32, vp, vp]
         L.h266_server_create.argtypes = [i32, u32, u64, C.POINTER(vp)]
@@ -203,8 +207,8 @@ class Context:
         _check(lib().h266_ctx_profile(self._h, ms, n))
         return {f: (ms[i], n[i]) for i, f in enumerate(PROF_FAMILIES)}
 
-    def plan(self, pic, fa: FilterArgsData) -> "ChainPlan":
-        return ChainPlan(self, pic, fa)
+    def plan(self, pic, fa: FilterArgsData, device_sideinfo: bool = False) -> "ChainPlan":
+        return ChainPlan(self, pic, fa, device_sideinfo)
 
     # -- filters ----------------------------------------------------------
     def apply_in_loop_filters(self, pic, fa: FilterArgsData):
@@ -264,13 +268,19 @@ class Context:
 class ChainPlan:
     """h266_chain_plan: one picture's side information resident on the device."""
 
-    def __init__(self, ctx: Context, pic, fa: FilterArgsData):
+    def __init__(self, ctx: Context, pic, fa: FilterArgsData, device_sideinfo: bool = False):
         self.ctx = ctx
         cp = pic.to_ctypes()
         a, keep = fa.to_ctypes()
         h = C.c_void_p()
-        _check(lib().h266_chain_plan_create(ctx._h, C.byref(cp), C.byref(a), C.byref(h)))
+        flags = PLAN_DEVICE_SIDEINFO if device_sideinfo else 0
+        _check(lib().h266_chain_plan_create_ex(ctx._h, C.byref(cp), C.byref(a), flags, C.byref(h)))
         self._h = h
+
+    @property
+    def device_sideinfo(self) -> bool:
+        """True when every execution derives the side information on the device."""
+        return bool(lib().h266_chain_plan_device_sideinfo(self._h))
 
     def execute(self, pic: DevicePicture):
         cp = pic.to_ctypes()

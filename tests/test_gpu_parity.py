@@ -262,19 +262,25 @@ def test_plan_batch_matches_oracle_on_mixed_pictures(ctx):
             pl.close()
 
 
-def _batched_plans_match_oracle(ctx, items, what):
+def _batched_plans_match_oracle(ctx, items, what, device_sideinfo=False, expect_device=None):
     """One batched execution of resident plans over `items` (the bench's
     value path), then per-picture launches of the same plans, each on fresh
-    samples, every picture compared with the oracle bit for bit."""
+    samples, every picture compared with the oracle bit for bit.  With
+    device_sideinfo, plans of pictures the device walk covers derive their
+    side information on the device at every execution (expect_device: which
+    pictures those are)."""
     import os
 
     import torch
 
     wants = [p.copy() for p, _ in items]
     oracle.apply_in_loop_filters_mt(wants, [f for _, f in items], os.cpu_count() or 1)
-    plans = [ctx.plan(p, f) for p, f in items]
+    plans = [ctx.plan(p, f, device_sideinfo=device_sideinfo) for p, f in items]
+    if expect_device is not None:  # True / False per picture, None: either
+        got = [pl.device_sideinfo for pl in plans]
+        assert all(e is None or g == e for g, e in zip(got, expect_device)), got
     try:
-        for mode in ("batched", "plain"):
+        for mode in ("batched", "batched", "plain"):
             devs = [native.DevicePicture.from_host(p) for p, _ in items]
             torch.cuda.synchronize()
             if mode == "batched":
@@ -295,6 +301,24 @@ def test_plan_batch_full_size_1080p_x4(ctx):
     """Four full-size pictures of the 1080p benchmark config (1920x1080
     10-bit, inter CUs, 4 luma APSs, CC-ALF, LMCS) in one batched launch."""
     _batched_plans_match_oracle(ctx, [W.config2(2000 + i) for i in range(4)], "1080p x4")
+
+
+def test_plan_batch_device_sideinfo_1080p_x4(ctx):
+    """Plans that derive the deblocking side information on the device at every
+    execution (batched CU maps and edge walk, then the grid-mode tile kernel):
+    four full-size 1080p benchmark pictures, twice batched and once per picture."""
+    _batched_plans_match_oracle(ctx, [W.config2(2100 + i) for i in range(4)], "1080p x4 device side info",
+                                device_sideinfo=True, expect_device=[True] * 4)
+
+
+def test_plan_batch_device_sideinfo_mixed_with_host_plans(ctx):
+    """One batch mixing device-walk plans (8-bit CTU 64, 10-bit 1080p-style,
+    416x240) with pictures the walk does not cover (4-sample CUs and sub-block
+    grids, deblocking only), which keep host-built segments."""
+    items = [WORKLOADS["ctb64_8bit"](60), small_c2(61), WORKLOADS["c1"](62), WORKLOADS["stress"](63),
+             _deblock_only(64), small_c2(65)]
+    _batched_plans_match_oracle(ctx, items, "mixed device/host side info", device_sideinfo=True,
+                                expect_device=[None, True, None, False, False, True])
 
 
 def test_plan_batch_2160p_tiles_x16(ctx):
