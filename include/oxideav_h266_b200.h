@@ -276,7 +276,33 @@ int h266_ctx_transfer_bytes(const h266_ctx *ctx, uint64_t *h2d, uint64_t *d2h);
 #define H266_PROF_COPY 3    /* plain plane copies into scratch              */
 #define H266_PROF_FAMILIES 4
 int h266_ctx_set_profiling(h266_ctx *ctx, int on);
+
+/* Launch-shape tuning.  No counterpart in the crate.  The project's autotuner
+ * (oxideav-h266_b200/autotune.py) sweeps these per picture geometry and bit
+ * depth and persists the winners in a JSON table, which the Python layer
+ * loads into a context with h266_ctx_set_tuning_for.  Keys and ranges:
+ *   "e2e_group"            pictures per group of h266_apply_in_loop_filters_batch (1..16, default 4)
+ *   "e2e_lanes"            streams those groups rotate over (1..4, default 3)
+ *   "sao_alf_ctas_per_sm"  SAO / ALF tile launches: 0 = one CTA per tile (default); 1..4 = a
+ *                          persistent launch of that many CTAs per SM draining a device queue of
+ *                          (picture, tile) items
+ *   "prep_threads"         host threads preparing pictures' side information (0 = half the host
+ *                          threads less two, 2..16; 1..64); a context-wide value
+ *   "e2e_copy_streams"     0: each group's copies on its own stream (default); 1: all uploads on
+ *                          one stream and all downloads on another
+ * h266_ctx_set_tuning sets the context's value; h266_ctx_set_tuning_for sets
+ * it for batches whose largest picture has that luma size and bit depth, which
+ * takes precedence.  Unknown keys or out-of-range values: H266_ERR_INVALID_ARGUMENT. */
+int h266_ctx_set_tuning(h266_ctx *ctx, const char *key, int64_t value);
+int h266_ctx_set_tuning_for(h266_ctx *ctx, uint32_t width, uint32_t height, uint32_t bit_depth, const char *key,
+                            int64_t value);
+int h266_ctx_get_tuning(const h266_ctx *ctx, const char *key, int64_t *value);
 int h266_ctx_profile(h266_ctx *ctx, double ms[H266_PROF_FAMILIES], uint64_t launches[H266_PROF_FAMILIES]);
+/* Host time of h266_apply_in_loop_filters_batch calls since the last call, in
+ * milliseconds: [0] preparing pictures (summed over the worker threads),
+ * [1] the issuing thread waiting for a preparation, [2] the issuing thread
+ * issuing copies and launches.  Resets the counters. */
+int h266_ctx_host_profile(h266_ctx *ctx, double ms[3]);
 
 /* ---- filters ------------------------------------------------------------ */
 

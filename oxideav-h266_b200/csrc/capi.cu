@@ -171,14 +171,37 @@ struct GroupSlot {
     walk.release();
   }
 };
+// Launch-shape knobs (h266_ctx_set_tuning); -1 in an override: not set.
+struct Tuning {
+  int e2e_group = 4, e2e_lanes = 3, sao_alf_ctas_per_sm = 0;
+  int prep_threads = 0;      // 0: the default count
+  int e2e_copy_streams = 0;  // 1: uploads and downloads on two streams of their own
+};
+struct TuningKey {
+  const char *name;
+  int Tuning::*field;
+  int lo, hi;
+};
+constexpr TuningKey kTuningKeys[] = {{"e2e_group", &Tuning::e2e_group, 1, 16},
+                                     {"e2e_lanes", &Tuning::e2e_lanes, 1, 4},
+                                     {"sao_alf_ctas_per_sm", &Tuning::sao_alf_ctas_per_sm, 0, 4},
+                                     {"prep_threads", &Tuning::prep_threads, 0, 64},
+                                     {"e2e_copy_streams", &Tuning::e2e_copy_streams, 0, 1}};
+
 struct GroupLane {
   cudaStream_t stream = nullptr;
   cudaEvent_t mark = nullptr;
+  // with separate copy streams: the group's uploads done, its kernels done,
+  // its downloads done (the slots are free again)
+  cudaEvent_t ev_up = nullptr, ev_comp = nullptr, ev_down = nullptr;
   std::vector<GroupSlot> slots;
   BatchBufs bb;
   int init(size_t n_slots) {
     H266_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     H266_CUDA(cudaEventCreateWithFlags(&mark, cudaEventDisableTiming));
+    H266_CUDA(cudaEventCreateWithFlags(&ev_up, cudaEventDisableTiming));
+    H266_CUDA(cudaEventCreateWithFlags(&ev_comp, cudaEventDisableTiming));
+    H266_CUDA(cudaEventCreateWithFlags(&ev_down, cudaEventDisableTiming));
     slots.resize(n_slots);
     return bb.init();
   }
@@ -186,9 +209,9 @@ struct GroupLane {
     if (stream) cudaStreamSynchronize(stream);
     for (GroupSlot &sl : slots) sl.release();
     bb.release();
-    if (mark) cudaEventDestroy(mark);
+    for (cudaEvent_t *e : {&mark, &ev_up, &ev_comp, &ev_down})
+      if (*e) cudaEventDestroy(*e), *e = nullptr;
     if (stream) cudaStreamDestroy(stream);
-    mark = nullptr;
     stream = nullptr;
   }
 };
@@ -208,13 +231,20 @@ struct h266_ctx {
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
   double prof_ms[H266_PROF_FAMILIES] = {0};
+  // host time of h266_apply_in_loop_filters_batch (h266_ctx_host_profile):
+  // preparation summed over workers, the issuing thread waiting for it, issuing
+  std::atomic<int64_t> host_ns[3] = {{0}, {0}, {0}};
   uint64_t prof_n[H266_PROF_FAMILIES] = {0};
   h266::BatchBufs batch;  // parameter tables of h266_chain_plan_execute_batch
   std::vector<std::unique_ptr<h266::GroupLane>> glanes;  // the end-to-end batch pipeline
+  cudaStream_t e2e_up = nullptr, e2e_down = nullptr;      // its copy streams
   bool force_scalar = false;  // H266_FORCE_SCALAR_ALF=1: scalar SAO/ALF kernel (cross-checks)
   bool force_global_deblock = false;  // H266_FORCE_GLOBAL_DEBLOCK=1: deblocking on global memory (cross-checks)
   bool force_strip_deblock = false;   // H266_FORCE_STRIP_DEBLOCK=1: strip kernels instead of tiles (cross-checks)
   bool force_host_sideinfo = false;   // H266_FORCE_HOST_SIDEINFO=1: never build side information on the device
+  // launch-shape tuning (h266_ctx_set_tuning): context values and per-geometry overrides
+  h266::Tuning tuning;
+  std::map<uint64_t, h266::Tuning> tuning_for;  // key: width << 32 | height << 8 | bit depth
 };
 
 namespace {
@@ -990,12 +1020,15 @@ bool device_sideinfo_allowed(const h266_ctx *ctx) {
 
 // Worker pool of the context (created on first use): as many threads as the
 // host offers, at most 16.
+// The context's preparation workers: the "prep_threads" tuning, else half the
+// host threads less two (2..16).  More workers prepare faster but slow the
+// issuing thread's copies and launches (measured on a 16-thread host: 6
+// workers gave the shortest end-to-end batch).
 TaskPool *ctx_pool(h266_ctx *ctx) {
-  if (!ctx->pool) {
-    unsigned n = std::thread::hardware_concurrency();
-    n = std::max(1u, std::min(n, 16u));
-    ctx->pool.reset(new TaskPool(n));
-  }
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned want = ctx->tuning.prep_threads > 0 ? (unsigned)ctx->tuning.prep_threads
+                                                     : std::max(2u, std::min(hw / 2 > 2 ? hw / 2 - 2 : 2u, 16u));
+  if (!ctx->pool || ctx->pool->size() != want) ctx->pool.reset(new TaskPool(want));
   return ctx->pool.get();
 }
 
@@ -1133,6 +1166,8 @@ int h266_ctx_destroy(h266_ctx *ctx) {
     l->release();
   }
   for (auto &l : ctx->glanes) l->release();
+  for (cudaStream_t st : {ctx->e2e_up, ctx->e2e_down})
+    if (st) cudaStreamSynchronize(st), cudaStreamDestroy(st);
   ctx->main.release();
   ctx->pool.reset();
   for (auto &e : ctx->ev_pool) cudaEventDestroy(e);
@@ -1916,13 +1951,27 @@ int h266_apply_in_loop_filters(h266_ctx *ctx, h266_picture *pic, const h266_in_l
 // lanes start after the work already queued on the context stream, and the
 // context stream waits for all of them before the call returns; host pictures
 // are complete on return.
+// The tuning of a batch: the override for its largest picture's geometry, else the context's.
+static const h266::Tuning &batch_tuning(const h266_ctx *ctx, uint32_t n, const h266_picture *const *pics) {
+  uint64_t best = 0, px = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const h266_picture &p = *pics[i];
+    const uint64_t a = (uint64_t)p.luma.width * p.luma.height;
+    if (a > px) {
+      px = a;
+      best = (uint64_t)p.luma.width << 32 | (uint64_t)(p.luma.height & 0xFFFFFF) << 8 | (p.luma.bit_depth & 0xFF);
+    }
+  }
+  const auto it = ctx->tuning_for.find(best);
+  return it == ctx->tuning_for.end() ? ctx->tuning : it->second;
+}
+
 int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *const *pics,
                                      const h266_in_loop_filter_args *const *args) {
-  // Groups of kGroup pictures rotate over kGroupLanes streams: per group the
-  // uploads (planes of host pictures, side information staged in pinned
-  // memory by the worker that prepared the picture), the LUTs, one batched
-  // execution (device walks, tile deblocking, SAO / ALF) and the downloads.
-  constexpr uint32_t kGroup = 4, kGroupLanes = 3;
+  // Groups of pictures rotate over streams: per group the uploads (planes of
+  // host pictures, side information staged in pinned memory by the worker
+  // that prepared the picture), the LUTs, one batched execution (device
+  // walks, tile deblocking, SAO / ALF) and the downloads.
   H266_TRY(check_ctx(ctx));
   if (n && (!pics || !args)) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL batch arrays");
   bool any_host = false;
@@ -1933,7 +1982,11 @@ int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *co
   }
   if (n <= 1) return n ? h266_apply_in_loop_filters(ctx, pics[0], args[0]) : H266_OK;
   Guard g(ctx->device);
+  const Tuning &tn = batch_tuning(ctx, n, pics);
+  const uint32_t kGroup = (uint32_t)tn.e2e_group, kGroupLanes = (uint32_t)tn.e2e_lanes;
   const uint32_t n_groups = (n + kGroup - 1) / kGroup, n_lanes = std::min(n_groups, kGroupLanes);
+  for (auto &l : ctx->glanes)  // a larger group than the lanes were made for: more slots
+    if (l->slots.size() < kGroup) l->slots.resize(kGroup);
   while (ctx->glanes.size() < n_lanes) {
     std::unique_ptr<GroupLane> l(new GroupLane());
     const int rc = l->init(kGroup);
@@ -1949,19 +2002,37 @@ int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *co
   TaskPool *pool = ctx_pool(ctx);
   const int device = ctx->device;
   const bool allow_dev = device_sideinfo_allowed(ctx);
+  using HClock = std::chrono::steady_clock;
+  auto ns_since = [](HClock::time_point t0) {
+    return (int64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(HClock::now() - t0).count();
+  };
   pool->start(n, [&](size_t i) {
+    const auto t0 = HClock::now();
     Prep &pr = *ctx->preps[i + 1];
     pr.staged_pinned = false;
     pr.rc = prepare_chain(pr, *pics[i], *args[i], nullptr, allow_dev);
     if (pr.rc == H266_OK && cudaSetDevice(device) == cudaSuccess) pr.rc = pr.stage();
     if (pr.rc != H266_OK) pr.msg = h266_last_error();
+    ctx->host_ns[0] += ns_since(t0);
   });
+  const bool copy_streams = tn.e2e_copy_streams != 0 && any_host;
+  if (copy_streams) {
+    for (cudaStream_t *st : {&ctx->e2e_up, &ctx->e2e_down}) {
+      if (!*st) H266_CUDA(cudaStreamCreateWithFlags(st, cudaStreamNonBlocking));
+      H266_CUDA(cudaStreamWaitEvent(*st, ctx->main.mark, 0));
+    }
+  }
   auto run_group = [&](uint32_t gi) -> int {
     GroupLane &L = *ctx->glanes[gi % n_lanes];
     std::vector<BatchItem> items;
     const uint32_t i0 = gi * kGroup, i1 = std::min(n, i0 + kGroup);
+    // uploads on the upload stream once the lane's previous downloads freed its slots
+    const cudaStream_t up = copy_streams ? ctx->e2e_up : L.stream;
+    if (copy_streams) H266_CUDA(cudaStreamWaitEvent(up, L.ev_down, 0));
     for (uint32_t i = i0; i < i1; ++i) {
+      const auto tw = HClock::now();
       pool->wait_item(i);
+      ctx->host_ns[1] += ns_since(tw);
       Prep &pr = *ctx->preps[i + 1];
       if (pr.rc != H266_OK) return set_error(pr.rc, pr.msg);
       GroupSlot &sl = L.slots[i - i0];
@@ -1977,13 +2048,16 @@ int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *co
         }
         const size_t row = (size_t)q.width * 2;
         H266_TRY(sl.io[k].ensure(row * q.height));
-        H266_CUDA(cudaMemcpy2DAsync(sl.io[k].ptr, row, q.samples, (size_t)q.stride * 2, row, q.height,
-                                    cudaMemcpyHostToDevice, L.stream));
+        if ((size_t)q.stride * 2 == row)  // contiguous rows: one linear copy
+          H266_CUDA(cudaMemcpyAsync(sl.io[k].ptr, q.samples, row * q.height, cudaMemcpyHostToDevice, up));
+        else
+          H266_CUDA(cudaMemcpy2DAsync(sl.io[k].ptr, row, q.samples, (size_t)q.stride * 2, row, q.height,
+                                      cudaMemcpyHostToDevice, up));
         it.P[k] = dplane(q, sl.io[k].as<uint16_t>(), q.width);
       }
       H266_TRY(sl.side.ensure(pr.blob.size()));
-      H266_CUDA(cudaMemcpyAsync(sl.side.ptr, pr.pinned.ptr, pr.blob.size(), cudaMemcpyHostToDevice, L.stream));
-      H266_CUDA(cudaEventRecord(pr.uploaded, L.stream));
+      H266_CUDA(cudaMemcpyAsync(sl.side.ptr, pr.pinned.ptr, pr.blob.size(), cudaMemcpyHostToDevice, up));
+      H266_CUDA(cudaEventRecord(pr.uploaded, up));
       ctx->h2d_bytes += pr.blob.size() + host_plane_bytes(pic);
       it.st = pr.st;
       it.st.base = sl.side.as<uint8_t>();
@@ -2013,7 +2087,16 @@ int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *co
       }
       items.push_back(it);
     }
+    if (copy_streams) {
+      H266_CUDA(cudaEventRecord(L.ev_up, up));
+      H266_CUDA(cudaStreamWaitEvent(L.stream, L.ev_up, 0));
+    }
     H266_TRY(exec_batch(ctx, L.bb, L.stream, items));
+    const cudaStream_t down = copy_streams ? ctx->e2e_down : L.stream;
+    if (copy_streams) {
+      H266_CUDA(cudaEventRecord(L.ev_comp, L.stream));
+      H266_CUDA(cudaStreamWaitEvent(down, L.ev_comp, 0));
+    }
     for (uint32_t i = i0; i < i1; ++i) {
       const h266_picture &pic = *pics[i];
       if (pic.mem == H266_MEM_DEVICE) continue;
@@ -2023,23 +2106,81 @@ int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *co
         const h266_plane &q = *pl[k];
         if ((uint64_t)q.width * q.height == 0) continue;
         const size_t row = (size_t)q.width * 2;
-        H266_CUDA(cudaMemcpy2DAsync(q.samples, (size_t)q.stride * 2, sl.io[k].ptr, row, row, q.height,
-                                    cudaMemcpyDeviceToHost, L.stream));
+        if ((size_t)q.stride * 2 == row)
+          H266_CUDA(cudaMemcpyAsync(q.samples, sl.io[k].ptr, row * q.height, cudaMemcpyDeviceToHost, down));
+        else
+          H266_CUDA(cudaMemcpy2DAsync(q.samples, (size_t)q.stride * 2, sl.io[k].ptr, row, row, q.height,
+                                      cudaMemcpyDeviceToHost, down));
       }
       ctx->d2h_bytes += host_plane_bytes(pic);
     }
+    if (copy_streams) H266_CUDA(cudaEventRecord(L.ev_down, down));
     return H266_OK;
   };
   int rc = H266_OK;
+  const auto ti = HClock::now();
   for (uint32_t gi = 0; gi < n_groups && rc == H266_OK; ++gi) rc = run_group(gi);
   pool->wait_all();
+  ctx->host_ns[2] += ns_since(ti);
   for (uint32_t l = 0; l < n_lanes; ++l) {
     GroupLane &L = *ctx->glanes[l];
     H266_CUDA(cudaEventRecord(L.mark, L.stream));
     H266_CUDA(cudaStreamWaitEvent(ctx->stream, L.mark, 0));
     if (any_host || rc != H266_OK) H266_CUDA(cudaStreamSynchronize(L.stream));
   }
+  if (copy_streams)
+    for (cudaStream_t st : {ctx->e2e_up, ctx->e2e_down}) {
+      H266_CUDA(cudaEventRecord(ctx->main.mark, st));
+      H266_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->main.mark, 0));
+      H266_CUDA(cudaStreamSynchronize(st));
+    }
   return rc;
+}
+
+static const h266::TuningKey *tuning_key(const char *key) {
+  if (!key) return nullptr;
+  for (const h266::TuningKey &k : h266::kTuningKeys)
+    if (std::strcmp(k.name, key) == 0) return &k;
+  return nullptr;
+}
+
+int h266_ctx_set_tuning(h266_ctx *ctx, const char *key, int64_t value) {
+  H266_TRY(check_ctx(ctx));
+  const h266::TuningKey *k = tuning_key(key);
+  if (!k) return set_error(H266_ERR_INVALID_ARGUMENT, std::string("unknown tuning key ") + (key ? key : "(null)"));
+  if (value < k->lo || value > k->hi) return set_error(H266_ERR_INVALID_ARGUMENT, std::string(key) + ": value out of range");
+  ctx->tuning.*(k->field) = (int)value;
+  for (auto &kv : ctx->tuning_for) kv.second.*(k->field) = (int)value;
+  return H266_OK;
+}
+
+int h266_ctx_set_tuning_for(h266_ctx *ctx, uint32_t width, uint32_t height, uint32_t bit_depth, const char *key,
+                            int64_t value) {
+  H266_TRY(check_ctx(ctx));
+  const h266::TuningKey *k = tuning_key(key);
+  if (!k) return set_error(H266_ERR_INVALID_ARGUMENT, std::string("unknown tuning key ") + (key ? key : "(null)"));
+  if (value < k->lo || value > k->hi) return set_error(H266_ERR_INVALID_ARGUMENT, std::string(key) + ": value out of range");
+  const uint64_t g = (uint64_t)width << 32 | (uint64_t)(height & 0xFFFFFF) << 8 | (bit_depth & 0xFF);
+  auto it = ctx->tuning_for.find(g);
+  if (it == ctx->tuning_for.end()) it = ctx->tuning_for.emplace(g, ctx->tuning).first;
+  it->second.*(k->field) = (int)value;
+  return H266_OK;
+}
+
+int h266_ctx_get_tuning(const h266_ctx *ctx, const char *key, int64_t *value) {
+  if (!ctx || !value) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL argument");
+  const h266::TuningKey *k = tuning_key(key);
+  if (!k) return set_error(H266_ERR_INVALID_ARGUMENT, std::string("unknown tuning key ") + (key ? key : "(null)"));
+  *value = ctx->tuning.*(k->field);
+  return H266_OK;
+}
+
+int h266_ctx_host_profile(h266_ctx *ctx, double ms[3]) {
+  H266_TRY(check_ctx(ctx));
+  if (!ms) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL out");
+  for (int k = 0; k < 3; ++k) ms[k] = (double)ctx->host_ns[k].exchange(0) / 1e6;
+  ms[2] -= ms[1];  // issuing excludes the waits
+  return H266_OK;
 }
 
 int h266_ctx_set_profiling(h266_ctx *ctx, int on) {

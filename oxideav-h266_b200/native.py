@@ -33,7 +33,8 @@ EXPORTS = [
     "h266_apply_deblocking_clipped",
     "h266_apply_sao_clipped", "h266_apply_alf_clipped", "h266_apply_in_loop_filters",
     "h266_apply_in_loop_filters_batch", "h266_ctx_set_profiling", "h266_ctx_profile", "h266_chain_plan_create",
-    "h266_chain_plan_create_ex", "h266_chain_plan_device_sideinfo",
+    "h266_chain_plan_create_ex", "h266_chain_plan_device_sideinfo", "h266_ctx_set_tuning", "h266_ctx_set_tuning_for",
+    "h266_ctx_get_tuning", "h266_ctx_host_profile",
     "h266_chain_plan_execute", "h266_chain_plan_execute_batch", "h266_chain_plan_destroy",
     "h266_apply_in_loop_filters_noalloc", "h266_server_create", "h266_server_submit", "h266_server_wait",
     "h266_server_stats", "h266_server_replay", "h266_server_destroy", "h266_alf_decide_and_apply_clipped",
@@ -78,6 +79,10 @@ def lib():
         L.h266_chain_plan_create.argtypes = [vp, vp, vp, C.POINTER(vp)]
         L.h266_chain_plan_create_ex.argtypes = [vp, vp, vp, u32, C.POINTER(vp)]
         L.h266_chain_plan_device_sideinfo.argtypes = [vp]
+        L.h266_ctx_set_tuning.argtypes = [vp, C.c_char_p, C.c_int64]
+        L.h266_ctx_set_tuning_for.argtypes = [vp, u32, u32, u32, C.c_char_p, C.c_int64]
+        L.h266_ctx_get_tuning.argtypes = [vp, C.c_char_p, C.POINTER(C.c_int64)]
+        L.h266_ctx_host_profile.argtypes = [vp, vp]
         L.h266_chain_plan_execute.argtypes = [vp, vp, vp]
         L.h266_chain_plan_execute_batch.argtypes = [vp, u32, vp, vp]
         L.h266_server_create.argtypes = [i32, u32, u64, C.POINTER(vp)]
@@ -196,6 +201,37 @@ class Context:
 
     def set_stream(self, stream_ptr: int | None):
         _check(lib().h266_ctx_set_stream(self._h, stream_ptr))
+
+    def set_tuning(self, key: str, value: int):
+        """A launch-shape knob for every batch (see h266_ctx_set_tuning)."""
+        _check(lib().h266_ctx_set_tuning(self._h, key.encode(), int(value)))
+
+    def set_tuning_for(self, width: int, height: int, bit_depth: int, key: str, value: int):
+        """A knob for batches whose largest picture has this luma size and bit depth."""
+        _check(lib().h266_ctx_set_tuning_for(self._h, width, height, bit_depth, key.encode(), int(value)))
+
+    def get_tuning(self, key: str) -> int:
+        v = C.c_int64()
+        _check(lib().h266_ctx_get_tuning(self._h, key.encode(), C.byref(v)))
+        return int(v.value)
+
+    def host_profile(self) -> dict:
+        """Host milliseconds of batch calls since the last query: preparation
+        (summed over workers), waiting for it, issuing."""
+        ms = (C.c_double * 3)()
+        _check(lib().h266_ctx_host_profile(self._h, ms))
+        return {"prepare": ms[0], "wait": ms[1], "issue": ms[2]}
+
+    def load_tuning(self, path) -> int:
+        """Loads an autotuner table (autotune.py's JSON): every entry's knobs
+        for its geometry.  Returns the number of entries."""
+        import json
+
+        table = json.loads(pathlib.Path(path).read_text())
+        for e in table["entries"]:
+            for k, v in e["best"].items():
+                self.set_tuning_for(e["width"], e["height"], e["bit_depth"], k, v)
+        return len(table["entries"])
 
     def set_profiling(self, on: bool):
         _check(lib().h266_ctx_set_profiling(self._h, int(on)))

@@ -159,6 +159,48 @@ def test_batch_pipelined_host_pictures(ctx):
         assert_same(got, want, f"batch picture {i}")
 
 
+@pytest.mark.parametrize("group,lanes,copy_streams,prep", [(1, 1, 0, 2), (2, 4, 1, 3), (8, 2, 0, 0), (3, 3, 1, 16)])
+def test_batch_launch_shapes_match_oracle(group, lanes, copy_streams, prep):
+    """The end-to-end batch under other tunings (group size, streams, copy
+    streams, preparation threads): the same results, bit for bit.  Pinned
+    host pictures, so the copies are asynchronous."""
+    import numpy as np
+    import torch
+
+    items = [BATCH_MIX[i % len(BATCH_MIX)](40 + i) for i in range(7)] + [small_c2(50), W.config1(51)]
+    pinned = []
+    for p, _ in items:
+        planes = []
+        for a in p.planes():
+            t = torch.empty(a.shape, dtype=torch.int16, pin_memory=True)
+            t.numpy().view(np.uint16)[...] = a
+            planes.append(t)
+        pinned.append((W.PictureData(*[t.numpy().view(np.uint16) for t in planes], p.bit_depth), planes))
+    with native.Context(0) as c:
+        for key, v in (("e2e_group", group), ("e2e_lanes", lanes), ("e2e_copy_streams", copy_streams),
+                       ("prep_threads", prep)):
+            c.set_tuning(key, v)
+            assert c.get_tuning(key) == v
+        for rnd in range(2):
+            for (p, _), (pic, _) in zip(items, pinned):
+                for dst, src in zip(pic.planes(), p.planes()):
+                    dst[...] = src
+            c.apply_in_loop_filters_batch([pic for pic, _ in pinned], [f for _, f in items])
+            for i, ((p, f), (pic, _)) in enumerate(zip(items, pinned)):
+                want = p.copy()
+                oracle.apply_in_loop_filters(want, f)
+                assert_same(pic, want, f"tuned batch round {rnd} picture {i}")
+
+
+def test_tuning_rejects_unknown_keys_and_ranges(ctx):
+    with pytest.raises(native.H266Error):
+        ctx.set_tuning("no_such_knob", 1)
+    with pytest.raises(native.H266Error):
+        ctx.set_tuning("e2e_group", 0)
+    with pytest.raises(native.H266Error):
+        ctx.set_tuning_for(1920, 1080, 10, "sao_alf_ctas_per_sm", 9)
+
+
 def test_batch_device_pictures_follow_context_stream(ctx):
     import torch
 
