@@ -381,9 +381,25 @@ def run_served(ctx, local_rank, seconds: float, rates=(1, 4, 8, 12)):
     return out
 
 
+TUNING_TABLE = ROOT / "oxideav-h266_b200" / "tuning_b200.json"
+
+
+def load_tuning(ctx) -> dict | None:
+    """Applies the autotuner's table (oxideav-h266_b200/autotune.py, run on
+    this GPU type) to the context; returns its entries' winners."""
+    if not TUNING_TABLE.exists():
+        return None
+    ctx.load_tuning(TUNING_TABLE)
+    t = json.loads(TUNING_TABLE.read_text())
+    return {e["name"]: e["best"] for e in t["entries"]}
+
+
 def run_configs(ctx, local_rank, stream, steps: int):
-    """The benchmark's batched configs on device-resident pictures: one
-    batched execution per step vs per-picture launches of the same plans."""
+    """The benchmark's batched configs on device-resident pictures: the tuned
+    batched execution (the autotuner's launch shape: a persistent SAO/ALF
+    launch draining the (picture, tile) queue where that won), the same batch
+    replayed as a captured CUDA graph, the default launch shape (one CTA per
+    tile), and per-picture launches of the same plans."""
     import torch
 
     from oxideav_h266_b200 import native
@@ -411,19 +427,34 @@ def run_configs(ctx, local_rank, stream, steps: int):
             torch.cuda.synchronize()
             return s0.elapsed_time(s1) / steps
 
-        ms_b = timed(lambda: ctx.execute_plans(plans, devs))
-        ms_p = timed(lambda: [pl.execute(d) for pl, d in zip(plans, devs)])
+        ms_t = timed(lambda: ctx.execute_plans(plans, devs))  # tuned (table loaded)
+        graph = ctx.batch_graph(plans, devs)
+        ms_g = timed(graph.launch)
         want = oracle_digests(items, os.cpu_count() or 1)
         par = {}
+        for mode, fn in (("tuned", lambda: ctx.execute_plans(plans, devs)), ("graph", graph.launch)):
+            restore_device(devs, items)
+            fn()
+            torch.cuda.synchronize()
+            par[mode] = parity_record([d.to_host() for d in devs], want)
+        graph.close()
+        saved = {k: ctx.get_tuning(k) for k in ("sao_alf_ctas_per_sm", "sao_alf_tile_h")}
+        ctx.set_tuning("sao_alf_ctas_per_sm", 0)  # the default shape (clears the table's overrides)
+        ctx.set_tuning("sao_alf_tile_h", 64)
+        ms_b = timed(lambda: ctx.execute_plans(plans, devs))
+        ms_p = timed(lambda: [pl.execute(d) for pl, d in zip(plans, devs)])
         for mode, fn in (("batched", lambda: ctx.execute_plans(plans, devs)),
                          ("plain", lambda: [pl.execute(d) for pl, d in zip(plans, devs)])):
             restore_device(devs, items)
             fn()
             torch.cuda.synchronize()
             par[mode] = parity_record([d.to_host() for d in devs], want)
+        for k, v in saved.items():
+            ctx.set_tuning(k, v)
+        load_tuning(ctx)
+        rate = lambda ms: {"ms_per_step": round(ms, 4), "mpx_per_s": round(px / ms / 1e3, 1)}
         out[name] = {"pictures": len(items), "mpx_per_step": round(px / 1e6, 2),
-                     "batched": {"ms_per_step": round(ms_b, 4), "mpx_per_s": round(px / ms_b / 1e3, 1)},
-                     "plain": {"ms_per_step": round(ms_p, 4), "mpx_per_s": round(px / ms_p / 1e3, 1)},
+                     "tuned": rate(ms_t), "graph": rate(ms_g), "batched": rate(ms_b), "plain": rate(ms_p),
                      "parity": par}
         for pl in plans:
             pl.close()
@@ -665,6 +696,7 @@ def run_ours(args, rank, world, local_rank):
     # are recorded on it (the legacy default stream's handle is 0, which the
     # library reads as "use the context's own stream").
     stream = torch.cuda.Stream(device=local_rank)
+    tuning = load_tuning(ctx)
     assert stream.cuda_stream != 0
     torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
@@ -866,7 +898,7 @@ def run_ours(args, rank, world, local_rank):
             "metric": METRIC, "value": round(value, 2), "unit": "Mpx/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic (seeded 1080p config generator)",
-            "config": workload_config(args.batch, world),
+            "config": dict(workload_config(args.batch, world), tuning=tuning),
             "roofline": roofline, "plain": plain, "fresh_sideinfo": fresh, "served": served, "configs": configs, "encoder_alf_trials": trials, "recon_io": recon,
             "cpu_baseline": cpu, "e2e": e2e, "parity": parity_summary(parity, served, configs),
             "gpu_launches": int(launches),

@@ -286,6 +286,8 @@ int h266_ctx_set_profiling(h266_ctx *ctx, int on);
  *   "sao_alf_ctas_per_sm"  SAO / ALF tile launches: 0 = one CTA per tile (default); 1..4 = a
  *                          persistent launch of that many CTAs per SM draining a device queue of
  *                          (picture, tile) items
+ *   "sao_alf_tile_h"       SAO / ALF tile height for CTBs of 64 and 128: 64 (default) or 32
+ *                          (values in between: 64)
  *   "prep_threads"         host threads preparing pictures' side information (0 = half the host
  *                          threads less two, 2..16; 1..64); a context-wide value
  *   "e2e_copy_streams"     0: each group's copies on its own stream (default); 1: all uploads on
@@ -522,6 +524,19 @@ int h266_chain_plan_device_sideinfo(const h266_chain_plan *plan);
 int h266_chain_plan_execute_batch(h266_ctx *ctx, uint32_t n, h266_chain_plan *const *plans,
                                   h266_picture *const *pics);
 int h266_chain_plan_destroy(h266_chain_plan *plan);
+/* A batched plan execution captured once into a CUDA graph and replayed with
+ * one launch.  No counterpart in the crate.  The graph holds the batch's
+ * parameter tables and refers to the plans and the pictures' device buffers
+ * as they were at create time: a replay filters whatever samples those
+ * buffers then hold, with the plans' side information; plans and buffers must
+ * outlive the graph.  Replays go on the context's stream and are
+ * bit-identical to h266_chain_plan_execute_batch on the same inputs.  The
+ * context's tuning at create time is baked in. */
+typedef struct h266_batch_graph h266_batch_graph;
+int h266_batch_graph_create(h266_ctx *ctx, uint32_t n, h266_chain_plan *const *plans, h266_picture *const *pics,
+                            h266_batch_graph **out);
+int h266_batch_graph_launch(h266_ctx *ctx, h266_batch_graph *graph);
+int h266_batch_graph_destroy(h266_batch_graph *graph);
 
 /* Served filter chain: a request loop for many concurrent streams.  No
  * counterpart in the crate, which filters one picture per call on the

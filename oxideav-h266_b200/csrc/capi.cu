@@ -133,6 +133,7 @@ struct Prep;  // host-side preparation of one picture's chain call
 // Parameter tables of batched plan executions: assembled on the host,
 // uploaded once per batch through pinned staging.
 struct BatchBufs {
+  bool capturing = false;  // recorded into a CUDA graph: no waits on events from outside the capture
   std::vector<uint8_t> blob;
   DevBuf side;
   Staging stage;
@@ -173,7 +174,7 @@ struct GroupSlot {
 };
 // Launch-shape knobs (h266_ctx_set_tuning); -1 in an override: not set.
 struct Tuning {
-  int e2e_group = 4, e2e_lanes = 3, sao_alf_ctas_per_sm = 0;
+  int e2e_group = 4, e2e_lanes = 3, sao_alf_ctas_per_sm = 0, sao_alf_tile_h = 64;
   int prep_threads = 0;      // 0: the default count
   int e2e_copy_streams = 0;  // 1: uploads and downloads on two streams of their own
 };
@@ -185,6 +186,7 @@ struct TuningKey {
 constexpr TuningKey kTuningKeys[] = {{"e2e_group", &Tuning::e2e_group, 1, 16},
                                      {"e2e_lanes", &Tuning::e2e_lanes, 1, 4},
                                      {"sao_alf_ctas_per_sm", &Tuning::sao_alf_ctas_per_sm, 0, 4},
+                                     {"sao_alf_tile_h", &Tuning::sao_alf_tile_h, 32, 64},
                                      {"prep_threads", &Tuning::prep_threads, 0, 64},
                                      {"e2e_copy_streams", &Tuning::e2e_copy_streams, 0, 1}};
 
@@ -867,8 +869,25 @@ struct BatchItem {
   int bd = 8;
   uint8_t *walk = nullptr;
 };
-int exec_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, std::vector<BatchItem> &items);
+int exec_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, std::vector<BatchItem> &items,
+               const Tuning &tn);
 }  // namespace h266
+
+// The tuning of a batch: the override for its largest picture's geometry, else the context's.
+static const h266::Tuning &batch_tuning(const h266_ctx *ctx, uint32_t n, const h266_picture *const *pics) {
+  uint64_t best = 0, px = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const h266_picture &p = *pics[i];
+    const uint64_t a = (uint64_t)p.luma.width * p.luma.height;
+    if (a > px) {
+      px = a;
+      best = (uint64_t)p.luma.width << 32 | (uint64_t)(p.luma.height & 0xFFFFFF) << 8 | (p.luma.bit_depth & 0xFF);
+    }
+  }
+  const auto it = ctx->tuning_for.find(best);
+  return it == ctx->tuning_for.end() ? ctx->tuning : it->second;
+}
+
 
 
 namespace {
@@ -1951,20 +1970,6 @@ int h266_apply_in_loop_filters(h266_ctx *ctx, h266_picture *pic, const h266_in_l
 // lanes start after the work already queued on the context stream, and the
 // context stream waits for all of them before the call returns; host pictures
 // are complete on return.
-// The tuning of a batch: the override for its largest picture's geometry, else the context's.
-static const h266::Tuning &batch_tuning(const h266_ctx *ctx, uint32_t n, const h266_picture *const *pics) {
-  uint64_t best = 0, px = 0;
-  for (uint32_t i = 0; i < n; ++i) {
-    const h266_picture &p = *pics[i];
-    const uint64_t a = (uint64_t)p.luma.width * p.luma.height;
-    if (a > px) {
-      px = a;
-      best = (uint64_t)p.luma.width << 32 | (uint64_t)(p.luma.height & 0xFFFFFF) << 8 | (p.luma.bit_depth & 0xFF);
-    }
-  }
-  const auto it = ctx->tuning_for.find(best);
-  return it == ctx->tuning_for.end() ? ctx->tuning : it->second;
-}
 
 int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *const *pics,
                                      const h266_in_loop_filter_args *const *args) {
@@ -2091,7 +2096,7 @@ int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *co
       H266_CUDA(cudaEventRecord(L.ev_up, up));
       H266_CUDA(cudaStreamWaitEvent(L.stream, L.ev_up, 0));
     }
-    H266_TRY(exec_batch(ctx, L.bb, L.stream, items));
+    H266_TRY(exec_batch(ctx, L.bb, L.stream, items, tn));
     const cudaStream_t down = copy_streams ? ctx->e2e_down : L.stream;
     if (copy_streams) {
       H266_CUDA(cudaEventRecord(L.ev_comp, L.stream));
@@ -2322,7 +2327,8 @@ int check_plan_batch(h266_ctx *ctx, uint32_t n, h266_chain_plan *const *plans, h
 // on the device (three launches for all of them), one tile-deblocking launch
 // and one SAO/ALF launch per kernel variant over every picture's tiles, and
 // per picture whatever the batched kernels do not take.
-int exec_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, std::vector<BatchItem> &items) {
+int exec_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, std::vector<BatchItem> &items,
+               const Tuning &tn) {
   const uint32_t n = (uint32_t)items.size();
   if (!n) return H266_OK;
   H266_TRY(bb.init());
@@ -2335,8 +2341,8 @@ int exec_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, std::vector<Ba
   std::vector<uint32_t> tile_first(1, 0), walk_first[3] = {{0}, {0}, {0}};  // clear, CU map, walk CTAs
   WalkBatchCounts walk_total;
   const size_t wis = walk_batch_item_size();
-  std::vector<Pass2Args> p2[8];
-  std::vector<uint32_t> p2_first[8];
+  std::vector<Pass2Args> p2[kPass2Variants];
+  std::vector<uint32_t> p2_first[kPass2Variants];
   const size_t tps = deblock_tile_params_size();
   for (uint32_t i = 0; i < n; ++i) {
     BatchItem &it = items[i];
@@ -2375,6 +2381,7 @@ int exec_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, std::vector<Ba
     r.variant = -1;
     if (r.packed) {
       Pass2Args a = it.args;
+      a.tile_h = tn.sao_alf_tile_h;
       bind_pass2(a, base, it.st, it.S, it.P);
       uint32_t c = 0;
       r.variant = pass2_packed_variant(a, it.do_sao, it.do_alf, &c);
@@ -2392,15 +2399,19 @@ int exec_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, std::vector<Ba
   const size_t off_wi = blob.put(walk_items.data(), walk_items.size());
   size_t off_wf[3];
   for (int k = 0; k < 3; ++k) off_wf[k] = blob.put(walk_first[k].data(), walk_first[k].size() * sizeof(uint32_t));
-  size_t off_p2[8] = {0}, off_p2f[8] = {0};
-  for (int v = 0; v < 8; ++v)
+  size_t off_p2[kPass2Variants] = {0}, off_p2f[kPass2Variants] = {0};
+  const uint32_t zero_queue[kPass2Variants] = {0};  // the persistent launches' item counters, zero at launch
+  const size_t off_q = blob.put(zero_queue, sizeof zero_queue);
+  for (int v = 0; v < kPass2Variants; ++v)
     if (!p2[v].empty()) {
       off_p2[v] = blob.put(p2[v].data(), p2[v].size() * sizeof(Pass2Args));
       off_p2f[v] = blob.put(p2_first[v].data(), p2_first[v].size() * sizeof(uint32_t));
     }
   H266_TRY(bb.side.ensure(b.size()));
-  H266_CUDA(cudaStreamWaitEvent(stream, bb.done, 0));  // earlier batches read bb.side (any stream)
-  H266_CUDA(cudaEventSynchronize(bb.staged));         // the previous upload has read the staging buffer
+  if (!bb.capturing) {
+    H266_CUDA(cudaStreamWaitEvent(stream, bb.done, 0));  // earlier batches read bb.side (any stream)
+    H266_CUDA(cudaEventSynchronize(bb.staged));         // the previous upload has read the staging buffer
+  }
   H266_TRY(bb.stage.ensure(b.size()));
   std::memcpy(bb.stage.ptr, b.data(), b.size());
   H266_CUDA(cudaMemcpyAsync(bb.side.ptr, bb.stage.ptr, b.size(), cudaMemcpyHostToDevice, stream));
@@ -2434,12 +2445,14 @@ int exec_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, std::vector<Ba
     if (!it.pass2 || runs[i].packed) continue;
     H266_TRY(run_pass2(ctx, stream, it.args, it.do_sao, it.do_alf, it.packed, it.st.base, it.st, it.S, it.P));
   }
-  for (int v = 0; v < 8; ++v)
+  for (int v = 0; v < kPass2Variants; ++v)
     if (!p2[v].empty()) {
       Prof pf(ctx, stream, H266_PROF_SAO_ALF);
       H266_TRY(launch_pass2_packed_batch(stream, v, reinterpret_cast<const Pass2Args *>(dside + off_p2[v]),
                                          reinterpret_cast<const uint32_t *>(dside + off_p2f[v]), (int)p2[v].size(),
-                                         p2_first[v].back(), &ctx->launches));
+                                         p2_first[v].back(), tn.sao_alf_ctas_per_sm,
+                                         reinterpret_cast<uint32_t *>(bb.side.as<uint8_t>() + off_q) + v,
+                                         &ctx->launches));
     }
   H266_CUDA(cudaEventRecord(bb.done, stream));
   return H266_OK;
@@ -2469,7 +2482,7 @@ int exec_plan_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, uint32_t 
     it.bd = pl.deblock_bd;
     it.walk = pl.walk.as<uint8_t>();
   }
-  return exec_batch(ctx, bb, stream, items);
+  return exec_batch(ctx, bb, stream, items, batch_tuning(ctx, n, pics));
 }
 }  // namespace h266
 
@@ -2482,6 +2495,82 @@ int h266_chain_plan_execute_batch(h266_ctx *ctx, uint32_t n, h266_chain_plan *co
   if (!n) return H266_OK;
   Guard g(ctx->device);
   return exec_plan_batch(ctx, ctx->batch, ctx->stream, n, plans, pics);
+}
+
+}  // extern "C"
+
+// A batched plan execution recorded once as a CUDA graph: its own parameter
+// tables (pinned staging and device copy, read by the graph's upload node on
+// every replay) and the instantiated graph.
+struct h266_batch_graph {
+  int device = 0;
+  h266::BatchBufs bb;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t stream = nullptr;  // the capture stream
+};
+
+extern "C" {
+
+int h266_batch_graph_destroy(h266_batch_graph *g) {
+  if (!g) return H266_OK;
+  Guard gd(g->device);
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  if (g->stream) cudaStreamDestroy(g->stream);
+  g->bb.release();
+  delete g;
+  return H266_OK;
+}
+
+int h266_batch_graph_create(h266_ctx *ctx, uint32_t n, h266_chain_plan *const *plans, h266_picture *const *pics,
+                            h266_batch_graph **out) {
+  H266_TRY(check_ctx(ctx));
+  if (!out) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL out");
+  *out = nullptr;
+  H266_TRY(check_plan_batch(ctx, n, plans, pics));
+  if (!n) return set_error(H266_ERR_INVALID_ARGUMENT, "empty batch");
+  Guard gd(ctx->device);
+  h266_batch_graph *g = new h266_batch_graph();
+  g->device = ctx->device;
+  auto fail = [&](int rc) {
+    h266_batch_graph_destroy(g);
+    return rc;
+  };
+  int rc = g->bb.init();
+  if (rc != H266_OK) return fail(rc);
+  cudaError_t e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return fail(cuda_error(e, "graph stream"));
+  g->bb.capturing = true;
+  const bool prof = ctx->prof;
+  ctx->prof = false;  // no profiling events inside the graph
+  // relaxed: the graph's own tables are allocated while recording
+  e = cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeRelaxed);
+  if (e != cudaSuccess) {
+    ctx->prof = prof;
+    return fail(cuda_error(e, "cudaStreamBeginCapture"));
+  }
+  rc = exec_plan_batch(ctx, g->bb, g->stream, n, plans, pics);
+  cudaGraph_t graph = nullptr;
+  e = cudaStreamEndCapture(g->stream, &graph);
+  ctx->prof = prof;
+  g->graph = graph;
+  if (rc != H266_OK) return fail(rc);
+  if (e != cudaSuccess) return fail(cuda_error(e, "cudaStreamEndCapture"));
+  e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+  if (e != cudaSuccess) return fail(cuda_error(e, "cudaGraphInstantiate"));
+  *out = g;
+  return H266_OK;
+}
+
+int h266_batch_graph_launch(h266_ctx *ctx, h266_batch_graph *g) {
+  H266_TRY(check_ctx(ctx));
+  if (!g) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL graph");
+  if (g->device != ctx->device) return set_error(H266_ERR_INVALID_ARGUMENT, "graph belongs to another device");
+  Guard gd(ctx->device);
+  H266_CUDA(cudaGraphLaunch(g->exec, ctx->stream));
+  ctx->launches += 1;
+  return H266_OK;
 }
 
 int h266_chain_plan_destroy(h266_chain_plan *plan) {

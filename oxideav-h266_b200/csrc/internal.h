@@ -272,6 +272,7 @@ struct Pass2Args {
   // alignment the TMA unit needs.
   CUtensorMap tmap[3];
   int tma;        // windows staged by TMA (else 16-byte vector loads)
+  int tile_h;     // tile height for CTBs of 64 and 128: 64 (also 0) or 32
   int sao_i8;     // every SAO offset of the picture fits a signed byte (the packed offset tables)
   DPlane src[3];  // input planes (post-deblock)
   DPlane dst[3];  // output planes
@@ -363,10 +364,14 @@ int launch_alf_luma_trials(cudaStream_t st, const Pass2Args &a, const DPlane &or
                            unsigned long long *d_sse, uint64_t *launches);
 int launch_alf_luma_decide(cudaStream_t st, CtbDev *d_ctbs, int n, unsigned long long *d_sse, int cols, int trials_run,
                            int16_t *d_decision, uint64_t *launches);
-// Batched packed pass: fills a's tile grid, returns the kernel variant (0..7)
-// and the picture's CTA count; pictures of one variant share a launch.
 int pass2_packed_variant(Pass2Args &a, bool do_sao, bool do_alf, uint32_t *ctas);
+// Batched packed pass: fills a's tile grid (a.tile_h chooses the tile height
+// for CTBs of 64 and 128), returns the kernel variant (0..11) and the
+// picture's CTA count; pictures of one variant share a launch.  With
+// ctas_per_sm > 0 the launch is persistent: that many CTAs per SM drain the
+// variant's (picture, tile) items through the counter *d_queue (zero at launch).
+constexpr int kPass2Variants = 12;
 int launch_pass2_packed_batch(cudaStream_t st, int variant, const Pass2Args *d_args, const uint32_t *d_first, int n,
-                              uint32_t ctas, uint64_t *launches);
+                              uint32_t ctas, int ctas_per_sm, uint32_t *d_queue, uint64_t *launches);
 
 }  // namespace h266

@@ -107,12 +107,12 @@ __device__ __forceinline__ uint64_t global_ns() {
   return t;
 }
 
-// Polls the barrier's phase 0 for at most kWaitNs.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar) {
-  if (mbar_try_wait(bar, 0)) return true;
+// Polls the barrier's phase `phase` for at most kWaitNs.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, uint32_t phase) {
+  if (mbar_try_wait(bar, phase)) return true;
   const uint64_t t0 = global_ns();
   for (;;) {
-    if (mbar_try_wait(bar, 0)) return true;
+    if (mbar_try_wait(bar, phase)) return true;
     if (global_ns() - t0 > kWaitNs) return false;
   }
 }
@@ -207,7 +207,8 @@ __device__ __forceinline__ uint32_t sao_pair(const SaoFast &f, const uint16_t *d
 // pairs (fast) or the remaining window samples around it (slow).
 struct FastRect {
   int x0, y0, npx, ny;
-  uint32_t magic;  // floor(i / npx) = umulhi(i, magic) for the indices used
+  uint32_t magic;  // floor(i / npx) = umulhi(i, magic) for the indices used (npx > 1)
+  __device__ int row_of(uint32_t i) const { return npx == 1 ? (int)i : (int)__umulhi(i, magic); }
   __device__ int pairs() const { return npx * ny; }
 };
 
@@ -220,7 +221,7 @@ __device__ __forceinline__ FastRect fast_rect(int x0, int x1, int y0, int y1) {
   r.npx = x1 > x0 ? (x1 - x0) / 2 : 0;
   r.ny = y1 > y0 ? y1 - y0 : 0;
   if (!r.npx || !r.ny) r.npx = r.ny = 0;
-  r.magic = r.npx ? 0xFFFFFFFFu / (uint32_t)r.npx + 1u : 0u;
+  r.magic = r.npx > 1 ? 0xFFFFFFFFu / (uint32_t)r.npx + 1u : 0u;  // 2^32 / 1 does not fit: row_of
   return r;
 }
 
@@ -292,8 +293,14 @@ __device__ __forceinline__ void load_words(Words<NW, B> &r, const uint16_t *p, i
 }
 
 // ---------------------------------------------------------------- the tile
-template <int W, int TH, bool DO_SAO, bool DO_ALF, bool GLOBAL_MAPS>
-__device__ __forceinline__ void sao_alf_tile3(const Pass2Args &a, const Pass2Args *maps, int tile) {
+// Tile `tile` of the picture whose parameters are `a` (tensor maps at `maps`).
+// PERSIST: the CTA runs many tiles on one barrier, initialised by the caller;
+// `phase` is the barrier's next phase and flips with every completed copy.
+// Returns false when the window copies did not land in time (the tile is left
+// unfiltered and counted; a persistent CTA stops then).
+template <int W, int TH, bool DO_SAO, bool DO_ALF, bool GLOBAL_MAPS, bool PERSIST = false>
+__device__ __forceinline__ bool sao_alf_tile3(const Pass2Args &a, const Pass2Args *maps, int tile,
+                                              uint32_t &phase) {
   using S = Smem3<W, TH>;
   extern __shared__ __align__(128) uint8_t smem_raw[];
   // TMA destinations need 128-byte aligned shared addresses: align the base
@@ -329,7 +336,7 @@ __device__ __forceinline__ void sao_alf_tile3(const Pass2Args &a, const Pass2Arg
   const bool tma = a.tma != 0;
 
   // ---- (1) SAO parameters of the 3x3 CTB neighbourhood; deblocked windows
-  if (tid == 0 && tma) mbar_init(&sm.bar, 1);
+  if (!PERSIST && tid == 0 && tma) mbar_init(&sm.bar, 1);
   int my_type = 0;
   if (tid < 27) {
     const int comp = tid / 9, n = tid % 9;
@@ -392,6 +399,8 @@ __device__ __forceinline__ void sao_alf_tile3(const Pass2Args &a, const Pass2Arg
                              (chroma_on[0] ? S::DC_BYTES : 0) + (chroma_on[1] ? S::DC_BYTES : 0);
       if (GLOBAL_MAPS)
         for (int c = 0; c < 3; ++c) tmap_acquire(&maps->tmap[c]);
+      // the previous tile's generic accesses of the window space come before these copies
+      if (PERSIST) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_expect_tx(&sm.bar, bytes);
       if (a.src[0].w > 0 && a.src[0].h > 0) tma_load_2d(sm.dL(), &maps->tmap[0], X0 - 8, Y0 - 4, &sm.bar);
 #pragma unroll
@@ -433,13 +442,14 @@ __device__ __forceinline__ void sao_alf_tile3(const Pass2Args &a, const Pass2Arg
     }
   }
   if (tma) {
-    bool ok = mbar_wait_bounded(&sm.bar);
+    bool ok = mbar_wait_bounded(&sm.bar, phase);
     ok = __syncthreads_and(ok);
     if (!ok) {  // the copies did not land: count the tile, let them finish (bounded), leave it unfiltered
       if (tid == 0) atomicAdd(&g_wait_timeouts, 1u);
-      mbar_wait_bounded(&sm.bar);
-      return;
+      mbar_wait_bounded(&sm.bar, phase);
+      return false;
     }
+    phase ^= 1u;
   }
 
   // ---- (2) post-SAO windows, clamped into the fetch rectangle
@@ -451,14 +461,14 @@ __device__ __forceinline__ void sao_alf_tile3(const Pass2Args &a, const Pass2Arg
     for (int i = tid; i < nf0 + nf1 + nf2; i += NT3) {
       if (i < nf0) {
         const FastRect &f = fr[0];
-        const int r = (int)__umulhi((uint32_t)i, f.magic), x = f.x0 + 2 * (i - r * f.npx), y = f.y0 + r;
+        const int r = f.row_of((uint32_t)i), x = f.x0 + 2 * (i - r * f.npx), y = f.y0 + r;
         const uint16_t *d = dL + (y - (Y0 - 4)) * S::DLW + (x - (X0 - 8));
         st32(&sm.sL[(y - (Y0 - 3)) * S::SLW + (x - (X0 - 4))], sao_pair(fs[0], d, maxv2));
       } else {
         const int cc = i < nf0 + nf1 ? 0 : 1;
         const int j = i - nf0 - (cc ? nf1 : 0);
         const FastRect &f = fr[1 + cc];
-        const int r = (int)__umulhi((uint32_t)j, f.magic), x = f.x0 + 2 * (j - r * f.npx), y = f.y0 + r;
+        const int r = f.row_of((uint32_t)j), x = f.x0 + 2 * (j - r * f.npx), y = f.y0 + r;
         const uint16_t *d = sm.dC(cc) + (y - (yc0 - 3)) * S::DCW + (x - (xc0 - 8));
         st32(&sm.sC[cc][(y - (yc0 - 2)) * S::SCW + (x - (xc0 - 4))], sao_pair(fs[1 + cc], d, maxv2));
       }
@@ -627,6 +637,9 @@ __device__ __forceinline__ void sao_alf_tile3(const Pass2Args &a, const Pass2Arg
         o.z = (uint32_t)v[4] | (uint32_t)v[5] << 16;
         o.w = (uint32_t)v[6 % SPT] | (uint32_t)v[7 % SPT] << 16;
         *reinterpret_cast<uint4 *>(out) = o;
+      } else if (vec && SPT == 4) {
+        *reinterpret_cast<uint2 *>(out) = make_uint2((uint32_t)v[0] | (uint32_t)v[1 % SPT] << 16,
+                                                     (uint32_t)v[2 % SPT] | (uint32_t)v[3 % SPT] << 16);
       } else if (vec && SPT == 2) {
         *reinterpret_cast<uint32_t *>(out) = (uint32_t)v[0] | (uint32_t)v[1 % SPT] << 16;
       } else {
@@ -653,7 +666,7 @@ __device__ __forceinline__ void sao_alf_tile3(const Pass2Args &a, const Pass2Arg
         for (int k = 0; k < 4 && gx + k < LD.w; ++k) out[k] = s4[k];
       }
     }
-    return;
+    return true;
   }
   __syncthreads();
 
@@ -744,11 +757,13 @@ __device__ __forceinline__ void sao_alf_tile3(const Pass2Args &a, const Pass2Arg
       for (int p = 0; p < 4 && gx + p < LD.w; ++p) out[p] = (uint16_t)o[p];
     }
   }
+  return true;
 }
 
 template <int W, int TH, bool DO_SAO, bool DO_ALF>
 __global__ void __launch_bounds__(NT3, 4) k_sao_alf_tiles(const __grid_constant__ Pass2Args a) {
-  sao_alf_tile3<W, TH, DO_SAO, DO_ALF, false>(a, &a, blockIdx.x);
+  uint32_t phase = 0;
+  sao_alf_tile3<W, TH, DO_SAO, DO_ALF, false>(a, &a, blockIdx.x, phase);
 }
 
 // Many pictures in one grid: CTAs [first[i], first[i + 1]) are the tiles of
@@ -768,7 +783,50 @@ __global__ void __launch_bounds__(NT3, 4) k_sao_alf_tiles_batch(const Pass2Args 
   uint4 *dst = reinterpret_cast<uint4 *>(&s_args);
   for (int i = threadIdx.x; i < (int)(sizeof(Pass2Args) / 16); i += blockDim.x) dst[i] = src[i];
   __syncthreads();
-  sao_alf_tile3<W, TH, DO_SAO, DO_ALF, true>(s_args, args + lo, (int)(blockIdx.x - first[lo]));
+  uint32_t phase = 0;
+  sao_alf_tile3<W, TH, DO_SAO, DO_ALF, true>(s_args, args + lo, (int)(blockIdx.x - first[lo]), phase);
+}
+
+// Persistent form of the batched launch: a fixed grid (a chosen number of
+// CTAs per SM) drains a device queue of (picture, tile) items -- `queue`
+// counts the items handed out (zero at launch) and items [first[i],
+// first[i + 1]) are picture i's tiles.  Every CTA keeps one barrier over its
+// tiles and reloads the picture's parameters only when the picture changes.
+// The queue only ever grows and no CTA waits for another, so the launch ends
+// once every item has been taken.
+template <int W, int TH, bool DO_SAO, bool DO_ALF>
+__global__ void __launch_bounds__(NT3, 4) k_sao_alf_tiles_queue(const Pass2Args *__restrict__ args,
+                                                                const uint32_t *__restrict__ first, int n,
+                                                                uint32_t total, uint32_t *__restrict__ queue) {
+  using S = Smem3<W, TH>;
+  extern __shared__ __align__(128) uint8_t smem_raw[];
+  S &sm = *reinterpret_cast<S *>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
+  __shared__ Pass2Args s_args;
+  __shared__ uint32_t s_item;
+  if (threadIdx.x == 0) mbar_init(&sm.bar, 1);
+  uint32_t phase = 0;
+  int cur = -1;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(queue, 1u);
+    __syncthreads();  // s_item; the previous tile's last reads of s_args and the windows
+    const uint32_t t = s_item;
+    if (t >= total) break;
+    int lo = 0, hi = n;  // first[lo] <= t < first[hi]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (first[mid] <= t) lo = mid;
+      else hi = mid;
+    }
+    if (lo != cur) {
+      const uint4 *src = reinterpret_cast<const uint4 *>(args + lo);
+      uint4 *dst = reinterpret_cast<uint4 *>(&s_args);
+      for (int i = threadIdx.x; i < (int)(sizeof(Pass2Args) / 16); i += blockDim.x) dst[i] = src[i];
+      cur = lo;
+    }
+    __syncthreads();
+    if (!sao_alf_tile3<W, TH, DO_SAO, DO_ALF, true, true>(s_args, args + lo, (int)(t - first[lo]), phase)) break;
+    __syncthreads();  // every thread is done with this tile before thread 0 takes the next item
+  }
 }
 
 template <int W, int TH>
@@ -776,8 +834,10 @@ constexpr size_t smem3() {
   return sizeof(Smem3<W, TH>) + 128;
 }
 
-// W x TH of a picture's tiles: 64 x 64 for CTBs of 64 and 128, 32 x 32 for 32.
+// W x TH of a picture's tiles: 64 x 64 (or 64 x 32 by tuning) for CTBs of 64
+// and 128, 32 x 32 for 32.
 inline int tile_w(int log2) { return log2 >= 6 ? 64 : 32; }
+inline int tile_h(const Pass2Args &a) { return tile_w(a.ctb_log2) == 64 && a.tile_h == 32 ? 32 : tile_w(a.ctb_log2); }
 
 // Once per kernel and device: the largest shared-memory carveout, so that four
 // CTAs of the tile kernel fit on an SM.
@@ -856,8 +916,9 @@ int launch_one(cudaStream_t st, const Pass2Args &in, bool do_sao, bool do_alf) {
 }  // namespace
 
 void pass2_tma_maps(Pass2Args &a) {
-  if (tile_w(a.ctb_log2) == 64) maps_for<64, 64>(a);
-  else maps_for<32, 32>(a);
+  if (tile_w(a.ctb_log2) == 32) maps_for<32, 32>(a);
+  else if (tile_h(a) == 32) maps_for<64, 32>(a);
+  else maps_for<64, 64>(a);
 }
 
 int pass2_wait_timeouts(uint32_t *count) {
@@ -869,38 +930,72 @@ int pass2_wait_timeouts(uint32_t *count) {
 }
 
 int pass2_packed_variant(Pass2Args &a, bool do_sao, bool do_alf, uint32_t *ctas) {
-  const int W = tile_w(a.ctb_log2);
+  const int W = tile_w(a.ctb_log2), TH = tile_h(a);
   a.tiles_x = (a.ext_w + W - 1) / W;
-  a.tiles_y = (a.ext_h + W - 1) / W;
+  a.tiles_y = (a.ext_h + TH - 1) / TH;
   *ctas = a.ext_w > 0 && a.ext_h > 0 ? (uint32_t)(a.tiles_x * a.tiles_y) : 0;
-  return (W == 64 ? 4 : 0) + (do_sao ? 2 : 0) + (do_alf ? 1 : 0);
+  return (W == 32 ? 0 : (TH == 64 ? 8 : 4)) + (do_sao ? 2 : 0) + (do_alf ? 1 : 0);
 }
 
-int launch_pass2_packed_batch(cudaStream_t st, int variant, const Pass2Args *d_args, const uint32_t *d_first, int n,
-                              uint32_t ctas, uint64_t *launches) {
-  if (!ctas || n <= 0) return H266_OK;
-  auto go = [&](auto kern, size_t shm) -> int {
+namespace {
+int sm_count() {
+  static std::atomic<int> cached{0};
+  int v = cached.load();
+  if (!v) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      v = 148;
+    cached.store(v);
+  }
+  return v;
+}
+
+template <int W, int TH, bool DO_SAO, bool DO_ALF>
+int launch_variant(cudaStream_t st, const Pass2Args *d_args, const uint32_t *d_first, int n, uint32_t ctas, int cps,
+                   uint32_t *d_queue) {
+  const size_t shm = smem3<W, TH>();
+  if (cps > 0 && d_queue) {
+    auto kern = k_sao_alf_tiles_queue<W, TH, DO_SAO, DO_ALF>;
+    H266_TRY(prepare_kernel(kern, shm));
+    const uint32_t grid = std::min<uint32_t>(ctas, (uint32_t)(sm_count() * cps));
+    kern<<<grid, NT3, shm, st>>>(d_args, d_first, n, ctas, d_queue);
+  } else {
+    auto kern = k_sao_alf_tiles_batch<W, TH, DO_SAO, DO_ALF>;
     H266_TRY(prepare_kernel(kern, shm));
     kern<<<ctas, NT3, shm, st>>>(d_args, d_first, n);
-    H266_CUDA(cudaGetLastError());
-    ++*launches;
-    return H266_OK;
-  };
-  switch (variant) {
-    case 7: return go(k_sao_alf_tiles_batch<64, 64, true, true>, smem3<64, 64>());
-    case 6: return go(k_sao_alf_tiles_batch<64, 64, true, false>, smem3<64, 64>());
-    case 5: return go(k_sao_alf_tiles_batch<64, 64, false, true>, smem3<64, 64>());
-    case 4: return go(k_sao_alf_tiles_batch<64, 64, false, false>, smem3<64, 64>());
-    case 3: return go(k_sao_alf_tiles_batch<32, 32, true, true>, smem3<32, 32>());
-    case 2: return go(k_sao_alf_tiles_batch<32, 32, true, false>, smem3<32, 32>());
-    case 1: return go(k_sao_alf_tiles_batch<32, 32, false, true>, smem3<32, 32>());
-    default: return go(k_sao_alf_tiles_batch<32, 32, false, false>, smem3<32, 32>());
   }
+  H266_CUDA(cudaGetLastError());
+  return H266_OK;
+}
+}  // namespace
+
+int launch_pass2_packed_batch(cudaStream_t st, int variant, const Pass2Args *d_args, const uint32_t *d_first, int n,
+                              uint32_t ctas, int ctas_per_sm, uint32_t *d_queue, uint64_t *launches) {
+  if (!ctas || n <= 0) return H266_OK;
+  int rc;
+  const int c = ctas_per_sm;
+  switch (variant) {
+    case 11: rc = launch_variant<64, 64, true, true>(st, d_args, d_first, n, ctas, c, d_queue); break;
+    case 10: rc = launch_variant<64, 64, true, false>(st, d_args, d_first, n, ctas, c, d_queue); break;
+    case 9: rc = launch_variant<64, 64, false, true>(st, d_args, d_first, n, ctas, c, d_queue); break;
+    case 8: rc = launch_variant<64, 64, false, false>(st, d_args, d_first, n, ctas, c, d_queue); break;
+    case 7: rc = launch_variant<64, 32, true, true>(st, d_args, d_first, n, ctas, c, d_queue); break;
+    case 6: rc = launch_variant<64, 32, true, false>(st, d_args, d_first, n, ctas, c, d_queue); break;
+    case 5: rc = launch_variant<64, 32, false, true>(st, d_args, d_first, n, ctas, c, d_queue); break;
+    case 4: rc = launch_variant<64, 32, false, false>(st, d_args, d_first, n, ctas, c, d_queue); break;
+    case 3: rc = launch_variant<32, 32, true, true>(st, d_args, d_first, n, ctas, c, d_queue); break;
+    case 2: rc = launch_variant<32, 32, true, false>(st, d_args, d_first, n, ctas, c, d_queue); break;
+    case 1: rc = launch_variant<32, 32, false, true>(st, d_args, d_first, n, ctas, c, d_queue); break;
+    default: rc = launch_variant<32, 32, false, false>(st, d_args, d_first, n, ctas, c, d_queue); break;
+  }
+  if (rc == H266_OK) ++*launches;
+  return rc;
 }
 
 int launch_pass2_packed(cudaStream_t st, const Pass2Args &a, bool do_sao, bool do_alf, uint64_t *launches) {
   if (a.ext_w <= 0 || a.ext_h <= 0) return H266_OK;
-  const int rc = tile_w(a.ctb_log2) == 64 ? launch_one<64, 64>(st, a, do_sao, do_alf)
+  const int rc = tile_w(a.ctb_log2) == 64 ? (tile_h(a) == 32 ? launch_one<64, 32>(st, a, do_sao, do_alf)
+                                                              : launch_one<64, 64>(st, a, do_sao, do_alf))
                                           : launch_one<32, 32>(st, a, do_sao, do_alf);
   if (rc == H266_OK) ++*launches;
   return rc;

@@ -34,7 +34,8 @@ EXPORTS = [
     "h266_apply_sao_clipped", "h266_apply_alf_clipped", "h266_apply_in_loop_filters",
     "h266_apply_in_loop_filters_batch", "h266_ctx_set_profiling", "h266_ctx_profile", "h266_chain_plan_create",
     "h266_chain_plan_create_ex", "h266_chain_plan_device_sideinfo", "h266_ctx_set_tuning", "h266_ctx_set_tuning_for",
-    "h266_ctx_get_tuning", "h266_ctx_host_profile",
+    "h266_ctx_get_tuning", "h266_ctx_host_profile", "h266_batch_graph_create", "h266_batch_graph_launch",
+    "h266_batch_graph_destroy",
     "h266_chain_plan_execute", "h266_chain_plan_execute_batch", "h266_chain_plan_destroy",
     "h266_apply_in_loop_filters_noalloc", "h266_server_create", "h266_server_submit", "h266_server_wait",
     "h266_server_stats", "h266_server_replay", "h266_server_destroy", "h266_alf_decide_and_apply_clipped",
@@ -83,6 +84,9 @@ def lib():
         L.h266_ctx_set_tuning_for.argtypes = [vp, u32, u32, u32, C.c_char_p, C.c_int64]
         L.h266_ctx_get_tuning.argtypes = [vp, C.c_char_p, C.POINTER(C.c_int64)]
         L.h266_ctx_host_profile.argtypes = [vp, vp]
+        L.h266_batch_graph_create.argtypes = [vp, u32, vp, vp, C.POINTER(vp)]
+        L.h266_batch_graph_launch.argtypes = [vp, vp]
+        L.h266_batch_graph_destroy.argtypes = [vp]
         L.h266_chain_plan_execute.argtypes = [vp, vp, vp]
         L.h266_chain_plan_execute_batch.argtypes = [vp, u32, vp, vp]
         L.h266_server_create.argtypes = [i32, u32, u64, C.POINTER(vp)]
@@ -252,6 +256,10 @@ class Context:
         a, keep = fa.to_ctypes()
         _check(lib().h266_apply_in_loop_filters(self._h, C.byref(cp), C.byref(a)))
 
+    def batch_graph(self, plans, pics) -> "BatchGraph":
+        """Records h266_chain_plan_execute_batch(plans, pics) as a CUDA graph."""
+        return BatchGraph(self, plans, pics)
+
     def execute_plans(self, plans, pics):
         """h266_chain_plan_execute_batch: plans[i] on device picture pics[i], batched launches."""
         cps = [p.to_ctypes() for p in pics]
@@ -325,6 +333,33 @@ class ChainPlan:
     def close(self):
         if self._h:
             lib().h266_chain_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BatchGraph:
+    """h266_batch_graph: a batched plan execution recorded as a CUDA graph."""
+
+    def __init__(self, ctx: "Context", plans, pics):
+        self.ctx = ctx
+        self._keep = [p.to_ctypes() for p in pics]
+        P = (C.c_void_p * len(plans))(*[pl._h.value for pl in plans])
+        Q = (C.c_void_p * len(pics))(*[C.addressof(c) for c in self._keep])
+        h = C.c_void_p()
+        _check(lib().h266_batch_graph_create(ctx._h, len(plans), P, Q, C.byref(h)))
+        self._h = h
+
+    def launch(self):
+        _check(lib().h266_batch_graph_launch(self.ctx._h, self._h))
+
+    def close(self):
+        if self._h:
+            lib().h266_batch_graph_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -62,6 +62,9 @@ WORKLOADS = {
     # rows not a multiple of 8 samples (unaligned strip loads), height not a
     # multiple of 4 (a partial last band)
     "odd_stride": lambda s: W.make_workload(7500 + s, 202, 138, 10, 5, inter_frac=0.5, ccalf=True, lmcs=True),
+    # CTB 32 with a last chroma tile of 4 columns (one sample pair per row inside
+    # the clip rectangle's interior) and aligned luma rows
+    "ctb32_tail4": lambda s: W.make_workload(7700 + s, 200, 136, 10, 5, ccalf=True, lmcs=True),
 }
 
 
@@ -373,6 +376,54 @@ def test_plan_batch_mixed_sizes_x12(ctx):
     """Mixed sizes as in the 64-picture batch (832x480 CTU 64 8-bit, 1080p and
     2160p 10-bit, each picture with its own ALF / CC-ALF / LMCS tables)."""
     _batched_plans_match_oracle(ctx, [W.config4(4000 + i) for i in range(12)], "mixed x12")
+
+
+@pytest.mark.parametrize("cps,tile_h", [(0, 32), (1, 64), (2, 32), (4, 64)])
+def test_plan_batch_persistent_and_tile_shapes(cps, tile_h):
+    """The batched SAO / ALF pass as a persistent launch draining the (picture,
+    tile) queue (cps CTAs per SM) and with 64 x 32 tiles, on pictures of mixed
+    sizes, CTB sizes and bit depths, plans with host- and device-built side
+    information: every result equal to the oracle's."""
+    items = [small_c2(80), WORKLOADS["ctb64_8bit"](81), WORKLOADS["c1"](82), WORKLOADS["stress"](83),
+             W.config2(84), W.make_workload(85, 200, 136, 10, 5, ccalf=True, lmcs=True)]
+    with native.Context(0) as c:
+        c.set_tuning("sao_alf_ctas_per_sm", cps)
+        c.set_tuning("sao_alf_tile_h", tile_h)
+        _batched_plans_match_oracle(c, items, f"cps {cps} tile_h {tile_h}", device_sideinfo=cps % 2 == 1)
+
+
+@pytest.mark.parametrize("cps", [0, 2])
+def test_batch_graph_replays_match_oracle(cps):
+    """A batched plan execution recorded once as a CUDA graph and replayed on
+    fresh samples three times (device-built and host-built side information,
+    one-CTA-per-tile and persistent SAO / ALF launches): bit-exact each time."""
+    import torch
+
+    items = [W.config2(90), small_c2(91), WORKLOADS["ctb64_8bit"](92), WORKLOADS["stress"](93)]
+    wants = [p.copy() for p, _ in items]
+    for w, (_, f) in zip(wants, items):
+        oracle.apply_in_loop_filters(w, f)
+    with native.Context(0) as c:
+        c.set_tuning("sao_alf_ctas_per_sm", cps)
+        plans = [c.plan(p, f, device_sideinfo=True) for p, f in items]
+        devs = [native.DevicePicture.from_host(p) for p, _ in items]
+        torch.cuda.synchronize()
+        g = c.batch_graph(plans, devs)
+        try:
+            for rnd in range(3):
+                for d, (p, _) in zip(devs, items):
+                    fresh = native.DevicePicture.from_host(p)
+                    for t, u in zip((d.luma, d.cb, d.cr), (fresh.luma, fresh.cb, fresh.cr)):
+                        t.copy_(u)
+                torch.cuda.synchronize()
+                g.launch()
+                c.synchronize()
+                for i, (d, w) in enumerate(zip(devs, wants)):
+                    assert_same(d.to_host(), w, f"graph replay {rnd} picture {i}")
+        finally:
+            g.close()
+            for pl in plans:
+                pl.close()
 
 
 def test_profiling_counts_every_family(ctx):
