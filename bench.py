@@ -357,8 +357,12 @@ def run_served(ctx, local_rank, seconds: float, rates=(1, 4, 8, 12)):
     out = {"streams": len(streams), "mix": "12x 832x480@60, 14x 1920x1080@60, 6x 3840x2160@30, 10-bit",
            "nominal_mpx_per_s": round(nominal_mpx, 1), "seconds": seconds, "ring_per_stream": SERVED_RING,
            "latency": "scheduled arrival to completion"}
-    for mode, max_batch in (("batched", 64), ("plain", 1)):
+    # continuous batching with the library's default batch cap (one 1080p
+    # picture's samples), with a 2160p cap, and plain per-request launches
+    for mode, max_batch, cap in (("batched", 64, None), ("batched_cap_2160p", 64, 3840 * 2160), ("plain", 1, None)):
         with native.Server(local_rank, max_batch=max_batch, memory_budget=40 << 30) as srv:
+            if cap is not None:
+                srv.set_batch_pixels(cap)
             warm = [srv.submit(plan, dev) for st in streams for plan, dev, _ in st["ring"]]
             for tk in warm:
                 srv.wait(tk)
@@ -597,6 +601,23 @@ def run_encoder_trials(ctx, local_rank, stream, steps: int, n_pics: int = 4):
     oracle.sao_chroma_merge(s_, r_, indep, 15, 9, bit_depth=10, ctb_log2=7)
     sao["chroma_merge"] = {"ms_per_picture": round(m_total / m_calls, 4), "launches": 23,
                            "cpu_oracle_ms_per_picture": round((time.perf_counter() - t0) * 1e3, 1)}
+    # the same merge batched over the 4 pictures: one launch per anti-diagonal for all of them
+    indeps = [native.sao_decide_picture(ctx, d_[0], d_[1], ctb_log2=7, bit_depth=10) for d_ in devs]
+    want_b = [native.sao_chroma_merge(ctx, d_[0], d_[1], ind, 15, 9, bit_depth=10, ctb_log2=7)
+              for d_, ind in zip(devs, indeps)]
+    run_b = lambda: native.sao_chroma_merge_batch(ctx, [d_[0] for d_ in devs], [d_[1] for d_ in devs], indeps,
+                                                  [(15, 9)] * len(devs), bit_depth=10, ctb_log2=7)
+    got_b = run_b()
+    same = all(np.array_equal(g[1], w[1]) and g[0].tobytes() == w[0].tobytes() for g, w in zip(got_b, want_b))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(max(1, steps)):
+        run_b()
+    b_ms = (time.perf_counter() - t0) * 1e3 / max(1, steps) / len(devs)
+    sao["chroma_merge_batch"] = {"pictures": len(devs), "ms_per_picture": round(b_ms, 4),
+                                 "launches_per_call": 23, "same_as_per_picture_calls": bool(same),
+                                 "path": "h266_sao_chroma_merge_batch on device pictures (host wall time per call, "
+                                         "records back in host memory)"}
     del devs
     torch.cuda.synchronize()
     return {"workload": "encoder luma ALF decision, 1920x1080 10-bit CTU 128, 16 fixed sets + 1 APS set",

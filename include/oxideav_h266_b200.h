@@ -372,6 +372,16 @@ int h266_sao_chroma_merge(h266_ctx *ctx, const h266_picture *src, const h266_pic
                           const h266_sao_ctb_params *independent, uint32_t w_ctbs, uint32_t h_ctbs,
                           uint32_t bit_depth, uint32_t ctb_log2_size_y, h266_sao_ctb_params *merged,
                           uint8_t *merge_map);
+/* The same merge for n pictures at once (device pictures, H266_MEM_DEVICE):
+ * each CTB anti-diagonal is one launch over the CTBs of every picture on it,
+ * so the diagonals' few CTBs per picture fill the GPU together.  Per picture
+ * i: srcs[i], pres[i], independent[i] (w_ctbs[i] x h_ctbs[i] records),
+ * merged[i] and merge_maps[i] as for h266_sao_chroma_merge; results are the
+ * same as n separate calls.  Returns when the results are in host memory. */
+int h266_sao_chroma_merge_batch(h266_ctx *ctx, uint32_t n, const h266_picture *const *srcs,
+                                const h266_picture *const *pres, const h266_sao_ctb_params *const *independent,
+                                const uint32_t *w_ctbs, const uint32_t *h_ctbs, uint32_t bit_depth,
+                                uint32_t ctb_log2_size_y, h266_sao_ctb_params *const *merged, uint8_t *const *merge_maps);
 
 /* ---- recon-side LMCS (src/lmcs.rs:169-290, src/ctu.rs:734-742, 1701-1815) */
 typedef struct h266_rect {
@@ -563,6 +573,11 @@ int h266_server_stats(h266_server *server, uint64_t *requests, uint64_t *batches
  * For load tests of a serving configuration. */
 int h266_server_replay(h266_server *server, uint32_t n, h266_chain_plan *const *plans, h266_picture *const *pics,
                        const double *arrival_s, const int32_t *after, double *latency_ms);
+/* A batch admits more than one request only while its pictures' luma samples
+ * stay within `px` (default 1920 x 1080; 0: no cap), so a large picture does
+ * not wait for a batch of smaller ones.  A batch of one request runs with
+ * per-kernel launches, like h266_chain_plan_execute. */
+int h266_server_set_batch_pixels(h266_server *server, uint64_t px);
 int h266_server_destroy(h266_server *server); /* drains the queue first */
 
 /* ---- allocation-free chain ---------------------------------------------------

@@ -1553,6 +1553,101 @@ int h266_sao_chroma_merge(h266_ctx *ctx, const h266_picture *src, const h266_pic
   return H266_OK;
 }
 
+int h266_sao_chroma_merge_batch(h266_ctx *ctx, uint32_t np, const h266_picture *const *srcs,
+                                const h266_picture *const *pres, const h266_sao_ctb_params *const *indeps,
+                                const uint32_t *wcs, const uint32_t *hcs, uint32_t bd, uint32_t log2,
+                                h266_sao_ctb_params *const *merged, uint8_t *const *maps) {
+  H266_TRY(check_ctx(ctx));
+  if (np && (!srcs || !pres || !indeps || !wcs || !hcs || !merged || !maps))
+    return set_error(H266_ERR_INVALID_ARGUMENT, "NULL batch arrays");
+  if (bd < 8 || bd > 16) return set_error(H266_ERR_INVALID_ARGUMENT, "bit_depth must be 8..16");
+  if (log2 < 1 || log2 > 7) return set_error(H266_ERR_INVALID_ARGUMENT, "ctb_log2_size_y must be 1..7");
+  // layout of the device work area: per picture its merged records, map and work, 256-byte sections
+  auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  std::vector<size_t> off_rec(np), off_map(np), off_work(np);
+  size_t total = 0;
+  uint32_t n_diags = 0;
+  for (uint32_t i = 0; i < np; ++i) {
+    const h266_picture *src = srcs[i], *pre = pres[i];
+    H266_TRY(check_picture(src));
+    H266_TRY(check_picture(pre));
+    if (src->mem != H266_MEM_DEVICE || pre->mem != H266_MEM_DEVICE)
+      return set_error(H266_ERR_INVALID_ARGUMENT, "the batched merge takes device pictures (H266_MEM_DEVICE)");
+    const uint64_t n = (uint64_t)wcs[i] * hcs[i];
+    if (n && (!indeps[i] || !merged[i] || !maps[i])) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL records / map");
+    if (n > (1u << 22)) return set_error(H266_ERR_UNSUPPORTED, "CTB grid too large");
+    if (pre->cb.width != pre->cr.width || pre->cb.height != pre->cr.height)
+      return set_error(H266_ERR_INVALID_ARGUMENT, "Cb and Cr planes differ in size");
+    if (src->cb.width < pre->cb.width || src->cb.height < pre->cb.height || src->cr.width < pre->cb.width ||
+        src->cr.height < pre->cb.height)
+      return set_error(H266_ERR_INVALID_ARGUMENT, "original chroma planes smaller than the reconstruction's");
+    off_rec[i] = total;
+    total += al(n * sizeof(h266_sao_ctb_params));
+    off_map[i] = total;
+    total += al(n);
+    off_work[i] = total;
+    total += al(sao_merge_work_bytes(n));
+    if (n) n_diags = std::max(n_diags, wcs[i] + hcs[i] - 1);
+  }
+  if (!np || !n_diags) return H266_OK;
+  Guard g(ctx->device);
+  Lane &ln = ctx->main;
+  H266_TRY(ln.walk.ensure(std::max<size_t>(total, 256)));
+  uint8_t *work = ln.walk.as<uint8_t>();
+  H266_CUDA(cudaMemsetAsync(work, 0, total, ln.stream));  // per-CTB arrival counts start at zero
+  // one upload: every picture's independent records, merge parameters and per-diagonal picture tables
+  Prep &pr = ctx_prep(ctx, 0);
+  pr.blob.clear();
+  Blob blob{pr.blob};
+  std::vector<size_t> off_ind(np);
+  for (uint32_t i = 0; i < np; ++i)
+    off_ind[i] = blob.put(indeps[i], (size_t)wcs[i] * hcs[i] * sizeof(h266_sao_ctb_params));
+  std::vector<uint32_t> first((size_t)n_diags * (np + 1), 0), totals(n_diags, 0);
+  for (uint32_t d = 0; d < n_diags; ++d)
+    for (uint32_t i = 0; i < np; ++i) {
+      const int wc = (int)wcs[i], hc = (int)hcs[i];
+      int c = 0;
+      if (wc && hc && (int)d <= wc + hc - 2) c = std::min(hc - 1, (int)d) - std::max(0, (int)d - (wc - 1)) + 1;
+      first[(size_t)d * (np + 1) + i + 1] = first[(size_t)d * (np + 1) + i] + (uint32_t)std::max(c, 0);
+      totals[d] = first[(size_t)d * (np + 1) + i + 1];
+    }
+  const size_t off_first = blob.put(first.data(), first.size() * sizeof(uint32_t));
+  const size_t asz = sao_merge_args_size();
+  std::vector<uint8_t> args(asz * np);
+  const size_t off_args = blob.put(args.data(), args.size());  // filled in below, once the base is known
+  uint8_t *base = nullptr;
+  H266_TRY(ln.side.ensure(pr.blob.size()));
+  base = ln.side.as<uint8_t>();
+  for (uint32_t i = 0; i < np; ++i) {
+    const h266_picture &src = *srcs[i], &pre = *pres[i];
+    const DPlane S[2] = {dplane(src.cb, src.cb.samples, (int64_t)std::max<uint64_t>(src.cb.stride, 1)),
+                         dplane(src.cr, src.cr.samples, (int64_t)std::max<uint64_t>(src.cr.stride, 1))};
+    const DPlane Q[2] = {dplane(pre.cb, pre.cb.samples, (int64_t)std::max<uint64_t>(pre.cb.stride, 1)),
+                         dplane(pre.cr, pre.cr.samples, (int64_t)std::max<uint64_t>(pre.cr.stride, 1))};
+    fill_sao_merge_args(pr.blob.data() + off_args + asz * i, S, Q, (int)bd, (1 << log2) / 2, (int)wcs[i], (int)hcs[i],
+                        reinterpret_cast<const h266_sao_ctb_params *>(base + off_ind[i]),
+                        reinterpret_cast<h266_sao_ctb_params *>(work + off_rec[i]), work + off_map[i],
+                        work + off_work[i]);
+  }
+  H266_TRY(upload_blob(ln, pr.blob, &base));
+  ctx->h2d_bytes += pr.blob.size();
+  {
+    Prof pf(ctx, ln.stream, H266_PROF_SAO_ALF);
+    H266_TRY(launch_sao_chroma_merge_batch(ln.stream, base + off_args, reinterpret_cast<const uint32_t *>(base + off_first),
+                                           (int)np, (int)n_diags, totals.data(), &ctx->launches));
+  }
+  for (uint32_t i = 0; i < np; ++i) {
+    const size_t n = (size_t)wcs[i] * hcs[i];
+    if (!n) continue;
+    H266_CUDA(cudaMemcpyAsync(merged[i], work + off_rec[i], n * sizeof(h266_sao_ctb_params), cudaMemcpyDeviceToHost,
+                              ln.stream));
+    H266_CUDA(cudaMemcpyAsync(maps[i], work + off_map[i], n, cudaMemcpyDeviceToHost, ln.stream));
+    ctx->d2h_bytes += n * (sizeof(h266_sao_ctb_params) + 1);
+  }
+  H266_CUDA(cudaStreamSynchronize(ln.stream));
+  return H266_OK;
+}
+
 int h266_sao_decide_picture(h266_ctx *ctx, const h266_picture *src, const h266_picture *rec, uint32_t log2,
                             uint32_t bd, uint32_t sao_luma, uint32_t sao_chroma, h266_sao_ctb_params *out,
                             uint64_t n_out) {
@@ -2282,14 +2377,12 @@ int h266_chain_plan_create_ex(h266_ctx *ctx, const h266_picture *pic, const h266
   return H266_OK;
 }
 
-int h266_chain_plan_execute(h266_ctx *ctx, h266_chain_plan *plan, h266_picture *pic) {
-  H266_TRY(check_ctx(ctx));
-  if (!plan) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL plan");
-  H266_TRY(check_picture(pic));
-  if (pic->mem != H266_MEM_DEVICE) return set_error(H266_ERR_INVALID_ARGUMENT, "plans execute on device pictures");
-  if (!same_geometry(*pic, plan->geom)) return set_error(H266_ERR_INVALID_ARGUMENT, "picture geometry differs from the plan");
-  if (plan->device != ctx->device) return set_error(H266_ERR_INVALID_ARGUMENT, "plan belongs to another device");
-  Guard g(ctx->device);
+}  // extern "C"
+
+namespace h266 {
+// One plan on one device picture, queued on `stream` with per-kernel launches
+// (no batch parameter tables); the caller has checked the pair.
+int exec_plan_single(h266_ctx *ctx, cudaStream_t stream, h266_chain_plan *plan, h266_picture *pic) {
   DPlane P[3], S[3];
   H266_TRY(picture_to_device(ctx->main, *pic, P));
   for (int i = 0; i < 3; ++i)
@@ -2301,9 +2394,24 @@ int h266_chain_plan_execute(h266_ctx *ctx, h266_chain_plan *plan, h266_picture *
   h.do_sao = plan->do_sao;
   h.do_alf = plan->do_alf;
   h.packed = plan->packed;
-  return exec_chain(ctx, ctx->stream, st.base, st, plan->db, h, plan->lmcs ? plan->lut.as<uint16_t>() : nullptr,
+  return exec_chain(ctx, stream, st.base, st, plan->db, h, plan->lmcs ? plan->lut.as<uint16_t>() : nullptr,
                     plan->deblock_bd, P, S, plan->walk.as<uint8_t>());
 }
+}  // namespace h266
+
+extern "C" {
+
+int h266_chain_plan_execute(h266_ctx *ctx, h266_chain_plan *plan, h266_picture *pic) {
+  H266_TRY(check_ctx(ctx));
+  if (!plan) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL plan");
+  H266_TRY(check_picture(pic));
+  if (pic->mem != H266_MEM_DEVICE) return set_error(H266_ERR_INVALID_ARGUMENT, "plans execute on device pictures");
+  if (!same_geometry(*pic, plan->geom)) return set_error(H266_ERR_INVALID_ARGUMENT, "picture geometry differs from the plan");
+  if (plan->device != ctx->device) return set_error(H266_ERR_INVALID_ARGUMENT, "plan belongs to another device");
+  Guard g(ctx->device);
+  return exec_plan_single(ctx, ctx->stream, plan, pic);
+}
+
 
 }  // extern "C"
 
@@ -2637,6 +2745,10 @@ struct ServerResult {
 struct h266_server {
   h266_ctx *ctx = nullptr;  // the server's own context, used by the dispatcher thread only
   uint32_t max_batch = 1;
+  // a batch grows past one request only while its luma samples stay within
+  // this (0: no cap): a large picture is not held back by the small ones it
+  // would share a batch with
+  uint64_t batch_px = 1920ull * 1080;
   uint64_t budget = 0;
   std::mutex mu;
   std::condition_variable cv_work, cv_flight, cv_done;
@@ -2668,10 +2780,13 @@ void server_dispatch(h266_server *s) {
     // admit in arrival order up to max_batch and the memory budget (an idle
     // server always admits the first request)
     std::vector<ServerReq> take;
-    uint64_t bytes = 0;
+    uint64_t bytes = 0, px = 0;
     while (!s->queue.empty() && take.size() < s->max_batch) {
       const ServerReq &r = s->queue.front();
       if ((s->inflight > 0 || !take.empty()) && s->inflight + bytes + r.bytes > s->budget) break;
+      const uint64_t rpx = (uint64_t)r.pic.luma.width * r.pic.luma.height;
+      if (!take.empty() && s->batch_px && px + rpx > s->batch_px) break;
+      px += rpx;
       bytes += r.bytes;
       take.push_back(r);
       s->queue.pop_front();
@@ -2690,7 +2805,9 @@ void server_dispatch(h266_server *s) {
       pics[i] = &take[i].pic;
     }
     ServerSlot &sl = s->slots[slot];
-    int rc = exec_plan_batch(s->ctx, sl.bb, sl.stream, (uint32_t)take.size(), plans.data(), pics.data());
+    // one request: per-kernel launches, no batch tables to build and upload
+    int rc = take.size() == 1 ? exec_plan_single(s->ctx, sl.stream, plans[0], pics[0])
+                              : exec_plan_batch(s->ctx, sl.bb, sl.stream, (uint32_t)take.size(), plans.data(), pics.data());
     std::string msg = rc == H266_OK ? std::string() : std::string(h266_last_error());
     if (cudaEventRecord(sl.done, sl.stream) != cudaSuccess && rc == H266_OK) {
       rc = H266_ERR_CUDA;
@@ -2869,6 +2986,13 @@ int h266_server_replay(h266_server *s, uint32_t n, h266_chain_plan *const *plans
   }
   collector.join();
   if (first_rc.load() != H266_OK) return set_error(first_rc.load(), first_msg);
+  return H266_OK;
+}
+
+int h266_server_set_batch_pixels(h266_server *s, uint64_t px) {
+  if (!s) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->batch_px = px;
   return H266_OK;
 }
 

@@ -350,6 +350,17 @@ int launch_sao_chroma_merge(cudaStream_t st, const DPlane src[2], const DPlane p
                             int w_ctbs, int h_ctbs, const h266_sao_ctb_params *d_indep, h266_sao_ctb_params *d_merged,
                             uint8_t *d_map, void *d_work, uint64_t *launches);
 inline size_t sao_merge_work_bytes(size_t n_ctbs) { return n_ctbs * 3 * 8 + n_ctbs * 4; }
+// Batched merge: one launch per anti-diagonal over many pictures.
+// fill_sao_merge_args writes one picture's parameters (sao_merge_args_size()
+// bytes; d_work laid out as sao_merge_work_bytes, its per-CTB counts zeroed by
+// the caller); d_first holds per diagonal the n + 1 prefix sums of the
+// pictures' CTB counts on it, h_totals the diagonals' totals.
+size_t sao_merge_args_size();
+void fill_sao_merge_args(void *out, const DPlane src[2], const DPlane pre[2], int bd, int chr_ctb, int w_ctbs,
+                         int h_ctbs, const h266_sao_ctb_params *d_indep, h266_sao_ctb_params *d_merged, uint8_t *d_map,
+                         void *d_work);
+int launch_sao_chroma_merge_batch(cudaStream_t st, const void *d_args, const uint32_t *d_first, int n, int n_diags,
+                                  const uint32_t *h_totals, uint64_t *launches);
 int launch_sao_decide(cudaStream_t st, const DPlane src[3], const DPlane rec[3], int bd, int log2, int w_ctbs,
                       int h_ctbs, bool luma_on, bool chroma_on, void *d_stats, uint32_t *d_err,
                       h266_sao_ctb_params *d_out, uint64_t *launches);

@@ -12,6 +12,8 @@
 // (src/sao_enc.rs:450-477).
 #include <climits>
 
+#include <cstring>
+
 #include "internal.h"
 
 namespace h266 {
@@ -340,8 +342,7 @@ constexpr int kMergeThreads = 512;
 // stored per CTB; the CTA that completes a CTB's set of candidates (per-CTB
 // arrival counter, zeroed by the host; no CTA waits for another) makes the
 // decision.
-__global__ void __launch_bounds__(kMergeThreads) k_sao_merge_diag(const __grid_constant__ MergeArgs a) {
-  const int ry = a.first_ry + blockIdx.x, rx = a.diag - ry, k = blockIdx.y;
+__device__ __forceinline__ void merge_cta(const MergeArgs &a, int ry, int rx, int k) {
   if ((k == 1 && rx == 0) || (k == 2 && ry == 0)) return;  // no such neighbour (uniform per CTA)
   const int i = ry * a.w_ctbs + rx;
   const int tid = threadIdx.x, maxv = (1 << a.bd) - 1;
@@ -397,7 +398,63 @@ __global__ void __launch_bounds__(kMergeThreads) k_sao_merge_diag(const __grid_c
   a.map[i] = (uint8_t)choice;
 }
 
+__global__ void __launch_bounds__(kMergeThreads) k_sao_merge_diag(const __grid_constant__ MergeArgs a) {
+  const int ry = a.first_ry + blockIdx.x;
+  merge_cta(a, ry, a.diag - ry, blockIdx.y);
+}
+
+// One anti-diagonal `diag` of many pictures: CTAs [first[p], first[p + 1]) of
+// the x dimension are picture p's CTBs on it (from its first row up), y the
+// candidate.  Pictures without CTBs on the diagonal have none.
+__global__ void __launch_bounds__(kMergeThreads) k_sao_merge_diag_batch(const MergeArgs *__restrict__ args,
+                                                                         const uint32_t *__restrict__ first, int n,
+                                                                         int diag) {
+  int lo = 0, hi = n;  // first[lo] <= blockIdx.x < first[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (first[mid] <= blockIdx.x) lo = mid;
+    else hi = mid;
+  }
+  const MergeArgs &a = args[lo];
+  const int ry0 = max(0, diag - (a.w_ctbs - 1));
+  const int ry = ry0 + (int)(blockIdx.x - first[lo]);
+  merge_cta(a, ry, diag - ry, blockIdx.y);
+}
+
 }  // namespace
+
+size_t sao_merge_args_size() { return sizeof(MergeArgs); }
+
+void fill_sao_merge_args(void *out, const DPlane src[2], const DPlane pre[2], int bd, int chr_ctb, int w_ctbs,
+                         int h_ctbs, const h266_sao_ctb_params *d_indep, h266_sao_ctb_params *d_merged, uint8_t *d_map,
+                         void *d_work) {
+  MergeArgs a{};
+  for (int c = 0; c < 2; ++c) {
+    a.src[c] = src[c];
+    a.pre[c] = pre[c];
+  }
+  a.bd = bd;
+  a.chr_ctb = chr_ctb;
+  a.w_ctbs = w_ctbs;
+  a.indep = d_indep;
+  a.merged = d_merged;
+  a.map = d_map;
+  a.sse = static_cast<unsigned long long *>(d_work);  // the layout of sao_merge_work_bytes; counts zeroed by the caller
+  a.count = reinterpret_cast<unsigned int *>(a.sse + (size_t)w_ctbs * h_ctbs * 3);
+  std::memcpy(out, &a, sizeof a);
+}
+
+int launch_sao_chroma_merge_batch(cudaStream_t st, const void *d_args, const uint32_t *d_first, int n, int n_diags,
+                                  const uint32_t *h_totals, uint64_t *launches) {
+  const MergeArgs *args = static_cast<const MergeArgs *>(d_args);
+  for (int d = 0; d < n_diags; ++d) {
+    if (!h_totals[d]) continue;
+    k_sao_merge_diag_batch<<<dim3(h_totals[d], 3), kMergeThreads, 0, st>>>(args, d_first + (size_t)d * (n + 1), n, d);
+    H266_CUDA(cudaGetLastError());
+    ++*launches;
+  }
+  return H266_OK;
+}
 
 int launch_sao_chroma_merge(cudaStream_t st, const DPlane src[2], const DPlane pre[2], int bd, int chr_ctb,
                             int w_ctbs, int h_ctbs, const h266_sao_ctb_params *d_indep, h266_sao_ctb_params *d_merged,

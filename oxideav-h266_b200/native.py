@@ -35,7 +35,7 @@ EXPORTS = [
     "h266_apply_in_loop_filters_batch", "h266_ctx_set_profiling", "h266_ctx_profile", "h266_chain_plan_create",
     "h266_chain_plan_create_ex", "h266_chain_plan_device_sideinfo", "h266_ctx_set_tuning", "h266_ctx_set_tuning_for",
     "h266_ctx_get_tuning", "h266_ctx_host_profile", "h266_batch_graph_create", "h266_batch_graph_launch",
-    "h266_batch_graph_destroy",
+    "h266_batch_graph_destroy", "h266_server_set_batch_pixels", "h266_sao_chroma_merge_batch",
     "h266_chain_plan_execute", "h266_chain_plan_execute_batch", "h266_chain_plan_destroy",
     "h266_apply_in_loop_filters_noalloc", "h266_server_create", "h266_server_submit", "h266_server_wait",
     "h266_server_stats", "h266_server_replay", "h266_server_destroy", "h266_alf_decide_and_apply_clipped",
@@ -87,6 +87,8 @@ def lib():
         L.h266_batch_graph_create.argtypes = [vp, u32, vp, vp, C.POINTER(vp)]
         L.h266_batch_graph_launch.argtypes = [vp, vp]
         L.h266_batch_graph_destroy.argtypes = [vp]
+        L.h266_server_set_batch_pixels.argtypes = [vp, u64]
+        L.h266_sao_chroma_merge_batch.argtypes = [vp, u32, vp, vp, vp, vp, vp, u32, u32, vp, vp]
         L.h266_chain_plan_execute.argtypes = [vp, vp, vp]
         L.h266_chain_plan_execute_batch.argtypes = [vp, u32, vp, vp]
         L.h266_server_create.argtypes = [i32, u32, u64, C.POINTER(vp)]
@@ -413,6 +415,10 @@ class Server:
                                         lat.ctypes.data))
         return lat
 
+    def set_batch_pixels(self, px: int):
+        """Cap on a batch's luma samples beyond its first request (0: none)."""
+        _check(lib().h266_server_set_batch_pixels(self._h, int(px)))
+
     def stats(self) -> tuple:
         r, b = C.c_uint64(), C.c_uint64()
         _check(lib().h266_server_stats(self._h, C.byref(r), C.byref(b)))
@@ -545,3 +551,21 @@ def sao_chroma_merge(ctx: Context, src, pre, indep, w_ctbs: int, h_ctbs: int, *,
     _check(lib().h266_sao_chroma_merge(ctx._h, C.byref(s_c), C.byref(p_c), ind.ctypes.data, w_ctbs, h_ctbs,
                                        bit_depth, ctb_log2, merged.ctypes.data, m.ctypes.data))
     return merged, m[: len(ind)]
+
+
+def sao_chroma_merge_batch(ctx: Context, srcs, pres, indeps, grids, *, bit_depth: int, ctb_log2: int):
+    """h266_sao_chroma_merge_batch on device pictures: one (merged, map) per
+    picture, grids[i] = (w_ctbs, h_ctbs)."""
+    n = len(srcs)
+    sc, pc = [s_.to_ctypes() for s_ in srcs], [p_.to_ctypes() for p_ in pres]
+    inds = [np.ascontiguousarray(x, dtype=abi.SAO_CTB_PARAMS) for x in indeps]
+    outs = [np.zeros_like(x) for x in inds]
+    maps = [np.zeros(max(len(x), 1), dtype=np.uint8) for x in inds]
+    arr = lambda xs: (C.c_void_p * n)(*xs)
+    wcs = (C.c_uint32 * n)(*[g[0] for g in grids])
+    hcs = (C.c_uint32 * n)(*[g[1] for g in grids])
+    _check(lib().h266_sao_chroma_merge_batch(ctx._h, n, arr([C.addressof(c) for c in sc]),
+                                             arr([C.addressof(c) for c in pc]), arr([x.ctypes.data for x in inds]),
+                                             wcs, hcs, bit_depth, ctb_log2, arr([x.ctypes.data for x in outs]),
+                                             arr([x.ctypes.data for x in maps])))
+    return [(o, m[: len(x)]) for o, m, x in zip(outs, maps, inds)]

@@ -209,3 +209,43 @@ def test_gpu_sao_merge_16bit_large_differences():
         got, gm = native.sao_chroma_merge(ctx, src, rec, indep, 4, 3, bit_depth=16, ctb_log2=6)
     assert np.array_equal(gm, wm)
     assert got.tobytes() == want.tobytes()
+
+
+def merge_pair(seed, w, h, bd, log2):
+    """A reconstruction and an original differing by seeded noise, as in cases()."""
+    rec, _ = W.make_workload(seed, w, h, bd, log2)
+    rng = np.random.Generator(np.random.PCG64(seed + 1))
+    src = rec.copy()
+    for name in ("luma", "cb", "cr"):
+        p = getattr(rec, name)
+        noise = rng.integers(-9, 10, size=p.shape) + (rng.random(p.shape) < 0.1) * 5
+        setattr(src, name, np.clip(p.astype(np.int64) + noise, 0, (1 << bd) - 1).astype(np.uint16))
+    return src, rec
+
+
+@pytest.mark.gpu
+def test_gpu_sao_merge_batch_matches_oracle():
+    """The batched merge (one launch per anti-diagonal over all pictures) on
+    pictures of different sizes and CTB grids (10-bit, CTB 64): each picture's
+    records and map equal to the oracle's."""
+    import torch
+    from oxideav_h266_b200 import native
+    bd, log2 = 10, 6
+    pairs = [merge_pair(8400 + i, w, h, bd, log2) for i, (w, h) in
+             enumerate([(640, 360), (202, 138), (1920, 1080), (64, 64), (832, 480)])]
+    ctb = 1 << log2
+    wants, indeps, grids = [], [], []
+    for src, rec in pairs:
+        ind = decide(src, rec, log2, bd)
+        wants.append(merge(src, rec, ind, log2, bd))
+        indeps.append(ind)
+        grids.append((-(-rec.width // ctb), -(-rec.height // ctb)))
+    with native.Context(0) as ctx:
+        srcs = [native.DevicePicture.from_host(s_) for s_, _ in pairs]
+        recs = [native.DevicePicture.from_host(r_) for _, r_ in pairs]
+        torch.cuda.synchronize()
+        for _ in range(2):  # twice: the work area is reused
+            got = native.sao_chroma_merge_batch(ctx, srcs, recs, indeps, grids, bit_depth=bd, ctb_log2=log2)
+            for i, ((gm, gmap), (wm, wmap)) in enumerate(zip(got, wants)):
+                assert np.array_equal(gmap, wmap), i
+                assert gm.tobytes() == wm.tobytes(), i
