@@ -44,10 +44,14 @@ import time
 ROOT = pathlib.Path(__file__).resolve().parent
 WIDTH, HEIGHT, BITDEPTH = 1920, 1080, 10
 METRIC = "filter-chain Mpx/s 1080p/2160p 10-bit bit-exact"
-# DRAM bytes (read + write) per luma pixel of the batched SAO/ALF launch, from one
-# ncu capture of that launch over 16 pictures of this workload (100 803 840 +
-# 63 711 232 B); the bench line scales it to its own batch and labels it so.
-SAO_ALF_TRAFFIC_PER_PX = (100803840 + 63711232) / (16 * 1920 * 1080)
+# From one ncu capture of the batched SAO/ALF launch (k_sao_alf_tiles_batch
+# <64, 64, 1, 1>) over 4 pictures of this workload: DRAM bytes read + written
+# (25 689 344 + 761 088 B; ncu flushes the caches before the launch, and the
+# output planes retire from L2 after it) and thread instructions per luma pixel
+# (thread_inst_executed); the bench line scales them to its own batch
+# and labels them so.
+SAO_ALF_TRAFFIC_PER_PX = (25689344 + 761088) / (4 * 1920 * 1080)
+SAO_ALF_THREAD_INST_PER_PX = 333.2  # 2 763 519 786 thread instructions / 4 pictures
 
 
 def _import_pkg():
@@ -171,6 +175,24 @@ def replica_value(px_per_step: float, steps: int, ms_local: float, dist=None, de
         world = dist.get_world_size()
     ms = float(t.item())
     return world * px_per_step * steps / (ms / 1e3) / 1e6, ms
+
+
+def issue_roofline(launch_s: float, px: int, clocks: dict, device: int) -> dict:
+    """The SAO/ALF launch against the integer issue rate, the bound of this
+    integer stencil: thread instructions per pixel (ncu) x pixels per launch /
+    the launch's CUDA-event time, against SMs x 4 schedulers x 32 lanes x the SM
+    clock sampled during the timed region."""
+    import torch
+
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+    peak = sms * 4 * 32 * mhz * 1e6
+    achieved = SAO_ALF_THREAD_INST_PER_PX * px / launch_s
+    return {"bound": "integer issue", "achieved_tinst_per_s": round(achieved / 1e12, 2),
+            "peak_tinst_per_s": round(peak / 1e12, 2), "unit": "T thread-instructions/s",
+            "frac": round(achieved / peak, 4), "thread_inst_per_px": SAO_ALF_THREAD_INST_PER_PX,
+            "source": "thread instructions per pixel from one ncu capture of this launch; time from CUDA events "
+                      "in this run; peak from the SM count and the sampled SM clock"}
 
 
 def replica_parity(rec: dict, dist=None, device=None) -> dict:
@@ -845,13 +867,14 @@ def run_ours(args, rank, world, local_rank):
     achieved = alg_bytes / per_launch_s / 1e9
     total_ms = sum(v[0] for v in prof.values())
     roofline = {
-        "kernel": "k_sao_alf_packed (SAO + ALF classification + 7x7/5x5 + CC-ALF tile pass)",
+        "kernel": "k_sao_alf_tiles_batch (SAO + ALF classification + 7x7/5x5 + CC-ALF tile pass, TMA-staged windows)",
         "bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
         "frac": round(achieved / peaks["hbm_gbs"], 4), "peak_source": peak_kind,
         "traffic": (round(SAO_ALF_TRAFFIC_PER_PX * WIDTH * HEIGHT * args.batch) if SAO_ALF_TRAFFIC_PER_PX else None),
-        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 16-picture launch, scaled to "
+        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 4-picture launch, scaled to "
                           "this launch's pictures",
         "algorithmic_bytes_per_launch": alg_bytes, "launch_us": round(per_launch_s * 1e6, 2),
+        "issue": issue_roofline(per_launch_s, WIDTH * HEIGHT * args.batch, clocks, local_rank),
         "pictures_per_launch": args.batch,
         "share_of_device_time": {k: round(v[0] / total_ms, 3) for k, v in prof.items() if total_ms > 0},
     }
