@@ -681,6 +681,7 @@ struct DbSide {
   // side information built on the device: the walk's inputs (pointers are
   // rebased onto the uploaded blob when the chain runs)
   bool device_walk = false, dw_sep = false, dw_mv = false, dw_mv_cu = false;
+  bool dw_tiles = false;  // device walk without chained footprints, out of place: the grid-mode tile kernel
   DeviceWalkIn dw{};
 };
 
@@ -755,12 +756,14 @@ DeviceWalkIn device_walk_in(const uint8_t *base, const Staged &st, const DbSide 
 
 int run_deblock(h266_ctx *ctx, cudaStream_t stream, const uint8_t *base, const Staged &st, const DbSide &db,
                 const DPlane src[3], const DPlane dst[3], const uint16_t *lut, int bd, uint8_t *walk = nullptr) {
-  if (db.device_walk) {  // side information built on the device, then the tile kernel on its grids
+  if (db.device_walk) {  // side information built on the device, then the tile or strip kernels on its grids
     if (!walk) return set_error(H266_ERR_INVALID_ARGUMENT, "device-built side information without walk scratch");
     Prof pf(ctx, stream, H266_PROF_DEBLOCK);
     DeviceWalkOut out;
     H266_TRY(launch_device_walk(stream, device_walk_in(base, st, db), walk, out, &ctx->launches));
-    return launch_deblock_tiles_grid(stream, src, dst, lut, bd, out, &ctx->launches);
+    const bool apart = src[0].s != dst[0].s && src[1].s != dst[1].s && src[2].s != dst[2].s;
+    if (db.dw_tiles && apart) return launch_deblock_tiles_grid(stream, src, dst, lut, bd, out, &ctx->launches);
+    return launch_deblock_strips_grid(stream, src, dst, lut, bd, out, &ctx->launches);
   }
   const StripSide v{reinterpret_cast<const EdgeSeg *>(base + st.seg[0]),
                     reinterpret_cast<const uint32_t *>(base + st.comp[0]),
@@ -892,10 +895,11 @@ static const h266::Tuning &batch_tuning(const h266_ctx *ctx, uint32_t n, const h
 
 namespace {
 
-// `allow_device`: a picture eligible for the device-built side information
-// (device_walk_eligible, and SAO or ALF on, so that deblocking runs out of
-// place) skips the host walk; its CU lists, motion grid and gate lists are
-// staged instead.
+// `allow_device`: a picture whose side information the device can build
+// (device_walk_mode non-zero) skips the host walk; its CU lists, motion grid
+// and gate lists are staged instead.  Pictures without chained footprints
+// and with SAO or ALF on (deblocking out of place) deblock with the grid-mode
+// tile kernel, the others with the grid-mode strip kernels.
 int prepare_chain(Prep &pr, const h266_picture &pic, const h266_in_loop_filter_args &a, TaskPool *pool,
                   bool allow_device = false) {
   pr.st = Staged{};
@@ -917,13 +921,14 @@ int prepare_chain(Prep &pr, const h266_picture &pic, const h266_in_loop_filter_a
   in.n_rows = a.n_clip_rows;
   H266_TRY(build_pass2(pic, in, pr.h));
   pr.blob.clear();
-  const bool dev = allow_device && (pr.h.do_sao || pr.h.do_alf) &&
-                   device_walk_eligible(pic, a.cus, a.n_cus, a.chroma_cus, a.n_chroma_cus, a.deblock,
-                                        a.chroma_format_idc);
-  if (dev) {
+  const int mode = allow_device ? device_walk_mode(pic, a.cus, a.n_cus, a.chroma_cus, a.n_chroma_cus, a.deblock,
+                                                   a.chroma_format_idc)
+                                : 0;
+  if (mode) {
     Blob blob{pr.blob};
     DbSide &db = pr.db;
     db.device_walk = true;
+    db.dw_tiles = mode == 1 && (pr.h.do_sao || pr.h.do_alf);
     db.dw_sep = a.chroma_cus != nullptr;
     db.dw_mv = a.mv_grid && a.mv_grid->cells && a.mv_grid->cells_w * a.mv_grid->cells_h;
     DeviceWalkIn &w = db.dw;
@@ -999,7 +1004,7 @@ DeviceWalkIn device_walk_in(const uint8_t *base, const Staged &st, const DbSide 
 int exec_chain(h266_ctx *ctx, cudaStream_t stream, const uint8_t *base, const Staged &st, const DbSide &db,
                const Pass2Host &h, const uint16_t *lut, int dbd, const DPlane P[3], const DPlane S[3],
                uint8_t *walk = nullptr) {
-  if (!h.do_sao && !h.do_alf) return run_deblock(ctx, stream, base, st, db, P, P, lut, dbd);
+  if (!h.do_sao && !h.do_alf) return run_deblock(ctx, stream, base, st, db, P, P, lut, dbd, walk);
   H266_TRY(run_deblock(ctx, stream, base, st, db, P, S, lut, dbd, walk));
   return run_pass2(ctx, stream, h.args, h.do_sao, h.do_alf, h.packed, base, st, S, P);
 }
@@ -2456,7 +2461,7 @@ int exec_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, std::vector<Ba
     BatchItem &it = items[i];
     Run &r = runs[i];
     const uint8_t *base = it.st.base;
-    r.tile = it.pass2 && (it.db.tiles_ok || it.db.device_walk) && !ctx->force_global_deblock &&
+    r.tile = it.pass2 && (it.db.device_walk ? it.db.dw_tiles : it.db.tiles_ok) && !ctx->force_global_deblock &&
              !ctx->force_strip_deblock;
     if (r.tile && it.db.device_walk) {  // the side information is derived on the device first, batched
       DeviceWalkOut g;

@@ -1282,6 +1282,12 @@ struct StripParams {
   uint32_t ctas[3];  // CTAs per plane
   const uint16_t *lut;
   int maxv;
+  // Grid mode (side information built on the device): the pass's segments in
+  // per-band cell grids, grid[p][band * grid_slots[p] + pos / unit] (bs 0:
+  // none), unit 4 luma / 8 chroma samples along the edge normal.
+  int grid_mode;
+  const EdgeSeg *grid[3];
+  uint32_t grid_slots[3], grid_bands[3];
 };
 
 // Shared-memory row pitch of the rows kernel: whole 16-byte vectors plus one
@@ -1363,6 +1369,65 @@ __device__ __forceinline__ void run_components(const StripParams &a, const Share
   }
 }
 
+// Grid mode: does the cell at slot s, whose footprint starts at `start`,
+// continue a run -- does an earlier footprint of the band end past `start`?
+// Footprints [pos - R(mflP), pos + R(mflQ)) reach at most 8 samples and
+// cells are 4 (luma) or 8 (chroma) samples apart, so only the 3 cells before
+// s can reach it.
+__device__ __forceinline__ bool continues_run(const EdgeSeg *cells, uint32_t s, int start) {
+  for (uint32_t t = s > 3 ? s - 3 : 0; t < s; ++t) {
+    const EdgeSeg f = cells[t];
+    if (f.bs && ((f.flags & 1) ? f.x : f.y) + reach_d(f.mfl & 15) > start) return true;
+  }
+  return false;
+}
+
+// Grid mode: the runs of bands [0, nb) of cell grid g (ns cells per band), one
+// lane group per run.  A run is a maximal sequence of occupied cells, in
+// position order, each starting before the furthest footprint end of the
+// cells before it: the host grouping's components, whose members come in
+// position order when every row and column of the CU map is in decode order
+// (checked on the host before the walk runs on the device).  Footprint starts
+// never decrease along a band (spacing 4, reach 4..8), so a run ends at the
+// first occupied cell that does not start inside it, and that cell lies
+// within 3 cells of the run's last member or not at all.
+template <int G, int PITCH>
+__device__ __forceinline__ void run_cell_runs(const StripParams &a, const SharedView &v, const EdgeSeg *g, uint32_t ns,
+                                              uint32_t nb) {
+  const int lane = threadIdx.x & 31, k = lane % G, base = lane - k;
+  const unsigned mask = ((1u << G) - 1) << base;
+  const uint32_t groups = blockDim.x / G, total = ns * nb;
+  for (uint32_t i = threadIdx.x / G; i < total; i += groups) {
+    const uint32_t b = i / ns, s = i - b * ns;
+    const EdgeSeg *cells = g + (size_t)b * ns;
+    EdgeSeg e = cells[s];
+    if (!e.bs) continue;
+    const bool vert = e.flags & 1;
+    int pos = vert ? e.x : e.y;
+    if (continues_run(cells, s, pos - reach_d(e.mfl >> 4))) continue;  // not the first of its run
+    int end = pos + reach_d(e.mfl & 15);
+    uint32_t cur = s;
+    for (;;) {
+      segment_group<G, PITCH>(v, e, a.maxv, k, base, mask);
+      __syncwarp(mask);
+      uint32_t nx = cur + 1;
+      bool found = false;
+      for (; nx < ns && nx <= cur + 3; ++nx) {
+        e = cells[nx];
+        if (e.bs) {
+          found = true;
+          break;
+        }
+      }
+      if (!found) break;
+      pos = vert ? e.x : e.y;
+      if (pos - reach_d(e.mfl >> 4) >= end) break;
+      end = max(end, pos + reach_d(e.mfl & 15));
+      cur = nx;
+    }
+  }
+}
+
 // Vertical pass: one CTA per band of rows, all planes in one grid.  Loads the
 // rows from src (luma through the LMCS LUT), filters, stores them to dst.
 __global__ void __launch_bounds__(128) k_deblock_rows(StripParams a) {
@@ -1392,10 +1457,18 @@ __global__ void __launch_bounds__(128) k_deblock_rows(StripParams a) {
     sm[r * ld + c] = lut ? lut[x] : x;
   }
   __syncthreads();
-  const uint32_t *bf = a.band_first + a.band_off[plane];
   const SharedView view{sm, ld, 0, y0, w, rows, w, src.h};
-  if (plane == 0) run_components<4, 0>(a, view, bf[band], bf[band + 1]);
-  else run_components<2, 0>(a, view, bf[band], bf[band + 1]);
+  if (a.grid_mode) {
+    if ((uint32_t)band < a.grid_bands[plane]) {
+      const EdgeSeg *g = a.grid[plane] + (size_t)band * a.grid_slots[plane];
+      if (plane == 0) run_cell_runs<4, 0>(a, view, g, a.grid_slots[plane], 1);
+      else run_cell_runs<2, 0>(a, view, g, a.grid_slots[plane], 1);
+    }
+  } else {
+    const uint32_t *bf = a.band_first + a.band_off[plane];
+    if (plane == 0) run_components<4, 0>(a, view, bf[band], bf[band + 1]);
+    else run_components<2, 0>(a, view, bf[band], bf[band + 1]);
+  }
   __syncthreads();
   const int nvo = vec_ok(dst) ? w / 8 : 0;
   for (int i = threadIdx.x; i < rows * nvo; i += blockDim.x) {
@@ -1432,12 +1505,22 @@ __global__ void __launch_bounds__(128, 8) k_deblock_cols(StripParams a) {
     }
   }
   __syncthreads();
-  const uint32_t *bf = a.band_first + a.band_off[plane];
-  const uint32_t nb = a.n_bands[plane];
-  const uint32_t b0 = min((uint32_t)(x0 / unit), nb), b1 = min((uint32_t)((x0 + kStripCols) / unit), nb);
   const SharedView view{sm, kStripCols, x0, 0, cols, h, p.w, h};
-  if (plane == 0) run_components<4, kStripCols>(a, view, bf[b0], bf[b1]);
-  else run_components<2, kStripCols>(a, view, bf[b0], bf[b1]);
+  if (a.grid_mode) {
+    const uint32_t nb = a.grid_bands[plane];
+    const uint32_t b0 = min((uint32_t)(x0 / unit), nb), b1 = min((uint32_t)((x0 + kStripCols) / unit), nb);
+    if (b1 > b0) {
+      const EdgeSeg *g = a.grid[plane] + (size_t)b0 * a.grid_slots[plane];
+      if (plane == 0) run_cell_runs<4, kStripCols>(a, view, g, a.grid_slots[plane], b1 - b0);
+      else run_cell_runs<2, kStripCols>(a, view, g, a.grid_slots[plane], b1 - b0);
+    }
+  } else {
+    const uint32_t *bf = a.band_first + a.band_off[plane];
+    const uint32_t nb = a.n_bands[plane];
+    const uint32_t b0 = min((uint32_t)(x0 / unit), nb), b1 = min((uint32_t)((x0 + kStripCols) / unit), nb);
+    if (plane == 0) run_components<4, kStripCols>(a, view, bf[b0], bf[b1]);
+    else run_components<2, kStripCols>(a, view, bf[b0], bf[b1]);
+  }
   __syncthreads();
   if (vec) {
     for (int i = threadIdx.x; i < h * kStripVec; i += blockDim.x) {
@@ -1824,6 +1907,65 @@ int launch_deblock_strips(cudaStream_t st, const DPlane src[3], const DPlane dst
   return H266_OK;
 }
 
+// Strip kernels on the device walk's cell grids: a CTA per row band of each
+// plane (vertical pass, src -> dst), then per 8-column strip (horizontal pass,
+// in place on dst).  Row bands follow the plane sizes, so planes without
+// segments (chroma of a 4:0:0 walk) are still copied.
+int launch_deblock_strips_grid(cudaStream_t st, const DPlane src[3], const DPlane dst[3], const uint16_t *lut,
+                               int bit_depth, const DeviceWalkOut &g, uint64_t *launches) {
+  StripParams a;
+  std::memset(&a, 0, sizeof a);
+  a.grid_mode = 1;
+  size_t smem_rows = 0, smem_cols = 0;
+  uint32_t ctas_rows = 0, ctas_cols = 0, rows[3], strips[3];
+  for (int i = 0; i < 3; ++i) {
+    a.src[i] = src[i];
+    a.dst[i] = dst[i];
+    const bool empty = (int64_t)src[i].w * src[i].h == 0;
+    const int unit = i ? 2 : 4;
+    rows[i] = empty ? 0 : (uint32_t)((src[i].h + unit - 1) / unit);
+    strips[i] = empty ? 0 : (uint32_t)((src[i].w + kStripCols - 1) / kStripCols);
+    if (!empty) {
+      smem_rows = std::max(smem_rows, rows_smem(src[i]));
+      smem_cols = std::max(smem_cols, cols_smem(src[i]));
+    }
+    ctas_rows += rows[i];
+    ctas_cols += strips[i];
+  }
+  if (smem_rows > (size_t)kMaxStripSmem || smem_cols > (size_t)kMaxStripSmem)
+    return set_error(H266_ERR_UNSUPPORTED, "deblock: planes too large for the strip kernels");
+  a.lut = lut;
+  a.maxv = (1 << bit_depth) - 1;
+  for (int i = 0; i < 3; ++i) {
+    a.grid[i] = g.grid[0][i];
+    a.grid_slots[i] = g.slots[0][i];
+    a.grid_bands[i] = g.bands[0][i];
+    a.ctas[i] = rows[i];
+  }
+  if (ctas_rows) {
+    if (smem_rows > 48 * 1024)
+      H266_CUDA(cudaFuncSetAttribute(k_deblock_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_rows));
+    k_deblock_rows<<<ctas_rows, 128, smem_rows, st>>>(a);
+    H266_CUDA(cudaGetLastError());
+    ++*launches;
+  }
+  a.lut = nullptr;
+  for (int i = 0; i < 3; ++i) {
+    a.grid[i] = g.grid[1][i];
+    a.grid_slots[i] = g.slots[1][i];
+    a.grid_bands[i] = g.bands[1][i];
+    a.ctas[i] = strips[i];
+  }
+  if (ctas_cols) {
+    if (smem_cols > 48 * 1024)
+      H266_CUDA(cudaFuncSetAttribute(k_deblock_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cols));
+    k_deblock_cols<<<ctas_cols, 128, smem_cols, st>>>(a);
+    H266_CUDA(cudaGetLastError());
+    ++*launches;
+  }
+  return H266_OK;
+}
+
 size_t deblock_tile_params_size() { return sizeof(TileParams); }
 
 uint32_t fill_deblock_tile_params(void *out, const DPlane src[3], const DPlane dst[3], const uint16_t *lut,
@@ -1895,50 +2037,84 @@ int launch_deblock(cudaStream_t st, const DPlane planes[3], int bit_depth, const
 }
 
 // ===================================================================== device-built side information
-bool device_walk_eligible(const h266_picture &pic, const h266_deblock_cu *cus, uint64_t n_cus,
-                          const h266_deblock_cu *chroma_cus, uint64_t n_chroma, const h266_deblock_params &params,
-                          uint32_t cfi) {
-  if (params.disabled || params.bit_depth < 8 || params.bit_depth > 16 || params.ctb_log2_size_y > 16) return false;
+int device_walk_mode(const h266_picture &pic, const h266_deblock_cu *cus, uint64_t n_cus,
+                     const h266_deblock_cu *chroma_cus, uint64_t n_chroma, const h266_deblock_params &params,
+                     uint32_t cfi) {
+  if (params.disabled || params.bit_depth < 8 || params.bit_depth > 16 || params.ctb_log2_size_y > 16) return 0;
+  if (cfi > 3) return 0;
   const int w = (int)pic.luma.width, h = (int)pic.luma.height;
+  if (w <= 0 || h <= 0) return 0;
   const bool chroma = (uint64_t)pic.cb.width * pic.cb.height != 0 || (uint64_t)pic.cr.width * pic.cr.height != 0;
-  if (cfi > 1 || (cfi == 0 && chroma)) return false;
+  if (n_cus > (uint64_t)INT32_MAX || n_chroma > (uint64_t)INT32_MAX) return 0;
+  // The tile kernel's condition: no two segments' footprints overlap, every
+  // one inside a cell of the tile halo -- luma CUs and transform blocks at
+  // least 8 samples, no sub-block edges, 4:2:0 or 4:0:0.
+  bool no_chains = cfi <= 1 && !(cfi == 0 && chroma);
   if (chroma && (pic.cb.width != (pic.luma.width + 1) / 2 || pic.cb.height != (pic.luma.height + 1) / 2 ||
                  pic.cr.width != pic.cb.width || pic.cr.height != pic.cb.height))
-    return false;
-  if (n_cus > (uint64_t)INT32_MAX || n_chroma > (uint64_t)INT32_MAX) return false;
-  // no CU overlaps another (the walk's emissions then never collide)
+    no_chains = false;
+  // The strip kernels' condition: a plane's row band and full-height strip fit
+  // their shared memory.
+  const h266_plane *pl[3] = {&pic.luma, &pic.cb, &pic.cr};
+  for (int i = 0; i < 3; ++i) {
+    const DPlane d{nullptr, 0, (int)pl[i]->width, (int)pl[i]->height};
+    if ((int64_t)d.w * d.h && (rows_smem(d) > (size_t)kMaxStripSmem || cols_smem(d) > (size_t)kMaxStripSmem))
+      return 0;
+  }
+  // CUs on the 4x4 grid, inside the picture, not overlapping (the walk's
+  // emissions then never share a grid cell), and in decode order along every
+  // row and column of the CU map: then a band's segments come out of the
+  // reference's walk in position order, the order the strip kernels run a
+  // chain of overlapping footprints in.
   const int cw4 = (w + 3) / 4, ch4 = (h + 3) / 4;
-  thread_local std::vector<uint8_t> seen;
+  thread_local std::vector<int32_t> map, last_col;
   const h266_deblock_cu *lists[2] = {cus, chroma_cus};
   const uint64_t counts[2] = {n_cus, chroma_cus ? n_chroma : 0};
   for (int l = 0; l < 2; ++l) {
     if (!lists[l]) continue;
-    seen.assign((size_t)cw4 * ch4, 0);
+    map.assign((size_t)cw4 * ch4, -1);
+    bool chains = false;  // 4-sample edges, sub-block edges or narrow transform blocks in this list
     for (uint64_t i = 0; i < counts[l]; ++i) {
       const h266_deblock_cu &c = lists[l][i];
-      if ((c.x | c.y | c.w | c.h) & 3 || c.w < 8 || c.h < 8) return false;  // 4-sample edges chain
-      if ((uint64_t)c.x + c.w > (uint64_t)w || (uint64_t)c.y + c.h > (uint64_t)h) return false;
-      if (c.has_num_sb) return false;  // sub-block edges (maxFilterLength 5 next to 8-spaced edges)
+      if ((c.x | c.y | c.w | c.h) & 3 || c.w == 0 || c.h == 0) return 0;
+      if ((uint64_t)c.x + c.w > (uint64_t)w || (uint64_t)c.y + c.h > (uint64_t)h) return 0;
+      if (c.has_tb_split && (c.tb_split.n_bounds < 1 || c.tb_split.n_bounds > 3)) return 0;
+      if (c.w < 8 || c.h < 8 || c.has_num_sb) chains = true;
       if (c.has_tb_split) {
         const uint32_t dim = c.tb_split.vertical ? c.w : c.h;
-        if (c.tb_split.n_bounds < 1 || c.tb_split.n_bounds > 3) return false;
         uint32_t prev = 0;
         for (int k = 0; k < c.tb_split.n_bounds; ++k) {
           const uint32_t b = c.tb_split.bounds[k];
-          if (b < prev + 8) return false;  // transform blocks narrower than 8
+          if (b < prev + 8) chains = true;
           prev = b;
         }
-        if (dim < prev + 8) return false;
+        if (dim < prev + 8) chains = true;
       }
       for (uint32_t y = c.y / 4; y < (c.y + c.h) / 4; ++y)
         for (uint32_t x = c.x / 4; x < (c.x + c.w) / 4; ++x) {
-          uint8_t &o = seen[(size_t)y * cw4 + x];
-          if (o) return false;
-          o = 1;
+          int32_t &o = map[(size_t)y * cw4 + x];
+          if (o >= 0) return 0;
+          o = (int32_t)i;
         }
     }
+    if (chains) no_chains = false;
+    // Only luma footprints chain (chroma edges are 8 chroma samples apart and
+    // reach 4), so only the luma list's order matters.
+    if (l != 0 || !chains) continue;
+    last_col.assign((size_t)cw4, -1);
+    for (int y = 0; y < ch4; ++y) {
+      int32_t last_row = -1;
+      const int32_t *row = map.data() + (size_t)y * cw4;
+      for (int x = 0; x < cw4; ++x) {
+        const int32_t v = row[x];
+        if (v < 0) continue;
+        if (v < last_row || v < last_col[x]) return 0;
+        last_row = v;
+        last_col[x] = v;
+      }
+    }
   }
-  return true;
+  return no_chains ? 1 : 2;
 }
 
 namespace {

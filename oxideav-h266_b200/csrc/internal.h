@@ -180,14 +180,19 @@ uint32_t fill_deblock_tile_params(void *out, const DPlane src[3], const DPlane d
 int launch_deblock_tiles_batch(cudaStream_t st, const void *d_params, const uint32_t *d_first, int n, uint32_t ctas,
                                uint64_t *launches);
 // ---------------------------------------------------------------- device-built side information
-// For pictures whose deblocking has no chained edges (every component one
-// segment: luma CUs and transform blocks at least 8x8, no sub-block edges,
-// no overlapping CUs, CUs inside the picture, 4:2:0 or 4:0:0), the edge walk
-// runs on the device from the CU list and the motion grid and writes each
-// segment to a dense per-band grid that the tile kernel scans.
-bool device_walk_eligible(const h266_picture &pic, const h266_deblock_cu *cus, uint64_t n_cus,
-                          const h266_deblock_cu *chroma_cus, uint64_t n_chroma, const h266_deblock_params &params,
-                          uint32_t cfi);
+// Device-built side information: the edge walk runs on the device from the
+// CU lists and the motion grid and writes each segment to a dense per-band
+// cell grid.  device_walk_mode returns 1 when no two segments' footprints can
+// overlap (luma CUs and transform blocks at least 8 samples, no sub-block
+// edges, 4:2:0 or 4:0:0): every cell is a component and the tile kernel scans
+// the grids; 2 when footprints may chain (the strip kernels run each band's
+// runs of cells in position order, which needs the luma CU list in decode
+// order along every row and column of its CU map); 0 when the host must build
+// the plan (CUs off the 4x4 grid, outside the picture or overlapping, CU lists
+// out of order, planes too large for the strip kernels, invalid input).
+int device_walk_mode(const h266_picture &pic, const h266_deblock_cu *cus, uint64_t n_cus,
+                     const h266_deblock_cu *chroma_cus, uint64_t n_chroma, const h266_deblock_params &params,
+                     uint32_t cfi);
 struct DeviceWalkIn {  // device pointers
   const h266_deblock_cu *cus, *chroma_cus;  // chroma_cus == cus for a single tree
   uint64_t n_cus, n_chroma;
@@ -211,6 +216,8 @@ int launch_device_walk(cudaStream_t st, const DeviceWalkIn &in, uint8_t *scratch
                        uint64_t *launches);
 int launch_deblock_tiles_grid(cudaStream_t st, const DPlane src[3], const DPlane dst[3], const uint16_t *lut,
                               int bit_depth, const DeviceWalkOut &g, uint64_t *launches);
+int launch_deblock_strips_grid(cudaStream_t st, const DPlane src[3], const DPlane dst[3], const uint16_t *lut,
+                               int bit_depth, const DeviceWalkOut &g, uint64_t *launches);
 // Batched device walk: fill_walk_batch_item writes one picture's item
 // (walk_batch_item_size() bytes) and its CTA counts per launch; the prefix
 // sums of those counts over the batch's pictures (n + 1 entries each) select

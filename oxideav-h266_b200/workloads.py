@@ -452,6 +452,31 @@ def make_workload(
     return pic, fa
 
 
+def with_chroma_format(pic: PictureData, fa: FilterArgsData, cfi: int, seed: int = 0):
+    """The picture and arguments re-cast to chroma format `cfi` (2: 4:2:2, 3:
+    4:4:4): chroma planes resampled to the format's size (nearest sample,
+    plus seeded noise so edges still filter) and every configuration's
+    chroma_format_idc set.  The crate's deblocking walk keeps its 4:2:0 chroma
+    grid for every format (src/deblock.rs), SAO and ALF subsample by the
+    format (src/sao.rs:344-351, src/alf.rs:161-168)."""
+    assert cfi in (2, 3)
+    rng = np.random.Generator(np.random.PCG64(seed + 991))
+    h, w = pic.luma.shape
+    ch, cw = (h, w) if cfi == 3 else (h, (w + 1) // 2)
+    mx = (1 << pic.bit_depth) - 1
+    planes = []
+    for c in (pic.cb, pic.cr):
+        ys = np.minimum(np.arange(ch) * c.shape[0] // ch, c.shape[0] - 1)
+        xs = np.minimum(np.arange(cw) * c.shape[1] // cw, c.shape[1] - 1)
+        up = c[ys][:, xs].astype(np.int64) + rng.integers(-2, 3, size=(ch, cw))
+        planes.append(np.ascontiguousarray(np.clip(up, 0, mx).astype(np.uint16)))
+    out = PictureData(pic.luma.copy(), planes[0], planes[1], pic.bit_depth)
+    fa.chroma_format_idc = cfi
+    fa.sao_cfg.chroma_format_idc = cfi
+    fa.alf_cfg.chroma_format_idc = cfi
+    return out, fa
+
+
 def config1(seed: int = 1000):
     """416x240 4:2:0 8-bit, CTU 128, all intra, SAO + one ALF APS, LMCS/CC-ALF off."""
     return make_workload(seed, 416, 240, 8, 7)

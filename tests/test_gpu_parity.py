@@ -65,6 +65,10 @@ WORKLOADS = {
     # CTB 32 with a last chroma tile of 4 columns (one sample pair per row inside
     # the clip rectangle's interior) and aligned luma rows
     "ctb32_tail4": lambda s: W.make_workload(7700 + s, 200, 136, 10, 5, ccalf=True, lmcs=True),
+    "stress_422": lambda s: W.with_chroma_format(*W.stress_workload(8000 + s), 2, s),
+    "stress_444": lambda s: W.with_chroma_format(*W.stress_workload(8100 + s), 3, s),
+    "stress_dual_444": lambda s: W.with_chroma_format(*W.stress_workload(8200 + s, dual_tree=True, bit_depth=8), 3, s),
+    "c1_422": lambda s: W.with_chroma_format(*W.config1(8300 + s), 2, s),
 }
 
 
@@ -356,14 +360,26 @@ def test_plan_batch_device_sideinfo_1080p_x4(ctx):
                                 device_sideinfo=True, expect_device=[True] * 4)
 
 
+def _out_of_order(seed):
+    """A stress picture whose CU list is not in decode order (two CUs of the
+    first CTB swapped): the device walk does not take it."""
+    pic, fa = W.stress_workload(seed)
+    cus = fa.cus.copy()
+    cus[[0, 1]] = cus[[1, 0]]
+    fa.cus = cus
+    return pic, fa
+
+
 def test_plan_batch_device_sideinfo_mixed_with_host_plans(ctx):
-    """One batch mixing device-walk plans (8-bit CTU 64, 10-bit 1080p-style,
-    416x240) with pictures the walk does not cover (4-sample CUs and sub-block
-    grids, deblocking only), which keep host-built segments."""
+    """One batch mixing device-walk plans on the grid-mode tile kernel (8-bit
+    CTU 64, 10-bit 1080p-style, 416x240), device-walk plans on the grid-mode
+    strip kernels (4-sample CUs and sub-block grids, deblocking only, 4:4:4)
+    and a picture the walk does not take (CU list out of decode order), which
+    keeps host-built segments."""
     items = [WORKLOADS["ctb64_8bit"](60), small_c2(61), WORKLOADS["c1"](62), WORKLOADS["stress"](63),
-             _deblock_only(64), small_c2(65)]
+             _deblock_only(64), small_c2(65), WORKLOADS["stress_444"](66), _out_of_order(67)]
     _batched_plans_match_oracle(ctx, items, "mixed device/host side info", device_sideinfo=True,
-                                expect_device=[None, True, None, False, False, True])
+                                expect_device=[True, True, True, True, True, True, True, False])
 
 
 def test_plan_batch_2160p_tiles_x16(ctx):
@@ -503,6 +519,81 @@ def test_device_built_side_information(ctx, kind):
     assert_same(got, want, f"device-built side information {kind}")
     lut = 1 if fa.lmcs is not None else 0
     assert launches == lut + 2 + 1 + 1  # LUT, CU map + walk, tiles, SAO/ALF
+
+
+CHAINED = ["stress", "stress_dual", "stress_tiles", "stress_422", "stress_444", "stress_dual_444", "c1_422"]
+
+
+@pytest.mark.parametrize("kind", CHAINED)
+@pytest.mark.parametrize("seed", [0, 1])
+def test_device_built_side_information_with_chained_edges(ctx, kind, seed):
+    """Pictures whose edge footprints chain (4-sample CUs, sub-block grids,
+    narrow transform blocks), dual trees, tile gates and 4:2:2 / 4:4:4 build
+    their side information on the device too: the walk into per-band grids,
+    then the strip kernels running each band's runs of cells in order.
+    Bit-exact against the oracle and against the host-built path."""
+    pic, fa = WORKLOADS[kind](20 + seed)
+    got, want = pic.copy(), pic.copy()
+    plan = ctx.plan(pic, fa, device_sideinfo=True)
+    try:
+        assert plan.device_sideinfo
+    finally:
+        plan.close()
+    l0 = ctx.kernel_launches
+    ctx.apply_in_loop_filters(got, fa)
+    launches = ctx.kernel_launches - l0
+    oracle.apply_in_loop_filters(want, fa)
+    assert_same(got, want, f"device-built side information, chained edges {kind}")
+    lut = 1 if fa.lmcs is not None else 0
+    trees = 2 if fa.chroma_cus is not None else 1
+    assert launches >= lut + trees + 1 + 2 + 1  # LUT, CU maps, walk, rows + columns, SAO/ALF
+
+
+@pytest.mark.parametrize("kind", ["stress_422", "stress_444", "stress_dual_444", "c1_422"])
+def test_host_built_side_information_chroma_formats(kind, monkeypatch):
+    """4:2:2 and 4:4:4 through the host-built plan (strip kernels on component
+    lists, scalar SAO/ALF) match the oracle, which walks chroma edges on the
+    crate's 4:2:0 grid for every format."""
+    monkeypatch.setenv("H266_FORCE_HOST_SIDEINFO", "1")
+    c = native.Context(0)
+    try:
+        pic, fa = WORKLOADS[kind](30)
+        got, want = pic.copy(), pic.copy()
+        c.apply_in_loop_filters(got, fa)
+        oracle.apply_in_loop_filters(want, fa)
+        assert_same(got, want, f"host-built side information {kind}")
+    finally:
+        c.close()
+
+
+def test_device_built_side_information_deblocking_only(ctx):
+    """Without SAO and ALF deblocking runs in place: device-built side
+    information with the strip kernels on the picture's own planes."""
+    pic, fa = _deblock_only(35)
+    got, want = pic.copy(), pic.copy()
+    ctx.apply_in_loop_filters(got, fa)
+    oracle.apply_in_loop_filters(want, fa)
+    assert_same(got, want, "device-built side information, in place")
+    plan = ctx.plan(pic, fa, device_sideinfo=True)
+    try:
+        assert plan.device_sideinfo
+    finally:
+        plan.close()
+
+
+def test_cu_list_out_of_decode_order_keeps_host_side_information(ctx):
+    """A CU list out of decode order along a row of the CU map (chained
+    footprints would then run in another order) is walked on the host."""
+    pic, fa = _out_of_order(36)
+    plan = ctx.plan(pic, fa, device_sideinfo=True)
+    try:
+        assert not plan.device_sideinfo
+    finally:
+        plan.close()
+    got, want = pic.copy(), pic.copy()
+    ctx.apply_in_loop_filters(got, fa)
+    oracle.apply_in_loop_filters(want, fa)
+    assert_same(got, want, "out-of-order CU list")
 
 
 def test_device_built_side_information_with_per_cell_motion(ctx):
