@@ -282,7 +282,8 @@ int h266_ctx_set_profiling(h266_ctx *ctx, int on);
  * depth and persists the winners in a JSON table, which the Python layer
  * loads into a context with h266_ctx_set_tuning_for.  Keys and ranges:
  *   "e2e_group"            pictures per group of h266_apply_in_loop_filters_batch (1..16, default 4)
- *   "e2e_lanes"            streams those groups rotate over (1..4, default 3)
+ *   "e2e_lanes"            slot sets (device buffers, a stream) those groups rotate over (1..16,
+ *                          default 4)
  *   "sao_alf_ctas_per_sm"  SAO / ALF tile launches: 0 = one CTA per tile (default); 1..4 = a
  *                          persistent launch of that many CTAs per SM draining a device queue of
  *                          (picture, tile) items
@@ -290,8 +291,9 @@ int h266_ctx_set_profiling(h266_ctx *ctx, int on);
  *                          (values in between: 64)
  *   "prep_threads"         host threads preparing pictures' side information (0 = half the host
  *                          threads less two, 2..16; 1..64); a context-wide value
- *   "e2e_copy_streams"     0: each group's copies on its own stream (default); 1: all uploads on
- *                          one stream and all downloads on another
+ *   "e2e_copy_streams"     1: every upload (planes, side information, batch tables) in issue order
+ *                          on one stream and every download on another (default); 0: each group's
+ *                          copies on its group's stream
  * h266_ctx_set_tuning sets the context's value; h266_ctx_set_tuning_for sets
  * it for batches whose largest picture has that luma size and bit depth, which
  * takes precedence.  Unknown keys or out-of-range values: H266_ERR_INVALID_ARGUMENT. */

@@ -174,9 +174,13 @@ struct GroupSlot {
 };
 // Launch-shape knobs (h266_ctx_set_tuning); -1 in an override: not set.
 struct Tuning {
-  int e2e_group = 4, e2e_lanes = 3, sao_alf_ctas_per_sm = 0, sao_alf_tile_h = 64;
-  int prep_threads = 0;      // 0: the default count
-  int e2e_copy_streams = 0;  // 1: uploads and downloads on two streams of their own
+  int e2e_group = 4, e2e_lanes = 4, sao_alf_ctas_per_sm = 0, sao_alf_tile_h = 64;
+  int prep_threads = 0;  // 0: the default count
+  // 1: every upload of the end-to-end batch (planes, side information, batch
+  // tables) in issue order on one stream and every download on another, so
+  // small latency-critical copies do not wait behind other lanes' planes in
+  // the copy engine (measured 9.0 against 10.3 ms per 32 x 1080p)
+  int e2e_copy_streams = 1;
 };
 struct TuningKey {
   const char *name;
@@ -184,7 +188,7 @@ struct TuningKey {
   int lo, hi;
 };
 constexpr TuningKey kTuningKeys[] = {{"e2e_group", &Tuning::e2e_group, 1, 16},
-                                     {"e2e_lanes", &Tuning::e2e_lanes, 1, 4},
+                                     {"e2e_lanes", &Tuning::e2e_lanes, 1, 16},
                                      {"sao_alf_ctas_per_sm", &Tuning::sao_alf_ctas_per_sm, 0, 4},
                                      {"sao_alf_tile_h", &Tuning::sao_alf_tile_h, 32, 64},
                                      {"prep_threads", &Tuning::prep_threads, 0, 64},
@@ -371,6 +375,12 @@ struct Blob {
     b.resize(off + n);
     if (n) std::memcpy(b.data() + off, p, n);
     return off;
+  }
+  // A section of n bytes for the caller to fill (before the next put / alloc).
+  uint8_t *alloc(size_t n, size_t &off) {
+    off = (b.size() + 255) & ~(size_t)255;
+    b.resize(off + n);
+    return b.data() + off;
   }
 };
 
@@ -667,6 +677,7 @@ struct Staged {
   size_t ctb = 0, tab = 0, pack = 0, seg[2] = {0, 0}, comp[2] = {0, 0}, band[2] = {0, 0};
   size_t tile_bounds = 0;
   size_t dw_cus = 0, dw_ccus = 0, dw_mv = 0, dw_cols = 0, dw_rows = 0;  // device-walk inputs
+  size_t dw_tails[2] = {0, 0};
   uint8_t *base = nullptr;
 };
 
@@ -873,7 +884,7 @@ struct BatchItem {
   uint8_t *walk = nullptr;
 };
 int exec_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, std::vector<BatchItem> &items,
-               const Tuning &tn);
+               const Tuning &tn, cudaStream_t upload = nullptr);
 }  // namespace h266
 
 // The tuning of a batch: the override for its largest picture's geometry, else the context's.
@@ -942,37 +953,60 @@ int prepare_chain(Prep &pr, const h266_picture &pic, const h266_in_loop_filter_a
     w.cfi = a.chroma_format_idc;
     w.w = (int)pic.luma.width;
     w.h = (int)pic.luma.height;
-    w.max_cu_dim = 4;
-    for (uint64_t i = 0; i < a.n_cus; ++i) w.max_cu_dim = std::max(w.max_cu_dim, std::max(a.cus[i].w, a.cus[i].h));
-    for (uint64_t i = 0; db.dw_sep && i < a.n_chroma_cus; ++i)
-      w.max_cu_dim = std::max(w.max_cu_dim, std::max(a.chroma_cus[i].w, a.chroma_cus[i].h));
+    w.sep = db.dw_sep;
     w.cw = (int)pic.cb.width;
     w.ch = (int)pic.cb.height;
-    pr.st.dw_cus = blob.put(a.cus, a.n_cus * sizeof(h266_deblock_cu));
-    if (db.dw_sep) pr.st.dw_ccus = blob.put(a.chroma_cus, a.n_chroma_cus * sizeof(h266_deblock_cu));
+    // the CU lists packed: every CU's head, the tails of CUs with a TU map or a TB split
+    w.max_cu_dim = 4;
+    const h266_deblock_cu *lists[2] = {a.cus, a.chroma_cus};
+    const uint64_t counts[2] = {a.n_cus, db.dw_sep ? a.n_chroma_cus : 0};
+    thread_local std::vector<CuTail> tails;
+    for (int l = 0; l < (db.dw_sep ? 2 : 1); ++l) {
+      size_t off;
+      uint8_t *heads = blob.alloc(counts[l] * kCuHeadBytes, off);
+      (l ? pr.st.dw_ccus : pr.st.dw_cus) = off;
+      tails.clear();
+      for (uint64_t i = 0; i < counts[l]; ++i) {
+        const h266_deblock_cu &c = lists[l][i];
+        std::memcpy(heads + i * kCuHeadBytes, &c, kCuHeadBytes);
+        w.max_cu_dim = std::max(w.max_cu_dim, std::max(c.w, c.h));
+        if (c.has_tu64 || c.has_tb_split) {
+          CuTail t;
+          t.index = (uint32_t)i;
+          std::memcpy(t.tail, reinterpret_cast<const uint8_t *>(&c) + kCuHeadBytes, sizeof t.tail);
+          tails.push_back(t);
+        }
+      }
+      w.n_tails[l] = tails.size();
+      pr.st.dw_tails[l] = blob.put(tails.data(), tails.size() * sizeof(CuTail));
+    }
     if (db.dw_mv) {
       // Motion by CU when the grid covers the picture and every luma CU's
       // cells agree (the walk reads motion only inside CUs): one record per
       // CU instead of one per 4x4 cell.
       const h266_deblock_mv_grid &g = *a.mv_grid;
       bool per_cu = g.cells_w >= (uint64_t)(w.w + 3) / 4 && g.cells_h >= (uint64_t)(w.h + 3) / 4;
-      thread_local std::vector<h266_deblock_mv_cell> rec;
-      rec.resize(a.n_cus);
+      // Intra CUs read no motion (bS 2 comes first), so only the others' records travel.
+      thread_local std::vector<CuMotionRec> rec;
+      rec.clear();
       for (uint64_t i = 0; i < a.n_cus && per_cu; ++i) {
         const h266_deblock_cu &c = a.cus[i];
+        if (c.intra) continue;
         const h266_deblock_mv_cell *first = &g.cells[(c.y / 4) * g.cells_w + c.x / 4];
-        for (uint32_t y = c.y / 4; y < (c.y + c.h) / 4 && per_cu; ++y) {
-          const h266_deblock_mv_cell *row = &g.cells[y * g.cells_w];
-          for (uint32_t x = c.x / 4; x < (c.x + c.w) / 4; ++x)
-            if (std::memcmp(&row[x], first, sizeof *first) != 0) {
-              per_cu = false;
-              break;
-            }
-        }
-        rec[i] = *first;
+        const size_t w4 = c.w / 4;
+        // every cell of the first row equals its left neighbour, every row the first
+        per_cu = w4 < 2 || std::memcmp(first + 1, first, (w4 - 1) * sizeof *first) == 0;
+        for (uint32_t y = c.y / 4 + 1; y < (c.y + c.h) / 4 && per_cu; ++y)
+          per_cu = std::memcmp(&g.cells[y * g.cells_w + c.x / 4], first, w4 * sizeof *first) == 0;
+        CuMotionRec r;
+        r.index = (uint32_t)i;
+        r.m = *first;
+        rec.push_back(r);
       }
       db.dw_mv_cu = per_cu;
-      if (per_cu) pr.st.dw_mv = blob.put(rec.data(), a.n_cus * sizeof(h266_deblock_mv_cell));
+      w.mv_by_cu = per_cu;
+      w.n_mv_recs = per_cu ? rec.size() : 0;
+      if (per_cu) pr.st.dw_mv = blob.put(rec.data(), rec.size() * sizeof(CuMotionRec));
       else pr.st.dw_mv = blob.put(a.mv_grid->cells, w.mv_w * w.mv_h * sizeof(h266_deblock_mv_cell));
     }
     pr.st.dw_cols = blob.put(a.no_filter_cols, a.n_no_filter_cols * sizeof(uint32_t));
@@ -990,10 +1024,13 @@ int prepare_chain(Prep &pr, const h266_picture &pic, const h266_in_loop_filter_a
 // The device walk's inputs rebased onto the uploaded blob at `base`.
 DeviceWalkIn device_walk_in(const uint8_t *base, const Staged &st, const DbSide &db) {
   DeviceWalkIn in = db.dw;
-  in.cus = reinterpret_cast<const h266_deblock_cu *>(base + st.dw_cus);
-  in.chroma_cus = db.dw_sep ? reinterpret_cast<const h266_deblock_cu *>(base + st.dw_ccus) : in.cus;
+  in.heads[0] = base + st.dw_cus;
+  in.heads[1] = db.dw_sep ? base + st.dw_ccus : in.heads[0];
+  for (int l = 0; l < 2; ++l) in.tails[l] = reinterpret_cast<const CuTail *>(base + st.dw_tails[db.dw_sep ? l : 0]);
+  if (!db.dw_sep) in.n_tails[1] = in.n_tails[0];
   in.mv_cells = db.dw_mv && !db.dw_mv_cu ? reinterpret_cast<const h266_deblock_mv_cell *>(base + st.dw_mv) : nullptr;
-  in.mv_per_cu = db.dw_mv && db.dw_mv_cu ? reinterpret_cast<const h266_deblock_mv_cell *>(base + st.dw_mv) : nullptr;
+  in.mv_recs = db.dw_mv && db.dw_mv_cu ? reinterpret_cast<const CuMotionRec *>(base + st.dw_mv) : nullptr;
+  in.mv_by_cu = db.dw_mv && db.dw_mv_cu;
   in.nf_cols = reinterpret_cast<const uint32_t *>(base + st.dw_cols);
   in.nf_rows = reinterpret_cast<const uint32_t *>(base + st.dw_rows);
   return in;
@@ -2134,16 +2171,12 @@ int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *co
     // uploads on the upload stream once the lane's previous downloads freed its slots
     const cudaStream_t up = copy_streams ? ctx->e2e_up : L.stream;
     if (copy_streams) H266_CUDA(cudaStreamWaitEvent(up, L.ev_down, 0));
+    // the planes first: they need no preparation, so the link starts at once
+    items.resize(i1 - i0);
     for (uint32_t i = i0; i < i1; ++i) {
-      const auto tw = HClock::now();
-      pool->wait_item(i);
-      ctx->host_ns[1] += ns_since(tw);
-      Prep &pr = *ctx->preps[i + 1];
-      if (pr.rc != H266_OK) return set_error(pr.rc, pr.msg);
       GroupSlot &sl = L.slots[i - i0];
       const h266_picture &pic = *pics[i];
-      const h266_in_loop_filter_args &a = *args[i];
-      BatchItem it;
+      BatchItem &it = items[i - i0];
       const h266_plane *pl[3] = {&pic.luma, &pic.cb, &pic.cr};
       for (int k = 0; k < 3; ++k) {
         const h266_plane &q = *pl[k];
@@ -2160,10 +2193,22 @@ int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *co
                                       cudaMemcpyHostToDevice, up));
         it.P[k] = dplane(q, sl.io[k].as<uint16_t>(), q.width);
       }
+      ctx->h2d_bytes += host_plane_bytes(pic);
+    }
+    // then each picture's side information once its worker has prepared it
+    for (uint32_t i = i0; i < i1; ++i) {
+      const auto tw = HClock::now();
+      pool->wait_item(i);
+      ctx->host_ns[1] += ns_since(tw);
+      Prep &pr = *ctx->preps[i + 1];
+      if (pr.rc != H266_OK) return set_error(pr.rc, pr.msg);
+      GroupSlot &sl = L.slots[i - i0];
+      const h266_in_loop_filter_args &a = *args[i];
+      BatchItem &it = items[i - i0];
       H266_TRY(sl.side.ensure(pr.blob.size()));
       H266_CUDA(cudaMemcpyAsync(sl.side.ptr, pr.pinned.ptr, pr.blob.size(), cudaMemcpyHostToDevice, up));
       H266_CUDA(cudaEventRecord(pr.uploaded, up));
-      ctx->h2d_bytes += pr.blob.size() + host_plane_bytes(pic);
+      ctx->h2d_bytes += pr.blob.size();
       it.st = pr.st;
       it.st.base = sl.side.as<uint8_t>();
       it.db = pr.db;
@@ -2190,13 +2235,12 @@ int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *co
         H266_TRY(sl.walk.ensure(device_walk_bytes(pr.db.dw)));
         it.walk = sl.walk.as<uint8_t>();
       }
-      items.push_back(it);
     }
     if (copy_streams) {
       H266_CUDA(cudaEventRecord(L.ev_up, up));
       H266_CUDA(cudaStreamWaitEvent(L.stream, L.ev_up, 0));
     }
-    H266_TRY(exec_batch(ctx, L.bb, L.stream, items, tn));
+    H266_TRY(exec_batch(ctx, L.bb, L.stream, items, tn, copy_streams ? up : nullptr));
     const cudaStream_t down = copy_streams ? ctx->e2e_down : L.stream;
     if (copy_streams) {
       H266_CUDA(cudaEventRecord(L.ev_comp, L.stream));
@@ -2440,8 +2484,11 @@ int check_plan_batch(h266_ctx *ctx, uint32_t n, h266_chain_plan *const *plans, h
 // on the device (three launches for all of them), one tile-deblocking launch
 // and one SAO/ALF launch per kernel variant over every picture's tiles, and
 // per picture whatever the batched kernels do not take.
+// `upload`: the stream that carries the parameter table's upload (the
+// end-to-end pipeline's upload stream, so that the table is copied in issue
+// order with the planes instead of competing with them); `stream` by default.
 int exec_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, std::vector<BatchItem> &items,
-               const Tuning &tn) {
+               const Tuning &tn, cudaStream_t upload) {
   const uint32_t n = (uint32_t)items.size();
   if (!n) return H266_OK;
   H266_TRY(bb.init());
@@ -2521,14 +2568,16 @@ int exec_batch(h266_ctx *ctx, BatchBufs &bb, cudaStream_t stream, std::vector<Ba
       off_p2f[v] = blob.put(p2_first[v].data(), p2_first[v].size() * sizeof(uint32_t));
     }
   H266_TRY(bb.side.ensure(b.size()));
+  const cudaStream_t ups = upload ? upload : stream;
   if (!bb.capturing) {
-    H266_CUDA(cudaStreamWaitEvent(stream, bb.done, 0));  // earlier batches read bb.side (any stream)
-    H266_CUDA(cudaEventSynchronize(bb.staged));         // the previous upload has read the staging buffer
+    H266_CUDA(cudaStreamWaitEvent(ups, bb.done, 0));  // earlier batches read bb.side (any stream)
+    H266_CUDA(cudaEventSynchronize(bb.staged));      // the previous upload has read the staging buffer
   }
   H266_TRY(bb.stage.ensure(b.size()));
   std::memcpy(bb.stage.ptr, b.data(), b.size());
-  H266_CUDA(cudaMemcpyAsync(bb.side.ptr, bb.stage.ptr, b.size(), cudaMemcpyHostToDevice, stream));
-  H266_CUDA(cudaEventRecord(bb.staged, stream));
+  H266_CUDA(cudaMemcpyAsync(bb.side.ptr, bb.stage.ptr, b.size(), cudaMemcpyHostToDevice, ups));
+  H266_CUDA(cudaEventRecord(bb.staged, ups));
+  if (ups != stream) H266_CUDA(cudaStreamWaitEvent(stream, bb.staged, 0));
   const uint8_t *dside = bb.side.as<uint8_t>();
   // deblocking: per picture where the tile kernel does not apply, then the batched walks and tiles
   for (uint32_t i = 0; i < n; ++i) {

@@ -2066,13 +2066,14 @@ int device_walk_mode(const h266_picture &pic, const h266_deblock_cu *cus, uint64
   // row and column of the CU map: then a band's segments come out of the
   // reference's walk in position order, the order the strip kernels run a
   // chain of overlapping footprints in.
-  const int cw4 = (w + 3) / 4, ch4 = (h + 3) / 4;
+  const int cw4 = (w + 3) / 4, ch4 = (h + 3) / 4, words = (cw4 + 63) / 64;
+  thread_local std::vector<uint64_t> bits;  // occupied 4x4 cells, one bit each
   thread_local std::vector<int32_t> map, last_col;
   const h266_deblock_cu *lists[2] = {cus, chroma_cus};
   const uint64_t counts[2] = {n_cus, chroma_cus ? n_chroma : 0};
   for (int l = 0; l < 2; ++l) {
     if (!lists[l]) continue;
-    map.assign((size_t)cw4 * ch4, -1);
+    bits.assign((size_t)words * ch4, 0);
     bool chains = false;  // 4-sample edges, sub-block edges or narrow transform blocks in this list
     for (uint64_t i = 0; i < counts[l]; ++i) {
       const h266_deblock_cu &c = lists[l][i];
@@ -2090,17 +2091,29 @@ int device_walk_mode(const h266_picture &pic, const h266_deblock_cu *cus, uint64
         }
         if (dim < prev + 8) chains = true;
       }
-      for (uint32_t y = c.y / 4; y < (c.y + c.h) / 4; ++y)
-        for (uint32_t x = c.x / 4; x < (c.x + c.w) / 4; ++x) {
-          int32_t &o = map[(size_t)y * cw4 + x];
-          if (o >= 0) return 0;
-          o = (int32_t)i;
+      const uint32_t x0 = c.x / 4, x1 = (c.x + c.w) / 4;
+      for (uint32_t y = c.y / 4; y < (c.y + c.h) / 4; ++y) {
+        uint64_t *row = bits.data() + (size_t)y * words;
+        for (uint32_t x = x0; x < x1;) {  // the run's part inside one 64-cell word
+          const uint32_t wi = x / 64, lo = x % 64, n = std::min<uint32_t>(x1 - x, 64 - lo);
+          const uint64_t m = (n == 64 ? ~0ull : ((1ull << n) - 1)) << lo;
+          if (row[wi] & m) return 0;  // overlaps an earlier CU
+          row[wi] |= m;
+          x += n;
         }
+      }
     }
     if (chains) no_chains = false;
     // Only luma footprints chain (chroma edges are 8 chroma samples apart and
     // reach 4), so only the luma list's order matters.
     if (l != 0 || !chains) continue;
+    map.assign((size_t)cw4 * ch4, -1);
+    for (uint64_t i = 0; i < counts[l]; ++i) {
+      const h266_deblock_cu &c = lists[l][i];
+      for (uint32_t y = c.y / 4; y < (c.y + c.h) / 4; ++y)
+        std::fill(map.begin() + (size_t)y * cw4 + c.x / 4, map.begin() + (size_t)y * cw4 + (c.x + c.w) / 4,
+                  (int32_t)i);
+    }
     last_col.assign((size_t)cw4, -1);
     for (int y = 0; y < ch4; ++y) {
       int32_t last_row = -1;
@@ -2152,13 +2165,18 @@ struct CuMotion {
 };
 
 struct WalkParams {
-  const h266_deblock_cu *cus[2];  // luma list, chroma list
+  h266_deblock_cu *cus[2];  // luma list, chroma list: full records, expanded in the walk's scratch
   uint32_t n[2];
+  const uint8_t *heads[2];  // the staged packed lists (see CuTail, CuMotionRec)
+  const CuTail *tails[2];
+  uint32_t n_tails[2];
+  const CuMotionRec *mv_recs;
+  uint32_t n_mv_recs;
   int32_t *cu_grid[2];
   int cw4, ch4;
   h266_deblock_mv_grid mv;
   int has_mv;
-  const h266_deblock_mv_cell *mv_per_cu;  // non-null: motion by luma CU instead of the grid
+  h266_deblock_mv_cell *mv_per_cu;  // non-null: motion by luma CU instead of the grid (expanded)
   const uint32_t *nf[2];  // columns (vertical pass), rows (horizontal pass)
   uint32_t n_nf[2];
   PlaneCfg cfg[3];
@@ -2166,15 +2184,52 @@ struct WalkParams {
   uint32_t slots[2][3], bands[2][3];
 };
 
-// CuGrid::build: cell -> CU covering it, the later CU winning (here: the larger index).
+// Items of a list's first walk launch: its CU heads, then its tails, then
+// (luma list) the motion records.
+__host__ __device__ inline uint32_t unpack_items(const WalkParams &a, int list) {
+  return a.n[list] + a.n_tails[list] + (list == 0 ? a.n_mv_recs : 0);
+}
+
+// Item i of list `list`: a CU head is copied into the CU's full record (whose
+// tail the clearing left zero) and the CU enters the CU map (CuGrid::build:
+// cell -> CU covering it, the later CU winning, here the larger index); a
+// tail or a motion record is copied into its CU's full record.
+__device__ __forceinline__ void unpack_item(const WalkParams &a, int list, uint32_t i) {
+  if (i < a.n[list]) {
+    const uint64_t *src = reinterpret_cast<const uint64_t *>(a.heads[list] + (size_t)i * kCuHeadBytes);
+    uint64_t *dst = reinterpret_cast<uint64_t *>(a.cus[list] + i);
+    uint64_t w[kCuHeadBytes / 8];
+#pragma unroll
+    for (int k = 0; k < (int)(kCuHeadBytes / 8); ++k) w[k] = src[k];
+#pragma unroll
+    for (int k = 0; k < (int)(kCuHeadBytes / 8); ++k) dst[k] = w[k];
+    const uint32_t cx = (uint32_t)w[0], cy = (uint32_t)(w[0] >> 32), cw = (uint32_t)w[1], ch = (uint32_t)(w[1] >> 32);
+    const int x0 = cx / 4, y0 = cy / 4;
+    const int x1 = min((int)((cx + cw + 3) / 4), a.cw4), y1 = min((int)((cy + ch + 3) / 4), a.ch4);
+    for (int y = y0; y < y1; ++y)
+      for (int x = x0; x < x1; ++x) atomicMax(&a.cu_grid[list][(size_t)y * a.cw4 + x], (int32_t)i);
+    return;
+  }
+  i -= a.n[list];
+  if (i < a.n_tails[list]) {
+    const CuTail &t = a.tails[list][i];
+    if (t.index >= a.n[list]) return;
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(t.tail);
+    uint32_t *dst = reinterpret_cast<uint32_t *>(reinterpret_cast<uint8_t *>(a.cus[list] + t.index) + kCuHeadBytes);
+#pragma unroll
+    for (int k = 0; k < 10; ++k) dst[k] = src[k];
+    return;
+  }
+  i -= a.n_tails[list];
+  if (list == 0 && i < a.n_mv_recs && a.mv_per_cu) {
+    const CuMotionRec &r = a.mv_recs[i];
+    if (r.index < a.n[0]) a.mv_per_cu[r.index] = r.m;
+  }
+}
+
 __global__ void k_cu_grid(const __grid_constant__ WalkParams a, int list) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.n[list]) return;
-  const h266_deblock_cu &c = a.cus[list][i];
-  const int x0 = c.x / 4, y0 = c.y / 4;
-  const int x1 = min((int)((c.x + c.w + 3) / 4), a.cw4), y1 = min((int)((c.y + c.h + 3) / 4), a.ch4);
-  for (int y = y0; y < y1; ++y)
-    for (int x = x0; x < x1; ++x) atomicMax(&a.cu_grid[list][(size_t)y * a.cw4 + x], (int32_t)i);
+  if (i < unpack_items(a, list)) unpack_item(a, list, i);
 }
 
 // The edge walk of one CU for one (plane, pass) list (blockIdx.y = plane * 2 +
@@ -2203,7 +2258,8 @@ __global__ void __launch_bounds__(128) k_walk(const __grid_constant__ WalkParams
 size_t align_up(size_t n) { return (n + 255) & ~(size_t)255; }
 
 struct WalkLayout {
-  size_t cu_grid[2], grid[2][3], total;
+  size_t cu_grid[2], full[2], mv_full, grid[2][3], total;
+  size_t zero_from;  // [0, zero_from) is set to all ones (CU maps), the rest to zero
   uint32_t slots[2][3], bands[2][3];
 };
 
@@ -2213,9 +2269,16 @@ WalkLayout walk_layout(const DeviceWalkIn &in) {
   size_t off = 0;
   for (int l = 0; l < 2; ++l) {
     L.cu_grid[l] = off;
-    if (l == 0 || in.chroma_cus != in.cus) off += align_up(cells * 4);
+    if (l == 0 || in.sep) off += align_up(cells * 4);
   }
-  if (in.chroma_cus == in.cus) L.cu_grid[1] = L.cu_grid[0];
+  if (!in.sep) L.cu_grid[1] = L.cu_grid[0];
+  L.zero_from = off;
+  L.full[0] = off;
+  off += align_up((size_t)in.n_cus * sizeof(h266_deblock_cu));
+  L.full[1] = in.sep ? off : L.full[0];
+  if (in.sep) off += align_up((size_t)in.n_chroma * sizeof(h266_deblock_cu));
+  L.mv_full = off;
+  if (in.mv_by_cu) off += align_up((size_t)in.n_cus * sizeof(h266_deblock_mv_cell));
   for (int d = 0; d < 2; ++d)
     for (int p = 0; p < 3; ++p) {
       const bool has = p == 0 || in.cfi != 0;
@@ -2241,17 +2304,24 @@ namespace {
 void fill_walk(const DeviceWalkIn &in, uint8_t *scratch, WalkParams &a, DeviceWalkOut &out, WalkLayout &L) {
   L = walk_layout(in);
   std::memset(&a, 0, sizeof a);
-  const bool sep = in.chroma_cus != in.cus;
-  a.cus[0] = in.cus;
-  a.cus[1] = in.chroma_cus;
+  const bool sep = in.sep;
+  a.cus[0] = reinterpret_cast<h266_deblock_cu *>(scratch + L.full[0]);
+  a.cus[1] = reinterpret_cast<h266_deblock_cu *>(scratch + L.full[1]);
   a.n[0] = (uint32_t)in.n_cus;
   a.n[1] = (uint32_t)(sep ? in.n_chroma : in.n_cus);
+  for (int l = 0; l < 2; ++l) {
+    a.heads[l] = in.heads[sep ? l : 0];
+    a.tails[l] = in.tails[sep ? l : 0];
+    a.n_tails[l] = (uint32_t)in.n_tails[sep ? l : 0];
+  }
+  a.mv_recs = in.mv_recs;
+  a.n_mv_recs = (uint32_t)in.n_mv_recs;
   a.cw4 = (in.w + 3) / 4;
   a.ch4 = (in.h + 3) / 4;
   a.cu_grid[0] = reinterpret_cast<int32_t *>(scratch + L.cu_grid[0]);
   a.cu_grid[1] = reinterpret_cast<int32_t *>(scratch + L.cu_grid[1]);
-  a.has_mv = in.mv_cells != nullptr || in.mv_per_cu != nullptr;
-  a.mv_per_cu = in.mv_per_cu;
+  a.has_mv = in.mv_cells != nullptr || in.mv_by_cu;
+  a.mv_per_cu = in.mv_by_cu ? reinterpret_cast<h266_deblock_mv_cell *>(scratch + L.mv_full) : nullptr;
   a.mv.cells = in.mv_cells;
   a.mv.cells_w = in.mv_w;
   a.mv.cells_h = in.mv_h;
@@ -2285,16 +2355,15 @@ int launch_device_walk(cudaStream_t st, const DeviceWalkIn &in, uint8_t *scratch
   WalkParams a;
   WalkLayout L;
   fill_walk(in, scratch, a, out, L);
-  const bool sep = in.chroma_cus != in.cus;
-  // CU maps to -1 (no CU), segment grids to bS 0 (no segment)
-  const size_t cells = (size_t)a.cw4 * a.ch4;
-  H266_CUDA(cudaMemsetAsync(a.cu_grid[0], 0xFF, cells * 4, st));
-  if (sep) H266_CUDA(cudaMemsetAsync(a.cu_grid[1], 0xFF, cells * 4, st));
-  H266_CUDA(cudaMemsetAsync(scratch + L.grid[0][0], 0, L.total - L.grid[0][0], st));
+  const bool sep = in.sep;
+  // CU maps to -1 (no CU); full CU records, motion and segment grids to 0 (bS 0: no segment)
+  H266_CUDA(cudaMemsetAsync(scratch, 0xFF, L.zero_from, st));
+  H266_CUDA(cudaMemsetAsync(scratch + L.zero_from, 0, L.total - L.zero_from, st));
   const int lists = in.cfi != 0 ? 6 : 2;
   for (int l = 0; l < (sep && in.cfi != 0 ? 2 : 1); ++l) {
-    if (!a.n[l]) continue;
-    k_cu_grid<<<(a.n[l] + 127) / 128, 128, 0, st>>>(a, l);
+    const uint32_t items = unpack_items(a, l);
+    if (!items) continue;
+    k_cu_grid<<<(items + 127) / 128, 128, 0, st>>>(a, l);
     H266_CUDA(cudaGetLastError());
     ++*launches;
   }
@@ -2355,15 +2424,10 @@ __global__ void __launch_bounds__(128) k_cu_grid_batch(const WalkBatchItem *__re
                                                        const uint32_t *__restrict__ first, int n) {
   const int p = batch_pick(first, n, blockIdx.x);
   const WalkParams &a = items[p].p;
-  const uint32_t lb = blockIdx.x - first[p], b0 = (a.n[0] + 127) / 128;
+  const uint32_t lb = blockIdx.x - first[p], b0 = (unpack_items(a, 0) + 127) / 128;
   const int list = lb < b0 ? 0 : 1;
   const uint32_t i = (lb - (list ? b0 : 0)) * 128 + threadIdx.x;
-  if (i >= a.n[list]) return;
-  const h266_deblock_cu &c = a.cus[list][i];
-  const int x0 = c.x / 4, y0 = c.y / 4;
-  const int x1 = min((int)((c.x + c.w + 3) / 4), a.cw4), y1 = min((int)((c.y + c.h + 3) / 4), a.ch4);
-  for (int y = y0; y < y1; ++y)
-    for (int x = x0; x < x1; ++x) atomicMax(&a.cu_grid[list][(size_t)y * a.cw4 + x], (int32_t)i);
+  if (i < unpack_items(a, list)) unpack_item(a, list, i);
 }
 
 // blockIdx.y = plane * 2 + pass, blockIdx.z = edge offset / step, as k_walk.
@@ -2406,14 +2470,14 @@ void fill_walk_batch_item(void *out, const DeviceWalkIn &in, uint8_t *scratch, D
   std::memset(&it, 0, sizeof it);
   WalkLayout L;
   fill_walk(in, scratch, it.p, g, L);
-  const bool sep = in.chroma_cus != in.cus;
+  const bool sep = in.sep;
   it.clear = reinterpret_cast<uint4 *>(scratch);
-  it.ff_vec = (uint32_t)(L.grid[0][0] / 16);  // the CU maps precede the grids (256-byte sections)
-  it.zero_vec = (uint32_t)((L.total - L.grid[0][0]) / 16);
+  it.ff_vec = (uint32_t)(L.zero_from / 16);  // the CU maps come first (256-byte sections)
+  it.zero_vec = (uint32_t)((L.total - L.zero_from) / 16);
   it.lists = in.cfi != 0 ? 6 : 2;
   it.cu_lists = sep && in.cfi != 0 ? 2 : 1;
   c.clear_ctas = (it.ff_vec + it.zero_vec + kClearVecPerCta - 1) / kClearVecPerCta;
-  c.grid_ctas = (it.p.n[0] + 127) / 128 + (it.cu_lists == 2 ? (it.p.n[1] + 127) / 128 : 0);
+  c.grid_ctas = (unpack_items(it.p, 0) + 127) / 128 + (it.cu_lists == 2 ? (unpack_items(it.p, 1) + 127) / 128 : 0);
   c.walk_ctas = (std::max(it.p.n[0], it.p.n[1]) + 127) / 128;
   c.offsets = (std::max<uint32_t>(4, in.max_cu_dim) + 3) / 4;
   std::memcpy(out, &it, sizeof it);

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <condition_variable>
+#include <cstddef>
 #include <cstdint>
 #include <functional>
 #include <mutex>
@@ -193,12 +194,33 @@ int launch_deblock_tiles_batch(cudaStream_t st, const void *d_params, const uint
 int device_walk_mode(const h266_picture &pic, const h266_deblock_cu *cus, uint64_t n_cus,
                      const h266_deblock_cu *chroma_cus, uint64_t n_chroma, const h266_deblock_params &params,
                      uint32_t cfi);
+// The CU lists travel to the device packed: per CU its first kCuHeadBytes
+// (position, size, QPs, flags, sub-block counts), and a CuTail (the 64-sample
+// TU map and TB split) only for CUs that have either; with motion by CU, a
+// CuMotionRec only for CUs that are not intra (intra CUs read no motion).
+// The walk's first launch expands them into full records in its scratch.
+constexpr size_t kCuHeadBytes = 56;
+static_assert(offsetof(h266_deblock_cu, tu64) == kCuHeadBytes, "CU head layout");
+static_assert(sizeof(h266_deblock_cu) == kCuHeadBytes + 40, "CU tail layout");
+struct CuTail {
+  uint32_t index;
+  uint8_t tail[40];  // bytes [kCuHeadBytes, sizeof(h266_deblock_cu)) of the CU
+};
+struct CuMotionRec {
+  uint32_t index;
+  h266_deblock_mv_cell m;
+};
 struct DeviceWalkIn {  // device pointers
-  const h266_deblock_cu *cus, *chroma_cus;  // chroma_cus == cus for a single tree
+  const uint8_t *heads[2];  // packed CU heads: luma list, chroma list (== heads[0] for a single tree)
+  const CuTail *tails[2];
+  uint64_t n_tails[2];
   uint64_t n_cus, n_chroma;
+  bool sep;                              // a separate chroma tree
   const h266_deblock_mv_cell *mv_cells;  // nullptr: no motion grid (or motion by CU)
   uint64_t mv_w, mv_h;
-  const h266_deblock_mv_cell *mv_per_cu;  // motion by luma CU when every CU's cells agree
+  const CuMotionRec *mv_recs;  // motion by luma CU (every CU's cells agree): the non-intra CUs' records
+  uint64_t n_mv_recs;
+  bool mv_by_cu;
   const uint32_t *nf_cols, *nf_rows;
   uint64_t n_cols, n_rows;
   h266_deblock_params params;

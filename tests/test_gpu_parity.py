@@ -166,7 +166,8 @@ def test_batch_pipelined_host_pictures(ctx):
         assert_same(got, want, f"batch picture {i}")
 
 
-@pytest.mark.parametrize("group,lanes,copy_streams,prep", [(1, 1, 0, 2), (2, 4, 1, 3), (8, 2, 0, 0), (3, 3, 1, 16)])
+@pytest.mark.parametrize("group,lanes,copy_streams,prep", [(1, 1, 0, 2), (2, 4, 1, 3), (8, 2, 0, 0), (3, 3, 1, 16),
+                                                          (1, 1, 1, 0), (2, 16, 1, 4)])
 def test_batch_launch_shapes_match_oracle(group, lanes, copy_streams, prep):
     """The end-to-end batch under other tunings (group size, streams, copy
     streams, preparation threads): the same results, bit for bit.  Pinned
