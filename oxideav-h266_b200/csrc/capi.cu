@@ -769,6 +769,7 @@ int run_deblock(h266_ctx *ctx, cudaStream_t stream, const uint8_t *base, const S
                 const DPlane src[3], const DPlane dst[3], const uint16_t *lut, int bd, uint8_t *walk = nullptr) {
   if (db.device_walk) {  // side information built on the device, then the tile or strip kernels on its grids
     if (!walk) return set_error(H266_ERR_INVALID_ARGUMENT, "device-built side information without walk scratch");
+    if (db.dw_tiles && !db.dw.tile_lists) return set_error(H266_ERR_UNSUPPORTED, "grid-mode tiles without tile lists");
     Prof pf(ctx, stream, H266_PROF_DEBLOCK);
     DeviceWalkOut out;
     H266_TRY(launch_device_walk(stream, device_walk_in(base, st, db), walk, out, &ctx->launches));
@@ -940,6 +941,7 @@ int prepare_chain(Prep &pr, const h266_picture &pic, const h266_in_loop_filter_a
     DbSide &db = pr.db;
     db.device_walk = true;
     db.dw_tiles = mode == 1 && (pr.h.do_sao || pr.h.do_alf);
+    db.dw.tile_lists = mode == 1;  // the walk lists each tile's cells (within the lists' caps in mode 1)
     db.dw_sep = a.chroma_cus != nullptr;
     db.dw_mv = a.mv_grid && a.mv_grid->cells && a.mv_grid->cells_w * a.mv_grid->cells_h;
     DeviceWalkIn &w = db.dw;

@@ -1564,10 +1564,13 @@ struct TileParams {
   int maxv;
   // Grid mode (side information built on the device): every component is one
   // segment, stored in grid[d][p][band * grid_slots[d][p] + pos / unit] (bs 0:
-  // none), unit 4 luma / 8 chroma samples along the edge normal.
+  // none), unit 4 luma / 8 chroma samples along the edge normal; the walk
+  // lists each tile's cells.
   int grid_mode;
   const EdgeSeg *grid[2][3];
   uint32_t grid_slots[2][3];
+  const uint32_t *grid_count;       // cells per (tile, pass, plane), listed by the walk
+  const uint32_t *grid_list[2][3];  // their grid indices, kTileListY / kTileListC per tile
 };
 
 constexpr int kTileBands = 32;  // bands of one tile and pass that a plane can have (at most 24)
@@ -1613,57 +1616,23 @@ __device__ __forceinline__ void store_window(const uint16_t *sm, int pitch, cons
 
 // Band counts and prefix sums of the tile's component ranges for (pass d,
 // plane p), by one warp.
-// Grid mode: the list of (pass d, plane p) of tile (tx, ty) by one warp,
-// scanning the grid cells of the tile's bands whose footprint reaches the
-// tile; s_off[kTileBands] receives the count.
-__device__ __forceinline__ void tile_grid_list(const TileParams &a, int d, int p, int tx, int ty, uint32_t *list,
-                                               uint32_t cap, uint32_t *s_off) {
+// Grid mode: the list of (pass d, plane p) of tile t, copied from the one
+// the device walk built; s_off[kTileBands] receives the count.
+__device__ __forceinline__ void tile_grid_list(const TileParams &a, int d, int p, int t, uint32_t *list, uint32_t cap,
+                                               uint32_t *s_off) {
   const int lane = threadIdx.x & 31;
-  const int tp = p ? kDeblockTile / 2 : kDeblockTile, halo = p ? kDeblockHaloC : kDeblockHaloY, unit = p ? 2 : 4;
-  const int pu = p ? 8 : 4;  // grid positions along the edge normal
-  const int nb = (int)a.n_bands[d][p], ns = (int)a.grid_slots[d][p];
-  const EdgeSeg *g = a.grid[d][p];
-  const DPlane &pl = a.src[p];
-  const int along = d == 0 ? pl.w : pl.h;
-  int b0, b1, t0, t1;  // bands; tile extent along the normal
-  if (d == 0) {
-    b0 = max(ty * tp - halo, 0) / unit;
-    b1 = min((ty * tp + tp + halo) / unit, nb);
-    t0 = tx * tp;
-    t1 = min(t0 + tp, along);
-  } else {
-    b0 = tx * tp / unit;
-    b1 = min((tx * tp + tp) / unit, nb);
-    t0 = ty * tp;
-    t1 = min(t0 + tp, along);
-  }
-  const int s0 = max(t0 - halo, 0) / pu, s1 = min((t1 + halo + pu - 1) / pu, ns);
-  uint32_t n = 0;
-  for (int b = b0; b < b1; ++b) {
-    for (int sb = s0; sb < s1; sb += 32) {
-      const int sl = sb + lane;
-      bool take = false;
-      uint32_t cell = 0;
-      if (sl < s1) {
-        cell = (uint32_t)b * ns + sl;
-        const EdgeSeg e = g[cell];
-        if (e.bs) {
-          const int pos = d == 0 ? e.x : e.y;
-          const int fs = max(pos - reach_d(e.mfl >> 4), 0), fe = min(pos + reach_d(e.mfl & 15), along);
-          take = fs < t1 && fe > t0;
-        }
-      }
-      const unsigned m = __ballot_sync(0xFFFFFFFFu, take);
-      const uint32_t rank = __popc(m & ((1u << lane) - 1));
-      if (take && n + rank < cap) list[n + rank] = cell;
-      n += __popc(m);
-    }
-  }
-  if (lane == 0) s_off[kTileBands] = min(n, cap);
+  const uint32_t n = min(a.grid_count[(size_t)t * 6 + d * 3 + p], cap);
+  const uint32_t *src = a.grid_list[d][p] + (size_t)t * cap;
+  for (uint32_t i = lane; i < n; i += 32) list[i] = src[i];
+  if (lane == 0) s_off[kTileBands] = n;
 }
 
-__device__ __forceinline__ void tile_prefix(const TileParams &a, int d, int p, int tx, int ty,
-                                            uint32_t *s_off /* kTileBands + 1 */, uint32_t *s_lo /* kTileBands */) {
+// Host-built lists: the tile's component ranges of (pass d, plane p), one
+// band per lane, written out as the tile's list of component indices (each
+// lane its band's range at the band's prefix offset); s_off[kTileBands]
+// receives the count.  The host keeps every tile's count within `cap`.
+__device__ __forceinline__ void tile_prefix(const TileParams &a, int d, int p, int tx, int ty, uint32_t *list,
+                                            uint32_t cap, uint32_t *s_off /* kTileBands + 1 */) {
   const int lane = threadIdx.x & 31;
   const int tp = p ? kDeblockTile / 2 : kDeblockTile, halo = p ? kDeblockHaloC : kDeblockHaloY, unit = p ? 2 : 4;
   const int nb = (int)a.n_bands[d][p];
@@ -1692,9 +1661,8 @@ __device__ __forceinline__ void tile_prefix(const TileParams &a, int d, int p, i
     const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
     if (lane >= o) incl += y;
   }
-  s_lo[lane] = lo;
-  s_off[lane + 1] = incl;
-  if (lane == 0) s_off[0] = 0;
+  for (uint32_t k = 0, o = incl - cnt; k < cnt && o + k < cap; ++k) list[o + k] = lo + k;
+  if (lane == 31) s_off[kTileBands] = min(incl, cap);
 }
 
 // The staged window of plane p of tile (tx, ty): the tile widened by the
@@ -1760,7 +1728,7 @@ __device__ __forceinline__ void run_tile_pass(const TileParams &a, uint16_t *sm,
 
 struct TileShared {
   uint32_t list_y[2][kTileListY], list_c[2][2][kTileListC];
-  uint32_t off[2][3][kTileBands + 1], lo[2][3][kTileBands];
+  uint32_t off[2][3][kTileBands + 1];  // [kTileBands]: list length
 };
 
 // Tile t of the picture whose parameters are `a`.
@@ -1770,32 +1738,24 @@ __device__ __forceinline__ void deblock_tile(const TileParams &a, int t) {
   auto &s_list_y = ts.list_y;
   auto &s_list_c = ts.list_c;
   auto &s_off = ts.off;
-  auto &s_lo = ts.lo;
   const int tx = t % (int)a.tiles_x, ty = t / (int)a.tiles_x;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, n_warps = blockDim.x >> 5;
-  // Warps 0-5 first read the component ranges of both passes (one warp per
-  // pass and plane) -- in grid mode they build the lists outright -- then
+  const int warp = threadIdx.x >> 5;
+  // Warps 0-5 first build the component lists of both passes (one warp per
+  // pass and plane, from the host's ranges or the device walk's grids), then
   // every thread loads the planes' regions.
   if (warp < 6) {
     const int d = warp / 3, p = warp % 3;
     if (a.grid_mode)
-      tile_grid_list(a, d, p, tx, ty, p == 0 ? s_list_y[d] : s_list_c[d][p - 1], p == 0 ? kTileListY : kTileListC,
+      tile_grid_list(a, d, p, t, p == 0 ? s_list_y[d] : s_list_c[d][p - 1], p == 0 ? kTileListY : kTileListC,
                      s_off[d][p]);
     else
-      tile_prefix(a, d, p, tx, ty, s_off[d][p], s_lo[d][p]);
+      tile_prefix(a, d, p, tx, ty, p == 0 ? s_list_y[d] : s_list_c[d][p - 1], p == 0 ? kTileListY : kTileListC,
+                  s_off[d][p]);
   }
 #pragma unroll
   for (int p = 0; p < 3; ++p) {
     const SharedView v = tile_view(a, sm, p, tx, ty);
     if (v.ww > 0 && v.wh > 0) load_window(v.s, v.ld, a.src[p], v.ox, v.oy, v.ww, v.wh, p == 0 ? a.lut : nullptr);
-  }
-  __syncthreads();
-  // expand the ranges into the lists: one warp per (pass, plane, band)
-  for (int task = warp; task < (a.grid_mode ? 0 : 6 * kTileBands); task += n_warps) {
-    const int dp = task / kTileBands, j = task % kTileBands, d = dp / 3, p = dp % 3;
-    const uint32_t o = s_off[d][p][j], cnt = s_off[d][p][j + 1] - o, lo = s_lo[d][p][j];
-    uint32_t *list = p == 0 ? s_list_y[d] : s_list_c[d][p - 1];
-    for (uint32_t i = lane; i < cnt; i += 32) list[o + i] = lo + i;
   }
   __syncthreads();
 #pragma unroll
@@ -2141,17 +2101,6 @@ struct DevCuGrid {  // CuGrid::cu_at on device memory
   }
 };
 
-struct GridEmit {  // a segment into its grid cell
-  EdgeSeg *g;
-  uint32_t slots, bands;
-  int unit, pu;
-  __device__ void operator()(const EdgeSeg &s) {
-    const bool vert = s.flags & 1;
-    const uint32_t band = (uint32_t)((vert ? s.y : s.x) / unit), pos = (uint32_t)((vert ? s.x : s.y) / pu);
-    if (band < bands && pos < slots) g[(size_t)band * slots + pos] = s;
-  }
-};
-
 // Motion by CU: every 4x4 cell of a CU carries the same motion (checked on
 // the host), so the cell's motion is its CU's record.
 struct CuMotion {
@@ -2182,6 +2131,61 @@ struct WalkParams {
   PlaneCfg cfg[3];
   EdgeSeg *grid[2][3];
   uint32_t slots[2][3], bands[2][3];
+  // Per-tile lists for the grid-mode tile kernel (null when the strip kernels
+  // consume the grids): tile_count[tile * 6 + pass * 3 + plane] cells, listed
+  // at tile_list[pass][plane][tile * cap], cap kTileListY (luma) or
+  // kTileListC (chroma).
+  uint32_t *tile_count;
+  uint32_t *tile_list[2][3];
+  uint32_t tiles_x, tiles_y;
+  int pw[3], ph[3];
+};
+
+// A segment into its grid cell and, for the tile kernel, into the list of
+// every tile it runs in: a vertical-pass segment in the tiles whose columns
+// its footprint reaches and whose rows widened by the halo hold its band, a
+// horizontal-pass segment in the tile holding its band whose rows its
+// footprint reaches (the host's index_tiles rule).  A picture the tile kernel
+// takes has no two footprints overlapping and edges at least 8 samples apart,
+// so a tile's list holds at most 24 bands x 12 luma (16 x 12 horizontal) or
+// 24 x 6 chroma cells, within the caps.
+struct GridEmit {
+  const WalkParams *a;
+  int d, p;
+  __device__ void operator()(const EdgeSeg &s) const {
+    const bool vert = s.flags & 1;
+    const int unit = p ? 2 : 4, pu = p ? 8 : 4;
+    const uint32_t band = (uint32_t)((vert ? s.y : s.x) / unit), pos = (uint32_t)((vert ? s.x : s.y) / pu);
+    const uint32_t slots = a->slots[d][p];
+    if (band >= a->bands[d][p] || pos >= slots) return;
+    const uint32_t cell = band * slots + pos;
+    a->grid[d][p][cell] = s;
+    if (!a->tile_count) return;
+    const int tp = p ? kDeblockTile / 2 : kDeblockTile, halo = p ? kDeblockHaloC : kDeblockHaloY;
+    const int along = vert ? a->pw[p] : a->ph[p], q = vert ? s.x : s.y, bc = vert ? s.y : s.x;
+    const int fs = max(q - reach_d(s.mfl >> 4), 0), fe = min(q + reach_d(s.mfl & 15), along);
+    if (fs >= fe) return;  // touches no sample of the plane
+    int x0, x1, y0, y1;    // tile columns and rows
+    if (vert) {
+      x0 = fs / tp;
+      x1 = (fe - 1) / tp;
+      y0 = bc - halo < 0 ? 0 : (bc - halo) / tp;
+      y1 = (bc + unit + halo - 1) / tp;
+    } else {
+      x0 = x1 = bc / tp;
+      y0 = fs / tp;
+      y1 = (fe - 1) / tp;
+    }
+    x1 = min(x1, (int)a->tiles_x - 1);
+    y1 = min(y1, (int)a->tiles_y - 1);
+    const uint32_t cap = p ? kTileListC : kTileListY;
+    for (int ty = y0; ty <= y1; ++ty)
+      for (int tx = x0; tx <= x1; ++tx) {
+        const uint32_t t = (uint32_t)ty * a->tiles_x + tx;
+        const uint32_t k = atomicAdd(a->tile_count + t * 6 + d * 3 + p, 1u);
+        if (k < cap) a->tile_list[d][p][(size_t)t * cap + k] = cell;
+      }
+  }
 };
 
 // Items of a list's first walk launch: its CU heads, then its tails, then
@@ -2245,7 +2249,7 @@ __global__ void __launch_bounds__(128) k_walk(const __grid_constant__ WalkParams
   const uint32_t off = blockIdx.z * step;
   if (off >= (d == 0 ? cu.w : cu.h)) return;
   const DevCuGrid grid{a.cu_grid[list], a.cw4, a.ch4};
-  GridEmit emit{a.grid[d][plane], a.slots[d][plane], a.bands[d][plane], plane ? 2 : 4, plane ? 8 : 4};
+  const GridEmit emit{&a, d, plane};
   if (plane == 0 && a.has_mv && a.mv_per_cu) {
     const CuMotion mv{&a.mv, a.mv_per_cu, DevCuGrid{a.cu_grid[0], a.cw4, a.ch4}};
     walk_cu(a.cus[list], grid, a.cfg[plane], d == 0, mv, a.nf[d], a.n_nf[d], i, emit, (int)off);
@@ -2258,8 +2262,8 @@ __global__ void __launch_bounds__(128) k_walk(const __grid_constant__ WalkParams
 size_t align_up(size_t n) { return (n + 255) & ~(size_t)255; }
 
 struct WalkLayout {
-  size_t cu_grid[2], full[2], mv_full, grid[2][3], total;
-  size_t zero_from;  // [0, zero_from) is set to all ones (CU maps), the rest to zero
+  size_t cu_grid[2], full[2], mv_full, grid[2][3], tile_count, tile_list[2][3], total;
+  size_t zero_from, zero_end;  // [0, zero_from) is set to all ones (CU maps), [zero_from, zero_end) to zero
   uint32_t slots[2][3], bands[2][3];
 };
 
@@ -2288,6 +2292,17 @@ WalkLayout walk_layout(const DeviceWalkIn &in) {
       L.slots[d][p] = has && pw > 0 && ph > 0 ? (uint32_t)(((d == 0 ? pw : ph) + pu - 1) / pu) : 0;
       L.grid[d][p] = off;
       off += align_up((size_t)L.bands[d][p] * L.slots[d][p] * sizeof(EdgeSeg));
+    }
+  const size_t tiles = in.tile_lists ? (size_t)((in.w + kDeblockTile - 1) / kDeblockTile) *
+                                           ((in.h + kDeblockTile - 1) / kDeblockTile)
+                                     : 0;
+  L.tile_count = off;
+  off += align_up(tiles * 6 * sizeof(uint32_t));
+  L.zero_end = off;
+  for (int d = 0; d < 2; ++d)
+    for (int p = 0; p < 3; ++p) {  // list entries are written before they are read: not cleared
+      L.tile_list[d][p] = off;
+      off += align_up(tiles * (p ? kTileListC : kTileListY) * sizeof(uint32_t));
     }
   L.total = off;
   return L;
@@ -2343,9 +2358,19 @@ void fill_walk(const DeviceWalkIn &in, uint8_t *scratch, WalkParams &a, DeviceWa
       out.grid[d][p] = a.grid[d][p];
       out.slots[d][p] = L.slots[d][p];
       out.bands[d][p] = L.bands[d][p];
+      a.tile_list[d][p] = in.tile_lists ? reinterpret_cast<uint32_t *>(scratch + L.tile_list[d][p]) : nullptr;
+      out.tile_list[d][p] = a.tile_list[d][p];
     }
   out.tiles_x = (uint32_t)((in.w + kDeblockTile - 1) / kDeblockTile);
   out.tiles_y = (uint32_t)((in.h + kDeblockTile - 1) / kDeblockTile);
+  a.tile_count = in.tile_lists ? reinterpret_cast<uint32_t *>(scratch + L.tile_count) : nullptr;
+  out.tile_count = a.tile_count;
+  a.tiles_x = out.tiles_x;
+  a.tiles_y = out.tiles_y;
+  a.pw[0] = in.w;
+  a.ph[0] = in.h;
+  a.pw[1] = a.pw[2] = in.cw;
+  a.ph[1] = a.ph[2] = in.ch;
 }
 
 }  // namespace
@@ -2358,7 +2383,7 @@ int launch_device_walk(cudaStream_t st, const DeviceWalkIn &in, uint8_t *scratch
   const bool sep = in.sep;
   // CU maps to -1 (no CU); full CU records, motion and segment grids to 0 (bS 0: no segment)
   H266_CUDA(cudaMemsetAsync(scratch, 0xFF, L.zero_from, st));
-  H266_CUDA(cudaMemsetAsync(scratch + L.zero_from, 0, L.total - L.zero_from, st));
+  H266_CUDA(cudaMemsetAsync(scratch + L.zero_from, 0, L.zero_end - L.zero_from, st));
   const int lists = in.cfi != 0 ? 6 : 2;
   for (int l = 0; l < (sep && in.cfi != 0 ? 2 : 1); ++l) {
     const uint32_t items = unpack_items(a, l);
@@ -2451,7 +2476,7 @@ __global__ void __launch_bounds__(128) k_walk_batch(const WalkBatchItem *__restr
   const uint32_t off = blockIdx.z * step;
   if (off >= (d == 0 ? cu.w : cu.h)) return;
   const DevCuGrid grid{a.cu_grid[list], a.cw4, a.ch4};
-  GridEmit emit{a.grid[d][plane], a.slots[d][plane], a.bands[d][plane], plane ? 2 : 4, plane ? 8 : 4};
+  const GridEmit emit{&a, d, plane};
   if (plane == 0 && a.has_mv && a.mv_per_cu) {
     const CuMotion mv{&a.mv, a.mv_per_cu, DevCuGrid{a.cu_grid[0], a.cw4, a.ch4}};
     walk_cu(a.cus[list], grid, a.cfg[plane], d == 0, mv, a.nf[d], a.n_nf[d], i, emit, (int)off);
@@ -2473,7 +2498,7 @@ void fill_walk_batch_item(void *out, const DeviceWalkIn &in, uint8_t *scratch, D
   const bool sep = in.sep;
   it.clear = reinterpret_cast<uint4 *>(scratch);
   it.ff_vec = (uint32_t)(L.zero_from / 16);  // the CU maps come first (256-byte sections)
-  it.zero_vec = (uint32_t)((L.total - L.zero_from) / 16);
+  it.zero_vec = (uint32_t)((L.zero_end - L.zero_from) / 16);
   it.lists = in.cfi != 0 ? 6 : 2;
   it.cu_lists = sep && in.cfi != 0 ? 2 : 1;
   c.clear_ctas = (it.ff_vec + it.zero_vec + kClearVecPerCta - 1) / kClearVecPerCta;
@@ -2517,8 +2542,10 @@ uint32_t fill_deblock_tile_params_grid(void *out, const DPlane src[3], const DPl
       a.n_bands[d][i] = g.bands[d][i];
       a.grid[d][i] = g.grid[d][i];
       a.grid_slots[d][i] = g.slots[d][i];
+      a.grid_list[d][i] = g.tile_list[d][i];
     }
   }
+  a.grid_count = g.tile_count;
   a.grid_mode = 1;
   a.lut = lut;
   a.tiles_x = g.tiles_x;
@@ -2539,8 +2566,10 @@ int launch_deblock_tiles_grid(cudaStream_t st, const DPlane src[3], const DPlane
       a.n_bands[d][i] = g.bands[d][i];
       a.grid[d][i] = g.grid[d][i];
       a.grid_slots[d][i] = g.slots[d][i];
+      a.grid_list[d][i] = g.tile_list[d][i];
     }
   }
+  a.grid_count = g.tile_count;
   a.grid_mode = 1;
   a.lut = lut;
   a.tiles_x = g.tiles_x;

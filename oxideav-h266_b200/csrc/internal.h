@@ -227,12 +227,15 @@ struct DeviceWalkIn {  // device pointers
   uint32_t cfi;
   int w, h, cw, ch;      // luma and chroma plane sizes
   uint32_t max_cu_dim;   // largest CU width or height of both lists
+  bool tile_lists;       // also list each tile's cells for the grid-mode tile kernel
 };
 size_t device_walk_bytes(const DeviceWalkIn &in);  // scratch for the CU maps and segment grids
 struct DeviceWalkOut {
   EdgeSeg *grid[2][3];
   uint32_t slots[2][3], bands[2][3];
   uint32_t tiles_x, tiles_y;
+  uint32_t *tile_count;       // with DeviceWalkIn::tile_lists: cells per (tile, pass, plane)
+  uint32_t *tile_list[2][3];  // and their grid indices, kTileListY / kTileListC per tile
 };
 int launch_device_walk(cudaStream_t st, const DeviceWalkIn &in, uint8_t *scratch, DeviceWalkOut &out,
                        uint64_t *launches);

@@ -270,11 +270,14 @@ class Context:
         _check(lib().h266_chain_plan_execute_batch(self._h, len(plans), P, Q))
 
     def apply_in_loop_filters_batch(self, pics, fas):
-        cps = [p.to_ctypes() for p in pics]
-        built = [f.to_ctypes() for f in fas]
-        P = (C.c_void_p * len(pics))(*[C.addressof(c) for c in cps])
-        A = (C.c_void_p * len(pics))(*[C.addressof(a) for a, _ in built])
-        _check(lib().h266_apply_in_loop_filters_batch(self._h, len(pics), P, A))
+        self.batch_call(pics, fas).run()
+
+    def batch_call(self, pics, fas) -> "BatchCall":
+        """The C argument arrays of h266_apply_in_loop_filters_batch over
+        (pics, fas), built once: run() makes the call (side information from
+        the CU lists, uploads, chain, downloads) on the samples the pictures'
+        buffers hold at that time."""
+        return BatchCall(self, pics, fas)
 
     def apply_deblocking_clipped(self, pic, fa: FilterArgsData):
         cp = pic.to_ctypes()
@@ -342,6 +345,22 @@ class ChainPlan:
             self.close()
         except Exception:
             pass
+
+
+class BatchCall:
+    """Prepared arguments of one h266_apply_in_loop_filters_batch call (the
+    C structs a caller fills once per picture; Context.batch_call)."""
+
+    def __init__(self, ctx: Context, pics, fas):
+        self._ctx = ctx
+        self._cps = [p.to_ctypes() for p in pics]
+        self._built = [f.to_ctypes() for f in fas]
+        self._n = len(pics)
+        self._P = (C.c_void_p * self._n)(*[C.addressof(c) for c in self._cps])
+        self._A = (C.c_void_p * self._n)(*[C.addressof(a) for a, _ in self._built])
+
+    def run(self):
+        _check(lib().h266_apply_in_loop_filters_batch(self._ctx._h, self._n, self._P, self._A))
 
 
 class BatchGraph:
