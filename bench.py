@@ -893,7 +893,7 @@ def run_ours(args, rank, world, local_rank):
             from oxideav_h266_b200.workloads import PictureData
 
             host.append((PictureData(*[x[1] for x in planes], p.bit_depth), planes, f))
-        e_steps = max(1, min(args.steps, 5))
+        e_steps = max(1, min(args.steps, 20))
         hps, hfs = [h[0] for h in host], [h[2] for h in host]
         call = ctx.batch_call(hps, hfs)  # the C argument structs, filled once as a caller would
         for _ in range(2):  # warm-up: lanes, worker pool, device buffers

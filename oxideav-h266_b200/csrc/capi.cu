@@ -1255,11 +1255,15 @@ int h266_ctx_synchronize(h266_ctx *ctx) {
   H266_TRY(check_ctx(ctx));
   Guard g(ctx->device);
   H266_CUDA(cudaStreamSynchronize(ctx->stream));
-  uint32_t timeouts = 0;
+  uint32_t timeouts = 0, db_timeouts = 0;
   H266_TRY(pass2_wait_timeouts(&timeouts));
+  H266_TRY(deblock_wait_timeouts(&db_timeouts));
   if (timeouts)
     return set_error(H266_ERR_TIMEOUT, std::to_string(timeouts) +
                                            " SAO/ALF tiles gave up waiting for their window copies (left unfiltered)");
+  if (db_timeouts)
+    return set_error(H266_ERR_TIMEOUT, std::to_string(db_timeouts) +
+                                           " deblocking tiles gave up waiting for their region copies (left unwritten)");
   return H266_OK;
 }
 

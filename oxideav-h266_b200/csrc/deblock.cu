@@ -23,6 +23,7 @@
 #include <numeric>
 
 #include "internal.h"
+#include "tma.cuh"
 
 namespace h266 {
 namespace {
@@ -1571,9 +1572,17 @@ struct TileParams {
   uint32_t grid_slots[2][3];
   const uint32_t *grid_count;       // cells per (tile, pass, plane), listed by the walk
   const uint32_t *grid_list[2][3];  // their grid indices, kTileListY / kTileListC per tile
+  // The regions staged by the TMA unit: one box per plane, kPitch wide and
+  // kRegion high, at the tile's origin less the halo (tma 0: vector loads).
+  int tma;
+  CUtensorMap tmap[3];
 };
 
-constexpr int kTileBands = 32;  // bands of one tile and pass that a plane can have (at most 24)
+constexpr int kTileBands = 32;
+
+// Tiles whose region copies did not complete within the poll limit (left
+// unwritten); read and cleared by deblock_wait_timeouts.
+__device__ unsigned int g_deblock_timeouts;  // bands of one tile and pass that a plane can have (at most 24)
 
 // Copies rows [oy, oy + wh) x columns [ox, ox + ww) of `src` (ox a multiple of
 // 8) to shared memory with row pitch `pitch`, mapping through `lut` if given.
@@ -1670,10 +1679,12 @@ __device__ __forceinline__ void tile_prefix(const TileParams &a, int d, int p, i
 __device__ __forceinline__ SharedView tile_view(const TileParams &a, uint16_t *sm, int p, int tx, int ty) {
   const DPlane &src = a.src[p];
   const int tp = p ? kDeblockTile / 2 : kDeblockTile, halo = p ? kDeblockHaloC : kDeblockHaloY;
-  uint16_t *base = p == 0 ? sm : sm + kRegionY * kPitchY + (p - 1) * kRegionC * kPitchC;
-  const int ox = max(tx * tp - halo, 0), oy = max(ty * tp - halo, 0);
+  const int pitch = p ? kPitchC : kPitchY;
+  uint16_t *box = p == 0 ? sm : sm + kRegionY * kPitchY + (p - 1) * kRegionC * kPitchC;
+  const int rx = tx * tp - halo, ry = ty * tp - halo;  // the box's origin, before clipping to the plane
+  const int ox = max(rx, 0), oy = max(ry, 0);
   const int ww = min(tx * tp + tp + halo, src.w) - ox, wh = min(ty * tp + tp + halo, src.h) - oy;
-  return SharedView{base, p ? kPitchC : kPitchY, ox, oy, max(ww, 0), max(wh, 0), src.w, src.h};
+  return SharedView{box + (oy - ry) * pitch + (ox - rx), pitch, ox, oy, max(ww, 0), max(wh, 0), src.w, src.h};
 }
 
 // The components of one pass of a tile, all three planes, spread over the
@@ -1729,20 +1740,38 @@ __device__ __forceinline__ void run_tile_pass(const TileParams &a, uint16_t *sm,
 struct TileShared {
   uint32_t list_y[2][kTileListY], list_c[2][2][kTileListC];
   uint32_t off[2][3][kTileBands + 1];  // [kTileBands]: list length
+  alignas(8) unsigned long long bar;   // completion of the TMA region copies
 };
 
 // Tile t of the picture whose parameters are `a`.
-__device__ __forceinline__ void deblock_tile(const TileParams &a, int t) {
-  extern __shared__ __align__(16) uint16_t sm[];
+__device__ __forceinline__ void deblock_tile(const TileParams &a, const TileParams *g, int t) {
+  extern __shared__ __align__(128) uint16_t sm_tile[];  // TMA destinations: 128-byte aligned
+  uint16_t *sm = sm_tile;
   __shared__ TileShared ts;
   auto &s_list_y = ts.list_y;
   auto &s_list_c = ts.list_c;
   auto &s_off = ts.off;
   const int tx = t % (int)a.tiles_x, ty = t / (int)a.tiles_x;
   const int warp = threadIdx.x >> 5;
-  // Warps 0-5 first build the component lists of both passes (one warp per
-  // pass and plane, from the host's ranges or the device walk's grids), then
-  // every thread loads the planes' regions.
+  // Thread 0 starts the TMA copies of the planes' regions; meanwhile warps
+  // 0-5 build the component lists of both passes (one warp per pass and
+  // plane, from the host's ranges or the device walk's grids).
+  if (a.tma && threadIdx.x == 0) {
+    tile_dev::mbar_init(&ts.bar, 1);
+    uint32_t bytes = 0;
+#pragma unroll
+    for (int p = 0; p < 3; ++p)
+      if (a.src[p].w > 0 && a.src[p].h > 0) bytes += (p ? kRegionC * kPitchC : kRegionY * kPitchY) * 2;
+    tile_dev::mbar_expect_tx(&ts.bar, bytes);
+#pragma unroll
+    for (int p = 0; p < 3; ++p) {
+      if (a.src[p].w <= 0 || a.src[p].h <= 0) continue;
+      const int tp = p ? kDeblockTile / 2 : kDeblockTile, halo = p ? kDeblockHaloC : kDeblockHaloY;
+      uint16_t *box = p == 0 ? sm : sm + kRegionY * kPitchY + (p - 1) * kRegionC * kPitchC;
+      tile_dev::tmap_acquire(&g->tmap[p]);
+      tile_dev::tma_load_2d(box, &g->tmap[p], tx * tp - halo, ty * tp - halo, &ts.bar);
+    }
+  }
   if (warp < 6) {
     const int d = warp / 3, p = warp % 3;
     if (a.grid_mode)
@@ -1752,12 +1781,32 @@ __device__ __forceinline__ void deblock_tile(const TileParams &a, int t) {
       tile_prefix(a, d, p, tx, ty, p == 0 ? s_list_y[d] : s_list_c[d][p - 1], p == 0 ? kTileListY : kTileListC,
                   s_off[d][p]);
   }
+  if (!a.tma) {
 #pragma unroll
-  for (int p = 0; p < 3; ++p) {
-    const SharedView v = tile_view(a, sm, p, tx, ty);
-    if (v.ww > 0 && v.wh > 0) load_window(v.s, v.ld, a.src[p], v.ox, v.oy, v.ww, v.wh, p == 0 ? a.lut : nullptr);
+    for (int p = 0; p < 3; ++p) {
+      const SharedView v = tile_view(a, sm, p, tx, ty);
+      if (v.ww > 0 && v.wh > 0) load_window(v.s, v.ld, a.src[p], v.ox, v.oy, v.ww, v.wh, p == 0 ? a.lut : nullptr);
+    }
+    __syncthreads();
+  } else {
+    __syncthreads();  // the barrier's initialisation and the lists
+    bool ok = tile_dev::mbar_wait_bounded(&ts.bar, 0);
+    if (ok && a.lut) {  // luma through the LMCS LUT, in place (the whole box: samples outside the plane are never read)
+      uint32_t *w = reinterpret_cast<uint32_t *>(sm);
+      for (int i = threadIdx.x; i < kRegionY * kPitchY / 2; i += blockDim.x) {
+        const uint32_t u = w[i];
+        w[i] = (uint32_t)a.lut[u & 0xFFFF] | (uint32_t)a.lut[u >> 16] << 16;
+      }
+    }
+    ok = __syncthreads_and(ok);
+    if (!ok) {  // the copies did not land in time: count it, let them finish (bounded), leave the tile
+      if (threadIdx.x == 0) {
+        atomicAdd(&g_deblock_timeouts, 1u);
+        tile_dev::mbar_wait_bounded(&ts.bar, 0);
+      }
+      return;
+    }
   }
-  __syncthreads();
 #pragma unroll
   for (int d = 0; d < 2; ++d) {
     run_tile_pass(a, sm, tx, ty, d, s_list_y[d], s_list_c[d][0], s_list_c[d][1], s_off[d][0][kTileBands],
@@ -1774,7 +1823,7 @@ __device__ __forceinline__ void deblock_tile(const TileParams &a, int t) {
 }
 
 __global__ void __launch_bounds__(kTileThreads, 4) k_deblock_tiles(const __grid_constant__ TileParams a) {
-  deblock_tile(a, blockIdx.x);
+  deblock_tile(a, &a, blockIdx.x);
 }
 
 // Many pictures in one grid: CTAs [first[i], first[i + 1]) are the tiles of
@@ -1793,7 +1842,7 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_deblock_tiles_batch(const T
   uint32_t *dst = reinterpret_cast<uint32_t *>(&s_params);
   for (int i = threadIdx.x; i < (int)(sizeof(TileParams) / 4); i += blockDim.x) dst[i] = src[i];
   __syncthreads();
-  deblock_tile(s_params, (int)(blockIdx.x - first[lo]));
+  deblock_tile(s_params, params + lo, (int)(blockIdx.x - first[lo]));
 }
 
 size_t rows_smem(const DPlane &p) { return (size_t)4 * row_pitch(p.w) * 2; }
@@ -1928,6 +1977,26 @@ int launch_deblock_strips_grid(cudaStream_t st, const DPlane src[3], const DPlan
 
 size_t deblock_tile_params_size() { return sizeof(TileParams); }
 
+int deblock_wait_timeouts(uint32_t *count) {
+  unsigned int v = 0, zero = 0;
+  H266_CUDA(cudaMemcpyFromSymbol(&v, g_deblock_timeouts, sizeof v));
+  if (v) H266_CUDA(cudaMemcpyToSymbol(g_deblock_timeouts, &zero, sizeof zero));
+  *count = v;
+  return H266_OK;
+}
+
+namespace {
+// The tensor maps of the tile kernel's region boxes (a.tma 0 when a plane
+// cannot be described: unaligned base or stride).
+void tile_tma_maps(TileParams &a) {
+  bool ok = true;
+  for (int p = 0; p < 3 && ok; ++p)
+    if (a.src[p].w > 0 && a.src[p].h > 0)
+      ok = encode_plane_map(&a.tmap[p], a.src[p], p ? kPitchC : kPitchY, p ? kRegionC : kRegionY);
+  a.tma = ok ? 1 : 0;
+}
+}  // namespace
+
 uint32_t fill_deblock_tile_params(void *out, const DPlane src[3], const DPlane dst[3], const uint16_t *lut,
                                   int bit_depth, const StripSide &v, const StripSide &h, const uint32_t *tile_bounds,
                                   const uint32_t tb_off[2][3], const uint32_t n_bands[2][3], uint32_t tiles_x,
@@ -1951,6 +2020,7 @@ uint32_t fill_deblock_tile_params(void *out, const DPlane src[3], const DPlane d
   a.tiles_x = tiles_x;
   a.tiles_y = tiles_y;
   a.maxv = (1 << bit_depth) - 1;
+  tile_tma_maps(a);
   std::memcpy(out, &a, sizeof a);
   return tiles_x * tiles_y;
 }
@@ -2551,6 +2621,7 @@ uint32_t fill_deblock_tile_params_grid(void *out, const DPlane src[3], const DPl
   a.tiles_x = g.tiles_x;
   a.tiles_y = g.tiles_y;
   a.maxv = (1 << bit_depth) - 1;
+  tile_tma_maps(a);
   std::memcpy(out, &a, sizeof a);
   return g.tiles_x * g.tiles_y;
 }
@@ -2575,6 +2646,7 @@ int launch_deblock_tiles_grid(cudaStream_t st, const DPlane src[3], const DPlane
   a.tiles_x = g.tiles_x;
   a.tiles_y = g.tiles_y;
   a.maxv = (1 << bit_depth) - 1;
+  tile_tma_maps(a);
   const uint64_t n = (uint64_t)g.tiles_x * g.tiles_y;
   if (!n) return H266_OK;
   k_deblock_tiles<<<(unsigned)n, kTileThreads, kTileSmem, st>>>(a);

@@ -330,6 +330,12 @@ int launch_pass2(cudaStream_t st, const Pass2Args &a, bool do_sao, bool do_alf, 
 // bases 16-byte aligned, strides multiples of 8 samples; otherwise a.tma = 0
 // and the kernel loads its windows itself).  Host only, allocates nothing.
 void pass2_tma_maps(Pass2Args &a);
+// A 2-D tensor map of plane p with a box_w x box_h box (u16 samples, zero
+// fill outside the plane); false when the plane's base or stride is not
+// 16-byte aligned or the driver entry point is missing.
+bool encode_plane_map(CUtensorMap *m, const DPlane &p, int box_w, int box_h);
+// Deblocking tiles whose region copies timed out since the last call (read and cleared).
+int deblock_wait_timeouts(uint32_t *count);
 // Timeouts of the tile kernels' bounded waits since the last call (the
 // kernels leave such a tile unfiltered and count it): 0 when none.
 int pass2_wait_timeouts(uint32_t *count);

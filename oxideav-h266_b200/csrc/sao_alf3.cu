@@ -29,6 +29,7 @@
 #include <utility>
 
 #include "alf_tile.cuh"
+#include "tma.cuh"
 
 namespace h266 {
 namespace {
@@ -69,59 +70,8 @@ struct Smem3 {
   __device__ uint4 *cell() { return reinterpret_cast<uint4 *>(u); }
 };
 
-// ---------------------------------------------------------------- TMA and mbarrier (PTX)
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(unsigned long long *bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-
-// 2-D tiled tensor load of the box at (x, y) (elements) into shared memory,
-// completing on `bar`.  x * 2 bytes is a multiple of 16 at every call site.
-__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, unsigned long long *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-          smem_u32(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
-      : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, uint32_t phase) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(phase)
-      : "memory");
-  return ok != 0;
-}
-
-__device__ __forceinline__ uint64_t global_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Polls the barrier's phase `phase` for at most kWaitNs.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, uint32_t phase) {
-  if (mbar_try_wait(bar, phase)) return true;
-  const uint64_t t0 = global_ns();
-  for (;;) {
-    if (mbar_try_wait(bar, phase)) return true;
-    if (global_ns() - t0 > kWaitNs) return false;
-  }
-}
-
-// A tensor map written to global memory before the launch, made visible to
-// the tensor-map proxy.
-__device__ __forceinline__ void tmap_acquire(const CUtensorMap *m) {
-  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(m) : "memory");
-}
+// TMA and mbarrier helpers (tma.cuh); waits give up after kWaitNs.
+using namespace tile_dev;
 
 // f(integral_constant<int, 0>) ... f(integral_constant<int, N - 1>): indices as constants
 template <class F, int... I>
@@ -442,11 +392,11 @@ __device__ __forceinline__ bool sao_alf_tile3(const Pass2Args &a, const Pass2Arg
     }
   }
   if (tma) {
-    bool ok = mbar_wait_bounded(&sm.bar, phase);
+    bool ok = mbar_wait_bounded(&sm.bar, phase, kWaitNs);
     ok = __syncthreads_and(ok);
     if (!ok) {  // the copies did not land: count the tile, let them finish (bounded), leave it unfiltered
       if (tid == 0) atomicAdd(&g_wait_timeouts, 1u);
-      mbar_wait_bounded(&sm.bar, phase);
+      mbar_wait_bounded(&sm.bar, phase, kWaitNs);
       return false;
     }
     phase ^= 1u;
@@ -884,6 +834,12 @@ bool encode_plane(CUtensorMap *m, const DPlane &p, int box_w, int box_h) {
              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
+
+}  // namespace
+
+bool encode_plane_map(CUtensorMap *m, const DPlane &p, int box_w, int box_h) { return encode_plane(m, p, box_w, box_h); }
+
+namespace {
 
 template <int W, int TH>
 void maps_for(Pass2Args &a) {
