@@ -18,6 +18,7 @@
 // Device side: one thread per component replays its segments with the
 // reference's clamped reads and bounds-checked Clip1 writes on global memory.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <memory>
 #include <numeric>
@@ -487,7 +488,7 @@ void index_tiles(const h266_picture &pic, uint32_t cfi, DeblockPlan &plan) {
   const int tiles_x = (int)plan.tiles_x, tiles_y = (int)plan.tiles_y;
   std::vector<uint32_t> &tb = plan.tile_bounds;
   tb.clear();
-  // per tile and pass: listed components per plane, checked against the shared lists
+  // per tile and pass: staged segments per plane, checked against the shared lists
   thread_local std::vector<uint32_t> load;
   load.assign((size_t)tiles_x * tiles_y * 3, 0);
   for (int d = 0; d < 2; ++d) {
@@ -531,8 +532,9 @@ void index_tiles(const h266_picture &pic, uint32_t cfi, DeblockPlan &plan) {
           while (hi < c1 && fs[hi - c0] < t1) ++hi;
           tb[base + ((size_t)b * n_t + t) * 2] = lo;
           tb[base + ((size_t)b * n_t + t) * 2 + 1] = hi;
-          // count the entries of the tiles that take this band's range
-          const uint32_t n = hi - lo;
+          // count the segments of the tiles that take this band's range (the
+          // tile kernel stages them in shared lists of kTileListY / kTileListC)
+          const uint32_t n = comp[hi] - comp[lo];
           if (!n) continue;
           if (d == 0) {
             const int band = (int)b * unit;
@@ -1625,23 +1627,69 @@ __device__ __forceinline__ void store_window(const uint16_t *sm, int pitch, cons
 
 // Band counts and prefix sums of the tile's component ranges for (pass d,
 // plane p), by one warp.
-// Grid mode: the list of (pass d, plane p) of tile t, copied from the one
-// the device walk built; s_off[kTileBands] receives the count.
-__device__ __forceinline__ void tile_grid_list(const TileParams &a, int d, int p, int t, uint32_t *list, uint32_t cap,
-                                               uint32_t *s_off) {
-  const int lane = threadIdx.x & 31;
-  const uint32_t n = min(a.grid_count[(size_t)t * 6 + d * 3 + p], cap);
-  const uint32_t *src = a.grid_list[d][p] + (size_t)t * cap;
-  for (uint32_t i = lane; i < n; i += 32) list[i] = src[i];
-  if (lane == 0) s_off[kTileBands] = n;
+// The staged window of plane p of tile (tx, ty): the tile widened by the
+// halo, clipped to the plane.  Recomputed where needed rather than kept live.
+__device__ __forceinline__ SharedView tile_view(const TileParams &a, uint16_t *sm, int p, int tx, int ty) {
+  const DPlane &src = a.src[p];
+  const int tp = p ? kDeblockTile / 2 : kDeblockTile, halo = p ? kDeblockHaloC : kDeblockHaloY;
+  const int pitch = p ? kPitchC : kPitchY;
+  uint16_t *box = p == 0 ? sm : sm + kRegionY * kPitchY + (p - 1) * kRegionC * kPitchC;
+  const int rx = tx * tp - halo, ry = ty * tp - halo;  // the box's origin, before clipping to the plane
+  const int ox = max(rx, 0), oy = max(ry, 0);
+  const int ww = min(tx * tp + tp + halo, src.w) - ox, wh = min(ty * tp + tp + halo, src.h) - oy;
+  return SharedView{box + (oy - ry) * pitch + (ox - rx), pitch, ox, oy, max(ww, 0), max(wh, 0), src.w, src.h};
 }
 
-// Host-built lists: the tile's component ranges of (pass d, plane p), one
-// band per lane, written out as the tile's list of component indices (each
-// lane its band's range at the band's prefix offset); s_off[kTileBands]
-// receives the count.  The host keeps every tile's count within `cap`.
-__device__ __forceinline__ void tile_prefix(const TileParams &a, int d, int p, int tx, int ty, uint32_t *list,
-                                            uint32_t cap, uint32_t *s_off /* kTileBands + 1 */) {
+// An EdgeSeg moved as three 32-bit words (every array of them here starts on
+// a 4-byte boundary: blob sections, grid cells and shared arrays).
+union SegWords {
+  EdgeSeg e;
+  uint32_t w[3];
+};
+__device__ __forceinline__ EdgeSeg seg_get(const EdgeSeg *p) {
+  const uint32_t *w = reinterpret_cast<const uint32_t *>(p);
+  SegWords u;
+  u.w[0] = w[0];
+  u.w[1] = w[1];
+  u.w[2] = w[2];
+  return u.e;
+}
+__device__ __forceinline__ void seg_copy(EdgeSeg *dst, const EdgeSeg *src) {
+  const uint32_t *s = reinterpret_cast<const uint32_t *>(src);
+  uint32_t *d = reinterpret_cast<uint32_t *>(dst);
+  const uint32_t a = s[0], b = s[1], c = s[2];
+  d[0] = a;
+  d[1] = b;
+  d[2] = c;
+}
+
+// The tile's components of one (pass, plane), staged in shared memory before
+// the filters run: their segments one component after another and each
+// component's first segment (start[n] ends the last one), so the filter
+// phase reads no global memory.
+struct TileStage {
+  EdgeSeg *seg;
+  uint16_t *start;
+  uint32_t cap;
+};
+
+// The largest b in [0, 31] with prefix[b] <= x (prefix non-decreasing,
+// prefix[0] = 0): the band holding entry x.
+__device__ __forceinline__ int band_of(const uint32_t *prefix, uint32_t x) {
+  int b = 0;
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1)
+    if (prefix[b + s] <= x) b += s;
+  return b;
+}
+
+// Host-built lists, by one warp: lane b reads the component range of band
+// b0 + b of the tile, the prefix sums over the lanes give each band's first
+// component and segment in the staged arrays, then the warp stages every
+// component start and segment.  `band` is the warp's scratch (4 x 33).  The
+// host keeps every tile's segment count within the caps.
+__device__ __forceinline__ uint32_t stage_host(const TileParams &a, int d, int p, int tx, int ty, const TileStage &st,
+                                               uint32_t (*band)[kTileBands + 1]) {
   const int lane = threadIdx.x & 31;
   const int tp = p ? kDeblockTile / 2 : kDeblockTile, halo = p ? kDeblockHaloC : kDeblockHaloY, unit = p ? 2 : 4;
   const int nb = (int)a.n_bands[d][p];
@@ -1657,129 +1705,158 @@ __device__ __forceinline__ void tile_prefix(const TileParams &a, int d, int p, i
     n_t = (int)a.tiles_y;
     t = ty;
   }
+  const uint32_t *comp = a.comp[d];
   const int b = b0 + lane;
-  uint32_t lo = 0, cnt = 0;
+  uint32_t lo = 0, cnt = 0, s0 = 0, ns = 0;
   if (b < b1) {
     const uint32_t *e = a.bounds + a.tb_off[d][p] + ((size_t)b * n_t + t) * 2;
     lo = e[0];
     cnt = e[1] - e[0];
+    if (cnt) {
+      s0 = comp[lo];
+      ns = comp[lo + cnt] - s0;
+    }
   }
-  uint32_t incl = cnt;
+  uint32_t ic = cnt, is = ns;  // inclusive prefix sums over the lanes
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-    if (lane >= o) incl += y;
+    const uint32_t yc = __shfl_up_sync(0xFFFFFFFFu, ic, o), ys = __shfl_up_sync(0xFFFFFFFFu, is, o);
+    if (lane >= o) {
+      ic += yc;
+      is += ys;
+    }
   }
-  for (uint32_t k = 0, o = incl - cnt; k < cnt && o + k < cap; ++k) list[o + k] = lo + k;
-  if (lane == 31) s_off[kTileBands] = min(incl, cap);
+  band[0][lane] = ic - cnt;
+  band[1][lane] = is - ns;
+  band[2][lane] = lo;
+  band[3][lane] = s0;
+  const uint32_t nc = min(__shfl_sync(0xFFFFFFFFu, ic, 31), st.cap), nseg = min(__shfl_sync(0xFFFFFFFFu, is, 31), st.cap);
+  __syncwarp();
+  for (uint32_t j = lane; j < nc; j += 32) {
+    const int k = band_of(band[0], j);
+    const uint32_t c = band[2][k] + j - band[0][k];
+    st.start[j] = (uint16_t)min(band[1][k] + comp[c] - band[3][k], nseg);
+  }
+  if (lane == 0) st.start[nc] = (uint16_t)nseg;
+  const EdgeSeg *segs = a.segs[d];
+  for (uint32_t i = lane; i < nseg; i += 32) {
+    const int k = band_of(band[1], i);
+    seg_copy(st.seg + i, segs + band[3][k] + i - band[1][k]);
+  }
+  return nc;
 }
 
-// The staged window of plane p of tile (tx, ty): the tile widened by the
-// halo, clipped to the plane.  Recomputed where needed rather than kept live.
-__device__ __forceinline__ SharedView tile_view(const TileParams &a, uint16_t *sm, int p, int tx, int ty) {
-  const DPlane &src = a.src[p];
-  const int tp = p ? kDeblockTile / 2 : kDeblockTile, halo = p ? kDeblockHaloC : kDeblockHaloY;
-  const int pitch = p ? kPitchC : kPitchY;
-  uint16_t *box = p == 0 ? sm : sm + kRegionY * kPitchY + (p - 1) * kRegionC * kPitchC;
-  const int rx = tx * tp - halo, ry = ty * tp - halo;  // the box's origin, before clipping to the plane
-  const int ox = max(rx, 0), oy = max(ry, 0);
-  const int ww = min(tx * tp + tp + halo, src.w) - ox, wh = min(ty * tp + tp + halo, src.h) - oy;
-  return SharedView{box + (oy - ry) * pitch + (ox - rx), pitch, ox, oy, max(ww, 0), max(wh, 0), src.w, src.h};
+// Grid mode, by one warp: the cells the device walk listed for (pass d,
+// plane p) of tile t, each its own component.
+__device__ __forceinline__ uint32_t stage_grid(const TileParams &a, int d, int p, int t, const TileStage &st) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t n = min(a.grid_count[(size_t)t * 6 + d * 3 + p], st.cap);
+  const uint32_t *src = a.grid_list[d][p] + (size_t)t * st.cap;
+  const EdgeSeg *g = a.grid[d][p];
+  for (uint32_t j = lane; j < n; j += 32) {
+    seg_copy(st.seg + j, g + src[j]);
+    st.start[j] = (uint16_t)j;
+  }
+  if (lane == 0) st.start[n] = (uint16_t)n;
+  return n;
 }
+
+struct TileShared {
+  alignas(16) EdgeSeg seg_y[2][kTileListY];
+  alignas(16) EdgeSeg seg_c[2][2][kTileListC];
+  uint16_t start_y[2][kTileListY + 1], start_c[2][2][kTileListC + 1];
+  uint32_t band[6][4][kTileBands + 1];  // stage_host scratch per (pass, plane)
+  uint32_t n_comp[2][3];
+  uint32_t task[2];                   // the passes' next warp task
+  alignas(8) unsigned long long bar;  // completion of the TMA region copies
+  __device__ TileStage stage(int d, int p) {
+    return p == 0 ? TileStage{seg_y[d], start_y[d], (uint32_t)kTileListY}
+                  : TileStage{seg_c[d][p - 1], start_c[d][p - 1], (uint32_t)kTileListC};
+  }
+};
 
 // The components of one pass of a tile, all three planes, spread over the
 // CTA's warps: a warp task is 8 luma components (groups of 4 lanes) or 16
-// chroma components (groups of 2), so no plane waits for another.
-__device__ __forceinline__ void run_tile_pass(const TileParams &a, uint16_t *sm, int tx, int ty, int d,
-                                              const uint32_t *list0, const uint32_t *list1, const uint32_t *list2,
-                                              uint32_t n0, uint32_t n1, uint32_t n2) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, n_warps = blockDim.x >> 5;
-  const EdgeSeg *segs = a.segs[d];
-  const uint32_t *comp = a.comp[d];
+// chroma components (groups of 2), so no plane waits for another; warps take
+// tasks from a shared counter, so a warp with long components does not hold
+// the others at the pass's barrier.
+__device__ __forceinline__ void run_tile_pass(const TileParams &a, uint16_t *sm, TileShared &ts, int tx, int ty,
+                                              int d) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t n0 = ts.n_comp[d][0], n1 = ts.n_comp[d][1], n2 = ts.n_comp[d][2];
   const uint32_t tasks0 = (n0 + 7) / 8, tasks1 = (n1 + 15) / 16, tasks2 = (n2 + 15) / 16;
   const uint32_t total = tasks0 + tasks1 + tasks2;
-  for (uint32_t t = warp; t < total; t += n_warps) {
+  for (;;) {
+    uint32_t t = 0;
+    if (lane == 0) t = atomicAdd(&ts.task[d], 1u);
+    t = __shfl_sync(0xFFFFFFFFu, t, 0);
+    if (t >= total) break;
     if (t < tasks0) {
       const int k = lane & 3, base = lane - k;
       const unsigned mask = 0xFu << base;
       const uint32_t j = t * 8 + (lane >> 2);
       if (j < n0) {
         const SharedView v = tile_view(a, sm, 0, tx, ty);
-        if (a.grid_mode) {
-          segment_group<4, kPitchY>(v, a.grid[d][0][list0[j]], a.maxv, k, base, mask);
-        } else {
-          const uint32_t c = list0[j], e = comp[c + 1];
-          for (uint32_t i = comp[c]; i < e; ++i) {
-            segment_group<4, kPitchY>(v, segs[i], a.maxv, k, base, mask);
-            __syncwarp(mask);
-          }
+        const uint32_t e = ts.start_y[d][j + 1];
+        for (uint32_t i = ts.start_y[d][j]; i < e; ++i) {
+          segment_group<4, kPitchY>(v, seg_get(&ts.seg_y[d][i]), a.maxv, k, base, mask);
+          __syncwarp(mask);
         }
       }
     } else {
       const bool cr = t >= tasks0 + tasks1;
+      const int c = cr ? 1 : 0;
       const uint32_t tt = t - tasks0 - (cr ? tasks1 : 0);
       const int k = lane & 1, base = lane - k;
       const unsigned mask = 0x3u << base;
       const uint32_t j = tt * 16 + (lane >> 1);
       if (j < (cr ? n2 : n1)) {
         const SharedView v = tile_view(a, sm, cr ? 2 : 1, tx, ty);
-        if (a.grid_mode) {
-          segment_group<2, kPitchC>(v, a.grid[d][cr ? 2 : 1][(cr ? list2 : list1)[j]], a.maxv, k, base, mask);
-        } else {
-          const uint32_t c = (cr ? list2 : list1)[j], e = comp[c + 1];
-          for (uint32_t i = comp[c]; i < e; ++i) {
-            segment_group<2, kPitchC>(v, segs[i], a.maxv, k, base, mask);
-            __syncwarp(mask);
-          }
+        const uint32_t e = ts.start_c[d][c][j + 1];
+        for (uint32_t i = ts.start_c[d][c][j]; i < e; ++i) {
+          segment_group<2, kPitchC>(v, seg_get(&ts.seg_c[d][c][i]), a.maxv, k, base, mask);
+          __syncwarp(mask);
         }
       }
     }
   }
 }
 
-struct TileShared {
-  uint32_t list_y[2][kTileListY], list_c[2][2][kTileListC];
-  uint32_t off[2][3][kTileBands + 1];  // [kTileBands]: list length
-  alignas(8) unsigned long long bar;   // completion of the TMA region copies
-};
-
-// Tile t of the picture whose parameters are `a`.
+// Tile t of the picture whose parameters are `a` (`g`: the same parameters in
+// global or parameter memory, for the tensor maps).
 __device__ __forceinline__ void deblock_tile(const TileParams &a, const TileParams *g, int t) {
   extern __shared__ __align__(128) uint16_t sm_tile[];  // TMA destinations: 128-byte aligned
   uint16_t *sm = sm_tile;
   __shared__ TileShared ts;
-  auto &s_list_y = ts.list_y;
-  auto &s_list_c = ts.list_c;
-  auto &s_off = ts.off;
   const int tx = t % (int)a.tiles_x, ty = t / (int)a.tiles_x;
   const int warp = threadIdx.x >> 5;
   // Thread 0 starts the TMA copies of the planes' regions; meanwhile warps
-  // 0-5 build the component lists of both passes (one warp per pass and
-  // plane, from the host's ranges or the device walk's grids).
-  if (a.tma && threadIdx.x == 0) {
-    tile_dev::mbar_init(&ts.bar, 1);
-    uint32_t bytes = 0;
+  // 0-5 stage the components of both passes (one warp per pass and plane,
+  // from the host's ranges or the device walk's lists).
+  if (threadIdx.x == 0) {
+    ts.task[0] = ts.task[1] = 0;
+    if (a.tma) {
+      tile_dev::mbar_init(&ts.bar, 1);
+      uint32_t bytes = 0;
 #pragma unroll
-    for (int p = 0; p < 3; ++p)
-      if (a.src[p].w > 0 && a.src[p].h > 0) bytes += (p ? kRegionC * kPitchC : kRegionY * kPitchY) * 2;
-    tile_dev::mbar_expect_tx(&ts.bar, bytes);
+      for (int p = 0; p < 3; ++p)
+        if (a.src[p].w > 0 && a.src[p].h > 0) bytes += (p ? kRegionC * kPitchC : kRegionY * kPitchY) * 2;
+      tile_dev::mbar_expect_tx(&ts.bar, bytes);
 #pragma unroll
-    for (int p = 0; p < 3; ++p) {
-      if (a.src[p].w <= 0 || a.src[p].h <= 0) continue;
-      const int tp = p ? kDeblockTile / 2 : kDeblockTile, halo = p ? kDeblockHaloC : kDeblockHaloY;
-      uint16_t *box = p == 0 ? sm : sm + kRegionY * kPitchY + (p - 1) * kRegionC * kPitchC;
-      tile_dev::tmap_acquire(&g->tmap[p]);
-      tile_dev::tma_load_2d(box, &g->tmap[p], tx * tp - halo, ty * tp - halo, &ts.bar);
+      for (int p = 0; p < 3; ++p) {
+        if (a.src[p].w <= 0 || a.src[p].h <= 0) continue;
+        const int tp = p ? kDeblockTile / 2 : kDeblockTile, halo = p ? kDeblockHaloC : kDeblockHaloY;
+        uint16_t *box = p == 0 ? sm : sm + kRegionY * kPitchY + (p - 1) * kRegionC * kPitchC;
+        tile_dev::tmap_acquire(&g->tmap[p]);
+        tile_dev::tma_load_2d(box, &g->tmap[p], tx * tp - halo, ty * tp - halo, &ts.bar);
+      }
     }
   }
   if (warp < 6) {
     const int d = warp / 3, p = warp % 3;
-    if (a.grid_mode)
-      tile_grid_list(a, d, p, t, p == 0 ? s_list_y[d] : s_list_c[d][p - 1], p == 0 ? kTileListY : kTileListC,
-                     s_off[d][p]);
-    else
-      tile_prefix(a, d, p, tx, ty, p == 0 ? s_list_y[d] : s_list_c[d][p - 1], p == 0 ? kTileListY : kTileListC,
-                  s_off[d][p]);
+    const uint32_t n = a.grid_mode ? stage_grid(a, d, p, t, ts.stage(d, p))
+                                   : stage_host(a, d, p, tx, ty, ts.stage(d, p), ts.band[warp]);
+    if ((threadIdx.x & 31) == 0) ts.n_comp[d][p] = n;
   }
   if (!a.tma) {
 #pragma unroll
@@ -1789,7 +1866,7 @@ __device__ __forceinline__ void deblock_tile(const TileParams &a, const TilePara
     }
     __syncthreads();
   } else {
-    __syncthreads();  // the barrier's initialisation and the lists
+    __syncthreads();  // the barrier's initialisation and the staged components
     bool ok = tile_dev::mbar_wait_bounded(&ts.bar, 0);
     if (ok && a.lut) {  // luma through the LMCS LUT, in place (the whole box: samples outside the plane are never read)
       uint32_t *w = reinterpret_cast<uint32_t *>(sm);
@@ -1809,8 +1886,7 @@ __device__ __forceinline__ void deblock_tile(const TileParams &a, const TilePara
   }
 #pragma unroll
   for (int d = 0; d < 2; ++d) {
-    run_tile_pass(a, sm, tx, ty, d, s_list_y[d], s_list_c[d][0], s_list_c[d][1], s_off[d][0][kTileBands],
-                  s_off[d][1][kTileBands], s_off[d][2][kTileBands]);
+    run_tile_pass(a, sm, ts, tx, ty, d);
     __syncthreads();
   }
 #pragma unroll
@@ -1977,6 +2053,24 @@ int launch_deblock_strips_grid(cudaStream_t st, const DPlane src[3], const DPlan
 
 size_t deblock_tile_params_size() { return sizeof(TileParams); }
 
+namespace {
+// The tile kernels' shared memory (staged components, parameters and the
+// regions, above the 48 KB default) and a full carveout, once per device.
+int prepare_tile_kernels() {
+  static std::atomic<uint64_t> done{0};
+  int dev = 0;
+  H266_CUDA(cudaGetDevice(&dev));
+  const uint64_t bit = 1ull << (dev & 63);
+  if (done.load(std::memory_order_relaxed) & bit) return H266_OK;
+  for (const void *k : {reinterpret_cast<const void *>(k_deblock_tiles), reinterpret_cast<const void *>(k_deblock_tiles_batch)}) {
+    H266_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem));
+    H266_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  }
+  done.fetch_or(bit);
+  return H266_OK;
+}
+}  // namespace
+
 int deblock_wait_timeouts(uint32_t *count) {
   unsigned int v = 0, zero = 0;
   H266_CUDA(cudaMemcpyFromSymbol(&v, g_deblock_timeouts, sizeof v));
@@ -2033,6 +2127,7 @@ int launch_deblock_tiles(cudaStream_t st, const DPlane src[3], const DPlane dst[
   const uint32_t n = fill_deblock_tile_params(&a, src, dst, lut, bit_depth, v, h, tile_bounds, tb_off, n_bands,
                                               tiles_x, tiles_y);
   if (!n) return H266_OK;
+  H266_TRY(prepare_tile_kernels());
   k_deblock_tiles<<<n, kTileThreads, kTileSmem, st>>>(a);
   H266_CUDA(cudaGetLastError());
   ++*launches;
@@ -2042,6 +2137,7 @@ int launch_deblock_tiles(cudaStream_t st, const DPlane src[3], const DPlane dst[
 int launch_deblock_tiles_batch(cudaStream_t st, const void *d_params, const uint32_t *d_first, int n, uint32_t ctas,
                                uint64_t *launches) {
   if (!ctas || n <= 0) return H266_OK;
+  H266_TRY(prepare_tile_kernels());
   k_deblock_tiles_batch<<<ctas, kTileThreads, kTileSmem, st>>>(static_cast<const TileParams *>(d_params), d_first, n);
   H266_CUDA(cudaGetLastError());
   ++*launches;
@@ -2649,6 +2745,7 @@ int launch_deblock_tiles_grid(cudaStream_t st, const DPlane src[3], const DPlane
   tile_tma_maps(a);
   const uint64_t n = (uint64_t)g.tiles_x * g.tiles_y;
   if (!n) return H266_OK;
+  H266_TRY(prepare_tile_kernels());
   k_deblock_tiles<<<(unsigned)n, kTileThreads, kTileSmem, st>>>(a);
   H266_CUDA(cudaGetLastError());
   ++*launches;
