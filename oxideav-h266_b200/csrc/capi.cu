@@ -971,7 +971,9 @@ int prepare_chain(Prep &pr, const h266_picture &pic, const h266_in_loop_filter_a
       for (uint64_t i = 0; i < counts[l]; ++i) {
         const h266_deblock_cu &c = lists[l][i];
         std::memcpy(heads + i * kCuHeadBytes, &c, kCuHeadBytes);
-        w.max_cu_dim = std::max(w.max_cu_dim, std::max(c.w, c.h));
+        // only sub-block grids, TB splits and 64-sample TU tiling put edges inside a CU
+        if (c.has_num_sb || c.has_tb_split || (c.has_tu64 && std::max(c.w, c.h) > 64))
+          w.max_cu_dim = std::max(w.max_cu_dim, std::max(c.w, c.h));
         if (c.has_tu64 || c.has_tb_split) {
           CuTail t;
           t.index = (uint32_t)i;

@@ -226,7 +226,8 @@ struct DeviceWalkIn {  // device pointers
   h266_deblock_params params;
   uint32_t cfi;
   int w, h, cw, ch;      // luma and chroma plane sizes
-  uint32_t max_cu_dim;   // largest CU width or height of both lists
+  uint32_t max_cu_dim;   // largest width or height of the CUs with edges inside them (4: none);
+                         // the walk launches offsets 0 .. max_cu_dim - 4 (step 4)
   bool tile_lists;       // also list each tile's cells for the grid-mode tile kernel
 };
 size_t device_walk_bytes(const DeviceWalkIn &in);  // scratch for the CU maps and segment grids
