@@ -942,6 +942,7 @@ int prepare_chain(Prep &pr, const h266_picture &pic, const h266_in_loop_filter_a
     db.device_walk = true;
     db.dw_tiles = mode == 1 && (pr.h.do_sao || pr.h.do_alf);
     db.dw.tile_lists = mode == 1;  // the walk lists each tile's cells (within the lists' caps in mode 1)
+    db.dw.tiles_consume = db.dw_tiles;
     db.dw_sep = a.chroma_cus != nullptr;
     db.dw_mv = a.mv_grid && a.mv_grid->cells && a.mv_grid->cells_w * a.mv_grid->cells_h;
     DeviceWalkIn &w = db.dw;

@@ -2360,10 +2360,13 @@ __host__ __device__ inline uint32_t unpack_items(const WalkParams &a, int list) 
   return a.n[list] + a.n_tails[list] + (list == 0 ? a.n_mv_recs : 0);
 }
 
-// Item i of list `list`: a CU head is copied into the CU's full record (whose
-// tail the clearing left zero) and the CU enters the CU map (CuGrid::build:
+// Item i of list `list`: a CU head is copied into the CU's full record (the
+// tail of a CU without TU map and TB split is never read, nor the motion of
+// an intra CU) and the CU enters the CU map (CuGrid::build:
 // cell -> CU covering it, the later CU winning, here the larger index); a
-// tail or a motion record is copied into its CU's full record.
+// tail or a motion record is copied into its CU's full record.  (The
+// pictures the device walk takes have no overlapping CUs, so each cell is
+// written by one CU: the crate's last-CU-wins rule needs no atomics.)
 __device__ __forceinline__ void unpack_item(const WalkParams &a, int list, uint32_t i) {
   if (i < a.n[list]) {
     const uint64_t *src = reinterpret_cast<const uint64_t *>(a.heads[list] + (size_t)i * kCuHeadBytes);
@@ -2377,7 +2380,7 @@ __device__ __forceinline__ void unpack_item(const WalkParams &a, int list, uint3
     const int x0 = cx / 4, y0 = cy / 4;
     const int x1 = min((int)((cx + cw + 3) / 4), a.cw4), y1 = min((int)((cy + ch + 3) / 4), a.ch4);
     for (int y = y0; y < y1; ++y)
-      for (int x = x0; x < x1; ++x) atomicMax(&a.cu_grid[list][(size_t)y * a.cw4 + x], (int32_t)i);
+      for (int x = x0; x < x1; ++x) a.cu_grid[list][(size_t)y * a.cw4 + x] = (int32_t)i;  // CUs never overlap here
     return;
   }
   i -= a.n[list];
@@ -2434,6 +2437,9 @@ struct WalkLayout {
 };
 
 WalkLayout walk_layout(const DeviceWalkIn &in) {
+  // [CU maps: set to -1][tile counts: 0][segment grids: 0 when the strip
+  // kernels scan them][full CU records, motion, tile lists: written before
+  // they are read, not cleared]
   WalkLayout L{};
   const size_t cells = (size_t)((in.w + 3) / 4) * ((in.h + 3) / 4);
   size_t off = 0;
@@ -2443,12 +2449,12 @@ WalkLayout walk_layout(const DeviceWalkIn &in) {
   }
   if (!in.sep) L.cu_grid[1] = L.cu_grid[0];
   L.zero_from = off;
-  L.full[0] = off;
-  off += align_up((size_t)in.n_cus * sizeof(h266_deblock_cu));
-  L.full[1] = in.sep ? off : L.full[0];
-  if (in.sep) off += align_up((size_t)in.n_chroma * sizeof(h266_deblock_cu));
-  L.mv_full = off;
-  if (in.mv_by_cu) off += align_up((size_t)in.n_cus * sizeof(h266_deblock_mv_cell));
+  const size_t tiles = in.tile_lists ? (size_t)((in.w + kDeblockTile - 1) / kDeblockTile) *
+                                           ((in.h + kDeblockTile - 1) / kDeblockTile)
+                                     : 0;
+  L.tile_count = off;
+  off += align_up(tiles * 6 * sizeof(uint32_t));
+  L.zero_end = off;
   for (int d = 0; d < 2; ++d)
     for (int p = 0; p < 3; ++p) {
       const bool has = p == 0 || in.cfi != 0;
@@ -2459,14 +2465,17 @@ WalkLayout walk_layout(const DeviceWalkIn &in) {
       L.grid[d][p] = off;
       off += align_up((size_t)L.bands[d][p] * L.slots[d][p] * sizeof(EdgeSeg));
     }
-  const size_t tiles = in.tile_lists ? (size_t)((in.w + kDeblockTile - 1) / kDeblockTile) *
-                                           ((in.h + kDeblockTile - 1) / kDeblockTile)
-                                     : 0;
-  L.tile_count = off;
-  off += align_up(tiles * 6 * sizeof(uint32_t));
-  L.zero_end = off;
+  // The tile kernel reads only the cells the walk listed (and wrote); the
+  // strip kernels scan every cell, so for them empty cells must read bS 0.
+  if (!in.tiles_consume) L.zero_end = off;
+  L.full[0] = off;
+  off += align_up((size_t)in.n_cus * sizeof(h266_deblock_cu));
+  L.full[1] = in.sep ? off : L.full[0];
+  if (in.sep) off += align_up((size_t)in.n_chroma * sizeof(h266_deblock_cu));
+  L.mv_full = off;
+  if (in.mv_by_cu) off += align_up((size_t)in.n_cus * sizeof(h266_deblock_mv_cell));
   for (int d = 0; d < 2; ++d)
-    for (int p = 0; p < 3; ++p) {  // list entries are written before they are read: not cleared
+    for (int p = 0; p < 3; ++p) {
       L.tile_list[d][p] = off;
       off += align_up(tiles * (p ? kTileListC : kTileListY) * sizeof(uint32_t));
     }

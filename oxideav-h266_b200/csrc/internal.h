@@ -229,6 +229,7 @@ struct DeviceWalkIn {  // device pointers
   uint32_t max_cu_dim;   // largest width or height of the CUs with edges inside them (4: none);
                          // the walk launches offsets 0 .. max_cu_dim - 4 (step 4)
   bool tile_lists;       // also list each tile's cells for the grid-mode tile kernel
+  bool tiles_consume;    // the tile kernel (not the strip kernels) reads the grids: empty cells need no clearing
 };
 size_t device_walk_bytes(const DeviceWalkIn &in);  // scratch for the CU maps and segment grids
 struct DeviceWalkOut {
