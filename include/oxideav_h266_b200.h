@@ -518,15 +518,23 @@ int h266_chain_plan_execute(h266_ctx *ctx, h266_chain_plan *plan, h266_picture *
  * the device first (the CU map and edge walk of apply_deblocking_clipped,
  * src/deblock.rs:630-983, the work the crate does on every call), batched
  * over the pictures of h266_chain_plan_execute_batch.  Pictures the device
- * walk does not cover (4-sample CUs or transform blocks, sub-block grids,
- * overlapping CUs, 4:2:2 / 4:4:4, no SAO / ALF) keep host-derived segments,
- * as without the flag. */
+ * walk does not take (h266_sideinfo_mode 0: CUs off the 4x4 grid, outside the
+ * picture or overlapping, a luma CU list with chained edges out of decode
+ * order) keep host-derived segments, as without the flag. */
 #define H266_PLAN_DEVICE_SIDEINFO 1u
 int h266_chain_plan_create_ex(h266_ctx *ctx, const h266_picture *pic, const h266_in_loop_filter_args *args,
                               uint32_t flags, h266_chain_plan **out);
 /* 1 when the plan derives its side information on the device at every
  * execution, 0 when it holds host-derived segments. */
 int h266_chain_plan_device_sideinfo(const h266_chain_plan *plan);
+/* Which deblocking side information a picture gets (host only, no context,
+ * no device): 0 built on the host (the crate's walk, src/deblock.rs:630-983);
+ * 1 built on the device, no two edge footprints can overlap (luma CUs and
+ * transform blocks of at least 8 samples, no sub-block grids, 4:2:0 or 4:0:0:
+ * the grid-mode tile kernel when SAO or ALF runs); 2 built on the device with
+ * footprints that may chain, other chroma formats (the grid-mode strip
+ * kernels).  Negative: an H266_ERR_* code for invalid arguments. */
+int h266_sideinfo_mode(const h266_picture *pic, const h266_in_loop_filter_args *args);
 /* Executes n plans on n device pictures (pics[i] with plans[i]; sizes may
  * differ) as one batch: one deblocking launch and one SAO / ALF launch per
  * kernel variant cover the tiles of every picture, so the GPU's tail between

@@ -2376,6 +2376,15 @@ int h266_chain_plan_create(h266_ctx *ctx, const h266_picture *pic, const h266_in
 
 int h266_chain_plan_device_sideinfo(const h266_chain_plan *plan) { return plan && plan->db.device_walk ? 1 : 0; }
 
+int h266_sideinfo_mode(const h266_picture *pic, const h266_in_loop_filter_args *args) {
+  if (!pic || !args) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL picture or args");
+  if (args->n_cus && !args->cus) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL CU list with nonzero length");
+  if (args->n_chroma_cus && !args->chroma_cus)
+    return set_error(H266_ERR_INVALID_ARGUMENT, "NULL chroma CU list with nonzero length");
+  return h266::device_walk_mode(*pic, args->cus, args->n_cus, args->chroma_cus, args->n_chroma_cus, args->deblock,
+                                args->chroma_format_idc);
+}
+
 int h266_chain_plan_create_ex(h266_ctx *ctx, const h266_picture *pic, const h266_in_loop_filter_args *args,
                               uint32_t flags, h266_chain_plan **out) {
   H266_TRY(check_ctx(ctx));

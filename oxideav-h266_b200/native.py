@@ -33,7 +33,8 @@ EXPORTS = [
     "h266_apply_deblocking_clipped",
     "h266_apply_sao_clipped", "h266_apply_alf_clipped", "h266_apply_in_loop_filters",
     "h266_apply_in_loop_filters_batch", "h266_ctx_set_profiling", "h266_ctx_profile", "h266_chain_plan_create",
-    "h266_chain_plan_create_ex", "h266_chain_plan_device_sideinfo", "h266_ctx_set_tuning", "h266_ctx_set_tuning_for",
+    "h266_chain_plan_create_ex", "h266_chain_plan_device_sideinfo", "h266_sideinfo_mode", "h266_ctx_set_tuning",
+    "h266_ctx_set_tuning_for",
     "h266_ctx_get_tuning", "h266_ctx_host_profile", "h266_batch_graph_create", "h266_batch_graph_launch",
     "h266_batch_graph_destroy", "h266_server_set_batch_pixels", "h266_sao_chroma_merge_batch",
     "h266_chain_plan_execute", "h266_chain_plan_execute_batch", "h266_chain_plan_destroy",
@@ -80,6 +81,7 @@ def lib():
         L.h266_chain_plan_create.argtypes = [vp, vp, vp, C.POINTER(vp)]
         L.h266_chain_plan_create_ex.argtypes = [vp, vp, vp, u32, C.POINTER(vp)]
         L.h266_chain_plan_device_sideinfo.argtypes = [vp]
+        L.h266_sideinfo_mode.argtypes = [vp, vp]
         L.h266_ctx_set_tuning.argtypes = [vp, C.c_char_p, C.c_int64]
         L.h266_ctx_set_tuning_for.argtypes = [vp, u32, u32, u32, C.c_char_p, C.c_int64]
         L.h266_ctx_get_tuning.argtypes = [vp, C.c_char_p, C.POINTER(C.c_int64)]
@@ -588,3 +590,15 @@ def sao_chroma_merge_batch(ctx: Context, srcs, pres, indeps, grids, *, bit_depth
                                              wcs, hcs, bit_depth, ctb_log2, arr([x.ctypes.data for x in outs]),
                                              arr([x.ctypes.data for x in maps])))
     return [(o, m[: len(x)]) for o, m, x in zip(outs, maps, inds)]
+
+
+def sideinfo_mode(pic, fa: FilterArgsData) -> int:
+    """h266_sideinfo_mode: 0 host-built side information, 1 device-built for
+    the tile kernel (no chained footprints), 2 device-built for the strip
+    kernels.  Host only: needs no GPU."""
+    cp = pic.to_ctypes()
+    a, keep = fa.to_ctypes()
+    r = lib().h266_sideinfo_mode(C.byref(cp), C.byref(a))
+    if r < 0:
+        _check(r)
+    return r
