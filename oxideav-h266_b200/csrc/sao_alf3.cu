@@ -285,8 +285,23 @@ __device__ __forceinline__ bool sao_alf_tile3(const Pass2Args &a, const Pass2Arg
   }
   const bool tma = a.tma != 0;
 
-  // ---- (1) SAO parameters of the 3x3 CTB neighbourhood; deblocked windows
-  if (!PERSIST && tid == 0 && tma) mbar_init(&sm.bar, 1);
+  // ---- (1) deblocked windows (thread 0 starts the copies first, so they
+  // overlap the rest of the phase); SAO parameters of the 3x3 CTB neighbourhood
+  if (tma && tid == 0) {
+    if (!PERSIST) mbar_init(&sm.bar, 1);
+    const uint32_t bytes = (a.src[0].w > 0 && a.src[0].h > 0 ? S::DL_BYTES : 0) +
+                           (chroma_on[0] ? S::DC_BYTES : 0) + (chroma_on[1] ? S::DC_BYTES : 0);
+    if (GLOBAL_MAPS)
+      for (int c = 0; c < 3; ++c) tmap_acquire(&maps->tmap[c]);
+    // the previous tile's generic accesses of the window space (ordered by the
+    // persistent loop's barrier) come before these copies
+    if (PERSIST) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&sm.bar, bytes);
+    if (a.src[0].w > 0 && a.src[0].h > 0) tma_load_2d(sm.dL(), &maps->tmap[0], X0 - 8, Y0 - 4, &sm.bar);
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+      if (chroma_on[c]) tma_load_2d(sm.dC(c), &maps->tmap[1 + c], xc0 - 8, yc0 - 3, &sm.bar);
+  }
   int my_type = 0;
   if (tid < 27) {
     const int comp = tid / 9, n = tid % 9;
@@ -342,22 +357,7 @@ __device__ __forceinline__ bool sao_alf_tile3(const Pass2Args &a, const Pass2Arg
     for (int c = 0; c < 2; ++c)
       if (chroma_on[c]) load(sm.dC(c), a.src[c + 1], xc0 - 8, yc0 - 3, S::DCW, S::DCH);
   }
-  __syncthreads();  // SAO parameters, the barrier's initialisation (and the vector-loaded windows)
-  if (tma) {
-    if (tid == 0) {
-      const uint32_t bytes = (a.src[0].w > 0 && a.src[0].h > 0 ? S::DL_BYTES : 0) +
-                             (chroma_on[0] ? S::DC_BYTES : 0) + (chroma_on[1] ? S::DC_BYTES : 0);
-      if (GLOBAL_MAPS)
-        for (int c = 0; c < 3; ++c) tmap_acquire(&maps->tmap[c]);
-      // the previous tile's generic accesses of the window space come before these copies
-      if (PERSIST) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_expect_tx(&sm.bar, bytes);
-      if (a.src[0].w > 0 && a.src[0].h > 0) tma_load_2d(sm.dL(), &maps->tmap[0], X0 - 8, Y0 - 4, &sm.bar);
-#pragma unroll
-      for (int c = 0; c < 2; ++c)
-        if (chroma_on[c]) tma_load_2d(sm.dC(c), &maps->tmap[1 + c], xc0 - 8, yc0 - 3, &sm.bar);
-    }
-  }
+  __syncthreads();  // SAO parameters, the barrier's initialisation (or the vector-loaded windows)
 
   // geometry of the packed SAO rectangles while the copies are in flight
   const unsigned any = sm.any_sao;
