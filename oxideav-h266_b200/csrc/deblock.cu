@@ -227,9 +227,142 @@ H266_HD inline int bs_of(uint32_t comp, const h266_deblock_cu &p, const h266_deb
   return 0;
 }
 
+// The walk geometry of a CU for one (plane, pass), shared by its edges
+// (deblock_cu_dir, src/deblock.rs:707-760).
+struct CuWalkGeo {
+  uint32_t n_cb, n_other, step, seg, nsb, sb, n8, last_sb, ctb_h_c;
+  bool chroma, filter_edge, off_grid;  // off_grid: a chroma CU off the 8-sample chroma edge grid
+};
+
+H266_HD inline CuWalkGeo cu_walk_geo(const h266_deblock_cu &cu, const PlaneCfg &pc, bool vert, const uint32_t *nf,
+                                     uint64_t n_nf) {
+  CuWalkGeo g;
+  g.chroma = pc.comp != 0;
+  g.off_grid = g.chroma && ((vert ? cu.x / pc.sub_w : cu.y / pc.sub_h) % 8) != 0;
+  g.n_cb = vert ? cu.w : cu.h;
+  g.n_other = vert ? cu.h : cu.w;
+  const uint32_t lead = vert ? cu.x : cu.y;
+  bool gated = false;
+  for (uint64_t i = 0; i < n_nf; ++i) gated |= nf[i] == lead;
+  g.filter_edge = lead != 0 && !gated;
+  g.step = g.chroma ? 8 * (vert ? pc.sub_w : pc.sub_h) : 4;
+  g.seg = g.chroma ? 2 * (vert ? pc.sub_h : pc.sub_w) : 4;
+  g.nsb = 1;
+  if (!g.chroma && cu.has_num_sb) g.nsb = std::max(vert ? cu.num_sb_x : cu.num_sb_y, 1u);
+  g.sb = std::max(8u, g.n_cb / g.nsb);
+  g.n8 = std::max(g.n_cb / 8, 1u);
+  g.last_sb = std::min(g.n8 - 1, g.nsb - 1);
+  g.ctb_h_c = pc.ctb / std::max(pc.sub_h, 1u);
+  return g;
+}
+
+// Along one edge only the P-side CU and the bS inputs change; the
+// maxFilterLengths, qP and flags that depend on the P-side CU are kept while
+// it stays the same (a fresh WalkMemo recomputes them: same values).
+struct WalkMemo {
+  int64_t pi = -2;
+  uint32_t mp = 0, mq = 0;
+  int qp = 0;
+};
+
+// The segment at position k along the edge at offset `off` of CU `idx`
+// (deblock_cu_dir's inner loop, src/deblock.rs:760-983): emitted when it
+// filters anything.  `grid.at(x, y)` is the CU covering luma sample (x, y)
+// (CuGrid::cu_at), -1 for none.
+#pragma nv_exec_check_disable
+template <class Grid, class Mv, class Emit>
+H266_HD inline void walk_segment(const h266_deblock_cu *cus_, const Grid &grid, const PlaneCfg &pc, bool vert,
+                                 const Mv &mv, size_t idx, const CuWalkGeo &g, uint32_t off, bool is_tb, bool is_sb,
+                                 uint32_t k, Emit &emit, WalkMemo &memo) {
+  const h266_deblock_cu &cu = cus_[idx];
+  const bool chroma = g.chroma, filter_edge = g.filter_edge;
+  const uint32_t n_cb = g.n_cb, nsb = g.nsb, sb = g.sb, n8 = g.n8, ctb_h_c = g.ctb_h_c;
+  Cu q_geo{cu};
+    const int qx = (int)(vert ? cu.x + off : cu.x + k), qy = (int)(vert ? cu.y + k : cu.y + off);
+    const int px = vert ? qx - 1 : qx, py = vert ? qy : qy - 1;
+    int64_t pi = off == 0 ? grid.at(px, py) : (int64_t)idx;
+    if (pi < 0 || (off == 0 && pi == (int64_t)idx)) return;
+    const h266_deblock_cu &p = cus_[pi];
+    const int bs = bs_of(pc.comp, p, cu, mv, px, py, qx, qy, is_tb, is_sb);
+    if (bs == 0) return;
+    uint32_t mp, mq;
+    int qp;
+    const bool ctb_row = !chroma && !vert && off == 0 && pc.ctb > 0 && cu.y % pc.ctb == 0;
+    if (pi == memo.pi) {
+      mp = memo.mp;
+      mq = memo.mq;
+      qp = memo.qp;
+    } else if (!chroma) {
+      mp = mq = 0;
+      if (is_tb) {
+        uint32_t wq = q_geo.tb_len(qx, qy, vert, false), wp = Cu{p}.tb_len(px, py, vert, false);
+        if (wp <= 4 || wq <= 4) mp = mq = 1;
+        else {
+          mp = wp >= 32 ? 7 : 3;
+          mq = wq >= 32 ? 7 : 3;
+        }
+      }
+      if (is_sb) {  // §8.8.3.4 overlay, src/deblock.rs:856-901
+        if (off == 0) {
+          if (nsb > 1) mq = std::min(mq, 5u);
+          if (p.has_num_sb) mp = std::min(mp, 5u);
+        } else {
+          auto tb_at = [&](int64_t z) {
+            if (z < 0 || z >= (int64_t)n_cb) return false;
+            return z == 0 ? filter_edge : q_geo.tb_boundary((uint32_t)z, vert, false);
+          };
+          if (is_tb) {
+            mp = std::min(mp, 5u);
+            mq = std::min(mq, 5u);
+          } else if (tb_at((int64_t)off - 4) || tb_at((int64_t)off + 4)) {
+            mp = mq = 1;
+          } else if (off / sb == 1 || off / sb == n8 - 1 || tb_at((int64_t)off - sb) || tb_at((int64_t)off + sb)) {
+            mp = mq = 2;
+          } else {
+            mp = mq = 3;
+          }
+        }
+      }
+      qp = (p.qp_y + cu.qp_y + 1) >> 1;  // eq. 1274 (no LADF)
+    } else {
+      const uint32_t sub = vert ? pc.sub_w : pc.sub_h;
+      const uint32_t wq = q_geo.tb_len(qx, qy, vert, true) / sub, wp = Cu{p}.tb_len(px, py, vert, true) / sub;
+      if (wp >= 8 && wq >= 8) {
+        const bool row = !vert && off == 0 && ctb_h_c > 0 && (cu.y / pc.sub_h) % ctb_h_c == 0;
+        mp = row ? 1 : 3;
+        mq = 3;
+      } else {
+        mp = mq = 1;
+      }
+      auto pick = [&](const h266_deblock_cu &c) {  // src/deblock.rs:1155-1163
+        if (c.qp_c[0] == INT32_MIN) return clampi(c.qp_y + pc.qp_off, 0, 63);
+        if (c.joint_cbcr2) return (int)c.qp_c[2];
+        return (int)c.qp_c[pc.comp == 1 ? 0 : 1];
+      };
+      qp = (pick(p) + pick(cu) + 1) >> 1;  // eq. 1343
+    }
+    memo.pi = pi;
+    memo.mp = mp;
+    memo.mq = mq;
+    memo.qp = qp;
+    const int beta = beta_of(qp + pc.beta_off * 2, pc.bd);
+    const int tc = tc_of(qp + 2 * (bs - 1) + pc.tc_off * 2, pc.bd);
+    if (tc == 0) return;  // every filter arm is a no-op at tC = 0
+    if (chroma && mp == 1 && mq == 1 && bs != 2) return;  // src/deblock.rs:1823, 1888
+    Emitted e;
+    e.s.x = (uint16_t)(chroma ? qx / (int)pc.sub_w : qx);
+    e.s.y = (uint16_t)(chroma ? qy / (int)pc.sub_h : qy);
+    e.s.beta = (uint16_t)beta;
+    e.s.tc = (uint16_t)tc;
+    e.s.plane = (uint8_t)pc.comp;
+    e.s.bs = (uint8_t)bs;
+    e.s.mfl = (uint8_t)(mp << 4 | mq);
+    e.s.flags = (uint8_t)((vert ? 1 : 0) | (ctb_row ? 2 : 0) | (p.plt ? 4 : 0) | (cu.plt ? 8 : 0));
+    emit(e.s);
+}
+
 // deblock_cu_dir (src/deblock.rs:707-983) for CU `idx`: every edge segment it
-// owns, in the reference's order, passed to `emit`.  `grid.at(x, y)` is the
-// CU covering luma sample (x, y) (CuGrid::cu_at), -1 for none.
+// owns, in the reference's order, passed to `emit`.
 #pragma nv_exec_check_disable
 // `only_off` >= 0 restricts the walk to the edge at that offset inside the CU
 // (the device runs one thread per offset).
@@ -237,114 +370,17 @@ template <class Grid, class Mv, class Emit>
 H266_HD void walk_cu(const h266_deblock_cu *cus_, const Grid &grid, const PlaneCfg &pc, bool vert, const Mv &mv,
                      const uint32_t *nf, uint64_t n_nf, size_t idx, Emit &emit, int only_off = -1) {
   const h266_deblock_cu &cu = cus_[idx];
-  const bool chroma = pc.comp != 0;
-  if (chroma && ((vert ? cu.x / pc.sub_w : cu.y / pc.sub_h) % 8) != 0) return;
-  const uint32_t n_cb = vert ? cu.w : cu.h, n_other = vert ? cu.h : cu.w, lead = vert ? cu.x : cu.y;
-  bool gated = false;
-  for (uint64_t i = 0; i < n_nf; ++i) gated |= nf[i] == lead;
-  const bool filter_edge = lead != 0 && !gated;
-  const uint32_t step = chroma ? 8 * (vert ? pc.sub_w : pc.sub_h) : 4;
-  const uint32_t seg = chroma ? 2 * (vert ? pc.sub_h : pc.sub_w) : 4;
-  uint32_t nsb = 1;
-  if (!chroma && cu.has_num_sb) nsb = std::max(vert ? cu.num_sb_x : cu.num_sb_y, 1u);
-  const uint32_t sb = std::max(8u, n_cb / nsb), n8 = std::max(n_cb / 8, 1u);
-  const uint32_t last_sb = std::min(n8 - 1, nsb - 1);
-  const uint32_t ctb_h_c = pc.ctb / std::max(pc.sub_h, 1u);
+  const CuWalkGeo g = cu_walk_geo(cu, pc, vert, nf, n_nf);
+  if (g.off_grid) return;
   Cu q_geo{cu};
-  for (uint32_t off = only_off >= 0 ? (uint32_t)only_off : 0; off < n_cb; off += step) {
+  for (uint32_t off = only_off >= 0 ? (uint32_t)only_off : 0; off < g.n_cb; off += g.step) {
     if (only_off >= 0 && off != (uint32_t)only_off) break;
-    const bool is_tb = off == 0 ? filter_edge : q_geo.tb_boundary(off, vert, chroma);
-    const bool is_sb = !chroma && off % sb == 0 && off / sb <= last_sb && (off > 0 || filter_edge);
+    const bool is_tb = off == 0 ? g.filter_edge : q_geo.tb_boundary(off, vert, g.chroma);
+    const bool is_sb = !g.chroma && off % g.sb == 0 && off / g.sb <= g.last_sb && (off > 0 || g.filter_edge);
     if (!is_tb && !is_sb) continue;
-    // Along one edge only the P-side CU and the bS inputs change; the
-    // maxFilterLengths, qP and flags that depend on the P-side CU are kept
-    // while it stays the same.
-    int64_t memo_pi = -2;
-    uint32_t memo_mp = 0, memo_mq = 0;
-    int memo_qp = 0;
-    for (uint32_t k = 0; k < n_other; k += seg) {
-      const int qx = (int)(vert ? cu.x + off : cu.x + k), qy = (int)(vert ? cu.y + k : cu.y + off);
-      const int px = vert ? qx - 1 : qx, py = vert ? qy : qy - 1;
-      int64_t pi = off == 0 ? grid.at(px, py) : (int64_t)idx;
-      if (pi < 0 || (off == 0 && pi == (int64_t)idx)) continue;
-      const h266_deblock_cu &p = cus_[pi];
-      const int bs = bs_of(pc.comp, p, cu, mv, px, py, qx, qy, is_tb, is_sb);
-      if (bs == 0) continue;
-      uint32_t mp, mq;
-      int qp;
-      const bool ctb_row = !chroma && !vert && off == 0 && pc.ctb > 0 && cu.y % pc.ctb == 0;
-      if (pi == memo_pi) {
-        mp = memo_mp;
-        mq = memo_mq;
-        qp = memo_qp;
-      } else if (!chroma) {
-        mp = mq = 0;
-        if (is_tb) {
-          uint32_t wq = q_geo.tb_len(qx, qy, vert, false), wp = Cu{p}.tb_len(px, py, vert, false);
-          if (wp <= 4 || wq <= 4) mp = mq = 1;
-          else {
-            mp = wp >= 32 ? 7 : 3;
-            mq = wq >= 32 ? 7 : 3;
-          }
-        }
-        if (is_sb) {  // §8.8.3.4 overlay, src/deblock.rs:856-901
-          if (off == 0) {
-            if (nsb > 1) mq = std::min(mq, 5u);
-            if (p.has_num_sb) mp = std::min(mp, 5u);
-          } else {
-            auto tb_at = [&](int64_t z) {
-              if (z < 0 || z >= (int64_t)n_cb) return false;
-              return z == 0 ? filter_edge : q_geo.tb_boundary((uint32_t)z, vert, false);
-            };
-            if (is_tb) {
-              mp = std::min(mp, 5u);
-              mq = std::min(mq, 5u);
-            } else if (tb_at((int64_t)off - 4) || tb_at((int64_t)off + 4)) {
-              mp = mq = 1;
-            } else if (off / sb == 1 || off / sb == n8 - 1 || tb_at((int64_t)off - sb) || tb_at((int64_t)off + sb)) {
-              mp = mq = 2;
-            } else {
-              mp = mq = 3;
-            }
-          }
-        }
-        qp = (p.qp_y + cu.qp_y + 1) >> 1;  // eq. 1274 (no LADF)
-      } else {
-        const uint32_t sub = vert ? pc.sub_w : pc.sub_h;
-        const uint32_t wq = q_geo.tb_len(qx, qy, vert, true) / sub, wp = Cu{p}.tb_len(px, py, vert, true) / sub;
-        if (wp >= 8 && wq >= 8) {
-          const bool row = !vert && off == 0 && ctb_h_c > 0 && (cu.y / pc.sub_h) % ctb_h_c == 0;
-          mp = row ? 1 : 3;
-          mq = 3;
-        } else {
-          mp = mq = 1;
-        }
-        auto pick = [&](const h266_deblock_cu &c) {  // src/deblock.rs:1155-1163
-          if (c.qp_c[0] == INT32_MIN) return clampi(c.qp_y + pc.qp_off, 0, 63);
-          if (c.joint_cbcr2) return (int)c.qp_c[2];
-          return (int)c.qp_c[pc.comp == 1 ? 0 : 1];
-        };
-        qp = (pick(p) + pick(cu) + 1) >> 1;  // eq. 1343
-      }
-      memo_pi = pi;
-      memo_mp = mp;
-      memo_mq = mq;
-      memo_qp = qp;
-      const int beta = beta_of(qp + pc.beta_off * 2, pc.bd);
-      const int tc = tc_of(qp + 2 * (bs - 1) + pc.tc_off * 2, pc.bd);
-      if (tc == 0) continue;  // every filter arm is a no-op at tC = 0
-      if (chroma && mp == 1 && mq == 1 && bs != 2) continue;  // src/deblock.rs:1823, 1888
-      Emitted e;
-      e.s.x = (uint16_t)(chroma ? qx / (int)pc.sub_w : qx);
-      e.s.y = (uint16_t)(chroma ? qy / (int)pc.sub_h : qy);
-      e.s.beta = (uint16_t)beta;
-      e.s.tc = (uint16_t)tc;
-      e.s.plane = (uint8_t)pc.comp;
-      e.s.bs = (uint8_t)bs;
-      e.s.mfl = (uint8_t)(mp << 4 | mq);
-      e.s.flags = (uint8_t)((vert ? 1 : 0) | (ctb_row ? 2 : 0) | (p.plt ? 4 : 0) | (cu.plt ? 8 : 0));
-      emit(e.s);
-    }
+    WalkMemo memo;
+    for (uint32_t k = 0; k < g.n_other; k += g.seg)
+      walk_segment(cus_, grid, pc, vert, mv, idx, g, off, is_tb, is_sb, k, emit, memo);
   }
 }
 
@@ -2644,21 +2680,56 @@ __global__ void __launch_bounds__(128) k_walk_batch(const WalkBatchItem *__restr
   const WalkParams &a = s;
   const int l = blockIdx.y, plane = l / 2, d = l % 2;
   const int list = plane ? 1 : 0;
+  const bool vert = d == 0;
+  const DevCuGrid grid{a.cu_grid[list], a.cw4, a.ch4};
+  const GridEmit emit{&a, d, plane};
+  auto with_mv = [&](auto &&f) {
+    if (plane == 0 && a.has_mv && a.mv_per_cu) f(CuMotion{&a.mv, a.mv_per_cu, DevCuGrid{a.cu_grid[0], a.cw4, a.ch4}});
+    else f(MvGrid{plane == 0 && a.has_mv ? &a.mv : nullptr});
+  };
+  if (blockIdx.z == 0) {
+    // The CUs' own edges (offset 0), packed: lane j of a warp counts the
+    // segments of CU base + j's edge, and the warp walks all 32 CUs'
+    // segments one per lane per round, so lanes stay busy whatever the CU
+    // sizes (no memo across segments: the same values, recomputed).
+    __shared__ uint32_t s_pre[4][32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t base = (blockIdx.x - first[p]) * blockDim.x + warp * 32, i = base + lane;
+    uint32_t nseg = 0;
+    if (i < a.n[list]) {
+      const CuWalkGeo g = cu_walk_geo(a.cus[list][i], a.cfg[plane], vert, a.nf[d], a.n_nf[d]);
+      if (!g.off_grid && g.filter_edge) nseg = (g.n_other + g.seg - 1) / g.seg;
+    }
+    uint32_t incl = nseg;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    s_pre[warp][lane] = incl - nseg;
+    const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    __syncwarp();
+    for (uint32_t t = lane; t < total; t += 32) {
+      const int j = band_of(s_pre[warp], t);  // the lane whose CU holds segment t
+      const size_t idx = base + j;
+      const CuWalkGeo g = cu_walk_geo(a.cus[list][idx], a.cfg[plane], vert, a.nf[d], a.n_nf[d]);
+      const uint32_t k = (t - s_pre[warp][j]) * g.seg;
+      with_mv([&](const auto &mv) {
+        WalkMemo memo;
+        walk_segment(a.cus[list], grid, a.cfg[plane], vert, mv, idx, g, 0, g.filter_edge, !g.chroma && g.filter_edge,
+                     k, emit, memo);
+      });
+    }
+    return;
+  }
+  // edges inside a CU (blockIdx.z = offset / step): one thread per CU
   const uint32_t i = (blockIdx.x - first[p]) * blockDim.x + threadIdx.x;
   if (i >= a.n[list]) return;
   const h266_deblock_cu &cu = a.cus[list][i];
-  const uint32_t step = plane ? 8 * (d == 0 ? a.cfg[plane].sub_w : a.cfg[plane].sub_h) : 4;
+  const uint32_t step = plane ? 8 * (vert ? a.cfg[plane].sub_w : a.cfg[plane].sub_h) : 4;
   const uint32_t off = blockIdx.z * step;
-  if (off >= (d == 0 ? cu.w : cu.h)) return;
-  const DevCuGrid grid{a.cu_grid[list], a.cw4, a.ch4};
-  const GridEmit emit{&a, d, plane};
-  if (plane == 0 && a.has_mv && a.mv_per_cu) {
-    const CuMotion mv{&a.mv, a.mv_per_cu, DevCuGrid{a.cu_grid[0], a.cw4, a.ch4}};
-    walk_cu(a.cus[list], grid, a.cfg[plane], d == 0, mv, a.nf[d], a.n_nf[d], i, emit, (int)off);
-  } else {
-    const MvGrid mv{plane == 0 && a.has_mv ? &a.mv : nullptr};
-    walk_cu(a.cus[list], grid, a.cfg[plane], d == 0, mv, a.nf[d], a.n_nf[d], i, emit, (int)off);
-  }
+  if (off >= (vert ? cu.w : cu.h)) return;
+  with_mv([&](const auto &mv) { walk_cu(a.cus[list], grid, a.cfg[plane], vert, mv, a.nf[d], a.n_nf[d], i, emit, (int)off); });
 }
 
 }  // namespace
