@@ -294,6 +294,9 @@ int h266_ctx_set_profiling(h266_ctx *ctx, int on);
  *   "e2e_copy_streams"     1: every upload (planes, side information, batch tables) in issue order
  *                          on one stream and every download on another (default); 0: each group's
  *                          copies on its group's stream
+ *   "e2e_ramp"             1: the batch starts and ends with groups of 1, 2, 4 ... pictures, so the
+ *                          first kernels start and the last downloads end sooner (default); 0: all
+ *                          groups of e2e_group pictures
  * h266_ctx_set_tuning sets the context's value; h266_ctx_set_tuning_for sets
  * it for batches whose largest picture has that luma size and bit depth, which
  * takes precedence.  Unknown keys or out-of-range values: H266_ERR_INVALID_ARGUMENT. */

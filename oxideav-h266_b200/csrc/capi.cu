@@ -181,6 +181,7 @@ struct Tuning {
   // small latency-critical copies do not wait behind other lanes' planes in
   // the copy engine (measured 9.0 against 10.3 ms per 32 x 1080p)
   int e2e_copy_streams = 1;
+  int e2e_ramp = 1;  // 1: the end-to-end batch starts and ends with groups of 1, 2, ... pictures
 };
 struct TuningKey {
   const char *name;
@@ -192,7 +193,8 @@ constexpr TuningKey kTuningKeys[] = {{"e2e_group", &Tuning::e2e_group, 1, 16},
                                      {"sao_alf_ctas_per_sm", &Tuning::sao_alf_ctas_per_sm, 0, 4},
                                      {"sao_alf_tile_h", &Tuning::sao_alf_tile_h, 32, 64},
                                      {"prep_threads", &Tuning::prep_threads, 0, 64},
-                                     {"e2e_copy_streams", &Tuning::e2e_copy_streams, 0, 1}};
+                                     {"e2e_copy_streams", &Tuning::e2e_copy_streams, 0, 1},
+                                     {"e2e_ramp", &Tuning::e2e_ramp, 0, 1}};
 
 struct GroupLane {
   cudaStream_t stream = nullptr;
@@ -2135,7 +2137,34 @@ int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *co
   Guard g(ctx->device);
   const Tuning &tn = batch_tuning(ctx, n, pics);
   const uint32_t kGroup = (uint32_t)tn.e2e_group, kGroupLanes = (uint32_t)tn.e2e_lanes;
-  const uint32_t n_groups = (n + kGroup - 1) / kGroup, n_lanes = std::min(n_groups, kGroupLanes);
+  // Group boundaries.  With e2e_ramp the batch starts and ends with small
+  // groups (1, 2, ... and ..., 2, 1 pictures): the first kernels and
+  // downloads start after one picture's upload instead of a whole group's,
+  // and the last group's kernels and downloads, which nothing overlaps, are
+  // one picture's.
+  std::vector<uint32_t> gb(1, 0);
+  {
+    std::vector<uint32_t> ramp;
+    for (uint32_t g = 1; g < kGroup; g *= 2) ramp.push_back(g);
+    uint32_t ends = 0;
+    for (uint32_t g : ramp) ends += 2 * g;
+    const bool use_ramp = tn.e2e_ramp && n >= ends + 2 * kGroup;
+    uint32_t left = n;
+    if (use_ramp)
+      for (uint32_t g : ramp) {
+        gb.push_back(gb.back() + g);
+        left -= g;
+      }
+    const uint32_t tail = use_ramp ? ends / 2 : 0;
+    while (left > tail) {
+      const uint32_t g = std::min(kGroup, left - tail);
+      gb.push_back(gb.back() + g);
+      left -= g;
+    }
+    if (use_ramp)
+      for (size_t k = ramp.size(); k-- > 0;) gb.push_back(gb.back() + ramp[k]);
+  }
+  const uint32_t n_groups = (uint32_t)gb.size() - 1, n_lanes = std::min(n_groups, kGroupLanes);
   for (auto &l : ctx->glanes)  // a larger group than the lanes were made for: more slots
     if (l->slots.size() < kGroup) l->slots.resize(kGroup);
   while (ctx->glanes.size() < n_lanes) {
@@ -2176,7 +2205,7 @@ int h266_apply_in_loop_filters_batch(h266_ctx *ctx, uint32_t n, h266_picture *co
   auto run_group = [&](uint32_t gi) -> int {
     GroupLane &L = *ctx->glanes[gi % n_lanes];
     std::vector<BatchItem> items;
-    const uint32_t i0 = gi * kGroup, i1 = std::min(n, i0 + kGroup);
+    const uint32_t i0 = gb[gi], i1 = gb[gi + 1];
     // uploads on the upload stream once the lane's previous downloads freed its slots
     const cudaStream_t up = copy_streams ? ctx->e2e_up : L.stream;
     if (copy_streams) H266_CUDA(cudaStreamWaitEvent(up, L.ev_down, 0));

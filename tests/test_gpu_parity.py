@@ -166,9 +166,10 @@ def test_batch_pipelined_host_pictures(ctx):
         assert_same(got, want, f"batch picture {i}")
 
 
-@pytest.mark.parametrize("group,lanes,copy_streams,prep", [(1, 1, 0, 2), (2, 4, 1, 3), (8, 2, 0, 0), (3, 3, 1, 16),
-                                                          (1, 1, 1, 0), (2, 16, 1, 4)])
-def test_batch_launch_shapes_match_oracle(group, lanes, copy_streams, prep):
+@pytest.mark.parametrize("group,lanes,copy_streams,prep,ramp", [(1, 1, 0, 2, 1), (2, 4, 1, 3, 1), (8, 2, 0, 0, 1),
+                                                               (3, 3, 1, 16, 1), (1, 1, 1, 0, 0), (2, 16, 1, 4, 0),
+                                                               (4, 2, 1, 0, 1)])
+def test_batch_launch_shapes_match_oracle(group, lanes, copy_streams, prep, ramp):
     """The end-to-end batch under other tunings (group size, streams, copy
     streams, preparation threads): the same results, bit for bit.  Pinned
     host pictures, so the copies are asynchronous."""
@@ -186,7 +187,7 @@ def test_batch_launch_shapes_match_oracle(group, lanes, copy_streams, prep):
         pinned.append((W.PictureData(*[t.numpy().view(np.uint16) for t in planes], p.bit_depth), planes))
     with native.Context(0) as c:
         for key, v in (("e2e_group", group), ("e2e_lanes", lanes), ("e2e_copy_streams", copy_streams),
-                       ("prep_threads", prep)):
+                       ("prep_threads", prep), ("e2e_ramp", ramp)):
             c.set_tuning(key, v)
             assert c.get_tuning(key) == v
         for rnd in range(2):
@@ -198,6 +199,21 @@ def test_batch_launch_shapes_match_oracle(group, lanes, copy_streams, prep):
                 want = p.copy()
                 oracle.apply_in_loop_filters(want, f)
                 assert_same(pic, want, f"tuned batch round {rnd} picture {i}")
+
+
+def test_batch_ramp_groups_match_oracle():
+    """16 host pictures in groups of 4 with the ramp (groups 1, 2, 4, 4, 2, 2,
+    1): every picture bit-exact."""
+    items = [(small_c2 if i % 2 else W.config1)(9000 + i) for i in range(16)]
+    pics = [p.copy() for p, _ in items]
+    with native.Context(0) as c:
+        c.set_tuning("e2e_group", 4)
+        c.set_tuning("e2e_ramp", 1)
+        c.apply_in_loop_filters_batch(pics, [f for _, f in items])
+    for i, ((p, f), got) in enumerate(zip(items, pics)):
+        want = p.copy()
+        oracle.apply_in_loop_filters(want, f)
+        assert_same(got, want, f"ramped batch picture {i}")
 
 
 def test_tuning_rejects_unknown_keys_and_ranges(ctx):
