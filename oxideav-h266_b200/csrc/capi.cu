@@ -966,14 +966,46 @@ int prepare_chain(Prep &pr, const h266_picture &pic, const h266_in_loop_filter_a
     const h266_deblock_cu *lists[2] = {a.cus, a.chroma_cus};
     const uint64_t counts[2] = {a.n_cus, db.dw_sep ? a.n_chroma_cus : 0};
     thread_local std::vector<CuTail> tails;
+    auto fits8 = [](int32_t v) { return v >= -127 && v <= 127; };
     for (int l = 0; l < (db.dw_sep ? 2 : 1); ++l) {
+      // compact heads when every CU of the list fits them (QPs and sub-block counts in 8 bits)
+      bool compact = true;
+      for (uint64_t i = 0; i < counts[l] && compact; ++i) {
+        const h266_deblock_cu &c = lists[l][i];
+        const bool legacy = c.qp_c[0] == INT32_MIN;
+        compact = fits8(c.qp_y) && (legacy || (fits8(c.qp_c[0]) && fits8(c.qp_c[1]) && fits8(c.qp_c[2]))) &&
+                  c.num_sb_x <= 255 && c.num_sb_y <= 255 && c.x + c.w <= 65535 && c.y + c.h <= 65535;
+      }
+      w.compact[l] = compact;
+      const size_t hb = compact ? sizeof(CuCompact) : kCuHeadBytes;
       size_t off;
-      uint8_t *heads = blob.alloc(counts[l] * kCuHeadBytes, off);
+      uint8_t *heads = blob.alloc(counts[l] * hb, off);
       (l ? pr.st.dw_ccus : pr.st.dw_cus) = off;
       tails.clear();
       for (uint64_t i = 0; i < counts[l]; ++i) {
         const h266_deblock_cu &c = lists[l][i];
-        std::memcpy(heads + i * kCuHeadBytes, &c, kCuHeadBytes);
+        if (compact) {
+          CuCompact k;
+          k.x = (uint16_t)c.x;
+          k.y = (uint16_t)c.y;
+          k.w = (uint16_t)c.w;
+          k.h = (uint16_t)c.h;
+          const bool legacy = c.qp_c[0] == INT32_MIN;
+          k.qp_y = (int8_t)c.qp_y;
+          k.qp_c[0] = legacy ? (int8_t)-128 : (int8_t)c.qp_c[0];
+          k.qp_c[1] = legacy ? (int8_t)0 : (int8_t)c.qp_c[1];
+          k.qp_c[2] = legacy ? (int8_t)0 : (int8_t)c.qp_c[2];
+          const uint8_t fl[13] = {c.intra,        c.tu_y_coded, c.tu_cb_coded, c.tu_cr_coded, c.bdpcm_luma,
+                                  c.bdpcm_chroma, c.plt,        c.joint_cbcr2, c.ciip,        c.ibc,
+                                  c.has_num_sb,   c.has_tu64,   c.has_tb_split};
+          k.flags = 0;
+          for (int b = 0; b < 13; ++b) k.flags |= (uint16_t)((fl[b] != 0) << b);
+          k.nsb_x = (uint8_t)c.num_sb_x;
+          k.nsb_y = (uint8_t)c.num_sb_y;
+          std::memcpy(heads + i * sizeof(CuCompact), &k, sizeof k);
+        } else {
+          std::memcpy(heads + i * kCuHeadBytes, &c, kCuHeadBytes);
+        }
         // only sub-block grids, TB splits and 64-sample TU tiling put edges inside a CU
         if (c.has_num_sb || c.has_tb_split || (c.has_tu64 && std::max(c.w, c.h) > 64))
           w.max_cu_dim = std::max(w.max_cu_dim, std::max(c.w, c.h));
@@ -1033,6 +1065,7 @@ DeviceWalkIn device_walk_in(const uint8_t *base, const Staged &st, const DbSide 
   DeviceWalkIn in = db.dw;
   in.heads[0] = base + st.dw_cus;
   in.heads[1] = db.dw_sep ? base + st.dw_ccus : in.heads[0];
+  if (!db.dw_sep) in.compact[1] = in.compact[0];
   for (int l = 0; l < 2; ++l) in.tails[l] = reinterpret_cast<const CuTail *>(base + st.dw_tails[db.dw_sep ? l : 0]);
   if (!db.dw_sep) in.n_tails[1] = in.n_tails[0];
   in.mv_cells = db.dw_mv && !db.dw_mv_cu ? reinterpret_cast<const h266_deblock_mv_cell *>(base + st.dw_mv) : nullptr;

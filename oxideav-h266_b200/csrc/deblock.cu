@@ -2318,7 +2318,8 @@ struct CuMotion {
 struct WalkParams {
   h266_deblock_cu *cus[2];  // luma list, chroma list: full records, expanded in the walk's scratch
   uint32_t n[2];
-  const uint8_t *heads[2];  // the staged packed lists (see CuTail, CuMotionRec)
+  const uint8_t *heads[2];  // the staged packed lists (see CuCompact, CuTail, CuMotionRec)
+  int compact[2];
   const CuTail *tails[2];
   uint32_t n_tails[2];
   const CuMotionRec *mv_recs;
@@ -2405,14 +2406,52 @@ __host__ __device__ inline uint32_t unpack_items(const WalkParams &a, int list) 
 // written by one CU: the crate's last-CU-wins rule needs no atomics.)
 __device__ __forceinline__ void unpack_item(const WalkParams &a, int list, uint32_t i) {
   if (i < a.n[list]) {
-    const uint64_t *src = reinterpret_cast<const uint64_t *>(a.heads[list] + (size_t)i * kCuHeadBytes);
-    uint64_t *dst = reinterpret_cast<uint64_t *>(a.cus[list] + i);
-    uint64_t w[kCuHeadBytes / 8];
+    uint32_t cx, cy, cw, ch;
+    if (a.compact[list]) {
+      const uint4 v = reinterpret_cast<const uint4 *>(a.heads[list])[i];
+      h266_deblock_cu &c = a.cus[list][i];
+      cx = v.x & 0xFFFF;
+      cy = v.x >> 16;
+      cw = v.y & 0xFFFF;
+      ch = v.y >> 16;
+      c.x = cx;
+      c.y = cy;
+      c.w = cw;
+      c.h = ch;
+      c.qp_y = (int8_t)(v.z & 0xFF);
+      const int q0 = (int8_t)((v.z >> 8) & 0xFF);
+      c.qp_c[0] = q0 == -128 ? INT32_MIN : q0;
+      c.qp_c[1] = (int8_t)((v.z >> 16) & 0xFF);
+      c.qp_c[2] = (int8_t)(v.z >> 24);
+      const uint32_t f = v.w & 0xFFFF;
+      c.intra = f & 1;
+      c.tu_y_coded = (f >> 1) & 1;
+      c.tu_cb_coded = (f >> 2) & 1;
+      c.tu_cr_coded = (f >> 3) & 1;
+      c.bdpcm_luma = (f >> 4) & 1;
+      c.bdpcm_chroma = (f >> 5) & 1;
+      c.plt = (f >> 6) & 1;
+      c.joint_cbcr2 = (f >> 7) & 1;
+      c.ciip = (f >> 8) & 1;
+      c.ibc = (f >> 9) & 1;
+      c.has_num_sb = (f >> 10) & 1;
+      c.has_tu64 = (f >> 11) & 1;
+      c.has_tb_split = (f >> 12) & 1;
+      c.num_sb_x = (v.w >> 16) & 0xFF;
+      c.num_sb_y = v.w >> 24;
+    } else {
+      const uint64_t *src = reinterpret_cast<const uint64_t *>(a.heads[list] + (size_t)i * kCuHeadBytes);
+      uint64_t *dst = reinterpret_cast<uint64_t *>(a.cus[list] + i);
+      uint64_t w[kCuHeadBytes / 8];
 #pragma unroll
-    for (int k = 0; k < (int)(kCuHeadBytes / 8); ++k) w[k] = src[k];
+      for (int k = 0; k < (int)(kCuHeadBytes / 8); ++k) w[k] = src[k];
 #pragma unroll
-    for (int k = 0; k < (int)(kCuHeadBytes / 8); ++k) dst[k] = w[k];
-    const uint32_t cx = (uint32_t)w[0], cy = (uint32_t)(w[0] >> 32), cw = (uint32_t)w[1], ch = (uint32_t)(w[1] >> 32);
+      for (int k = 0; k < (int)(kCuHeadBytes / 8); ++k) dst[k] = w[k];
+      cx = (uint32_t)w[0];
+      cy = (uint32_t)(w[0] >> 32);
+      cw = (uint32_t)w[1];
+      ch = (uint32_t)(w[1] >> 32);
+    }
     const int x0 = cx / 4, y0 = cy / 4;
     const int x1 = min((int)((cx + cw + 3) / 4), a.cw4), y1 = min((int)((cy + ch + 3) / 4), a.ch4);
     for (int y = y0; y < y1; ++y)
@@ -2537,6 +2576,7 @@ void fill_walk(const DeviceWalkIn &in, uint8_t *scratch, WalkParams &a, DeviceWa
   a.n[1] = (uint32_t)(sep ? in.n_chroma : in.n_cus);
   for (int l = 0; l < 2; ++l) {
     a.heads[l] = in.heads[sep ? l : 0];
+    a.compact[l] = in.compact[sep ? l : 0] ? 1 : 0;
     a.tails[l] = in.tails[sep ? l : 0];
     a.n_tails[l] = (uint32_t)in.n_tails[sep ? l : 0];
   }

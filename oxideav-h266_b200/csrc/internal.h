@@ -202,6 +202,18 @@ int device_walk_mode(const h266_picture &pic, const h266_deblock_cu *cus, uint64
 constexpr size_t kCuHeadBytes = 56;
 static_assert(offsetof(h266_deblock_cu, tu64) == kCuHeadBytes, "CU head layout");
 static_assert(sizeof(h266_deblock_cu) == kCuHeadBytes + 40, "CU tail layout");
+// The compact head (16 bytes) used when every CU of a list fits it: 16-bit
+// position and size, 8-bit QPs (qp_c[0] -128: the legacy sentinel, the other
+// two then unused), the CU's flags as bits (every use of them is boolean),
+// 8-bit sub-block counts.
+struct CuCompact {
+  uint16_t x, y, w, h;
+  int8_t qp_y, qp_c[3];
+  uint16_t flags;  // bit order: intra, tu_y/cb/cr_coded, bdpcm_luma/chroma, plt, joint_cbcr2, ciip, ibc,
+                   // has_num_sb, has_tu64, has_tb_split
+  uint8_t nsb_x, nsb_y;
+};
+static_assert(sizeof(CuCompact) == 16, "compact CU head");
 struct CuTail {
   uint32_t index;
   uint8_t tail[40];  // bytes [kCuHeadBytes, sizeof(h266_deblock_cu)) of the CU
@@ -212,6 +224,7 @@ struct CuMotionRec {
 };
 struct DeviceWalkIn {  // device pointers
   const uint8_t *heads[2];  // packed CU heads: luma list, chroma list (== heads[0] for a single tree)
+  bool compact[2];          // the list's heads are CuCompact records (else kCuHeadBytes each)
   const CuTail *tails[2];
   uint64_t n_tails[2];
   uint64_t n_cus, n_chroma;
