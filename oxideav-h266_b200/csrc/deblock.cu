@@ -1577,13 +1577,15 @@ __global__ void __launch_bounds__(128, 8) k_deblock_cols(StripParams a) {
 
 // ------------------------------------------------------------ tile kernel
 // One CTA per 64x64 luma tile and its 32x32 chroma tiles.  The tile's region
-// -- the tile widened by the halo, clipped to the plane -- is loaded once
-// (luma through the LMCS LUT), the vertical-pass components that reach the
+// -- the tile widened by the halo -- is staged once by TMA box loads (luma
+// then through the LMCS LUT in shared memory) while the tile's components are
+// staged in shared memory; the vertical-pass components that reach the
 // tile's columns in the widened rows run, then the horizontal-pass components
 // that reach the tile, and the tile itself is stored.  A component that two
 // tiles need runs in both on the same samples, so no CTA reads another's
-// output.  Components span at most the halo (checked on the host), so every
-// clamped read of a listed component stays inside the region.
+// output.  Components span at most the halo (checked on the host, or by
+// construction for the device walk's pictures), so every clamped read of a
+// listed component stays inside the region.
 constexpr int kTileThreads = 256;
 constexpr int kRegionY = kDeblockTile + 2 * kDeblockHaloY;      // 96
 constexpr int kRegionC = kDeblockTile / 2 + 2 * kDeblockHaloC;  // 48
