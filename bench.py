@@ -719,6 +719,20 @@ def run_recon_io(ctx, local_rank, stream, steps: int, peak_gbs: float):
     return out
 
 
+def run_recon_only(args, local_rank):
+    """The recon_io leg alone, --steps calls per entry (a profiling target)."""
+    import torch
+
+    from oxideav_h266_b200 import native
+
+    torch.cuda.set_device(local_rank)
+    ctx = native.Context(local_rank)
+    stream = torch.cuda.Stream(device=local_rank)
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    print(json.dumps(run_recon_io(ctx, local_rank, stream, args.steps, measured_peaks()[0]["hbm_gbs"])), flush=True)
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -1006,6 +1020,8 @@ def main():
     ap.add_argument("--trials", type=int, default=1, help="measure the encoder ALF trial decision (0: skip)")
     ap.add_argument("--served-seconds", type=float, default=2.0,
                     help="seconds of Poisson arrivals per served measurement (0: skip)")
+    ap.add_argument("--recon-only", action="store_true",
+                    help="time only the recon-side calls (forward map, residual add, dump) and print their JSON")
     args = ap.parse_args()
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         # one process per GPU: relaunch this command under torch.distributed.run
@@ -1021,7 +1037,9 @@ def main():
         print(f"bench: --gpus {args.gpus} but WORLD_SIZE={world}; running {world} replicas", file=sys.stderr)
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     _import_pkg()
-    if args.impl == "reference":
+    if args.recon_only:
+        run_recon_only(args, local_rank)
+    elif args.impl == "reference":
         run_reference(args, rank, world)
     else:
         run_ours(args, rank, world, local_rank)

@@ -77,6 +77,29 @@ struct Staging {
   }
 };
 
+// Device scratch that the kernels using it hand back in its resting state
+// (counters at zero, owners cleared): filled on allocation and after a call
+// that did not complete, not on every call.
+struct CleanBuf {
+  DevBuf buf;
+  bool clean = false;
+  // Room for `bytes`, resting (all zero) on the stream; resting again only
+  // once the caller reports a completed call with done().
+  int ensure(size_t bytes, cudaStream_t st) {
+    const size_t cap = buf.cap;
+    H266_TRY(buf.ensure(bytes));
+    if (buf.cap != cap) clean = false;
+    if (!clean) H266_CUDA(cudaMemsetAsync(buf.ptr, 0, buf.cap, st));
+    clean = false;
+    return H266_OK;
+  }
+  void done() { clean = true; }
+  void release() {
+    buf.release();
+    clean = false;
+  }
+};
+
 }  // namespace h266
 
 using namespace h266;
@@ -94,6 +117,11 @@ struct Lane {
   DevBuf io[3];       // device copies of host pictures
   DevBuf scratch[3];  // deblocked planes read by the SAO / ALF pass
   DevBuf lut;         // LMCS inverse LUT
+  DevBuf fwd_lut;     // LMCS forward LUT of fwd_key (valid when fwd_ok)
+  h266_lmcs_derived fwd_key{};
+  bool fwd_ok = false;
+  CleanBuf fwd_cover;  // forward map: error word, then the coverage counters
+  CleanBuf res_cover;  // residual add: overlap word, then the Cb and Cr cell owners
   DevBuf side;        // side information
   DevBuf walk;        // CU maps and segment grids of device-built side information
   Staging stage;
@@ -115,6 +143,10 @@ struct Lane {
       scratch[i].release();
     }
     lut.release();
+    fwd_lut.release();
+    fwd_ok = false;
+    fwd_cover.release();
+    res_cover.release();
     side.release();
     walk.release();
     if (stage.ptr) cudaFreeHost(stage.ptr);
@@ -244,6 +276,8 @@ struct h266_ctx {
   std::atomic<int64_t> host_ns[3] = {{0}, {0}, {0}};
   uint64_t prof_n[H266_PROF_FAMILIES] = {0};
   h266::BatchBufs batch;  // parameter tables of h266_chain_plan_execute_batch
+  std::vector<h266::RectPiece> fwd_pieces;  // forward-map pieces (capacity kept between calls)
+  std::vector<h266::ResPiece> res_pieces;   // residual-add pieces (capacity kept between calls)
   std::vector<std::unique_ptr<h266::GroupLane>> glanes;  // the end-to-end batch pipeline
   cudaStream_t e2e_up = nullptr, e2e_down = nullptr;      // its copy streams
   bool force_scalar = false;  // H266_FORCE_SCALAR_ALF=1: scalar SAO/ALF kernel (cross-checks)
@@ -393,6 +427,20 @@ int upload_blob(Lane &ln, const std::vector<uint8_t> &blob, uint8_t **dev_base) 
   H266_TRY(ln.stage.ensure(n));
   std::memcpy(ln.stage.ptr, blob.data(), n);
   H266_CUDA(cudaMemcpyAsync(ln.side.ptr, ln.stage.ptr, n, cudaMemcpyHostToDevice, ln.stream));
+  H266_CUDA(cudaEventRecord(ln.staged, ln.stream));
+  *dev_base = ln.side.as<uint8_t>();
+  return H266_OK;
+}
+
+// The same from caller memory, copied once into the staging buffer.
+int upload_raw(Lane &ln, const void *p, size_t n, uint8_t **dev_base) {
+  H266_TRY(ln.side.ensure(std::max<size_t>(n, 1)));
+  H266_CUDA(cudaEventSynchronize(ln.staged));
+  H266_TRY(ln.stage.ensure(std::max<size_t>(n, 1)));
+  if (n) {
+    std::memcpy(ln.stage.ptr, p, n);
+    H266_CUDA(cudaMemcpyAsync(ln.side.ptr, ln.stage.ptr, n, cudaMemcpyHostToDevice, ln.stream));
+  }
   H266_CUDA(cudaEventRecord(ln.staged, ln.stream));
   *dev_base = ln.side.as<uint8_t>();
   return H266_OK;
@@ -1164,42 +1212,52 @@ namespace {
 // launch works on disjoint rectangles and groups run in list order.
 // Cells are g x g samples, g the coarsest grid every rectangle edge lies on
 // (CU and TB edges: 4 luma / 2 chroma), so the test stays exact.
+// One bit per cell of a grid of 2^sh x 2^sh samples over a plane: the
+// rectangles one launch may take in any order are those whose cells are all
+// still clear.
 struct Coverage {
-  uint32_t w = 0, h = 0, wpr = 0, g = 1;
+  uint32_t wpr = 0, sh = 0;
   std::vector<uint64_t> bits;
-  void reset(uint32_t w_, uint32_t h_, uint32_t g_) {
-    g = g_;
-    w = (w_ + g - 1) / g;
-    h = (h_ + g - 1) / g;
-    wpr = (w + 63) / 64;
-    bits.assign((size_t)wpr * h, 0);
+  void reset(uint32_t w, uint32_t h, uint32_t sh_) {
+    sh = sh_;
+    const uint32_t g = 1u << sh;
+    wpr = (((w + g - 1) >> sh) + 63) / 64;
+    bits.assign((size_t)wpr * ((h + g - 1) >> sh), 0);
   }
   void clear() { std::fill(bits.begin(), bits.end(), 0); }
-  template <class F>
-  bool each(uint32_t x, uint32_t y, uint32_t rw, uint32_t rh, F f) {  // f(word, mask) until it returns true
-    for (uint32_t r = y; r < y + rh; ++r)
-      for (uint32_t wi = x / 64; wi <= (x + rw - 1) / 64; ++wi) {
-        const uint32_t lo = std::max(x, wi * 64) - wi * 64, hi = std::min(x + rw, wi * 64 + 64) - wi * 64;
-        const uint64_t m = (hi - lo == 64 ? ~0ull : (((1ull << (hi - lo)) - 1) << lo));
-        if (f(bits[(size_t)r * wpr + wi], m)) return true;
-      }
-    return false;
-  }
-  bool meets(uint32_t x, uint32_t y, uint32_t rw, uint32_t rh) {  // sample coordinates on the g grid
-    return each(x / g, y / g, (rw + g - 1) / g, (rh + g - 1) / g, [](uint64_t &b, uint64_t m) { return (b & m) != 0; });
-  }
-  void mark(uint32_t x, uint32_t y, uint32_t rw, uint32_t rh) {
-    each(x / g, y / g, (rw + g - 1) / g, (rh + g - 1) / g, [](uint64_t &b, uint64_t m) {
-      b |= m;
-      return false;
-    });
+  // Marks the rectangle's cells and returns true; returns false, marking
+  // nothing, when one of them is marked already.
+  bool claim(uint32_t x, uint32_t y, uint32_t rw, uint32_t rh) {
+    const uint32_t g = 1u << sh;
+    const uint32_t cx = x >> sh, cw = (rw + g - 1) >> sh, ch = (rh + g - 1) >> sh;
+    const uint32_t w0 = cx >> 6, w1 = (cx + cw - 1) >> 6;
+    uint64_t *row = bits.data() + (size_t)(y >> sh) * wpr;
+    auto mask = [&](uint32_t wi) {
+      const uint32_t lo = std::max(cx, wi * 64) - wi * 64, hi = std::min(cx + cw, wi * 64 + 64) - wi * 64;
+      return hi - lo == 64 ? ~0ull : (((1ull << (hi - lo)) - 1) << lo);
+    };
+    if (w0 == w1) {  // the common case: one word per row
+      const uint64_t m = mask(w0);
+      uint64_t hit = 0;
+      for (uint32_t r = 0; r < ch; ++r) hit |= row[(size_t)r * wpr + w0] & m;
+      if (hit) return false;
+      for (uint32_t r = 0; r < ch; ++r) row[(size_t)r * wpr + w0] |= m;
+      return true;
+    }
+    for (uint32_t r = 0; r < ch; ++r)
+      for (uint32_t wi = w0; wi <= w1; ++wi)
+        if (row[(size_t)r * wpr + wi] & mask(wi)) return false;
+    for (uint32_t r = 0; r < ch; ++r)
+      for (uint32_t wi = w0; wi <= w1; ++wi) row[(size_t)r * wpr + wi] |= mask(wi);
+    return true;
   }
 };
 
-// The coarsest of 4, 2, 1 dividing every value folded into `acc` (an OR).
-uint32_t grid_of(uint32_t acc) { return (acc & 3) == 0 ? 4 : ((acc & 1) == 0 ? 2 : 1); }
+// log2 of the coarsest of 4, 2, 1 dividing every value folded into `acc` (an OR).
+uint32_t grid_shift(uint32_t acc) { return (acc & 3) == 0 ? 2 : ((acc & 1) == 0 ? 1 : 0); }
 
-constexpr uint32_t kPieceSamples = 4096;
+constexpr uint32_t kPieceSamples = 1024;  // residual-add piece
+constexpr uint32_t kPieceCells = 1024;    // forward-map count piece
 
 h266_picture plane_view(const h266_picture &pic, int keep) {  // the picture with only plane `keep` (-1: chroma)
   h266_picture v = pic;
@@ -1794,66 +1852,74 @@ int h266_lmcs_forward_map_luma_rects(h266_ctx *ctx, h266_picture *pic, const h26
   H266_TRY(check_lmcs(lmcs, 0, 0));
   if (n && !rects) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL rects with nonzero length");
   const uint32_t W = pic->luma.width, H = pic->luma.height;
-  std::vector<RectPiece> pieces;
-  std::vector<uint32_t> group_end;
-  auto clipped = [&](const h266_rect &r, uint32_t &rw, uint32_t &rh) {  // clipped as src/ctu.rs:1718-1719
-    if (r.x >= W || r.y >= H || !r.w || !r.h) return false;
-    rw = (uint32_t)std::min<uint64_t>((uint64_t)r.x + r.w, W) - r.x;
-    rh = (uint32_t)std::min<uint64_t>((uint64_t)r.y + r.h, H) - r.y;
-    return true;
-  };
-  uint32_t acc = 0;
-  for (uint64_t i = 0; i < n; ++i) {
-    uint32_t rw, rh;
-    if (clipped(rects[i], rw, rh)) acc |= rects[i].x | rects[i].y | (rects[i].x + rw) | (rects[i].y + rh);
-  }
-  Coverage cov;
-  cov.reset(W, H, grid_of(acc));
+  // Rectangles clipped as src/ctu.rs:1718-1719; the grid is the coarsest that
+  // every clipped edge lies on, the span box their union's bounds.
+  std::vector<RectPiece> &pieces = ctx->fwd_pieces;
+  pieces.clear();
+  pieces.reserve(n);
+  uint32_t acc = 0, x0 = W, y0 = H, x1 = 0, y1 = 0;
   for (uint64_t i = 0; i < n; ++i) {
     const h266_rect &r = rects[i];
-    uint32_t rw, rh;
-    if (!clipped(r, rw, rh)) continue;
-    if (cov.meets(r.x, r.y, rw, rh)) {
-      group_end.push_back((uint32_t)pieces.size());
-      cov.clear();
-    }
-    cov.mark(r.x, r.y, rw, rh);
-    const uint32_t rows = std::max<uint32_t>(1, kPieceSamples / rw);
-    for (uint32_t y = 0; y < rh; y += rows) pieces.push_back(RectPiece{r.x, r.y + y, rw, std::min(rows, rh - y)});
+    if (r.x >= W || r.y >= H || !r.w || !r.h) continue;
+    const uint32_t rw = (uint32_t)std::min<uint64_t>((uint64_t)r.x + r.w, W) - r.x;
+    const uint32_t rh = (uint32_t)std::min<uint64_t>((uint64_t)r.y + r.h, H) - r.y;
+    acc |= r.x | r.y | (r.x + rw) | (r.y + rh);
+    x0 = std::min(x0, r.x);
+    y0 = std::min(y0, r.y);
+    x1 = std::max(x1, r.x + rw);
+    y1 = std::max(y1, r.y + rh);
+    pieces.push_back(RectPiece{r.x, r.y, rw, rh});
   }
-  group_end.push_back((uint32_t)pieces.size());
+  const uint32_t sh = grid_shift(acc);
+  // Pieces of at most kPieceCells cells, split at rows of the grid.
+  for (size_t i = 0, e = pieces.size(); i < e; ++i) {
+    RectPiece &r = pieces[i];
+    const uint32_t cols = r.w >> sh, rows = r.h >> sh;
+    if ((uint64_t)cols * rows <= kPieceCells) continue;
+    const uint32_t step = std::max<uint32_t>(1, kPieceCells / cols) << sh;
+    for (uint32_t y = step; y < r.h; y += step)
+      pieces.push_back(RectPiece{r.x, r.y + y, r.w, std::min(step, r.h - y)});
+    pieces[i].h = step;
+  }
   Guard g(ctx->device);
   Lane &ln = ctx->main;
   const h266_picture lv = plane_view(*pic, 0);
   DPlane P[3];
   H266_TRY(picture_to_device(ln, lv, P));
   ctx->h2d_bytes += host_plane_bytes(lv);
-  H266_TRY(ln.lut.ensure(65536 * 2));
-  H266_TRY(launch_lmcs_fwd_lut(ln.stream, ln.lut.as<uint16_t>(), *lmcs, &ctx->launches));
-  Prep &pr = ctx_prep(ctx, 0);
-  pr.blob.clear();
-  Blob blob{pr.blob};
-  const size_t off = blob.put(pieces.data(), pieces.size() * sizeof(RectPiece));
+  const bool fresh = ln.fwd_ok && std::memcmp(&ln.fwd_key, lmcs, sizeof *lmcs) == 0;
+  if (!fresh) {  // the table is rebuilt only when the LMCS parameters change
+    ln.fwd_ok = false;
+    H266_TRY(ln.fwd_lut.ensure(65536 * 2));
+    H266_TRY(launch_lmcs_fwd_lut(ln.stream, ln.fwd_lut.as<uint16_t>(), *lmcs, &ctx->launches));
+  }
   uint8_t *base = nullptr;
-  H266_TRY(upload_blob(ln, pr.blob, &base));
-  ctx->h2d_bytes += pr.blob.size();
-  H266_TRY(ln.walk.ensure(16));
-  uint32_t *d_err = ln.walk.as<uint32_t>();
-  H266_CUDA(cudaMemsetAsync(d_err, 0, 4, ln.stream));
+  H266_TRY(upload_raw(ln, pieces.data(), pieces.size() * sizeof(RectPiece), &base));
+  ctx->h2d_bytes += pieces.size() * sizeof(RectPiece);
+  FwdCover cov{};
+  cov.sh = sh;
+  cov.pitch = (W + (1u << sh) - 1) >> sh;
+  const size_t cells = (size_t)cov.pitch * ((H + (1u << sh) - 1) >> sh);
+  cov.x0 = x0;
+  cov.y0 = y0;
+  cov.x1 = x1;
+  cov.y1 = y1;
+  H266_TRY(ln.fwd_cover.ensure(16 + cells * 4, ln.stream));
+  uint32_t *d_err = ln.fwd_cover.buf.as<uint32_t>();
+  cov.cnt = d_err + 4;
   {
     Prof pf(ctx, ln.stream, H266_PROF_LMCS);
-    uint32_t g0 = 0;
-    for (uint32_t ge : group_end) {
-      H266_TRY(launch_lmcs_fwd_rects(ln.stream, P[0], ln.lut.as<uint16_t>(),
-                                     reinterpret_cast<const RectPiece *>(base + off) + g0, ge - g0,
-                                     lmcs->bit_depth < 16, d_err, &ctx->launches));
-      g0 = ge;
-    }
+    H266_TRY(launch_lmcs_fwd_cover(ln.stream, P[0], ln.fwd_lut.as<uint16_t>(),
+                                   reinterpret_cast<const RectPiece *>(base), (uint32_t)pieces.size(), cov,
+                                   lmcs->bit_depth < 16, d_err, &ctx->launches));
   }
   H266_TRY(picture_from_device(ln, lv, false));
   ctx->d2h_bytes += host_plane_bytes(lv);
   uint32_t err = 0;
   H266_TRY(sync_read(ln, &err, d_err, 4));
+  ln.fwd_key = *lmcs;
+  ln.fwd_ok = true;
+  if (!err) ln.fwd_cover.done();  // counters back at zero (a raised error word is cleared by the next call's fill)
   if (err) return set_error(H266_ERR_INVALID_ARGUMENT, "forward LMCS: a sample above (1 << BitDepth) - 1 has no bin");
   return H266_OK;
 }
@@ -1912,14 +1978,10 @@ int h266_lmcs_add_chroma_residual(h266_ctx *ctx, h266_picture *pic, uint32_t bd,
   H266_TRY(check_picture(pic));
   if (bd < 8 || bd > 16) return set_error(H266_ERR_INVALID_ARGUMENT, "bit_depth must be 8..16");
   if (n && (!blocks || !res)) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL blocks / residuals");
+  if (n >= 0xFFFFFFFFull) return set_error(H266_ERR_UNSUPPORTED, "too many residual blocks");
   const h266_plane *cp[2] = {&pic->cb, &pic->cr};
-  uint32_t acc = 0;
-  for (uint64_t i = 0; i < n; ++i) acc |= blocks[i].x | blocks[i].y | blocks[i].w | blocks[i].h;
-  Coverage cov[2];
-  cov[0].reset(pic->cb.width, pic->cb.height, grid_of(acc));
-  cov[1].reset(pic->cr.width, pic->cr.height, grid_of(acc));
-  std::vector<ResPiece> pieces;
-  std::vector<uint32_t> group_end;
+  uint32_t acc = 0, bx0[2] = {UINT32_MAX, UINT32_MAX}, by0[2] = {UINT32_MAX, UINT32_MAX}, bx1[2] = {0, 0},
+           by1[2] = {0, 0};
   for (uint64_t i = 0; i < n; ++i) {
     const h266_chroma_res_block &b = blocks[i];
     if (b.plane != 1 && b.plane != 2) return set_error(H266_ERR_INVALID_ARGUMENT, "residual block plane must be 1 or 2");
@@ -1929,20 +1991,15 @@ int h266_lmcs_add_chroma_residual(h266_ctx *ctx, h266_picture *pic, uint32_t bd,
       return set_error(H266_ERR_INVALID_ARGUMENT, "chroma TB does not fit in the plane");
     if (b.res_offset > n_res || (uint64_t)b.w * b.h > n_res - b.res_offset)
       return set_error(H266_ERR_INVALID_ARGUMENT, "chroma TB residuals run past n_res");
+    acc |= b.x | b.y | b.w | b.h;
     if (!b.w || !b.h) continue;
-    Coverage &c = cov[b.plane - 1];
-    if (c.meets(b.x, b.y, b.w, b.h)) {
-      group_end.push_back((uint32_t)pieces.size());
-      cov[0].clear();
-      cov[1].clear();
-    }
-    c.mark(b.x, b.y, b.w, b.h);
-    const uint32_t rows = std::max<uint32_t>(1, kPieceSamples / b.w);
-    for (uint32_t y = 0; y < b.h; y += rows)
-      pieces.push_back(ResPiece{b.x, b.y + y, b.w, std::min(rows, b.h - y), b.plane, b.var_scale,
-                                b.res_offset + (uint64_t)y * b.w, b.w, 0});
+    const int k = b.plane - 1;
+    bx0[k] = std::min(bx0[k], b.x);
+    by0[k] = std::min(by0[k], b.y);
+    bx1[k] = std::max(bx1[k], b.x + b.w);
+    by1[k] = std::max(by1[k], b.y + b.h);
   }
-  group_end.push_back((uint32_t)pieces.size());
+  const uint32_t sh = grid_shift(acc);
   Guard g(ctx->device);
   Lane &ln = ctx->main;
   const h266_picture cv = plane_view(*pic, -1);
@@ -1956,19 +2013,74 @@ int h266_lmcs_add_chroma_residual(h266_ctx *ctx, h266_picture *pic, uint32_t bd,
     d_res = ln.scratch[0].as<int32_t>();
     ctx->h2d_bytes += n_res * 4;
   }
-  Prep &pr = ctx_prep(ctx, 0);
-  pr.blob.clear();
-  Blob blob{pr.blob};
-  const size_t off = blob.put(pieces.data(), pieces.size() * sizeof(ResPiece));
+  // Pairwise disjoint TBs (the usual list) take one owner pass and one add
+  // pass in any order; the device reports an overlap, and then the add runs
+  // as ordered launches of disjoint TBs instead.
   uint8_t *base = nullptr;
-  H266_TRY(upload_blob(ln, pr.blob, &base));
-  ctx->h2d_bytes += pr.blob.size();
+  H266_TRY(upload_raw(ln, blocks, n * sizeof(h266_chroma_res_block), &base));
+  ctx->h2d_bytes += n * sizeof(h266_chroma_res_block);
+  ResCover c{};
+  c.sh = sh;
+  size_t cells[2];
+  for (int k = 0; k < 2; ++k) {
+    const uint32_t gsz = 1u << sh;
+    c.pitch[k] = (cp[k]->width + gsz - 1) >> sh;
+    cells[k] = (size_t)c.pitch[k] * ((cp[k]->height + gsz - 1) >> sh);
+    c.x0[k] = bx1[k] ? bx0[k] : 0;
+    c.y0[k] = by1[k] ? by0[k] : 0;
+    c.x1[k] = bx1[k];
+    c.y1[k] = by1[k];
+  }
+  H266_TRY(ln.res_cover.ensure(16 + (cells[0] + cells[1]) * 4, ln.stream));
+  uint32_t *d_overlap = ln.res_cover.buf.as<uint32_t>();
+  c.own[0] = d_overlap + 4;
+  c.own[1] = c.own[0] + cells[0];
+  {
+    Prof pf(ctx, ln.stream, H266_PROF_LMCS);
+    H266_TRY(launch_chroma_residual_cover(ln.stream, P[1], P[2], reinterpret_cast<const h266_chroma_res_block *>(base),
+                                          (uint32_t)n, d_res, (int)bd, c, d_overlap, &ctx->launches));
+  }
+  H266_TRY(picture_from_device(ln, cv, false));
+  uint32_t overlap = 0;
+  H266_TRY(sync_read(ln, &overlap, d_overlap, 4));
+  ctx->d2h_bytes += host_plane_bytes(cv);
+  if (!overlap) {
+    ln.res_cover.done();  // owners cleared by the add pass
+    return H266_OK;
+  }
+  // Ordered launches: the host splits the list into runs of pairwise
+  // disjoint TBs with a coverage bitmap; the planes are as they came in.
+  Coverage cov[2];
+  cov[0].reset(pic->cb.width, pic->cb.height, sh);
+  cov[1].reset(pic->cr.width, pic->cr.height, sh);
+  std::vector<ResPiece> &pieces = ctx->res_pieces;
+  pieces.clear();
+  pieces.reserve(n);
+  std::vector<uint32_t> group_end;
+  for (uint64_t i = 0; i < n; ++i) {
+    const h266_chroma_res_block &b = blocks[i];
+    if (!b.w || !b.h) continue;
+    Coverage &cc = cov[b.plane - 1];
+    if (!cc.claim(b.x, b.y, b.w, b.h)) {  // overlaps a TB of the open launch: a new launch, in list order
+      group_end.push_back((uint32_t)pieces.size());
+      cov[0].clear();
+      cov[1].clear();
+      cc.claim(b.x, b.y, b.w, b.h);
+    }
+    const uint32_t rows = std::max<uint32_t>(1, kPieceSamples / b.w);
+    for (uint32_t y = 0; y < b.h; y += rows)
+      pieces.push_back(ResPiece{b.x, b.y + y, b.w, std::min(rows, b.h - y), b.plane, b.var_scale,
+                                b.res_offset + (uint64_t)y * b.w, b.w, 0});
+  }
+  group_end.push_back((uint32_t)pieces.size());
+  H266_TRY(upload_raw(ln, pieces.data(), pieces.size() * sizeof(ResPiece), &base));
+  ctx->h2d_bytes += pieces.size() * sizeof(ResPiece);
   {
     Prof pf(ctx, ln.stream, H266_PROF_LMCS);
     uint32_t g0 = 0;
     for (uint32_t ge : group_end) {
-      H266_TRY(launch_chroma_residual(ln.stream, P[1], P[2], reinterpret_cast<const ResPiece *>(base + off) + g0,
-                                      ge - g0, d_res, (int)bd, &ctx->launches));
+      H266_TRY(launch_chroma_residual(ln.stream, P[1], P[2], reinterpret_cast<const ResPiece *>(base) + g0, ge - g0,
+                                      d_res, (int)bd, &ctx->launches));
       g0 = ge;
     }
   }

@@ -358,10 +358,18 @@ int pass2_wait_timeouts(uint32_t *count);
 int launch_pass2_packed(cudaStream_t st, const Pass2Args &a, bool do_sao, bool do_alf, uint64_t *launches);
 
 // ---------------------------------------------------------------- recon-side LMCS, output dump (recon.cu)
-struct RectPiece {  // a piece of a forward-map rectangle: <= 4096 samples, inside the plane
+struct RectPiece {  // a piece of a forward-map rectangle, inside the plane, on whole coverage cells
   uint32_t x, y, w, h;
 };
-struct ResPiece {  // a piece of a chroma TB's residual add
+// How many of a call's rectangles cover each cell of a grid of 2^sh x 2^sh
+// luma samples (every rectangle edge of the call lies on the grid), and the
+// box the rectangles span.
+struct FwdCover {
+  uint32_t *cnt;       // pitch x ceil(height / 2^sh) counters: zero before the count launch, zero again after the apply launch
+  uint32_t pitch, sh;  // counters per row, grid shift
+  uint32_t x0, y0, x1, y1;
+};
+struct ResPiece {  // a piece of a chroma TB's residual add: <= 1024 samples
   uint32_t x, y, w, h;
   uint32_t plane, var_scale;
   uint64_t res_offset;  // residual of (x, y)
@@ -377,8 +385,28 @@ struct OutPlanes {
   uint64_t n[3], total;  // output samples per plane, and in all
 };
 int launch_lmcs_fwd_lut(cudaStream_t st, uint16_t *d_lut, const h266_lmcs_derived &l, uint64_t *launches);
-int launch_lmcs_fwd_rects(cudaStream_t st, DPlane p, const uint16_t *d_lut, const RectPiece *d_pieces, uint32_t n,
-                          bool check, uint32_t *d_err, uint64_t *launches);
+// The forward map of a rectangle list in two launches: the coverage count of
+// every cell (one warp per piece), then one pass over the span box mapping
+// each sample as many times as rectangles cover it.
+int launch_lmcs_fwd_cover(cudaStream_t st, DPlane p, const uint16_t *d_lut, const RectPiece *d_pieces, uint32_t n,
+                          const FwdCover &c, bool check, uint32_t *d_err, uint64_t *launches);
+// The chroma TBs of a residual-add call on a grid of 2^sh x 2^sh chroma
+// samples (every TB edge of the call lies on it): per plane the owner of
+// each cell (TB index + 1, 0 none) and the box the plane's TBs span.
+struct ResCover {
+  uint32_t *own[2];  // Cb, Cr: pitch x ceil(height / 2^sh) owners, all 0 between calls
+  uint32_t pitch[2], sh;
+  uint32_t x0[2], y0[2], x1[2], y1[2];
+};
+// The residual add in two launches when the call's TBs are pairwise
+// disjoint: the owner of every cell (one warp per TB; a cell claimed twice
+// raises *overlap), then one pass over each plane's box adding each
+// sample's residual; with *overlap raised the pass returns at once, leaving
+// the planes as they were (and the owners set) for the ordered launches of
+// launch_chroma_residual.
+int launch_chroma_residual_cover(cudaStream_t st, DPlane cb, DPlane cr, const h266_chroma_res_block *d_blocks,
+                                 uint32_t n, const int32_t *d_res, int bd, const ResCover &c, uint32_t *d_overlap,
+                                 uint64_t *launches);
 int launch_lmcs_cvs(cudaStream_t st, DPlane luma, const h266_lmcs_cvs_block *d_blocks, uint32_t n, int size_y,
                     const CvsTables &t, uint32_t *d_out, uint64_t *launches);
 int launch_chroma_residual(cudaStream_t st, DPlane cb, DPlane cr, const ResPiece *d_pieces, uint32_t n,

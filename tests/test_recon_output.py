@@ -74,6 +74,36 @@ def res_case(seed, cw, ch, n, bd):
     return b, res
 
 
+def res_tiling(seed, cw, ch, bd):
+    """Disjoint chroma TBs covering both planes (a quadtree over 32x32 blocks,
+    leaves clipped to the plane), in a shuffled order, with their residuals."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    leaves = []
+
+    def split(x, y, s, plane):
+        if x >= cw or y >= ch:
+            return
+        if s > 4 and rng.random() < 0.55:
+            for dy in (0, s // 2):
+                for dx in (0, s // 2):
+                    split(x + dx, y + dy, s // 2, plane)
+            return
+        leaves.append((x, y, min(s, cw - x), min(s, ch - y), plane))
+    for plane in (1, 2):
+        for y in range(0, ch, 32):
+            for x in range(0, cw, 32):
+                split(x, y, 32, plane)
+    order = rng.permutation(len(leaves))
+    b = np.zeros(len(leaves), dtype=abi.RES_BLOCK)
+    off = 0
+    for i, k in enumerate(order):
+        x, y, w, h, plane = leaves[k]
+        b[i] = (x, y, w, h, plane, abi.NO_VAR_SCALE if i % 3 == 0 else int(rng.integers(512, 16384)), off)
+        off += w * h
+    res = rng.integers(-(2 << bd), 2 << bd, size=off, dtype=np.int32)
+    return b, res
+
+
 def dump_numpy(pic, crop, cfi, bd):
     """The dump layout restated with numpy (examples/decode_dump.rs:24-40)."""
     x, y, w, h = crop
@@ -245,6 +275,68 @@ def test_gpu_chroma_residual(ctx, bd):
     native.lmcs_add_chroma_residual(ctx, got, bd, res, b)
     assert np.array_equal(got.cb, want.cb) and np.array_equal(got.cr, want.cr)
     assert np.array_equal(got.luma, pic.luma)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("size", [(832, 480), (418, 242), (1920, 1080)])
+@pytest.mark.parametrize("device", [False, True])
+def test_gpu_chroma_residual_disjoint(ctx, size, device):
+    """Disjoint TBs (the single owner pass and add pass), on host and device
+    pictures; 418x242 gives odd chroma edges (a 1-sample grid)."""
+    import torch
+    from oxideav_h266_b200 import native
+    bd = 10
+    pic = picture(80 + size[0], size[0], size[1], bd)
+    b, res = res_tiling(81 + size[0], pic.cb.shape[1], pic.cb.shape[0], bd)
+    want = pic.copy()
+    oracle.lmcs_add_chroma_residual(want, bd, res, b)
+    if device:
+        dp = native.DevicePicture.from_host(pic)
+        native.lmcs_add_chroma_residual(ctx, dp, bd, torch.tensor(res, device="cuda"), b)
+        torch.cuda.synchronize()
+        got = dp.to_host()
+    else:
+        got = pic.copy()
+        native.lmcs_add_chroma_residual(ctx, got, bd, res, b)
+    assert np.array_equal(got.cb, want.cb) and np.array_equal(got.cr, want.cr)
+    assert np.array_equal(got.luma, pic.luma)
+
+
+@pytest.mark.gpu
+def test_gpu_recon_call_sequences(ctx):
+    """Calls that switch between the single-pass and the ordered forms, grids
+    and picture sizes on one context, with a failing call in between: each
+    result matches the oracle (the device counters and owners a call uses
+    are left clean for the next one, or refilled after a call that did not
+    complete)."""
+    from oxideav_h266_b200 import native
+    bd = 10
+    d = seeded_lmcs(90)
+    steps = [("fwd", 1920, 1080, False), ("fwd", 416, 240, True), ("fail", 640, 360, None), ("fwd", 1920, 1080, False),
+             ("fwd", 418, 242, True), ("fwd", 640, 360, False), ("res", 832, 480, False), ("res", 832, 480, True),
+             ("res", 418, 242, False), ("fail", 640, 360, None), ("res", 1920, 1080, False), ("fwd", 1920, 1080, False)]
+    for i, (kind, w, h, overlap) in enumerate(steps):
+        pic = picture(100 + i, w, h, bd)
+        if kind == "fail":
+            bad = pic.copy()
+            bad.luma[3, 5] = 1500
+            one = np.zeros(1, dtype=abi.RECT)
+            one[0] = (0, 0, 64, 64)
+            with pytest.raises(native.H266Error):
+                native.lmcs_forward_map_luma_rects(ctx, bad, d, one)
+            continue
+        want, got = pic.copy(), pic.copy()
+        if kind == "fwd":
+            r = rects_case(110 + i, w, h, 300, overlap)
+            assert oracle.lmcs_forward_map_luma_rects(want, d, r) == 0
+            native.lmcs_forward_map_luma_rects(ctx, got, d, r)
+            assert np.array_equal(got.luma, want.luma), i
+        else:
+            cw, ch = pic.cb.shape[1], pic.cb.shape[0]
+            b, res = res_case(120 + i, cw, ch, 600, bd) if overlap else res_tiling(120 + i, cw, ch, bd)
+            oracle.lmcs_add_chroma_residual(want, bd, res, b)
+            native.lmcs_add_chroma_residual(ctx, got, bd, res, b)
+            assert np.array_equal(got.cb, want.cb) and np.array_equal(got.cr, want.cr), i
 
 
 @pytest.mark.gpu
