@@ -608,9 +608,11 @@ int h266_server_destroy(h266_server *server); /* drains the queue first */
  *     H266_ERR_UNSUPPORTED and a message naming both sizes (1920x1080 4:2:0
  *     fits; 3840x2160 does not).
  *   - Every call looks up the array's device address on the current device
- *     (cudaGetSymbolAddress, which allocates nothing).  The first call on a
- *     device also loads the library's device code there, so make that first
- *     call before any stream capture begins.
+ *     (cudaGetSymbolAddress, which allocates nothing).
+ *   - Every call builds the side information on the host and copies it from
+ *     ordinary (pageable) host memory that is gone when the call returns, so
+ *     the call cannot be recorded into a CUDA graph; graph replays of the
+ *     chain are h266_batch_graph_create / h266_batch_graph_launch.
  *   - All calls share the one array and every call overwrites it: calls whose
  *     work overlaps on the GPU (other streams, other threads) race.  Serialize
  *     them on one stream.
