@@ -158,12 +158,12 @@ __device__ __forceinline__ void luma_cells(const uint16_t *sL, uint4 *cell) {
     for (int d = 0; d < 2; ++d) {
       const int r = 2 * cy + d + 1;  // sL row of the position: y = Y0 - 2 + 2cy + d
       const int c = 2 * cx + d + 2;  // sL col: x = X0 - 2 + 2cx + d
-      const uint16_t *row = &sL[r * S::SLW + c];
+      const uint16_t *row = &sL[r * S::SLP + c];
       const int c2 = 2 * row[0];
       g.x += abs(c2 - row[-1] - row[1]);
-      g.y += abs(c2 - row[-S::SLW] - row[S::SLW]);
-      g.z += abs(c2 - row[-S::SLW - 1] - row[S::SLW + 1]);
-      g.w += abs(c2 - row[-S::SLW + 1] - row[S::SLW - 1]);
+      g.y += abs(c2 - row[-S::SLP] - row[S::SLP]);
+      g.z += abs(c2 - row[-S::SLP - 1] - row[S::SLP + 1]);
+      g.w += abs(c2 - row[-S::SLP + 1] - row[S::SLP - 1]);
     }
     cell[i] = g;
   }
@@ -193,7 +193,7 @@ __device__ __forceinline__ void luma_classes(const uint16_t *sL, const uint4 *ce
       int sh = 0, sv = 0, sd0 = 0, sd1 = 0;
       for (int j = min_y; j <= max_y; ++j) {
         const int gy = y_ctb + y4 + j;
-        const uint16_t *rc = &sL[pad(gy) * S::SLW], *ru = &sL[pad(gy - 1) * S::SLW], *rd = &sL[pad(gy + 1) * S::SLW];
+        const uint16_t *rc = &sL[pad(gy) * S::SLP], *ru = &sL[pad(gy - 1) * S::SLP], *rd = &sL[pad(gy + 1) * S::SLP];
         for (int i = (j & 1) ? -1 : -2; i <= 5; i += 2) {
           const int c = 4 * bx + i + 4;
           const int c2 = 2 * rc[c];
@@ -243,10 +243,10 @@ __device__ __forceinline__ void luma_run(const S &sm, int j, int bx, int yr, int
   table45(yr, ctb, shift, y1, y2, y3);
   const int r = j + 3;
   const int c0 = 4 * bx + 4;
-  const uint16_t *R0 = &sm.sL[r * S::SLW];
-  const uint16_t *U1 = R0 - y1 * S::SLW, *D1 = R0 + y1 * S::SLW;
-  const uint16_t *U2 = R0 - y2 * S::SLW, *D2 = R0 + y2 * S::SLW;
-  const uint16_t *U3 = R0 - y3 * S::SLW, *D3 = R0 + y3 * S::SLW;
+  const uint16_t *R0 = &sm.sL[r * S::SLP];
+  const uint16_t *U1 = R0 - y1 * S::SLP, *D1 = R0 + y1 * S::SLP;
+  const uint16_t *U2 = R0 - y2 * S::SLP, *D2 = R0 + y2 * S::SLP;
+  const uint16_t *U3 = R0 - y3 * S::SLP, *D3 = R0 + y3 * S::SLP;
   const uint32_t cur[2] = {pair_at<0>(R0, c0), pair_at<0>(R0, c0 + 2)};
   const uint32_t ncur[2] = {neg2(cur[0]), neg2(cur[1])};
   int acc[4] = {0, 0, 0, 0};
@@ -280,10 +280,10 @@ __device__ __forceinline__ void luma_sums(const S &sm, int j, int bx, int yr, in
   int y1, y2, y3;
   table45(yr, ctb, shift, y1, y2, y3);
   const int c0 = 4 * bx + 4;
-  const uint16_t *R0 = &sm.sL[(j + 3) * S::SLW];
-  const uint16_t *U1 = R0 - y1 * S::SLW, *D1 = R0 + y1 * S::SLW;
-  const uint16_t *U2 = R0 - y2 * S::SLW, *D2 = R0 + y2 * S::SLW;
-  const uint16_t *U3 = R0 - y3 * S::SLW, *D3 = R0 + y3 * S::SLW;
+  const uint16_t *R0 = &sm.sL[(j + 3) * S::SLP];
+  const uint16_t *U1 = R0 - y1 * S::SLP, *D1 = R0 + y1 * S::SLP;
+  const uint16_t *U2 = R0 - y2 * S::SLP, *D2 = R0 + y2 * S::SLP;
+  const uint16_t *U3 = R0 - y3 * S::SLP, *D3 = R0 + y3 * S::SLP;
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
     const int c = c0 + 2 * q;

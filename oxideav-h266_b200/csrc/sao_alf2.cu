@@ -24,6 +24,7 @@ constexpr int NT = 256;
 template <int W>
 struct TrialSmem {
   static constexpr int SLW = W + 8, SLH = TH + 6;        // pre-ALF luma [X0-4, X1+4) x [Y0-3, Y1+3)
+  static constexpr int SLP = SLW;                         // its row pitch
   static constexpr int CW = W / 2 + 2, CH = TH / 2 + 2;  // 2x2 Laplacian cells
   alignas(16) uint16_t sL[SLH * SLW];
   alignas(16) uint4 cell[CH * CW];

@@ -50,6 +50,11 @@ struct Smem3 {
   static constexpr int CW = W / 2 + 2, CH = TH / 2 + 2;     // 2x2 Laplacian cells
   static constexpr int DCW = W / 2 + 16, DCH = TH / 2 + 6;  // deblocked chroma [x-8, x+8) x [y-3, y+3)
   static constexpr int SCW = W / 2 + 8, SCH = TH / 2 + 4;   // post-SAO chroma [x-4, x+4) x [y-2, y+2)
+  // Row pitches of the post-SAO windows: 4 samples past the widths, so that
+  // the chroma-phase threads (8 chroma rows of 4 runs per warp) reading luma
+  // rows 2 apart, or chroma rows 1 apart, spread over more shared-memory
+  // banks; multiples of 4 samples keep the 8-byte row alignment.
+  static constexpr int SLP = SLW + 4, SCP = SCW + 4;
   static constexpr int DL_BYTES = DLH * DLW * 2, DC_BYTES = DCH * DCW * 2;
   static constexpr int DC_OFF = (DL_BYTES + 127) & ~127;
   static constexpr int DC_STRIDE = (DC_BYTES + 127) & ~127;
@@ -59,8 +64,8 @@ struct Smem3 {
   // the deblocked windows (TMA destinations); the Laplacian cells reuse the
   // space once the post-SAO windows exist
   alignas(128) uint8_t u[U_BYTES];
-  alignas(16) uint16_t sL[SLH * SLW];
-  alignas(16) uint16_t sC[2][SCH * SCW];
+  alignas(16) uint16_t sL[SLH * SLP];
+  alignas(16) uint16_t sC[2][SCH * SCP];
   uint8_t cls_f[(TH / 4) * (W / 4)], cls_t[(TH / 4) * (W / 4)];
   SaoLocal sao[3][9];
   alignas(8) unsigned long long bar;
@@ -413,14 +418,14 @@ __device__ __forceinline__ bool sao_alf_tile3(const Pass2Args &a, const Pass2Arg
         const FastRect &f = fr[0];
         const int r = f.row_of((uint32_t)i), x = f.x0 + 2 * (i - r * f.npx), y = f.y0 + r;
         const uint16_t *d = dL + (y - (Y0 - 4)) * S::DLW + (x - (X0 - 8));
-        st32(&sm.sL[(y - (Y0 - 3)) * S::SLW + (x - (X0 - 4))], sao_pair(fs[0], d, maxv2));
+        st32(&sm.sL[(y - (Y0 - 3)) * S::SLP + (x - (X0 - 4))], sao_pair(fs[0], d, maxv2));
       } else {
         const int cc = i < nf0 + nf1 ? 0 : 1;
         const int j = i - nf0 - (cc ? nf1 : 0);
         const FastRect &f = fr[1 + cc];
         const int r = f.row_of((uint32_t)j), x = f.x0 + 2 * (j - r * f.npx), y = f.y0 + r;
         const uint16_t *d = sm.dC(cc) + (y - (yc0 - 3)) * S::DCW + (x - (xc0 - 8));
-        st32(&sm.sC[cc][(y - (yc0 - 2)) * S::SCW + (x - (xc0 - 4))], sao_pair(fs[1 + cc], d, maxv2));
+        st32(&sm.sC[cc][(y - (yc0 - 2)) * S::SCP + (x - (xc0 - 4))], sao_pair(fs[1 + cc], d, maxv2));
       }
     }
     // the rest sample by sample: neighbouring CTBs, clamped positions, edges of the clip rectangle
@@ -438,7 +443,7 @@ __device__ __forceinline__ bool sao_alf_tile3(const Pass2Args &a, const Pass2Arg
           const SaoLocal &p = sm.sao[0][((ay >> log2) - ry + 1) * 3 + ((ax >> log2) - rx + 1)];
           if (p.type) v = sao_one(p, ax, ay, maxv, d);
         }
-        sm.sL[(y - (Y0 - 3)) * S::SLW + (x - (X0 - 4))] = (uint16_t)v;
+        sm.sL[(y - (Y0 - 3)) * S::SLP + (x - (X0 - 4))] = (uint16_t)v;
       } else {
         const int cc = i < ns0 + ns1 ? 0 : 1;
         const int j = i - ns0 - (cc ? ns1 : 0);
@@ -452,7 +457,7 @@ __device__ __forceinline__ bool sao_alf_tile3(const Pass2Args &a, const Pass2Arg
           const SaoLocal &p = sm.sao[cc + 1][(((ay * 2) >> log2) - ry + 1) * 3 + (((ax * 2) >> log2) - rx + 1)];
           if (p.type) v = sao_one(p, ax, ay, maxv, d);
         }
-        sm.sC[cc][(y - (yc0 - 2)) * S::SCW + (x - (xc0 - 4))] = (uint16_t)v;
+        sm.sC[cc][(y - (yc0 - 2)) * S::SCP + (x - (xc0 - 4))] = (uint16_t)v;
       }
     }
   }
@@ -475,7 +480,7 @@ __device__ __forceinline__ bool sao_alf_tile3(const Pass2Args &a, const Pass2Arg
       const int ccf = (DO_ALF && me) ? me->cc_filt[cc] : -1;
       const int ctb_c = ctb / 2, y_ctb_c = y_ctb / 2;
       const int c0 = i0 + 4;
-      const uint16_t *R0 = &sm.sC[cc][(jj + 2) * S::SCW + c0];
+      const uint16_t *R0 = &sm.sC[cc][(jj + 2) * S::SCP + c0];
       int v[SPT];
       {
         Words<NP + 2, 1> w0;
@@ -523,11 +528,11 @@ __device__ __forceinline__ bool sao_alf_tile3(const Pass2Args &a, const Pass2Arg
         using I1 = std::integral_constant<int, 1>;
         using Im1 = std::integral_constant<int, -1>;
         using I2 = std::integral_constant<int, 2>;
-        load_words<NP + 2, 1, (NP > 1)>(ra, R0 + y2 * S::SCW, 1, NP + 1);
-        load_words<NP + 2, 1, (NP > 1)>(rb, R0 - y2 * S::SCW, 1, NP + 1);
+        load_words<NP + 2, 1, (NP > 1)>(ra, R0 + y2 * S::SCP, 1, NP + 1);
+        load_words<NP + 2, 1, (NP > 1)>(rb, R0 - y2 * S::SCP, 1, NP + 1);
         tap(ra, rb, I0{}, 0);
-        load_words<NP + 2, 1, (NP > 1)>(ra, R0 + y1 * S::SCW, 0, NP + 2);
-        load_words<NP + 2, 1, (NP > 1)>(rb, R0 - y1 * S::SCW, 0, NP + 2);
+        load_words<NP + 2, 1, (NP > 1)>(ra, R0 + y1 * S::SCP, 0, NP + 2);
+        load_words<NP + 2, 1, (NP > 1)>(rb, R0 - y1 * S::SCP, 0, NP + 2);
         tap(ra, rb, I1{}, 1);
         tap(ra, rb, I0{}, 2);
         tap(ra, rb, Im1{}, 3);
@@ -554,26 +559,24 @@ __device__ __forceinline__ bool sao_alf_tile3(const Pass2Args &a, const Pass2Arg
           else if (yline == ctb - 6 || yline == ctb - 3) { yp2 = 1; }
         }
         // luma words of the run: word k = samples (2 i0 + 2 + 2k, +1) of a window row (col 2 i0 + 4 = luma x of i0)
-        const uint16_t *L0 = &sm.sL[(2 * jj + 3) * S::SLW + 2 * i0 + 4];
+        const uint16_t *L0 = &sm.sL[(2 * jj + 3) * S::SLP + 2 * i0 + 4];
+        // 8-byte loads for word pairs (k, k + 1), k odd (L0 is 8-byte aligned when SPT > 2)
         constexpr int LW = SPT + 1;
-        uint32_t wt[LW], wm[LW], wb[LW], w2[LW];
-#pragma unroll
-        for (int k = 0; k < LW; ++k) {
-          wt[k] = ld32(L0 - yp1 * S::SLW - 2 + 2 * k);
-          wm[k] = ld32(L0 - 2 + 2 * k);
-          wb[k] = ld32(L0 + yp1 * S::SLW - 2 + 2 * k);
-          w2[k] = ld32(L0 + yp2 * S::SLW - 2 + 2 * k);
-        }
+        Words<LW, 1> wt, wm, wb, w2;
+        load_words<LW, 1, (SPT > 2)>(wt, L0 - yp1 * S::SLP, 0, LW);
+        load_words<LW, 1, (SPT > 2)>(wm, L0, 0, LW);
+        load_words<LW, 1, (SPT > 2)>(wb, L0 + yp1 * S::SLP, 0, LW);
+        load_words<LW, 1, (SPT > 2)>(w2, L0 + yp2 * S::SLP, 0, LW);
 #pragma unroll
         for (int k = 0; k < SPT; ++k) {
           // chroma sample k: luma (2k - 1, 2k) in word k, (2k, 2k + 1) in word k + 1
-          int s = __dp2a_lo((int)wt[k + 1], (int)k1, 0);
-          s = __dp2a_hi((int)wm[k], (int)k1, s);
-          s = __dp2a_lo((int)wm[k + 1], (int)k2, s);
-          s = __dp2a_hi((int)wb[k], (int)k2, s);
-          s = __dp2a_lo((int)wb[k + 1], (int)k3, s);
-          s = __dp2a_hi((int)w2[k + 1], (int)k3, s);
-          const int ctr = (int)(wm[k + 1] & 0xFFFF);
+          int s = __dp2a_lo((int)wt.w[k + 1], (int)k1, 0);
+          s = __dp2a_hi((int)wm.w[k], (int)k1, s);
+          s = __dp2a_lo((int)wm.w[k + 1], (int)k2, s);
+          s = __dp2a_hi((int)wb.w[k], (int)k2, s);
+          s = __dp2a_lo((int)wb.w[k + 1], (int)k3, s);
+          s = __dp2a_hi((int)w2.w[k + 1], (int)k3, s);
+          const int ctr = (int)(wm.w[k + 1] & 0xFFFF);
           s -= ctr * csum;
           v[k] = clampd(v[k] + clampd((s + 64) >> 7, -half, half - 1), 0, maxv);
         }
@@ -606,7 +609,7 @@ __device__ __forceinline__ bool sao_alf_tile3(const Pass2Args &a, const Pass2Arg
       const int j = p / (W / 4), i = (p % (W / 4)) * 4;
       const int gx = X0 + i, gy = Y0 + j;
       if (gy >= LD.h || gx >= LD.w) continue;
-      const uint2 v = ld64(&sm.sL[(j + 3) * S::SLW + i + 4]);
+      const uint2 v = ld64(&sm.sL[(j + 3) * S::SLP + i + 4]);
       uint16_t *out = LD.s + (int64_t)gy * LD.stride + gx;
       if (gx + 4 <= LD.w && ((uintptr_t)out & 7) == 0) {
         *reinterpret_cast<uint2 *>(out) = v;
@@ -646,7 +649,7 @@ __device__ __forceinline__ bool sao_alf_tile3(const Pass2Args &a, const Pass2Arg
     if (gy >= LD.h || gx >= LD.w) continue;
     int shift, y1, y2, y3;
     table45(gy - y_ctb, ctb, shift, y1, y2, y3);
-    const uint16_t *R0 = &sm.sL[(j + 3) * S::SLW + 4 * bx + 4];
+    const uint16_t *R0 = &sm.sL[(j + 3) * S::SLP + 4 * bx + 4];
     int acc[4] = {0, 0, 0, 0};
     uint32_t cur[2], ncur[2];
     // words k of a row: samples (c0 - 4 + 2k, +1), c0 = the run's first sample
@@ -677,16 +680,16 @@ __device__ __forceinline__ bool sao_alf_tile3(const Pass2Args &a, const Pass2Arg
     tap(ru, ru, I3{}, 9);
     tap(ru, ru, I2{}, 10);
     tap(ru, ru, I1{}, 11);
-    load_words<6, 2, true>(ru, R0 + y3 * S::SLW, 2, 4);
-    load_words<6, 2, true>(rd, R0 - y3 * S::SLW, 2, 4);
+    load_words<6, 2, true>(ru, R0 + y3 * S::SLP, 2, 4);
+    load_words<6, 2, true>(rd, R0 - y3 * S::SLP, 2, 4);
     tap(ru, rd, I0{}, 0);
-    load_words<6, 2, true>(ru, R0 + y2 * S::SLW, 1, 5);
-    load_words<6, 2, true>(rd, R0 - y2 * S::SLW, 1, 5);
+    load_words<6, 2, true>(ru, R0 + y2 * S::SLP, 1, 5);
+    load_words<6, 2, true>(rd, R0 - y2 * S::SLP, 1, 5);
     tap(ru, rd, I1{}, 1);
     tap(ru, rd, I0{}, 2);
     tap(ru, rd, Im1{}, 3);
-    load_words<6, 2, true>(ru, R0 + y1 * S::SLW, 1, 5);
-    load_words<6, 2, true>(rd, R0 - y1 * S::SLW, 1, 5);
+    load_words<6, 2, true>(ru, R0 + y1 * S::SLP, 1, 5);
+    load_words<6, 2, true>(rd, R0 - y1 * S::SLP, 1, 5);
     tap(ru, rd, I2{}, 4);
     tap(ru, rd, I1{}, 5);
     tap(ru, rd, I0{}, 6);
