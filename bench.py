@@ -46,12 +46,12 @@ WIDTH, HEIGHT, BITDEPTH = 1920, 1080, 10
 METRIC = "filter-chain Mpx/s 1080p/2160p 10-bit bit-exact"
 # From one ncu capture of the batched SAO/ALF launch (k_sao_alf_tiles_batch
 # <64, 64, 1, 1>) over 4 pictures of this workload: DRAM bytes read + written
-# (25 689 600 + 1 112 832 B; ncu flushes the caches before the launch, and the
+# (25 679 616 + 1 021 696 B; ncu flushes the caches before the launch, and the
 # output planes retire from L2 after it) and thread instructions per luma pixel
-# (thread_inst_executed); the bench line scales them to its own batch
-# and labels them so.
-SAO_ALF_TRAFFIC_PER_PX = (25689600 + 1112832) / (4 * 1920 * 1080)
-SAO_ALF_THREAD_INST_PER_PX = 332.5  # 2 757 985 962 thread instructions / 4 pictures
+# (warp instructions x threads per warp instruction); the bench line scales
+# them to its own batch and labels them so.
+SAO_ALF_TRAFFIC_PER_PX = (25679616 + 1021696) / (4 * 1920 * 1080)
+SAO_ALF_THREAD_INST_PER_PX = 332.6  # 87 940 862 warp instructions x 31.37 threads / 4 pictures
 
 
 def _import_pkg():
