@@ -1851,6 +1851,7 @@ int h266_lmcs_forward_map_luma_rects(h266_ctx *ctx, h266_picture *pic, const h26
   if (!lmcs) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL lmcs");
   H266_TRY(check_lmcs(lmcs, 0, 0));
   if (n && !rects) return set_error(H266_ERR_INVALID_ARGUMENT, "NULL rects with nonzero length");
+  if (n > (1ull << 28)) return set_error(H266_ERR_UNSUPPORTED, "too many rectangles");
   const uint32_t W = pic->luma.width, H = pic->luma.height;
   // Rectangles clipped as src/ctu.rs:1718-1719; the grid is the coarsest that
   // every clipped edge lies on, the span box their union's bounds.
@@ -1873,13 +1874,14 @@ int h266_lmcs_forward_map_luma_rects(h266_ctx *ctx, h266_picture *pic, const h26
   const uint32_t sh = grid_shift(acc);
   // Pieces of at most kPieceCells cells, split at rows of the grid.
   for (size_t i = 0, e = pieces.size(); i < e; ++i) {
-    RectPiece &r = pieces[i];
+    const RectPiece r = pieces[i];  // a copy: the appends below may move the array
     const uint32_t cols = r.w >> sh, rows = r.h >> sh;
     if ((uint64_t)cols * rows <= kPieceCells) continue;
     const uint32_t step = std::max<uint32_t>(1, kPieceCells / cols) << sh;
     for (uint32_t y = step; y < r.h; y += step)
       pieces.push_back(RectPiece{r.x, r.y + y, r.w, std::min(step, r.h - y)});
     pieces[i].h = step;
+    if (pieces.size() > (1ull << 30)) return set_error(H266_ERR_UNSUPPORTED, "rectangles too large");
   }
   Guard g(ctx->device);
   Lane &ln = ctx->main;
