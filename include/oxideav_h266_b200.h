@@ -432,7 +432,8 @@ typedef struct h266_chroma_res_block { /* one chroma TB of the inter residual ad
  * folded by lmcs_scale_chroma_residuals (src/ctu.rs:734-742, eqs. 1219/1220)
  * when it has a varScale, is added to the plane with Clip1, TB by TB in list
  * order (overlapping TBs add in order).  `res` is host memory for
- * H266_MEM_HOST pictures and device memory for H266_MEM_DEVICE ones. */
+ * H266_MEM_HOST pictures and device memory for H266_MEM_DEVICE ones.  Waits
+ * for the context stream. */
 int h266_lmcs_add_chroma_residual(h266_ctx *ctx, h266_picture *pic, uint32_t bit_depth, const int32_t *res,
                                   uint64_t n_res, const h266_chroma_res_block *blocks, uint64_t n);
 
