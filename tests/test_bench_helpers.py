@@ -1,7 +1,8 @@
-"""The measurement helpers of bench.py that need no GPU: the clock-record
-rejection rule, the per-plane parity records (a mistake planted in the
-oracle's output is caught), their summary over legs, and the integer-issue
-roofline arithmetic against a stand-in device with the B200's SM count."""
+"""The measurement helpers of bench.py that need no GPU: the clock sampler's
+reading of nvidia-smi lines and the clock-record rejection rule, the
+per-plane parity records (a mistake planted in the oracle's output is
+caught), their summary over legs, and the integer-issue roofline arithmetic
+against a stand-in device with the B200's SM count."""
 import types
 
 import numpy as np
@@ -80,3 +81,29 @@ def test_workload_config_names_the_benchmark_batch():
     c = bench.workload_config(32, 1)
     assert c["workload"] == "c2_1080p10_x32" and (c["width"], c["height"], c["bit_depth"]) == (1920, 1080, 10)
     assert c["parallelism"] == "replicas x1" and "larger than L2" in c["l2"]
+
+
+def test_clock_sampler_summary_reads_this_gpus_lines_after_the_priming_ones():
+    s = bench.ClockSampler("GPU-aaa")
+    s.proc = object()  # stands for the nvidia-smi process; summary() only reads the file
+    lines = ["GPU-aaa, 900, 1965, 120.5, 0x0, Not Active, Not Active, Not Active, Not Active",  # before the timed region
+             "GPU-aaa, 1965, 1965, 650.0, 0x0, Not Active, Not Active, Not Active, Not Active",
+             "GPU-bbb, 300, 1965, 90.0, 0x0, Active, Not Active, Not Active, Not Active",  # another GPU of the host
+             "GPU-aaa, 1905, 1965, 990.0, 0x4, Not Active, Not Active, Not Active, Active",
+             "GPU-aaa, 1935, 1965, 700.0, 0x0, Not Active, Not Active, Not Active, Not Active",
+             "garbage"]
+    s.path.write_text("\n".join(lines) + "\n")
+    s.skip = 1
+    c = s.summary()
+    assert c["samples"] == 3 and c["sm_mhz"] == 1935.0 and c["sm_max_mhz"] == 1965.0
+    assert c["reasons"] == ["sw_power_cap"] and c["power_w_max"] == 990.0
+    assert not bench.bad_clocks(c)
+    assert not s.path.exists()
+
+
+def test_clock_sampler_without_samples_says_so():
+    s = bench.ClockSampler("GPU-aaa")
+    assert s.summary()["reasons"] == ["nvidia-smi unavailable"]
+    s.proc = object()
+    s.path.write_text("")
+    assert s.summary()["reasons"] == ["no samples"]
